@@ -1,0 +1,1016 @@
+/*
+ * fe_oracle.c -- TEST INFRASTRUCTURE ONLY: CPU FP64 restatement of the reference substep.
+ *
+ * Loaded by the tests, the smoke check and the CPU-baseline leg of bench.py as the checker of the
+ * CUDA path; never part of the product.  Compiled with -ffp-contract=off so that every multiply and
+ * add rounds separately, exactly as the reference's x86-64 build does.
+ *
+ * Reference file:line citations are relative to the reference project's src/ directory.
+ */
+#include "fe_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../fluide_engine_b200/csrc/fe_keys.h"
+#include "../fluide_engine_b200/csrc/fe_seed.h"
+
+/* Collider SDF value with no colliders (3d/collider_collection.cpp:3,38). */
+#define OR_MAX_DISTANCE 1.7976931348623157E+30
+
+typedef struct {
+    int x, y, z;
+} dim3i;
+
+static inline size_t ix3(dim3i d, int i, int j, int k) { return (size_t)i + (size_t)d.x * ((size_t)j + (size_t)d.y * (size_t)k); }
+static inline size_t cnt3(dim3i d) { return (size_t)d.x * (size_t)d.y * (size_t)d.z; }
+
+struct or_sim {
+    or_desc d;
+    dim3i n;                 /* cells */
+    dim3i du, dv, dw;        /* face array sizes */
+    double h[3];             /* gridSpacing = domainSize / gridSize (hybrid_simulator.cpp:8) */
+    double xo[3], yo[3], zo[3];       /* velocity-grid data origins */
+    double rxo[3], ryo[3], rzo[3];    /* FLIP residual-grid data origins */
+    double sdf_origin[3];    /* domain origin + h/2 (hybrid_simulator.cpp:15) */
+    size_t np;
+    double *pos, *vel, *C;   /* AoS: 3, 3, 9 doubles per particle; C rows cX, cY, cZ */
+    double *u, *v, *w;
+    double *su, *sv, *sw;    /* FLIPSimulator::_velocityResiduals */
+    uint8_t *mu, *mv, *mw;   /* Fluid3::xMarkers/yMarkers/zMarkers */
+    double* sdf;             /* Fluid3::sdf */
+    uint8_t* marks;          /* SinglePhasePressureSolver::_fluidMarkers */
+    double* p;               /* LinearSystem::x, kept between substeps (linear_system.cpp:13-18) */
+    double* b;               /* LinearSystem::b */
+    int cg_it;
+    double cg_res;
+};
+
+/* ---------------------------------------------------------------- math_utils.hpp restatements */
+
+/* Clamp(val, maxVal, minVal) (common/math_utils.hpp:13-28). */
+static inline double clampd(double val, double maxv, double minv)
+{
+    if (val < minv) return minv;
+    if (val > maxv) return maxv;
+    return val;
+}
+
+/* Lerp (common/math_utils.hpp:30-34). */
+double or_lerp(double a, double b, double f) { return (1 - f) * a + f * b; }
+
+/* Trilerp via Bilerp (common/math_utils.hpp:36-46). c = x000,x100,x010,x110,x001,x101,x011,x111. */
+double or_trilerp(const double c[8], double fx, double fy, double fz)
+{
+    double b0 = or_lerp(or_lerp(c[0], c[1], fx), or_lerp(c[2], c[3], fx), fy);
+    double b1 = or_lerp(or_lerp(c[4], c[5], fx), or_lerp(c[6], c[7], fx), fy);
+    return or_lerp(b0, b1, fz);
+}
+
+/* GetBarycentric with iLow = 0 (common/math_utils.hpp:48-73). */
+static inline void barycentric(double x, int iHigh, int* i, double* f)
+{
+    double s = floor(x);
+    int ii = (int)s;
+    if (0 == iHigh) {
+        ii = 0;
+        *f = 0;
+    } else if (ii < 0) {
+        ii = 0;
+        *f = 0;
+    } else if (ii > iHigh - 1) {
+        ii = iHigh - 1;
+        *f = 1;
+    } else {
+        *f = x - s;
+    }
+    *i = ii;
+}
+
+typedef struct {
+    int i[8], j[8], k[8];
+} idx8;
+
+/* GetCooridnatesAndWeights (common/math_utils.hpp:75-112). */
+static void coords_weights(dim3i size, const double origin[3], const double h[3], const double x[3], idx8* id,
+                           double w[8])
+{
+    int i, j, k;
+    double fx, fy, fz;
+    double nx = (x[0] - origin[0]) / h[0], ny = (x[1] - origin[1]) / h[1], nz = (x[2] - origin[2]) / h[2];
+    barycentric(nx, size.x - 1, &i, &fx);
+    barycentric(ny, size.y - 1, &j, &fy);
+    barycentric(nz, size.z - 1, &k, &fz);
+    int ip1 = i + 1 < size.x - 1 ? i + 1 : size.x - 1;
+    int jp1 = j + 1 < size.y - 1 ? j + 1 : size.y - 1;
+    int kp1 = k + 1 < size.z - 1 ? k + 1 : size.z - 1;
+    const int ii[8] = {i, ip1, i, ip1, i, ip1, i, ip1};
+    const int jj[8] = {j, j, jp1, jp1, j, j, jp1, jp1};
+    const int kk[8] = {k, k, k, k, kp1, kp1, kp1, kp1};
+    for (int t = 0; t < 8; ++t) {
+        id->i[t] = ii[t];
+        id->j[t] = jj[t];
+        id->k[t] = kk[t];
+    }
+    w[0] = (1.00 - fx) * (1.00 - fy) * (1.00 - fz);
+    w[1] = fx * (1.00 - fy) * (1.00 - fz);
+    w[2] = (1.00 - fx) * fy * (1.00 - fz);
+    w[3] = fx * fy * (1.00 - fz);
+    w[4] = (1.00 - fx) * (1.00 - fy) * fz;
+    w[5] = fx * (1.00 - fy) * fz;
+    w[6] = (1.00 - fx) * fy * fz;
+    w[7] = fx * fy * fz;
+}
+
+/* GetCooridnatesAndGradientWeights (common/math_utils.hpp:114-176); g[t][0..2] per corner. */
+static void coords_grad_weights(dim3i size, const double origin[3], const double h[3], const double x[3], idx8* id,
+                                double g[8][3])
+{
+    int i, j, k;
+    double fx, fy, fz;
+    double nx = (x[0] - origin[0]) / h[0], ny = (x[1] - origin[1]) / h[1], nz = (x[2] - origin[2]) / h[2];
+    double ihx = 1 / h[0], ihy = 1 / h[1], ihz = 1 / h[2];
+    barycentric(nx, size.x - 1, &i, &fx);
+    barycentric(ny, size.y - 1, &j, &fy);
+    barycentric(nz, size.z - 1, &k, &fz);
+    int ip1 = i + 1 < size.x - 1 ? i + 1 : size.x - 1;
+    int jp1 = j + 1 < size.y - 1 ? j + 1 : size.y - 1;
+    int kp1 = k + 1 < size.z - 1 ? k + 1 : size.z - 1;
+    const int ii[8] = {i, ip1, i, ip1, i, ip1, i, ip1};
+    const int jj[8] = {j, j, jp1, jp1, j, j, jp1, jp1};
+    const int kk[8] = {k, k, k, k, kp1, kp1, kp1, kp1};
+    for (int t = 0; t < 8; ++t) {
+        id->i[t] = ii[t];
+        id->j[t] = jj[t];
+        id->k[t] = kk[t];
+    }
+    g[0][0] = -ihx * (1 - fy) * (1 - fz);
+    g[0][1] = -ihy * (1 - fx) * (1 - fz);
+    g[0][2] = -ihz * (1 - fx) * (1 - fy);
+    g[1][0] = ihx * (1 - fy) * (1 - fz);
+    g[1][1] = fx * (-ihy) * (1 - fz);
+    g[1][2] = fx * (1 - fy) * (-ihz);
+    g[2][0] = (-ihx) * fy * (1 - fz);
+    g[2][1] = (1 - fx) * ihy * (1 - fz);
+    g[2][2] = (1 - fx) * fy * (-ihz);
+    g[3][0] = ihx * fy * (1 - fz);
+    g[3][1] = fx * ihy * (1 - fz);
+    g[3][2] = fx * fy * (-ihz);
+    g[4][0] = (-ihx) * (1 - fy) * fz;
+    g[4][1] = (1 - fx) * (-ihy) * fz;
+    g[4][2] = (1 - fx) * (1 - fy) * ihz;
+    g[5][0] = ihx * (1 - fy) * fz;
+    g[5][1] = fx * (-ihy) * fz;
+    g[5][2] = fx * (1 - fy) * ihz;
+    g[6][0] = (-ihx) * fy * fz;
+    g[6][1] = (1 - fx) * ihy * fz;
+    g[6][2] = (1 - fx) * fy * ihz;
+    g[7][0] = ihx * fy * fz;
+    g[7][1] = fx * ihy * fz;
+    g[7][2] = fx * fy * ihz;
+}
+
+/* Clamped trilinear sample shared by FaceCenteredGrid3D::SampleArray
+ * (grid_systems/face_centered_grid3d.cpp:339-371) and ScalarGrid3D::Sample (3d/scalar_grid3d.cpp:33-65). */
+static double sample3(const double* arr, dim3i size, const double origin[3], const double h[3], const double pos[3])
+{
+    int i, j, k;
+    double fx, fy, fz;
+    double nx = (pos[0] - origin[0]) / h[0], ny = (pos[1] - origin[1]) / h[1], nz = (pos[2] - origin[2]) / h[2];
+    barycentric(nx, size.x - 1, &i, &fx);
+    barycentric(ny, size.y - 1, &j, &fy);
+    barycentric(nz, size.z - 1, &k, &fz);
+    int ip1 = i + 1 < size.x - 1 ? i + 1 : size.x - 1;
+    int jp1 = j + 1 < size.y - 1 ? j + 1 : size.y - 1;
+    int kp1 = k + 1 < size.z - 1 ? k + 1 : size.z - 1;
+    double c[8] = {arr[ix3(size, i, j, k)],   arr[ix3(size, ip1, j, k)],   arr[ix3(size, i, jp1, k)],
+                   arr[ix3(size, ip1, jp1, k)], arr[ix3(size, i, j, kp1)],   arr[ix3(size, ip1, j, kp1)],
+                   arr[ix3(size, i, jp1, kp1)], arr[ix3(size, ip1, jp1, kp1)]};
+    return or_trilerp(c, fx, fy, fz);
+}
+
+double or_sample_face_array(const double* arr, const int size[3], const double origin[3], const double h[3],
+                            const double pos[3])
+{
+    dim3i d = {size[0], size[1], size[2]};
+    return sample3(arr, d, origin, h, pos);
+}
+
+double or_scalar_sample(const double* arr, const int size[3], const double origin[3], const double h[3],
+                        const double pos[3])
+{
+    dim3i d = {size[0], size[1], size[2]};
+    return sample3(arr, d, origin, h, pos);
+}
+
+/* ExtrapolateToRegion (common/math_utils.hpp:186-253). */
+static void extrapolate_to_region(const double* input, const uint8_t* valid, dim3i size, size_t iters, double* output)
+{
+    size_t n = cnt3(size);
+    uint8_t* valid0 = (uint8_t*)malloc(n);
+    uint8_t* valid1 = (uint8_t*)malloc(n);
+    memcpy(valid0, valid, n);
+    memcpy(valid1, valid, n);
+    if (output != input) memcpy(output, input, n * sizeof(double));
+    for (size_t it = 0; it < iters; ++it) {
+        for (int i = 0; i < size.x; ++i)
+            for (int j = 0; j < size.y; ++j)
+                for (int k = 0; k < size.z; ++k) {
+                    size_t c = ix3(size, i, j, k);
+                    if (!valid0[c]) {
+                        double sum = 0;
+                        unsigned count = 0;
+                        if (i + 1 < size.x && valid0[ix3(size, i + 1, j, k)]) { sum += output[ix3(size, i + 1, j, k)]; ++count; }
+                        if (i > 0 && valid0[ix3(size, i - 1, j, k)]) { sum += output[ix3(size, i - 1, j, k)]; ++count; }
+                        if (j + 1 < size.y && valid0[ix3(size, i, j + 1, k)]) { sum += output[ix3(size, i, j + 1, k)]; ++count; }
+                        if (j > 0 && valid0[ix3(size, i, j - 1, k)]) { sum += output[ix3(size, i, j - 1, k)]; ++count; }
+                        if (k + 1 < size.z && valid0[ix3(size, i, j, k + 1)]) { sum += output[ix3(size, i, j, k + 1)]; ++count; }
+                        if (k > 0 && valid0[ix3(size, i, j, k - 1)]) { sum += output[ix3(size, i, j, k - 1)]; ++count; }
+                        if (count > 0) {
+                            output[c] = sum / count;
+                            valid1[c] = 1;
+                        }
+                    } else {
+                        valid1[c] = 1;
+                    }
+                }
+        /* valid0.Swap(valid1): valid0 takes the grown mask, valid1 the previous one. */
+        uint8_t* t = valid0;
+        valid0 = valid1;
+        valid1 = t;
+    }
+    free(valid0);
+    free(valid1);
+}
+
+/* ---------------------------------------------------------------- construction */
+
+static void* xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
+
+or_sim* or_create(const or_desc* d)
+{
+    if (!d || d->n[0] < 2 || d->n[1] < 2 || d->n[2] < 2) return NULL;
+    or_sim* s = (or_sim*)calloc(1, sizeof(or_sim));
+    s->d = *d;
+    s->n = (dim3i){d->n[0], d->n[1], d->n[2]};
+    s->du = (dim3i){d->n[0] + 1, d->n[1], d->n[2]};
+    s->dv = (dim3i){d->n[0], d->n[1] + 1, d->n[2]};
+    s->dw = (dim3i){d->n[0], d->n[1], d->n[2] + 1};
+    for (int a = 0; a < 3; ++a) s->h[a] = d->size[a] / (double)d->n[a]; /* hybrid_simulator.cpp:8 */
+    /* FaceCenteredGrid3D::CalculateDataOrigins (grid_systems/face_centered_grid3d.cpp:324-332) runs inside
+     * SetGridSpacing before SetOrigin (hybrid_simulator.cpp:11-12), and Grid3D::SetOrigin does not recompute
+     * them, so the velocity grid's data origins are taken from origin (0,0,0).  The FLIP residual grid is
+     * constructed with the domain origin (flip_simulator.cpp:5). */
+    const double zero[3] = {0, 0, 0};
+    const double* o = zero;
+    s->xo[0] = o[0] + s->h[0] * 0;
+    s->xo[1] = o[1] + s->h[1] * 0.5;
+    s->xo[2] = o[2] + s->h[2] * 0.5;
+    s->yo[0] = o[0] + s->h[0] * 0.5;
+    s->yo[1] = o[1] + s->h[1] * 0;
+    s->yo[2] = o[2] + s->h[2] * 0.5;
+    s->zo[0] = o[0] + s->h[0] * 0.5;
+    s->zo[1] = o[1] + s->h[1] * 0.5;
+    s->zo[2] = o[2] + s->h[2] * 0;
+    o = d->origin;
+    s->rxo[0] = o[0] + s->h[0] * 0;
+    s->rxo[1] = o[1] + s->h[1] * 0.5;
+    s->rxo[2] = o[2] + s->h[2] * 0.5;
+    s->ryo[0] = o[0] + s->h[0] * 0.5;
+    s->ryo[1] = o[1] + s->h[1] * 0;
+    s->ryo[2] = o[2] + s->h[2] * 0.5;
+    s->rzo[0] = o[0] + s->h[0] * 0.5;
+    s->rzo[1] = o[1] + s->h[1] * 0.5;
+    s->rzo[2] = o[2] + s->h[2] * 0;
+    for (int a = 0; a < 3; ++a) s->sdf_origin[a] = d->origin[a] + s->h[a] / 2.0;
+    size_t nc = cnt3(s->n);
+    s->u = (double*)xcalloc(cnt3(s->du), sizeof(double));
+    s->v = (double*)xcalloc(cnt3(s->dv), sizeof(double));
+    s->w = (double*)xcalloc(cnt3(s->dw), sizeof(double));
+    s->su = (double*)xcalloc(cnt3(s->du), sizeof(double));
+    s->sv = (double*)xcalloc(cnt3(s->dv), sizeof(double));
+    s->sw = (double*)xcalloc(cnt3(s->dw), sizeof(double));
+    s->mu = (uint8_t*)xcalloc(cnt3(s->du), 1);
+    s->mv = (uint8_t*)xcalloc(cnt3(s->dv), 1);
+    s->mw = (uint8_t*)xcalloc(cnt3(s->dw), 1);
+    s->sdf = (double*)xcalloc(nc, sizeof(double));
+    s->marks = (uint8_t*)xcalloc(nc, 1);
+    s->p = (double*)xcalloc(nc, sizeof(double));
+    s->b = (double*)xcalloc(nc, sizeof(double));
+    return s;
+}
+
+void or_destroy(or_sim* s)
+{
+    if (!s) return;
+    free(s->pos); free(s->vel); free(s->C);
+    free(s->u); free(s->v); free(s->w);
+    free(s->su); free(s->sv); free(s->sw);
+    free(s->mu); free(s->mv); free(s->mw);
+    free(s->sdf); free(s->marks); free(s->p); free(s->b);
+    free(s);
+}
+
+int or_set_particles(or_sim* s, size_t n, const double* pos, const double* vel, const double* C)
+{
+    free(s->pos); free(s->vel); free(s->C);
+    s->np = n;
+    s->pos = (double*)xcalloc(3 * n, sizeof(double));
+    s->vel = (double*)xcalloc(3 * n, sizeof(double));
+    s->C = (double*)xcalloc(9 * n, sizeof(double));
+    if (pos) memcpy(s->pos, pos, 3 * n * sizeof(double));
+    if (vel) memcpy(s->vel, vel, 3 * n * sizeof(double));
+    if (C) memcpy(s->C, C, 9 * n * sizeof(double));
+    return 0;
+}
+
+size_t or_num_particles(const or_sim* s) { return s->np; }
+
+void or_get_particles(const or_sim* s, double* pos, double* vel, double* C)
+{
+    if (pos) memcpy(pos, s->pos, 3 * s->np * sizeof(double));
+    if (vel) memcpy(vel, s->vel, 3 * s->np * sizeof(double));
+    if (C) memcpy(C, s->C, 9 * s->np * sizeof(double));
+}
+
+void or_get_grid(const or_sim* s, double* u, double* v, double* w)
+{
+    if (u) memcpy(u, s->u, cnt3(s->du) * sizeof(double));
+    if (v) memcpy(v, s->v, cnt3(s->dv) * sizeof(double));
+    if (w) memcpy(w, s->w, cnt3(s->dw) * sizeof(double));
+}
+
+void or_set_grid(or_sim* s, const double* u, const double* v, const double* w)
+{
+    if (u) memcpy(s->u, u, cnt3(s->du) * sizeof(double));
+    if (v) memcpy(s->v, v, cnt3(s->dv) * sizeof(double));
+    if (w) memcpy(s->w, w, cnt3(s->dw) * sizeof(double));
+}
+
+void or_get_pressure(const or_sim* s, double* p) { memcpy(p, s->p, cnt3(s->n) * sizeof(double)); }
+void or_set_pressure(or_sim* s, const double* p) { memcpy(s->p, p, cnt3(s->n) * sizeof(double)); }
+void or_get_marks(const or_sim* s, uint8_t* m) { memcpy(m, s->marks, cnt3(s->n)); }
+void or_get_sdf(const or_sim* s, double* sdf) { memcpy(sdf, s->sdf, cnt3(s->n) * sizeof(double)); }
+void or_get_rhs(const or_sim* s, double* b) { memcpy(b, s->b, cnt3(s->n) * sizeof(double)); }
+
+void or_get_face_markers(const or_sim* s, uint8_t* mu, uint8_t* mv, uint8_t* mw)
+{
+    if (mu) memcpy(mu, s->mu, cnt3(s->du));
+    if (mv) memcpy(mv, s->mv, cnt3(s->dv));
+    if (mw) memcpy(mw, s->mw, cnt3(s->dw));
+}
+
+void or_get_snapshot(const or_sim* s, double* u, double* v, double* w)
+{
+    if (u) memcpy(u, s->su, cnt3(s->du) * sizeof(double));
+    if (v) memcpy(v, s->sv, cnt3(s->dv) * sizeof(double));
+    if (w) memcpy(w, s->sw, cnt3(s->dw) * sizeof(double));
+}
+
+/* ---------------------------------------------------------------- P2G */
+
+/* PICSimulator::TransferParticles2Grid (pic_simulator.cpp:356-437), FLIPSimulator (flip_simulator.cpp:25-119)
+ * and APICSimulator (apic_simulator.cpp:15-118).  PIC and APIC pass the CELL count as the clamp size
+ * (pic_simulator.cpp:389,397,405; apic_simulator.cpp:58,71,84), FLIP the face-array size (flip_simulator.cpp:58). */
+void or_stage_p2g(or_sim* s)
+{
+    size_t nu = cnt3(s->du), nv = cnt3(s->dv), nw = cnt3(s->dw);
+    double* uw = (double*)xcalloc(nu, sizeof(double));
+    double* vw = (double*)xcalloc(nv, sizeof(double));
+    double* ww = (double*)xcalloc(nw, sizeof(double));
+    memset(s->u, 0, nu * sizeof(double));
+    memset(s->v, 0, nv * sizeof(double));
+    memset(s->w, 0, nw * sizeof(double));
+    memset(s->mu, 0, nu);
+    memset(s->mv, 0, nv);
+    memset(s->mw, 0, nw);
+    const int flip = s->d.solver == OR_FLIP, apic = s->d.solver == OR_APIC;
+    dim3i szu = flip ? s->du : s->n, szv = flip ? s->dv : s->n, szw = flip ? s->dw : s->n;
+    const double* O = s->d.origin;
+    const double* S = s->d.size;
+    double hh[3] = {s->h[0] / 2.0, s->h[1] / 2.0, s->h[2] / 2.0}; /* apic_simulator.cpp:52 */
+    for (size_t pi = 0; pi < s->np; ++pi) {
+        const double* x = s->pos + 3 * pi;
+        const double* vel = s->vel + 3 * pi;
+        const double* cx = s->C + 9 * pi;
+        idx8 id;
+        double wt[8];
+        /* u */
+        double pc[3] = {x[0], x[1], x[2]};
+        if (apic) {
+            pc[1] = clampd(pc[1], O[1] + S[1] - hh[1], O[1] + hh[1]);
+            pc[2] = clampd(pc[2], O[2] + S[2] - hh[2], O[2] + hh[2]);
+        }
+        coords_weights(szu, s->xo, s->h, x, &id, wt);
+        for (int t = 0; t < 8; ++t) {
+            size_t f = ix3(s->du, id.i[t], id.j[t], id.k[t]);
+            double val = vel[0];
+            if (apic) {
+                double g0 = s->xo[0] + s->h[0] * (double)id.i[t];
+                double g1 = s->xo[1] + s->h[1] * (double)id.j[t];
+                double g2 = s->xo[2] + s->h[2] * (double)id.k[t];
+                double term = cx[0] * (g0 - pc[0]) + cx[1] * (g1 - pc[1]) + cx[2] * (g2 - pc[2]);
+                val = vel[0] + term;
+            }
+            s->u[f] += val * wt[t];
+            uw[f] += wt[t];
+            s->mu[f] = 1;
+        }
+        /* v */
+        pc[0] = x[0]; pc[1] = x[1]; pc[2] = x[2];
+        if (apic) {
+            pc[0] = clampd(pc[0], O[0] + S[0] - hh[0], O[0] + hh[0]);
+            pc[2] = clampd(pc[2], O[2] + S[2] - hh[2], O[2] + hh[2]);
+        }
+        coords_weights(szv, s->yo, s->h, x, &id, wt);
+        for (int t = 0; t < 8; ++t) {
+            size_t f = ix3(s->dv, id.i[t], id.j[t], id.k[t]);
+            double val = vel[1];
+            if (apic) {
+                const double* cy = cx + 3;
+                double g0 = s->yo[0] + s->h[0] * (double)id.i[t];
+                double g1 = s->yo[1] + s->h[1] * (double)id.j[t];
+                double g2 = s->yo[2] + s->h[2] * (double)id.k[t];
+                double term = cy[0] * (g0 - pc[0]) + cy[1] * (g1 - pc[1]) + cy[2] * (g2 - pc[2]);
+                val = vel[1] + term;
+            }
+            s->v[f] += val * wt[t];
+            vw[f] += wt[t];
+            s->mv[f] = 1;
+        }
+        /* w */
+        pc[0] = x[0]; pc[1] = x[1]; pc[2] = x[2];
+        if (apic) {
+            pc[0] = clampd(pc[0], O[0] + S[0] - hh[0], O[0] + hh[0]);
+            pc[1] = clampd(pc[1], O[1] + S[1] - hh[1], O[1] + hh[1]);
+        }
+        coords_weights(szw, s->zo, s->h, x, &id, wt);
+        for (int t = 0; t < 8; ++t) {
+            size_t f = ix3(s->dw, id.i[t], id.j[t], id.k[t]);
+            double val = vel[2];
+            if (apic) {
+                const double* cz = cx + 6;
+                double g0 = s->zo[0] + s->h[0] * (double)id.i[t];
+                double g1 = s->zo[1] + s->h[1] * (double)id.j[t];
+                double g2 = s->zo[2] + s->h[2] * (double)id.k[t];
+                double term = cz[0] * (g0 - pc[0]) + cz[1] * (g1 - pc[1]) + cz[2] * (g2 - pc[2]);
+                val = vel[2] + term;
+            }
+            s->w[f] += val * wt[t];
+            ww[f] += wt[t];
+            s->mw[f] = 1;
+        }
+    }
+    for (size_t f = 0; f < nu; ++f) if (uw[f] > 0.0) s->u[f] /= uw[f];
+    for (size_t f = 0; f < nv; ++f) if (vw[f] > 0.0) s->v[f] /= vw[f];
+    for (size_t f = 0; f < nw; ++f) if (ww[f] > 0.0) s->w[f] /= ww[f];
+    if (flip) { /* flip_simulator.cpp:107-118 */
+        memcpy(s->su, s->u, nu * sizeof(double));
+        memcpy(s->sv, s->v, nv * sizeof(double));
+        memcpy(s->sw, s->w, nw * sizeof(double));
+    }
+    free(uw); free(vw); free(ww);
+}
+
+/* ---------------------------------------------------------------- particle SDF */
+
+/* HashGridParticleSearcher::GetBucketIndex / GetHashKeyFromBucketIndex with a 64^3 table
+ * (particle_systems/hash_grid_particle_searcher.cpp:133-152, particle_system.cpp:30-34). */
+static inline int bucket_of(double x, double spacing) { return (int)floor(x / spacing); }
+static inline int wrap64(int b)
+{
+    /* int % size_t converts b to size_t first; for 64 this equals the non-negative modulo. */
+    return (int)((size_t)(long long)b % (size_t)64);
+}
+static inline size_t hash_key(int bx, int by, int bz)
+{
+    return (size_t)((wrap64(bz) * 64 + wrap64(by)) * 64 + wrap64(bx));
+}
+
+/* PICSimulator::BuildSignedDistanceField (pic_simulator.cpp:452-475) with HashGridParticleSearcher::Build and
+ * ForEachNearbyPoint (hash_grid_particle_searcher.cpp:14-32, 97-126, 154-204).  ExtrapolateIntoCollider
+ * (pic_simulator.cpp:497-519) is the identity with no colliders: every node is valid. */
+void or_stage_sdf(or_sim* s)
+{
+    double maxH = s->h[0] > (s->h[1] > s->h[2] ? s->h[1] : s->h[2]) ? s->h[0] : (s->h[1] > s->h[2] ? s->h[1] : s->h[2]);
+    double radious = 1.2 * maxH / sqrt(2.0);
+    double band = 2.0 * radious;
+    double spacing = 2 * radious;
+    size_t nb = (size_t)64 * 64 * 64;
+    size_t* start = (size_t*)xcalloc(nb + 1, sizeof(size_t));
+    size_t* list = (size_t*)xcalloc(s->np, sizeof(size_t));
+    size_t* key = (size_t*)xcalloc(s->np, sizeof(size_t));
+    for (size_t pi = 0; pi < s->np; ++pi) {
+        const double* x = s->pos + 3 * pi;
+        key[pi] = hash_key(bucket_of(x[0], spacing), bucket_of(x[1], spacing), bucket_of(x[2], spacing));
+        start[key[pi] + 1]++;
+    }
+    for (size_t b = 0; b < nb; ++b) start[b + 1] += start[b];
+    size_t* fill = (size_t*)xcalloc(nb, sizeof(size_t));
+    for (size_t pi = 0; pi < s->np; ++pi) list[start[key[pi]] + fill[key[pi]]++] = pi; /* push_back order */
+    const double R2 = band * band;
+    for (int i = 0; i < s->n.x; ++i)
+        for (int j = 0; j < s->n.y; ++j)
+            for (int k = 0; k < s->n.z; ++k) {
+                double q[3] = {s->sdf_origin[0] + i * s->h[0], s->sdf_origin[1] + j * s->h[1],
+                               s->sdf_origin[2] + k * s->h[2]}; /* Grid3D::GridIndexToPosition */
+                double minDistance = band;
+                if (s->np > 0) {
+                    int ob[3] = {bucket_of(q[0], spacing), bucket_of(q[1], spacing), bucket_of(q[2], spacing)};
+                    int nbk[8][3];
+                    for (int t = 0; t < 8; ++t) { nbk[t][0] = ob[0]; nbk[t][1] = ob[1]; nbk[t][2] = ob[2]; }
+                    int dx = ((ob[0] + 0.5f) * spacing <= q[0]) ? 1 : -1;
+                    int dy = ((ob[1] + 0.5f) * spacing <= q[1]) ? 1 : -1;
+                    int dz = ((ob[2] + 0.5f) * spacing <= q[2]) ? 1 : -1;
+                    nbk[4][0] += dx; nbk[5][0] += dx; nbk[6][0] += dx; nbk[7][0] += dx;
+                    nbk[2][1] += dy; nbk[3][1] += dy; nbk[6][1] += dy; nbk[7][1] += dy;
+                    nbk[1][2] += dz; nbk[3][2] += dz; nbk[5][2] += dz; nbk[7][2] += dz;
+                    for (int t = 0; t < 8; ++t) {
+                        size_t kk = hash_key(nbk[t][0], nbk[t][1], nbk[t][2]);
+                        for (size_t e = start[kk]; e < start[kk + 1]; ++e) {
+                            const double* x = s->pos + 3 * list[e];
+                            double ddx = x[0] - q[0], ddy = x[1] - q[1], ddz = x[2] - q[2];
+                            double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                            if (d2 <= R2) {
+                                double dist = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+                                if (dist < minDistance) minDistance = dist; /* std::min keeps the first on ties */
+                            }
+                        }
+                    }
+                }
+                s->sdf[ix3(s->n, i, j, k)] = minDistance - radious;
+            }
+    free(start); free(list); free(key); free(fill);
+}
+
+/* SinglePhasePressureSolver::BuildMarkers (fluid_solvers/single_phase_pressure_solver.cpp:30-48).  The collider
+ * SDF is positive everywhere, so the BOUNDRY branch is never taken. */
+void or_build_markers(or_sim* s)
+{
+    for (int i = 0; i < s->n.x; ++i)
+        for (int j = 0; j < s->n.y; ++j)
+            for (int k = 0; k < s->n.z; ++k) {
+                /* FaceCenteredGrid3D::GetCellCenterPos (face_centered_grid3d.cpp:318-321) */
+                double c[3] = {(s->d.origin[0] + 0.5 * s->h[0]) + s->h[0] * i,
+                               (s->d.origin[1] + 0.5 * s->h[1]) + s->h[1] * j,
+                               (s->d.origin[2] + 0.5 * s->h[2]) + s->h[2] * k};
+                double v = sample3(s->sdf, s->n, s->sdf_origin, s->h, c);
+                s->marks[ix3(s->n, i, j, k)] = v < 0 ? OR_FLUID : OR_AIR;
+            }
+}
+
+/* ---------------------------------------------------------------- grid passes */
+
+/* PICSimulator::ExtrapolateVelocityToAir (pic_simulator.cpp:477-495). */
+void or_stage_extrapolate(or_sim* s)
+{
+    size_t iters = (size_t)ceil(s->d.max_cfl);
+    size_t nu = cnt3(s->du), nv = cnt3(s->dv), nw = cnt3(s->dw);
+    double* prev = (double*)malloc((nu > nv ? (nu > nw ? nu : nw) : (nv > nw ? nv : nw)) * sizeof(double));
+    memcpy(prev, s->u, nu * sizeof(double));
+    extrapolate_to_region(prev, s->mu, s->du, iters, s->u);
+    memcpy(prev, s->v, nv * sizeof(double));
+    extrapolate_to_region(prev, s->mv, s->dv, iters, s->v);
+    memcpy(prev, s->w, nw * sizeof(double));
+    extrapolate_to_region(prev, s->mw, s->dw, iters, s->w);
+    free(prev);
+}
+
+/* BlockedBoundryConditionSolver::ConstrainVelocity (fluid_solvers/blocked_boundry_condition_solver.cpp:18-291).
+ * Without colliders only the wall-layer zeroing (:198-244) changes the grid. */
+void or_stage_bc(or_sim* s)
+{
+    for (int k = 0; k < s->du.z; ++k)
+        for (int j = 0; j < s->du.y; ++j) {
+            s->u[ix3(s->du, 0, j, k)] = 0;
+            s->u[ix3(s->du, s->du.x - 1, j, k)] = 0;
+        }
+    for (int k = 0; k < s->dv.z; ++k)
+        for (int i = 0; i < s->dv.x; ++i) {
+            s->v[ix3(s->dv, i, 0, k)] = 0;
+            s->v[ix3(s->dv, i, s->dv.y - 1, k)] = 0;
+        }
+    for (int j = 0; j < s->dw.y; ++j)
+        for (int i = 0; i < s->dw.x; ++i) {
+            s->w[ix3(s->dw, i, j, 0)] = 0;
+            s->w[ix3(s->dw, i, j, s->dw.z - 1)] = 0;
+        }
+}
+
+/* PICSimulator::ComputeExternalForces (pic_simulator.cpp:203-212) with one DirectionalField
+ * (forces/external_force.cpp:4-29, forces/directional_field.cpp:13-16). */
+void or_stage_forces(or_sim* s, double dt)
+{
+    size_t nu = cnt3(s->du), nv = cnt3(s->dv), nw = cnt3(s->dw);
+    for (size_t f = 0; f < nu; ++f) s->u[f] += dt * s->d.gravity[0];
+    for (size_t f = 0; f < nv; ++f) s->v[f] += dt * s->d.gravity[1];
+    for (size_t f = 0; f < nw; ++f) s->w[f] += dt * s->d.gravity[2];
+    or_stage_bc(s);
+}
+
+/* ---------------------------------------------------------------- pressure */
+
+typedef struct {
+    double c, r, u, f; /* LinearSystemMatrixRow center, right, up, front (linear_system/linear_system.hpp:9-15) */
+} row4;
+
+/* BLAS::Dot (linear_system/blas.cpp:4-19): i outer, k inner. */
+static double blas_dot(const double* a, const double* b, dim3i n)
+{
+    double r = 0;
+    for (int i = 0; i < n.x; ++i)
+        for (int j = 0; j < n.y; ++j)
+            for (int k = 0; k < n.z; ++k) r += a[ix3(n, i, j, k)] * b[ix3(n, i, j, k)];
+    return r;
+}
+
+/* BLAS::Residual (linear_system/blas.cpp:21-36). */
+static void blas_residual(const row4* A, const double* x, const double* b, double* out, dim3i n)
+{
+    for (int i = 0; i < n.x; ++i)
+        for (int j = 0; j < n.y; ++j)
+            for (int k = 0; k < n.z; ++k) {
+                size_t c = ix3(n, i, j, k);
+                out[c] = b[c] - A[c].c * x[c] - ((i > 0) ? A[ix3(n, i - 1, j, k)].r * x[ix3(n, i - 1, j, k)] : 0.0) -
+                         ((i + 1 < n.x) ? A[c].r * x[ix3(n, i + 1, j, k)] : 0.0) -
+                         ((j > 0) ? A[ix3(n, i, j - 1, k)].u * x[ix3(n, i, j - 1, k)] : 0.0) -
+                         ((j + 1 < n.y) ? A[c].u * x[ix3(n, i, j + 1, k)] : 0.0) -
+                         ((k > 0) ? A[ix3(n, i, j, k - 1)].f * x[ix3(n, i, j, k - 1)] : 0.0) -
+                         ((k + 1 < n.z) ? A[c].f * x[ix3(n, i, j, k + 1)] : 0.0);
+            }
+}
+
+/* BLAS::MatrixVectorMultiplication (linear_system/blas.cpp:68-83). */
+static void blas_spmv(const row4* A, const double* v, double* out, dim3i n)
+{
+    for (int i = 0; i < n.x; ++i)
+        for (int j = 0; j < n.y; ++j)
+            for (int k = 0; k < n.z; ++k) {
+                size_t c = ix3(n, i, j, k);
+                out[c] = A[c].c * v[c] + ((i > 0) ? A[ix3(n, i - 1, j, k)].r * v[ix3(n, i - 1, j, k)] : 0.0) +
+                         ((i + 1 < n.x) ? A[c].r * v[ix3(n, i + 1, j, k)] : 0.0) +
+                         ((j > 0) ? A[ix3(n, i, j - 1, k)].u * v[ix3(n, i, j - 1, k)] : 0.0) +
+                         ((j + 1 < n.y) ? A[c].u * v[ix3(n, i, j + 1, k)] : 0.0) +
+                         ((k > 0) ? A[ix3(n, i, j, k - 1)].f * v[ix3(n, i, j, k - 1)] : 0.0) +
+                         ((k + 1 < n.z) ? A[c].f * v[ix3(n, i, j, k + 1)] : 0.0);
+            }
+}
+
+/* BLAS::AXpY (linear_system/blas.cpp:38-44): out = a*x + y. */
+static void blas_axpy(double a, const double* x, const double* y, double* out, size_t n)
+{
+    for (size_t c = 0; c < n; ++c) out[c] = a * x[c] + y[c];
+}
+
+/* SinglePhasePressureSolver::BuildSystem (fluid_solvers/single_phase_pressure_solver.cpp:99-164);
+ * b uses FaceCenteredGrid3D::DivergenceAtCallCenter (grid_systems/face_centered_grid3d.cpp:157-166). */
+static void build_system(dim3i n, const double h[3], const uint8_t* m, const double* u, const double* v,
+                         const double* w, row4* A, double* b)
+{
+    dim3i du = {n.x + 1, n.y, n.z}, dv = {n.x, n.y + 1, n.z}, dw = {n.x, n.y, n.z + 1};
+    double ih[3] = {1.0 / h[0], 1.0 / h[1], 1.0 / h[2]};
+    double ih2[3] = {ih[0] * ih[0], ih[1] * ih[1], ih[2] * ih[2]};
+    for (int i = 0; i < n.x; ++i)
+        for (int j = 0; j < n.y; ++j)
+            for (int k = 0; k < n.z; ++k) {
+                size_t c = ix3(n, i, j, k);
+                row4* row = &A[c];
+                row->c = row->r = row->u = row->f = 0.0;
+                b[c] = 0.0;
+                if (m[c] == OR_FLUID) {
+                    double left = u[ix3(du, i, j, k)], right = u[ix3(du, i + 1, j, k)];
+                    double down = v[ix3(dv, i, j, k)], up = v[ix3(dv, i, j + 1, k)];
+                    double back = w[ix3(dw, i, j, k)], front = w[ix3(dw, i, j, k + 1)];
+                    b[c] = (right - left) / h[0] + (up - down) / h[1] + (front - back) / h[2];
+                    if (i + 1 < n.x && m[ix3(n, i + 1, j, k)] != OR_BOUNDRY) {
+                        row->c += ih2[0];
+                        if (m[ix3(n, i + 1, j, k)] == OR_FLUID) row->r -= ih2[0];
+                    }
+                    if (i > 0 && m[ix3(n, i - 1, j, k)] != OR_BOUNDRY) row->c += ih2[0];
+                    if (j + 1 < n.y && m[ix3(n, i, j + 1, k)] != OR_BOUNDRY) {
+                        row->c += ih2[1];
+                        if (m[ix3(n, i, j + 1, k)] == OR_FLUID) row->u -= ih2[1];
+                    }
+                    if (j > 0 && m[ix3(n, i, j - 1, k)] != OR_BOUNDRY) row->c += ih2[1];
+                    if (k + 1 < n.z && m[ix3(n, i, j, k + 1)] != OR_BOUNDRY) {
+                        row->c += ih2[2];
+                        if (m[ix3(n, i, j, k + 1)] == OR_FLUID) row->f -= ih2[2];
+                    }
+                    if (k > 0 && m[ix3(n, i, j, k - 1)] != OR_BOUNDRY) row->c += ih2[2];
+                } else {
+                    row->c = 1.0;
+                }
+            }
+}
+
+/* ConjugateGradientSolver::Solve (linear_system/conjugate_gradient_solver.cpp:14-55) with tolerance
+ * rel * BLAS::L2Norm(b); x is the warm start and is updated in place.  Returns the iteration count. */
+static int cg_solve(const row4* A, const double* b, double* x, dim3i n, double rel, int maxIt)
+{
+    size_t N = cnt3(n);
+    double* r = (double*)malloc(N * sizeof(double));
+    double* d = (double*)malloc(N * sizeof(double));
+    double* q = (double*)malloc(N * sizeof(double));
+    double* s = (double*)malloc(N * sizeof(double));
+    double tol = rel * sqrt(blas_dot(b, b, n));
+    blas_residual(A, x, b, r, n);
+    memcpy(d, r, N * sizeof(double));
+    double sigmaNew = blas_dot(r, d, n);
+    int it = 0, trigger = 0;
+    while (sigmaNew > tol * tol && it < maxIt) {
+        blas_spmv(A, d, q, n);
+        double alpha = sigmaNew / blas_dot(d, q, n);
+        blas_axpy(alpha, d, x, x, N);
+        if (trigger || (it % 50 == 0 && it > 0)) {
+            blas_residual(A, x, b, r, n);
+            trigger = 0;
+        } else {
+            blas_axpy(-alpha, q, r, r, N);
+        }
+        memcpy(s, r, N * sizeof(double));
+        double sigmaOld = sigmaNew;
+        sigmaNew = blas_dot(r, s, n);
+        if (sigmaNew > sigmaOld) trigger = 1;
+        double beta = sigmaNew / sigmaOld;
+        blas_axpy(beta, d, s, d, N);
+        it++;
+    }
+    free(r); free(d); free(q); free(s);
+    return it;
+}
+
+static double true_rel_residual(const row4* A, const double* b, const double* x, dim3i n)
+{
+    size_t N = cnt3(n);
+    double* r = (double*)malloc(N * sizeof(double));
+    blas_residual(A, x, b, r, n);
+    double rn = sqrt(blas_dot(r, r, n)), bn = sqrt(blas_dot(b, b, n));
+    free(r);
+    return bn > 0 ? rn / bn : rn;
+}
+
+/* SinglePhasePressureSolver::ApplyPressure (fluid_solvers/single_phase_pressure_solver.cpp:56-92): output
+ * equals the input except the +x/+y/+z faces of FLUID cells whose neighbour is not BOUNDRY. */
+static void apply_pressure(dim3i n, const double h[3], const uint8_t* m, const double* p, double* u, double* v,
+                           double* w)
+{
+    dim3i du = {n.x + 1, n.y, n.z}, dv = {n.x, n.y + 1, n.z}, dw = {n.x, n.y, n.z + 1};
+    double sc[3] = {1.0 / h[0], 1.0 / h[1], 1.0 / h[2]};
+    /* Reads of in(...) are of faces no other cell writes, so updating in place equals out = in + ... */
+    for (int i = 0; i < n.x; ++i)
+        for (int j = 0; j < n.y; ++j)
+            for (int k = 0; k < n.z; ++k) {
+                if (m[ix3(n, i, j, k)] != OR_FLUID) continue;
+                double pc = p[ix3(n, i, j, k)];
+                if (i + 1 < n.x && m[ix3(n, i + 1, j, k)] != OR_BOUNDRY)
+                    u[ix3(du, i + 1, j, k)] = u[ix3(du, i + 1, j, k)] + sc[0] * (p[ix3(n, i + 1, j, k)] - pc);
+                if (j + 1 < n.y && m[ix3(n, i, j + 1, k)] != OR_BOUNDRY)
+                    v[ix3(dv, i, j + 1, k)] = v[ix3(dv, i, j + 1, k)] + sc[1] * (p[ix3(n, i, j + 1, k)] - pc);
+                if (k + 1 < n.z && m[ix3(n, i, j, k + 1)] != OR_BOUNDRY)
+                    w[ix3(dw, i, j, k + 1)] = w[ix3(dw, i, j, k + 1)] + sc[2] * (p[ix3(n, i, j, k + 1)] - pc);
+            }
+}
+
+int or_project(const int nn[3], const double h[3], const uint8_t* marks, double* u, double* v, double* w, double* p,
+               double rel_tol, int max_it, double* rel_residual)
+{
+    dim3i n = {nn[0], nn[1], nn[2]};
+    size_t N = cnt3(n);
+    row4* A = (row4*)malloc(N * sizeof(row4));
+    double* b = (double*)malloc(N * sizeof(double));
+    build_system(n, h, marks, u, v, w, A, b);
+    int it = cg_solve(A, b, p, n, rel_tol, max_it);
+    if (rel_residual) *rel_residual = true_rel_residual(A, b, p, n);
+    apply_pressure(n, h, marks, p, u, v, w);
+    free(A);
+    free(b);
+    return it;
+}
+
+/* PICSimulator::ComputePressure (pic_simulator.cpp:224-229) -> SinglePhasePressureSolver::Solve
+ * (fluid_solvers/single_phase_pressure_solver.cpp:21-28), then ApplyBoundryCondition. */
+void or_stage_pressure(or_sim* s, double dt)
+{
+    (void)dt; /* neither dt nor density enters the solve (single_phase_pressure_solver.cpp:59-60) */
+    or_build_markers(s);
+    size_t N = cnt3(s->n);
+    row4* A = (row4*)malloc(N * sizeof(row4));
+    build_system(s->n, s->h, s->marks, s->u, s->v, s->w, A, s->b);
+    s->cg_it = cg_solve(A, s->b, s->p, s->n, s->d.cg_rel_tol, s->d.cg_max_it);
+    s->cg_res = true_rel_residual(A, s->b, s->p, s->n);
+    apply_pressure(s->n, s->h, s->marks, s->p, s->u, s->v, s->w);
+    free(A);
+    or_stage_bc(s);
+}
+
+double or_divergence_l2(const or_sim* s)
+{
+    double acc = 0;
+    for (int k = 0; k < s->n.z; ++k)
+        for (int j = 0; j < s->n.y; ++j)
+            for (int i = 0; i < s->n.x; ++i) {
+                if (s->marks[ix3(s->n, i, j, k)] != OR_FLUID) continue;
+                double dv = (s->u[ix3(s->du, i + 1, j, k)] - s->u[ix3(s->du, i, j, k)]) / s->h[0] +
+                            (s->v[ix3(s->dv, i, j + 1, k)] - s->v[ix3(s->dv, i, j, k)]) / s->h[1] +
+                            (s->w[ix3(s->dw, i, j, k + 1)] - s->w[ix3(s->dw, i, j, k)]) / s->h[2];
+                acc += dv * dv;
+            }
+    return sqrt(acc);
+}
+
+/* ---------------------------------------------------------------- G2P and advection */
+
+/* FaceCenteredGrid3D::Sample (grid_systems/face_centered_grid3d.cpp:138-144) on the velocity grid. */
+static void sample_velocity(const or_sim* s, const double* u, const double* v, const double* w, const double* xo,
+                            const double* yo, const double* zo, const double pos[3], double out[3])
+{
+    out[0] = sample3(u, s->du, xo, s->h, pos);
+    out[1] = sample3(v, s->dv, yo, s->h, pos);
+    out[2] = sample3(w, s->dw, zo, s->h, pos);
+}
+
+/* TransferGrid2Particles: PIC (pic_simulator.cpp:439-450), FLIP (flip_simulator.cpp:121-161),
+ * APIC (apic_simulator.cpp:120-176). */
+void or_stage_g2p(or_sim* s)
+{
+    if (s->d.solver == OR_FLIP) {
+        size_t nu = cnt3(s->du), nv = cnt3(s->dv), nw = cnt3(s->dw);
+        for (size_t f = 0; f < nu; ++f) s->su[f] = s->u[f] - s->su[f];
+        for (size_t f = 0; f < nv; ++f) s->sv[f] = s->v[f] - s->sv[f];
+        for (size_t f = 0; f < nw; ++f) s->sw[f] = s->w[f] - s->sw[f];
+        double fb = s->d.blend;
+        for (size_t pi = 0; pi < s->np; ++pi) {
+            double* vel = s->vel + 3 * pi;
+            const double* x = s->pos + 3 * pi;
+            double dv[3], pic[3];
+            sample_velocity(s, s->su, s->sv, s->sw, s->rxo, s->ryo, s->rzo, x, dv);
+            double flip[3] = {vel[0] + dv[0], vel[1] + dv[1], vel[2] + dv[2]};
+            if (fb > 0.0) {
+                sample_velocity(s, s->u, s->v, s->w, s->xo, s->yo, s->zo, x, pic);
+                for (int a = 0; a < 3; ++a) flip[a] = (1 - fb) * flip[a] + fb * pic[a];
+            }
+            vel[0] = flip[0]; vel[1] = flip[1]; vel[2] = flip[2];
+        }
+        return;
+    }
+    if (s->d.solver == OR_PIC) {
+        for (size_t pi = 0; pi < s->np; ++pi)
+            sample_velocity(s, s->u, s->v, s->w, s->xo, s->yo, s->zo, s->pos + 3 * pi, s->vel + 3 * pi);
+        return;
+    }
+    /* APIC */
+    const double* O = s->d.origin;
+    const double* S = s->d.size;
+    double hh[3] = {s->h[0] / 2.0, s->h[1] / 2.0, s->h[2] / 2.0};
+    for (size_t pi = 0; pi < s->np; ++pi) {
+        const double* x = s->pos + 3 * pi;
+        double* c = s->C + 9 * pi;
+        sample_velocity(s, s->u, s->v, s->w, s->xo, s->yo, s->zo, x, s->vel + 3 * pi);
+        for (int a = 0; a < 9; ++a) c[a] = 0;
+        idx8 id;
+        double g[8][3];
+        double pc[3] = {x[0], clampd(x[1], O[1] + S[1] - hh[1], O[1] + hh[1]), clampd(x[2], O[2] + S[2] - hh[2], O[2] + hh[2])};
+        coords_grad_weights(s->n, s->xo, s->h, pc, &id, g);
+        for (int t = 0; t < 8; ++t) {
+            double val = s->u[ix3(s->du, id.i[t], id.j[t], id.k[t])];
+            c[0] += g[t][0] * val; c[1] += g[t][1] * val; c[2] += g[t][2] * val;
+        }
+        pc[0] = clampd(x[0], O[0] + S[0] - hh[0], O[0] + hh[0]); pc[1] = x[1];
+        pc[2] = clampd(x[2], O[2] + S[2] - hh[2], O[2] + hh[2]);
+        coords_grad_weights(s->n, s->yo, s->h, pc, &id, g);
+        for (int t = 0; t < 8; ++t) {
+            double val = s->v[ix3(s->dv, id.i[t], id.j[t], id.k[t])];
+            c[3] += g[t][0] * val; c[4] += g[t][1] * val; c[5] += g[t][2] * val;
+        }
+        pc[0] = clampd(x[0], O[0] + S[0] - hh[0], O[0] + hh[0]);
+        pc[1] = clampd(x[1], O[1] + S[1] - hh[1], O[1] + hh[1]); pc[2] = x[2];
+        coords_grad_weights(s->n, s->zo, s->h, pc, &id, g);
+        for (int t = 0; t < 8; ++t) {
+            double val = s->w[ix3(s->dw, id.i[t], id.j[t], id.k[t])];
+            c[6] += g[t][0] * val; c[7] += g[t][1] * val; c[8] += g[t][2] * val;
+        }
+    }
+}
+
+/* PICSimulator::MoveParticles (pic_simulator.cpp:239-312).  The collider response never fires: the
+ * collider SDF is positive everywhere. */
+void or_stage_move(or_sim* s, double dt)
+{
+    unsigned nsub = (unsigned)(s->d.max_cfl > 1.0 ? s->d.max_cfl : 1.0);
+    double sdt = dt / nsub;
+    const double* O = s->d.origin;
+    const double* S = s->d.size;
+    for (size_t pi = 0; pi < s->np; ++pi) {
+        double* x = s->pos + 3 * pi;
+        double* vel = s->vel + 3 * pi;
+        double pt0[3] = {x[0], x[1], x[2]}, pt1[3] = {x[0], x[1], x[2]};
+        for (unsigned t = 0; t < nsub; ++t) {
+            double v0[3], mid[3], mv[3];
+            sample_velocity(s, s->u, s->v, s->w, s->xo, s->yo, s->zo, pt0, v0);
+            for (int a = 0; a < 3; ++a) mid[a] = pt0[a] + 0.5 * sdt * v0[a];
+            sample_velocity(s, s->u, s->v, s->w, s->xo, s->yo, s->zo, mid, mv);
+            for (int a = 0; a < 3; ++a) pt1[a] = pt0[a] + sdt * mv[a];
+            for (int a = 0; a < 3; ++a) pt0[a] = pt1[a];
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (pt1[a] <= O[a]) { pt1[a] = O[a]; vel[a] = 0.0; }
+            if (pt1[a] >= O[a] + S[a]) { pt1[a] = O[a] + S[a]; vel[a] = 0.0; }
+        }
+        x[0] = pt1[0]; x[1] = pt1[1]; x[2] = pt1[2];
+    }
+}
+
+/* PICSimulator::ComputeAdvection (pic_simulator.cpp:231-237). */
+void or_stage_advection(or_sim* s, double dt)
+{
+    or_stage_extrapolate(s);
+    or_stage_bc(s);
+    or_stage_g2p(s);
+    or_stage_move(s, dt);
+}
+
+/* PICSimulator::OnAdvanceTimeStep (pic_simulator.cpp:111-154) with OnBeginAdvanceTimeStep (:156-196).
+ * No emitters; BuildCollider leaves the collider SDF at its constant; viscosity 0 skips diffusion. */
+void or_substep(or_sim* s, double dt)
+{
+    or_stage_p2g(s);
+    or_stage_sdf(s);
+    or_stage_extrapolate(s);
+    or_stage_bc(s);
+    or_stage_forces(s, dt);
+    or_stage_pressure(s, dt);
+    or_stage_advection(s, dt);
+}
+
+/* PICSimulator::Cfl (pic_simulator.cpp:80-97). */
+double or_cfl(const or_sim* s, double dt)
+{
+    double maxV = 0.0;
+    for (int i = 0; i < s->n.x; ++i)
+        for (int j = 0; j < s->n.y; ++j)
+            for (int k = 0; k < s->n.z; ++k) {
+                double cx = 0.5 * (s->u[ix3(s->du, i, j, k)] + s->u[ix3(s->du, i + 1, j, k)]);
+                double cy = 0.5 * (s->v[ix3(s->dv, i, j, k)] + s->v[ix3(s->dv, i, j + 1, k)]);
+                double cz = 0.5 * (s->w[ix3(s->dw, i, j, k)] + s->w[ix3(s->dw, i, j, k + 1)]);
+                double vx = fabs(cx) + dt * 0.0, vy = fabs(cy) + dt * -9.8, vz = fabs(cz) + dt * 0.0;
+                maxV = maxV > vx ? maxV : vx;
+                maxV = maxV > vy ? maxV : vy;
+                maxV = maxV > vz ? maxV : vz;
+            }
+    double minH = s->h[0] < (s->h[1] < s->h[2] ? s->h[1] : s->h[2]) ? s->h[0] : (s->h[1] < s->h[2] ? s->h[1] : s->h[2]);
+    return maxV * dt / minH;
+}
+
+/* PICSimulator::NumberOfSubTimeSteps (pic_simulator.cpp:349-354). */
+unsigned or_number_of_substeps(const or_sim* s, double dt)
+{
+    double c = ceil(or_cfl(s, dt) / s->d.max_cfl);
+    return (unsigned)(c > 1.0 ? c : 1.0);
+}
+
+/* PhysicsAnimation::AdvanceTimeStep (physics_animation.cpp:64-92). */
+int or_advance_time(or_sim* s, double frame_dt)
+{
+    double remaining = frame_dt;
+    int count = 0;
+    while (remaining > 0.0000000001) {
+        unsigned n = or_number_of_substeps(s, remaining);
+        double sub = remaining / (double)n;
+        or_substep(s, sub);
+        remaining -= sub;
+        ++count;
+    }
+    return count;
+}
+
+int or_cg_iterations(const or_sim* s) { return s->cg_it; }
+double or_cg_rel_residual(const or_sim* s) { return s->cg_res; }
+
+/* ---------------------------------------------------------------- keys and seeding */
+
+void or_sort_keys(const float* pos, size_t n, const int dims[3], const float origin[3], const float inv_h[3],
+                  uint32_t* keys_sorted, uint32_t* perm)
+{
+    uint32_t space = fe_key_space(dims[0], dims[1], dims[2]);
+    uint32_t* key = (uint32_t*)malloc((n ? n : 1) * sizeof(uint32_t));
+    size_t* start = (size_t*)calloc((size_t)space + 1, sizeof(size_t));
+    for (size_t i = 0; i < n; ++i) {
+        key[i] = fe_particle_key(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], origin, inv_h, dims[0], dims[1], dims[2]);
+        start[key[i] + 1]++;
+    }
+    for (uint32_t k = 0; k < space; ++k) start[k + 1] += start[k];
+    for (size_t i = 0; i < n; ++i) {
+        size_t slot = start[key[i]]++;
+        perm[slot] = (uint32_t)i;
+        keys_sorted[slot] = key[i];
+    }
+    free(key);
+    free(start);
+}
+
+size_t or_seed_regions(const void* regions, int nreg, const int n[3], const double origin[3], const double h[3],
+                       uint64_t seed, float* pos, float* vel, size_t cap)
+{
+    return fe_seed_regions((const fe_region*)regions, nreg, n, origin, h, seed, pos, vel, cap);
+}

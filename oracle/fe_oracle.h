@@ -1,0 +1,110 @@
+/*
+ * fe_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU, FP64, single-threaded restatement of the reference's hybrid particle-grid substep
+ * (AleksanderSiwek/Fluide_Engine, src/pic_simulator.cpp, flip_simulator.cpp, apic_simulator.cpp
+ * and the solvers they call).  It is the checker for the CUDA path: only the tests, the smoke
+ * check and the CPU-baseline leg of the benchmark may load it.  Nothing in the product links it.
+ *
+ * Every function keeps the reference's floating-point operation order, so on identical inputs
+ * it reproduces the serial reference build bit for bit (pinned by tests/test_oracle_vs_reference.py
+ * against the reference compiled from its own sources, and by the reference's known-answer tests
+ * restated in tests/test_oracle_known_answers.py).
+ *
+ * Scope: the no-collider, no-emitter, zero-viscosity scenes of the benchmark configurations.  With
+ * no colliders the collider SDF is 1.7976931348623157e30 everywhere (3d/collider_collection.cpp:3,38),
+ * which makes the collider branches of BlockedBoundryConditionSolver::ConstrainVelocity, the
+ * BOUNDRY marker and ExtrapolateIntoCollider provable no-ops; they are restated as such.
+ */
+#ifndef FE_ORACLE_H
+#define FE_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OR_PIC = 0, OR_FLIP = 1, OR_APIC = 2 };
+enum { OR_AIR = 0, OR_FLUID = 1, OR_BOUNDRY = 2 };
+
+typedef struct {
+    int n[3];            /* cells per axis */
+    double origin[3];    /* domain origin (BoundingBox3D::GetOrigin) */
+    double size[3];      /* domain extents (BoundingBox3D::GetSize) */
+    int solver;          /* OR_PIC / OR_FLIP / OR_APIC */
+    double blend;        /* FLIPSimulator::_blendingFactor, reference default 0.05 */
+    double gravity[3];   /* DirectionalField strength */
+    double max_cfl;      /* HybridSimulator::_maxCfl */
+    double cg_rel_tol;   /* CG stops when r.r <= (rel * ||b||_2)^2 */
+    int cg_max_it;       /* ConjugateGradientSolver::_maxNumberOfIterations */
+} or_desc;
+
+typedef struct or_sim or_sim;
+
+or_sim* or_create(const or_desc* d);
+void or_destroy(or_sim* s);
+
+int or_set_particles(or_sim* s, size_t n, const double* pos, const double* vel, const double* C);
+size_t or_num_particles(const or_sim* s);
+void or_get_particles(const or_sim* s, double* pos, double* vel, double* C);
+
+/* Grid state: u (nx+1)*ny*nz, v nx*(ny+1)*nz, w nx*ny*(nz+1), x-fastest; p, sdf, marks nx*ny*nz. */
+void or_get_grid(const or_sim* s, double* u, double* v, double* w);
+void or_set_grid(or_sim* s, const double* u, const double* v, const double* w);
+void or_get_pressure(const or_sim* s, double* p);
+void or_set_pressure(or_sim* s, const double* p);
+void or_get_marks(const or_sim* s, uint8_t* marks);
+void or_get_sdf(const or_sim* s, double* sdf);
+void or_get_face_markers(const or_sim* s, uint8_t* mu, uint8_t* mv, uint8_t* mw);
+void or_get_snapshot(const or_sim* s, double* u, double* v, double* w);
+void or_get_rhs(const or_sim* s, double* b);
+
+/* Substep stages, in the order PICSimulator::OnAdvanceTimeStep runs them. */
+void or_stage_p2g(or_sim* s);                       /* TransferParticles2Grid (virtual per solver) */
+void or_stage_sdf(or_sim* s);                       /* BuildSignedDistanceField */
+void or_stage_extrapolate(or_sim* s);               /* ExtrapolateVelocityToAir */
+void or_stage_bc(or_sim* s);                        /* ApplyBoundryCondition */
+void or_stage_forces(or_sim* s, double dt);         /* ComputeExternalForces (forces + BC) */
+void or_stage_pressure(or_sim* s, double dt);       /* ComputePressure (markers, system, CG, apply, BC) */
+void or_stage_advection(or_sim* s, double dt);      /* ComputeAdvection (extrap, BC, G2P, move) */
+void or_stage_g2p(or_sim* s);                       /* TransferGrid2Particles only */
+void or_stage_move(or_sim* s, double dt);           /* MoveParticles only */
+void or_build_markers(or_sim* s);                   /* SinglePhasePressureSolver::BuildMarkers only */
+
+void or_substep(or_sim* s, double dt);              /* PICSimulator::OnAdvanceTimeStep */
+double or_cfl(const or_sim* s, double dt);          /* PICSimulator::Cfl */
+unsigned or_number_of_substeps(const or_sim* s, double dt); /* PICSimulator::NumberOfSubTimeSteps */
+int or_advance_time(or_sim* s, double frame_dt);    /* PhysicsAnimation::AdvanceTimeStep; returns substeps */
+
+int or_cg_iterations(const or_sim* s);              /* iterations of the last solve */
+double or_cg_rel_residual(const or_sim* s);         /* true ||b - A p|| / ||b|| after the last solve */
+double or_divergence_l2(const or_sim* s);           /* ||div u||_2 over FLUID cells of the current grid */
+
+/* Reference known-answer helpers (common/math_utils.hpp, grid_systems/face_centered_grid3d.cpp). */
+double or_lerp(double a, double b, double f);
+double or_trilerp(const double c[8], double fx, double fy, double fz);
+double or_sample_face_array(const double* arr, const int size[3], const double origin[3], const double h[3],
+                            const double pos[3]);
+double or_scalar_sample(const double* arr, const int size[3], const double origin[3], const double h[3],
+                        const double pos[3]);
+
+/* Standalone pressure projection on a caller-supplied grid with caller-supplied markers
+ * (SinglePhasePressureSolver::Solve with the CG of conjugate_gradient_solver.cpp). */
+int or_project(const int n[3], const double h[3], const uint8_t* marks, double* u, double* v, double* w,
+               double* p, double rel_tol, int max_it, double* rel_residual);
+
+/* Stable counting sort of FP32 particle positions by fe_keys.h cell key; writes keys and perm. */
+void or_sort_keys(const float* pos, size_t n, const int dims[3], const float origin[3], const float inv_h[3],
+                  uint32_t* keys_sorted, uint32_t* perm);
+
+/* Seeding of the analytic scenes (fe_seed.h), for CPU-only tests. */
+size_t or_seed_regions(const void* regions, int nreg, const int n[3], const double origin[3], const double h[3],
+                       uint64_t seed, float* pos, float* vel, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FE_ORACLE_H */

@@ -1,0 +1,246 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// A C-ABI driver around the reference's own CPU simulators (PICSimulator / FLIPSimulator /
+// APICSimulator of AleksanderSiwek/Fluide_Engine), compiled from the reference sources by
+// oracle/build_ref.py into oracle/_ref/.  It pins the C restatement (fe_oracle.c) and serves as the
+// timed CPU baseline.  It seeds particles directly (the public API only seeds through std::rand in
+// PICSimulator::InitializeParticles, pic_simulator.cpp:521-548), swaps in a relative-tolerance CG
+// (the reference CG stops on an absolute r.r, conjugate_gradient_solver.cpp:26), and exposes the
+// protected substep stages so single stages can be compared.
+//
+// Private members are reached with the usual test-only access trick; layout is unchanged.
+#define private public
+#define protected public
+#include "pic_simulator.hpp"
+#include "flip_simulator.hpp"
+#include "apic_simulator.hpp"
+#include "fluid_solvers/single_phase_pressure_solver.hpp"
+#include "linear_system/conjugate_gradient_solver.hpp"
+#include "linear_system/blas.hpp"
+#include "linear_system/cuda_jacobi_iteration_solver.hpp"
+#include "forces/directional_field.hpp"
+#undef private
+#undef protected
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <iostream>
+#include <sstream>
+
+// The reference constructs CudaJacobiIterationSolver as its default pressure solver
+// (fluid_solvers/single_phase_pressure_solver.cpp:11); the harness replaces it before any solve, so
+// the CPU build only needs the class to exist.  These definitions are the harness's own.
+CudaJacobiIterationSolver::CudaJacobiIterationSolver(size_t maxNumberOfIterations, size_t residualCheckInterval,
+                                                     double tolerance)
+    : _maxNumberOfIterations(maxNumberOfIterations), _toleranceCheckInterval(residualCheckInterval),
+      _tolerance(tolerance), _iteration(0), _wasMemoryAllocatedOnDevice(false)
+{
+}
+CudaJacobiIterationSolver::~CudaJacobiIterationSolver() {}
+void CudaJacobiIterationSolver::Solve(LinearSystem*) { throw std::runtime_error("CUDA Jacobi is not built on the CPU"); }
+
+namespace {
+
+// ConjugateGradientSolver with tol = rel * ||b||_2, as BASELINE's "CG to relative residual".
+struct RelTolCG : public LinearSystemSolver {
+    double rel;
+    size_t maxIt;
+    size_t lastIterations = 0;
+    RelTolCG(double r, size_t m) : rel(r), maxIt(m) {}
+    void Solve(LinearSystem* system) override
+    {
+        double tol = rel * BLAS::L2Norm(system->b);
+        ConjugateGradientSolver cg(maxIt, tol);
+        cg.Solve(system);
+    }
+};
+
+struct Handle {
+    int solver;
+    std::shared_ptr<PICSimulator> sim;
+    std::shared_ptr<SinglePhasePressureSolver> pressure;
+    std::shared_ptr<RelTolCG> cg;
+    std::streambuf* saved = nullptr;
+    std::ostringstream sink;
+};
+
+void quiet(Handle* h, bool on)
+{
+    if (on) h->saved = std::cout.rdbuf(h->sink.rdbuf());
+    else if (h->saved) { std::cout.rdbuf(h->saved); h->sink.str(""); }
+}
+
+template <class F>
+void each3(const Array3<double>& a, F f)
+{
+    const auto& s = a.GetSize();
+    for (size_t k = 0; k < s.z; ++k)
+        for (size_t j = 0; j < s.y; ++j)
+            for (size_t i = 0; i < s.x; ++i) f(i, j, k, i + s.x * (j + s.y * k));
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ref_create(int solver, int nx, int ny, int nz, const double* origin, const double* size, double blend,
+                 const double* gravity, double max_cfl, double cg_rel_tol, int cg_max_it)
+{
+    Handle* h = new Handle();
+    h->solver = solver;
+    Vector3<size_t> n(nx, ny, nz);
+    BoundingBox3D domain(Vector3<double>(origin[0], origin[1], origin[2]), Vector3<double>(size[0], size[1], size[2]));
+    quiet(h, true);
+    if (solver == 0) h->sim = std::make_shared<PICSimulator>(n, domain);
+    else if (solver == 1) {
+        auto f = std::make_shared<FLIPSimulator>(n, domain);
+        f->SetBlendingFactor(blend);
+        h->sim = f;
+    } else h->sim = std::make_shared<APICSimulator>(n, domain);
+    h->pressure = std::make_shared<SinglePhasePressureSolver>();
+    h->cg = std::make_shared<RelTolCG>(cg_rel_tol, (size_t)cg_max_it);
+    h->pressure->SetLinearSystemSolver(h->cg);
+    h->sim->SetPressureSolver(h->pressure);
+    h->sim->SetMaxClf(max_cfl);
+    h->sim->AddExternalForce(std::make_shared<DirectionalField>(Vector3<double>(gravity[0], gravity[1], gravity[2])));
+    quiet(h, false);
+    return h;
+}
+
+void ref_destroy(void* p) { delete (Handle*)p; }
+
+void ref_set_particles(void* p, size_t n, const double* pos, const double* vel, const double* C)
+{
+    Handle* h = (Handle*)p;
+    auto& ps = h->sim->_fluid.particleSystem;
+    std::vector<Vector3<double>> P(n), V(n);
+    for (size_t i = 0; i < n; ++i) {
+        P[i] = Vector3<double>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        V[i] = vel ? Vector3<double>(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]) : Vector3<double>(0, 0, 0);
+    }
+    if (ps.GetParticleNumber() == 0) ps.AddParticles(n, P, h->sim->PARTICLE_POSITION_KEY);
+    ps.Resize(n);
+    ps.SetVectorValues(h->sim->PARTICLE_POSITION_KEY, P);
+    ps.SetVectorValues(h->sim->PARTICLE_VELOCITY_KEY, V);
+    if (h->solver == 2) {
+        auto* a = (APICSimulator*)h->sim.get();
+        a->_cX.assign(n, Vector3<double>(0, 0, 0));
+        a->_cY.assign(n, Vector3<double>(0, 0, 0));
+        a->_cZ.assign(n, Vector3<double>(0, 0, 0));
+        if (C)
+            for (size_t i = 0; i < n; ++i) {
+                a->_cX[i] = Vector3<double>(C[9 * i + 0], C[9 * i + 1], C[9 * i + 2]);
+                a->_cY[i] = Vector3<double>(C[9 * i + 3], C[9 * i + 4], C[9 * i + 5]);
+                a->_cZ[i] = Vector3<double>(C[9 * i + 6], C[9 * i + 7], C[9 * i + 8]);
+            }
+    }
+}
+
+size_t ref_num_particles(void* p) { return ((Handle*)p)->sim->GetNumberOfParticles(); }
+
+void ref_get_particles(void* p, double* pos, double* vel, double* C)
+{
+    Handle* h = (Handle*)p;
+    auto& ps = h->sim->_fluid.particleSystem;
+    const auto& P = ps.GetVectorValues(h->sim->PARTICLE_POSITION_KEY);
+    const auto& V = ps.GetVectorValues(h->sim->PARTICLE_VELOCITY_KEY);
+    for (size_t i = 0; i < P.size(); ++i) {
+        if (pos) { pos[3 * i] = P[i].x; pos[3 * i + 1] = P[i].y; pos[3 * i + 2] = P[i].z; }
+        if (vel) { vel[3 * i] = V[i].x; vel[3 * i + 1] = V[i].y; vel[3 * i + 2] = V[i].z; }
+    }
+    if (C && h->solver == 2) {
+        auto* a = (APICSimulator*)h->sim.get();
+        for (size_t i = 0; i < a->_cX.size(); ++i) {
+            const Vector3<double>* r[3] = {&a->_cX[i], &a->_cY[i], &a->_cZ[i]};
+            for (int t = 0; t < 3; ++t) { C[9 * i + 3 * t] = r[t]->x; C[9 * i + 3 * t + 1] = r[t]->y; C[9 * i + 3 * t + 2] = r[t]->z; }
+        }
+    }
+}
+
+void ref_get_grid(void* p, double* u, double* v, double* w)
+{
+    Handle* h = (Handle*)p;
+    auto& g = h->sim->_fluid.velocityGrid;
+    each3(g.GetDataXRef(), [&](size_t i, size_t j, size_t k, size_t f) { u[f] = g.x(i, j, k); });
+    each3(g.GetDataYRef(), [&](size_t i, size_t j, size_t k, size_t f) { v[f] = g.y(i, j, k); });
+    each3(g.GetDataZRef(), [&](size_t i, size_t j, size_t k, size_t f) { w[f] = g.z(i, j, k); });
+}
+
+void ref_set_grid(void* p, const double* u, const double* v, const double* w)
+{
+    Handle* h = (Handle*)p;
+    auto& g = h->sim->_fluid.velocityGrid;
+    each3(g.GetDataXRef(), [&](size_t i, size_t j, size_t k, size_t f) { g.x(i, j, k) = u[f]; });
+    each3(g.GetDataYRef(), [&](size_t i, size_t j, size_t k, size_t f) { g.y(i, j, k) = v[f]; });
+    each3(g.GetDataZRef(), [&](size_t i, size_t j, size_t k, size_t f) { g.z(i, j, k) = w[f]; });
+}
+
+void ref_get_pressure(void* p, double* out)
+{
+    Handle* h = (Handle*)p;
+    const auto& x = h->pressure->_system.x;
+    if (x.GetSize().x == 0) return;
+    each3(x, [&](size_t i, size_t j, size_t k, size_t f) { out[f] = x(i, j, k); });
+}
+
+void ref_set_pressure(void* p, const double* in)
+{
+    Handle* h = (Handle*)p;
+    auto& x = h->pressure->_system.x;
+    x.Resize(h->sim->GetResolution());
+    each3(x, [&](size_t i, size_t j, size_t k, size_t f) { x(i, j, k) = in[f]; });
+}
+
+void ref_get_marks(void* p, uint8_t* out)
+{
+    Handle* h = (Handle*)p;
+    const auto& m = h->pressure->_fluidMarkers;
+    const auto& s = m.GetSize();
+    for (size_t k = 0; k < s.z; ++k)
+        for (size_t j = 0; j < s.y; ++j)
+            for (size_t i = 0; i < s.x; ++i) out[i + s.x * (j + s.y * k)] = (uint8_t)m(i, j, k);
+}
+
+void ref_get_sdf(void* p, double* out)
+{
+    Handle* h = (Handle*)p;
+    const auto& s = h->sim->_fluid.sdf;
+    each3(s, [&](size_t i, size_t j, size_t k, size_t f) { out[f] = s(i, j, k); });
+}
+
+void ref_get_face_markers(void* p, uint8_t* mu, uint8_t* mv, uint8_t* mw)
+{
+    Handle* h = (Handle*)p;
+    auto& f = h->sim->_fluid;
+    const Array3<int>* arr[3] = {&f.xMarkers, &f.yMarkers, &f.zMarkers};
+    uint8_t* out[3] = {mu, mv, mw};
+    for (int a = 0; a < 3; ++a) {
+        const auto& s = arr[a]->GetSize();
+        for (size_t k = 0; k < s.z; ++k)
+            for (size_t j = 0; j < s.y; ++j)
+                for (size_t i = 0; i < s.x; ++i) out[a][i + s.x * (j + s.y * k)] = (uint8_t)(*arr[a])(i, j, k);
+    }
+}
+
+// Stage entry points (protected hooks of PICSimulator, pic_simulator.hpp:55-80).
+void ref_stage_p2g(void* p) { Handle* h = (Handle*)p; quiet(h, true); h->sim->TransferParticles2Grid(); quiet(h, false); }
+void ref_stage_sdf(void* p) { Handle* h = (Handle*)p; quiet(h, true); h->sim->BuildSignedDistanceField(); quiet(h, false); }
+void ref_stage_begin(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->BeginAdvanceTimeStep(dt); quiet(h, false); }
+void ref_stage_forces(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeExternalForces(dt); quiet(h, false); }
+void ref_stage_pressure(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputePressure(dt); quiet(h, false); }
+void ref_stage_advection(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeAdvection(dt); quiet(h, false); }
+void ref_substep(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->OnAdvanceTimeStep(dt); quiet(h, false); }
+double ref_cfl(void* p, double dt) { Handle* h = (Handle*)p; return h->sim->Cfl(dt); }
+
+// PhysicsAnimation::AdvanceSingleFrame (physics_animation.cpp:17-21) with a Frame of interval dt.
+void ref_advance_frame(void* p, double dt)
+{
+    Handle* h = (Handle*)p;
+    quiet(h, true);
+    h->sim->SetCurrentFrame(Frame(dt)); /* index 0: AdvanceSingleFrame advances exactly one frame of dt */
+    h->sim->AdvanceSingleFrame();
+    quiet(h, false);
+}
+
+}  // extern "C"

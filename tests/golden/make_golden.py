@@ -1,0 +1,72 @@
+"""Generates the golden fixtures in this directory from the reference's own CPU simulator.
+
+Run from the repository root with the reference built (python oracle/build_ref.py):
+
+    python tests/golden/make_golden.py
+
+Each fixture is one substep of a small seeded scene (dam-break block, 8 particles per cell) run by
+the serial build of the reference (PICSimulator / FLIPSimulator / APICSimulator::OnAdvanceTimeStep
+behind oracle/ref_harness.cpp): the inputs (FP32 positions widened to FP64, velocities, APIC C,
+warm-start pressure) and the outputs after P2G, after the particle SDF, and after the whole substep.
+The fixtures travel with the repository, so the oracle restatement can be re-pinned on machines
+that do not have the reference sources.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+import oracle  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+CASES = [
+    # name, n, solver, region, seed, max_cfl, origin
+    ("flip_12", (12, 12, 12), oracle.FLIP, (0.0, 0.0, 0.0, 0.4, 0.6, 1.0), 0, 1.0, (0.0, 0.0, 0.0)),
+    ("pic_12x10x8", (12, 10, 8), oracle.PIC, (0.0, 0.0, 0.0, 0.5, 0.5, 0.7), 1, 2.0, (0.0, 0.0, 0.0)),
+    ("apic_10", (10, 10, 10), oracle.APIC, (0.2, 0.0, 0.1, 0.7, 0.5, 0.9), 2, 1.0, (0.0, 0.0, 0.0)),
+    ("flip_16_cfl3", (16, 16, 16), oracle.FLIP, (0.0, 0.0, 0.0, 0.4, 0.6, 1.0), 3, 3.0, (0.0, 0.0, 0.0)),
+]
+
+
+def scene(n, region, seed, origin):
+    lo = tuple(origin[a] + region[a] for a in range(3))
+    hi = tuple(origin[a] + region[3 + a] for a in range(3))
+    pos, _ = oracle.seed_regions([dict(kind=0, lo=lo, hi=hi)], n, origin, (1, 1, 1), seed)
+    rng = np.random.default_rng(100 + seed)
+    vel = (rng.standard_normal(pos.shape) * 0.5).astype(np.float32)
+    C = (rng.standard_normal((pos.shape[0], 9)) * 0.2).astype(np.float32)
+    p0 = rng.standard_normal((n[2], n[1], n[0])) * 1e-3
+    return pos.astype(np.float64), vel.astype(np.float64), C.astype(np.float64), p0
+
+
+def make(name, n, solver, region, seed, max_cfl, origin, dt=1.0 / 240.0):
+    pos, vel, C, p0 = scene(n, region, seed, origin)
+    kw = dict(origin=origin, max_cfl=max_cfl, cg_rel_tol=1e-6, cg_max_it=500)
+    r = oracle.RefSim(n, solver, **kw)
+    r.set_particles(pos, vel, C)
+    r.set_pressure(p0)
+    r.stage("p2g")
+    p2g = r.grid()
+    r.stage("sdf")
+    sdf = r.sdf()
+    r = oracle.RefSim(n, solver, **kw)
+    r.set_particles(pos, vel, C)
+    r.set_pressure(p0)
+    r.substep(dt)
+    u, v, w = r.grid()
+    P, V, CC = r.particles()
+    np.savez_compressed(
+        os.path.join(OUT, name + ".npz"), n=np.array(n), solver=solver, max_cfl=max_cfl, dt=dt,
+        origin=np.array(origin), pos=pos, vel=vel, C=C, p0=p0, p2g_u=p2g[0], p2g_v=p2g[1], p2g_w=p2g[2], sdf=sdf,
+        out_u=u, out_v=v, out_w=w, out_p=r.pressure(), out_marks=r.marks(), out_pos=P, out_vel=V, out_C=CC)
+
+
+if __name__ == "__main__":
+    if not oracle.ref_available("serial"):
+        sys.exit("build the reference first: python oracle/build_ref.py")
+    for c in CASES:
+        make(*c)
+        print("wrote", c[0])
