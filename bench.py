@@ -1,0 +1,302 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 hybrid particle-grid substep (particle-steps/s).
+
+Workload (one GPU): the FLIP dam break on a 128^3 MAC grid over the unit cube with solid walls; the
+fluid block [0,0.4]x[0,0.6]x[0,1] is seeded with 8 jittered particles per cell (subcell rule, seed 0;
+4,021,248 particles), FLIP ratio 0.95, gravity (0,-9.81,0), fixed dt = 1/240 s, pressure by FP32 CG
+inside FP64 refinement to relative residual 1e-6.  A "step" is one substep of the whole hot path
+(sort, P2G, marking, grid passes, pressure solve, G2P + advection) on the device-resident state.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 128]
+
+Under torchrun every rank runs its own independent scene (replicas: a scene does not shard), the timed
+region is bracketed by a barrier + synchronize, and the slowest rank's device time is used.  One JSON
+line is printed by rank 0.  `--impl reference` times the reference's own CPU simulator (built from its
+sources into oracle/_ref by oracle/build_ref.py) on the host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+BOX = (0.0, 0.0, 0.0, 0.4, 0.6, 1.0)
+DT = 1.0 / 240.0
+
+
+def workload_config(n, steps, warmup, n_gpus, np_):
+    return {
+        "workload": "FLIP dam break %d^3, box [0,0.4]x[0,0.6]x[0,1], 8 particles/cell (seed 0), dt=1/240, "
+                    "FP32 CG in FP64 refinement to rel 1e-6" % n,
+        "grid": [n, n, n], "particles": np_, "solver": "FLIP 0.95", "dt": DT, "cg_rel_tol": 1e-6, "max_cfl": 1.0,
+        "substeps_timed": steps, "warmup": warmup, "parallelism": "replicas x%d" % n_gpus,
+        "l2": "working set > 126 MB L2 (particles alone %.0f MB); no flush" % (np_ * 24 / 1e6),
+    }
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per fluid-cell CG iteration from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "k_cg_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_unit:"):
+                    return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def reference_sample(n, steps, cores_hint=None):
+    """Times the reference's own threaded CPU simulator on the workload; returns (value, info)."""
+    import numpy as np
+    import oracle
+
+    variant = "threaded" if oracle.ref_available("threaded") else None
+    pos, vel = oracle.seed_regions([dict(kind=0, lo=BOX[:3], hi=BOX[3:])], (n, n, n), (0, 0, 0), (1, 1, 1), 0)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    if variant:
+        sim = oracle.RefSim((n, n, n), oracle.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=500, variant=variant)
+        kind = "reference"
+        threads = os.cpu_count()  # std::thread::hardware_concurrency() threads per parallel loop
+    else:
+        sim = oracle.OracleSim((n, n, n), oracle.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=500)
+        kind = "port"
+        threads = 1
+    sim.set_particles(pos.astype(np.float64), vel.astype(np.float64))
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        sim.substep(DT)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = pos.shape[0] * steps / total
+    info = {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
+            "sample": "%d substep(s) of the %d^3 FLIP dam break from rest (%d particles), %.1f s; host has %d cores"
+                      % (steps, n, pos.shape[0], total, cores)}
+    return value, total / steps * 1e3, info
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n_gpus = args.gpus
+    steps = max(1, min(args.steps, args.ref_steps))
+    value, ms, info = reference_sample(args.n, steps)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": n_gpus, "steps": steps, "warmup": 0,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded analytic scene)", "impl": "reference",
+            "config": workload_config(args.n, steps, 0, 1, None), "cpu_baseline": info,
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["config"]["particles"] = int(round(value * ms / 1e3))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=240)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--ref-steps", type=int, default=1, help="substeps of the CPU reference sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    args.warmup = max(args.warmup, 3)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import fluide_engine_b200 as fe
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    n = args.n
+    pos, vel = fe.seed_regions([dict(kind=0, lo=BOX[:3], hi=BOX[3:])], (n, n, n), (0, 0, 0), (1, 1, 1), 0)
+    N = pos.shape[0]
+    scene = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, device=local)
+    stream = torch.cuda.Stream()
+    scene.set_stream(stream.cuda_stream)
+    scene.set_particles(pos, vel)
+    scene.step(DT, args.warmup)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    barrier()
+    launches0 = fe.kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    stats, phase_ms = scene.step_profiled(DT, args.steps)
+    ev1.record(stream)
+    barrier()
+    launches = fe.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * N * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel: the persistent CG kernel (solve phase = exactly one launch)
+    cg_ms = phase_ms[:, 1].astype(np.float64)
+    fluid = np.array([s["fluid_cells"] for s in stats], dtype=np.float64)
+    its = np.array([s["cg_iterations"] for s in stats], dtype=np.float64)
+    refs = np.array([s["refinements"] for s in stats], dtype=np.float64)
+    alg_bytes = fluid * (its * 41.0 + (refs + 1.0) * 45.0)  # per launch: inner iterations + FP64 residual passes
+    peak, peak_kind = peaks()
+    achieved = alg_bytes.sum() / (cg_ms.sum() / 1e3) / 1e9
+    per_unit = profile_traffic()
+    units = fluid * (its + refs + 1.0)
+    traffic = float(per_unit * units.mean()) if per_unit else None
+    phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
+
+    # end to end through the public API with host buffers: H2D particles, one substep, D2H particles
+    pin_pos = torch.from_numpy(pos).pin_memory()
+    pin_vel = torch.zeros((N, 3), dtype=torch.float32).pin_memory()
+    P, V, _ = scene.particles()
+    pin_pos.copy_(torch.from_numpy(P))
+    pin_vel.copy_(torch.from_numpy(V))
+    out_pos = torch.empty((N, 3), dtype=torch.float32).pin_memory()
+    out_vel = torch.empty((N, 3), dtype=torch.float32).pin_memory()
+    L = fe.lib()
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        fe._abi.check(L.fe_scene_set_particles(scene.handle, fe._abi.ptr(pin_pos), fe._abi.ptr(pin_vel), None, N))
+        fe._abi.check(L.fe_scene_step(scene.handle, DT, 1, None))
+        fe._abi.check(L.fe_scene_get_particles(scene.handle, fe._abi.ptr(out_pos), fe._abi.ptr(out_vel), None, N))
+        pin_pos.copy_(out_pos)
+        pin_vel.copy_(out_vel)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * N * e2e_steps / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            _, _, cpu = reference_sample(n, args.ref_steps)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": None, "kind": "unavailable", "sample": str(ex)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded analytic scene)",
+            "config": workload_config(n, args.steps, args.warmup, world, N),
+            "roofline": {"bound": "hbm", "kernel": "k_cg (persistent FP32 CG + FP64 refinement, one launch/substep)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": float(alg_bytes.mean()),
+                         "note": "algorithmic bytes = fluid cells x (41 B x inner iterations + 45 B x FP64 residual "
+                                 "passes); at 128^3 the CG working set is L2-resident"},
+            "phases": {"share": {"pre_solve": phase_share[0], "cg_solve": phase_share[1], "post_solve": phase_share[2]},
+                       "ms_per_substep": (phase_ms.mean(axis=0)).tolist()},
+            "solver": {"cg_iterations_mean": float(its.mean()), "refinements_mean": float(refs.mean()),
+                       "rel_residual_max": float(max(s["rel_residual"] for s in stats)),
+                       "converged_all": bool(all(s["converged"] for s in stats)),
+                       "fluid_cells_mean": float(fluid.mean())},
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(N * 24),
+                    "d2h_bytes_per_step": int(N * 24), "steps": e2e_steps,
+                    "path": "fe_scene_set_particles(host) + fe_scene_step(1) + fe_scene_get_particles(host)"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

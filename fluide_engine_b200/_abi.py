@@ -1,0 +1,161 @@
+"""ctypes binding of the C ABI declared in include/fluide_b200.h.
+
+The product path is the sm_100a library libfluide_b200.so built in-tree by build.py; importing this
+module never falls back to anything else: if the library is missing it raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libfluide_b200.so")
+
+FE_OK = 0
+FE_ERR_CUDA, FE_ERR_BAD_ARG, FE_ERR_OOM, FE_ERR_NOT_CONVERGED, FE_ERR_TIMEOUT, FE_ERR_STATE, FE_ERR_NO_DEVICE = range(1, 8)
+PIC, FLIP, APIC = 0, 1, 2
+AIR, FLUID, BOUNDRY = 0, 1, 2
+(STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P, STAGE_MOVE) = range(8)
+
+STATUS_NAMES = {0: "FE_OK", 1: "FE_ERR_CUDA", 2: "FE_ERR_BAD_ARG", 3: "FE_ERR_OOM", 4: "FE_ERR_NOT_CONVERGED",
+                5: "FE_ERR_TIMEOUT", 6: "FE_ERR_STATE", 7: "FE_ERR_NO_DEVICE"}
+
+# Every symbol include/fluide_b200.h declares (checked by the CPU test suite).
+EXPORTS = [
+    "fe_scene_desc_default", "fe_scene_create", "fe_scene_destroy", "fe_scene_set_particles", "fe_scene_get_particles",
+    "fe_scene_num_particles", "fe_scene_step", "fe_scene_step_profiled", "fe_scene_advance_frame", "fe_scene_cfl", "fe_scene_run_stages",
+    "fe_scene_get_grid", "fe_scene_set_grid", "fe_scene_set_pressure", "fe_scene_get_face_markers",
+    "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_get_sort", "fe_scene_divergence",
+    "fe_scene_set_stream", "fe_scene_synchronize", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
+    "fe_abi_version",
+]
+
+
+class FluideError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32 * 3), ("origin", ctypes.c_double * 3), ("size", ctypes.c_double * 3),
+                ("solver", ctypes.c_int32), ("flip_blend", ctypes.c_double), ("gravity", ctypes.c_double * 3),
+                ("max_cfl", ctypes.c_double), ("cg_rel_tol", ctypes.c_double), ("cg_max_it", ctypes.c_int32),
+                ("cg_inner_tol", ctypes.c_double), ("max_refine", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("max_particles", ctypes.c_uint64)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("cg_iterations", ctypes.c_int32), ("refinements", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("fluid_cells", ctypes.c_int32), ("rel_residual", ctypes.c_double), ("b_norm", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Region(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("lo", ctypes.c_double * 3), ("hi", ctypes.c_double * 3),
+                ("vel", ctypes.c_double * 3)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libfluide_b200.so (building it first when nvcc is available and the library is stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH) and os.path.exists("/usr/local/cuda/bin/nvcc"):
+        from . import build as _build
+        _build.build()
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libfluide_b200.so is not built (run python fluide_engine_b200/build.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    F = ctypes.POINTER(ctypes.c_float)
+    D = ctypes.POINTER(ctypes.c_double)
+    U8 = ctypes.POINTER(ctypes.c_uint8)
+    U32 = ctypes.POINTER(ctypes.c_uint32)
+    I = ctypes.c_int
+    L.fe_scene_desc_default.argtypes = [ctypes.POINTER(SceneDesc)]
+    L.fe_scene_create.argtypes = [ctypes.POINTER(SceneDesc), ctypes.POINTER(P)]
+    L.fe_scene_destroy.argtypes = [P]
+    L.fe_scene_set_particles.argtypes = [P, P, P, P, ctypes.c_uint64]
+    L.fe_scene_get_particles.argtypes = [P, P, P, P, ctypes.c_uint64]
+    L.fe_scene_num_particles.argtypes = [P, ctypes.POINTER(ctypes.c_uint64)]
+    L.fe_scene_step.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats)]
+    L.fe_scene_step_profiled.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats),
+                                         ctypes.POINTER(ctypes.c_float)]
+    L.fe_scene_advance_frame.argtypes = [P, ctypes.c_double, ctypes.POINTER(ctypes.c_int32)]
+    L.fe_scene_cfl.argtypes = [P, ctypes.c_double, D]
+    L.fe_scene_run_stages.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.c_int32]
+    L.fe_scene_get_grid.argtypes = [P, P, P, P, P, P]
+    L.fe_scene_set_grid.argtypes = [P, P, P, P]
+    L.fe_scene_set_pressure.argtypes = [P, P]
+    L.fe_scene_get_face_markers.argtypes = [P, P, P, P]
+    L.fe_scene_get_snapshot.argtypes = [P, P, P, P]
+    L.fe_scene_get_rhs.argtypes = [P, P]
+    L.fe_scene_get_fluid_sdf.argtypes = [P, P]
+    L.fe_scene_get_sort.argtypes = [P, P, P, ctypes.c_uint64]
+    L.fe_scene_divergence.argtypes = [P, D]
+    L.fe_scene_set_stream.argtypes = [P, P]
+    L.fe_scene_synchronize.argtypes = [P]
+    L.fe_kernel_launch_count.restype = ctypes.c_uint64
+    L.fe_seed_regions.restype = ctypes.c_uint64
+    L.fe_seed_regions.argtypes = [P, ctypes.c_int32, P, P, P, ctypes.c_uint64, P, P, ctypes.c_uint64]
+    L.fe_last_error.restype = ctypes.c_char_p
+    L.fe_abi_version.restype = ctypes.c_int32
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if fn.restype is ctypes.c_int or fn.restype is None:
+            fn.restype = ctypes.c_int
+    L.fe_kernel_launch_count.restype = ctypes.c_uint64
+    L.fe_seed_regions.restype = ctypes.c_uint64
+    L.fe_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != FE_OK:
+        raise FluideError(status, lib().fe_last_error().decode(errors="replace"))
+
+
+def ptr(a):
+    """Raw pointer of a numpy array, a torch tensor (host or device) or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return ctypes.c_void_p(a.ctypes.data)
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous()
+        return ctypes.c_void_p(a.data_ptr())
+    if isinstance(a, int):
+        return ctypes.c_void_p(a)
+    raise TypeError("unsupported buffer type %r" % type(a))
+
+
+def kernel_launch_count():
+    return int(lib().fe_kernel_launch_count())
+
+
+def seed_regions(regions, n, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), seed=0):
+    """Seeds particles with the library's subcell rule.  regions: dicts {kind 0 box/1 sphere, lo, hi, vel}."""
+    L = lib()
+    arr = (Region * len(regions))()
+    for i, r in enumerate(regions):
+        arr[i].kind = r.get("kind", 0)
+        for a in range(3):
+            arr[i].lo[a] = r["lo"][a]
+            arr[i].hi[a] = r["hi"][a] if a < len(r["hi"]) else 0.0
+            arr[i].vel[a] = r.get("vel", (0.0, 0.0, 0.0))[a]
+    n3 = (ctypes.c_int32 * 3)(*n)
+    o = (ctypes.c_double * 3)(*origin)
+    s = (ctypes.c_double * 3)(*size)
+    cnt = L.fe_seed_regions(ctypes.cast(arr, ctypes.c_void_p), len(regions), n3, o, s, seed, None, None, 0)
+    pos = np.zeros((cnt, 3), dtype=np.float32)
+    vel = np.zeros((cnt, 3), dtype=np.float32)
+    L.fe_seed_regions(ctypes.cast(arr, ctypes.c_void_p), len(regions), n3, o, s, seed, ptr(pos), ptr(vel), cnt)
+    return pos, vel

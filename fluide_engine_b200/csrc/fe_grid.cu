@@ -1,0 +1,323 @@
+// fe_grid.cu -- face-grid passes of the substep.
+//
+//   K_extrap   one pass of ExtrapolateToRegion (common/math_utils.hpp:186-253): an invalid face takes
+//              the mean of its valid 6-neighbours (order i+1, i-1, j+1, j-1, k+1, k-1) and becomes
+//              valid.  Passes ping-pong between the two velocity buffers, so ceil(maxCfl) passes before
+//              the solve and as many after it leave the result in the buffer the substep started with.
+//              The last pass of each group is fused with what follows it in the reference:
+//   pre        ExtrapolateVelocityToAir, ApplyBoundryCondition, gravity, ApplyBoundryCondition
+//              (pic_simulator.cpp:186-211): wall faces end at 0, every other face gains dt*g.
+//   post       ExtrapolateVelocityToAir, ApplyBoundryCondition (pic_simulator.cpp:233-234).
+//              With no colliders ApplyBoundryCondition reduces to zeroing the six wall face layers
+//              (fluid_solvers/blocked_boundry_condition_solver.cpp:198-244).
+//   K_rhs      b = div u on FLUID cells (DivergenceAtCallCenter, grid_systems/face_centered_grid3d.cpp:
+//              157-166, evaluated in FP64 from the FP32 faces), 0 elsewhere.
+//   K_apply    u_{i+1} += (p_{i+1} - p_i) / h for FLUID cells i toward +x/+y/+z only
+//              (fluid_solvers/single_phase_pressure_solver.cpp:56-92); wall faces are never touched.
+//   K_cfl      max over cells of |u_cc| + dt*(0,-9.8,0) component-wise (pic_simulator.cpp:80-97).
+#include "fe_internal.cuh"
+
+namespace fe {
+namespace {
+
+struct FaceArrays {
+    const float* in[3];
+    float* out[3];
+    const uint8_t* vin[3];
+    uint8_t* vout[3];
+};
+
+enum { kModePlain = 0, kModePre = 1, kModePost = 2 };
+
+template <int MODE>
+__global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid, float gx, float gy, float gz)
+{
+    const size_t nu = (size_t)(nx + 1) * ny * nz, nv = (size_t)nx * (ny + 1) * nz, nw = (size_t)nx * ny * (nz + 1);
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= nu + nv + nw) return;
+    int c, sx, sy, sz;
+    size_t f;
+    if (t < nu) { c = 0; f = t; sx = nx + 1; sy = ny; sz = nz; }
+    else if (t < nu + nv) { c = 1; f = t - nu; sx = nx; sy = ny + 1; sz = nz; }
+    else { c = 2; f = t - nu - nv; sx = nx; sy = ny; sz = nz + 1; }
+    const int i = (int)(f % sx), j = (int)((f / sx) % sy), k = (int)(f / ((size_t)sx * sy));
+    const float* in = fa.in[c];
+    const uint8_t* vin = fa.vin[c];
+    float val = in[f];
+    uint8_t valid = vin[f];
+    if (!valid) {
+        float sum = 0.f;
+        unsigned count = 0;
+        const size_t sxy = (size_t)sx * sy;
+        if (i + 1 < sx && vin[f + 1]) { sum += in[f + 1]; ++count; }
+        if (i > 0 && vin[f - 1]) { sum += in[f - 1]; ++count; }
+        if (j + 1 < sy && vin[f + sx]) { sum += in[f + sx]; ++count; }
+        if (j > 0 && vin[f - sx]) { sum += in[f - sx]; ++count; }
+        if (k + 1 < sz && vin[f + sxy]) { sum += in[f + sxy]; ++count; }
+        if (k > 0 && vin[f - sxy]) { sum += in[f - sxy]; ++count; }
+        if (count > 0) {
+            val = sum / (float)count;
+            valid = 1;
+        }
+    }
+    if (write_valid) fa.vout[c][f] = valid;
+    if (MODE != kModePlain) {
+        const bool wall = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1)) ||
+                          (c == 2 && (k == 0 || k == sz - 1));
+        if (wall) val = 0.f;
+        else if (MODE == kModePre) val += (c == 0 ? gx : (c == 1 ? gy : gz));
+    }
+    fa.out[c][f] = val;
+}
+
+__global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
+                      const float* __restrict__ w)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const size_t nc = (size_t)nx * ny * nz;
+    size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    double b = 0.0;
+    if (v.marks[c] == FE_CELL_FLUID) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        const double left = u[idx3(i, j, k, nx + 1, ny)], right = u[idx3(i + 1, j, k, nx + 1, ny)];
+        const double down = vv[idx3(i, j, k, nx, ny + 1)], up = vv[idx3(i, j + 1, k, nx, ny + 1)];
+        const double back = w[idx3(i, j, k, nx, ny)], front = w[idx3(i, j, k + 1, nx, ny)];
+        b = (right - left) / v.h[0] + (up - down) / v.h[1] + (front - back) / v.h[2];
+    }
+    v.b[c] = b;
+}
+
+__global__ void k_apply(SceneView v, float* u, float* vv, float* w)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz, nww = (size_t)nx * ny * (nz + 1);
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= nu + nvv + nww) return;
+    const double* p = v.p;
+    if (t < nu) {
+        const int i = (int)(t % (nx + 1)), j = (int)((t / (nx + 1)) % ny), k = (int)(t / ((size_t)(nx + 1) * ny));
+        if (i < 1 || i > nx - 1) return;
+        const size_t cm = idx3(i - 1, j, k, nx, ny);
+        if (v.marks[cm] != FE_CELL_FLUID) return;
+        u[t] = (float)((double)u[t] + v.inv_h[0] * (p[cm + 1] - p[cm]));
+    } else if (t < nu + nvv) {
+        const size_t f = t - nu;
+        const int i = (int)(f % nx), j = (int)((f / nx) % (ny + 1)), k = (int)(f / ((size_t)nx * (ny + 1)));
+        if (j < 1 || j > ny - 1) return;
+        const size_t cm = idx3(i, j - 1, k, nx, ny);
+        if (v.marks[cm] != FE_CELL_FLUID) return;
+        vv[f] = (float)((double)vv[f] + v.inv_h[1] * (p[cm + nx] - p[cm]));
+    } else {
+        const size_t f = t - nu - nvv;
+        const int i = (int)(f % nx), j = (int)((f / nx) % ny), k = (int)(f / ((size_t)nx * ny));
+        if (k < 1 || k > nz - 1) return;
+        const size_t cm = idx3(i, j, k - 1, nx, ny);
+        if (v.marks[cm] != FE_CELL_FLUID) return;
+        w[f] = (float)((double)w[f] + v.inv_h[2] * (p[cm + (size_t)nx * ny] - p[cm]));
+    }
+}
+
+__global__ void k_cfl(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
+                      const float* __restrict__ w, double dt, unsigned long long* out_bits)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const size_t nc = (size_t)nx * ny * nz;
+    double m = 0.0;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        const double cx = 0.5 * ((double)u[idx3(i, j, k, nx + 1, ny)] + (double)u[idx3(i + 1, j, k, nx + 1, ny)]);
+        const double cy = 0.5 * ((double)vv[idx3(i, j, k, nx, ny + 1)] + (double)vv[idx3(i, j + 1, k, nx, ny + 1)]);
+        const double cz = 0.5 * ((double)w[idx3(i, j, k, nx, ny)] + (double)w[idx3(i, j, k + 1, nx, ny)]);
+        m = fmax(m, fabs(cx) + dt * 0.0);
+        m = fmax(m, fabs(cy) + dt * -9.8);
+        m = fmax(m, fabs(cz) + dt * 0.0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void k_divergence(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
+                             const float* __restrict__ w, double* out)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const size_t nc = (size_t)nx * ny * nz;
+    double acc = 0.0;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        if (v.marks[c] != FE_CELL_FLUID) continue;
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        const double d = ((double)u[idx3(i + 1, j, k, nx + 1, ny)] - u[idx3(i, j, k, nx + 1, ny)]) / v.h[0] +
+                         ((double)vv[idx3(i, j + 1, k, nx, ny + 1)] - vv[idx3(i, j, k, nx, ny + 1)]) / v.h[1] +
+                         ((double)w[idx3(i, j, k + 1, nx, ny)] - w[idx3(i, j, k, nx, ny)]) / v.h[2];
+        acc += d * d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+__global__ void k_scatter_out(SceneView v, float* pos, float* vel, float* C)
+{
+    uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s >= v.np) return;
+    const uint64_t d = v.pid[s];
+    if (pos) { pos[3 * d] = v.px[s]; pos[3 * d + 1] = v.py[s]; pos[3 * d + 2] = v.pz[s]; }
+    if (vel) { vel[3 * d] = v.vx[s]; vel[3 * d + 1] = v.vy[s]; vel[3 * d + 2] = v.vz[s]; }
+    if (C && v.solver == FE_SOLVER_APIC)
+        for (int a = 0; a < 9; ++a) C[9 * d + a] = v.c[a][s];
+}
+
+size_t faces_total(const SceneView& v)
+{
+    return (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz + (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz +
+           (size_t)v.g.nx * v.g.ny * (v.g.nz + 1);
+}
+
+// Runs `depth` extrapolation passes starting from buffer A (v.u..) whose last pass applies MODE;
+// the face markers v.mu.. are read-only, the validity ping-pong uses v.mu2.. and the crit scratch.
+template <int MODE>
+cudaError_t run_extrap_group(const SceneView& v, float* const src[3], float* const dst_final[3], float* const other[3],
+                             int depth, float gx, float gy, float gz, cudaStream_t st)
+{
+    const size_t total = faces_total(v);
+    const unsigned nb = (unsigned)((total + 255) / 256);
+    const float* in[3] = {src[0], src[1], src[2]};
+    const uint8_t* vin[3] = {v.mu, v.mv, v.mw};
+    // validity buffers alternate between two scratch sets laid out inside mu2 (size 2 * faces)
+    const size_t nu = (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz, nvv = (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz;
+    uint8_t* vset[2][3] = {{v.mu2, v.mu2 + nu, v.mu2 + nu + nvv},
+                           {v.mu2 + total, v.mu2 + total + nu, v.mu2 + total + nu + nvv}};
+    static_assert(MODE != kModePlain, "the last pass carries the pre or post tail");
+    for (int pass = 0; pass < depth; ++pass) {
+        const bool last = pass == depth - 1;
+        FaceArrays fa;
+        float* const* out = last ? dst_final : ((pass & 1) ? src : other);
+        for (int c = 0; c < 3; ++c) {
+            fa.in[c] = in[c];
+            fa.out[c] = out[c];
+            fa.vin[c] = vin[c];
+            fa.vout[c] = vset[pass & 1][c];
+        }
+        if (last) k_extrap<MODE><<<nb, 256, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, false, gx, gy, gz);
+        else k_extrap<kModePlain><<<nb, 256, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, true, 0.f, 0.f, 0.f);
+        count_launch();
+        for (int c = 0; c < 3; ++c) {
+            in[c] = out[c];
+            vin[c] = vset[pass & 1][c];
+        }
+    }
+    return cudaGetLastError();
+}
+
+__global__ void k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g, float gx, float gy,
+                            float gz)
+{
+    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz, nww = (size_t)nx * ny * (nz + 1);
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= nu + nvv + nww) return;
+    int c, sx, sy, sz;
+    size_t f;
+    float* a;
+    if (t < nu) { c = 0; f = t; sx = nx + 1; sy = ny; sz = nz; a = u; }
+    else if (t < nu + nvv) { c = 1; f = t - nu; sx = nx; sy = ny + 1; sz = nz; a = vv; }
+    else { c = 2; f = t - nu - nvv; sx = nx; sy = ny; sz = nz + 1; a = w; }
+    const int i = (int)(f % sx), j = (int)((f / sx) % sy), k = (int)(f / ((size_t)sx * sy));
+    const bool wall = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1)) ||
+                      (c == 2 && (k == 0 || k == sz - 1));
+    if (wall) a[f] = 0.f;
+    else if (add_g) a[f] += (c == 0 ? gx : (c == 1 ? gy : gz));
+}
+
+}  // namespace
+
+// Buffer convention: A = (v.u, v.v, v.w) holds the substep's velocity at its start and end; B =
+// (v.u2, v.v2, v.w2).  With depth d, the pre group leaves the velocity in A if d is even, else in B.
+cudaError_t launch_pre(const SceneView& v, double dt, cudaStream_t st)
+{
+    const float gx = (float)(dt * v.gravity[0]), gy = (float)(dt * v.gravity[1]), gz = (float)(dt * v.gravity[2]);
+    float* A[3] = {v.u, v.v, v.w};
+    float* B[3] = {v.u2, v.v2, v.w2};
+    const int d = v.extrap_depth;
+    if (d <= 0) {
+        const size_t total = faces_total(v);
+        k_wall_tail<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny, v.g.nz, true, gx, gy, gz);
+        count_launch();
+        return cudaGetLastError();
+    }
+    float* const* fin = (d & 1) ? B : A;
+    return run_extrap_group<kModePre>(v, A, fin, B, d, gx, gy, gz, st);
+}
+
+cudaError_t launch_post(const SceneView& v, cudaStream_t st)
+{
+    float* A[3] = {v.u, v.v, v.w};
+    float* B[3] = {v.u2, v.v2, v.w2};
+    const int d = v.extrap_depth;
+    if (d <= 0) {
+        const size_t total = faces_total(v);
+        k_wall_tail<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny, v.g.nz, false, 0, 0, 0);
+        count_launch();
+        return cudaGetLastError();
+    }
+    float* const* src = (d & 1) ? B : A;
+    float* const* oth = (d & 1) ? A : B;
+    // d passes starting at src end in A when d is odd (src = B), and in A when d is even (src = A)
+    return run_extrap_group<kModePost>(v, src, A, oth, d, 0.f, 0.f, 0.f, st);
+}
+
+static inline void pressure_buffers(const SceneView& v, const float*& u, const float*& vv, const float*& w)
+{
+    const bool b = v.extrap_depth > 0 && (v.extrap_depth & 1);
+    u = b ? v.u2 : v.u;
+    vv = b ? v.v2 : v.v;
+    w = b ? v.w2 : v.w;
+}
+
+cudaError_t launch_rhs(const SceneView& v, cudaStream_t st)
+{
+    const float *u, *vv, *w;
+    pressure_buffers(v, u, vv, w);
+    const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
+    k_rhs<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(v, u, vv, w);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply(const SceneView& v, cudaStream_t st)
+{
+    const float *u, *vv, *w;
+    pressure_buffers(v, u, vv, w);
+    const size_t total = faces_total(v);
+    k_apply<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(v, (float*)u, (float*)vv, (float*)w);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cfl(const SceneView& v, double dt, double* out_max, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(out_max, 0, sizeof(double), st);
+    if (e != cudaSuccess) return e;
+    k_cfl<<<148 * 4, 256, 0, st>>>(v, v.u, v.v, v.w, dt, (unsigned long long*)out_max);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_divergence(const SceneView& v, double* out, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), st);
+    if (e != cudaSuccess) return e;
+    k_divergence<<<148 * 4, 256, 0, st>>>(v, v.u, v.v, v.w, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_out(const SceneView& v, float* pos, float* vel, float* C, cudaStream_t st)
+{
+    if (v.np == 0) return cudaSuccess;
+    k_scatter_out<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, pos, vel, C);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace fe

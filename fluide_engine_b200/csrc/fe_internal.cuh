@@ -1,0 +1,176 @@
+// fe_internal.cuh -- shared device state and helpers of the B200 substep kernels.
+//
+// Layout in HBM (one scene):
+//   particles  FP32 struct of arrays px,py,pz,vx,vy,vz (+ c0..c8 for APIC), kept sorted by cell key,
+//              double-buffered for the sort's gather; pid = original particle index.
+//   MAC grid   FP32 u (nx+1)ny nz, v nx(ny+1)nz, w nx ny(nz+1), x-fastest as the reference's Array3;
+//              ping-pong copies for extrapolation, FP32 FLIP snapshot, u8 face markers, FP32 P2G
+//              accumulators (numerator, weight).
+//   cells      u8 marks (AIR 0 / FLUID 1), FP64 pressure (warm start kept between substeps),
+//              FP64 right-hand side, FP32 CG vectors r, d (two), q, x.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fluide_b200.h"
+#include "fe_keys.h"
+
+namespace fe {
+
+constexpr int kMaxRefineDefault = 12;
+
+struct GridDims {
+    int nx, ny, nz;
+    int tnx, tny, tnz;      // tiles per axis
+    uint32_t key_space;     // tiles * 512
+};
+
+// Everything a kernel needs, passed by value.
+struct SceneView {
+    GridDims g;
+    int solver;
+    uint64_t np;
+    // geometry (FP64 master copies; FP32 views for the particle kernels)
+    double h[3], inv_h[3], origin[3], size[3];
+    float hf[3], inv_hf[3], originf[3], sizef[3];
+    float xo[3], yo[3], zo[3];        // velocity-grid data origins (origin-independent, see fe_scene.cu)
+    float rxo[3], ryo[3], rzo[3];     // FLIP residual-grid data origins
+    float blend;
+    double gravity[3];
+    double max_cfl;
+    int extrap_depth, rk_substeps;
+    // particles
+    float *px, *py, *pz, *vx, *vy, *vz;
+    float* c[9];
+    uint32_t* pid;
+    // sort scratch
+    uint32_t *key, *rank, *perm, *cell_count, *cell_start;
+    // grid
+    float *u, *v, *w;
+    float *u2, *v2, *w2;
+    float *su, *sv, *sw;
+    float *nu, *nv, *nw;   // P2G numerators
+    float *du, *dv, *dw;   // P2G weights
+    uint8_t *mu, *mv, *mw; // P2G face markers
+    uint8_t *mu2, *mv2, *mw2; // extrapolation validity ping-pong
+    uint8_t* marks;
+    double *p, *b;
+    // marking tables (per axis, FP64)
+    double* q_pos[3];      // sdf node coordinate of each index
+    int* q_b0[3];          // hash bucket of the node
+    int* q_b1[3];          // the second bucket chosen by the half test
+    uint8_t* q_exact[3];   // 1 if the cell-centre sample hits the node exactly
+    int* q_i0[3];          // GetBarycentric index of the cell-centre sample
+    double* q_f[3];        // GetBarycentric fraction of the cell-centre sample
+    double sdf_origin[3];
+    double radius, band, bucket;   // r = 1.2 max(h)/sqrt(2), 2r, hash spacing 2r
+    uint32_t* crit_list;   // cells whose mark needs the full trilinear sample
+    uint32_t* crit_count;
+    uint8_t* crit_flag;
+    int any_inexact;
+};
+
+// Error bookkeeping (fe_scene.cu).
+fe_status set_error(fe_status st, const char* fmt, ...);
+fe_status cuda_check(cudaError_t e, const char* what);
+void count_launch(uint64_t n = 1);
+
+#define FE_CUDA(call)                                                      \
+    do {                                                                   \
+        cudaError_t e_ = (call);                                           \
+        if (e_ != cudaSuccess) return ::fe::cuda_check(e_, #call);        \
+    } while (0)
+
+__host__ __device__ __forceinline__ size_t idx3(int i, int j, int k, int sx, int sy)
+{
+    return (size_t)i + (size_t)sx * ((size_t)j + (size_t)sy * (size_t)k);
+}
+
+// GetBarycentric with iLow = 0 (common/math_utils.hpp:48-73), FP32.
+__device__ __forceinline__ void bary(float x, int iHigh, int& i, float& f)
+{
+    float s = floorf(x);
+    int ii = (int)s;  // cvt.rzi saturates, so huge or NaN inputs stay finite
+    if (iHigh == 0 || ii < 0 || !(x == x)) {
+        ii = 0;
+        f = 0.f;
+    } else if (ii > iHigh - 1) {
+        ii = iHigh - 1;
+        f = 1.f;
+    } else {
+        f = x - s;
+    }
+    i = ii;
+}
+
+// Clamped trilinear sample of a face array (FaceCenteredGrid3D::SampleArray,
+// grid_systems/face_centered_grid3d.cpp:339-371), FP32, Lerp order of common/math_utils.hpp:30-46.
+__device__ __forceinline__ float lerpf_ref(float a, float b, float f) { return (1.f - f) * a + f * b; }
+
+struct Stencil {
+    int i, j, k, ip, jp, kp;
+    float fx, fy, fz;
+};
+
+__device__ __forceinline__ Stencil stencil(float x, float y, float z, const float o[3], const float ih[3], int sx,
+                                           int sy, int sz)
+{
+    Stencil s;
+    bary((x - o[0]) * ih[0], sx - 1, s.i, s.fx);
+    bary((y - o[1]) * ih[1], sy - 1, s.j, s.fy);
+    bary((z - o[2]) * ih[2], sz - 1, s.k, s.fz);
+    s.ip = min(s.i + 1, sx - 1);
+    s.jp = min(s.j + 1, sy - 1);
+    s.kp = min(s.k + 1, sz - 1);
+    return s;
+}
+
+__device__ __forceinline__ float sample_st(const float* __restrict__ a, const Stencil& s, int sx, int sy)
+{
+    float c000 = __ldg(a + idx3(s.i, s.j, s.k, sx, sy)), c100 = __ldg(a + idx3(s.ip, s.j, s.k, sx, sy));
+    float c010 = __ldg(a + idx3(s.i, s.jp, s.k, sx, sy)), c110 = __ldg(a + idx3(s.ip, s.jp, s.k, sx, sy));
+    float c001 = __ldg(a + idx3(s.i, s.j, s.kp, sx, sy)), c101 = __ldg(a + idx3(s.ip, s.j, s.kp, sx, sy));
+    float c011 = __ldg(a + idx3(s.i, s.jp, s.kp, sx, sy)), c111 = __ldg(a + idx3(s.ip, s.jp, s.kp, sx, sy));
+    float b0 = lerpf_ref(lerpf_ref(c000, c100, s.fx), lerpf_ref(c010, c110, s.fx), s.fy);
+    float b1 = lerpf_ref(lerpf_ref(c001, c101, s.fx), lerpf_ref(c011, c111, s.fx), s.fy);
+    return lerpf_ref(b0, b1, s.fz);
+}
+
+__device__ __forceinline__ float sample_face(const float* __restrict__ a, float x, float y, float z, const float o[3],
+                                             const float ih[3], int sx, int sy, int sz)
+{
+    Stencil s = stencil(x, y, z, o, ih, sx, sy, sz);
+    return sample_st(a, s, sx, sy);
+}
+
+// Kernel launchers (one per .cu file).
+cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, size_t scan_tmp_bytes);
+size_t sort_scan_tmp_bytes(uint32_t n);
+cudaError_t launch_gather(const SceneView& v, const SceneView& dst, cudaStream_t st);
+cudaError_t launch_p2g(const SceneView& v, cudaStream_t st);
+cudaError_t launch_mark(const SceneView& v, cudaStream_t st);
+cudaError_t launch_fluid_sdf(const SceneView& v, double* out, cudaStream_t st);
+cudaError_t launch_pre(const SceneView& v, double dt, cudaStream_t st);
+cudaError_t launch_post(const SceneView& v, cudaStream_t st);
+cudaError_t launch_rhs(const SceneView& v, cudaStream_t st);
+cudaError_t launch_apply(const SceneView& v, cudaStream_t st);
+cudaError_t launch_g2p(const SceneView& v, double dt, bool do_g2p, bool do_move, cudaStream_t st);
+cudaError_t launch_cfl(const SceneView& v, double dt, double* out_max, cudaStream_t st);
+cudaError_t launch_divergence(const SceneView& v, double* out, cudaStream_t st);
+cudaError_t launch_scatter_out(const SceneView& v, float* pos, float* vel, float* C, cudaStream_t st);
+
+// CG solver (fe_cg.cu).
+struct CgWork {
+    float *r, *d0, *d1, *q, *x;
+    double* partial;        // [blocks][4]
+    unsigned* bar;          // [0] count, [1] generation
+    int* err;
+    fe_step_stats* stats;   // device
+    int blocks, threads;
+};
+cudaError_t cg_prepare(CgWork& w, int device);
+cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, double inner_tol, int max_it, int max_refine,
+                      cudaStream_t st);
+
+}  // namespace fe

@@ -1,0 +1,181 @@
+// fe_mark.cu -- FLUID / AIR cell marking (K_mark), bit-exact with the reference.
+//
+// Reference: PICSimulator::BuildSignedDistanceField (pic_simulator.cpp:452-475) builds, at every
+// cell-centred node c, sdf(c) = min(2r, min |p - c| over the particles its hash searcher visits) - r
+// with r = 1.2 max(h) / sqrt(2); HashGridParticleSearcher::ForEachNearbyPoint
+// (particle_systems/hash_grid_particle_searcher.cpp:97-126,154-204) visits the particles of 8 buckets of
+// edge 2r (the node's bucket and, per axis, the neighbour on the side of the node's half) whose squared
+// distance is <= (2r)^2.  SinglePhasePressureSolver::BuildMarkers (fluid_solvers/
+// single_phase_pressure_solver.cpp:30-48) then marks a cell FLUID iff the trilinear sample of sdf at
+// the cell centre is < 0.
+//
+// When the cell-centre sample lands exactly on node c (every power-of-two grid on an origin-0 domain,
+// checked per axis on the host), the mark is FLUID iff some visited particle has |p - c| < r, because
+// a - r < 0 <=> a < r in IEEE arithmetic.  K_mark therefore scatters from particles: each particle tests
+// the few nodes within r of it with the reference's exact FP64 expressions (no fused multiply-add,
+// correctly rounded sqrt, the same bucket membership) and stores FLUID.  On axes where the sample is off
+// the node by a rounding error, the sign of the sample equals the sign of the node value unless the
+// node value is within ~1e-15 r of zero; such "critical" cells are listed and re-evaluated with the full
+// band SDF and the reference's trilinear sample by k_mark_fixup.  The result is byte-identical to the
+// reference in every case.
+#include "fe_internal.cuh"
+
+namespace fe {
+namespace {
+
+__device__ __forceinline__ double dist2_ref(double px, double py, double pz, double cx, double cy, double cz)
+{
+    // (p - c).GetLengthSquared() = x*x + y*y + z*z, left to right, each operation rounded
+    double dx = __dsub_rn(px, cx), dy = __dsub_rn(py, cy), dz = __dsub_rn(pz, cz);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ int bucket_of(double x, double spacing)
+{
+    return (int)floor(__ddiv_rn(x, spacing));
+}
+
+__device__ __forceinline__ bool visited(const SceneView& v, int pbx, int pby, int pbz, int i, int j, int k)
+{
+    return (pbx == v.q_b0[0][i] || pbx == v.q_b1[0][i]) && (pby == v.q_b0[1][j] || pby == v.q_b1[1][j]) &&
+           (pbz == v.q_b0[2][k] || pbz == v.q_b1[2][k]);
+}
+
+__global__ void k_mark(SceneView v, double R2, double crit_eps)
+{
+    uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (p >= v.np) return;
+    const double X[3] = {(double)v.px[p], (double)v.py[p], (double)v.pz[p]};
+    const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
+    int lo[3], hi[3], pb[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        // nodes within r along this axis, widened by one node on each side (the exact test filters)
+        double t = (X[a] - v.sdf_origin[a]) * v.inv_h[a];
+        double rr = v.radius * v.inv_h[a];
+        int l = (int)floor(t - rr) - 1, h = (int)floor(t + rr) + 1;
+        lo[a] = max(l, 0);
+        hi[a] = min(h, n[a] - 1);
+        pb[a] = bucket_of(X[a], v.bucket);
+    }
+    for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+                if (!visited(v, pb[0], pb[1], pb[2], i, j, k)) continue;
+                const double d2 = dist2_ref(X[0], X[1], X[2], v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]);
+                if (!(d2 <= R2)) continue;
+                const double dist = __dsqrt_rn(d2);
+                const size_t c = idx3(i, j, k, n[0], n[1]);
+                if (dist < v.radius) v.marks[c] = FE_CELL_FLUID;
+                if (v.any_inexact && !(v.q_exact[0][i] && v.q_exact[1][j] && v.q_exact[2][k]) &&
+                    fabs(dist - v.radius) <= crit_eps) {
+                    unsigned* word = (unsigned*)(v.crit_flag + (c & ~(size_t)3));
+                    unsigned bit = 1u << (8 * (c & 3));
+                    if (!(atomicOr(word, bit) & bit)) {
+                        uint32_t slot = atomicAdd(v.crit_count, 1u);
+                        v.crit_list[slot] = (uint32_t)c;
+                    }
+                }
+            }
+}
+
+// Band-limited SDF value of node (i, j, k) exactly as BuildSignedDistanceField computes it.
+__device__ double node_sdf(const SceneView& v, int i, int j, int k, double R2)
+{
+    const double q[3] = {v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]};
+    double minDistance = v.band;
+    const int c0[3] = {i, j, k};
+    const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
+    int lo[3], hi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = max(c0[a] - 2, 0);
+        hi[a] = min(c0[a] + 2, n[a] - 1);
+    }
+    for (int cz = lo[2]; cz <= hi[2]; ++cz)
+        for (int cy = lo[1]; cy <= hi[1]; ++cy)
+            for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+                const uint32_t key = fe_cell_key(cx, cy, cz, n[0], n[1]);
+                for (uint32_t p = v.cell_start[key]; p < v.cell_start[key + 1]; ++p) {
+                    const double X = v.px[p], Y = v.py[p], Z = v.pz[p];
+                    if (!visited(v, bucket_of(X, v.bucket), bucket_of(Y, v.bucket), bucket_of(Z, v.bucket), i, j, k))
+                        continue;
+                    const double d2 = dist2_ref(X, Y, Z, q[0], q[1], q[2]);
+                    if (!(d2 <= R2)) continue;
+                    const double dist = __dsqrt_rn(d2);
+                    if (dist < minDistance) minDistance = dist;
+                }
+            }
+    return __dsub_rn(minDistance, v.radius);
+}
+
+__device__ __forceinline__ double lerp_ref(double a, double b, double f)
+{
+    return __dadd_rn(__dmul_rn(__dsub_rn(1.0, f), a), __dmul_rn(f, b));
+}
+
+// ScalarGrid3D::Sample at the cell centre (3d/scalar_grid3d.cpp:33-65) with exact band SDF values.
+__device__ double sample_cell_sdf(const SceneView& v, int i, int j, int k, double R2)
+{
+    const int i0 = v.q_i0[0][i], j0 = v.q_i0[1][j], k0 = v.q_i0[2][k];
+    const double fx = v.q_f[0][i], fy = v.q_f[1][j], fz = v.q_f[2][k];
+    const int ip = min(i0 + 1, v.g.nx - 1), jp = min(j0 + 1, v.g.ny - 1), kp = min(k0 + 1, v.g.nz - 1);
+    const double c000 = node_sdf(v, i0, j0, k0, R2), c100 = node_sdf(v, ip, j0, k0, R2);
+    const double c010 = node_sdf(v, i0, jp, k0, R2), c110 = node_sdf(v, ip, jp, k0, R2);
+    const double c001 = node_sdf(v, i0, j0, kp, R2), c101 = node_sdf(v, ip, j0, kp, R2);
+    const double c011 = node_sdf(v, i0, jp, kp, R2), c111 = node_sdf(v, ip, jp, kp, R2);
+    const double b0 = lerp_ref(lerp_ref(c000, c100, fx), lerp_ref(c010, c110, fx), fy);
+    const double b1 = lerp_ref(lerp_ref(c001, c101, fx), lerp_ref(c011, c111, fx), fy);
+    return lerp_ref(b0, b1, fz);
+}
+
+__global__ void k_mark_fixup(SceneView v, double R2, uint32_t cap)
+{
+    const uint32_t count = min(*v.crit_count, cap);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const uint32_t c = v.crit_list[t];
+        const int i = c % v.g.nx, j = (c / v.g.nx) % v.g.ny, k = c / (v.g.nx * v.g.ny);
+        v.marks[c] = sample_cell_sdf(v, i, j, k, R2) < 0.0 ? FE_CELL_FLUID : FE_CELL_AIR;
+    }
+}
+
+__global__ void k_fluid_sdf(SceneView v, double R2, double* out)
+{
+    const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = c % v.g.nx, j = (c / v.g.nx) % v.g.ny, k = c / ((size_t)v.g.nx * v.g.ny);
+        out[c] = v.np ? node_sdf(v, i, j, k, R2) : __dsub_rn(v.band, v.radius);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_mark(const SceneView& v, cudaStream_t st)
+{
+    const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
+    cudaError_t e = cudaMemsetAsync(v.marks, FE_CELL_AIR, nc, st);
+    if (e != cudaSuccess) return e;
+    const double R2 = v.band * v.band;
+    if (v.any_inexact) {
+        if ((e = cudaMemsetAsync(v.crit_flag, 0, (nc + 3) & ~(size_t)3, st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(v.crit_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+    }
+    if (v.np > 0) {
+        k_mark<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, R2, 1e-9 * v.radius);
+        count_launch();
+        if (v.any_inexact) {
+            k_mark_fixup<<<148, 128, 0, st>>>(v, R2, (uint32_t)nc);
+            count_launch();
+        }
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fluid_sdf(const SceneView& v, double* out, cudaStream_t st)
+{
+    k_fluid_sdf<<<148 * 8, 128, 0, st>>>(v, v.band * v.band, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace fe

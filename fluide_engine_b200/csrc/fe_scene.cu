@@ -1,0 +1,970 @@
+// fe_scene.cu -- scene lifecycle, substep orchestration (CUDA graphs) and the C ABI of fluide_b200.h.
+//
+// One substep is the reference's PICSimulator::OnAdvanceTimeStep (pic_simulator.cpp:111-154) with no
+// emitters, no colliders and zero viscosity:
+//   SORT -> P2G -> MARK -> PRE (extrapolate, BC, gravity, BC) -> PRESSURE (rhs, CG, apply) ->
+//   POST (extrapolate, BC) -> G2P + MOVE
+// For a fixed dt a substep is captured once as three CUDA graphs (pre-solve, solve, post-solve) per
+// particle-buffer parity (the sort gathers into the other buffer set, so substeps alternate between two
+// graph sets) and replayed; the phase split lets the profiled entry point time the CG kernel with events.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "fe_internal.cuh"
+#include "fe_seed.h"
+
+namespace fe {
+
+static thread_local char g_err[512] = "";
+static std::atomic<uint64_t> g_launches{0};
+static thread_local bool g_capturing = false;
+static thread_local uint64_t g_capture_launches = 0;
+
+fe_status set_error(fe_status st, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return st;
+}
+
+fe_status cuda_check(cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return FE_OK;
+    if (e == cudaErrorMemoryAllocation) return set_error(FE_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+        return set_error(FE_ERR_NO_DEVICE, "%s: %s", what, cudaGetErrorString(e));
+    return set_error(FE_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+void count_launch(uint64_t n)
+{
+    if (g_capturing) g_capture_launches += n;
+    else g_launches += n;
+}
+
+namespace {
+
+__global__ void k_set_particles(SceneView v, const float* pos, const float* vel, const float* C, uint64_t n)
+{
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    v.px[i] = pos[3 * i];
+    v.py[i] = pos[3 * i + 1];
+    v.pz[i] = pos[3 * i + 2];
+    v.vx[i] = vel ? vel[3 * i] : 0.f;
+    v.vy[i] = vel ? vel[3 * i + 1] : 0.f;
+    v.vz[i] = vel ? vel[3 * i + 2] : 0.f;
+    v.pid[i] = (uint32_t)i;
+    if (v.solver == FE_SOLVER_APIC)
+        for (int a = 0; a < 9; ++a) v.c[a][i] = C ? C[9 * i + a] : 0.f;
+}
+
+__global__ void k_sorted_keys(SceneView v, uint32_t* out)
+{
+    uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s >= v.np) return;
+    out[s] = v.key[v.perm[s]];
+}
+
+__global__ void k_perm_ids(const uint32_t* perm, const uint32_t* pid_old, uint32_t* out, uint64_t n)
+{
+    uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    out[s] = pid_old[perm[s]];
+}
+
+struct ParticleSet {
+    float *px, *py, *pz, *vx, *vy, *vz;
+    float* c[9];
+    uint32_t* pid;
+};
+
+}  // namespace
+}  // namespace fe
+
+using namespace fe;
+
+struct fe_scene {
+    fe_scene_desc desc;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    SceneView base;            // grid + scratch pointers; particle pointers filled per parity
+    ParticleSet set[2];
+    int parity = 0;            // which particle set holds the particles
+    int grid_cur = 0;          // 0: velocity in buffer A (u,v,w), 1: in buffer B (u2,v2,w2)
+    uint64_t cap = 0;
+    bool have_particles = false;
+    std::vector<void*> allocs;         // grid-lifetime allocations
+    std::vector<void*> particle_allocs;
+    void* scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    CgWork cg{};
+    double* d_scalar = nullptr;        // CFL / divergence result
+    float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
+    uint32_t* staging_u32 = nullptr;
+    fe_step_stats* stats_ring = nullptr;
+    // graphs per particle parity, valid for graph_dt
+    cudaGraphExec_t graph[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    uint64_t graph_kernels[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    double graph_dt = -1.0;
+    bool graphs_disabled = false;
+    std::mutex mu;
+};
+
+namespace {
+
+SceneView view_of(const fe_scene* s, int parity)
+{
+    SceneView v = s->base;
+    const ParticleSet& p = s->set[parity];
+    v.px = p.px; v.py = p.py; v.pz = p.pz;
+    v.vx = p.vx; v.vy = p.vy; v.vz = p.vz;
+    for (int a = 0; a < 9; ++a) v.c[a] = p.c[a];
+    v.pid = p.pid;
+    return v;
+}
+
+template <class T>
+cudaError_t dalloc(std::vector<void*>& list, T** out, size_t count)
+{
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
+    if (e != cudaSuccess) return e;
+    list.push_back(p);
+    *out = (T*)p;
+    return cudaSuccess;
+}
+
+void free_list(std::vector<void*>& list)
+{
+    for (void* p : list) cudaFree(p);
+    list.clear();
+}
+
+void drop_graphs(fe_scene* s)
+{
+    for (int i = 0; i < 2; ++i)
+        for (int ph = 0; ph < 3; ++ph)
+            if (s->graph[i][ph]) {
+                cudaGraphExecDestroy(s->graph[i][ph]);
+                s->graph[i][ph] = nullptr;
+            }
+    s->graph_dt = -1.0;
+}
+
+// GetBarycentric (common/math_utils.hpp:48-73) in FP64 on the host.
+void bary_host(double x, int iHigh, int* i, double* f)
+{
+    double sfl = std::floor(x);
+    int ii = (int)sfl;
+    if (iHigh == 0 || ii < 0) { ii = 0; *f = 0; }
+    else if (ii > iHigh - 1) { ii = iHigh - 1; *f = 1; }
+    else *f = x - sfl;
+    *i = ii;
+}
+
+fe_status alloc_grid(fe_scene* s)
+{
+    SceneView& v = s->base;
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const size_t nc = (size_t)nx * ny * nz;
+    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz, nww = (size_t)nx * ny * (nz + 1);
+    const size_t nf = nu + nvv + nww;
+    auto& L = s->allocs;
+    float *A, *B, *S, *N, *D;
+    uint8_t *M, *M2;
+    FE_CUDA(dalloc(L, &A, nf));
+    FE_CUDA(dalloc(L, &B, nf));
+    FE_CUDA(dalloc(L, &S, nf));
+    FE_CUDA(dalloc(L, &N, nf));
+    FE_CUDA(dalloc(L, &D, nf));
+    FE_CUDA(dalloc(L, &M, nf));
+    FE_CUDA(dalloc(L, &M2, 2 * nf));
+    v.u = A; v.v = A + nu; v.w = A + nu + nvv;
+    v.u2 = B; v.v2 = B + nu; v.w2 = B + nu + nvv;
+    v.su = S; v.sv = S + nu; v.sw = S + nu + nvv;
+    v.nu = N; v.nv = N + nu; v.nw = N + nu + nvv;
+    v.du = D; v.dv = D + nu; v.dw = D + nu + nvv;
+    v.mu = M; v.mv = M + nu; v.mw = M + nu + nvv;
+    v.mu2 = M2; v.mv2 = M2 + nu; v.mw2 = M2 + nu + nvv;
+    FE_CUDA(cudaMemset(A, 0, nf * sizeof(float)));
+    FE_CUDA(cudaMemset(B, 0, nf * sizeof(float)));
+    FE_CUDA(cudaMemset(S, 0, nf * sizeof(float)));
+    FE_CUDA(cudaMemset(M, 0, nf));
+    FE_CUDA(dalloc(L, &v.marks, nc));
+    FE_CUDA(cudaMemset(v.marks, 0, nc));
+    FE_CUDA(dalloc(L, &v.p, nc));
+    FE_CUDA(cudaMemset(v.p, 0, nc * sizeof(double)));
+    FE_CUDA(dalloc(L, &v.b, nc));
+    FE_CUDA(cudaMemset(v.b, 0, nc * sizeof(double)));
+    // sort scratch over the key space
+    FE_CUDA(dalloc(L, &v.cell_count, v.g.key_space));
+    FE_CUDA(dalloc(L, &v.cell_start, (size_t)v.g.key_space + 1));
+    FE_CUDA(cudaMemset(v.cell_start, 0, ((size_t)v.g.key_space + 1) * sizeof(uint32_t)));
+    s->scan_tmp_bytes = sort_scan_tmp_bytes(v.g.key_space);
+    uint8_t* tmp;
+    FE_CUDA(dalloc(L, &tmp, s->scan_tmp_bytes));
+    s->scan_tmp = tmp;
+    // CG vectors
+    CgWork& w = s->cg;
+    FE_CUDA(dalloc(L, &w.r, nc));
+    FE_CUDA(dalloc(L, &w.d0, nc));
+    FE_CUDA(dalloc(L, &w.d1, nc));
+    FE_CUDA(dalloc(L, &w.q, nc));
+    FE_CUDA(dalloc(L, &w.x, nc));
+    FE_CUDA(cg_prepare(w, s->device));
+    FE_CUDA(dalloc(L, &w.partial, (size_t)w.blocks * 4));
+    FE_CUDA(dalloc(L, &w.bar, 8));
+    FE_CUDA(cudaMemset(w.bar, 0, 8 * sizeof(unsigned)));
+    FE_CUDA(dalloc(L, &w.err, 1));
+    FE_CUDA(cudaMemset(w.err, 0, sizeof(int)));
+    FE_CUDA(dalloc(L, &s->stats_ring, (size_t)1 << 16));
+    w.stats = s->stats_ring;
+    FE_CUDA(dalloc(L, &s->d_scalar, 4));
+    // marking tables
+    const int n[3] = {nx, ny, nz};
+    double maxH = std::max(v.h[0], std::max(v.h[1], v.h[2]));
+    v.radius = 1.2 * maxH / std::sqrt(2.0);  // pic_simulator.cpp:458-460
+    v.band = 2.0 * v.radius;
+    v.bucket = 2 * v.radius;                 // BuildSearcher(..., 2 * radious), pic_simulator.cpp:462
+    v.any_inexact = 0;
+    for (int a = 0; a < 3; ++a) {
+        std::vector<double> qpos(n[a]), qf(n[a]);
+        std::vector<int> b0(n[a]), b1(n[a]), i0(n[a]);
+        std::vector<uint8_t> ex(n[a]);
+        for (int i = 0; i < n[a]; ++i) {
+            qpos[i] = v.sdf_origin[a] + i * v.h[a];                          // Grid3D::GridIndexToPosition
+            b0[i] = (int)std::floor(qpos[i] / v.bucket);                     // GetBucketIndex
+            b1[i] = (((float)b0[i] + 0.5f) * v.bucket <= qpos[i]) ? b0[i] + 1 : b0[i] - 1;  // GetNearbyKeys
+            double cc = (v.origin[a] + 0.5 * v.h[a]) + v.h[a] * i;          // GetCellCenterPos
+            double t = (cc - v.sdf_origin[a]) / v.h[a];                      // ScalarGrid3D::Sample
+            bary_host(t, n[a] - 1, &i0[i], &qf[i]);
+            ex[i] = ((qf[i] == 0.0 && i0[i] == i) || (qf[i] == 1.0 && i0[i] + 1 == i)) ? 1 : 0;
+            if (!ex[i]) v.any_inexact = 1;
+        }
+        FE_CUDA(dalloc(L, &v.q_pos[a], n[a]));
+        FE_CUDA(dalloc(L, &v.q_f[a], n[a]));
+        FE_CUDA(dalloc(L, &v.q_b0[a], n[a]));
+        FE_CUDA(dalloc(L, &v.q_b1[a], n[a]));
+        FE_CUDA(dalloc(L, &v.q_i0[a], n[a]));
+        FE_CUDA(dalloc(L, &v.q_exact[a], n[a]));
+        FE_CUDA(cudaMemcpy(v.q_pos[a], qpos.data(), n[a] * sizeof(double), cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemcpy(v.q_f[a], qf.data(), n[a] * sizeof(double), cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemcpy(v.q_b0[a], b0.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemcpy(v.q_b1[a], b1.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemcpy(v.q_i0[a], i0.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemcpy(v.q_exact[a], ex.data(), n[a], cudaMemcpyHostToDevice));
+    }
+    if (v.any_inexact) {
+        FE_CUDA(dalloc(L, &v.crit_list, nc));
+        FE_CUDA(dalloc(L, &v.crit_count, 1));
+        FE_CUDA(dalloc(L, &v.crit_flag, (nc + 3) & ~(size_t)3));
+    }
+    return FE_OK;
+}
+
+fe_status alloc_particles(fe_scene* s, uint64_t cap)
+{
+    drop_graphs(s);
+    free_list(s->particle_allocs);
+    auto& L = s->particle_allocs;
+    const bool apic = s->desc.solver == FE_SOLVER_APIC;
+    for (int k = 0; k < 2; ++k) {
+        ParticleSet& p = s->set[k];
+        FE_CUDA(dalloc(L, &p.px, cap));
+        FE_CUDA(dalloc(L, &p.py, cap));
+        FE_CUDA(dalloc(L, &p.pz, cap));
+        FE_CUDA(dalloc(L, &p.vx, cap));
+        FE_CUDA(dalloc(L, &p.vy, cap));
+        FE_CUDA(dalloc(L, &p.vz, cap));
+        FE_CUDA(dalloc(L, &p.pid, cap));
+        for (int a = 0; a < 9; ++a) {
+            p.c[a] = nullptr;
+            if (apic) FE_CUDA(dalloc(L, &p.c[a], cap));
+        }
+    }
+    SceneView& v = s->base;
+    FE_CUDA(dalloc(L, &v.key, cap));
+    FE_CUDA(dalloc(L, &v.rank, cap));
+    FE_CUDA(dalloc(L, &v.perm, cap));
+    FE_CUDA(dalloc(L, &s->staging, cap * 9));
+    FE_CUDA(dalloc(L, &s->staging_u32, cap));
+    s->cap = cap;
+    return FE_OK;
+}
+
+// Makes the velocity live in buffer `want` (0 = A, 1 = B); only stage-by-stage runs ever need the copy.
+cudaError_t ensure_grid(fe_scene* s, int want)
+{
+    if (s->grid_cur == want) return cudaSuccess;
+    const SceneView& v = s->base;
+    const size_t nf = (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz + (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz +
+                      (size_t)v.g.nx * v.g.ny * (v.g.nz + 1);
+    float* src = s->grid_cur ? v.u2 : v.u;
+    float* dst = want ? v.u2 : v.u;
+    s->grid_cur = want;
+    return cudaMemcpyAsync(dst, src, nf * sizeof(float), cudaMemcpyDeviceToDevice, s->stream);
+}
+
+int pressure_buffer(const fe_scene* s) { return (s->base.extrap_depth > 0 && (s->base.extrap_depth & 1)) ? 1 : 0; }
+
+// Internal steps of one substep; the public fe_stage ids map onto ranges of them.
+enum { kStepSort, kStepP2g, kStepMark, kStepPre, kStepRhs, kStepCg, kStepApply, kStepPost, kStepG2p, kStepMove,
+       kStepCount };
+
+int first_step(int stage)
+{
+    static const int m[FE_STAGE_COUNT] = {kStepSort, kStepP2g, kStepMark, kStepPre, kStepRhs, kStepPost, kStepG2p, kStepMove};
+    return m[stage];
+}
+int last_step(int stage)
+{
+    static const int m[FE_STAGE_COUNT] = {kStepSort, kStepP2g, kStepMark, kStepPre, kStepApply, kStepPost, kStepG2p, kStepMove};
+    return m[stage];
+}
+
+// Enqueues internal steps [first, last] of one substep on s->stream.
+fe_status enqueue_steps(fe_scene* s, double dt, int first, int last)
+{
+    cudaStream_t st = s->stream;
+    for (int step = first; step <= last; ++step) {
+        SceneView v = view_of(s, s->parity);
+        switch (step) {
+        case kStepSort: {
+            FE_CUDA(launch_sort(v, st, s->scan_tmp, s->scan_tmp_bytes));
+            SceneView dst = view_of(s, s->parity ^ 1);
+            FE_CUDA(launch_gather(v, dst, st));
+            s->parity ^= 1;
+            break;
+        }
+        case kStepP2g:
+            FE_CUDA(launch_p2g(v, st));
+            s->grid_cur = 0;
+            break;
+        case kStepMark:
+            FE_CUDA(launch_mark(v, st));
+            break;
+        case kStepPre:
+            FE_CUDA(ensure_grid(s, 0));
+            FE_CUDA(launch_pre(v, dt, st));
+            s->grid_cur = pressure_buffer(s);
+            break;
+        case kStepRhs:
+            FE_CUDA(ensure_grid(s, pressure_buffer(s)));
+            FE_CUDA(launch_rhs(v, st));
+            break;
+        case kStepCg:
+            FE_CUDA(launch_cg(v, s->cg, s->desc.cg_rel_tol, s->desc.cg_inner_tol, s->desc.cg_max_it,
+                              s->desc.max_refine, st));
+            break;
+        case kStepApply:
+            FE_CUDA(ensure_grid(s, pressure_buffer(s)));
+            FE_CUDA(launch_apply(v, st));
+            break;
+        case kStepPost:
+            FE_CUDA(ensure_grid(s, pressure_buffer(s)));
+            FE_CUDA(launch_post(v, st));
+            s->grid_cur = 0;
+            break;
+        case kStepG2p:
+            FE_CUDA(ensure_grid(s, 0));
+            if (last >= kStepMove) {
+                FE_CUDA(launch_g2p(v, dt, true, true, st));
+                step = kStepMove;
+            } else {
+                FE_CUDA(launch_g2p(v, dt, true, false, st));
+            }
+            break;
+        case kStepMove:
+            FE_CUDA(ensure_grid(s, 0));
+            FE_CUDA(launch_g2p(v, dt, false, true, st));
+            break;
+        default:
+            return set_error(FE_ERR_BAD_ARG, "unknown step %d", step);
+        }
+    }
+    return FE_OK;
+}
+
+fe_status enqueue_stages(fe_scene* s, double dt, int first_stage, int last_stage)
+{
+    return enqueue_steps(s, dt, first_step(first_stage), last_step(last_stage));
+}
+
+// The three phases a substep graph is split into: everything before the solve, the solve, the rest.
+const int kPhaseFirst[3] = {kStepSort, kStepCg, kStepApply};
+const int kPhaseLast[3] = {kStepRhs, kStepCg, kStepMove};
+
+fe_status check_device_error(fe_scene* s)
+{
+    int err = 0;
+    FE_CUDA(cudaMemcpyAsync(&err, s->cg.err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    if (err) {
+        cudaMemsetAsync(s->cg.err, 0, sizeof(int), s->stream);
+        cudaMemsetAsync(s->cg.bar, 0, 2 * sizeof(unsigned), s->stream);
+        cudaStreamSynchronize(s->stream);
+        return set_error((fe_status)err, "pressure solve: grid barrier wait exceeded its limit");
+    }
+    return FE_OK;
+}
+
+fe_status capture_graphs(fe_scene* s, int parity, double dt)
+{
+    const int saved_parity = s->parity, saved_grid = s->grid_cur;
+    s->parity = parity;
+    s->grid_cur = 0;
+    fe_status result = FE_OK;
+    for (int ph = 0; ph < 3 && result == FE_OK; ++ph) {
+        cudaGraph_t g = nullptr;
+        g_capturing = true;
+        g_capture_launches = 0;
+        cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+        fe_status st = e == cudaSuccess ? enqueue_steps(s, dt, kPhaseFirst[ph], kPhaseLast[ph])
+                                        : cuda_check(e, "begin capture");
+        cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+        g_capturing = false;
+        if (st != FE_OK) {
+            if (g) cudaGraphDestroy(g);
+            result = st;
+            break;
+        }
+        if (e2 != cudaSuccess) {
+            result = cuda_check(e2, "end capture");
+            break;
+        }
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            result = cuda_check(e, "graph instantiate");
+            break;
+        }
+        s->graph[parity][ph] = exec;
+        s->graph_kernels[parity][ph] = g_capture_launches;
+    }
+    s->parity = saved_parity;
+    s->grid_cur = saved_grid;
+    return result;
+}
+
+// One substep: the three phase graphs of the current parity (captured on first use for this dt); when
+// `ev` is non-null, events ev[0..3] are recorded before, between and after the phases.
+fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
+{
+    if (!s->graphs_disabled) {
+        if (s->graph_dt != dt) {
+            drop_graphs(s);
+            s->graph_dt = dt;
+        }
+        const int par = s->parity;
+        if (!s->graph[par][0]) {
+            fe_status st = capture_graphs(s, par, dt);
+            if (st != FE_OK) {
+                // Capture is an optimisation; fall back to direct launches.
+                cudaGetLastError();
+                s->graphs_disabled = true;
+                drop_graphs(s);
+            }
+        }
+    }
+    if (s->graphs_disabled) {
+        for (int ph = 0; ph < 3; ++ph) {
+            if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
+            fe_status st = enqueue_steps(s, dt, kPhaseFirst[ph], kPhaseLast[ph]);
+            if (st != FE_OK) return st;
+        }
+        if (ev) FE_CUDA(cudaEventRecord(ev[3], s->stream));
+        return FE_OK;
+    }
+    const int par = s->parity;
+    for (int ph = 0; ph < 3; ++ph) {
+        if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
+        FE_CUDA(cudaGraphLaunch(s->graph[par][ph], s->stream));
+        g_launches += s->graph_kernels[par][ph];
+    }
+    if (ev) FE_CUDA(cudaEventRecord(ev[3], s->stream));
+    s->parity ^= 1;  // the sort inside the first graph flipped the buffer sets
+    s->grid_cur = 0;
+    return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fe_status fe_scene_desc_default(fe_scene_desc* d)
+{
+    if (!d) return set_error(FE_ERR_BAD_ARG, "null descriptor");
+    memset(d, 0, sizeof(*d));
+    d->n[0] = d->n[1] = d->n[2] = 32;
+    d->size[0] = d->size[1] = d->size[2] = 1.0;
+    d->solver = FE_SOLVER_FLIP;
+    d->flip_blend = 0.05;
+    d->gravity[1] = -9.81;
+    d->max_cfl = 3.0;
+    d->cg_rel_tol = 1e-6;
+    d->cg_max_it = 2000;
+    d->cg_inner_tol = 1e-3;
+    d->max_refine = kMaxRefineDefault;
+    d->device = 0;
+    return FE_OK;
+}
+
+fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
+{
+    if (!desc || !out) return set_error(FE_ERR_BAD_ARG, "null argument");
+    *out = nullptr;
+    for (int a = 0; a < 3; ++a) {
+        if (desc->n[a] < 2 || desc->n[a] > 4096) return set_error(FE_ERR_BAD_ARG, "grid size must be in [2, 4096]");
+        if (!(desc->size[a] > 0.0)) return set_error(FE_ERR_BAD_ARG, "domain size must be positive");
+    }
+    if ((uint64_t)fe_key_space(desc->n[0], desc->n[1], desc->n[2]) >= (1ull << 32) - 2)
+        return set_error(FE_ERR_BAD_ARG, "grid too large for 32-bit cell keys");
+    if (desc->solver < FE_SOLVER_PIC || desc->solver > FE_SOLVER_APIC) return set_error(FE_ERR_BAD_ARG, "bad solver");
+    if (!(desc->max_cfl > 0.0) || desc->max_cfl > 64.0) return set_error(FE_ERR_BAD_ARG, "max_cfl must be in (0, 64]");
+    if (!(desc->cg_rel_tol > 0.0) || desc->cg_max_it < 1) return set_error(FE_ERR_BAD_ARG, "bad CG settings");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return set_error(FE_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    if (desc->device < 0 || desc->device >= ndev) return set_error(FE_ERR_BAD_ARG, "device %d out of range", desc->device);
+    FE_CUDA(cudaSetDevice(desc->device));
+
+    fe_scene* s = new (std::nothrow) fe_scene();
+    if (!s) return set_error(FE_ERR_OOM, "host allocation failed");
+    s->desc = *desc;
+    if (s->desc.cg_inner_tol <= 0.0 || s->desc.cg_inner_tol >= 1.0) s->desc.cg_inner_tol = 1e-3;
+    if (s->desc.max_refine <= 0) s->desc.max_refine = kMaxRefineDefault;
+    s->device = desc->device;
+    SceneView& v = s->base;
+    memset(&v, 0, sizeof(v));
+    v.g.nx = desc->n[0];
+    v.g.ny = desc->n[1];
+    v.g.nz = desc->n[2];
+    v.g.tnx = fe_tiles(v.g.nx);
+    v.g.tny = fe_tiles(v.g.ny);
+    v.g.tnz = fe_tiles(v.g.nz);
+    v.g.key_space = fe_key_space(v.g.nx, v.g.ny, v.g.nz);
+    v.solver = desc->solver;
+    for (int a = 0; a < 3; ++a) {
+        v.h[a] = desc->size[a] / (double)desc->n[a];  // hybrid_simulator.cpp:8
+        v.inv_h[a] = 1.0 / v.h[a];
+        v.origin[a] = desc->origin[a];
+        v.size[a] = desc->size[a];
+        v.hf[a] = (float)v.h[a];
+        v.inv_hf[a] = (float)((double)desc->n[a] / desc->size[a]);
+        v.originf[a] = (float)desc->origin[a];
+        v.sizef[a] = (float)desc->size[a];
+        v.gravity[a] = desc->gravity[a];
+        v.sdf_origin[a] = desc->origin[a] + v.h[a] / 2.0;  // hybrid_simulator.cpp:15
+    }
+    // Velocity-grid data origins: CalculateDataOrigins (grid_systems/face_centered_grid3d.cpp:324-332) runs in
+    // SetGridSpacing before SetOrigin (hybrid_simulator.cpp:11-12) and is not re-run, so they ignore the domain
+    // origin.  The FLIP residual grid is built with the origin (flip_simulator.cpp:5).
+    const double half[3][3] = {{0, 0.5, 0.5}, {0.5, 0, 0.5}, {0.5, 0.5, 0}};
+    for (int a = 0; a < 3; ++a) {
+        v.xo[a] = (float)(0.0 + v.h[a] * half[0][a]);
+        v.yo[a] = (float)(0.0 + v.h[a] * half[1][a]);
+        v.zo[a] = (float)(0.0 + v.h[a] * half[2][a]);
+        v.rxo[a] = (float)(desc->origin[a] + v.h[a] * half[0][a]);
+        v.ryo[a] = (float)(desc->origin[a] + v.h[a] * half[1][a]);
+        v.rzo[a] = (float)(desc->origin[a] + v.h[a] * half[2][a]);
+    }
+    v.blend = (float)desc->flip_blend;
+    v.max_cfl = desc->max_cfl;
+    v.extrap_depth = (int)std::ceil(desc->max_cfl);                         // pic_simulator.cpp:491
+    v.rk_substeps = (int)(unsigned)std::max(desc->max_cfl, 1.0);            // pic_simulator.cpp:255
+    fe_status st = alloc_grid(s);
+    if (st == FE_OK) {
+        e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) st = cuda_check(e, "stream create");
+        s->stream = s->own_stream;
+    }
+    if (st == FE_OK && desc->max_particles > 0) st = alloc_particles(s, desc->max_particles);
+    if (st != FE_OK) {
+        free_list(s->allocs);
+        free_list(s->particle_allocs);
+        if (s->own_stream) cudaStreamDestroy(s->own_stream);
+        delete s;
+        return st;
+    }
+    *out = s;
+    return FE_OK;
+}
+
+fe_status fe_scene_destroy(fe_scene* s)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    drop_graphs(s);
+    free_list(s->allocs);
+    free_list(s->particle_allocs);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
+    return FE_OK;
+}
+
+fe_status fe_scene_set_particles(fe_scene* s, const float* pos, const float* vel, const float* C, uint64_t n)
+{
+    if (!s || (!pos && n)) return set_error(FE_ERR_BAD_ARG, "null argument");
+    if (n >= (1ull << 32) - 1) return set_error(FE_ERR_BAD_ARG, "at most 2^32-2 particles per scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    if (n > s->cap || !s->set[0].px) {
+        FE_CUDA(cudaStreamSynchronize(s->stream));
+        fe_status st = alloc_particles(s, std::max<uint64_t>(n, 1));
+        if (st != FE_OK) return st;
+    }
+    if (n != s->base.np) drop_graphs(s);
+    s->base.np = n;
+    s->parity = 0;
+    if (n) {
+        // staging holds 9 floats per particle: pos at [0, 3n), vel at [3n, 6n); C reuses it afterwards
+        float* stp = s->staging;
+        FE_CUDA(cudaMemcpyAsync(stp, pos, n * 3 * sizeof(float), cudaMemcpyDefault, s->stream));
+        if (vel) FE_CUDA(cudaMemcpyAsync(stp + 3 * n, vel, n * 3 * sizeof(float), cudaMemcpyDefault, s->stream));
+        SceneView v = view_of(s, 0);
+        k_set_particles<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(v, stp, vel ? stp + 3 * n : nullptr,
+                                                                          nullptr, n);
+        count_launch();
+        FE_CUDA(cudaGetLastError());
+        if (C && s->desc.solver == FE_SOLVER_APIC) {
+            // stream order: the copy below starts after k_set_particles consumed the staging buffer
+            FE_CUDA(cudaMemcpyAsync(stp, C, n * 9 * sizeof(float), cudaMemcpyDefault, s->stream));
+            for (int a = 0; a < 9; ++a)  // deinterleave: c[a][i] = C[9 i + a]
+                FE_CUDA(cudaMemcpy2DAsync(v.c[a], sizeof(float), stp + a, 9 * sizeof(float), sizeof(float), n,
+                                          cudaMemcpyDeviceToDevice, s->stream));
+        }
+    }
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    s->have_particles = true;
+    return FE_OK;
+}
+
+fe_status fe_scene_get_particles(fe_scene* s, float* pos, float* vel, float* C, uint64_t n)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (n != s->base.np) return set_error(FE_ERR_BAD_ARG, "particle count mismatch (%llu vs %llu)",
+                                          (unsigned long long)n, (unsigned long long)s->base.np);
+    if (!n) return FE_OK;
+    FE_CUDA(cudaSetDevice(s->device));
+    SceneView v = view_of(s, s->parity);
+    float* stp = s->staging;
+    const bool wantC = C && s->desc.solver == FE_SOLVER_APIC;
+    FE_CUDA(launch_scatter_out(v, pos ? stp : nullptr, vel ? stp + 3 * n : nullptr, nullptr, s->stream));
+    if (pos) FE_CUDA(cudaMemcpyAsync(pos, stp, n * 3 * sizeof(float), cudaMemcpyDefault, s->stream));
+    if (vel) FE_CUDA(cudaMemcpyAsync(vel, stp + 3 * n, n * 3 * sizeof(float), cudaMemcpyDefault, s->stream));
+    if (wantC) {
+        FE_CUDA(cudaStreamSynchronize(s->stream));
+        FE_CUDA(launch_scatter_out(v, nullptr, nullptr, stp, s->stream));
+        FE_CUDA(cudaMemcpyAsync(C, stp, n * 9 * sizeof(float), cudaMemcpyDefault, s->stream));
+    } else if (C) {
+        std::vector<float> z(n * 9, 0.f);
+        FE_CUDA(cudaMemcpyAsync(C, z.data(), n * 9 * sizeof(float), cudaMemcpyDefault, s->stream));
+        FE_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_num_particles(const fe_scene* s, uint64_t* n)
+{
+    if (!s || !n) return set_error(FE_ERR_BAD_ARG, "null argument");
+    *n = s->base.np;
+    return FE_OK;
+}
+
+fe_status fe_scene_step(fe_scene* s, double dt, int32_t nsub, fe_step_stats* stats)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
+    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles before stepping");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    if (stats) FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), s->stream));
+    for (int i = 0; i < nsub; ++i) {
+        fe_status st = run_substep(s, dt, nullptr);
+        if (st != FE_OK) return st;
+    }
+    if (stats && nsub > 0) {
+        const int cnt = std::min(nsub, 1 << 16);
+        FE_CUDA(cudaMemcpyAsync(stats, s->stats_ring, cnt * sizeof(fe_step_stats), cudaMemcpyDeviceToHost, s->stream));
+        fe_status st = check_device_error(s);
+        if (st != FE_OK) return st;
+    }
+    return FE_OK;
+}
+
+fe_status fe_scene_step_profiled(fe_scene* s, double dt, int32_t nsub, fe_step_stats* stats, float* phase_ms)
+{
+    if (!s || !phase_ms) return set_error(FE_ERR_BAD_ARG, "null argument");
+    if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
+    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles before stepping");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    std::vector<cudaEvent_t> ev((size_t)nsub * 4);
+    for (auto& e : ev) FE_CUDA(cudaEventCreate(&e));
+    fe_status st = FE_OK;
+    if (stats) FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), s->stream));
+    for (int i = 0; i < nsub && st == FE_OK; ++i) st = run_substep(s, dt, &ev[(size_t)i * 4]);
+    if (st == FE_OK) {
+        cudaError_t e = cudaStreamSynchronize(s->stream);
+        for (int i = 0; i < nsub && e == cudaSuccess; ++i)
+            for (int ph = 0; ph < 3 && e == cudaSuccess; ++ph)
+                e = cudaEventElapsedTime(&phase_ms[i * 3 + ph], ev[(size_t)i * 4 + ph], ev[(size_t)i * 4 + ph + 1]);
+        st = cuda_check(e, "phase timing");
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (st != FE_OK) return st;
+    if (stats && nsub > 0) {
+        const int cnt = std::min(nsub, 1 << 16);
+        FE_CUDA(cudaMemcpyAsync(stats, s->stats_ring, cnt * sizeof(fe_step_stats), cudaMemcpyDeviceToHost, s->stream));
+    }
+    return check_device_error(s);
+}
+
+fe_status fe_scene_cfl(fe_scene* s, double dt, double* cfl)
+{
+    if (!s || !cfl) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    FE_CUDA(ensure_grid(s, 0));
+    FE_CUDA(launch_cfl(s->base, dt, s->d_scalar, s->stream));
+    double m = 0;
+    FE_CUDA(cudaMemcpyAsync(&m, s->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    const double minH = std::min(s->base.h[0], std::min(s->base.h[1], s->base.h[2]));
+    *cfl = m * dt / minH;  // pic_simulator.cpp:94-96
+    return FE_OK;
+}
+
+fe_status fe_scene_advance_frame(fe_scene* s, double frame_dt, int32_t* substeps)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    if (!(frame_dt > 0.0)) return set_error(FE_ERR_BAD_ARG, "frame_dt must be > 0");
+    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles before stepping");
+    double remaining = frame_dt;
+    int count = 0;
+    while (remaining > 0.0000000001) {  // physics_animation.cpp:76
+        double cfl = 0;
+        fe_status st = fe_scene_cfl(s, remaining, &cfl);
+        if (st != FE_OK) return st;
+        const double c = std::ceil(cfl / s->desc.max_cfl);
+        const unsigned n = (unsigned)std::max(c, 1.0);  // pic_simulator.cpp:353
+        const double sub = remaining / (double)n;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            FE_CUDA(cudaSetDevice(s->device));
+            st = enqueue_stages(s, sub, FE_STAGE_SORT, FE_STAGE_MOVE);
+            if (st != FE_OK) return st;
+        }
+        remaining -= sub;
+        ++count;
+        if (count > 100000) return set_error(FE_ERR_STATE, "substep count exploded (non-finite velocities?)");
+    }
+    if (substeps) *substeps = count;
+    return check_device_error(s);
+}
+
+fe_status fe_scene_run_stages(fe_scene* s, double dt, int32_t first, int32_t last)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    if (first < 0 || last >= FE_STAGE_COUNT || first > last) return set_error(FE_ERR_BAD_ARG, "bad stage range");
+    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles before stepping");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), s->stream));
+    fe_status st = enqueue_stages(s, dt, first, last);
+    if (st != FE_OK) return st;
+    return check_device_error(s);
+}
+
+fe_status fe_scene_get_grid(fe_scene* s, float* u, float* v, float* w, double* p, uint8_t* marks)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const SceneView& b = s->base;
+    const size_t nu = (size_t)(b.g.nx + 1) * b.g.ny * b.g.nz, nvv = (size_t)b.g.nx * (b.g.ny + 1) * b.g.nz,
+                 nww = (size_t)b.g.nx * b.g.ny * (b.g.nz + 1), nc = (size_t)b.g.nx * b.g.ny * b.g.nz;
+    const float* src = s->grid_cur ? b.u2 : b.u;
+    if (u) FE_CUDA(cudaMemcpyAsync(u, src, nu * 4, cudaMemcpyDefault, s->stream));
+    if (v) FE_CUDA(cudaMemcpyAsync(v, src + nu, nvv * 4, cudaMemcpyDefault, s->stream));
+    if (w) FE_CUDA(cudaMemcpyAsync(w, src + nu + nvv, nww * 4, cudaMemcpyDefault, s->stream));
+    if (p) FE_CUDA(cudaMemcpyAsync(p, b.p, nc * 8, cudaMemcpyDefault, s->stream));
+    if (marks) FE_CUDA(cudaMemcpyAsync(marks, b.marks, nc, cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_set_grid(fe_scene* s, const float* u, const float* v, const float* w)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const SceneView& b = s->base;
+    const size_t nu = (size_t)(b.g.nx + 1) * b.g.ny * b.g.nz, nvv = (size_t)b.g.nx * (b.g.ny + 1) * b.g.nz,
+                 nww = (size_t)b.g.nx * b.g.ny * (b.g.nz + 1);
+    float* dst = s->grid_cur ? b.u2 : b.u;
+    if (u) FE_CUDA(cudaMemcpyAsync(dst, u, nu * 4, cudaMemcpyDefault, s->stream));
+    if (v) FE_CUDA(cudaMemcpyAsync(dst + nu, v, nvv * 4, cudaMemcpyDefault, s->stream));
+    if (w) FE_CUDA(cudaMemcpyAsync(dst + nu + nvv, w, nww * 4, cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_set_pressure(fe_scene* s, const double* p)
+{
+    if (!s || !p) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+    FE_CUDA(cudaMemcpyAsync(s->base.p, p, nc * 8, cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_get_face_markers(fe_scene* s, uint8_t* mu, uint8_t* mv, uint8_t* mw)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const SceneView& b = s->base;
+    const size_t nu = (size_t)(b.g.nx + 1) * b.g.ny * b.g.nz, nvv = (size_t)b.g.nx * (b.g.ny + 1) * b.g.nz,
+                 nww = (size_t)b.g.nx * b.g.ny * (b.g.nz + 1);
+    if (mu) FE_CUDA(cudaMemcpyAsync(mu, b.mu, nu, cudaMemcpyDefault, s->stream));
+    if (mv) FE_CUDA(cudaMemcpyAsync(mv, b.mv, nvv, cudaMemcpyDefault, s->stream));
+    if (mw) FE_CUDA(cudaMemcpyAsync(mw, b.mw, nww, cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_get_snapshot(fe_scene* s, float* u, float* v, float* w)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const SceneView& b = s->base;
+    const size_t nu = (size_t)(b.g.nx + 1) * b.g.ny * b.g.nz, nvv = (size_t)b.g.nx * (b.g.ny + 1) * b.g.nz,
+                 nww = (size_t)b.g.nx * b.g.ny * (b.g.nz + 1);
+    if (u) FE_CUDA(cudaMemcpyAsync(u, b.su, nu * 4, cudaMemcpyDefault, s->stream));
+    if (v) FE_CUDA(cudaMemcpyAsync(v, b.sv, nvv * 4, cudaMemcpyDefault, s->stream));
+    if (w) FE_CUDA(cudaMemcpyAsync(w, b.sw, nww * 4, cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_get_rhs(fe_scene* s, double* b)
+{
+    if (!s || !b) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+    FE_CUDA(cudaMemcpyAsync(b, s->base.b, nc * 8, cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf)
+{
+    if (!s || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
+    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles first");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    // the band SDF gathers through cell ranges, so sort the current particles first
+    fe_status st = enqueue_stages(s, 1.0, FE_STAGE_SORT, FE_STAGE_SORT);
+    if (st != FE_OK) return st;
+    const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+    double* tmp = nullptr;
+    FE_CUDA(cudaMallocAsync((void**)&tmp, nc * sizeof(double), s->stream));
+    cudaError_t e = launch_fluid_sdf(view_of(s, s->parity), tmp, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sdf, tmp, nc * 8, cudaMemcpyDefault, s->stream);
+    cudaFreeAsync(tmp, s->stream);
+    FE_CUDA(e);
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_get_sort(fe_scene* s, uint32_t* keys, uint32_t* perm, uint64_t n)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (n != s->base.np) return set_error(FE_ERR_BAD_ARG, "particle count mismatch");
+    if (!n) return FE_OK;
+    FE_CUDA(cudaSetDevice(s->device));
+    SceneView v = view_of(s, s->parity);
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    if (keys) {
+        k_sorted_keys<<<nb, 256, 0, s->stream>>>(v, s->staging_u32);
+        count_launch();
+        FE_CUDA(cudaMemcpyAsync(keys, s->staging_u32, n * 4, cudaMemcpyDefault, s->stream));
+        FE_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    if (perm) {
+        // slot -> particle id (the ids the particles carried before the last sort)
+        SceneView prev = view_of(s, s->parity ^ 1);
+        k_perm_ids<<<nb, 256, 0, s->stream>>>(v.perm, prev.pid, s->staging_u32, n);
+        count_launch();
+        FE_CUDA(cudaMemcpyAsync(perm, s->staging_u32, n * 4, cudaMemcpyDefault, s->stream));
+    }
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_divergence(fe_scene* s, double* l2)
+{
+    if (!s || !l2) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    FE_CUDA(ensure_grid(s, 0));
+    FE_CUDA(launch_divergence(s->base, s->d_scalar, s->stream));
+    double acc = 0;
+    FE_CUDA(cudaMemcpyAsync(&acc, s->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    *l2 = std::sqrt(acc);
+    return FE_OK;
+}
+
+fe_status fe_scene_set_stream(fe_scene* s, void* stream)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    return FE_OK;
+}
+
+fe_status fe_scene_synchronize(fe_scene* s)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    return check_device_error(s);
+}
+
+uint64_t fe_kernel_launch_count(void) { return g_launches.load(); }
+
+uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[3], const double origin[3],
+                         const double size[3], uint64_t seed, float* pos, float* vel, uint64_t cap)
+{
+    if (!regions || nregions <= 0 || !n || !origin || !size) return 0;
+    const int nn[3] = {n[0], n[1], n[2]};
+    const double h[3] = {size[0] / n[0], size[1] / n[1], size[2] / n[2]};
+    return fe_seed_regions_host((const fe_region*)regions, nregions, nn, origin, h, seed, pos, vel, cap);
+}
+
+const char* fe_last_error(void) { return g_err; }
+
+int32_t fe_abi_version(void) { return 10000; }
+
+}  // extern "C"

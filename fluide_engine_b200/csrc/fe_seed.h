@@ -57,7 +57,7 @@ static inline int fe_region_contains(const fe_region* g, double x, double y, dou
  * origin[3].  Writes at most `cap` particles (xyz interleaved) when pos != NULL and returns the
  * number of particles the rule produces, so a first call with pos == NULL sizes the buffers.
  */
-static inline size_t fe_seed_regions(const fe_region* reg, int nreg, const int n[3], const double origin[3],
+static inline size_t fe_seed_regions_host(const fe_region* reg, int nreg, const int n[3], const double origin[3],
                                      const double h[3], uint64_t seed, float* pos, float* vel, size_t cap)
 {
     fe_rng rng;

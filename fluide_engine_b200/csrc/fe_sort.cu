@@ -1,0 +1,203 @@
+// fe_sort.cu -- cell keys and the stable counting sort of particles by key.
+//
+// The reference has no sort: its P2G scatters from the unsorted particle array with racy += from
+// many threads (pic_simulator.cpp:384-412).  Here particles are kept in cell-key order so that every
+// 8x8x8 tile's particles form one contiguous run (fe_keys.h); P2G then splats a tile in shared memory
+// and the marking scatter writes within a tile's neighbourhood.
+//
+// Stable counting sort, O(N + K):
+//   k_keys     key of each particle, rank = atomic slot in its cell (order among equal keys arbitrary)
+//   scan       exclusive prefix sum of the per-cell counts -> cell_start (K + 1 entries)
+//   k_place    perm[cell_start[key] + rank] = particle
+//   k_segsort  each cell's run re-ordered by particle index, which makes the result identical to a
+//              stable sort by key (the oracle is a CPU stable counting sort of the same keys)
+//   k_gather   particle arrays permuted into the second buffer set
+#include "fe_internal.cuh"
+
+namespace fe {
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void k_keys(SceneView v)
+{
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= v.np) return;
+    uint32_t key = fe_particle_key(v.px[i], v.py[i], v.pz[i], v.originf, v.inv_hf, v.g.nx, v.g.ny, v.g.nz);
+    v.key[i] = key;
+    v.rank[i] = atomicAdd(v.cell_count + key, 1u);
+}
+
+// Inclusive block scan of one value per thread; returns the block total through *total.
+__device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* warp_sums, uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        warp_sums[lane] = s;
+    }
+    __syncthreads();
+    uint32_t before = wid > 0 ? warp_sums[wid - 1] : 0u;
+    *total = warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return x + before;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_partials(const uint32_t* __restrict__ in, uint32_t n,
+                                                                  uint32_t* __restrict__ block_sums)
+{
+    __shared__ uint32_t ws[32];
+    uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t s = 0;
+#pragma unroll
+    for (int t = 0; t < kScanItems; ++t)
+        if (base + t < n) s += in[base + t];
+    uint32_t total;
+    block_incl_scan(s, ws, &total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+// Exclusive scan of the block sums by a single block, looping over chunks of kScanTile.
+__global__ void __launch_bounds__(kScanThreads) k_scan_block_sums(uint32_t* __restrict__ sums, uint32_t nb)
+{
+    __shared__ uint32_t ws[32];
+    uint32_t carry = 0;
+    for (uint32_t chunk = 0; chunk < nb; chunk += kScanTile) {
+        uint32_t base = chunk + threadIdx.x * kScanItems;
+        uint32_t vals[kScanItems];
+        uint32_t s = 0;
+#pragma unroll
+        for (int t = 0; t < kScanItems; ++t) {
+            vals[t] = base + t < nb ? sums[base + t] : 0u;
+            s += vals[t];
+        }
+        uint32_t total;
+        uint32_t incl = block_incl_scan(s, ws, &total);
+        uint32_t run = carry + incl - s;
+#pragma unroll
+        for (int t = 0; t < kScanItems; ++t) {
+            if (base + t < nb) sums[base + t] = run;
+            run += vals[t];
+        }
+        carry += total;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_final(const uint32_t* __restrict__ in, uint32_t n,
+                                                               const uint32_t* __restrict__ block_off,
+                                                               uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t ws[32];
+    uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t vals[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int t = 0; t < kScanItems; ++t) {
+        vals[t] = base + t < n ? in[base + t] : 0u;
+        s += vals[t];
+    }
+    uint32_t total;
+    uint32_t incl = block_incl_scan(s, ws, &total);
+    uint32_t run = block_off[blockIdx.x] + incl - s;
+#pragma unroll
+    for (int t = 0; t < kScanItems; ++t) {
+        if (base + t < n) out[base + t] = run;
+        run += vals[t];
+    }
+    if (base + kScanItems >= n && base < n) out[n] = run;  // the thread holding the last element writes the total
+}
+
+__global__ void k_place(SceneView v)
+{
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= v.np) return;
+    v.perm[v.cell_start[v.key[i]] + v.rank[i]] = (uint32_t)i;
+}
+
+__global__ void k_segsort(SceneView v)
+{
+    uint32_t key = blockIdx.x * blockDim.x + threadIdx.x;
+    if (key >= v.g.key_space) return;
+    uint32_t b = v.cell_start[key], e = v.cell_start[key + 1];
+    if (e - b < 2) return;
+    uint32_t* a = v.perm;
+    for (uint32_t i = b + 1; i < e; ++i) {  // insertion sort: runs are short (about 8 per cell)
+        uint32_t x = a[i];
+        uint32_t j = i;
+        while (j > b && a[j - 1] > x) {
+            a[j] = a[j - 1];
+            --j;
+        }
+        a[j] = x;
+    }
+}
+
+__global__ void k_gather(SceneView src, SceneView dst, int ncomp)
+{
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= src.np) return;
+    uint32_t j = src.perm[i];
+    dst.px[i] = src.px[j];
+    dst.py[i] = src.py[j];
+    dst.pz[i] = src.pz[j];
+    dst.vx[i] = src.vx[j];
+    dst.vy[i] = src.vy[j];
+    dst.vz[i] = src.vz[j];
+    dst.pid[i] = src.pid[j];
+    for (int c = 0; c < ncomp; ++c) dst.c[c][i] = src.c[c][j];
+}
+
+}  // namespace
+
+size_t sort_scan_tmp_bytes(uint32_t n) { return ((n + kScanTile - 1) / kScanTile + 1) * sizeof(uint32_t); }
+
+cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, size_t scan_tmp_bytes)
+{
+    const uint32_t K = v.g.key_space;
+    cudaError_t e = cudaMemsetAsync(v.cell_count, 0, (size_t)K * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const int T = 256;
+    unsigned pb = (unsigned)((v.np + T - 1) / T);
+    if (v.np > 0) {
+        k_keys<<<pb, T, 0, st>>>(v);
+        count_launch();
+    }
+    uint32_t nb = (K + kScanTile - 1) / kScanTile;
+    if (sort_scan_tmp_bytes(K) > scan_tmp_bytes) return cudaErrorInvalidValue;
+    uint32_t* sums = (uint32_t*)scan_tmp;
+    k_scan_partials<<<nb, kScanThreads, 0, st>>>(v.cell_count, K, sums);
+    k_scan_block_sums<<<1, kScanThreads, 0, st>>>(sums, nb);
+    k_scan_final<<<nb, kScanThreads, 0, st>>>(v.cell_count, K, sums, v.cell_start);
+    count_launch(3);
+    if (v.np > 0) {
+        k_place<<<pb, T, 0, st>>>(v);
+        k_segsort<<<(K + T - 1) / T, T, 0, st>>>(v);
+        count_launch(2);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather(const SceneView& v, const SceneView& dst, cudaStream_t st)
+{
+    if (v.np == 0) return cudaSuccess;
+    const int T = 256;
+    k_gather<<<(unsigned)((v.np + T - 1) / T), T, 0, st>>>(v, dst, v.solver == FE_SOLVER_APIC ? 9 : 0);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace fe

@@ -1,0 +1,164 @@
+"""Scene: one device-resident simulation behind the C ABI (include/fluide_b200.h)."""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, ptr
+
+
+def face_shapes(n):
+    """numpy shapes (z, y, x) of the u, v, w face arrays; memory is x-fastest like the reference's Array3."""
+    nx, ny, nz = n
+    return (nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx)
+
+
+class Scene:
+    """Owns an fe_scene.  All arrays exchanged are numpy (host) unless a torch CUDA tensor is passed."""
+
+    def __init__(self, n, solver=_abi.FLIP, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), flip_blend=0.05,
+                 gravity=(0.0, -9.81, 0.0), max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-3,
+                 max_refine=12, device=0, max_particles=0):
+        L = _abi.lib()
+        d = _abi.SceneDesc()
+        check(L.fe_scene_desc_default(ctypes.byref(d)))
+        for a in range(3):
+            d.n[a] = int(n[a])
+            d.origin[a] = origin[a]
+            d.size[a] = size[a]
+            d.gravity[a] = gravity[a]
+        d.solver, d.flip_blend, d.max_cfl = solver, flip_blend, max_cfl
+        d.cg_rel_tol, d.cg_max_it, d.cg_inner_tol, d.max_refine = cg_rel_tol, cg_max_it, cg_inner_tol, max_refine
+        d.device, d.max_particles = device, max_particles
+        h = ctypes.c_void_p()
+        check(L.fe_scene_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self._L = L
+        self.n = tuple(int(x) for x in n)
+        self.solver = solver
+        self.desc = d
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fe_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # particles -----------------------------------------------------------------------------------
+    def set_particles(self, pos, vel=None, C=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float32) if isinstance(pos, np.ndarray) else pos
+        vel = np.ascontiguousarray(vel, dtype=np.float32) if isinstance(vel, np.ndarray) else vel
+        C = np.ascontiguousarray(C, dtype=np.float32) if isinstance(C, np.ndarray) else C
+        check(self._L.fe_scene_set_particles(self._h, ptr(pos), ptr(vel), ptr(C), int(pos.shape[0])))
+
+    def num_particles(self):
+        n = ctypes.c_uint64()
+        check(self._L.fe_scene_num_particles(self._h, ctypes.byref(n)))
+        return n.value
+
+    def particles(self):
+        N = self.num_particles()
+        pos = np.zeros((N, 3), dtype=np.float32)
+        vel = np.zeros((N, 3), dtype=np.float32)
+        C = np.zeros((N, 9), dtype=np.float32)
+        check(self._L.fe_scene_get_particles(self._h, ptr(pos), ptr(vel), ptr(C), N))
+        return pos, vel, C
+
+    # stepping ------------------------------------------------------------------------------------
+    def step(self, dt, nsub=1, stats=True):
+        if stats:
+            arr = (_abi.StepStats * max(nsub, 1))()
+            check(self._L.fe_scene_step(self._h, dt, nsub, arr))
+            return [arr[i].as_dict() for i in range(nsub)]
+        check(self._L.fe_scene_step(self._h, dt, nsub, None))
+        return None
+
+    def step_profiled(self, dt, nsub):
+        """Like step(), plus per-substep phase times in ms: array [nsub, 3] = (pre-solve, CG solve, post-solve)."""
+        arr = (_abi.StepStats * max(nsub, 1))()
+        ms = np.zeros((max(nsub, 1), 3), dtype=np.float32)
+        check(self._L.fe_scene_step_profiled(self._h, dt, nsub, arr, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return [arr[i].as_dict() for i in range(nsub)], ms[:nsub]
+
+    def set_stream(self, stream_handle):
+        """Issues the scene's work on an external cudaStream_t (an int handle, e.g. torch stream.cuda_stream)."""
+        check(self._L.fe_scene_set_stream(self._h, ctypes.c_void_p(stream_handle) if stream_handle else None))
+
+    def advance_frame(self, frame_dt):
+        n = ctypes.c_int32()
+        check(self._L.fe_scene_advance_frame(self._h, frame_dt, ctypes.byref(n)))
+        return n.value
+
+    def run_stages(self, dt, first, last):
+        check(self._L.fe_scene_run_stages(self._h, dt, first, last))
+
+    def cfl(self, dt):
+        c = ctypes.c_double()
+        check(self._L.fe_scene_cfl(self._h, dt, ctypes.byref(c)))
+        return c.value
+
+    def synchronize(self):
+        check(self._L.fe_scene_synchronize(self._h))
+
+    # grid ----------------------------------------------------------------------------------------
+    def grid(self):
+        su, sv, sw = face_shapes(self.n)
+        u, v, w = (np.zeros(s, dtype=np.float32) for s in (su, sv, sw))
+        nx, ny, nz = self.n
+        p = np.zeros((nz, ny, nx), dtype=np.float64)
+        m = np.zeros((nz, ny, nx), dtype=np.uint8)
+        check(self._L.fe_scene_get_grid(self._h, ptr(u), ptr(v), ptr(w), ptr(p), ptr(m)))
+        return u, v, w, p, m
+
+    def set_grid(self, u, v, w):
+        u, v, w = (np.ascontiguousarray(a, dtype=np.float32) for a in (u, v, w))
+        check(self._L.fe_scene_set_grid(self._h, ptr(u), ptr(v), ptr(w)))
+
+    def set_pressure(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        check(self._L.fe_scene_set_pressure(self._h, ptr(p)))
+
+    def face_markers(self):
+        su, sv, sw = face_shapes(self.n)
+        a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
+        check(self._L.fe_scene_get_face_markers(self._h, ptr(a), ptr(b), ptr(c)))
+        return a, b, c
+
+    def snapshot(self):
+        su, sv, sw = face_shapes(self.n)
+        a, b, c = (np.zeros(s, dtype=np.float32) for s in (su, sv, sw))
+        check(self._L.fe_scene_get_snapshot(self._h, ptr(a), ptr(b), ptr(c)))
+        return a, b, c
+
+    def rhs(self):
+        nx, ny, nz = self.n
+        b = np.zeros((nz, ny, nx), dtype=np.float64)
+        check(self._L.fe_scene_get_rhs(self._h, ptr(b)))
+        return b
+
+    def fluid_sdf(self):
+        nx, ny, nz = self.n
+        s = np.zeros((nz, ny, nx), dtype=np.float64)
+        check(self._L.fe_scene_get_fluid_sdf(self._h, ptr(s)))
+        return s
+
+    def sort_result(self):
+        N = self.num_particles()
+        keys = np.zeros(N, dtype=np.uint32)
+        perm = np.zeros(N, dtype=np.uint32)
+        check(self._L.fe_scene_get_sort(self._h, ptr(keys), ptr(perm), N))
+        return keys, perm
+
+    def divergence(self):
+        d = ctypes.c_double()
+        check(self._L.fe_scene_divergence(self._h, ctypes.byref(d)))
+        return d.value

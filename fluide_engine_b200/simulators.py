@@ -1,0 +1,284 @@
+"""Python mirror of the reference's simulator API for the substep path.
+
+Same class and method names as the reference's pybind11 module PyFluidEngine
+(python_wrapper/simulators_wrapper.cu:36-85, frame_wrapper.cpp, vector3_wrapper.cpp,
+bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp) and C++ classes (pic_simulator.hpp:27-43,
+hybrid_simulator.hpp:10-41, physics_animation.hpp:8-19, flip_simulator.hpp:9-16), backed by one
+device-resident Scene.  Only what the substep needs is implemented; entry points of components outside
+it (mesh initialisation, colliders, emitters, viscosity, surface extraction) raise NotImplementedError
+with the reason instead of silently doing something else.
+"""
+import numpy as np
+
+from . import _abi
+from .scene import Scene
+
+
+class Vector3D:
+    """Vector3<double> (common/vector3.hpp)."""
+
+    def __init__(self, x=0.0, y=None, z=None):
+        if y is None:
+            y = z = x
+        self.x, self.y, self.z = float(x), float(y), float(z)
+
+    def __iter__(self):
+        return iter((self.x, self.y, self.z))
+
+    def __repr__(self):
+        return "Vector3D(%g, %g, %g)" % (self.x, self.y, self.z)
+
+
+class Vector3S(Vector3D):
+    """Vector3<size_t>."""
+
+    def __init__(self, x=0, y=None, z=None):
+        if y is None:
+            y = z = x
+        self.x, self.y, self.z = int(x), int(y), int(z)
+
+
+class BoundingBox3D:
+    """BoundingBox3D(origin, size) (3d/bounding_box_3d.cpp:4-8)."""
+
+    def __init__(self, origin=Vector3D(0.0), size=Vector3D(1.0)):
+        self._origin, self._size = Vector3D(*origin), Vector3D(*size)
+
+    def GetOrigin(self):
+        return self._origin
+
+    def GetSize(self):
+        return self._size
+
+
+class Frame:
+    """Frame(timeIntervalInSeconds) with an index (common/frame.cpp:3-49)."""
+
+    def __init__(self, timeIntervalInSeconds=1.0 / 60.0):
+        self._dt = float(timeIntervalInSeconds)
+        self._index = 0
+
+    def GetIndex(self):
+        return self._index
+
+    def GetTimeIntervalInSeconds(self):
+        return self._dt
+
+    def GetTimeInSeconds(self):
+        return self._index * self._dt
+
+    def Advance(self):
+        self._index += 1
+
+
+class ExternalForce:
+    pass
+
+
+class DirectionalField(ExternalForce):
+    """Uniform force field (forces/directional_field.cpp:3-21)."""
+
+    def __init__(self, strength=Vector3D(0.0, -9.81, 0.0)):
+        self._strength = Vector3D(*strength)
+
+    def Sample(self, position=None):
+        return self._strength
+
+    def SetStrength(self, strength):
+        self._strength = Vector3D(*strength)
+
+
+class HybridSimulator:
+    """HybridSimulator (hybrid_simulator.cpp:4-110) over a device Scene."""
+
+    _solver = _abi.PIC
+
+    def __init__(self, gridSize, domain, device=0):
+        self._n = (int(gridSize.x), int(gridSize.y), int(gridSize.z))
+        self._domain = domain
+        o, s = domain.GetOrigin(), domain.GetSize()
+        self._origin = (o.x, o.y, o.z)
+        self._size = (s.x, s.y, s.z)
+        self._h = tuple(self._size[a] / self._n[a] for a in range(3))
+        self._maxCfl = 3.0              # hybrid_simulator.cpp:21
+        self._particlesPerBlok = 16     # hybrid_simulator.cpp:22
+        self._viscosity = 0.0
+        self._density = 1.0
+        self._blend = 0.05
+        self._forces = []
+        self._device = device
+        self._scene = None
+        self._pending = None            # (pos, vel, C) until the scene exists
+        self._currentFrame = Frame()
+        self._currentTime = 0.0
+        self._cg = dict(cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-3, max_refine=12)
+        self.last_stats = []
+
+    # settings -------------------------------------------------------------------------------------
+    def MaxCfl(self):
+        return self._maxCfl
+
+    def SetMaxClf(self, maxCfl):
+        self._rebuild(lambda: setattr(self, "_maxCfl", float(maxCfl)))
+
+    SetMaxCfl = SetMaxClf  # the name the reference's Python example calls (python_example.py:30)
+
+    def GetViscosity(self):
+        return self._viscosity
+
+    def SetViscosity(self, viscosity):
+        if viscosity != 0.0:
+            raise NotImplementedError("viscosity (BackwardEulerDiffusionSolver) is outside the substep path")
+        self._viscosity = 0.0
+
+    def GetDensity(self):
+        return self._density
+
+    def SetDensity(self, density):
+        self._density = float(density)  # unused by the projection, as in the reference
+
+    def GetParticlesPerBlock(self):
+        return self._particlesPerBlok
+
+    def SetParticlesPerBlock(self, n):
+        self._particlesPerBlok = int(n)
+
+    def GetOrigin(self):
+        return Vector3D(*self._origin)
+
+    def GetResolution(self):
+        return Vector3S(*self._n)
+
+    def GetGridSpacing(self):
+        return Vector3D(*self._h)
+
+    def GetNumberOfParticles(self):
+        if self._scene is not None:
+            return self._scene.num_particles()
+        return 0 if self._pending is None else self._pending[0].shape[0]
+
+    def SetPressureSolverSettings(self, cg_rel_tol=None, cg_max_it=None, cg_inner_tol=None, max_refine=None):
+        upd = {k: v for k, v in dict(cg_rel_tol=cg_rel_tol, cg_max_it=cg_max_it, cg_inner_tol=cg_inner_tol,
+                                     max_refine=max_refine).items() if v is not None}
+        self._rebuild(lambda: self._cg.update(upd))
+
+    # forces / scene contents ----------------------------------------------------------------------
+    def AddExternalForce(self, force):
+        if not isinstance(force, DirectionalField):
+            raise NotImplementedError("only DirectionalField forces are on the substep path")
+        self._rebuild(lambda: self._forces.append(force))
+
+    def AddCollider(self, collider):
+        raise NotImplementedError("colliders are outside the substep path (no benchmark scene has one)")
+
+    def AddEmitter(self, emitter):
+        raise NotImplementedError("emitters are outside the substep path (no benchmark scene has one)")
+
+    def InitializeFromTriangleMesh(self, mesh):
+        raise NotImplementedError("mesh seeding (Mesh2SDF) is outside the substep path; use InitializeFromRegions")
+
+    def GetSurface(self, mesh):
+        raise NotImplementedError("surface extraction (marching cubes) is outside the substep path")
+
+    def InitializeFromRegions(self, regions, seed=0):
+        """Seeds boxes / spheres with the deterministic subcell rule (8 particles per cell)."""
+        pos, vel = _abi.seed_regions(regions, self._n, self._origin, self._size, seed)
+        self.SetParticles(pos, vel)
+        return pos.shape[0]
+
+    def SetParticles(self, pos, vel=None, C=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        vel = np.zeros_like(pos) if vel is None else np.ascontiguousarray(vel, dtype=np.float32)
+        self._pending = (pos, vel, C)
+        if self._scene is not None:
+            self._scene.set_particles(pos, vel, C)
+            self._pending = None
+
+    def GetParticles(self):
+        if self._scene is not None:
+            return self._scene.particles()
+        if self._pending is None:
+            return np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), np.zeros((0, 9), np.float32)
+        p, v, c = self._pending
+        return p, v, (np.zeros((p.shape[0], 9), np.float32) if c is None else c)
+
+    def GetFluidSdf(self):
+        return self._ensure_scene().fluid_sdf()
+
+    def Cfl(self, timeIntervalInSeconds):
+        return self._ensure_scene().cfl(timeIntervalInSeconds)
+
+    # PhysicsAnimation -----------------------------------------------------------------------------
+    def SetCurrentFrame(self, frame):
+        self._currentFrame = frame
+
+    def GetCurrentFrame(self):
+        return self._currentFrame
+
+    def GetCurrentTimeInSeconds(self):
+        return self._currentTime
+
+    def AdvanceSingleFrame(self):
+        """PhysicsAnimation::AdvanceSingleFrame (physics_animation.cpp:17-21, 48-61, 64-92)."""
+        scene = self._ensure_scene()
+        self._currentTime = self._currentFrame.GetTimeInSeconds()
+        dt = self._currentFrame.GetTimeIntervalInSeconds()
+        n = scene.advance_frame(dt)
+        self._currentTime += dt
+        self._currentFrame.Advance()
+        return n
+
+    def AdvanceFixedSubsteps(self, dt, nsub, stats=True):
+        """nsub substeps of exactly dt (the benchmark configurations' fixed-dt mode)."""
+        self.last_stats = self._ensure_scene().step(dt, nsub, stats=stats) or []
+        return self.last_stats
+
+    # internals ------------------------------------------------------------------------------------
+    def _gravity(self):
+        g = [0.0, 0.0, 0.0]
+        for f in self._forces:
+            s = f.Sample()
+            g = [g[0] + s.x, g[1] + s.y, g[2] + s.z]
+        return tuple(g)
+
+    def _ensure_scene(self):
+        if self._scene is None:
+            self._scene = Scene(self._n, solver=self._solver, origin=self._origin, size=self._size,
+                                flip_blend=self._blend, gravity=self._gravity(), max_cfl=self._maxCfl,
+                                device=self._device, **self._cg)
+            if self._pending is not None:
+                p, v, c = self._pending
+                self._scene.set_particles(p, v, c)
+                self._pending = None
+        return self._scene
+
+    def _rebuild(self, change):
+        """Applies a settings change; a live scene is rebuilt with its particles and pressure kept."""
+        if self._scene is None:
+            change()
+            return
+        pos, vel, C = self._scene.particles()
+        p = self._scene.grid()[3]
+        self._scene.close()
+        self._scene = None
+        change()
+        self._pending = (pos, vel, C if self._solver == _abi.APIC else None)
+        self._ensure_scene().set_pressure(p)
+
+
+class PICSimulator(HybridSimulator):
+    _solver = _abi.PIC
+
+
+class FLIPSimulator(HybridSimulator):
+    _solver = _abi.FLIP
+
+    def SetBlendingFactor(self, factor):
+        self._rebuild(lambda: setattr(self, "_blend", float(factor)))
+
+    def GetBlendingFactor(self):
+        return self._blend
+
+
+class APICSimulator(HybridSimulator):
+    _solver = _abi.APIC

@@ -1,0 +1,171 @@
+/*
+ * fluide_b200.h -- C ABI of the B200-native hybrid particle-grid (PIC / FLIP / APIC) substep.
+ *
+ * One fe_scene owns one simulation's state resident in HBM: FP32 particles (struct of arrays,
+ * kept sorted by cell key), the FP32 staggered MAC grid, FP64 pressure and the solver scratch.
+ * All entry points return an fe_status; no entry point throws or aborts.  Pointers passed for
+ * particle / grid data may be host or device pointers (they are copied with cudaMemcpyDefault).
+ * Layouts match the reference: face arrays u (nx+1)*ny*nz, v nx*(ny+1)*nz, w nx*ny*(nz+1) and cell
+ * arrays nx*ny*nz, all x-fastest (common/array3.hpp:65-85); particle arrays are xyz-interleaved.
+ *
+ * Reference citations are relative to AleksanderSiwek/Fluide_Engine's src/ directory.
+ */
+#ifndef FLUIDE_B200_H
+#define FLUIDE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FE_OK = 0,
+    FE_ERR_CUDA = 1,           /* a CUDA runtime call failed; fe_last_error() has the message */
+    FE_ERR_BAD_ARG = 2,        /* invalid argument (null handle, size mismatch, bad descriptor) */
+    FE_ERR_OOM = 3,            /* device allocation failed */
+    FE_ERR_NOT_CONVERGED = 4,  /* pressure solve hit its iteration cap (state is still advanced) */
+    FE_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up; the context stays usable */
+    FE_ERR_STATE = 6,          /* call out of order (e.g. step before particles are set) */
+    FE_ERR_NO_DEVICE = 7       /* no CUDA device / the library was built without device code */
+} fe_status;
+
+typedef enum { FE_SOLVER_PIC = 0, FE_SOLVER_FLIP = 1, FE_SOLVER_APIC = 2 } fe_solver_kind;
+
+typedef enum { FE_CELL_AIR = 0, FE_CELL_FLUID = 1, FE_CELL_BOUNDRY = 2 } fe_cell_mark;
+
+/* Scene description.  Mirrors the state the reference constructors fix:
+ * PICSimulator(gridSize, domain) (pic_simulator.cpp:17-26, hybrid_simulator.cpp:4-25),
+ * FLIPSimulator::SetBlendingFactor (flip_simulator.cpp:15-18), HybridSimulator::SetMaxClf
+ * (hybrid_simulator.cpp:92-95), DirectionalField gravity (forces/directional_field.cpp:3-16) and the
+ * pressure solver settings (linear_system/conjugate_gradient_solver.cpp:3-7). */
+typedef struct {
+    int32_t n[3];            /* cells per axis (gridSize) */
+    double origin[3];        /* BoundingBox3D origin */
+    double size[3];          /* BoundingBox3D size; grid spacing h = size / n */
+    int32_t solver;          /* fe_solver_kind */
+    double flip_blend;       /* v = (1 - blend) * flip + blend * pic; reference default 0.05 */
+    double gravity[3];       /* external acceleration added to every face each substep */
+    double max_cfl;          /* extrapolation depth ceil(max_cfl), RK2 sub-steps max(max_cfl,1) */
+    double cg_rel_tol;       /* stop when ||b - A p||_2 <= cg_rel_tol * ||b||_2 (FP64 test) */
+    int32_t cg_max_it;       /* cap on inner FP32 CG iterations per pressure solve */
+    double cg_inner_tol;     /* relative residual reduction asked of each FP32 inner solve */
+    int32_t max_refine;      /* cap on FP64 outer refinement steps per pressure solve */
+    int32_t device;          /* CUDA device ordinal */
+    uint64_t max_particles;  /* capacity; 0 = sized by the first fe_scene_set_particles */
+} fe_scene_desc;
+
+/* Per-substep statistics. */
+typedef struct {
+    int32_t cg_iterations;     /* inner FP32 CG iterations */
+    int32_t refinements;       /* FP64 outer refinement steps */
+    int32_t converged;         /* 1 if ||b - A p|| <= tol * ||b|| */
+    int32_t fluid_cells;       /* number of FLUID-marked cells */
+    double rel_residual;       /* final FP64 ||b - A p|| / ||b|| */
+    double b_norm;             /* ||b||_2 (divergence before projection over FLUID cells) */
+} fe_step_stats;
+
+typedef struct fe_scene fe_scene;
+
+/* Stages of one substep, in PICSimulator::OnAdvanceTimeStep order (pic_simulator.cpp:111-196). */
+typedef enum {
+    FE_STAGE_SORT = 0,       /* cell keys + stable counting sort (no reference counterpart) */
+    FE_STAGE_P2G = 1,        /* TransferParticles2Grid (pic :356-437, flip :25-119, apic :15-118) */
+    FE_STAGE_MARK = 2,       /* BuildSignedDistanceField + BuildMarkers (pic :452-475, single_phase :30-48) */
+    FE_STAGE_PRE = 3,        /* ExtrapolateVelocityToAir + BC + gravity + BC (pic :186-212) */
+    FE_STAGE_PRESSURE = 4,   /* BuildSystem + CG + ApplyPressure + BC (pic :224-229) */
+    FE_STAGE_POST = 5,       /* ExtrapolateVelocityToAir + BC (pic :233-234) */
+    FE_STAGE_G2P = 6,        /* TransferGrid2Particles (pic :439-450, flip :121-161, apic :120-176) */
+    FE_STAGE_MOVE = 7,       /* MoveParticles (pic :239-312) */
+    FE_STAGE_COUNT = 8
+} fe_stage;
+
+/* Fills *d with the reference defaults (maxCfl 3 from hybrid_simulator.cpp:21, blend 0.05 from
+ * flip_simulator.cpp:5, gravity (0,-9.81,0), CG rel 1e-6 / 500 iterations). */
+fe_status fe_scene_desc_default(fe_scene_desc* d);
+
+/* Creates a scene on desc->device.  Replaces PICSimulator/FLIPSimulator/APICSimulator construction
+ * (pic_simulator.cpp:17-26, flip_simulator.cpp:4-8, apic_simulator.cpp:4-7). */
+fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out);
+
+/* Frees all device memory of the scene. */
+fe_status fe_scene_destroy(fe_scene* s);
+
+/* Sets the particles: pos and vel are n*3 floats (xyz interleaved), C is n*9 floats (rows cX, cY, cZ
+ * of apic_simulator.hpp:21-23) or NULL for zero.  Replaces ParticleSystem::AddParticles /
+ * SetVectorValues (particle_systems/particle_system.cpp:36-44,97-107) and APICSimulator::_cX.. */
+fe_status fe_scene_set_particles(fe_scene* s, const float* pos, const float* vel, const float* C, uint64_t n);
+
+/* Copies the particles out in the order they were set (ParticleSystem::GetVectorValues,
+ * particle_systems/particle_system.cpp:133-141).  Any pointer may be NULL. */
+fe_status fe_scene_get_particles(fe_scene* s, float* pos, float* vel, float* C, uint64_t n);
+
+/* Number of particles (HybridSimulator::GetNumberOfParticles, hybrid_simulator.cpp:87-90). */
+fe_status fe_scene_num_particles(const fe_scene* s, uint64_t* n);
+
+/* Runs nsub substeps of fixed length dt (PICSimulator::OnAdvanceTimeStep, pic_simulator.cpp:111-154),
+ * replayed as three captured CUDA graphs per substep.  stats may be NULL (no host synchronisation then); else it
+ * receives nsub entries and the call synchronises the scene's stream. */
+fe_status fe_scene_step(fe_scene* s, double dt, int32_t nsub, fe_step_stats* stats);
+
+/* fe_scene_step with per-substep device timing: CUDA events recorded on the scene's stream before, between
+ * and after the three phase graphs of each substep (pre-solve: SORT..PRE + rhs; solve: the CG kernel;
+ * post-solve: apply..MOVE).  phase_ms receives nsub * 3 floats; the call synchronises. */
+fe_status fe_scene_step_profiled(fe_scene* s, double dt, int32_t nsub, fe_step_stats* stats, float* phase_ms);
+
+/* Advances one frame of length frame_dt with the reference's CFL-adaptive substepping
+ * (PhysicsAnimation::AdvanceSingleFrame / AdvanceTimeStep, physics_animation.cpp:17-21,64-92, with
+ * PICSimulator::NumberOfSubTimeSteps, pic_simulator.cpp:349-354).  *substeps receives the count. */
+fe_status fe_scene_advance_frame(fe_scene* s, double frame_dt, int32_t* substeps);
+
+/* CFL number of the current grid for interval dt (PICSimulator::Cfl, pic_simulator.cpp:80-97). */
+fe_status fe_scene_cfl(fe_scene* s, double dt, double* cfl);
+
+/* Runs stages [first, last] of one substep of length dt (for stage-by-stage parity checks). */
+fe_status fe_scene_run_stages(fe_scene* s, double dt, int32_t first, int32_t last);
+
+/* Grid access (Fluid3 velocityGrid / SinglePhasePressureSolver::GetPressure / _fluidMarkers,
+ * fluid3.hpp:10-26, single_phase_pressure_solver.cpp:50-53).  Any pointer may be NULL. */
+fe_status fe_scene_get_grid(fe_scene* s, float* u, float* v, float* w, double* p, uint8_t* marks);
+fe_status fe_scene_set_grid(fe_scene* s, const float* u, const float* v, const float* w);
+fe_status fe_scene_set_pressure(fe_scene* s, const double* p);
+/* P2G face markers (Fluid3 xMarkers/yMarkers/zMarkers) and the FLIP snapshot (FLIPSimulator::
+ * _velocityResiduals right after P2G, flip_simulator.cpp:107-118). */
+fe_status fe_scene_get_face_markers(fe_scene* s, uint8_t* mu, uint8_t* mv, uint8_t* mw);
+fe_status fe_scene_get_snapshot(fe_scene* s, float* u, float* v, float* w);
+/* Right-hand side b = div u of the last pressure solve (SinglePhasePressureSolver::BuildSystem b). */
+fe_status fe_scene_get_rhs(fe_scene* s, double* b);
+/* Band-limited particle SDF on the cell-centred grid (HybridSimulator::GetFluidSdf, hybrid_simulator.cpp:82-85,
+ * as built by PICSimulator::BuildSignedDistanceField, pic_simulator.cpp:452-475), FP64. */
+fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf);
+/* Sorted cell keys and the permutation of the last sort (slot -> particle id), n entries each. */
+fe_status fe_scene_get_sort(fe_scene* s, uint32_t* keys, uint32_t* perm, uint64_t n);
+/* Post-projection ||div u||_2 over FLUID cells of the current grid (FP64). */
+fe_status fe_scene_divergence(fe_scene* s, double* l2);
+
+/* Stream the scene's work is issued on (a cudaStream_t); NULL selects the scene's own stream. */
+fe_status fe_scene_set_stream(fe_scene* s, void* stream);
+fe_status fe_scene_synchronize(fe_scene* s);
+
+/* Number of kernels the library launched since load (counts graph-launched kernels too). */
+uint64_t fe_kernel_launch_count(void);
+
+/* Deterministic seeding of analytic box / sphere regions (subcell-centre rule).  Region layout:
+ * {int32 kind (0 box, 1 sphere); double lo[3]; double hi[3] (sphere: hi[0] = radius); double vel[3]}.
+ * Returns the particle count; pos/vel (n*3 floats) are written when non-NULL, at most cap particles.
+ * Replaces PICSimulator::InitializeParticles' std::rand() seeding (pic_simulator.cpp:521-548). */
+uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[3], const double origin[3],
+                         const double size[3], uint64_t seed, float* pos, float* vel, uint64_t cap);
+
+/* Message of the last error on the calling thread ("" if none). */
+const char* fe_last_error(void);
+
+/* ABI version: major * 10000 + minor * 100 + patch. */
+int32_t fe_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLUIDE_B200_H */

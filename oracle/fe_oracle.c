@@ -1012,5 +1012,5 @@ void or_sort_keys(const float* pos, size_t n, const int dims[3], const float ori
 size_t or_seed_regions(const void* regions, int nreg, const int n[3], const double origin[3], const double h[3],
                        uint64_t seed, float* pos, float* vel, size_t cap)
 {
-    return fe_seed_regions((const fe_region*)regions, nreg, n, origin, h, seed, pos, vel, cap);
+    return fe_seed_regions_host((const fe_region*)regions, nreg, n, origin, h, seed, pos, vel, cap);
 }
