@@ -169,6 +169,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--ref-steps", type=int, default=1, help="substeps of the CPU reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -191,7 +192,8 @@ def main():
     n = args.n
     pos, vel = fe.seed_regions([dict(kind=0, lo=BOX[:3], hi=BOX[3:])], (n, n, n), (0, 0, 0), (1, 1, 1), 0)
     N = pos.shape[0]
-    scene = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, device=local)
+    scene = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_inner_tol=args.cg_inner_tol,
+                     device=local)
     stream = torch.cuda.Stream()
     scene.set_stream(stream.cuda_stream)
     scene.set_particles(pos, vel)

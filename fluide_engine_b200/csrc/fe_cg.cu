@@ -7,19 +7,22 @@
 // it with unpreconditioned CG warm-started from the previous pressure (linear_system/
 // conjugate_gradient_solver.cpp:14-55, linear_system.cpp:13-18).
 //
-// Here the FLUID-cell system is solved matrix-free from the cell marks (no stored matrix rows):
-//   outer (FP64): r = b - A p, ||r||, convergence test ||r|| <= tol ||b||; p += e after each inner solve
-//   inner (FP32): CG on A e = r, dot products accumulated in FP64, until the inner residual fell by
-//                 cg_inner_tol (or far enough to meet the outer target)
-// Each inner iteration is two passes separated by grid-wide reductions:
-//   A: d' = r + beta d, q = A d' (neighbour d' recomputed from the neighbour r and d, so no extra pass),
-//      partial d'.q
-//   B: x += alpha d', r -= alpha q, partial r.r
+// Here the FLUID-cell system is solved matrix-free from the cell marks:
+//   setup      the FLUID cells are compacted, in cell order, into one list shared evenly by all threads
+//              (block counts -> grid barrier -> block offsets -> ordered block compaction), with a 6-bit
+//              in-domain-neighbour mask per entry; every non-FLUID entry of p and of the FP32 vectors is
+//              0, which makes the stencil branch-free over neighbours
+//   outer FP64 r = b - A p, ||r||, test ||r|| <= tol ||b||; after each inner solve p += e
+//   inner FP32 Chronopoulos-Gear CG on A e = r (dot products accumulated in FP64): per iteration ONE pass
+//              p = r + beta p, s = w + beta s, e += alpha p, r' = r - alpha s, w' = A r' and the two dot
+//              products (r', r') and (w', r'), then ONE grid-wide reduction.  w' = A r' needs the
+//              neighbours' r', which each thread recomputes as r - alpha (w + beta s) from the previous
+//              iteration's neighbour values; r, w and s ping-pong so those stay intact within the pass.
 // The grid-wide barrier is a counter + generation word with a bounded spin: if a block waits longer than
-// ~3 s it records FE_ERR_TIMEOUT, every block leaves its loops and the kernel returns, so a stuck solve
-// surfaces as a status instead of a hung device.  Partial sums are written per block and summed by every
-// block in the same fixed order, so all blocks take identical branch decisions and results are
-// deterministic.  Non-FLUID entries of every vector are held at 0, which makes the stencil branch-free.
+// a few seconds it records FE_ERR_TIMEOUT, every block leaves its loops and the kernel returns, so a stuck
+// solve surfaces as a status instead of a hung device.  Dot products travel with the barrier: the last
+// block to arrive sums the per-block partials in a fixed order and publishes the totals, so all blocks
+// take identical branch decisions and results are deterministic.
 #include "fe_internal.cuh"
 
 #include <cuda/atomic>
@@ -28,7 +31,7 @@ namespace fe {
 namespace {
 
 constexpr int kCgThreads = 1024;
-constexpr unsigned long long kSpinLimit = 1ull << 25;
+constexpr unsigned long long kSpinLimit = 1ull << 26;
 
 struct CgParams {
     double rel_tol, inner_tol;
@@ -38,6 +41,8 @@ struct CgParams {
     unsigned stats_cap;
 };
 
+// Grid-wide barrier (no reduction).  Thread 0 arrives with an acq_rel increment; the last arriver resets
+// the counter and bumps the generation word the others spin on (bounded).
 __device__ __forceinline__ bool grid_sync(unsigned* bar, int* err, unsigned nblocks)
 {
     __syncthreads();
@@ -53,12 +58,11 @@ __device__ __forceinline__ bool grid_sync(unsigned* bar, int* err, unsigned nblo
         } else {
             unsigned long long spins = 0;
             while (gen.load(cuda::memory_order_acquire) == g) {
-                if (e.load(cuda::memory_order_relaxed) != 0) break;
                 if (++spins > kSpinLimit) {
                     e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
                     break;
                 }
-                if (spins > 32) __nanosleep(64);
+                if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) break;
             }
         }
         __threadfence();
@@ -67,10 +71,16 @@ __device__ __forceinline__ bool grid_sync(unsigned* bar, int* err, unsigned nblo
     return *(volatile int*)err == 0;
 }
 
-// Block-wide sum of up to 4 doubles; result valid in all threads.
+// Grid-wide sum of N doubles fused with the barrier.  Each block reduces to warp 0, lane 0 publishes the
+// block partial and arrives; the last block to arrive sums all partials with its warp 0 in a fixed order
+// (so every run and every block sees the same bits), publishes the totals and releases the generation;
+// the other blocks' warp 0 waits (bounded) and reads the totals.  Two __syncthreads per call.
 template <int N>
-__device__ __forceinline__ void block_sum(double (&v)[N], double* sh /* [32 * N] */)
+__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w)
 {
+    static_assert(N <= 4, "at most 4 sums per reduction");
+    // warp partials use sh[0, 32 N), the totals sh[128, 128 + N): disjoint, so a warp that races ahead into
+    // the next reduction cannot overwrite totals another warp has not read yet
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < N; ++k)
@@ -82,166 +92,301 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* sh /* [32 * N]
     __syncthreads();
     if (wid == 0) {
         const int nw = blockDim.x >> 5;
+        double part[N];
 #pragma unroll
         for (int k = 0; k < N; ++k) {
             double s = lane < nw ? sh[lane * N + k] : 0.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            v[k] = s;
+            part[k] = s;
         }
-        if (lane == 0)
+        unsigned last = 0, g = 0;
+        if (lane == 0) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) sh[32 * N + k] = v[k];
+            for (int k = 0; k < N; ++k) w.partial[blockIdx.x * 4 + k] = part[k];
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(w.bar[0]);
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(w.bar[1]);
+            g = gen.load(cuda::memory_order_acquire);
+            __threadfence();
+            last = count.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1 ? 1u : 0u;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        double* totals = (double*)(w.partial + 4 * gridDim.x);
+        if (last) {
+            __threadfence();
+            double t[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) t[k] = 0.0;
+            for (int b = lane; b < (int)gridDim.x; b += 32)
+#pragma unroll
+                for (int k = 0; k < N; ++k) t[k] += __ldcg(w.partial + b * 4 + k);
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+            if (lane == 0) {
+#pragma unroll
+                for (int k = 0; k < N; ++k) __stcg(totals + k, t[k]);
+                __threadfence();
+                cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(w.bar[0]);
+                cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(w.bar[1]);
+                count.store(0u, cuda::memory_order_relaxed);
+                gen.store(g + 1u, cuda::memory_order_release);
+#pragma unroll
+                for (int k = 0; k < N; ++k) sh[128 + k] = t[k];
+            }
+        } else {
+            if (lane == 0) {
+                cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(w.bar[1]);
+                cuda::atomic_ref<int, cuda::thread_scope_device> e(*w.err);
+                unsigned long long spins = 0;
+                while (gen.load(cuda::memory_order_acquire) == g) {
+                    if (++spins > kSpinLimit) {
+                        e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
+                        break;
+                    }
+                    if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) break;
+                }
+                __threadfence();
+#pragma unroll
+                for (int k = 0; k < N; ++k) sh[128 + k] = __ldcg(totals + k);
+            }
+        }
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < N; ++k) v[k] = sh[32 * N + k];
-    __syncthreads();
+    for (int k = 0; k < N; ++k) v[k] = sh[128 + k];
+    return *(volatile int*)w.err == 0;
 }
 
-// Publishes this block's N partials, synchronises the grid and returns the grid-wide sums (identical in
-// every block).  Returns false when the barrier gave up.
-template <int N>
-__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh, const CgWork& w)
+// Block-wide sum of one double, valid in all threads (setup only).
+__device__ __forceinline__ double block_sum1(double x, double* sh)
 {
-    block_sum<N>(v, sh);
-    if (threadIdx.x == 0)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-        for (int k = 0; k < N; ++k) w.partial[blockIdx.x * 4 + k] = v[k];
-    if (!grid_sync(w.bar, w.err, gridDim.x)) return false;
-    double s[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) s[k] = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-#pragma unroll
-        for (int k = 0; k < N; ++k) s[k] += __ldcg(w.partial + b * 4 + k);
-    block_sum<N>(s, sh);
-#pragma unroll
-    for (int k = 0; k < N; ++k) v[k] = s[k];
-    return true;
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sh[k];
+    __syncthreads();
+    return s;
+}
+
+enum : uint32_t { kXm = 1, kXp = 2, kYm = 4, kYp = 8, kZm = 16, kZp = 32 };
+
+struct Stencil7 {
+    int sx;
+    int sxy;
+    float ih2[3];
+};
+
+// (A v)_c for the FLUID row c with in-domain mask m, non-FLUID entries of v being 0.
+template <class F>
+__device__ __forceinline__ float apply_row(const Stencil7& st, int c, uint32_t m, F val)
+{
+    const float vc = val(c);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (m & kXm) ax += vc - val(c - 1);
+    if (m & kXp) ax += vc - val(c + 1);
+    if (m & kYm) ay += vc - val(c - st.sx);
+    if (m & kYp) ay += vc - val(c + st.sx);
+    if (m & kZm) az += vc - val(c - st.sxy);
+    if (m & kZp) az += vc - val(c + st.sxy);
+    return st.ih2[0] * ax + st.ih2[1] * ay + st.ih2[2] * az;
 }
 
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgParams prm)
 {
     __shared__ double sh[32 * 4 + 4];
+    __shared__ uint32_t s_warp[32];
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
-    const size_t sxy = (size_t)nx * ny;
-    const size_t nc = sxy * nz;
-    const size_t T = (size_t)gridDim.x * blockDim.x;
-    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const int sxy = nx * ny;
+    const int nc = sxy * nz;
+    const int T = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint8_t* __restrict__ marks = v.marks;
     const double ih2d[3] = {v.inv_h[0] * v.inv_h[0], v.inv_h[1] * v.inv_h[1], v.inv_h[2] * v.inv_h[2]};
-    const float ih2[3] = {(float)ih2d[0], (float)ih2d[1], (float)ih2d[2]};
-    float* __restrict__ r = w.r;
-    float* __restrict__ q = w.q;
-    float* __restrict__ x = w.x;
-    double* __restrict__ p = v.p;
+    Stencil7 st;
+    st.sx = nx;
+    st.sxy = sxy;
+    st.ih2[0] = (float)ih2d[0];
+    st.ih2[1] = (float)ih2d[1];
+    st.ih2[2] = (float)ih2d[2];
+    double* __restrict__ p64 = v.p;
     const double* __restrict__ b = v.b;
+    float* __restrict__ R[2] = {w.r0, w.r1};
+    float* __restrict__ W[2] = {w.w0, w.w1};
+    float* __restrict__ S[2] = {w.s0, w.s1};
+    float* __restrict__ P = w.pv;
+    float* __restrict__ X = w.x;
+    uint32_t* __restrict__ list = w.list;
 
-    // Pass 0: ||b||^2 and FLUID count; non-FLUID entries of p and of every FP32 vector set to 0.
+    // ---- setup: zero non-FLUID entries, ||b||^2, per-block FLUID counts over the block's cell range
+    const int chunk = (nc + gridDim.x - 1) / gridDim.x;
+    const int cb = min(nc, (int)blockIdx.x * chunk), ce = min(nc, cb + chunk);
     double acc[2] = {0.0, 0.0};
-    for (size_t c = tid; c < nc; c += T) {
+    for (int c = cb + threadIdx.x; c < ce; c += blockDim.x) {
         if (marks[c] == FE_CELL_FLUID) {
             acc[0] += b[c] * b[c];
             acc[1] += 1.0;
         } else {
-            p[c] = 0.0;
-            r[c] = 0.f;
-            w.d0[c] = 0.f;
-            w.d1[c] = 0.f;
-            q[c] = 0.f;
-            x[c] = 0.f;
+            p64[c] = 0.0;
+            R[0][c] = 0.f;
+            R[1][c] = 0.f;
+            W[0][c] = 0.f;
+            W[1][c] = 0.f;
+            S[0][c] = 0.f;
+            S[1][c] = 0.f;
         }
     }
-    if (!grid_reduce<2>(acc, sh, w)) return;
-    const double bnorm = sqrt(acc[0]);
-    const int fluid = (int)acc[1];
+    // block offset = FLUID count of all earlier blocks (fixed order), total = all blocks
+    const double mine = block_sum1(acc[1], sh);
+    if (threadIdx.x == 0) w.partial[blockIdx.x * 4 + 2] = mine;
+    double tot[2] = {acc[0], acc[1]};
+    if (!grid_reduce<2>(tot, sh, w)) return;
+    const double bnorm = sqrt(tot[0]);
+    const int F = (int)tot[1];
+    double before = 0.0;
+    for (int bb = threadIdx.x; bb < (int)blockIdx.x; bb += blockDim.x) before += __ldcg(w.partial + bb * 4 + 2);
+    before = block_sum1(before, sh);
+    // ordered compaction of this block's FLUID cells with their in-domain masks
+    uint32_t base = (uint32_t)before;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int c0 = cb; c0 < ce; c0 += blockDim.x) {
+        const int c = c0 + threadIdx.x;
+        const bool fl = c < ce && marks[c] == FE_CELL_FLUID;
+        const unsigned bal = __ballot_sync(0xffffffffu, fl);
+        if (lane == 0) s_warp[wid] = __popc(bal);
+        __syncthreads();
+        uint32_t off = 0, total = 0;
+        for (int k = 0; k < nwarp; ++k) {
+            const uint32_t x = s_warp[k];
+            off += k < wid ? x : 0u;
+            total += x;
+        }
+        if (fl) {
+            const int i = c % nx, j = (c / nx) % ny, k = c / sxy;
+            uint32_t m = (i > 0 ? kXm : 0u) | (i + 1 < nx ? kXp : 0u) | (j > 0 ? kYm : 0u) | (j + 1 < ny ? kYp : 0u) |
+                         (k > 0 ? kZm : 0u) | (k + 1 < nz ? kZp : 0u);
+            const uint32_t slot = base + off + __popc(bal & ((1u << lane) - 1u));
+            list[slot] = ((uint32_t)c << 6) | m;
+        }
+        base += total;
+        __syncthreads();
+    }
+    if (!grid_sync(w.bar, w.err, gridDim.x)) return;
     const double target = prm.rel_tol * bnorm;
+    if (bnorm == 0.0) {
+        for (int e = tid; e < F; e += T) p64[list[e] >> 6] = 0.0;
+    }
 
     int total_it = 0, refinements = 0;
     double rnorm = 0.0;
-    bool converged = false;
-    for (;;) {
-        // Outer residual r = b - A p in FP64 (stored in FP32 for the inner solve).
-        double racc[2] = {0.0, 0.0};
-        for (size_t c = tid; c < nc; c += T) {
-            if (marks[c] != FE_CELL_FLUID) continue;
-            const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / sxy);
-            const double pc = p[c];
-            double ap = 0.0;
-            if (i > 0) ap += ih2d[0] * (pc - p[c - 1]);
-            if (i + 1 < nx) ap += ih2d[0] * (pc - p[c + 1]);
-            if (j > 0) ap += ih2d[1] * (pc - p[c - nx]);
-            if (j + 1 < ny) ap += ih2d[1] * (pc - p[c + nx]);
-            if (k > 0) ap += ih2d[2] * (pc - p[c - sxy]);
-            if (k + 1 < nz) ap += ih2d[2] * (pc - p[c + sxy]);
-            const double rr = b[c] - ap;
-            const float rf = (float)rr;
-            r[c] = rf;
-            x[c] = 0.f;
-            w.d0[c] = 0.f;
+    bool converged = bnorm == 0.0;
+    int cur = 0;  // ping-pong index of r, w, s
+    while (!converged) {
+        // ---- outer residual r = b - A p in FP64, stored in FP32 for the inner solve
+        double racc[1] = {0.0};
+        for (int e = tid; e < F; e += T) {
+            const uint32_t ent = list[e];
+            const int c = (int)(ent >> 6);
+            const uint32_t m = ent & 63u;
+            const double pc = p64[c];
+            double ax = 0.0, ay = 0.0, az = 0.0;
+            if (m & kXm) ax += pc - p64[c - 1];
+            if (m & kXp) ax += pc - p64[c + 1];
+            if (m & kYm) ay += pc - p64[c - nx];
+            if (m & kYp) ay += pc - p64[c + nx];
+            if (m & kZm) az += pc - p64[c - sxy];
+            if (m & kZp) az += pc - p64[c + sxy];
+            const double rr = b[c] - (ih2d[0] * ax + ih2d[1] * ay + ih2d[2] * az);
+            R[0][c] = (float)rr;
             racc[0] += rr * rr;
-            racc[1] += (double)rf * (double)rf;
         }
-        if (!grid_reduce<2>(racc, sh, w)) return;
+        cur = 0;
+        if (!grid_reduce<1>(racc, sh, w)) return;
         rnorm = sqrt(racc[0]);
-        if (rnorm <= target || bnorm == 0.0) {
+        if (rnorm <= target) {
             converged = true;
             break;
         }
         if (refinements >= prm.max_refine || total_it >= prm.max_it) break;
         ++refinements;
 
-        // Inner FP32 CG on A e = r.
-        double rho = racc[1];
-        const double rho0 = rho;
-        double want = fmax(prm.inner_tol, 0.25 * target / rnorm);
-        const double stop = want * want * rho0;
-        double beta = 0.0;
-        int parity = 0;
-        while (total_it < prm.max_it) {
-            const float bf = (float)beta;
-            float* __restrict__ dold = parity ? w.d1 : w.d0;
-            float* __restrict__ dnew = parity ? w.d0 : w.d1;
-            double a1[1] = {0.0};
-            for (size_t c = tid; c < nc; c += T) {
-                if (marks[c] != FE_CELL_FLUID) continue;
-                const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / sxy);
-                const float dn = r[c] + bf * dold[c];
-                float ax = 0.f, ay = 0.f, az = 0.f;
-                if (i > 0) ax += dn - (r[c - 1] + bf * dold[c - 1]);
-                if (i + 1 < nx) ax += dn - (r[c + 1] + bf * dold[c + 1]);
-                if (j > 0) ay += dn - (r[c - nx] + bf * dold[c - nx]);
-                if (j + 1 < ny) ay += dn - (r[c + nx] + bf * dold[c + nx]);
-                if (k > 0) az += dn - (r[c - sxy] + bf * dold[c - sxy]);
-                if (k + 1 < nz) az += dn - (r[c + sxy] + bf * dold[c + sxy]);
-                const float qq = ih2[0] * ax + ih2[1] * ay + ih2[2] * az;
-                dnew[c] = dn;
-                q[c] = qq;
-                a1[0] += (double)dn * (double)qq;
-            }
-            if (!grid_reduce<1>(a1, sh, w)) return;
-            if (!(a1[0] > 0.0)) break;  // breakdown (A d = 0): nothing left to reduce in FP32
-            const double alpha = rho / a1[0];
-            const float af = (float)alpha;
-            double a2[1] = {0.0};
-            for (size_t c = tid; c < nc; c += T) {
-                if (marks[c] != FE_CELL_FLUID) continue;
-                x[c] += af * dnew[c];
-                const float rn = r[c] - af * q[c];
-                r[c] = rn;
-                a2[0] += (double)rn * (double)rn;
-            }
-            if (!grid_reduce<1>(a2, sh, w)) return;
-            ++total_it;
-            beta = a2[0] / rho;
-            rho = a2[0];
-            parity ^= 1;
-            if (rho <= stop) break;
+        // ---- inner Chronopoulos-Gear CG on A e = r; w0 = A r0 and the first dot products
+        double d0[2] = {0.0, 0.0};
+        for (int e = tid; e < F; e += T) {
+            const uint32_t ent = list[e];
+            const int c = (int)(ent >> 6);
+            const float* __restrict__ r0 = R[0];
+            const float wc = apply_row(st, c, ent & 63u, [&](int q) { return r0[q]; });
+            const float rc = r0[c];
+            W[0][c] = wc;
+            X[c] = 0.f;
+            P[c] = 0.f;
+            S[0][c] = 0.f;
+            d0[0] += (double)rc * (double)rc;
+            d0[1] += (double)wc * (double)rc;
         }
-        // p += e (FP64); the next residual pass reads neighbours' p, hence the barrier.
-        for (size_t c = tid; c < nc; c += T)
-            if (marks[c] == FE_CELL_FLUID) p[c] += (double)x[c];
+        if (!grid_reduce<2>(d0, sh, w)) return;
+        double gamma = d0[0], delta = d0[1];
+        const double gamma0 = gamma;
+        const double want = fmax(prm.inner_tol, 0.25 * target / rnorm);
+        const double stop = want * want * gamma0;
+        double alpha_prev = 1.0, gamma_prev = 1.0;
+        bool first = true;
+        while (total_it < prm.max_it) {
+            double beta = 0.0, alpha;
+            if (first) {
+                alpha = gamma / delta;
+            } else {
+                beta = gamma / gamma_prev;
+                alpha = gamma / (delta - beta * gamma / alpha_prev);
+            }
+            if (!(alpha > 0.0) || !isfinite(alpha)) break;  // FP32 breakdown: leave it to the outer loop
+            first = false;
+            const float af = (float)alpha, bf = (float)beta;
+            const float* __restrict__ r = R[cur];
+            const float* __restrict__ wv = W[cur];
+            const float* __restrict__ s = S[cur];
+            float* __restrict__ rn = R[cur ^ 1];
+            float* __restrict__ wn = W[cur ^ 1];
+            float* __restrict__ sn = S[cur ^ 1];
+            double dd[2] = {0.0, 0.0};
+            for (int e = tid; e < F; e += T) {
+                const uint32_t ent = list[e];
+                const int c = (int)(ent >> 6);
+                // r'(q) = r(q) - alpha (w(q) + beta s(q)) for this cell and its neighbours
+                auto rnew = [&](int q) { return r[q] - af * (wv[q] + bf * s[q]); };
+                const float snew = wv[c] + bf * s[c];
+                const float pnew = r[c] + bf * P[c];
+                const float rc = r[c] - af * snew;
+                const float wc = apply_row(st, c, ent & 63u, rnew);
+                P[c] = pnew;
+                X[c] += af * pnew;
+                sn[c] = snew;
+                rn[c] = rc;
+                wn[c] = wc;
+                dd[0] += (double)rc * (double)rc;
+                dd[1] += (double)wc * (double)rc;
+            }
+            if (!grid_reduce<2>(dd, sh, w)) return;
+            ++total_it;
+            cur ^= 1;
+            gamma_prev = gamma;
+            alpha_prev = alpha;
+            gamma = dd[0];
+            delta = dd[1];
+            if (gamma <= stop) break;
+        }
+        // ---- p += e (FP64); the next residual pass reads neighbours' p, hence the barrier
+        for (int e = tid; e < F; e += T) {
+            const int c = (int)(list[e] >> 6);
+            p64[c] += (double)X[c];
+        }
         if (!grid_sync(w.bar, w.err, gridDim.x)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && prm.stats_ring) {
@@ -250,7 +395,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
         s.cg_iterations = total_it;
         s.refinements = refinements;
         s.converged = converged ? 1 : 0;
-        s.fluid_cells = fluid;
+        s.fluid_cells = F;
         s.rel_residual = bnorm > 0.0 ? rnorm / bnorm : rnorm;
         s.b_norm = bnorm;
         prm.stats_ring[slot] = s;

@@ -41,8 +41,9 @@ __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid
     else if (t < nu + nv) { c = 1; f = t - nu; sx = nx; sy = ny + 1; sz = nz; }
     else { c = 2; f = t - nu - nv; sx = nx; sy = ny; sz = nz + 1; }
     const int i = (int)(f % sx), j = (int)((f / sx) % sy), k = (int)(f / ((size_t)sx * sy));
-    const float* in = fa.in[c];
-    const uint8_t* vin = fa.vin[c];
+    // select by value (a runtime index into the parameter arrays would spill them to local memory)
+    const float* in = c == 0 ? fa.in[0] : (c == 1 ? fa.in[1] : fa.in[2]);
+    const uint8_t* vin = c == 0 ? fa.vin[0] : (c == 1 ? fa.vin[1] : fa.vin[2]);
     float val = in[f];
     uint8_t valid = vin[f];
     if (!valid) {
@@ -60,14 +61,14 @@ __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid
             valid = 1;
         }
     }
-    if (write_valid) fa.vout[c][f] = valid;
+    if (write_valid) (c == 0 ? fa.vout[0] : (c == 1 ? fa.vout[1] : fa.vout[2]))[f] = valid;
     if (MODE != kModePlain) {
         const bool wall = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1)) ||
                           (c == 2 && (k == 0 || k == sz - 1));
         if (wall) val = 0.f;
         else if (MODE == kModePre) val += (c == 0 ? gx : (c == 1 ? gy : gz));
     }
-    fa.out[c][f] = val;
+    (c == 0 ? fa.out[0] : (c == 1 ? fa.out[1] : fa.out[2]))[f] = val;
 }
 
 __global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,

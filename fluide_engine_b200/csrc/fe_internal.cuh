@@ -7,7 +7,7 @@
 //              ping-pong copies for extrapolation, FP32 FLIP snapshot, u8 face markers, FP32 P2G
 //              accumulators (numerator, weight).
 //   cells      u8 marks (AIR 0 / FLUID 1), FP64 pressure (warm start kept between substeps),
-//              FP64 right-hand side, FP32 CG vectors r, d (two), q, x.
+//              FP64 right-hand side, FP32 CG vectors (r, w, s twice; p, x) and the compacted FLUID list.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -162,7 +162,8 @@ cudaError_t launch_scatter_out(const SceneView& v, float* pos, float* vel, float
 
 // CG solver (fe_cg.cu).
 struct CgWork {
-    float *r, *d0, *d1, *q, *x;
+    float *r0, *r1, *w0, *w1, *s0, *s1, *pv, *x;  // FP32 inner-CG vectors (r, w, s ping-pong)
+    uint32_t* list;         // compacted FLUID cells: (cell << 6) | in-domain neighbour mask
     double* partial;        // [blocks][4]
     unsigned* bar;          // [0] count, [1] generation
     int* err;

@@ -35,33 +35,48 @@ __device__ __forceinline__ int bucket_of(double x, double spacing)
     return (int)floor(__ddiv_rn(x, spacing));
 }
 
+// floor(x / spacing) exactly as the reference computes it; the multiply by the reciprocal decides it
+// unless the quotient is within 1e-9 of an integer, where the correctly rounded division is used.
+__device__ __forceinline__ int bucket_fast(double x, double spacing, double inv_spacing)
+{
+    const double q = x * inv_spacing;
+    const double fq = floor(q);
+    const double fr = q - fq;
+    if (fr > 1e-9 && fr < 1.0 - 1e-9) return (int)fq;
+    return bucket_of(x, spacing);
+}
+
 __device__ __forceinline__ bool visited(const SceneView& v, int pbx, int pby, int pbz, int i, int j, int k)
 {
     return (pbx == v.q_b0[0][i] || pbx == v.q_b1[0][i]) && (pby == v.q_b0[1][j] || pby == v.q_b1[1][j]) &&
            (pbz == v.q_b0[2][k] || pbz == v.q_b1[2][k]);
 }
 
-__global__ void k_mark(SceneView v, double R2, double crit_eps)
+// One thread per particle: the nodes within r of it (2 per axis for cubic cells, where 2r = 1.7 h;
+// more along an axis whose spacing is finer than max(h)) get the reference's exact FP64 test.
+__global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double crit_eps)
 {
     uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (p >= v.np) return;
     const double X[3] = {(double)v.px[p], (double)v.py[p], (double)v.pz[p]};
     const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
+    const double inv_bucket = 1.0 / v.bucket;
     int lo[3], hi[3], pb[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        // nodes within r along this axis, widened by one node on each side (the exact test filters)
-        double t = (X[a] - v.sdf_origin[a]) * v.inv_h[a];
-        double rr = v.radius * v.inv_h[a];
-        int l = (int)floor(t - rr) - 1, h = (int)floor(t + rr) + 1;
-        lo[a] = max(l, 0);
-        hi[a] = min(h, n[a] - 1);
-        pb[a] = bucket_of(X[a], v.bucket);
+        // nodes i with |q_i - x| < r, widened by 1e-6 h (the exact test below decides)
+        const double t = (X[a] - v.sdf_origin[a]) * v.inv_h[a];
+        const double rr = v.radius * v.inv_h[a] + 1e-6;
+        lo[a] = max((int)floor(t - rr) + 1, 0);
+        hi[a] = min((int)floor(t + rr), n[a] - 1);
+        pb[a] = bucket_fast(X[a], v.bucket, inv_bucket);
     }
-    for (int k = lo[2]; k <= hi[2]; ++k)
-        for (int j = lo[1]; j <= hi[1]; ++j)
+    for (int k = lo[2]; k <= hi[2]; ++k) {
+        if (pb[2] != v.q_b0[2][k] && pb[2] != v.q_b1[2][k]) continue;
+        for (int j = lo[1]; j <= hi[1]; ++j) {
+            if (pb[1] != v.q_b0[1][j] && pb[1] != v.q_b1[1][j]) continue;
             for (int i = lo[0]; i <= hi[0]; ++i) {
-                if (!visited(v, pb[0], pb[1], pb[2], i, j, k)) continue;
+                if (pb[0] != v.q_b0[0][i] && pb[0] != v.q_b1[0][i]) continue;
                 const double d2 = dist2_ref(X[0], X[1], X[2], v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]);
                 if (!(d2 <= R2)) continue;
                 const double dist = __dsqrt_rn(d2);
@@ -77,6 +92,8 @@ __global__ void k_mark(SceneView v, double R2, double crit_eps)
                     }
                 }
             }
+        }
+    }
 }
 
 // Band-limited SDF value of node (i, j, k) exactly as BuildSignedDistanceField computes it.
@@ -89,8 +106,10 @@ __device__ double node_sdf(const SceneView& v, int i, int j, int k, double R2)
     int lo[3], hi[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        lo[a] = max(c0[a] - 2, 0);
-        hi[a] = min(c0[a] + 2, n[a] - 1);
+        // particles within the band 2r of the node lie in cells within ceil(2r/h + 0.5) of it
+        const int reach = (int)ceil(v.band * v.inv_h[a] + 0.5) + 1;
+        lo[a] = max(c0[a] - reach, 0);
+        hi[a] = min(c0[a] + reach, n[a] - 1);
     }
     for (int cz = lo[2]; cz <= hi[2]; ++cz)
         for (int cy = lo[1]; cy <= hi[1]; ++cy)

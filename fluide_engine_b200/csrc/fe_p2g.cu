@@ -61,7 +61,13 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(SceneView v)
     const float hi[3] = {v.originf[0] + v.sizef[0] - 0.5f * v.hf[0], v.originf[1] + v.sizef[1] - 0.5f * v.hf[1],
                          v.originf[2] + v.sizef[2] - 0.5f * v.hf[2]};
 
-    for (uint32_t p = beg + threadIdx.x; p < end; p += blockDim.x) {
+    // Thread -> particle map that keeps a warp's lanes on different cells: with about 8 particles per
+    // cell, consecutive particles share their 24 face targets, so lane l of warp w takes particle
+    // base + 8 l + w of each 256-particle window and shared-memory atomics rarely collide.
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (uint32_t base = beg; base < end; base += blockDim.x) {
+        const uint32_t p = base + (uint32_t)(lane * nwarps + warp);
+        if (p >= end) continue;
         const float x = v.px[p], y = v.py[p], z = v.pz[p];
         const float vel[3] = {v.vx[p], v.vy[p], v.vz[p]};
 #pragma unroll
@@ -107,16 +113,18 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(SceneView v)
     }
     __syncthreads();
 
-    for (int t = threadIdx.x; t < 3 * kBoxFaces; t += blockDim.x) {
-        const int c = t / kBoxFaces, l = t - c * kBoxFaces;
-        if (!s_mk[c][l]) continue;
-        const int li = l % kBox, lj = (l / kBox) % kBox, lk = l / (kBox * kBox);
-        const int gi = bx + li, gj = by + lj, gk = bz + lk;
-        if (gi < 0 || gj < 0 || gk < 0 || gi >= fsx[c] || gj >= fsy[c] || gk >= fsz[c]) continue;
-        const size_t f = idx3(gi, gj, gk, fsx[c], fsy[c]);
-        atomicAdd(gnum[c] + f, s_num[c][l]);
-        atomicAdd(gden[c] + f, s_den[c][l]);
-        gmk[c][f] = 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        for (int l = threadIdx.x; l < kBoxFaces; l += blockDim.x) {
+            if (!s_mk[c][l]) continue;
+            const int li = l % kBox, lj = (l / kBox) % kBox, lk = l / (kBox * kBox);
+            const int gi = bx + li, gj = by + lj, gk = bz + lk;
+            if (gi < 0 || gj < 0 || gk < 0 || gi >= fsx[c] || gj >= fsy[c] || gk >= fsz[c]) continue;
+            const size_t f = idx3(gi, gj, gk, fsx[c], fsy[c]);
+            atomicAdd(gnum[c] + f, s_num[c][l]);
+            atomicAdd(gden[c] + f, s_den[c][l]);
+            gmk[c][f] = 1;
+        }
     }
 }
 

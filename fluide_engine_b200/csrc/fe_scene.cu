@@ -216,13 +216,14 @@ fe_status alloc_grid(fe_scene* s)
     s->scan_tmp = tmp;
     // CG vectors
     CgWork& w = s->cg;
-    FE_CUDA(dalloc(L, &w.r, nc));
-    FE_CUDA(dalloc(L, &w.d0, nc));
-    FE_CUDA(dalloc(L, &w.d1, nc));
-    FE_CUDA(dalloc(L, &w.q, nc));
-    FE_CUDA(dalloc(L, &w.x, nc));
+    float* vec;
+    FE_CUDA(dalloc(L, &vec, nc * 8));
+    FE_CUDA(cudaMemset(vec, 0, nc * 8 * sizeof(float)));
+    w.r0 = vec; w.r1 = vec + nc; w.w0 = vec + 2 * nc; w.w1 = vec + 3 * nc;
+    w.s0 = vec + 4 * nc; w.s1 = vec + 5 * nc; w.pv = vec + 6 * nc; w.x = vec + 7 * nc;
+    FE_CUDA(dalloc(L, &w.list, nc));
     FE_CUDA(cg_prepare(w, s->device));
-    FE_CUDA(dalloc(L, &w.partial, (size_t)w.blocks * 4));
+    FE_CUDA(dalloc(L, &w.partial, (size_t)w.blocks * 4 + 4));  // per-block partials + totals
     FE_CUDA(dalloc(L, &w.bar, 8));
     FE_CUDA(cudaMemset(w.bar, 0, 8 * sizeof(unsigned)));
     FE_CUDA(dalloc(L, &w.err, 1));
@@ -514,7 +515,7 @@ fe_status fe_scene_desc_default(fe_scene_desc* d)
     d->max_cfl = 3.0;
     d->cg_rel_tol = 1e-6;
     d->cg_max_it = 2000;
-    d->cg_inner_tol = 1e-3;
+    d->cg_inner_tol = 1e-4;
     d->max_refine = kMaxRefineDefault;
     d->device = 0;
     return FE_OK;
@@ -530,6 +531,8 @@ fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
     }
     if ((uint64_t)fe_key_space(desc->n[0], desc->n[1], desc->n[2]) >= (1ull << 32) - 2)
         return set_error(FE_ERR_BAD_ARG, "grid too large for 32-bit cell keys");
+    if ((uint64_t)desc->n[0] * desc->n[1] * desc->n[2] >= (1ull << 26))
+        return set_error(FE_ERR_BAD_ARG, "at most 2^26 cells per scene (the solver packs cell indices in 26 bits)");
     if (desc->solver < FE_SOLVER_PIC || desc->solver > FE_SOLVER_APIC) return set_error(FE_ERR_BAD_ARG, "bad solver");
     if (!(desc->max_cfl > 0.0) || desc->max_cfl > 64.0) return set_error(FE_ERR_BAD_ARG, "max_cfl must be in (0, 64]");
     if (!(desc->cg_rel_tol > 0.0) || desc->cg_max_it < 1) return set_error(FE_ERR_BAD_ARG, "bad CG settings");
@@ -542,7 +545,7 @@ fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
     fe_scene* s = new (std::nothrow) fe_scene();
     if (!s) return set_error(FE_ERR_OOM, "host allocation failed");
     s->desc = *desc;
-    if (s->desc.cg_inner_tol <= 0.0 || s->desc.cg_inner_tol >= 1.0) s->desc.cg_inner_tol = 1e-3;
+    if (s->desc.cg_inner_tol <= 0.0 || s->desc.cg_inner_tol >= 1.0) s->desc.cg_inner_tol = 1e-4;
     if (s->desc.max_refine <= 0) s->desc.max_refine = kMaxRefineDefault;
     s->device = desc->device;
     SceneView& v = s->base;

@@ -111,7 +111,7 @@ class HybridSimulator:
         self._pending = None            # (pos, vel, C) until the scene exists
         self._currentFrame = Frame()
         self._currentTime = 0.0
-        self._cg = dict(cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-3, max_refine=12)
+        self._cg = dict(cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-4, max_refine=12)
         self.last_stats = []
 
     # settings -------------------------------------------------------------------------------------
