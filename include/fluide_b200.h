@@ -144,6 +144,21 @@ fe_status fe_scene_get_sort(fe_scene* s, uint32_t* keys, uint32_t* perm, uint64_
 /* Post-projection ||div u||_2 over FLUID cells of the current grid (FP64). */
 fe_status fe_scene_divergence(fe_scene* s, double* l2);
 
+/* Pressure projection of a caller-owned MAC grid that allocates no device memory.  No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc/cudaFree on this path (a per-frame or
+ * real-time callback where an allocation's implicit device synchronisation would stall, memory owned by
+ * another allocator, or setup that runs while a stream is being captured).  All pointers except n, h and
+ * stats are device pointers: marks (nx*ny*nz, FE_CELL_*), u/v/w (face arrays, updated in place),
+ * p (pressure, warm start in, solution out).  Runs the scene path's pressure stage (rhs, CG in FP64
+ * refinement to rel_tol, apply) on `stream` (NULL = legacy default stream) and synchronises it.
+ * Scratch lives in one static device array of about 11.6 MB per device, so grids are limited to 2^18
+ * cells (e.g. 64^3); larger grids return FE_ERR_BAD_ARG.  The first call on a device resolves the
+ * array's address (cudaGetSymbolAddress) and must come before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race, so issue them on one stream.  stats (host) may be NULL. */
+fe_status fe_project_noalloc(const int32_t n[3], const double h[3], const uint8_t* marks, float* u, float* v,
+                             float* w, double* p, double rel_tol, int32_t max_it, void* stream,
+                             fe_step_stats* stats);
+
 /* Stream the scene's work is issued on (a cudaStream_t); NULL selects the scene's own stream. */
 fe_status fe_scene_set_stream(fe_scene* s, void* stream);
 fe_status fe_scene_synchronize(fe_scene* s);
