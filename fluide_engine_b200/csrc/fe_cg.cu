@@ -20,9 +20,9 @@
 //              iteration's neighbour values; r, w and s ping-pong so those stay intact within the pass.
 // The grid-wide barrier is a counter + generation word with a bounded spin: if a block waits longer than
 // a few seconds it records FE_ERR_TIMEOUT, every block leaves its loops and the kernel returns, so a stuck
-// solve surfaces as a status instead of a hung device.  Dot products travel with the barrier: the last
-// block to arrive sums the per-block partials in a fixed order and publishes the totals, so all blocks
-// take identical branch decisions and results are deterministic.
+// solve surfaces as a status instead of a hung device.  Dot products travel with the barrier: blocks
+// add their partials into a rotating totals slot before arriving and read the totals once after it, so
+// all blocks take identical branch decisions.
 #include "fe_internal.cuh"
 
 #include <cuda/atomic>
@@ -41,42 +41,59 @@ struct CgParams {
     unsigned stats_cap;
 };
 
-// Grid-wide barrier (no reduction).  Thread 0 arrives with an acq_rel increment; the last arriver resets
-// the counter and bumps the generation word the others spin on (bounded).
-__device__ __forceinline__ bool grid_sync(unsigned* bar, int* err, unsigned nblocks)
+// Barrier generations count modulo 65535 (a multiple of 3), so the three rotating totals slots keep their
+// order across the wrap.
+__device__ __forceinline__ unsigned next_gen(unsigned g) { return g + 1u == 65535u ? 0u : g + 1u; }
+
+// Grid-wide barrier.  bar[0] packs the arrival count (low 16 bits) and the generation (high 16 bits), so
+// one acq_rel fetch_add both arrives and learns the generation; the last arriver resets the count and
+// bumps the generation with a release store, the others spin (bounded) with acquire loads.  The
+// release/acquire pair at device scope, with the __syncthreads on either side, orders every thread's
+// memory traffic of the block across the barrier.  Returns false when the wait gave up.
+// The last arriver also zeroes the totals slot of the next generation (see grid_reduce).
+__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals)
+{
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> word(bar[0]);
+    const unsigned old = word.fetch_add(1u, cuda::memory_order_acq_rel);
+    const unsigned gen = old >> 16;
+    if ((old & 0xffffu) == nblocks - 1) {
+        double* next = totals + 4 * (next_gen(gen) % 3u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) next[k] = 0.0;
+        word.store(next_gen(gen) << 16, cuda::memory_order_release);
+        return true;
+    }
+    cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
+    unsigned long long spins = 0;
+    while ((word.load(cuda::memory_order_acquire) >> 16) == gen) {
+        if (++spins > kSpinLimit) {
+            e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
+            return false;
+        }
+        if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
-        cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(bar[1]);
-        cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
-        const unsigned g = gen.load(cuda::memory_order_acquire);
-        __threadfence();
-        if (count.fetch_add(1u, cuda::memory_order_acq_rel) == nblocks - 1) {
-            count.store(0u, cuda::memory_order_relaxed);
-            gen.store(g + 1u, cuda::memory_order_release);
-        } else {
-            unsigned long long spins = 0;
-            while (gen.load(cuda::memory_order_acquire) == g) {
-                if (++spins > kSpinLimit) {
-                    e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
-                    break;
-                }
-                if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) break;
-            }
-        }
-        __threadfence();
+        bar_arrive_wait(w.bar, w.err, gridDim.x, w.partial);
+        gen = next_gen(gen);
     }
     __syncthreads();
-    return *(volatile int*)err == 0;
+    return *(volatile int*)w.err == 0;
 }
 
-// Grid-wide sum of N doubles fused with the barrier.  Each block reduces to warp 0, lane 0 publishes the
-// block partial and arrives; the last block to arrive sums all partials with its warp 0 in a fixed order
-// (so every run and every block sees the same bits), publishes the totals and releases the generation;
-// the other blocks' warp 0 waits (bounded) and reads the totals.  Two __syncthreads per call.
+// Grid-wide sum of N doubles fused with the barrier.  Each block reduces to warp 0, whose lane 0 adds
+// the block partials into the totals slot of this barrier (FP64 red.add, ordered before the arrival by
+// its release) and arrives; after the barrier it reads the totals once.  Three total slots rotate: the
+// last arriver of barrier k zeroes slot k+1 before releasing it, and slot k is read only until the
+// readers arrive at barrier k+1.  All blocks read the same final totals, so their branch decisions
+// agree (the summation order, and hence the last bits, can vary from run to run).
 template <int N>
-__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w)
+__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w, unsigned& gen)
 {
     static_assert(N <= 4, "at most 4 sums per reduction");
     // warp partials use sh[0, 32 N), the totals sh[128, 128 + N): disjoint, so a warp that races ahead into
@@ -100,58 +117,40 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] 
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             part[k] = s;
         }
-        unsigned last = 0, g = 0;
         if (lane == 0) {
+            // slot of this barrier: generation modulo 3; thread 0 tracks the generation itself (it takes
+            // part in every barrier), which saves a load round trip per barrier
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> word(w.bar[0]);
+            double* totals = w.partial;  // [3][4]
+            double* slot = totals + 4 * (gen % 3u);  // zeroed by the release of this generation
 #pragma unroll
-            for (int k = 0; k < N; ++k) w.partial[blockIdx.x * 4 + k] = part[k];
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(w.bar[0]);
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(w.bar[1]);
-            g = gen.load(cuda::memory_order_acquire);
-            __threadfence();
-            last = count.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1 ? 1u : 0u;
-        }
-        last = __shfl_sync(0xffffffffu, last, 0);
-        g = __shfl_sync(0xffffffffu, g, 0);
-        double* totals = (double*)(w.partial + 4 * gridDim.x);
-        if (last) {
-            __threadfence();
-            double t[N];
+            for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
+            const unsigned old = word.fetch_add(1u, cuda::memory_order_acq_rel);
+            bool ok = true;
+            if ((old & 0xffffu) == gridDim.x - 1) {
+                double* next = totals + 4 * (next_gen(old >> 16) % 3u);
 #pragma unroll
-            for (int k = 0; k < N; ++k) t[k] = 0.0;
-            for (int b = lane; b < (int)gridDim.x; b += 32)
-#pragma unroll
-                for (int k = 0; k < N; ++k) t[k] += __ldcg(w.partial + b * 4 + k);
-#pragma unroll
-            for (int k = 0; k < N; ++k)
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
-            if (lane == 0) {
-#pragma unroll
-                for (int k = 0; k < N; ++k) __stcg(totals + k, t[k]);
-                __threadfence();
-                cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(w.bar[0]);
-                cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(w.bar[1]);
-                count.store(0u, cuda::memory_order_relaxed);
-                gen.store(g + 1u, cuda::memory_order_release);
-#pragma unroll
-                for (int k = 0; k < N; ++k) sh[128 + k] = t[k];
-            }
-        } else {
-            if (lane == 0) {
-                cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(w.bar[1]);
+                for (int k = 0; k < 4; ++k) next[k] = 0.0;
+                word.store(next_gen(old >> 16) << 16, cuda::memory_order_release);
+            } else {
                 cuda::atomic_ref<int, cuda::thread_scope_device> e(*w.err);
                 unsigned long long spins = 0;
-                while (gen.load(cuda::memory_order_acquire) == g) {
+                while ((word.load(cuda::memory_order_acquire) >> 16) == (old >> 16)) {
                     if (++spins > kSpinLimit) {
                         e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
+                        ok = false;
                         break;
                     }
-                    if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) break;
+                    if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) {
+                        ok = false;
+                        break;
+                    }
                 }
-                __threadfence();
-#pragma unroll
-                for (int k = 0; k < N; ++k) sh[128 + k] = __ldcg(totals + k);
             }
+            gen = next_gen(gen);
+            if (ok)
+#pragma unroll
+                for (int k = 0; k < N; ++k) sh[128 + k] = __ldcg(slot + k);
         }
     }
     __syncthreads();
@@ -224,6 +223,10 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
     float* __restrict__ X = w.x;
     uint32_t* __restrict__ list = w.list;
 
+    // barrier generation as of this launch (thread 0 keeps it from here on)
+    unsigned gen = 0;
+    if (threadIdx.x == 0) gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[0]).load(cuda::memory_order_relaxed) >> 16;
+
     // ---- setup: zero non-FLUID entries, ||b||^2, per-block FLUID counts over the block's cell range
     const int chunk = (nc + gridDim.x - 1) / gridDim.x;
     const int cb = min(nc, (int)blockIdx.x * chunk), ce = min(nc, cb + chunk);
@@ -244,13 +247,13 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
     }
     // block offset = FLUID count of all earlier blocks (fixed order), total = all blocks
     const double mine = block_sum1(acc[1], sh);
-    if (threadIdx.x == 0) w.partial[blockIdx.x * 4 + 2] = mine;
+    if (threadIdx.x == 0) w.partial[16 + blockIdx.x] = mine;
     double tot[2] = {acc[0], acc[1]};
-    if (!grid_reduce<2>(tot, sh, w)) return;
+    if (!grid_reduce<2>(tot, sh, w, gen)) return;
     const double bnorm = sqrt(tot[0]);
     const int F = (int)tot[1];
     double before = 0.0;
-    for (int bb = threadIdx.x; bb < (int)blockIdx.x; bb += blockDim.x) before += __ldcg(w.partial + bb * 4 + 2);
+    for (int bb = threadIdx.x; bb < (int)blockIdx.x; bb += blockDim.x) before += __ldcg(w.partial + 16 + bb);
     before = block_sum1(before, sh);
     // ordered compaction of this block's FLUID cells with their in-domain masks
     uint32_t base = (uint32_t)before;
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
         base += total;
         __syncthreads();
     }
-    if (!grid_sync(w.bar, w.err, gridDim.x)) return;
+    if (!grid_sync(w, gen)) return;
     const double target = prm.rel_tol * bnorm;
     if (bnorm == 0.0) {
         for (int e = tid; e < F; e += T) p64[list[e] >> 6] = 0.0;
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
             racc[0] += rr * rr;
         }
         cur = 0;
-        if (!grid_reduce<1>(racc, sh, w)) return;
+        if (!grid_reduce<1>(racc, sh, w, gen)) return;
         rnorm = sqrt(racc[0]);
         if (rnorm <= target) {
             converged = true;
@@ -331,7 +334,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
             d0[0] += (double)rc * (double)rc;
             d0[1] += (double)wc * (double)rc;
         }
-        if (!grid_reduce<2>(d0, sh, w)) return;
+        if (!grid_reduce<2>(d0, sh, w, gen)) return;
         double gamma = d0[0], delta = d0[1];
         const double gamma0 = gamma;
         const double want = fmax(prm.inner_tol, 0.25 * target / rnorm);
@@ -373,7 +376,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
                 dd[0] += (double)rc * (double)rc;
                 dd[1] += (double)wc * (double)rc;
             }
-            if (!grid_reduce<2>(dd, sh, w)) return;
+            if (!grid_reduce<2>(dd, sh, w, gen)) return;
             ++total_it;
             cur ^= 1;
             gamma_prev = gamma;
@@ -387,7 +390,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
             const int c = (int)(list[e] >> 6);
             p64[c] += (double)X[c];
         }
-        if (!grid_sync(w.bar, w.err, gridDim.x)) return;
+        if (!grid_sync(w, gen)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && prm.stats_ring) {
         const unsigned slot = atomicAdd(prm.stats_counter, 1u) % prm.stats_cap;

@@ -12,7 +12,7 @@
 // host-side stand-in, not a device address.  The first call on each device (with that device current)
 // resolves the address once and caches it; make that first call before any stream capture begins.
 // All calls on a device share the one array and it keeps the previous call's contents: what must start
-// at zero (barrier words, error flag, statistics counter) is cleared on the caller's stream at the start
+// at zero (barrier words, reduction totals, error flag, statistics counter) is cleared on the caller's stream at the start
 // of every call, and calls whose work overlaps on the GPU (different streams, or host threads issuing
 // concurrently) race on the array -- serialise them on one stream.
 //
@@ -122,8 +122,9 @@ extern "C" fe_status fe_project_noalloc(const int32_t n[3], const double h[3], c
     view.p = p;
     view.b = (double*)(base + kOffB);
 
-    // barrier words, error flag and statistics counter start at zero on every call
+    // barrier words, reduction totals slots, error flag and statistics counter start at zero on every call
     FE_CUDA(cudaMemsetAsync(work.bar, 0, 8 * sizeof(unsigned), s));
+    FE_CUDA(cudaMemsetAsync(work.partial, 0, 12 * sizeof(double), s));
     FE_CUDA(cudaMemsetAsync(work.err, 0, sizeof(int), s));
     FE_CUDA(launch_rhs(view, s));
     FE_CUDA(launch_cg(view, work, rel_tol, 1e-4, max_it, kMaxRefineDefault, s));

@@ -223,7 +223,8 @@ fe_status alloc_grid(fe_scene* s)
     w.s0 = vec + 4 * nc; w.s1 = vec + 5 * nc; w.pv = vec + 6 * nc; w.x = vec + 7 * nc;
     FE_CUDA(dalloc(L, &w.list, nc));
     FE_CUDA(cg_prepare(w, s->device));
-    FE_CUDA(dalloc(L, &w.partial, (size_t)w.blocks * 4 + 4));  // per-block partials + totals
+    FE_CUDA(dalloc(L, &w.partial, (size_t)w.blocks * 4 + 16));  // 3 rotating totals slots + per-block counts
+    FE_CUDA(cudaMemset(w.partial, 0, ((size_t)w.blocks * 4 + 16) * sizeof(double)));
     FE_CUDA(dalloc(L, &w.bar, 8));
     FE_CUDA(cudaMemset(w.bar, 0, 8 * sizeof(unsigned)));
     FE_CUDA(dalloc(L, &w.err, 1));
@@ -413,6 +414,7 @@ fe_status check_device_error(fe_scene* s)
     if (err) {
         cudaMemsetAsync(s->cg.err, 0, sizeof(int), s->stream);
         cudaMemsetAsync(s->cg.bar, 0, 2 * sizeof(unsigned), s->stream);
+        cudaMemsetAsync(s->cg.partial, 0, 12 * sizeof(double), s->stream);  // totals slots restart at zero
         cudaStreamSynchronize(s->stream);
         return set_error((fe_status)err, "pressure solve: grid barrier wait exceeded its limit");
     }
