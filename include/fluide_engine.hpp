@@ -1,0 +1,319 @@
+// fluide_engine.hpp -- the reference's C++ simulator API for the substep path, over the C ABI.
+//
+// Drop-in for the classes a caller of AleksanderSiwek/Fluide_Engine uses to run the PIC / FLIP / APIC
+// substep: PhysicsAnimation (physics_animation.hpp:8-29), HybridSimulator (hybrid_simulator.hpp:10-41),
+// PICSimulator (pic_simulator.hpp:27-43), FLIPSimulator (flip_simulator.hpp:9-16), APICSimulator
+// (apic_simulator.hpp:9-15), Frame (common/frame.hpp), BoundingBox3D (3d/bounding_box_3d.hpp),
+// DirectionalField (forces/directional_field.hpp) and Vector3 (common/vector3.hpp), with the same names
+// and argument meaning.  State lives on the GPU in one fe_scene (include/fluide_b200.h), created on the
+// first step after particles exist.  Entry points of components outside the substep (mesh seeding,
+// colliders, emitters, viscosity, surface extraction) throw std::logic_error saying so; errors of the
+// library throw fluide::Error carrying the fe_status.  Header-only; link with libfluide_b200.so.
+#ifndef FLUIDE_ENGINE_HPP
+#define FLUIDE_ENGINE_HPP
+
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fluide_b200.h"
+
+namespace fluide {
+class Error : public std::runtime_error {
+  public:
+    Error(fe_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+    fe_status status;
+};
+inline void check(fe_status s)
+{
+    if (s != FE_OK) throw Error(s, std::string("fluide_b200: ") + fe_last_error());
+}
+}  // namespace fluide
+
+template <typename T>
+class Vector3 {
+  public:
+    Vector3(T v = T()) : x(v), y(v), z(v) {}
+    Vector3(T x_, T y_, T z_) : x(x_), y(y_), z(z_) {}
+    T x, y, z;
+};
+
+class BoundingBox3D {
+  public:
+    BoundingBox3D(Vector3<double> origin = Vector3<double>(0), Vector3<double> size = Vector3<double>(1))
+        : _origin(origin), _size(size) {}
+    Vector3<double> GetOrigin() const { return _origin; }
+    Vector3<double> GetSize() const { return _size; }
+    void SetOrigin(Vector3<double> o) { _origin = o; }
+    void SetSize(Vector3<double> s) { _size = s; }
+
+  private:
+    Vector3<double> _origin, _size;
+};
+
+class Frame {
+  public:
+    Frame() = default;
+    explicit Frame(double timeIntervalInSeconds) : _timeIntervalInSeconds(timeIntervalInSeconds) {}
+    void Advance() { ++_index; }
+    Frame& operator++() { Advance(); return *this; }
+    Frame operator++(int) { Frame r = *this; Advance(); return r; }
+    unsigned long GetIndex() const { return _index; }
+    double GetTimeIntervalInSeconds() const { return _timeIntervalInSeconds; }
+    double GetTimeInSeconds() const { return _index * _timeIntervalInSeconds; }
+
+  private:
+    unsigned long _index = 0;
+    double _timeIntervalInSeconds = 1 / 60.0f;  // common/frame.hpp:22
+};
+
+class ExternalForce {
+  public:
+    virtual ~ExternalForce() = default;
+    virtual Vector3<double> Sample(const Vector3<double>& position) const = 0;
+};
+
+class DirectionalField : public ExternalForce {
+  public:
+    explicit DirectionalField(Vector3<double> strength = Vector3<double>(0.0, -9.81, 0.0)) : _strength(strength) {}
+    Vector3<double> Sample(const Vector3<double>&) const override { return _strength; }
+    void SetStrength(Vector3<double> s) { _strength = s; }
+
+  private:
+    Vector3<double> _strength;
+};
+
+// Region description for InitializeFromRegions (layout of the C ABI's fe_seed_regions records).
+struct fe_region_desc {
+    int32_t kind;     // 0 box, 1 sphere
+    double lo[3];     // box lower corner / sphere centre
+    double hi[3];     // box upper corner / hi[0] = sphere radius
+    double vel[3];    // initial velocity
+};
+
+class TriangleMesh;
+class Collider;
+class Emitter;
+
+class PhysicsAnimation {
+  public:
+    virtual ~PhysicsAnimation() = default;
+    // physics_animation.cpp:17-21 + OnUpdate :48-61: advance by one frame of the current frame's interval
+    void AdvanceSingleFrame()
+    {
+        Frame f = _currentFrame;
+        ++f;
+        _currentTime = _currentFrame.GetTimeInSeconds();
+        _numberOfTimeSteps = AdvanceTimeStep(f.GetTimeIntervalInSeconds());
+        _currentTime += f.GetTimeIntervalInSeconds();
+        _currentFrame = f;
+    }
+    void SetCurrentFrame(const Frame& frame) { _currentFrame = frame; }
+    Frame GetCurrentFrame() const { return _currentFrame; }
+    double GetCurrentTimeInSeconds() const { return _currentTime; }
+    void SetNumberOfSubTimesteps(unsigned n) { _numberOfSubTimesteps = n; }
+    unsigned GetNumberOfSubTimeSteps() const { return _numberOfTimeSteps; }
+
+  protected:
+    virtual unsigned AdvanceTimeStep(double timeIntervalInSeconds) = 0;
+    Frame _currentFrame;
+    double _currentTime = 0.0;
+    unsigned _numberOfSubTimesteps = 1;
+    unsigned _numberOfTimeSteps = 0;
+};
+
+class HybridSimulator : public PhysicsAnimation {
+  public:
+    HybridSimulator(const Vector3<size_t>& gridSize, const BoundingBox3D& domain, fe_solver_kind kind)
+        : _n(gridSize), _domain(domain), _kind(kind)
+    {
+        fluide::check(fe_scene_desc_default(&_desc));
+        _desc.n[0] = (int32_t)gridSize.x;
+        _desc.n[1] = (int32_t)gridSize.y;
+        _desc.n[2] = (int32_t)gridSize.z;
+        const Vector3<double> o = domain.GetOrigin(), s = domain.GetSize();
+        _desc.origin[0] = o.x; _desc.origin[1] = o.y; _desc.origin[2] = o.z;
+        _desc.size[0] = s.x; _desc.size[1] = s.y; _desc.size[2] = s.z;
+        _desc.solver = kind;
+        _desc.max_cfl = 3.0;  // hybrid_simulator.cpp:21
+        _desc.gravity[0] = _desc.gravity[1] = _desc.gravity[2] = 0.0;
+    }
+    ~HybridSimulator() override
+    {
+        if (_scene) fe_scene_destroy(_scene);
+    }
+    HybridSimulator(const HybridSimulator&) = delete;
+    HybridSimulator& operator=(const HybridSimulator&) = delete;
+
+    double Cfl(double timeIntervalInSeconds)
+    {
+        double c = 0.0;
+        fluide::check(fe_scene_cfl(Scene(), timeIntervalInSeconds, &c));
+        return c;
+    }
+    double MaxCfl() const { return _desc.max_cfl; }
+    double GetViscosity() const { return 0.0; }
+    double GetDensity() const { return _density; }
+    size_t GetParticlesPerBlock() const { return _particlesPerBlok; }
+    Vector3<double> GetOrigin() const { return _domain.GetOrigin(); }
+    Vector3<size_t> GetResolution() const { return _n; }
+    Vector3<double> GetGridSpacing() const
+    {
+        const Vector3<double> s = _domain.GetSize();
+        return Vector3<double>(s.x / _n.x, s.y / _n.y, s.z / _n.z);
+    }
+    size_t GetNumberOfParticles() const
+    {
+        if (!_scene) return _pos.size() / 3;
+        uint64_t n = 0;
+        fluide::check(fe_scene_num_particles(_scene, &n));
+        return (size_t)n;
+    }
+    void SetMaxClf(double maxCfl) { Reconfigure([&] { _desc.max_cfl = maxCfl; }); }
+    void SetViscosity(double viscosity)
+    {
+        if (viscosity != 0.0) throw std::logic_error("viscosity (BackwardEulerDiffusionSolver) is outside the substep path");
+    }
+    void SetDensity(double density) { _density = density; }  // unused by the projection, as in the reference
+    void SetParticlesPerBlock(size_t n) { _particlesPerBlok = n; }
+
+    // Pressure solver settings (the reference swaps LinearSystemSolver objects, pic_simulator.cpp:56-59).
+    void SetPressureSolverTolerance(double relTol, int maxIterations)
+    {
+        Reconfigure([&] { _desc.cg_rel_tol = relTol; _desc.cg_max_it = maxIterations; });
+    }
+
+    // Particle seeding and access (the reference seeds only through InitializeParticles' std::rand).
+    size_t InitializeFromRegions(const std::vector<fe_region_desc>& regions, uint64_t seed = 0);
+    void SetParticles(const std::vector<float>& pos, const std::vector<float>& vel, const std::vector<float>& C = {})
+    {
+        _pos = pos;
+        _vel = vel.empty() ? std::vector<float>(pos.size(), 0.f) : vel;
+        _C = C;
+        if (_scene) Upload();
+    }
+    void GetParticles(std::vector<float>& pos, std::vector<float>& vel, std::vector<float>* C = nullptr)
+    {
+        if (!_scene) {
+            pos = _pos;
+            vel = _vel;
+            if (C) *C = _C;
+            return;
+        }
+        const size_t n = GetNumberOfParticles();
+        pos.resize(3 * n);
+        vel.resize(3 * n);
+        if (C) C->resize(9 * n);
+        fluide::check(fe_scene_get_particles(_scene, pos.data(), vel.data(), C ? C->data() : nullptr, n));
+    }
+
+    // Fixed-dt substeps (the benchmark configurations' mode); stats may be null.
+    void AdvanceFixedSubsteps(double dt, int nsub, fe_step_stats* stats = nullptr)
+    {
+        fluide::check(fe_scene_step(Scene(), dt, nsub, stats));
+    }
+
+    void AddExternalForce(const std::shared_ptr<ExternalForce> newForce)
+    {
+        Reconfigure([&] {
+            const Vector3<double> g = newForce->Sample(Vector3<double>(0));
+            _desc.gravity[0] += g.x;
+            _desc.gravity[1] += g.y;
+            _desc.gravity[2] += g.z;
+        });
+        _forces.push_back(newForce);
+    }
+    void AddCollider(std::shared_ptr<Collider>) { throw std::logic_error("colliders are outside the substep path"); }
+    void AddEmitter(std::shared_ptr<Emitter>) { throw std::logic_error("emitters are outside the substep path"); }
+    void InitializeFromTriangleMesh(const TriangleMesh&)
+    {
+        throw std::logic_error("mesh seeding (Mesh2SDF) is outside the substep path; use InitializeFromRegions");
+    }
+    void GetSurface(TriangleMesh&) { throw std::logic_error("surface extraction is outside the substep path"); }
+
+    fe_scene* Scene()
+    {
+        if (!_scene) {
+            fluide::check(fe_scene_create(&_desc, &_scene));
+            Upload();
+        }
+        return _scene;
+    }
+
+  protected:
+    unsigned AdvanceTimeStep(double timeIntervalInSeconds) override
+    {
+        int32_t n = 0;
+        fluide::check(fe_scene_advance_frame(Scene(), timeIntervalInSeconds, &n));
+        return (unsigned)n;
+    }
+    template <class F>
+    void Reconfigure(F change)
+    {
+        if (_scene) {  // keep the particles: read them back, rebuild with the new settings
+            GetParticles(_pos, _vel, _kind == FE_SOLVER_APIC ? &_C : nullptr);
+            fe_scene_destroy(_scene);
+            _scene = nullptr;
+        }
+        change();
+    }
+    void Upload()
+    {
+        const size_t n = _pos.size() / 3;
+        if (n == 0) return;
+        fluide::check(fe_scene_set_particles(_scene, _pos.data(), _vel.data(), _C.empty() ? nullptr : _C.data(), n));
+    }
+
+    Vector3<size_t> _n;
+    BoundingBox3D _domain;
+    fe_solver_kind _kind;
+    fe_scene_desc _desc{};
+    fe_scene* _scene = nullptr;
+    double _density = 1.0;
+    size_t _particlesPerBlok = 16;  // hybrid_simulator.cpp:22
+    std::vector<float> _pos, _vel, _C;
+    std::vector<std::shared_ptr<ExternalForce>> _forces;
+};
+
+inline size_t HybridSimulator::InitializeFromRegions(const std::vector<fe_region_desc>& regions, uint64_t seed)
+{
+    const int32_t n[3] = {(int32_t)_n.x, (int32_t)_n.y, (int32_t)_n.z};
+    const double o[3] = {_desc.origin[0], _desc.origin[1], _desc.origin[2]};
+    const double s[3] = {_desc.size[0], _desc.size[1], _desc.size[2]};
+    const uint64_t cnt = fe_seed_regions(regions.data(), (int32_t)regions.size(), n, o, s, seed, nullptr, nullptr, 0);
+    std::vector<float> pos(3 * cnt), vel(3 * cnt);
+    fe_seed_regions(regions.data(), (int32_t)regions.size(), n, o, s, seed, pos.data(), vel.data(), cnt);
+    SetParticles(pos, vel);
+    return (size_t)cnt;
+}
+
+class PICSimulator : public HybridSimulator {
+  public:
+    PICSimulator(const Vector3<size_t>& gridSize, const BoundingBox3D& domain)
+        : HybridSimulator(gridSize, domain, FE_SOLVER_PIC) {}
+
+  protected:
+    PICSimulator(const Vector3<size_t>& gridSize, const BoundingBox3D& domain, fe_solver_kind kind)
+        : HybridSimulator(gridSize, domain, kind) {}
+};
+
+class FLIPSimulator : public PICSimulator {
+  public:
+    FLIPSimulator(const Vector3<size_t>& gridSize, const BoundingBox3D& domain)
+        : PICSimulator(gridSize, domain, FE_SOLVER_FLIP) {}
+    // flip_simulator.cpp:15-23: v = Lerp(flip, pic, factor), default 0.05
+    void SetBlendingFactor(double factor) { Reconfigure([&] { _desc.flip_blend = factor; }); }
+    double GetBlendingFactor() const { return _desc.flip_blend; }
+};
+
+class APICSimulator : public PICSimulator {
+  public:
+    APICSimulator(const Vector3<size_t>& gridSize, const BoundingBox3D& domain)
+        : PICSimulator(gridSize, domain, FE_SOLVER_APIC) {}
+};
+
+#endif  // FLUIDE_ENGINE_HPP
