@@ -26,7 +26,8 @@ EXPORTS = [
     "fe_scene_num_particles", "fe_scene_step", "fe_scene_step_profiled", "fe_scene_advance_frame", "fe_scene_cfl", "fe_scene_run_stages",
     "fe_scene_get_grid", "fe_scene_set_grid", "fe_scene_set_pressure", "fe_scene_get_face_markers",
     "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_get_sort", "fe_scene_divergence",
-    "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
+    "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy",
+    "fe_batch_step", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
     "fe_abi_version",
 ]
 
@@ -103,6 +104,9 @@ def lib():
     L.fe_project_noalloc.argtypes = [P, P, P, P, P, P, P, ctypes.c_double, ctypes.c_int32, P,
                                      ctypes.POINTER(StepStats)]
     L.fe_scene_synchronize.argtypes = [P]
+    L.fe_batch_create.argtypes = [ctypes.POINTER(P), ctypes.c_int32, ctypes.POINTER(P)]
+    L.fe_batch_destroy.argtypes = [P]
+    L.fe_batch_step.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats)]
     L.fe_kernel_launch_count.restype = ctypes.c_uint64
     L.fe_seed_regions.restype = ctypes.c_uint64
     L.fe_seed_regions.argtypes = [P, ctypes.c_int32, P, P, P, ctypes.c_uint64, P, P, ctypes.c_uint64]

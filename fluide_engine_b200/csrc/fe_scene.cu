@@ -16,6 +16,7 @@
 #include <new>
 #include <vector>
 
+#include "fe_batch.cuh"
 #include "fe_internal.cuh"
 #include "fe_seed.h"
 
@@ -971,5 +972,259 @@ uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[
 const char* fe_last_error(void) { return g_err; }
 
 int32_t fe_abi_version(void) { return 10000; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------- batches
+//
+// A batch advances many independent scenes together: per substep, every scene's pre-solve phase runs on
+// its own stream, ONE persistent kernel solves all scenes' pressure systems (fe_batch_cg.cu), and every
+// scene's post-solve phase runs on its own stream again.  The whole batch substep is captured as one CUDA
+// graph (fork/join across the scenes' streams) per particle-buffer parity and replayed.
+
+struct fe_batch {
+    std::vector<fe_scene*> scenes;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    BatchWork work{};
+    std::vector<void*> allocs;
+    std::vector<cudaEvent_t> events;   // 2 per scene + 2
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint64_t graph_kernels[2] = {0, 0};
+    double graph_dt = -1.0;
+    int parity = 0;
+    double rel_tol = 1e-6, inner_tol = 1e-4;
+    int max_it = 2000, max_refine = kMaxRefineDefault;
+};
+
+namespace {
+
+void batch_drop_graphs(fe_batch* b)
+{
+    for (int i = 0; i < 2; ++i)
+        if (b->graph[i]) {
+            cudaGraphExecDestroy(b->graph[i]);
+            b->graph[i] = nullptr;
+        }
+    b->graph_dt = -1.0;
+}
+
+// Enqueues one batch substep on b->stream with fork/join over the scenes' streams.
+fe_status batch_enqueue(fe_batch* b, double dt)
+{
+    const int S = (int)b->scenes.size();
+    cudaEvent_t fork0 = b->events[2 * S], fork1 = b->events[2 * S + 1];
+    FE_CUDA(cudaEventRecord(fork0, b->stream));
+    for (int i = 0; i < S; ++i) {
+        fe_scene* s = b->scenes[i];
+        FE_CUDA(cudaStreamWaitEvent(s->stream, fork0, 0));
+        fe_status st = enqueue_steps(s, dt, kStepSort, kStepRhs);
+        if (st != FE_OK) return st;
+        FE_CUDA(cudaEventRecord(b->events[2 * i], s->stream));
+        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
+    }
+    FE_CUDA(launch_batch_cg(b->work, S, b->rel_tol, b->inner_tol, b->max_it, b->max_refine, b->stream));
+    FE_CUDA(cudaEventRecord(fork1, b->stream));
+    for (int i = 0; i < S; ++i) {
+        fe_scene* s = b->scenes[i];
+        FE_CUDA(cudaStreamWaitEvent(s->stream, fork1, 0));
+        fe_status st = enqueue_steps(s, dt, kStepApply, kStepMove);
+        if (st != FE_OK) return st;
+        FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
+        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
+    }
+    return FE_OK;
+}
+
+fe_status batch_capture(fe_batch* b, int parity, double dt)
+{
+    const int S = (int)b->scenes.size();
+    std::vector<int> par(S), grid(S);
+    for (int i = 0; i < S; ++i) {
+        par[i] = b->scenes[i]->parity;
+        grid[i] = b->scenes[i]->grid_cur;
+    }
+    cudaGraph_t g = nullptr;
+    g_capturing = true;
+    g_capture_launches = 0;
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    fe_status st = e == cudaSuccess ? batch_enqueue(b, dt) : cuda_check(e, "begin capture");
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    g_capturing = false;
+    for (int i = 0; i < S; ++i) {
+        b->scenes[i]->parity = par[i];
+        b->scenes[i]->grid_cur = grid[i];
+    }
+    if (st != FE_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e2 != cudaSuccess) return cuda_check(e2, "end capture");
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_check(e, "graph instantiate");
+    b->graph[parity] = exec;
+    b->graph_kernels[parity] = g_capture_launches;
+    return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out)
+{
+    if (!scenes || !out || count < 1) return set_error(FE_ERR_BAD_ARG, "need at least one scene");
+    if (count > kBatchMaxScenes) return set_error(FE_ERR_BAD_ARG, "at most %d scenes per batch", kBatchMaxScenes);
+    *out = nullptr;
+    const int dev = scenes[0]->device;
+    for (int i = 0; i < count; ++i) {
+        if (!scenes[i]) return set_error(FE_ERR_BAD_ARG, "null scene %d", i);
+        if (scenes[i]->device != dev) return set_error(FE_ERR_BAD_ARG, "all scenes of a batch must share a device");
+        if (!scenes[i]->have_particles) return set_error(FE_ERR_STATE, "scene %d has no particles", i);
+        for (int j = 0; j < i; ++j)
+            if (scenes[j] == scenes[i]) return set_error(FE_ERR_BAD_ARG, "scene %d appears twice", i);
+    }
+    FE_CUDA(cudaSetDevice(dev));
+    fe_batch* b = new (std::nothrow) fe_batch();
+    if (!b) return set_error(FE_ERR_OOM, "host allocation failed");
+    b->scenes.assign(scenes, scenes + count);
+    b->device = dev;
+    const fe_scene_desc& d0 = scenes[0]->desc;
+    b->rel_tol = d0.cg_rel_tol;
+    b->inner_tol = d0.cg_inner_tol;
+    b->max_it = d0.cg_max_it;
+    b->max_refine = d0.max_refine;
+    auto fail = [&](fe_status st) {
+        free_list(b->allocs);
+        for (auto e : b->events) cudaEventDestroy(e);
+        if (b->stream) cudaStreamDestroy(b->stream);
+        delete b;
+        return st;
+    };
+    std::vector<BatchScene> table(count);
+    std::vector<long long> offs(count + 1, 0);
+    for (int i = 0; i < count; ++i) {
+        fe_scene* s = scenes[i];
+        const SceneView& v = s->base;
+        BatchScene& t = table[i];
+        t.nx = v.g.nx;
+        t.ny = v.g.ny;
+        t.nz = v.g.nz;
+        for (int a = 0; a < 3; ++a) {
+            t.ih2d[a] = v.inv_h[a] * v.inv_h[a];
+            t.ih2[a] = (float)t.ih2d[a];
+        }
+        t.marks = v.marks;
+        t.p = v.p;
+        t.b = v.b;
+        t.r0 = s->cg.r0; t.r1 = s->cg.r1; t.w0 = s->cg.w0; t.w1 = s->cg.w1;
+        t.s0 = s->cg.s0; t.s1 = s->cg.s1; t.pv = s->cg.pv; t.x = s->cg.x;
+        t.stats_ring = s->stats_ring;
+        t.stats_counter = s->cg.bar + 2;
+        offs[i + 1] = offs[i] + (long long)v.g.nx * v.g.ny * v.g.nz;
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuda_check(e, "stream create"));
+    b->events.resize(2 * count + 2);
+    for (auto& ev : b->events)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_check(e, "event"));
+    BatchWork& w = b->work;
+    if ((e = batch_cg_blocks(dev, &w.blocks)) != cudaSuccess) return fail(cuda_check(e, "batch occupancy"));
+    BatchScene* d_table;
+    long long* d_offs;
+    uint32_t* d_list;
+    uint8_t* d_lscene;
+    unsigned *d_bc, *d_bar;
+    double* d_tot;
+    int* d_err;
+    if ((e = dalloc(b->allocs, &d_table, count)) != cudaSuccess ||
+        (e = dalloc(b->allocs, &d_offs, count + 1)) != cudaSuccess ||
+        (e = dalloc(b->allocs, &d_list, (size_t)offs[count])) != cudaSuccess ||
+        (e = dalloc(b->allocs, &d_lscene, (size_t)offs[count])) != cudaSuccess ||
+        (e = dalloc(b->allocs, &d_bc, 2 * (size_t)w.blocks)) != cudaSuccess ||
+        (e = dalloc(b->allocs, &d_tot, 3 * (size_t)kBatchMaxScenes * 2)) != cudaSuccess ||
+        (e = dalloc(b->allocs, &d_bar, 4)) != cudaSuccess || (e = dalloc(b->allocs, &d_err, 1)) != cudaSuccess)
+        return fail(cuda_check(e, "batch allocation"));
+    if ((e = cudaMemcpy(d_table, table.data(), count * sizeof(BatchScene), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(d_offs, offs.data(), (count + 1) * sizeof(long long), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(d_tot, 0, 3 * kBatchMaxScenes * 2 * sizeof(double))) != cudaSuccess ||
+        (e = cudaMemset(d_bar, 0, 4 * sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMemset(d_err, 0, sizeof(int))) != cudaSuccess)
+        return fail(cuda_check(e, "batch setup"));
+    w.scenes = d_table;
+    w.cell_offset = d_offs;
+    w.list = d_list;
+    w.list_scene = d_lscene;
+    w.block_count = d_bc;
+    w.totals = d_tot;
+    w.bar = d_bar;
+    w.err = d_err;
+    for (fe_scene* s : b->scenes) {  // finish whatever the scenes had queued before they join the batch
+        if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return fail(cuda_check(e, "scene sync"));
+    }
+    *out = b;
+    return FE_OK;
+}
+
+fe_status fe_batch_destroy(fe_batch* b)
+{
+    if (!b) return set_error(FE_ERR_BAD_ARG, "null batch");
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    batch_drop_graphs(b);
+    free_list(b->allocs);
+    for (auto e : b->events) cudaEventDestroy(e);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return FE_OK;
+}
+
+fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats)
+{
+    if (!b) return set_error(FE_ERR_BAD_ARG, "null batch");
+    if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
+    const int S = (int)b->scenes.size();
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (fe_scene* s : b->scenes) locks.emplace_back(s->mu);
+    FE_CUDA(cudaSetDevice(b->device));
+    if (stats)
+        for (fe_scene* s : b->scenes) FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), b->stream));
+    for (int it = 0; it < nsub; ++it) {
+        if (b->graph_dt != dt) {
+            batch_drop_graphs(b);
+            b->graph_dt = dt;
+        }
+        const int par = b->parity;
+        if (!b->graph[par]) {
+            fe_status st = batch_capture(b, par, dt);
+            if (st != FE_OK) return st;
+        }
+        FE_CUDA(cudaGraphLaunch(b->graph[par], b->stream));
+        g_launches += b->graph_kernels[par];
+        b->parity ^= 1;
+        for (fe_scene* s : b->scenes) {
+            s->parity ^= 1;
+            s->grid_cur = 0;
+        }
+    }
+    FE_CUDA(cudaStreamSynchronize(b->stream));
+    int err = 0;
+    FE_CUDA(cudaMemcpy(&err, b->work.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        cudaMemset(b->work.err, 0, sizeof(int));
+        cudaMemset(b->work.bar, 0, 4 * sizeof(unsigned));
+        cudaMemset(b->work.totals, 0, 3 * kBatchMaxScenes * 2 * sizeof(double));
+        return set_error((fe_status)err, "batched pressure solve: grid barrier wait exceeded its limit");
+    }
+    if (stats && nsub > 0) {
+        const int cnt = std::min(nsub, 1 << 16);
+        for (int i = 0; i < S; ++i)
+            FE_CUDA(cudaMemcpy(stats + (size_t)i * nsub, b->scenes[i]->stats_ring, cnt * sizeof(fe_step_stats),
+                               cudaMemcpyDeviceToHost));
+    }
+    return FE_OK;
+}
 
 }  // extern "C"

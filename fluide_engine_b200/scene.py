@@ -162,3 +162,35 @@ class Scene:
         d = ctypes.c_double()
         check(self._L.fe_scene_divergence(self._h, ctypes.byref(d)))
         return d.value
+
+
+class Batch:
+    """Many scenes advanced together (fe_batch_*): one batched pressure solve per substep, one CUDA graph."""
+
+    def __init__(self, scenes):
+        self.scenes = list(scenes)
+        self._L = _abi.lib()
+        arr = (ctypes.c_void_p * len(self.scenes))(*[s.handle.value for s in self.scenes])
+        h = ctypes.c_void_p()
+        check(self._L.fe_batch_create(arr, len(self.scenes), ctypes.byref(h)))
+        self._h = h
+
+    def step(self, dt, nsub=1, stats=True):
+        S = len(self.scenes)
+        if stats:
+            arr = (_abi.StepStats * max(1, S * nsub))()
+            check(self._L.fe_batch_step(self._h, dt, nsub, arr))
+            return [[arr[i * nsub + k].as_dict() for k in range(nsub)] for i in range(S)]
+        check(self._L.fe_batch_step(self._h, dt, nsub, None))
+        return None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fe_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
