@@ -159,6 +159,137 @@ def run_reference_arm(args):
     return 0
 
 
+def run_batched(args):
+    """Batched independent scenes vs the same scenes one at a time on the plain single-scene path.
+
+    Scenes: cubic grids drawn from {32,48,64,96,128}, a dam-break block with extents U[0.2,0.6] per axis,
+    8 particles per cell, solver drawn from PIC / FLIP(0.95) / APIC (seed 2).  Both arms use the same
+    pressure tolerance (rel 1e-6); times are wall clock around synchronised device work.
+    """
+    import numpy as np
+    import torch
+
+    import fluide_engine_b200 as fe
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(2)
+    specs = []
+    for k in range(args.scenes):
+        n = int(rng.choice([32, 48, 64, 96, 128]))
+        ext = rng.uniform(0.2, 0.6, 3)
+        solver = int(rng.integers(0, 3))
+        specs.append((n, solver, tuple(float(e) for e in ext), k))
+
+    def build():
+        out = []
+        for n, solver, ext, k in specs:
+            pos, vel = fe.seed_regions([dict(kind=0, lo=(0.0, 0.0, 0.0), hi=ext)], (n, n, n), seed=k)
+            sc = fe.Scene((n, n, n), solver=solver, max_cfl=1.0, cg_rel_tol=1e-6)
+            sc.set_particles(pos, vel)
+            out.append(sc)
+        return out
+
+    particles = None
+    # one at a time (each scene's own graph-captured substeps, scene after scene)
+    scenes = build()
+    particles = sum(sc.num_particles() for sc in scenes)
+    for sc in scenes:
+        sc.step(DT, args.warmup, stats=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res_alone = []
+    for sc in scenes:
+        st = sc.step(DT, args.steps, stats=True)
+        res_alone.append(max(x["rel_residual"] for x in st))
+    torch.cuda.synchronize()
+    t_alone = time.perf_counter() - t0
+    for sc in scenes:
+        sc.close()
+    # batched
+    scenes = build()
+    batch = fe.Batch(scenes)
+    batch.step(DT, args.warmup, stats=False)
+    torch.cuda.synchronize()
+    launches0 = fe.kernel_launch_count()
+    t0 = time.perf_counter()
+    st = batch.step(DT, args.steps, stats=True)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    launches = fe.kernel_launch_count() - launches0
+    res_batch = [max(x["rel_residual"] for x in s_) for s_ in st]
+    conv = all(x["converged"] for s_ in st for x in s_)
+    batch.close()
+    for sc in scenes:
+        sc.close()
+    v_batch = particles * args.steps / t_batch
+    v_alone = particles * args.steps / t_alone
+    line = {"metric": METRIC, "value": v_batch, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_batch / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 refinement)",
+            "data": "synthetic (seeded analytic scenes)", "workload_kind": "batched",
+            "config": {"workload": "%d batched scenes, n in {32,48,64,96,128}, block extents U[0.2,0.6], "
+                                   "solver U{PIC,FLIP,APIC} (seed 2), dt=1/240, CG rel 1e-6" % len(specs),
+                       "scenes": [[n, ["PIC", "FLIP", "APIC"][sv]] for n, sv, _, _ in specs],
+                       "particles_total": particles, "timing": "wall clock around synchronised device work"},
+            "one_at_a_time": {"value": v_alone, "ms_per_step_all_scenes": t_alone / args.steps * 1e3},
+            "batched_over_one_at_a_time": v_batch / v_alone,
+            "accuracy": {"rel_residual_max_batched": max(res_batch), "rel_residual_max_alone": max(res_alone),
+                         "converged_all": conv},
+            "gpu_launches": int(launches)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_served(args):
+    """Served request stream (the served configuration scaled down in duration and resolution; see --trace-*)."""
+    import numpy as np
+    import torch
+
+    import fluide_engine_b200 as fe
+    from fluide_engine_b200 import serving
+
+    torch.cuda.set_device(0)
+    res = tuple(int(x) for x in args.trace_res.split(","))
+    fr = tuple(int(x) for x in args.trace_frames.split(","))
+    jobs = serving.poisson_trace(args.trace_rate, args.trace_seconds, 3, resolutions=res, frames=fr)
+    srv = serving.Server(hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), max_batch=args.max_batch)
+    for j in jobs:
+        srv.submit(j)
+    wall, psteps = srv.run()
+    p50, p99 = srv.latency_percentiles()
+    served = psteps / wall
+    # the same jobs one at a time through the plain single-scene path (frame by frame)
+    t_alone, ps_alone, ms_alone = 0.0, 0, []
+    for j in jobs:
+        pos, vel = fe.seed_regions(j.regions, (j.n,) * 3, seed=j.seed)
+        sc = fe.Scene((j.n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6)
+        sc.set_particles(pos, vel)
+        torch.cuda.synchronize()
+        for _ in range(j.frames):
+            t0 = time.perf_counter()
+            sc.step(j.dt, j.substeps_per_frame, stats=False)
+            sc.synchronize()
+            dt_ = time.perf_counter() - t0
+            ms_alone.append(dt_ * 1e3)
+            t_alone += dt_
+            ps_alone += pos.shape[0] * j.substeps_per_frame
+        sc.close()
+    line = {"metric": METRIC, "value": served, "unit": METRIC, "n_gpus": 1, "steps": int(sum(j.frames * j.substeps_per_frame for j in jobs)),
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded Poisson trace)", "workload_kind": "served",
+            "config": {"workload": "Poisson %.0f jobs/s for %.0f s (seed 3), APIC pool+sphere, n in %s, %s frames x 4 "
+                                   "substeps, dt=1/480, HBM budget %.0f GB, batch <= %d"
+                                   % (args.trace_rate, args.trace_seconds, list(res), list(fr), args.hbm_budget_gb,
+                                      args.max_batch), "jobs": len(jobs)},
+            "frame_ms": {"p50": p50, "p99": p99},
+            "one_at_a_time": {"value": ps_alone / t_alone, "frame_ms_p50": float(np.percentile(ms_alone, 50)),
+                              "frame_ms_p99": float(np.percentile(ms_alone, 99)),
+                              "note": "compute time only (no queueing), so its latency is a lower bound"},
+            "served_over_one_at_a_time": served / (ps_alone / t_alone), "wall_s": wall}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -170,9 +301,21 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=1, help="substeps of the CPU reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "served"])
+    ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
+    ap.add_argument("--trace-rate", type=float, default=20.0)
+    ap.add_argument("--trace-seconds", type=float, default=3.0)
+    ap.add_argument("--trace-res", default="32,48,64")
+    ap.add_argument("--trace-frames", default="4,16")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
+    ap.add_argument("--max-batch", type=int, default=32)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "served":
+        return run_served(args)
     args.warmup = max(args.warmup, 3)
 
     import numpy as np

@@ -31,6 +31,7 @@ namespace fe {
 namespace {
 
 constexpr int kCgThreads = 1024;
+constexpr int kMultiThreads = 256;
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
 struct CgParams {
@@ -75,11 +76,11 @@ __device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigne
     return true;
 }
 
-__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen)
+__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        bar_arrive_wait(w.bar, w.err, gridDim.x, w.partial);
+        bar_arrive_wait(w.bar, w.err, (unsigned)nblk, w.partial);
         gen = next_gen(gen);
     }
     __syncthreads();
@@ -93,7 +94,8 @@ __device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen)
 // readers arrive at barrier k+1.  All blocks read the same final totals, so their branch decisions
 // agree (the summation order, and hence the last bits, can vary from run to run).
 template <int N>
-__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w, unsigned& gen)
+__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w, unsigned& gen,
+                                            int nblk)
 {
     static_assert(N <= 4, "at most 4 sums per reduction");
     // warp partials use sh[0, 32 N), the totals sh[128, 128 + N): disjoint, so a warp that races ahead into
@@ -127,7 +129,7 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] 
             for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
             const unsigned old = word.fetch_add(1u, cuda::memory_order_acq_rel);
             bool ok = true;
-            if ((old & 0xffffu) == gridDim.x - 1) {
+            if ((old & 0xffffu) == (unsigned)nblk - 1) {
                 double* next = totals + 4 * (next_gen(old >> 16) % 3u);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) next[k] = 0.0;
@@ -197,15 +199,18 @@ __device__ __forceinline__ float apply_row(const Stencil7& st, int c, uint32_t m
     return st.ih2[0] * ax + st.ih2[1] * ay + st.ih2[2] * az;
 }
 
-__global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgParams prm)
+// The solver body, run by `nblk` blocks of which this is block `blk` (a whole grid for one scene, or a
+// block range of a multi-scene launch, see k_multi_cg); every barrier and reduction spans those blocks.
+__device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, const CgParams& prm, const int blk,
+                                        const int nblk)
 {
     __shared__ double sh[32 * 4 + 4];
     __shared__ uint32_t s_warp[32];
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
     const int sxy = nx * ny;
     const int nc = sxy * nz;
-    const int T = gridDim.x * blockDim.x;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int T = nblk * blockDim.x;
+    const int tid = blk * blockDim.x + threadIdx.x;
     const uint8_t* __restrict__ marks = v.marks;
     const double ih2d[3] = {v.inv_h[0] * v.inv_h[0], v.inv_h[1] * v.inv_h[1], v.inv_h[2] * v.inv_h[2]};
     Stencil7 st;
@@ -228,8 +233,8 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
     if (threadIdx.x == 0) gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[0]).load(cuda::memory_order_relaxed) >> 16;
 
     // ---- setup: zero non-FLUID entries, ||b||^2, per-block FLUID counts over the block's cell range
-    const int chunk = (nc + gridDim.x - 1) / gridDim.x;
-    const int cb = min(nc, (int)blockIdx.x * chunk), ce = min(nc, cb + chunk);
+    const int chunk = (nc + nblk - 1) / nblk;
+    const int cb = min(nc, blk * chunk), ce = min(nc, cb + chunk);
     double acc[2] = {0.0, 0.0};
     for (int c = cb + threadIdx.x; c < ce; c += blockDim.x) {
         if (marks[c] == FE_CELL_FLUID) {
@@ -247,13 +252,13 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
     }
     // block offset = FLUID count of all earlier blocks (fixed order), total = all blocks
     const double mine = block_sum1(acc[1], sh);
-    if (threadIdx.x == 0) w.partial[16 + blockIdx.x] = mine;
+    if (threadIdx.x == 0) w.partial[16 + blk] = mine;
     double tot[2] = {acc[0], acc[1]};
-    if (!grid_reduce<2>(tot, sh, w, gen)) return;
+    if (!grid_reduce<2>(tot, sh, w, gen, nblk)) return;
     const double bnorm = sqrt(tot[0]);
     const int F = (int)tot[1];
     double before = 0.0;
-    for (int bb = threadIdx.x; bb < (int)blockIdx.x; bb += blockDim.x) before += __ldcg(w.partial + 16 + bb);
+    for (int bb = threadIdx.x; bb < blk; bb += blockDim.x) before += __ldcg(w.partial + 16 + bb);
     before = block_sum1(before, sh);
     // ordered compaction of this block's FLUID cells with their in-domain masks
     uint32_t base = (uint32_t)before;
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
         base += total;
         __syncthreads();
     }
-    if (!grid_sync(w, gen)) return;
+    if (!grid_sync(w, gen, nblk)) return;
     const double target = prm.rel_tol * bnorm;
     if (bnorm == 0.0) {
         for (int e = tid; e < F; e += T) p64[list[e] >> 6] = 0.0;
@@ -310,7 +315,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
             racc[0] += rr * rr;
         }
         cur = 0;
-        if (!grid_reduce<1>(racc, sh, w, gen)) return;
+        if (!grid_reduce<1>(racc, sh, w, gen, nblk)) return;
         rnorm = sqrt(racc[0]);
         if (rnorm <= target) {
             converged = true;
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
             d0[0] += (double)rc * (double)rc;
             d0[1] += (double)wc * (double)rc;
         }
-        if (!grid_reduce<2>(d0, sh, w, gen)) return;
+        if (!grid_reduce<2>(d0, sh, w, gen, nblk)) return;
         double gamma = d0[0], delta = d0[1];
         const double gamma0 = gamma;
         const double want = fmax(prm.inner_tol, 0.25 * target / rnorm);
@@ -376,7 +381,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
                 dd[0] += (double)rc * (double)rc;
                 dd[1] += (double)wc * (double)rc;
             }
-            if (!grid_reduce<2>(dd, sh, w, gen)) return;
+            if (!grid_reduce<2>(dd, sh, w, gen, nblk)) return;
             ++total_it;
             cur ^= 1;
             gamma_prev = gamma;
@@ -390,9 +395,9 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
             const int c = (int)(list[e] >> 6);
             p64[c] += (double)X[c];
         }
-        if (!grid_sync(w, gen)) return;
+        if (!grid_sync(w, gen, nblk)) return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && prm.stats_ring) {
+    if (blk == 0 && threadIdx.x == 0 && prm.stats_ring) {
         const unsigned slot = atomicAdd(prm.stats_counter, 1u) % prm.stats_cap;
         fe_step_stats s;
         s.cg_iterations = total_it;
@@ -405,7 +410,59 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
     }
 }
 
+__global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgParams prm)
+{
+    cg_body(v, w, prm, blockIdx.x, gridDim.x);
+}
+
+// Many scenes in one cooperative launch: blocks [start[s], start[s+1]) solve scene s with their own barrier
+// and reductions, so scenes iterate independently and concurrently.
+__global__ void __launch_bounds__(kMultiThreads) k_multi_cg(const MultiCgScene* __restrict__ scenes, int S)
+{
+    int sc = 0;
+    while (sc + 1 < S && (int)blockIdx.x >= scenes[sc + 1].block_start) ++sc;
+    const MultiCgScene& m = scenes[sc];
+    CgParams prm;
+    prm.rel_tol = m.rel_tol;
+    prm.inner_tol = m.inner_tol;
+    prm.max_it = m.max_it;
+    prm.max_refine = m.max_refine;
+    prm.stats_ring = m.work.stats;
+    prm.stats_counter = m.work.bar + 2;
+    prm.stats_cap = 1u << 16;
+    cg_body(m.view, m.work, prm, (int)blockIdx.x - m.block_start, m.block_count);
+}
+
 }  // namespace
+
+cudaError_t multi_cg_capacity(int device, int* max_blocks, int* threads)
+{
+    int sms = 0, per_sm = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_multi_cg, kMultiThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    *max_blocks = sms * per_sm;
+    *threads = kMultiThreads;
+    return cudaSuccess;
+}
+
+cudaError_t launch_multi_cg(const MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)total_blocks);
+    cfg.blockDim = dim3((unsigned)kMultiThreads);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_multi_cg, scenes, S);
+    count_launch();
+    return e;
+}
 
 cudaError_t cg_prepare(CgWork& w, int device)
 {

@@ -19,6 +19,8 @@
 namespace fe {
 
 constexpr int kMaxRefineDefault = 12;
+constexpr int kMaxCgBlocks = 4096;  // solver blocks one scene can be given (sizes its partial-sum buffer)
+constexpr int kBatchMaxScenes = 64;
 
 struct GridDims {
     int nx, ny, nz;
@@ -171,6 +173,18 @@ struct CgWork {
     int blocks, threads;
 };
 cudaError_t cg_prepare(CgWork& w, int device);
+
+// One scene of a multi-scene pressure solve (fe_cg.cu k_multi_cg): the scene's grid view and solver
+// buffers, its solver settings and the block range [block_start, block_start + block_count) that solves it.
+struct MultiCgScene {
+    SceneView view;
+    CgWork work;
+    double rel_tol, inner_tol;
+    int max_it, max_refine;
+    int block_start, block_count;
+};
+cudaError_t multi_cg_capacity(int device, int* max_blocks, int* threads);
+cudaError_t launch_multi_cg(const MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st);
 cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, double inner_tol, int max_it, int max_refine,
                       cudaStream_t st);
 

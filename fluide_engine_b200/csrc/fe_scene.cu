@@ -11,12 +11,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <new>
 #include <vector>
 
-#include "fe_batch.cuh"
 #include "fe_internal.cuh"
 #include "fe_seed.h"
 
@@ -224,8 +224,9 @@ fe_status alloc_grid(fe_scene* s)
     w.s0 = vec + 4 * nc; w.s1 = vec + 5 * nc; w.pv = vec + 6 * nc; w.x = vec + 7 * nc;
     FE_CUDA(dalloc(L, &w.list, nc));
     FE_CUDA(cg_prepare(w, s->device));
-    FE_CUDA(dalloc(L, &w.partial, (size_t)w.blocks * 4 + 16));  // 3 rotating totals slots + per-block counts
-    FE_CUDA(cudaMemset(w.partial, 0, ((size_t)w.blocks * 4 + 16) * sizeof(double)));
+    // 3 rotating totals slots (12 doubles) + per-block FLUID counts of up to kMaxCgBlocks solver blocks
+    FE_CUDA(dalloc(L, &w.partial, 16 + (size_t)kMaxCgBlocks));
+    FE_CUDA(cudaMemset(w.partial, 0, (16 + (size_t)kMaxCgBlocks) * sizeof(double)));
     FE_CUDA(dalloc(L, &w.bar, 8));
     FE_CUDA(cudaMemset(w.bar, 0, 8 * sizeof(unsigned)));
     FE_CUDA(dalloc(L, &w.err, 1));
@@ -978,7 +979,8 @@ int32_t fe_abi_version(void) { return 10000; }
 // ------------------------------------------------------------------------------------------- batches
 //
 // A batch advances many independent scenes together: per substep, every scene's pre-solve phase runs on
-// its own stream, ONE persistent kernel solves all scenes' pressure systems (fe_batch_cg.cu), and every
+// its own stream, ONE cooperative launch solves all scenes' pressure systems (k_multi_cg: each scene on its
+// own block range with its own barrier, so scenes iterate independently and concurrently), and every
 // scene's post-solve phase runs on its own stream again.  The whole batch substep is captured as one CUDA
 // graph (fork/join across the scenes' streams) per particle-buffer parity and replayed.
 
@@ -986,16 +988,21 @@ struct fe_batch {
     std::vector<fe_scene*> scenes;
     int device = 0;
     cudaStream_t stream = nullptr;
-    BatchWork work{};
+    MultiCgScene* table = nullptr;     // device copy of the per-scene solver table
+    int total_blocks = 0;
     std::vector<void*> allocs;
     std::vector<cudaEvent_t> events;   // 2 per scene + 2
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_kernels[2] = {0, 0};
     double graph_dt = -1.0;
     int parity = 0;
-    double rel_tol = 1e-6, inner_tol = 1e-4;
-    int max_it = 2000, max_refine = kMaxRefineDefault;
+    int64_t steps_done = 0;   // substeps since creation: a young batch replays per-scene graphs
 };
+
+// A batch replays its scenes' own phase graphs around the multi-scene solve for its first
+// kBatchCaptureAfter substeps (creating a batch then costs no capture, which is what a server with
+// changing membership needs); after that the whole batch substep is captured as one graph.
+constexpr int64_t kBatchCaptureAfter = 8;
 
 namespace {
 
@@ -1023,7 +1030,7 @@ fe_status batch_enqueue(fe_batch* b, double dt)
         FE_CUDA(cudaEventRecord(b->events[2 * i], s->stream));
         FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
     }
-    FE_CUDA(launch_batch_cg(b->work, S, b->rel_tol, b->inner_tol, b->max_it, b->max_refine, b->stream));
+    FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
     FE_CUDA(cudaEventRecord(fork1, b->stream));
     for (int i = 0; i < S; ++i) {
         fe_scene* s = b->scenes[i];
@@ -1033,6 +1040,47 @@ fe_status batch_enqueue(fe_batch* b, double dt)
         FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
         FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
     }
+    return FE_OK;
+}
+
+// One batch substep from the scenes' own captured phase graphs (pre-solve and post-solve, captured once
+// per scene and dt) around the multi-scene solve, forked and joined over the scenes' streams.
+fe_status batch_step_scene_graphs(fe_batch* b, double dt)
+{
+    const int S = (int)b->scenes.size();
+    for (fe_scene* s : b->scenes) {
+        if (s->graph_dt != dt) {
+            drop_graphs(s);
+            s->graph_dt = dt;
+        }
+        if (!s->graph[s->parity][0]) {
+            fe_status st = capture_graphs(s, s->parity, dt);
+            if (st != FE_OK) return st;
+        }
+    }
+    cudaEvent_t fork0 = b->events[2 * S], fork1 = b->events[2 * S + 1];
+    FE_CUDA(cudaEventRecord(fork0, b->stream));
+    for (int i = 0; i < S; ++i) {
+        fe_scene* s = b->scenes[i];
+        FE_CUDA(cudaStreamWaitEvent(s->stream, fork0, 0));
+        FE_CUDA(cudaGraphLaunch(s->graph[s->parity][0], s->stream));
+        g_launches += s->graph_kernels[s->parity][0];
+        FE_CUDA(cudaEventRecord(b->events[2 * i], s->stream));
+        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
+    }
+    FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
+    FE_CUDA(cudaEventRecord(fork1, b->stream));
+    for (int i = 0; i < S; ++i) {
+        fe_scene* s = b->scenes[i];
+        FE_CUDA(cudaStreamWaitEvent(s->stream, fork1, 0));
+        FE_CUDA(cudaGraphLaunch(s->graph[s->parity][2], s->stream));
+        g_launches += s->graph_kernels[s->parity][2];
+        FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
+        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
+        s->parity ^= 1;  // the pre-solve graph's sort flipped the particle buffer sets
+        s->grid_cur = 0;
+    }
+    b->parity ^= 1;
     return FE_OK;
 }
 
@@ -1091,11 +1139,6 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
     if (!b) return set_error(FE_ERR_OOM, "host allocation failed");
     b->scenes.assign(scenes, scenes + count);
     b->device = dev;
-    const fe_scene_desc& d0 = scenes[0]->desc;
-    b->rel_tol = d0.cg_rel_tol;
-    b->inner_tol = d0.cg_inner_tol;
-    b->max_it = d0.cg_max_it;
-    b->max_refine = d0.max_refine;
     auto fail = [&](fe_status st) {
         free_list(b->allocs);
         for (auto e : b->events) cudaEventDestroy(e);
@@ -1103,64 +1146,52 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
         delete b;
         return st;
     };
-    std::vector<BatchScene> table(count);
-    std::vector<long long> offs(count + 1, 0);
+    // Solver blocks per scene, proportional to its particle count (a proxy for its FLUID cells), at least
+    // one each; the multi-scene launch fills the device's co-resident capacity.
+    int capacity = 0, threads = 0;
+    cudaError_t e = multi_cg_capacity(dev, &capacity, &threads);
+    if (e != cudaSuccess) return fail(cuda_check(e, "multi-scene occupancy"));
+    capacity = std::min(capacity, kMaxCgBlocks);
+    if (capacity < count) return fail(set_error(FE_ERR_BAD_ARG, "more scenes than solver blocks (%d)", capacity));
+    double total_np = 0.0;
+    for (int i = 0; i < count; ++i) total_np += (double)scenes[i]->base.np;
+    std::vector<int> nblk(count, 1);
+    int used = count;
+    for (int i = 0; i < count; ++i) {
+        const int extra = (int)std::floor((capacity - count) * (double)scenes[i]->base.np / std::max(total_np, 1.0));
+        nblk[i] += extra;
+        used += extra;
+    }
+    for (int k = 0; used < capacity; ++k, ++used) {  // leftovers to the largest scenes
+        int best = 0;
+        for (int i = 1; i < count; ++i)
+            if (scenes[i]->base.np > scenes[best]->base.np) best = i;
+        nblk[(best + k) % count] += 1;
+    }
+    std::vector<MultiCgScene> table(count);
+    int start = 0;
     for (int i = 0; i < count; ++i) {
         fe_scene* s = scenes[i];
-        const SceneView& v = s->base;
-        BatchScene& t = table[i];
-        t.nx = v.g.nx;
-        t.ny = v.g.ny;
-        t.nz = v.g.nz;
-        for (int a = 0; a < 3; ++a) {
-            t.ih2d[a] = v.inv_h[a] * v.inv_h[a];
-            t.ih2[a] = (float)t.ih2d[a];
-        }
-        t.marks = v.marks;
-        t.p = v.p;
-        t.b = v.b;
-        t.r0 = s->cg.r0; t.r1 = s->cg.r1; t.w0 = s->cg.w0; t.w1 = s->cg.w1;
-        t.s0 = s->cg.s0; t.s1 = s->cg.s1; t.pv = s->cg.pv; t.x = s->cg.x;
-        t.stats_ring = s->stats_ring;
-        t.stats_counter = s->cg.bar + 2;
-        offs[i + 1] = offs[i] + (long long)v.g.nx * v.g.ny * v.g.nz;
+        MultiCgScene& t = table[i];
+        t.view = s->base;
+        t.work = s->cg;
+        t.rel_tol = s->desc.cg_rel_tol;
+        t.inner_tol = s->desc.cg_inner_tol;
+        t.max_it = s->desc.cg_max_it;
+        t.max_refine = s->desc.max_refine;
+        t.block_start = start;
+        t.block_count = nblk[i];
+        start += nblk[i];
     }
-    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    b->total_blocks = start;
+    e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_check(e, "stream create"));
     b->events.resize(2 * count + 2);
     for (auto& ev : b->events)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_check(e, "event"));
-    BatchWork& w = b->work;
-    if ((e = batch_cg_blocks(dev, &w.blocks)) != cudaSuccess) return fail(cuda_check(e, "batch occupancy"));
-    BatchScene* d_table;
-    long long* d_offs;
-    uint32_t* d_list;
-    uint8_t* d_lscene;
-    unsigned *d_bc, *d_bar;
-    double* d_tot;
-    int* d_err;
-    if ((e = dalloc(b->allocs, &d_table, count)) != cudaSuccess ||
-        (e = dalloc(b->allocs, &d_offs, count + 1)) != cudaSuccess ||
-        (e = dalloc(b->allocs, &d_list, (size_t)offs[count])) != cudaSuccess ||
-        (e = dalloc(b->allocs, &d_lscene, (size_t)offs[count])) != cudaSuccess ||
-        (e = dalloc(b->allocs, &d_bc, 2 * (size_t)w.blocks)) != cudaSuccess ||
-        (e = dalloc(b->allocs, &d_tot, 3 * (size_t)kBatchMaxScenes * 2)) != cudaSuccess ||
-        (e = dalloc(b->allocs, &d_bar, 4)) != cudaSuccess || (e = dalloc(b->allocs, &d_err, 1)) != cudaSuccess)
-        return fail(cuda_check(e, "batch allocation"));
-    if ((e = cudaMemcpy(d_table, table.data(), count * sizeof(BatchScene), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(d_offs, offs.data(), (count + 1) * sizeof(long long), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemset(d_tot, 0, 3 * kBatchMaxScenes * 2 * sizeof(double))) != cudaSuccess ||
-        (e = cudaMemset(d_bar, 0, 4 * sizeof(unsigned))) != cudaSuccess ||
-        (e = cudaMemset(d_err, 0, sizeof(int))) != cudaSuccess)
+    if ((e = dalloc(b->allocs, &b->table, count)) != cudaSuccess) return fail(cuda_check(e, "batch allocation"));
+    if ((e = cudaMemcpy(b->table, table.data(), count * sizeof(MultiCgScene), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(cuda_check(e, "batch setup"));
-    w.scenes = d_table;
-    w.cell_offset = d_offs;
-    w.list = d_list;
-    w.list_scene = d_lscene;
-    w.block_count = d_bc;
-    w.totals = d_tot;
-    w.bar = d_bar;
-    w.err = d_err;
     for (fe_scene* s : b->scenes) {  // finish whatever the scenes had queued before they join the batch
         if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return fail(cuda_check(e, "scene sync"));
     }
@@ -1192,6 +1223,13 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
     if (stats)
         for (fe_scene* s : b->scenes) FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), b->stream));
     for (int it = 0; it < nsub; ++it) {
+        if (b->steps_done < kBatchCaptureAfter || std::any_of(b->scenes.begin(), b->scenes.end(),
+                                                                 [](fe_scene* s) { return s->graphs_disabled; })) {
+            fe_status st = batch_step_scene_graphs(b, dt);
+            if (st != FE_OK) return st;
+            ++b->steps_done;
+            continue;
+        }
         if (b->graph_dt != dt) {
             batch_drop_graphs(b);
             b->graph_dt = dt;
@@ -1203,6 +1241,7 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
         }
         FE_CUDA(cudaGraphLaunch(b->graph[par], b->stream));
         g_launches += b->graph_kernels[par];
+        ++b->steps_done;
         b->parity ^= 1;
         for (fe_scene* s : b->scenes) {
             s->parity ^= 1;
@@ -1210,13 +1249,9 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
         }
     }
     FE_CUDA(cudaStreamSynchronize(b->stream));
-    int err = 0;
-    FE_CUDA(cudaMemcpy(&err, b->work.err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) {
-        cudaMemset(b->work.err, 0, sizeof(int));
-        cudaMemset(b->work.bar, 0, 4 * sizeof(unsigned));
-        cudaMemset(b->work.totals, 0, 3 * kBatchMaxScenes * 2 * sizeof(double));
-        return set_error((fe_status)err, "batched pressure solve: grid barrier wait exceeded its limit");
+    for (fe_scene* s : b->scenes) {
+        fe_status st = check_device_error(s);
+        if (st != FE_OK) return st;
     }
     if (stats && nsub > 0) {
         const int cnt = std::min(nsub, 1 << 16);

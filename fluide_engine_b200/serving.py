@@ -114,6 +114,8 @@ class Server:
             changed = self._retire(now)
             changed |= self._admit(now)
             if not self.running:
+                if not self.waiting:
+                    break
                 # idle until the next arrival
                 time.sleep(max(0.0, min(0.01, self.waiting[0][0] - now)))
                 continue

@@ -164,11 +164,12 @@ fe_status fe_scene_set_stream(fe_scene* s, void* stream);
 fe_status fe_scene_synchronize(fe_scene* s);
 
 /* Batches: many independent scenes (up to 64, one device) advanced together.  Per substep every scene's
- * pre-solve phase runs on its own stream, ONE persistent kernel solves all scenes' pressure systems over a
- * flat (scene, cell) work list with one shared grid barrier per iteration, and every scene's post-solve
- * phase runs on its own stream; the batch substep is one captured CUDA graph.  Results equal each scene
- * stepped alone (same algorithm and tolerances, those of the first scene).  No reference counterpart: the
- * reference runs one simulator per process (PhysicsAnimation::AdvanceSingleFrame, physics_animation.cpp:17-21). */
+ * pre-solve phase runs on its own stream, ONE cooperative launch solves all scenes' pressure systems (each
+ * scene on its own block range, sized by its particle count, with its own grid barrier, so the scenes
+ * iterate independently and concurrently), and every scene's post-solve phase runs on its own stream; the
+ * batch substep is one captured CUDA graph.  Results equal each scene stepped alone (same algorithm, each
+ * scene's own tolerances).  No reference counterpart: the reference runs one simulator per process
+ * (PhysicsAnimation::AdvanceSingleFrame, physics_animation.cpp:17-21). */
 typedef struct fe_batch fe_batch;
 fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out);
 fe_status fe_batch_destroy(fe_batch* b);
