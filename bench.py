@@ -258,22 +258,25 @@ def run_served(args):
     wall, psteps = srv.run()
     p50, p99 = srv.latency_percentiles()
     served = psteps / wall
-    # the same jobs one at a time through the plain single-scene path (frame by frame)
-    t_alone, ps_alone, ms_alone = 0.0, 0, []
-    for j in jobs:
+    # the same trace served one job at a time (FIFO) through the plain single-scene path: a job starts at
+    # max(arrival, end of the previous job); setup (seeding, scene creation) is inside the measured time as
+    # it is for the server
+    clock, ps_alone, ms_alone = 0.0, 0, []
+    for j in sorted(jobs, key=lambda x: x.arrival):
+        start = max(j.arrival, clock)
+        t_job = time.perf_counter()
         pos, vel = fe.seed_regions(j.regions, (j.n,) * 3, seed=j.seed)
         sc = fe.Scene((j.n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6)
         sc.set_particles(pos, vel)
-        torch.cuda.synchronize()
         for _ in range(j.frames):
             t0 = time.perf_counter()
             sc.step(j.dt, j.substeps_per_frame, stats=False)
             sc.synchronize()
-            dt_ = time.perf_counter() - t0
-            ms_alone.append(dt_ * 1e3)
-            t_alone += dt_
+            ms_alone.append((time.perf_counter() - t0) * 1e3)
             ps_alone += pos.shape[0] * j.substeps_per_frame
         sc.close()
+        clock = start + (time.perf_counter() - t_job)
+    t_alone = clock
     line = {"metric": METRIC, "value": served, "unit": METRIC, "n_gpus": 1, "steps": int(sum(j.frames * j.substeps_per_frame for j in jobs)),
             "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded Poisson trace)", "workload_kind": "served",
@@ -282,9 +285,11 @@ def run_served(args):
                                    % (args.trace_rate, args.trace_seconds, list(res), list(fr), args.hbm_budget_gb,
                                       args.max_batch), "jobs": len(jobs)},
             "frame_ms": {"p50": p50, "p99": p99},
-            "one_at_a_time": {"value": ps_alone / t_alone, "frame_ms_p50": float(np.percentile(ms_alone, 50)),
+            "one_at_a_time": {"value": ps_alone / t_alone, "makespan_s": t_alone,
+                              "frame_ms_p50": float(np.percentile(ms_alone, 50)),
                               "frame_ms_p99": float(np.percentile(ms_alone, 99)),
-                              "note": "compute time only (no queueing), so its latency is a lower bound"},
+                              "note": "FIFO over the same arrival trace, one job at a time; frame latency excludes "
+                                      "the queueing delay before a job starts"},
             "served_over_one_at_a_time": served / (ps_alone / t_alone), "wall_s": wall}
     print(json.dumps(line), flush=True)
     return 0

@@ -1192,9 +1192,7 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
     if ((e = dalloc(b->allocs, &b->table, count)) != cudaSuccess) return fail(cuda_check(e, "batch allocation"));
     if ((e = cudaMemcpy(b->table, table.data(), count * sizeof(MultiCgScene), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(cuda_check(e, "batch setup"));
-    for (fe_scene* s : b->scenes) {  // finish whatever the scenes had queued before they join the batch
-        if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return fail(cuda_check(e, "scene sync"));
-    }
+    // no host synchronisation: a scene's earlier work precedes the batch's work in its own stream order
     *out = b;
     return FE_OK;
 }
