@@ -41,6 +41,23 @@ def workload_config(n, steps, warmup, n_gpus, np_):
     }
 
 
+def max_over_ranks(x, device):
+    """The slowest rank's value of a time (every rank calls this at the same point); x itself on one rank."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, particles_per_rank, steps, seconds):
+    """Whole-job particle-steps/s of `world` independent replicas timed by the slowest rank."""
+    return world * particles_per_rank * steps / seconds
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -149,12 +166,12 @@ def run_reference_arm(args):
     n_gpus = args.gpus
     steps = max(1, min(args.steps, args.ref_steps))
     value, ms, info = reference_sample(args.n, steps)
+    particles = int(round(value * ms / 1e3))
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": n_gpus, "steps": steps, "warmup": 0,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded analytic scene)", "impl": "reference",
-            "config": workload_config(args.n, steps, 0, 1, None), "cpu_baseline": info,
+            "config": workload_config(args.n, steps, 0, 1, particles), "cpu_baseline": info,
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    line["config"]["particles"] = int(round(value * ms / 1e3))
     print(json.dumps(line), flush=True)
     return 0
 
@@ -262,19 +279,29 @@ def run_served(args):
     # max(arrival, end of the previous job); setup (seeding, scene creation) is inside the measured time as
     # it is for the server
     clock, ps_alone, ms_alone = 0.0, 0, []
+    alone_split = {"seed": 0.0, "create": 0.0, "step": 0.0, "retire": 0.0}
     for j in sorted(jobs, key=lambda x: x.arrival):
         start = max(j.arrival, clock)
         t_job = time.perf_counter()
         pos, vel = fe.seed_regions(j.regions, (j.n,) * 3, seed=j.seed)
+        t1 = time.perf_counter()
         sc = fe.Scene((j.n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6)
         sc.set_particles(pos, vel)
+        t2 = time.perf_counter()
         for _ in range(j.frames):
             t0 = time.perf_counter()
             sc.step(j.dt, j.substeps_per_frame, stats=False)
             sc.synchronize()
             ms_alone.append((time.perf_counter() - t0) * 1e3)
             ps_alone += pos.shape[0] * j.substeps_per_frame
+        t3 = time.perf_counter()
+        sc.particles()
         sc.close()
+        t4 = time.perf_counter()
+        alone_split["seed"] += t1 - t_job
+        alone_split["create"] += t2 - t1
+        alone_split["step"] += t3 - t2
+        alone_split["retire"] += t4 - t3
         clock = start + (time.perf_counter() - t_job)
     t_alone = clock
     line = {"metric": METRIC, "value": served, "unit": METRIC, "n_gpus": 1, "steps": int(sum(j.frames * j.substeps_per_frame for j in jobs)),
@@ -288,9 +315,11 @@ def run_served(args):
             "one_at_a_time": {"value": ps_alone / t_alone, "makespan_s": t_alone,
                               "frame_ms_p50": float(np.percentile(ms_alone, 50)),
                               "frame_ms_p99": float(np.percentile(ms_alone, 99)),
+                              "time_s": alone_split,
                               "note": "FIFO over the same arrival trace, one job at a time; frame latency excludes "
                                       "the queueing delay before a job starts"},
-            "served_over_one_at_a_time": served / (ps_alone / t_alone), "wall_s": wall}
+            "served_over_one_at_a_time": served / (ps_alone / t_alone), "wall_s": wall,
+            "server_time_s": dict(srv.timing), "batch_rebuilds": srv.rebuilds}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -363,12 +392,8 @@ def main():
     barrier()
     launches = fe.kernel_launch_count() - launches0
     clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * N * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), "cuda")
+    value = replica_throughput(world, N, args.steps, ms / 1e3)
 
     # roofline of the dominant kernel: the persistent CG kernel (solve phase = exactly one launch)
     cg_ms = phase_ms[:, 1].astype(np.float64)
@@ -402,12 +427,8 @@ def main():
         pin_pos.copy_(out_pos)
         pin_vel.copy_(out_vel)
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * N * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, "cuda")
+    e2e_value = replica_throughput(world, N, e2e_steps, e2e_s)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -8,9 +8,15 @@
 // Stable counting sort, O(N + K):
 //   k_keys     key of each particle, rank = atomic slot in its cell (order among equal keys arbitrary)
 //   scan       exclusive prefix sum of the per-cell counts -> cell_start (K + 1 entries)
-//   k_place    perm[cell_start[key] + rank] = particle
-//   k_segsort  each cell's run re-ordered by particle index, which makes the result identical to a
-//              stable sort by key (the oracle is a CPU stable counting sort of the same keys)
+//   k_place    perm[cell_start[key] + rank] = particle (a cell's run in arbitrary order)
+//   k_cellrank each particle's final slot = run start + the number of particles of its run with a smaller
+//              index, so the runs end up ordered by particle index and the result is identical to a stable
+//              sort by key (the oracle is a CPU stable counting sort of the same keys); O(run length) per
+//              particle, all particles of a run in parallel
+//   k_bigcell  runs longer than kBigCell (particles piled into one cell, e.g. clamped into a wall corner)
+//              are ordered by one block each with a bitonic network instead, so the cost stays
+//              O(n log^2 n) per run rather than O(n^2)
+//   k_place_final  perm[final slot] = particle
 //   k_gather   particle arrays permuted into the second buffer set
 #include "fe_internal.cuh"
 
@@ -121,29 +127,77 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const uint32_t* __r
     if (base + kScanItems >= n && base < n) out[n] = run;  // the thread holding the last element writes the total
 }
 
-__global__ void k_place(SceneView v)
+// After the scan the per-cell counts are dead until the next sort, so cell_count doubles as the list of
+// long runs (their keys, at most key_space of them); how many there are is counted in the word after the
+// scan's block sums (scan scratch holds nb + 2 words).
+constexpr uint32_t kBigCell = 1024;
+constexpr int kBigCellBlocks = 32;
+
+__global__ void k_place(SceneView v, uint32_t* __restrict__ long_count)
 {
     uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= v.np) return;
+    if (i == 0) *long_count = 0u;  // the long-run list starts empty
     v.perm[v.cell_start[v.key[i]] + v.rank[i]] = (uint32_t)i;
 }
 
-__global__ void k_segsort(SceneView v)
+// rank[x] = final slot of particle x (rank's atomic slots were consumed by k_place).
+__global__ void k_cellrank(SceneView v, uint32_t* __restrict__ long_count)
 {
-    uint32_t key = blockIdx.x * blockDim.x + threadIdx.x;
-    if (key >= v.g.key_space) return;
-    uint32_t b = v.cell_start[key], e = v.cell_start[key + 1];
-    if (e - b < 2) return;
-    uint32_t* a = v.perm;
-    for (uint32_t i = b + 1; i < e; ++i) {  // insertion sort: runs are short (about 8 per cell)
-        uint32_t x = a[i];
-        uint32_t j = i;
-        while (j > b && a[j - 1] > x) {
-            a[j] = a[j - 1];
-            --j;
-        }
-        a[j] = x;
+    uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s >= v.np) return;
+    const uint32_t* __restrict__ perm = v.perm;
+    const uint32_t x = perm[s];
+    const uint32_t key = v.key[x];
+    const uint32_t b = v.cell_start[key], e = v.cell_start[key + 1];
+    if (e - b > kBigCell) {
+        if (s == b) v.cell_count[atomicAdd(long_count, 1u)] = key;
+        return;
     }
+    uint32_t r = 0;
+    for (uint32_t t = b; t < e; ++t) r += perm[t] < x ? 1u : 0u;
+    v.rank[x] = b + r;
+}
+
+// One block per listed long run.  Ascending-only bitonic network (each merge of size k starts with the
+// mirrored comparator i <-> i ^ (k - 1), then half-cleaners of distance k/4 .. 1) over the run padded to
+// a power of two; padded positions count as +infinity, so a pair whose upper element is past the run's
+// end never swaps and is skipped.  Sorted in place in perm, then rank[x] = final slot.
+__global__ void __launch_bounds__(1024) k_bigcell(SceneView v, const uint32_t* __restrict__ long_count)
+{
+    const uint32_t count = *long_count;
+    for (uint32_t li = blockIdx.x; li < count; li += gridDim.x) {
+        const uint32_t key = v.cell_count[li];
+        const uint32_t b = v.cell_start[key], n = v.cell_start[key + 1] - b;
+        uint32_t* a = v.perm + b;
+        uint32_t P = 1;
+        while (P < n) P <<= 1;
+        for (uint32_t k = 2; k <= P; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < (P >> 1); i += blockDim.x) {
+                    const uint32_t lo = (i / j) * 2u * j + (i % j);
+                    const uint32_t hi = j == (k >> 1) ? lo ^ (k - 1u) : lo + j;  // mirrored first, then half-cleaners
+                    if (hi < n) {
+                        const uint32_t x = a[lo], y = a[hi];
+                        if (x > y) {
+                            a[lo] = y;
+                            a[hi] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) v.rank[a[t]] = b + t;
+        __syncthreads();
+    }
+}
+
+__global__ void k_place_final(SceneView v)
+{
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= v.np) return;
+    v.perm[v.rank[i]] = (uint32_t)i;
 }
 
 __global__ void k_gather(SceneView src, SceneView dst, int ncomp)
@@ -163,7 +217,8 @@ __global__ void k_gather(SceneView src, SceneView dst, int ncomp)
 
 }  // namespace
 
-size_t sort_scan_tmp_bytes(uint32_t n) { return ((n + kScanTile - 1) / kScanTile + 1) * sizeof(uint32_t); }
+// block sums (nb words), one spare, and the long-run counter
+size_t sort_scan_tmp_bytes(uint32_t n) { return ((n + kScanTile - 1) / kScanTile + 2) * sizeof(uint32_t); }
 
 cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, size_t scan_tmp_bytes)
 {
@@ -184,9 +239,12 @@ cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, siz
     k_scan_final<<<nb, kScanThreads, 0, st>>>(v.cell_count, K, sums, v.cell_start);
     count_launch(3);
     if (v.np > 0) {
-        k_place<<<pb, T, 0, st>>>(v);
-        k_segsort<<<(K + T - 1) / T, T, 0, st>>>(v);
-        count_launch(2);
+        uint32_t* long_count = sums + nb + 1;
+        k_place<<<pb, T, 0, st>>>(v, long_count);
+        k_cellrank<<<pb, T, 0, st>>>(v, long_count);
+        k_bigcell<<<kBigCellBlocks, 1024, 0, st>>>(v, long_count);
+        k_place_final<<<pb, T, 0, st>>>(v);
+        count_launch(4);
     }
     return cudaGetLastError();
 }

@@ -10,6 +10,7 @@ substep to the end of its last; aggregate particle-steps/s counts every running 
 The reference has no serving layer: it runs one simulator per process frame by frame
 (SimulationRunner::RunSimulation, simulation_runner.cpp:17-55).
 """
+import collections
 import heapq
 import time
 from dataclasses import dataclass, field
@@ -38,6 +39,7 @@ class Job:
     finished_at: float = None
     frames_done: int = 0
     frame_ms: list = field(default_factory=list)
+    seeded: tuple = None        # (pos, vel) once seeded, kept while the job waits for memory
 
 
 def scene_bytes(n, particles, solver):
@@ -63,6 +65,10 @@ class Server:
         self.done = []
         self.batch = None
         self.particle_steps = 0
+        # wall seconds by activity: seeding, scene creation + upload, batch rebuilds, batched substeps
+        # (launch + device time), retirement (read-back + release), idle waits for arrivals
+        self.timing = collections.defaultdict(float)
+        self.rebuilds = 0
 
     def submit(self, job):
         heapq.heappush(self.waiting, (job.arrival, job.job_id, job))
@@ -71,16 +77,23 @@ class Server:
         changed = False
         while self.waiting and self.waiting[0][0] <= now and len(self.running) < self.max_batch:
             _, _, job = self.waiting[0]
-            pos, vel = _abi.seed_regions(job.regions, (job.n,) * 3, seed=job.seed)
+            if job.seeded is None:
+                t = time.perf_counter()
+                job.seeded = _abi.seed_regions(job.regions, (job.n,) * 3, seed=job.seed)
+                self.timing["seed"] += time.perf_counter() - t
+            pos, vel = job.seeded
             need = scene_bytes(job.n, pos.shape[0], job.solver)
             if self.used + need > self.budget:
                 if not self.running:
                     raise MemoryError("job %d needs %d bytes, more than the whole budget" % (job.job_id, need))
                 break  # wait for running jobs to leave
             heapq.heappop(self.waiting)
+            t = time.perf_counter()
             job.scene = Scene((job.n,) * 3, solver=job.solver, max_cfl=1.0, cg_rel_tol=self.cg_rel_tol,
                               device=self.device)
             job.scene.set_particles(pos, vel)
+            job.seeded = None
+            self.timing["create"] += time.perf_counter() - t
             job.particles = pos.shape[0]
             job.admitted_at = now
             job.bytes = need
@@ -92,6 +105,7 @@ class Server:
     def _retire(self, now):
         keep = []
         changed = False
+        t = time.perf_counter()
         for job in self.running:
             if job.frames_done >= job.frames:
                 job.finished_at = now
@@ -104,6 +118,7 @@ class Server:
             else:
                 keep.append(job)
         self.running = keep
+        self.timing["retire"] += time.perf_counter() - t
         return changed
 
     def run(self, on_frame=None):
@@ -117,12 +132,17 @@ class Server:
                 if not self.waiting:
                     break
                 # idle until the next arrival
+                t = time.perf_counter()
                 time.sleep(max(0.0, min(0.01, self.waiting[0][0] - now)))
+                self.timing["idle"] += time.perf_counter() - t
                 continue
             if changed or self.batch is None:
+                t = time.perf_counter()
                 if self.batch is not None:
                     self.batch.close()
                 self.batch = Batch([j.scene for j in self.running])
+                self.rebuilds += 1
+                self.timing["batch_build"] += time.perf_counter() - t
             # one frame of the common substep pattern: jobs share dt and substeps per frame within a batch
             groups = {}
             for j in self.running:
@@ -136,6 +156,7 @@ class Server:
                     b.step(dt, nsub, stats=False)
                     b.close()
                 ms = (time.perf_counter() - f0) * 1e3
+                self.timing["step"] += ms / 1e3
                 for j in jobs:
                     j.frames_done += 1
                     j.frame_ms.append(ms)

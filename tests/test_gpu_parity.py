@@ -52,6 +52,29 @@ def test_sort_bit_exact(n):
     assert np.array_equal(P, pos) and np.array_equal(V, vel)
 
 
+@pytest.mark.parametrize("pile", [(0, 40), (1500, 5), (5000, 2), (70000, 1)])
+def test_sort_bit_exact_piled_cells(pile):
+    """Cells holding hundreds to tens of thousands of particles (particles clamped onto a wall corner pile up
+    at one point): runs below and above the long-run threshold, next to ordinary cells."""
+    count, groups = pile
+    n = (16, 16, 16)
+    rng = np.random.default_rng(11 + count)
+    base = rng.uniform(0.0, 1.0, (20000, 3)).astype(np.float32)
+    corners = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [0.5, 0.0, 0.25], [0.999, 0.03, 0.5],
+                        [0.31, 0.77, 0.0]], dtype=np.float32)
+    piles = [np.repeat(corners[k % len(corners)][None], count + 37 * k, axis=0) for k in range(groups)]
+    pos = np.concatenate([base] + piles)
+    pos = pos[rng.permutation(pos.shape[0])]  # piles interleaved with the rest in particle order
+    g = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0)
+    g.set_particles(pos, np.zeros_like(pos))
+    g.run_stages(1 / 240, fe.STAGE_SORT, fe.STAGE_SORT)
+    keys, perm = g.sort_result()
+    k_ref, p_ref = oracle.sort_keys(pos, n, (0, 0, 0), (1, 1, 1))
+    assert np.array_equal(keys, k_ref)
+    assert np.array_equal(perm, p_ref)
+    g.close()
+
+
 @pytest.mark.parametrize("solver", [fe.PIC, fe.FLIP, fe.APIC])
 @pytest.mark.parametrize("n", [(16, 16, 16), (20, 12, 9)])
 def test_p2g(solver, n):
