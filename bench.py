@@ -319,7 +319,8 @@ def run_served(args):
                               "note": "FIFO over the same arrival trace, one job at a time; frame latency excludes "
                                       "the queueing delay before a job starts"},
             "served_over_one_at_a_time": served / (ps_alone / t_alone), "wall_s": wall,
-            "server_time_s": dict(srv.timing), "batch_rebuilds": srv.rebuilds}
+            "server_time_s": dict(srv.timing), "batch_rebuilds": srv.rebuilds, "scenes_reused": srv.reused,
+            "device_step_ratio": alone_split["step"] / max(srv.timing["step"], 1e-9)}
     print(json.dumps(line), flush=True)
     return 0
 

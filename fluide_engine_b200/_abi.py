@@ -22,12 +22,13 @@ STATUS_NAMES = {0: "FE_OK", 1: "FE_ERR_CUDA", 2: "FE_ERR_BAD_ARG", 3: "FE_ERR_OO
 
 # Every symbol include/fluide_b200.h declares (checked by the CPU test suite).
 EXPORTS = [
-    "fe_scene_desc_default", "fe_scene_create", "fe_scene_destroy", "fe_scene_set_particles", "fe_scene_get_particles",
+    "fe_scene_desc_default", "fe_scene_create", "fe_scene_destroy", "fe_scene_set_particles", "fe_scene_reset",
+    "fe_scene_get_particles",
     "fe_scene_num_particles", "fe_scene_step", "fe_scene_step_profiled", "fe_scene_advance_frame", "fe_scene_cfl", "fe_scene_run_stages",
     "fe_scene_get_grid", "fe_scene_set_grid", "fe_scene_set_pressure", "fe_scene_get_face_markers",
     "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_get_sort", "fe_scene_divergence",
-    "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy",
-    "fe_batch_step", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
+    "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
+    "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
     "fe_abi_version",
 ]
 
@@ -83,6 +84,7 @@ def lib():
     L.fe_scene_create.argtypes = [ctypes.POINTER(SceneDesc), ctypes.POINTER(P)]
     L.fe_scene_destroy.argtypes = [P]
     L.fe_scene_set_particles.argtypes = [P, P, P, P, ctypes.c_uint64]
+    L.fe_scene_reset.argtypes = [P]
     L.fe_scene_get_particles.argtypes = [P, P, P, P, ctypes.c_uint64]
     L.fe_scene_num_particles.argtypes = [P, ctypes.POINTER(ctypes.c_uint64)]
     L.fe_scene_step.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats)]
@@ -105,8 +107,11 @@ def lib():
                                      ctypes.POINTER(StepStats)]
     L.fe_scene_synchronize.argtypes = [P]
     L.fe_batch_create.argtypes = [ctypes.POINTER(P), ctypes.c_int32, ctypes.POINTER(P)]
+    L.fe_batch_set_scenes.argtypes = [P, ctypes.POINTER(P), ctypes.c_int32]
     L.fe_batch_destroy.argtypes = [P]
     L.fe_batch_step.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats)]
+    L.fe_batch_step_profiled.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats),
+                                         ctypes.POINTER(ctypes.c_float)]
     L.fe_kernel_launch_count.restype = ctypes.c_uint64
     L.fe_seed_regions.restype = ctypes.c_uint64
     L.fe_seed_regions.argtypes = [P, ctypes.c_int32, P, P, P, ctypes.c_uint64, P, P, ctypes.c_uint64]

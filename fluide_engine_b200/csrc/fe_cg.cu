@@ -202,7 +202,7 @@ __device__ __forceinline__ float apply_row(const Stencil7& st, int c, uint32_t m
 // The solver body, run by `nblk` blocks of which this is block `blk` (a whole grid for one scene, or a
 // block range of a multi-scene launch, see k_multi_cg); every barrier and reduction spans those blocks.
 __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, const CgParams& prm, const int blk,
-                                        const int nblk)
+                                        const int nblk, int* out_its = nullptr, int* out_fluid = nullptr)
 {
     __shared__ double sh[32 * 4 + 4];
     __shared__ uint32_t s_warp[32];
@@ -397,6 +397,10 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
         }
         if (!grid_sync(w, gen, nblk)) return;
     }
+    if (blk == 0 && threadIdx.x == 0 && out_its) {
+        *out_its = total_it;
+        *out_fluid = F;
+    }
     if (blk == 0 && threadIdx.x == 0 && prm.stats_ring) {
         const unsigned slot = atomicAdd(prm.stats_counter, 1u) % prm.stats_cap;
         fe_step_stats s;
@@ -417,11 +421,11 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
 
 // Many scenes in one cooperative launch: blocks [start[s], start[s+1]) solve scene s with their own barrier
 // and reductions, so scenes iterate independently and concurrently.
-__global__ void __launch_bounds__(kMultiThreads) k_multi_cg(const MultiCgScene* __restrict__ scenes, int S)
+__global__ void __launch_bounds__(kMultiThreads) k_multi_cg(MultiCgScene* __restrict__ scenes, int S)
 {
     int sc = 0;
     while (sc + 1 < S && (int)blockIdx.x >= scenes[sc + 1].block_start) ++sc;
-    const MultiCgScene& m = scenes[sc];
+    MultiCgScene& m = scenes[sc];
     CgParams prm;
     prm.rel_tol = m.rel_tol;
     prm.inner_tol = m.inner_tol;
@@ -430,7 +434,56 @@ __global__ void __launch_bounds__(kMultiThreads) k_multi_cg(const MultiCgScene* 
     prm.stats_ring = m.work.stats;
     prm.stats_counter = m.work.bar + 2;
     prm.stats_cap = 1u << 16;
-    cg_body(m.view, m.work, prm, (int)blockIdx.x - m.block_start, m.block_count);
+    int its = 0, fluid = 0;
+    const int blk = (int)blockIdx.x - m.block_start;
+    cg_body(m.view, m.work, prm, blk, m.block_count, &its, &fluid);
+    if (blk == 0 && threadIdx.x == 0) {  // read by the next solve's k_multi_partition
+        m.last_its = its;
+        m.last_fluid = fluid;
+    }
+}
+
+// One thread splits total_blocks among the scenes before a multi-scene solve: one block each, the rest in
+// proportion to the previous solve's work of the scene (FLUID cells x (inner iterations + 3 residual
+// passes); weight0 before its first solve), leftovers to the heaviest scenes.  Scenes then take about
+// equally long, instead of the scene with the most iterations finishing last on a small share.
+__global__ void k_multi_partition(MultiCgScene* __restrict__ scenes, int S, int total_blocks)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double wsum = 0.0;
+    for (int i = 0; i < S; ++i) {
+        const MultiCgScene& m = scenes[i];
+        const double w = m.last_its >= 0 ? (double)m.last_fluid * (double)(m.last_its + 3) : m.weight0;
+        wsum += fmax(w, 0.0);
+    }
+    const int spare = total_blocks - S;
+    int start = 0, used = 0;
+    for (int i = 0; i < S; ++i) {
+        MultiCgScene& m = scenes[i];
+        const double w = fmax(m.last_its >= 0 ? (double)m.last_fluid * (double)(m.last_its + 3) : m.weight0, 0.0);
+        const int extra = wsum > 0.0 ? (int)floor(spare * (w / wsum)) : spare / S;
+        m.block_count = 1 + extra;
+        used += 1 + extra;
+    }
+    // leftovers (fewer than S) one each to the heaviest scenes, heaviest first
+    for (int left = total_blocks - used; left > 0; --left) {
+        int best = -1;
+        double bw = -1.0;
+        for (int i = 0; i < S; ++i) {
+            const MultiCgScene& m = scenes[i];
+            double w = m.last_its >= 0 ? (double)m.last_fluid * (double)(m.last_its + 3) : m.weight0;
+            w = w / (double)m.block_count;  // work per block: give the block where it is most needed
+            if (w > bw) {
+                bw = w;
+                best = i;
+            }
+        }
+        scenes[best].block_count += 1;
+    }
+    for (int i = 0; i < S; ++i) {
+        scenes[i].block_start = start;
+        start += scenes[i].block_count;
+    }
 }
 
 }  // namespace
@@ -448,8 +501,10 @@ cudaError_t multi_cg_capacity(int device, int* max_blocks, int* threads)
     return cudaSuccess;
 }
 
-cudaError_t launch_multi_cg(const MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st)
+cudaError_t launch_multi_cg(MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st)
 {
+    k_multi_partition<<<1, 32, 0, st>>>(scenes, S, total_blocks);
+    count_launch();
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)total_blocks);
     cfg.blockDim = dim3((unsigned)kMultiThreads);

@@ -181,10 +181,13 @@ struct MultiCgScene {
     CgWork work;
     double rel_tol, inner_tol;
     int max_it, max_refine;
-    int block_start, block_count;
+    int block_start, block_count;  // this scene's block range, re-split before every solve
+    int last_its, last_fluid;      // the previous solve's inner iterations and FLUID cells (-1 / 0: none yet)
+    double weight0;                // expected solve work before any solve has run
 };
 cudaError_t multi_cg_capacity(int device, int* max_blocks, int* threads);
-cudaError_t launch_multi_cg(const MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st);
+// Re-splits total_blocks among the S scenes in proportion to their last solve's work, then solves them.
+cudaError_t launch_multi_cg(MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st);
 cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, double inner_tol, int max_it, int max_refine,
                       cudaStream_t st);
 

@@ -658,6 +658,35 @@ fe_status fe_scene_set_particles(fe_scene* s, const float* pos, const float* vel
     return FE_OK;
 }
 
+fe_status fe_scene_reset(fe_scene* s)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const SceneView& v = s->base;
+    const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
+    const size_t nf = (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz + (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz +
+                      (size_t)v.g.nx * v.g.ny * (v.g.nz + 1);
+    cudaStream_t st = s->stream;
+    // what fe_scene_create zeroes: both velocity buffers, the FLIP snapshot, face markers, cell marks,
+    // pressure (the solver's warm start), right-hand side, sort offsets, solver vectors and scratch
+    FE_CUDA(cudaMemsetAsync(v.u, 0, nf * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(v.u2, 0, nf * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(v.su, 0, nf * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(v.mu, 0, nf, st));
+    FE_CUDA(cudaMemsetAsync(v.marks, 0, nc, st));
+    FE_CUDA(cudaMemsetAsync(v.p, 0, nc * sizeof(double), st));
+    FE_CUDA(cudaMemsetAsync(v.b, 0, nc * sizeof(double), st));
+    FE_CUDA(cudaMemsetAsync(v.cell_start, 0, ((size_t)v.g.key_space + 1) * sizeof(uint32_t), st));
+    FE_CUDA(cudaMemsetAsync(s->cg.r0, 0, nc * 8 * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(s->cg.partial, 0, (16 + (size_t)kMaxCgBlocks) * sizeof(double), st));
+    FE_CUDA(cudaMemsetAsync(s->cg.bar, 0, 8 * sizeof(unsigned), st));
+    FE_CUDA(cudaMemsetAsync(s->cg.err, 0, sizeof(int), st));
+    FE_CUDA(cudaStreamSynchronize(st));
+    s->grid_cur = 0;
+    return FE_OK;
+}
+
 fe_status fe_scene_get_particles(fe_scene* s, float* pos, float* vel, float* C, uint64_t n)
 {
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
@@ -1045,7 +1074,7 @@ fe_status batch_enqueue(fe_batch* b, double dt)
 
 // One batch substep from the scenes' own captured phase graphs (pre-solve and post-solve, captured once
 // per scene and dt) around the multi-scene solve, forked and joined over the scenes' streams.
-fe_status batch_step_scene_graphs(fe_batch* b, double dt)
+fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = nullptr)
 {
     const int S = (int)b->scenes.size();
     for (fe_scene* s : b->scenes) {
@@ -1059,6 +1088,7 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt)
         }
     }
     cudaEvent_t fork0 = b->events[2 * S], fork1 = b->events[2 * S + 1];
+    if (ev) FE_CUDA(cudaEventRecord(ev[0], b->stream));
     FE_CUDA(cudaEventRecord(fork0, b->stream));
     for (int i = 0; i < S; ++i) {
         fe_scene* s = b->scenes[i];
@@ -1068,7 +1098,9 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt)
         FE_CUDA(cudaEventRecord(b->events[2 * i], s->stream));
         FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
     }
+    if (ev) FE_CUDA(cudaEventRecord(ev[1], b->stream));
     FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
+    if (ev) FE_CUDA(cudaEventRecord(ev[2], b->stream));
     FE_CUDA(cudaEventRecord(fork1, b->stream));
     for (int i = 0; i < S; ++i) {
         fe_scene* s = b->scenes[i];
@@ -1080,7 +1112,90 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt)
         s->parity ^= 1;  // the pre-solve graph's sort flipped the particle buffer sets
         s->grid_cur = 0;
     }
+    if (ev) FE_CUDA(cudaEventRecord(ev[3], b->stream));
     b->parity ^= 1;
+    return FE_OK;
+}
+
+fe_status batch_check_scenes(fe_scene* const* scenes, int32_t count)
+{
+    if (!scenes || count < 1) return set_error(FE_ERR_BAD_ARG, "need at least one scene");
+    if (count > kBatchMaxScenes) return set_error(FE_ERR_BAD_ARG, "at most %d scenes per batch", kBatchMaxScenes);
+    for (int i = 0; i < count; ++i) {
+        if (!scenes[i]) return set_error(FE_ERR_BAD_ARG, "null scene %d", i);
+        if (scenes[i]->device != scenes[0]->device)
+            return set_error(FE_ERR_BAD_ARG, "all scenes of a batch must share a device");
+        if (!scenes[i]->have_particles) return set_error(FE_ERR_STATE, "scene %d has no particles", i);
+        for (int j = 0; j < i; ++j)
+            if (scenes[j] == scenes[i]) return set_error(FE_ERR_BAD_ARG, "scene %d appears twice", i);
+    }
+    return FE_OK;
+}
+
+// Sets the batch's scenes: the solver table (in the table allocated once for kBatchMaxScenes entries) with
+// each scene's first block split, join events, and no captured graphs (the next substeps replay the scenes'
+// own phase graphs until the batch graph is captured again).  No device allocation.
+fe_status batch_set_members(fe_batch* b, fe_scene* const* scenes, int32_t count)
+{
+    // Solver blocks per scene before its first solve, proportional to its expected solve work (particle
+    // count as a proxy for its FLUID cells x grid extent, as CG iterations grow with the extent), at least
+    // one block each; before every later solve k_multi_partition re-splits the blocks by the scenes'
+    // measured work.  The multi-scene launch fills the device's co-resident capacity.
+    int capacity = 0, threads = 0;
+    cudaError_t e = multi_cg_capacity(b->device, &capacity, &threads);
+    if (e != cudaSuccess) return cuda_check(e, "multi-scene occupancy");
+    capacity = std::min(capacity, kMaxCgBlocks);
+    if (capacity < count) return set_error(FE_ERR_BAD_ARG, "more scenes than solver blocks (%d)", capacity);
+    std::vector<double> work(count);
+    double total_work = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const GridDims& g = scenes[i]->base.g;
+        // about np / 8 FLUID cells x about 3 x extent inner iterations, the scale of a measured solve's work
+        work[i] = (double)scenes[i]->base.np / 8.0 * 3.0 * (double)std::max(g.nx, std::max(g.ny, g.nz));
+        total_work += work[i];
+    }
+    std::vector<int> nblk(count, 1);
+    int used = count;
+    for (int i = 0; i < count; ++i) {
+        const int extra = (int)std::floor((capacity - count) * work[i] / std::max(total_work, 1.0));
+        nblk[i] += extra;
+        used += extra;
+    }
+    for (int k = 0; used < capacity; ++k, ++used) {  // leftovers to the largest scenes
+        int best = 0;
+        for (int i = 1; i < count; ++i)
+            if (work[i] > work[best]) best = i;
+        nblk[(best + k) % count] += 1;
+    }
+    std::vector<MultiCgScene> table(count);
+    int start = 0;
+    for (int i = 0; i < count; ++i) {
+        fe_scene* s = scenes[i];
+        MultiCgScene& t = table[i];
+        t.view = s->base;
+        t.work = s->cg;
+        t.rel_tol = s->desc.cg_rel_tol;
+        t.inner_tol = s->desc.cg_inner_tol;
+        t.max_it = s->desc.cg_max_it;
+        t.max_refine = s->desc.max_refine;
+        t.block_start = start;
+        t.block_count = nblk[i];
+        t.last_its = -1;  // no solve yet: k_multi_partition uses weight0
+        t.last_fluid = 0;
+        t.weight0 = work[i];
+        start += nblk[i];
+    }
+    batch_drop_graphs(b);
+    while ((int)b->events.size() < 2 * count + 2) {
+        cudaEvent_t ev;
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_check(e, "event");
+        b->events.push_back(ev);
+    }
+    if ((e = cudaMemcpy(b->table, table.data(), count * sizeof(MultiCgScene), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_check(e, "batch setup");
+    b->scenes.assign(scenes, scenes + count);
+    b->total_blocks = start;
+    b->steps_done = 0;
     return FE_OK;
 }
 
@@ -1123,17 +1238,11 @@ extern "C" {
 
 fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out)
 {
-    if (!scenes || !out || count < 1) return set_error(FE_ERR_BAD_ARG, "need at least one scene");
-    if (count > kBatchMaxScenes) return set_error(FE_ERR_BAD_ARG, "at most %d scenes per batch", kBatchMaxScenes);
+    if (!out) return set_error(FE_ERR_BAD_ARG, "null argument");
     *out = nullptr;
+    fe_status vst = batch_check_scenes(scenes, count);
+    if (vst != FE_OK) return vst;
     const int dev = scenes[0]->device;
-    for (int i = 0; i < count; ++i) {
-        if (!scenes[i]) return set_error(FE_ERR_BAD_ARG, "null scene %d", i);
-        if (scenes[i]->device != dev) return set_error(FE_ERR_BAD_ARG, "all scenes of a batch must share a device");
-        if (!scenes[i]->have_particles) return set_error(FE_ERR_STATE, "scene %d has no particles", i);
-        for (int j = 0; j < i; ++j)
-            if (scenes[j] == scenes[i]) return set_error(FE_ERR_BAD_ARG, "scene %d appears twice", i);
-    }
     FE_CUDA(cudaSetDevice(dev));
     fe_batch* b = new (std::nothrow) fe_batch();
     if (!b) return set_error(FE_ERR_OOM, "host allocation failed");
@@ -1146,55 +1255,25 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
         delete b;
         return st;
     };
-    // Solver blocks per scene, proportional to its particle count (a proxy for its FLUID cells), at least
-    // one each; the multi-scene launch fills the device's co-resident capacity.
-    int capacity = 0, threads = 0;
-    cudaError_t e = multi_cg_capacity(dev, &capacity, &threads);
-    if (e != cudaSuccess) return fail(cuda_check(e, "multi-scene occupancy"));
-    capacity = std::min(capacity, kMaxCgBlocks);
-    if (capacity < count) return fail(set_error(FE_ERR_BAD_ARG, "more scenes than solver blocks (%d)", capacity));
-    double total_np = 0.0;
-    for (int i = 0; i < count; ++i) total_np += (double)scenes[i]->base.np;
-    std::vector<int> nblk(count, 1);
-    int used = count;
-    for (int i = 0; i < count; ++i) {
-        const int extra = (int)std::floor((capacity - count) * (double)scenes[i]->base.np / std::max(total_np, 1.0));
-        nblk[i] += extra;
-        used += extra;
-    }
-    for (int k = 0; used < capacity; ++k, ++used) {  // leftovers to the largest scenes
-        int best = 0;
-        for (int i = 1; i < count; ++i)
-            if (scenes[i]->base.np > scenes[best]->base.np) best = i;
-        nblk[(best + k) % count] += 1;
-    }
-    std::vector<MultiCgScene> table(count);
-    int start = 0;
-    for (int i = 0; i < count; ++i) {
-        fe_scene* s = scenes[i];
-        MultiCgScene& t = table[i];
-        t.view = s->base;
-        t.work = s->cg;
-        t.rel_tol = s->desc.cg_rel_tol;
-        t.inner_tol = s->desc.cg_inner_tol;
-        t.max_it = s->desc.cg_max_it;
-        t.max_refine = s->desc.max_refine;
-        t.block_start = start;
-        t.block_count = nblk[i];
-        start += nblk[i];
-    }
-    b->total_blocks = start;
-    e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_check(e, "stream create"));
-    b->events.resize(2 * count + 2);
-    for (auto& ev : b->events)
-        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_check(e, "event"));
-    if ((e = dalloc(b->allocs, &b->table, count)) != cudaSuccess) return fail(cuda_check(e, "batch allocation"));
-    if ((e = cudaMemcpy(b->table, table.data(), count * sizeof(MultiCgScene), cudaMemcpyHostToDevice)) != cudaSuccess)
-        return fail(cuda_check(e, "batch setup"));
+    if ((e = dalloc(b->allocs, &b->table, kBatchMaxScenes)) != cudaSuccess) return fail(cuda_check(e, "batch allocation"));
+    fe_status st = batch_set_members(b, scenes, count);
+    if (st != FE_OK) return fail(st);
     // no host synchronisation: a scene's earlier work precedes the batch's work in its own stream order
     *out = b;
     return FE_OK;
+}
+
+fe_status fe_batch_set_scenes(fe_batch* b, fe_scene* const* scenes, int32_t count)
+{
+    if (!b) return set_error(FE_ERR_BAD_ARG, "null batch");
+    fe_status st = batch_check_scenes(scenes, count);
+    if (st != FE_OK) return st;
+    if (scenes[0]->device != b->device) return set_error(FE_ERR_BAD_ARG, "all scenes of a batch must share a device");
+    FE_CUDA(cudaSetDevice(b->device));
+    FE_CUDA(cudaStreamSynchronize(b->stream));  // no solve of the old membership may still read the table
+    return batch_set_members(b, scenes, count);
 }
 
 fe_status fe_batch_destroy(fe_batch* b)
@@ -1207,6 +1286,45 @@ fe_status fe_batch_destroy(fe_batch* b)
     for (auto e : b->events) cudaEventDestroy(e);
     cudaStreamDestroy(b->stream);
     delete b;
+    return FE_OK;
+}
+
+fe_status fe_batch_step_profiled(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats, float* phase_ms)
+{
+    if (!b || !phase_ms) return set_error(FE_ERR_BAD_ARG, "null argument");
+    if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
+    const int S = (int)b->scenes.size();
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (fe_scene* s : b->scenes) locks.emplace_back(s->mu);
+    FE_CUDA(cudaSetDevice(b->device));
+    if (stats)
+        for (fe_scene* s : b->scenes) FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), b->stream));
+    std::vector<cudaEvent_t> ev((size_t)nsub * 4);
+    for (auto& e : ev) FE_CUDA(cudaEventCreate(&e));
+    fe_status st = FE_OK;
+    for (int it = 0; it < nsub && st == FE_OK; ++it) {
+        st = batch_step_scene_graphs(b, dt, &ev[(size_t)it * 4]);
+        ++b->steps_done;
+    }
+    if (st == FE_OK) {
+        cudaError_t e = cudaStreamSynchronize(b->stream);
+        for (int i = 0; i < nsub && e == cudaSuccess; ++i)
+            for (int ph = 0; ph < 3 && e == cudaSuccess; ++ph)
+                e = cudaEventElapsedTime(&phase_ms[i * 3 + ph], ev[(size_t)i * 4 + ph], ev[(size_t)i * 4 + ph + 1]);
+        st = cuda_check(e, "phase timing");
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (st != FE_OK) return st;
+    for (fe_scene* s : b->scenes) {
+        fe_status cst = check_device_error(s);
+        if (cst != FE_OK) return cst;
+    }
+    if (stats && nsub > 0) {
+        const int cnt = std::min(nsub, 1 << 16);
+        for (int i = 0; i < S; ++i)
+            FE_CUDA(cudaMemcpy(stats + (size_t)i * nsub, b->scenes[i]->stats_ring, cnt * sizeof(fe_step_stats),
+                               cudaMemcpyDeviceToHost));
+    }
     return FE_OK;
 }
 

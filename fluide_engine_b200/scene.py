@@ -60,6 +60,10 @@ class Scene:
         C = np.ascontiguousarray(C, dtype=np.float32) if isinstance(C, np.ndarray) else C
         check(self._L.fe_scene_set_particles(self._h, ptr(pos), ptr(vel), ptr(C), int(pos.shape[0])))
 
+    def reset(self):
+        """Back to the freshly created state (grid, pressure warm start, solver scratch), keeping allocations."""
+        check(self._L.fe_scene_reset(self._h))
+
     def num_particles(self):
         n = ctypes.c_uint64()
         check(self._L.fe_scene_num_particles(self._h, ctypes.byref(n)))
@@ -175,6 +179,13 @@ class Batch:
         check(self._L.fe_batch_create(arr, len(self.scenes), ctypes.byref(h)))
         self._h = h
 
+    def set_scenes(self, scenes):
+        """Changes the batch's scenes in place (no device allocation)."""
+        scenes = list(scenes)
+        arr = (ctypes.c_void_p * len(scenes))(*[s.handle.value for s in scenes])
+        check(self._L.fe_batch_set_scenes(self._h, arr, len(scenes)))
+        self.scenes = scenes
+
     def step(self, dt, nsub=1, stats=True):
         S = len(self.scenes)
         if stats:
@@ -183,6 +194,16 @@ class Batch:
             return [[arr[i * nsub + k].as_dict() for k in range(nsub)] for i in range(S)]
         check(self._L.fe_batch_step(self._h, dt, nsub, None))
         return None
+
+    def step_profiled(self, dt, nsub):
+        """Like step(), plus per-substep phase times in ms: array [nsub, 3] = (all pre-solve, multi-scene solve,
+        all post-solve); returns (stats per scene per substep, times)."""
+        S = len(self.scenes)
+        arr = (_abi.StepStats * max(1, S * nsub))()
+        ms = np.zeros((max(nsub, 1), 3), dtype=np.float32)
+        check(self._L.fe_batch_step_profiled(self._h, dt, nsub, arr,
+                                             ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return [[arr[i * nsub + k].as_dict() for k in range(nsub)] for i in range(S)], ms[:nsub]
 
     def close(self):
         if getattr(self, "_h", None):

@@ -97,6 +97,13 @@ fe_status fe_scene_destroy(fe_scene* s);
  * SetVectorValues (particle_systems/particle_system.cpp:36-44,97-107) and APICSimulator::_cX.. */
 fe_status fe_scene_set_particles(fe_scene* s, const float* pos, const float* vel, const float* C, uint64_t n);
 
+/* Returns the scene to the state fe_scene_create leaves it in -- velocity buffers, FLIP snapshot, face and
+ * cell markers, pressure (the next solve's warm start, linear_system.cpp:13-18), right-hand side and solver
+ * scratch zeroed -- while keeping its allocations, particles and captured graphs, so a server can reuse the
+ * scene for a new job of the same grid and solver without allocating.  No reference counterpart (a
+ * reference simulator lives for one run). */
+fe_status fe_scene_reset(fe_scene* s);
+
 /* Copies the particles out in the order they were set (ParticleSystem::GetVectorValues,
  * particle_systems/particle_system.cpp:133-141).  Any pointer may be NULL. */
 fe_status fe_scene_get_particles(fe_scene* s, float* pos, float* vel, float* C, uint64_t n);
@@ -165,7 +172,7 @@ fe_status fe_scene_synchronize(fe_scene* s);
 
 /* Batches: many independent scenes (up to 64, one device) advanced together.  Per substep every scene's
  * pre-solve phase runs on its own stream, ONE cooperative launch solves all scenes' pressure systems (each
- * scene on its own block range, sized by its particle count, with its own grid barrier, so the scenes
+ * scene on its own block range, sized by particle count x grid extent, with its own grid barrier, so the scenes
  * iterate independently and concurrently), and every scene's post-solve phase runs on its own stream; the
  * batch substep is one captured CUDA graph.  Results equal each scene stepped alone (same algorithm, each
  * scene's own tolerances).  No reference counterpart: the reference runs one simulator per process
@@ -173,8 +180,16 @@ fe_status fe_scene_synchronize(fe_scene* s);
 typedef struct fe_batch fe_batch;
 fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out);
 fe_status fe_batch_destroy(fe_batch* b);
+/* Replaces the batch's scenes (same rules as fe_batch_create) without allocating or freeing device memory:
+ * a server whose running set changes between frames keeps one batch; the batch graph is captured again
+ * once the new membership has run a few substeps.  Waits for the batch's earlier work to finish. */
+fe_status fe_batch_set_scenes(fe_batch* b, fe_scene* const* scenes, int32_t count);
 /* nsub substeps of dt for every scene; stats (NULL or count * nsub entries, scene-major) as fe_scene_step. */
 fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats);
+/* fe_batch_step with per-substep device timing of the batch's three phases (all scenes' pre-solve, the
+ * multi-scene solve, all scenes' post-solve; events on the batch stream between the joins), replaying the
+ * scenes' own phase graphs around the solve launch; phase_ms receives nsub * 3 floats; synchronises. */
+fe_status fe_batch_step_profiled(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats, float* phase_ms);
 
 /* Number of kernels the library launched since load (counts graph-launched kernels too). */
 uint64_t fe_kernel_launch_count(void);

@@ -97,3 +97,78 @@ def test_server_admission_respects_budget():
         srv.submit(j)
     srv.run(on_frame=lambda jobs_, ms: peak.append(len(srv.running)))
     assert max(peak) <= 2 and len(srv.done) == 4
+
+
+def test_scene_reset_matches_fresh_scene():
+    """A scene that ran one job, reset and given new particles, steps like a freshly created scene."""
+    dt = 1.0 / 240.0
+    used = make(SPECS[1], 3)
+    used.step(dt, 6)  # leaves pressure (warm start), grid and solver state behind
+    used.reset()
+    fresh = make(SPECS[1], 9)
+    pos, vel, _ = fresh.particles()
+    used.set_particles(pos, vel)
+    p_used = used.grid()[3]
+    assert not np.any(p_used)  # the warm start is gone
+    st_u = used.step(dt, 3)
+    st_f = fresh.step(dt, 3)
+    assert [x["fluid_cells"] for x in st_u] == [x["fluid_cells"] for x in st_f]
+    Pu, Vu, _ = used.particles()
+    Pf, Vf, _ = fresh.particles()
+    assert rel_l2(Pu, Pf) < 1e-5
+    assert rel_l2(Vu, Vf) < 1e-4
+
+
+def test_batch_step_profiled_phases():
+    dt = 1.0 / 240.0
+    scenes = [make(sp, i) for i, sp in enumerate(SPECS[:3])]
+    b = fe.Batch(scenes)
+    stats, ms = b.step_profiled(dt, 3)
+    b.close()
+    assert ms.shape == (3, 3) and np.all(ms > 0)
+    assert len(stats) == 3 and all(len(s) == 3 for s in stats)
+    assert all(x["converged"] == 1 for s in stats for x in s)
+
+
+def test_server_reuses_scenes_and_matches_alone():
+    """Jobs of one shape served one after another (one slot): later jobs run on reset, reused scenes."""
+    regions = [dict(kind=0, lo=(0.0, 0.0, 0.0), hi=(0.4, 0.5, 0.6))]
+    jobs = [serving.Job(job_id=k, n=24, solver=fe.APIC, regions=regions, frames=2, substeps_per_frame=2,
+                        dt=1.0 / 240.0, arrival=0.0, seed=20 + k) for k in range(3)]
+    srv = serving.Server(hbm_budget_bytes=2 << 30, max_batch=1)
+    for j in jobs:
+        srv.submit(j)
+    srv.run()
+    assert len(srv.done) == 3 and srv.reused == 2
+    for j in srv.done:
+        pos, vel = fe.seed_regions(j.regions, (j.n,) * 3, seed=j.seed)
+        s = fe.Scene((j.n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6)
+        s.set_particles(pos, vel)
+        s.step(j.dt, j.frames * j.substeps_per_frame)
+        P, V, C = s.particles()
+        assert rel_l2(j.final[0], P) < 1e-5
+        assert rel_l2(j.final[1], V) < 1e-4
+        s.close()
+
+
+def test_batch_membership_change_matches_alone():
+    """One batch whose scenes change between substeps (fe_batch_set_scenes): every scene still matches the
+    same scene stepped alone for the same number of substeps."""
+    dt = 1.0 / 240.0
+    a, b, c = (make(SPECS[k], 30 + k) for k in (0, 1, 2))
+    ra, rb, rc = (make(SPECS[k], 30 + k) for k in (0, 1, 2))
+    batch = fe.Batch([a, b])
+    batch.step(dt, 3)
+    batch.set_scenes([b, c])       # a leaves, c joins
+    batch.step(dt, 10)             # long enough for the batch graph to be captured with the new members
+    batch.set_scenes([c, a, b])    # a returns
+    batch.step(dt, 2)
+    batch.close()
+    ra.step(dt, 5)
+    rb.step(dt, 15)
+    rc.step(dt, 12)
+    for m, r in ((a, ra), (b, rb), (c, rc)):
+        Pm, Vm, _ = m.particles()
+        Pr, Vr, _ = r.particles()
+        assert rel_l2(Pm, Pr) < 1e-5
+        assert rel_l2(Vm, Vr) < 1e-4
