@@ -32,6 +32,7 @@ namespace {
 
 constexpr int kCgThreads = 1024;
 constexpr int kMultiThreads = 256;
+constexpr int kListCache = 8192;  // FLUID-list entries cached in shared memory per block (32 KB)
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
 struct CgParams {
@@ -46,27 +47,29 @@ struct CgParams {
 // order across the wrap.
 __device__ __forceinline__ unsigned next_gen(unsigned g) { return g + 1u == 65535u ? 0u : g + 1u; }
 
-// Grid-wide barrier.  bar[0] packs the arrival count (low 16 bits) and the generation (high 16 bits), so
-// one acq_rel fetch_add both arrives and learns the generation; the last arriver resets the count and
-// bumps the generation with a release store, the others spin (bounded) with acquire loads.  The
-// release/acquire pair at device scope, with the __syncthreads on either side, orders every thread's
-// memory traffic of the block across the barrier.  Returns false when the wait gave up.
-// The last arriver also zeroes the totals slot of the next generation (see grid_reduce).
-__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals)
+// Grid-wide barrier on two words in different 128-byte lines: bar[0] counts arrivals (one acq_rel
+// fetch_add per block), bar[32] holds the generation.  The last arriver resets the count, zeroes the totals
+// slot of the next generation and bumps the generation with a release store; the others poll the
+// generation (bounded) with acquire loads, away from the line the arrivals hit.  The release/acquire pair at
+// device scope, with the __syncthreads on either side, orders every thread's memory traffic of the block
+// across the barrier.  `gen` is the generation this barrier started in (tracked by thread 0).  Returns
+// false when the wait gave up.
+__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals, unsigned gen)
 {
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> word(bar[0]);
-    const unsigned old = word.fetch_add(1u, cuda::memory_order_acq_rel);
-    const unsigned gen = old >> 16;
-    if ((old & 0xffffu) == nblocks - 1) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
+    const unsigned old = count.fetch_add(1u, cuda::memory_order_acq_rel);
+    if (old == nblocks - 1) {
         double* next = totals + 4 * (next_gen(gen) % 3u);
 #pragma unroll
         for (int k = 0; k < 4; ++k) next[k] = 0.0;
-        word.store(next_gen(gen) << 16, cuda::memory_order_release);
+        count.store(0u, cuda::memory_order_relaxed);
+        genw.store(next_gen(gen), cuda::memory_order_release);
         return true;
     }
     cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
     unsigned long long spins = 0;
-    while ((word.load(cuda::memory_order_acquire) >> 16) == gen) {
+    while (genw.load(cuda::memory_order_acquire) == gen) {
         if (++spins > kSpinLimit) {
             e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
             return false;
@@ -80,7 +83,7 @@ __device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nb
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        bar_arrive_wait(w.bar, w.err, (unsigned)nblk, w.partial);
+        bar_arrive_wait(w.bar, w.err, (unsigned)nblk, w.partial, gen);
         gen = next_gen(gen);
     }
     __syncthreads();
@@ -92,7 +95,9 @@ __device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nb
 // its release) and arrives; after the barrier it reads the totals once.  Three total slots rotate: the
 // last arriver of barrier k zeroes slot k+1 before releasing it, and slot k is read only until the
 // readers arrive at barrier k+1.  All blocks read the same final totals, so their branch decisions
-// agree (the summation order, and hence the last bits, can vary from run to run).
+// agree (the summation order, and hence the last bits, can vary from run to run).  (Per-block slots summed
+// by the last arriver avoid the floating-point atomics but put one more L2 round trip on the critical
+// path, which measured slower.)
 template <int N>
 __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w, unsigned& gen,
                                             int nblk)
@@ -122,33 +127,11 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] 
         if (lane == 0) {
             // slot of this barrier: generation modulo 3; thread 0 tracks the generation itself (it takes
             // part in every barrier), which saves a load round trip per barrier
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> word(w.bar[0]);
             double* totals = w.partial;  // [3][4]
             double* slot = totals + 4 * (gen % 3u);  // zeroed by the release of this generation
 #pragma unroll
             for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
-            const unsigned old = word.fetch_add(1u, cuda::memory_order_acq_rel);
-            bool ok = true;
-            if ((old & 0xffffu) == (unsigned)nblk - 1) {
-                double* next = totals + 4 * (next_gen(old >> 16) % 3u);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) next[k] = 0.0;
-                word.store(next_gen(old >> 16) << 16, cuda::memory_order_release);
-            } else {
-                cuda::atomic_ref<int, cuda::thread_scope_device> e(*w.err);
-                unsigned long long spins = 0;
-                while ((word.load(cuda::memory_order_acquire) >> 16) == (old >> 16)) {
-                    if (++spins > kSpinLimit) {
-                        e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
-                        ok = false;
-                        break;
-                    }
-                    if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) {
-                        ok = false;
-                        break;
-                    }
-                }
-            }
+            const bool ok = bar_arrive_wait(w.bar, w.err, (unsigned)nblk, totals, gen);
             gen = next_gen(gen);
             if (ok)
 #pragma unroll
@@ -206,6 +189,10 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
 {
     __shared__ double sh[32 * 4 + 4];
     __shared__ uint32_t s_warp[32];
+    // the FLUID list does not change during a solve: each thread keeps its first list entries in shared
+    // memory (entry k of thread t at s_list[k * blockDim.x + t]), which takes one dependent L2 round trip
+    // out of every pass
+    __shared__ uint32_t s_list[kListCache];
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
     const int sxy = nx * ny;
     const int nc = sxy * nz;
@@ -230,7 +217,7 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
 
     // barrier generation as of this launch (thread 0 keeps it from here on)
     unsigned gen = 0;
-    if (threadIdx.x == 0) gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[0]).load(cuda::memory_order_relaxed) >> 16;
+    if (threadIdx.x == 0) gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[32]).load(cuda::memory_order_relaxed);
 
     // ---- setup: zero non-FLUID entries, ||b||^2, per-block FLUID counts over the block's cell range
     const int chunk = (nc + nblk - 1) / nblk;
@@ -286,6 +273,12 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
         __syncthreads();
     }
     if (!grid_sync(w, gen, nblk)) return;
+    const int kc = kListCache / (int)blockDim.x;
+    {
+        int k = 0;
+        for (int e = tid; e < F && k < kc; e += T, ++k) s_list[k * blockDim.x + threadIdx.x] = __ldcg(list + e);
+    }
+    auto entry = [&](int k, int e) -> uint32_t { return k < kc ? s_list[k * blockDim.x + threadIdx.x] : list[e]; };
     const double target = prm.rel_tol * bnorm;
     if (bnorm == 0.0) {
         for (int e = tid; e < F; e += T) p64[list[e] >> 6] = 0.0;
@@ -298,8 +291,8 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
     while (!converged) {
         // ---- outer residual r = b - A p in FP64, stored in FP32 for the inner solve
         double racc[1] = {0.0};
-        for (int e = tid; e < F; e += T) {
-            const uint32_t ent = list[e];
+        for (int e = tid, k = 0; e < F; e += T, ++k) {
+            const uint32_t ent = entry(k, e);
             const int c = (int)(ent >> 6);
             const uint32_t m = ent & 63u;
             const double pc = p64[c];
@@ -326,8 +319,8 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
 
         // ---- inner Chronopoulos-Gear CG on A e = r; w0 = A r0 and the first dot products
         double d0[2] = {0.0, 0.0};
-        for (int e = tid; e < F; e += T) {
-            const uint32_t ent = list[e];
+        for (int e = tid, k = 0; e < F; e += T, ++k) {
+            const uint32_t ent = entry(k, e);
             const int c = (int)(ent >> 6);
             const float* __restrict__ r0 = R[0];
             const float wc = apply_row(st, c, ent & 63u, [&](int q) { return r0[q]; });
@@ -364,8 +357,8 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
             float* __restrict__ wn = W[cur ^ 1];
             float* __restrict__ sn = S[cur ^ 1];
             double dd[2] = {0.0, 0.0};
-            for (int e = tid; e < F; e += T) {
-                const uint32_t ent = list[e];
+            for (int e = tid, k = 0; e < F; e += T, ++k) {
+                const uint32_t ent = entry(k, e);
                 const int c = (int)(ent >> 6);
                 // r'(q) = r(q) - alpha (w(q) + beta s(q)) for this cell and its neighbours
                 auto rnew = [&](int q) { return r[q] - af * (wv[q] + bf * s[q]); };
@@ -391,8 +384,8 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
             if (gamma <= stop) break;
         }
         // ---- p += e (FP64); the next residual pass reads neighbours' p, hence the barrier
-        for (int e = tid; e < F; e += T) {
-            const int c = (int)(list[e] >> 6);
+        for (int e = tid, k = 0; e < F; e += T, ++k) {
+            const int c = (int)(entry(k, e) >> 6);
             p64[c] += (double)X[c];
         }
         if (!grid_sync(w, gen, nblk)) return;

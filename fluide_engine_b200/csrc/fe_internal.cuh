@@ -20,6 +20,12 @@ namespace fe {
 
 constexpr int kMaxRefineDefault = 12;
 constexpr int kMaxCgBlocks = 4096;  // solver blocks one scene can be given (sizes its partial-sum buffer)
+// Grid-barrier words of one solver: [0] arrival count, [2] statistics counter, [32] generation (its own
+// 128-byte line, so the blocks polling it do not contend with the arrivals on [0]).
+constexpr int kCgBarWords = 64;
+// Doubles of one solver's partial buffer for up to max_blocks blocks: the reduction totals slots, then the
+// per-block FLUID counts of the solver's setup.
+constexpr size_t cg_partial_doubles(size_t max_blocks) { return 16 + max_blocks; }
 constexpr int kBatchMaxScenes = 64;
 
 struct GridDims {
@@ -166,8 +172,8 @@ cudaError_t launch_scatter_out(const SceneView& v, float* pos, float* vel, float
 struct CgWork {
     float *r0, *r1, *w0, *w1, *s0, *s1, *pv, *x;  // FP32 inner-CG vectors (r, w, s ping-pong)
     uint32_t* list;         // compacted FLUID cells: (cell << 6) | in-domain neighbour mask
-    double* partial;        // [blocks][4]
-    unsigned* bar;          // [0] count, [1] generation
+    double* partial;        // [0, 12) three rotating reduction totals slots, [16, 16 + max blocks) FLUID counts
+    unsigned* bar;          // kCgBarWords barrier words
     int* err;
     fe_step_stats* stats;   // device
     int blocks, threads;

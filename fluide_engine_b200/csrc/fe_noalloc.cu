@@ -35,8 +35,8 @@ constexpr size_t kOffB = 0;                                                     
 constexpr size_t kOffVec = align256(kOffB + kMaxCells * sizeof(double));          // 8 FP32 CG vectors
 constexpr size_t kOffList = align256(kOffVec + 8 * kMaxCells * sizeof(float));     // compacted FLUID list
 constexpr size_t kOffPartial = align256(kOffList + kMaxCells * sizeof(uint32_t));  // partials + totals
-constexpr size_t kOffBar = align256(kOffPartial + (4 * kMaxBlocks + 4) * sizeof(double));
-constexpr size_t kOffErr = align256(kOffBar + 8 * sizeof(unsigned));
+constexpr size_t kOffBar = align256(kOffPartial + cg_partial_doubles(kMaxBlocks) * sizeof(double));
+constexpr size_t kOffErr = align256(kOffBar + kCgBarWords * sizeof(unsigned));
 constexpr size_t kOffStats = align256(kOffErr + sizeof(int));
 constexpr size_t kScratchBytes = align256(kOffStats + kStatsRing * sizeof(fe_step_stats));
 
@@ -122,8 +122,9 @@ extern "C" fe_status fe_project_noalloc(const int32_t n[3], const double h[3], c
     view.p = p;
     view.b = (double*)(base + kOffB);
 
-    // barrier words, reduction totals slots, error flag and statistics counter start at zero on every call
-    FE_CUDA(cudaMemsetAsync(work.bar, 0, 8 * sizeof(unsigned), s));
+    // barrier words (arrival count, generation, statistics counter), reduction totals slots and the error
+    // flag start at zero on every call
+    FE_CUDA(cudaMemsetAsync(work.bar, 0, kCgBarWords * sizeof(unsigned), s));
     FE_CUDA(cudaMemsetAsync(work.partial, 0, 12 * sizeof(double), s));
     FE_CUDA(cudaMemsetAsync(work.err, 0, sizeof(int), s));
     FE_CUDA(launch_rhs(view, s));

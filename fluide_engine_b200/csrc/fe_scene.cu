@@ -225,10 +225,10 @@ fe_status alloc_grid(fe_scene* s)
     FE_CUDA(dalloc(L, &w.list, nc));
     FE_CUDA(cg_prepare(w, s->device));
     // 3 rotating totals slots (12 doubles) + per-block FLUID counts of up to kMaxCgBlocks solver blocks
-    FE_CUDA(dalloc(L, &w.partial, 16 + (size_t)kMaxCgBlocks));
-    FE_CUDA(cudaMemset(w.partial, 0, (16 + (size_t)kMaxCgBlocks) * sizeof(double)));
-    FE_CUDA(dalloc(L, &w.bar, 8));
-    FE_CUDA(cudaMemset(w.bar, 0, 8 * sizeof(unsigned)));
+    FE_CUDA(dalloc(L, &w.partial, cg_partial_doubles(kMaxCgBlocks)));
+    FE_CUDA(cudaMemset(w.partial, 0, cg_partial_doubles(kMaxCgBlocks) * sizeof(double)));
+    FE_CUDA(dalloc(L, &w.bar, kCgBarWords));
+    FE_CUDA(cudaMemset(w.bar, 0, kCgBarWords * sizeof(unsigned)));
     FE_CUDA(dalloc(L, &w.err, 1));
     FE_CUDA(cudaMemset(w.err, 0, sizeof(int)));
     FE_CUDA(dalloc(L, &s->stats_ring, (size_t)1 << 16));
@@ -415,7 +415,7 @@ fe_status check_device_error(fe_scene* s)
     FE_CUDA(cudaStreamSynchronize(s->stream));
     if (err) {
         cudaMemsetAsync(s->cg.err, 0, sizeof(int), s->stream);
-        cudaMemsetAsync(s->cg.bar, 0, 2 * sizeof(unsigned), s->stream);
+        cudaMemsetAsync(s->cg.bar, 0, kCgBarWords * sizeof(unsigned), s->stream);  // count and generation
         cudaMemsetAsync(s->cg.partial, 0, 12 * sizeof(double), s->stream);  // totals slots restart at zero
         cudaStreamSynchronize(s->stream);
         return set_error((fe_status)err, "pressure solve: grid barrier wait exceeded its limit");
@@ -679,8 +679,8 @@ fe_status fe_scene_reset(fe_scene* s)
     FE_CUDA(cudaMemsetAsync(v.b, 0, nc * sizeof(double), st));
     FE_CUDA(cudaMemsetAsync(v.cell_start, 0, ((size_t)v.g.key_space + 1) * sizeof(uint32_t), st));
     FE_CUDA(cudaMemsetAsync(s->cg.r0, 0, nc * 8 * sizeof(float), st));
-    FE_CUDA(cudaMemsetAsync(s->cg.partial, 0, (16 + (size_t)kMaxCgBlocks) * sizeof(double), st));
-    FE_CUDA(cudaMemsetAsync(s->cg.bar, 0, 8 * sizeof(unsigned), st));
+    FE_CUDA(cudaMemsetAsync(s->cg.partial, 0, cg_partial_doubles(kMaxCgBlocks) * sizeof(double), st));
+    FE_CUDA(cudaMemsetAsync(s->cg.bar, 0, kCgBarWords * sizeof(unsigned), st));
     FE_CUDA(cudaMemsetAsync(s->cg.err, 0, sizeof(int), st));
     FE_CUDA(cudaStreamSynchronize(st));
     s->grid_cur = 0;
