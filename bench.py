@@ -176,6 +176,77 @@ def run_reference_arm(args):
     return 0
 
 
+def run_pool(args):
+    """APIC sphere drop into a pool on a 256^3 grid (about 42M particles): the pool fills y < 0.3 and a sphere
+    of radius 0.15 at (0.5, 0.7, 0.5) starts at velocity (0, -2, 0); 8 jittered particles per cell (seed 1),
+    dt = 1/480, FP32 inner CG inside FP64 refinement to relative residual 1e-8.  The largest single-scene
+    configuration: particle state (about 5 GB) and the solver's vectors exceed the 126 MB L2."""
+    import numpy as np
+    import torch
+
+    import fluide_engine_b200 as fe
+
+    torch.cuda.set_device(0)
+    n = args.n or 256
+    regions = [dict(kind=0, lo=(0.0, 0.0, 0.0), hi=(1.0, 0.3, 1.0)),
+               dict(kind=1, lo=(0.5, 0.7, 0.5), hi=(0.15,), vel=(0.0, -2.0, 0.0))]
+    t_seed = time.perf_counter()
+    pos, vel = fe.seed_regions(regions, (n, n, n), seed=1)
+    t_seed = time.perf_counter() - t_seed
+    N = pos.shape[0]
+    dt = 1.0 / 480.0
+    scene = fe.Scene((n, n, n), solver=fe.APIC, max_cfl=1.0, cg_rel_tol=1e-8, cg_max_it=4000, max_refine=24)
+    stream = torch.cuda.Stream()
+    scene.set_stream(stream.cuda_stream)
+    scene.set_particles(pos, vel)
+    del pos, vel
+    scene.step(dt, args.warmup)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    launches0 = fe.kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    stats, phase_ms = scene.step_profiled(dt, args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = fe.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    value = N * args.steps / (ms / 1e3)
+    cg_ms = phase_ms[:, 1].astype(np.float64)
+    fluid = np.array([s["fluid_cells"] for s in stats], dtype=np.float64)
+    its = np.array([s["cg_iterations"] for s in stats], dtype=np.float64)
+    refs = np.array([s["refinements"] for s in stats], dtype=np.float64)
+    alg_bytes = fluid * (its * 41.0 + (refs + 1.0) * 45.0)
+    peak, peak_kind = peaks()
+    achieved = alg_bytes.sum() / (cg_ms.sum() / 1e3) / 1e9
+    phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded analytic scene)", "workload_kind": "pool256",
+        "config": {"workload": "APIC sphere drop into a pool %d^3, pool y<0.3 + sphere r=0.15 at (0.5,0.7,0.5) "
+                               "v=(0,-2,0), 8 particles/cell (seed 1), dt=1/480, FP32 CG in FP64 refinement to "
+                               "rel 1e-8" % n, "grid": [n, n, n], "particles": N, "solver": "APIC",
+                   "substeps_timed": args.steps, "warmup": args.warmup, "seeding_s": t_seed,
+                   "l2": "working set > 126 MB L2 (particles alone %.0f MB); no flush" % (N * 60 / 1e6)},
+        "roofline": {"bound": "hbm", "kernel": "k_cg (persistent FP32 CG + FP64 refinement, one launch/substep)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": float(alg_bytes.mean())},
+        "phases": {"share": {"pre_solve": phase_share[0], "cg_solve": phase_share[1], "post_solve": phase_share[2]},
+                   "ms_per_substep": (phase_ms.mean(axis=0)).tolist()},
+        "solver": {"cg_iterations_mean": float(its.mean()), "cg_iterations_max": float(its.max()),
+                   "refinements_mean": float(refs.mean()),
+                   "rel_residual_max": float(max(s["rel_residual"] for s in stats)),
+                   "converged_all": bool(all(s["converged"] for s in stats)), "fluid_cells_mean": float(fluid.mean())},
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    scene.close()
+    return 0
+
+
 def run_batched(args):
     """Batched independent scenes vs the same scenes one at a time on the plain single-scene path.
 
@@ -331,12 +402,12 @@ def main():
     ap.add_argument("--steps", type=int, default=240)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--n", type=int, default=None, help="grid cells per axis (default 128; 256 for pool256)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--ref-steps", type=int, default=1, help="substeps of the CPU reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
-    ap.add_argument("--workload", default="single", choices=["single", "batched", "served"])
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "served", "pool256"])
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
     ap.add_argument("--trace-rate", type=float, default=20.0)
     ap.add_argument("--trace-seconds", type=float, default=3.0)
@@ -346,11 +417,15 @@ def main():
     ap.add_argument("--max-batch", type=int, default=32)
     args = ap.parse_args()
     if args.impl == "reference":
+        args.n = args.n or 128
         return run_reference_arm(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "served":
         return run_served(args)
+    if args.workload == "pool256":
+        return run_pool(args)
+    args.n = args.n or 128
     args.warmup = max(args.warmup, 3)
 
     import numpy as np
