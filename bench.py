@@ -409,10 +409,12 @@ def main():
     ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
     ap.add_argument("--workload", default="single", choices=["single", "batched", "served", "pool256"])
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
+    # served: 20 jobs/s as the served configuration, over 6 s instead of 10 min and with resolutions <= 128 so
+    # that a run takes tens of seconds; the work still exceeds the arrival window several times (saturated)
     ap.add_argument("--trace-rate", type=float, default=20.0)
-    ap.add_argument("--trace-seconds", type=float, default=3.0)
-    ap.add_argument("--trace-res", default="32,48,64")
-    ap.add_argument("--trace-frames", default="4,16")
+    ap.add_argument("--trace-seconds", type=float, default=6.0)
+    ap.add_argument("--trace-res", default="32,48,64,96,128")
+    ap.add_argument("--trace-frames", default="8,24")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     ap.add_argument("--max-batch", type=int, default=32)
     args = ap.parse_args()

@@ -134,20 +134,58 @@ SceneView view_of(const fe_scene* s, int parity)
     return v;
 }
 
-template <class T>
-cudaError_t dalloc(std::vector<void*>& list, T** out, size_t count)
+// Device memory of scenes and batches comes from one stream-ordered pool per device that keeps freed
+// memory cached (release threshold: unlimited): creating and destroying scenes -- what a server does per job --
+// then costs no driver allocation and no device-wide synchronisation once the pool has grown to the working
+// set, unlike cudaMalloc / cudaFree (cudaFree waits for the whole device).  Allocations and frees are ordered
+// on the stream they are issued on.
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxPoolDevices] = {};
+
+cudaError_t device_pool(int device, cudaMemPool_t* out)
 {
+    if (device < 0 || device >= kMaxPoolDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[device]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = ~0ull;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return e;
+        }
+        g_pool[device] = pool;
+    }
+    *out = g_pool[device];
+    return cudaSuccess;
+}
+
+template <class T>
+cudaError_t dalloc(std::vector<void*>& list, T** out, size_t count, int device, cudaStream_t st)
+{
+    cudaMemPool_t pool;
+    cudaError_t e = device_pool(device, &pool);
+    if (e != cudaSuccess) return e;
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
+    e = cudaMallocFromPoolAsync(&p, count * sizeof(T) + 16, pool, st);
     if (e != cudaSuccess) return e;
     list.push_back(p);
     *out = (T*)p;
     return cudaSuccess;
 }
 
-void free_list(std::vector<void*>& list)
+// Returns the allocations to the pool in `st`'s order (after the work already issued on it).
+void free_list(std::vector<void*>& list, cudaStream_t st)
 {
-    for (void* p : list) cudaFree(p);
+    for (void* p : list) cudaFreeAsync(p, st);
     list.clear();
 }
 
@@ -181,15 +219,17 @@ fe_status alloc_grid(fe_scene* s)
     const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz, nww = (size_t)nx * ny * (nz + 1);
     const size_t nf = nu + nvv + nww;
     auto& L = s->allocs;
+    const int dev = s->device;
+    cudaStream_t st = s->own_stream;
     float *A, *B, *S, *N, *D;
     uint8_t *M, *M2;
-    FE_CUDA(dalloc(L, &A, nf));
-    FE_CUDA(dalloc(L, &B, nf));
-    FE_CUDA(dalloc(L, &S, nf));
-    FE_CUDA(dalloc(L, &N, nf));
-    FE_CUDA(dalloc(L, &D, nf));
-    FE_CUDA(dalloc(L, &M, nf));
-    FE_CUDA(dalloc(L, &M2, 2 * nf));
+    FE_CUDA(dalloc(L, &A, nf, dev, st));
+    FE_CUDA(dalloc(L, &B, nf, dev, st));
+    FE_CUDA(dalloc(L, &S, nf, dev, st));
+    FE_CUDA(dalloc(L, &N, nf, dev, st));
+    FE_CUDA(dalloc(L, &D, nf, dev, st));
+    FE_CUDA(dalloc(L, &M, nf, dev, st));
+    FE_CUDA(dalloc(L, &M2, 2 * nf, dev, st));
     v.u = A; v.v = A + nu; v.w = A + nu + nvv;
     v.u2 = B; v.v2 = B + nu; v.w2 = B + nu + nvv;
     v.su = S; v.sv = S + nu; v.sw = S + nu + nvv;
@@ -197,43 +237,43 @@ fe_status alloc_grid(fe_scene* s)
     v.du = D; v.dv = D + nu; v.dw = D + nu + nvv;
     v.mu = M; v.mv = M + nu; v.mw = M + nu + nvv;
     v.mu2 = M2; v.mv2 = M2 + nu; v.mw2 = M2 + nu + nvv;
-    FE_CUDA(cudaMemset(A, 0, nf * sizeof(float)));
-    FE_CUDA(cudaMemset(B, 0, nf * sizeof(float)));
-    FE_CUDA(cudaMemset(S, 0, nf * sizeof(float)));
-    FE_CUDA(cudaMemset(M, 0, nf));
-    FE_CUDA(dalloc(L, &v.marks, nc));
-    FE_CUDA(cudaMemset(v.marks, 0, nc));
-    FE_CUDA(dalloc(L, &v.p, nc));
-    FE_CUDA(cudaMemset(v.p, 0, nc * sizeof(double)));
-    FE_CUDA(dalloc(L, &v.b, nc));
-    FE_CUDA(cudaMemset(v.b, 0, nc * sizeof(double)));
+    FE_CUDA(cudaMemsetAsync(A, 0, nf * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(B, 0, nf * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(S, 0, nf * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(M, 0, nf, st));
+    FE_CUDA(dalloc(L, &v.marks, nc, dev, st));
+    FE_CUDA(cudaMemsetAsync(v.marks, 0, nc, st));
+    FE_CUDA(dalloc(L, &v.p, nc, dev, st));
+    FE_CUDA(cudaMemsetAsync(v.p, 0, nc * sizeof(double), st));
+    FE_CUDA(dalloc(L, &v.b, nc, dev, st));
+    FE_CUDA(cudaMemsetAsync(v.b, 0, nc * sizeof(double), st));
     // sort scratch over the key space
-    FE_CUDA(dalloc(L, &v.cell_count, v.g.key_space));
-    FE_CUDA(dalloc(L, &v.cell_start, (size_t)v.g.key_space + 1));
-    FE_CUDA(cudaMemset(v.cell_start, 0, ((size_t)v.g.key_space + 1) * sizeof(uint32_t)));
+    FE_CUDA(dalloc(L, &v.cell_count, v.g.key_space, dev, st));
+    FE_CUDA(dalloc(L, &v.cell_start, (size_t)v.g.key_space + 1, dev, st));
+    FE_CUDA(cudaMemsetAsync(v.cell_start, 0, ((size_t)v.g.key_space + 1) * sizeof(uint32_t), st));
     s->scan_tmp_bytes = sort_scan_tmp_bytes(v.g.key_space);
     uint8_t* tmp;
-    FE_CUDA(dalloc(L, &tmp, s->scan_tmp_bytes));
+    FE_CUDA(dalloc(L, &tmp, s->scan_tmp_bytes, dev, st));
     s->scan_tmp = tmp;
     // CG vectors
     CgWork& w = s->cg;
     float* vec;
-    FE_CUDA(dalloc(L, &vec, nc * 8));
-    FE_CUDA(cudaMemset(vec, 0, nc * 8 * sizeof(float)));
+    FE_CUDA(dalloc(L, &vec, nc * 8, dev, st));
+    FE_CUDA(cudaMemsetAsync(vec, 0, nc * 8 * sizeof(float), st));
     w.r0 = vec; w.r1 = vec + nc; w.w0 = vec + 2 * nc; w.w1 = vec + 3 * nc;
     w.s0 = vec + 4 * nc; w.s1 = vec + 5 * nc; w.pv = vec + 6 * nc; w.x = vec + 7 * nc;
-    FE_CUDA(dalloc(L, &w.list, nc));
+    FE_CUDA(dalloc(L, &w.list, nc, dev, st));
     FE_CUDA(cg_prepare(w, s->device));
     // 3 rotating totals slots (12 doubles) + per-block FLUID counts of up to kMaxCgBlocks solver blocks
-    FE_CUDA(dalloc(L, &w.partial, cg_partial_doubles(kMaxCgBlocks)));
-    FE_CUDA(cudaMemset(w.partial, 0, cg_partial_doubles(kMaxCgBlocks) * sizeof(double)));
-    FE_CUDA(dalloc(L, &w.bar, kCgBarWords));
-    FE_CUDA(cudaMemset(w.bar, 0, kCgBarWords * sizeof(unsigned)));
-    FE_CUDA(dalloc(L, &w.err, 1));
-    FE_CUDA(cudaMemset(w.err, 0, sizeof(int)));
-    FE_CUDA(dalloc(L, &s->stats_ring, (size_t)1 << 16));
+    FE_CUDA(dalloc(L, &w.partial, cg_partial_doubles(kMaxCgBlocks), dev, st));
+    FE_CUDA(cudaMemsetAsync(w.partial, 0, cg_partial_doubles(kMaxCgBlocks) * sizeof(double), st));
+    FE_CUDA(dalloc(L, &w.bar, kCgBarWords, dev, st));
+    FE_CUDA(cudaMemsetAsync(w.bar, 0, kCgBarWords * sizeof(unsigned), st));
+    FE_CUDA(dalloc(L, &w.err, 1, dev, st));
+    FE_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+    FE_CUDA(dalloc(L, &s->stats_ring, (size_t)1 << 16, dev, st));
     w.stats = s->stats_ring;
-    FE_CUDA(dalloc(L, &s->d_scalar, 4));
+    FE_CUDA(dalloc(L, &s->d_scalar, 4, dev, st));
     // marking tables
     const int n[3] = {nx, ny, nz};
     double maxH = std::max(v.h[0], std::max(v.h[1], v.h[2]));
@@ -255,53 +295,56 @@ fe_status alloc_grid(fe_scene* s)
             ex[i] = ((qf[i] == 0.0 && i0[i] == i) || (qf[i] == 1.0 && i0[i] + 1 == i)) ? 1 : 0;
             if (!ex[i]) v.any_inexact = 1;
         }
-        FE_CUDA(dalloc(L, &v.q_pos[a], n[a]));
-        FE_CUDA(dalloc(L, &v.q_f[a], n[a]));
-        FE_CUDA(dalloc(L, &v.q_b0[a], n[a]));
-        FE_CUDA(dalloc(L, &v.q_b1[a], n[a]));
-        FE_CUDA(dalloc(L, &v.q_i0[a], n[a]));
-        FE_CUDA(dalloc(L, &v.q_exact[a], n[a]));
-        FE_CUDA(cudaMemcpy(v.q_pos[a], qpos.data(), n[a] * sizeof(double), cudaMemcpyHostToDevice));
-        FE_CUDA(cudaMemcpy(v.q_f[a], qf.data(), n[a] * sizeof(double), cudaMemcpyHostToDevice));
-        FE_CUDA(cudaMemcpy(v.q_b0[a], b0.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice));
-        FE_CUDA(cudaMemcpy(v.q_b1[a], b1.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice));
-        FE_CUDA(cudaMemcpy(v.q_i0[a], i0.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice));
-        FE_CUDA(cudaMemcpy(v.q_exact[a], ex.data(), n[a], cudaMemcpyHostToDevice));
+        FE_CUDA(dalloc(L, &v.q_pos[a], n[a], dev, st));
+        FE_CUDA(dalloc(L, &v.q_f[a], n[a], dev, st));
+        FE_CUDA(dalloc(L, &v.q_b0[a], n[a], dev, st));
+        FE_CUDA(dalloc(L, &v.q_b1[a], n[a], dev, st));
+        FE_CUDA(dalloc(L, &v.q_i0[a], n[a], dev, st));
+        FE_CUDA(dalloc(L, &v.q_exact[a], n[a], dev, st));
+        FE_CUDA(cudaMemcpyAsync(v.q_pos[a], qpos.data(), n[a] * sizeof(double), cudaMemcpyHostToDevice, st));
+        FE_CUDA(cudaMemcpyAsync(v.q_f[a], qf.data(), n[a] * sizeof(double), cudaMemcpyHostToDevice, st));
+        FE_CUDA(cudaMemcpyAsync(v.q_b0[a], b0.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice, st));
+        FE_CUDA(cudaMemcpyAsync(v.q_b1[a], b1.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice, st));
+        FE_CUDA(cudaMemcpyAsync(v.q_i0[a], i0.data(), n[a] * sizeof(int), cudaMemcpyHostToDevice, st));
+        FE_CUDA(cudaMemcpyAsync(v.q_exact[a], ex.data(), n[a], cudaMemcpyHostToDevice, st));
+        FE_CUDA(cudaStreamSynchronize(st));  // the host tables above are freed at the end of this iteration
     }
     if (v.any_inexact) {
-        FE_CUDA(dalloc(L, &v.crit_list, nc));
-        FE_CUDA(dalloc(L, &v.crit_count, 1));
-        FE_CUDA(dalloc(L, &v.crit_flag, (nc + 3) & ~(size_t)3));
+        FE_CUDA(dalloc(L, &v.crit_list, nc, dev, st));
+        FE_CUDA(dalloc(L, &v.crit_count, 1, dev, st));
+        FE_CUDA(dalloc(L, &v.crit_flag, (nc + 3) & ~(size_t)3, dev, st));
     }
+    // everything above is complete before any other stream touches the scene
+    FE_CUDA(cudaStreamSynchronize(st));
     return FE_OK;
 }
 
 fe_status alloc_particles(fe_scene* s, uint64_t cap)
 {
     drop_graphs(s);
-    free_list(s->particle_allocs);
+    free_list(s->particle_allocs, s->stream);
     auto& L = s->particle_allocs;
     const bool apic = s->desc.solver == FE_SOLVER_APIC;
     for (int k = 0; k < 2; ++k) {
         ParticleSet& p = s->set[k];
-        FE_CUDA(dalloc(L, &p.px, cap));
-        FE_CUDA(dalloc(L, &p.py, cap));
-        FE_CUDA(dalloc(L, &p.pz, cap));
-        FE_CUDA(dalloc(L, &p.vx, cap));
-        FE_CUDA(dalloc(L, &p.vy, cap));
-        FE_CUDA(dalloc(L, &p.vz, cap));
-        FE_CUDA(dalloc(L, &p.pid, cap));
+        FE_CUDA(dalloc(L, &p.px, cap, s->device, s->stream));
+        FE_CUDA(dalloc(L, &p.py, cap, s->device, s->stream));
+        FE_CUDA(dalloc(L, &p.pz, cap, s->device, s->stream));
+        FE_CUDA(dalloc(L, &p.vx, cap, s->device, s->stream));
+        FE_CUDA(dalloc(L, &p.vy, cap, s->device, s->stream));
+        FE_CUDA(dalloc(L, &p.vz, cap, s->device, s->stream));
+        FE_CUDA(dalloc(L, &p.pid, cap, s->device, s->stream));
         for (int a = 0; a < 9; ++a) {
             p.c[a] = nullptr;
-            if (apic) FE_CUDA(dalloc(L, &p.c[a], cap));
+            if (apic) FE_CUDA(dalloc(L, &p.c[a], cap, s->device, s->stream));
         }
     }
     SceneView& v = s->base;
-    FE_CUDA(dalloc(L, &v.key, cap));
-    FE_CUDA(dalloc(L, &v.rank, cap));
-    FE_CUDA(dalloc(L, &v.perm, cap));
-    FE_CUDA(dalloc(L, &s->staging, cap * 9));
-    FE_CUDA(dalloc(L, &s->staging_u32, cap));
+    FE_CUDA(dalloc(L, &v.key, cap, s->device, s->stream));
+    FE_CUDA(dalloc(L, &v.rank, cap, s->device, s->stream));
+    FE_CUDA(dalloc(L, &v.perm, cap, s->device, s->stream));
+    FE_CUDA(dalloc(L, &s->staging, cap * 9, s->device, s->stream));
+    FE_CUDA(dalloc(L, &s->staging_u32, cap, s->device, s->stream));
     s->cap = cap;
     return FE_OK;
 }
@@ -590,17 +633,20 @@ fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
     v.max_cfl = desc->max_cfl;
     v.extrap_depth = (int)std::ceil(desc->max_cfl);                         // pic_simulator.cpp:491
     v.rk_substeps = (int)(unsigned)std::max(desc->max_cfl, 1.0);            // pic_simulator.cpp:255
-    fe_status st = alloc_grid(s);
-    if (st == FE_OK) {
-        e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
-        if (e != cudaSuccess) st = cuda_check(e, "stream create");
-        s->stream = s->own_stream;
-    }
+    fe_status st = FE_OK;
+    e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) st = cuda_check(e, "stream create");
+    s->stream = s->own_stream;
+    if (st == FE_OK) st = alloc_grid(s);
     if (st == FE_OK && desc->max_particles > 0) st = alloc_particles(s, desc->max_particles);
     if (st != FE_OK) {
-        free_list(s->allocs);
-        free_list(s->particle_allocs);
-        if (s->own_stream) cudaStreamDestroy(s->own_stream);
+        if (s->own_stream) {
+            cudaStreamSynchronize(s->own_stream);
+            free_list(s->allocs, s->own_stream);
+            free_list(s->particle_allocs, s->own_stream);
+            cudaStreamSynchronize(s->own_stream);
+            cudaStreamDestroy(s->own_stream);
+        }
         delete s;
         return st;
     }
@@ -614,9 +660,10 @@ fe_status fe_scene_destroy(fe_scene* s)
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     drop_graphs(s);
-    free_list(s->allocs);
-    free_list(s->particle_allocs);
-    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    // back to the pool in the own stream's order (the scene's work on any stream is complete here)
+    free_list(s->allocs, s->own_stream);
+    free_list(s->particle_allocs, s->own_stream);
+    cudaStreamDestroy(s->own_stream);  // its pending frees still run
     delete s;
     return FE_OK;
 }
@@ -1249,7 +1296,7 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
     b->scenes.assign(scenes, scenes + count);
     b->device = dev;
     auto fail = [&](fe_status st) {
-        free_list(b->allocs);
+        if (b->stream) free_list(b->allocs, b->stream);
         for (auto e : b->events) cudaEventDestroy(e);
         if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
@@ -1257,7 +1304,9 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
     };
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_check(e, "stream create"));
-    if ((e = dalloc(b->allocs, &b->table, kBatchMaxScenes)) != cudaSuccess) return fail(cuda_check(e, "batch allocation"));
+    if ((e = dalloc(b->allocs, &b->table, kBatchMaxScenes, dev, b->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
+        return fail(cuda_check(e, "batch allocation"));
     fe_status st = batch_set_members(b, scenes, count);
     if (st != FE_OK) return fail(st);
     // no host synchronisation: a scene's earlier work precedes the batch's work in its own stream order
@@ -1282,7 +1331,7 @@ fe_status fe_batch_destroy(fe_batch* b)
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
     batch_drop_graphs(b);
-    free_list(b->allocs);
+    free_list(b->allocs, b->stream);
     for (auto e : b->events) cudaEventDestroy(e);
     cudaStreamDestroy(b->stream);
     delete b;
