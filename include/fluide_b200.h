@@ -89,7 +89,9 @@ fe_status fe_scene_desc_default(fe_scene_desc* d);
  * (pic_simulator.cpp:17-26, flip_simulator.cpp:4-8, apic_simulator.cpp:4-7). */
 fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out);
 
-/* Frees all device memory of the scene. */
+/* Releases the scene.  Its device memory returns to the library's stream-ordered pool for the device, which
+ * keeps freed memory cached for later scenes (creating and destroying scenes then costs no driver allocation
+ * and no device-wide synchronisation); the pool's memory is returned to the driver when the process exits. */
 fe_status fe_scene_destroy(fe_scene* s);
 
 /* Sets the particles: pos and vel are n*3 floats (xyz interleaved), C is n*9 floats (rows cX, cY, cZ
