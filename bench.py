@@ -68,9 +68,33 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per fluid-cell CG iteration from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "k_cg_traffic.txt")
+def mg_coarse_cells(n):
+    """Cells of the multigrid levels >= 1 for an n^3 grid (each axis halved, rounding up, until <= 8)."""
+    dims, total = [n, n, n], 0
+    while max(dims) > 8:
+        dims = [(d + 1) // 2 for d in dims]
+        total += dims[0] * dims[1] * dims[2]
+    return total
+
+
+def uses_multigrid(n, pressure_solver):
+    return pressure_solver == "mgpcg" or (pressure_solver == "auto" and n ** 3 >= (1 << 20))
+
+
+def solver_alg_bytes(fluid, its, refs, n, multigrid):
+    """Algorithmic bytes of one pressure solve (numpy arrays per substep).  Plain CG: 41 B per FLUID cell per
+    inner iteration.  Multigrid-preconditioned CG: 68 B per FLUID cell per inner iteration over the five
+    level-0 passes (update + pre-smoothing residual 28, restriction read 4, pre-smoothed correction 8,
+    post-smoothing 12, search direction 16) plus 30 B per cell of every coarser level (residual, restriction,
+    correction, smoothing).  Both: 45 B per FLUID cell per FP64 residual pass (refinements + 1)."""
+    if multigrid:
+        return fluid * (its * 68.0 + (refs + 1.0) * 45.0) + its * 30.0 * mg_coarse_cells(n)
+    return fluid * (its * 41.0 + (refs + 1.0) * 45.0)
+
+
+def profile_traffic(multigrid=False):
+    """DRAM bytes per unit of solver work from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "k_mgcg_traffic.txt" if multigrid else "k_cg_traffic.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -195,7 +219,8 @@ def run_pool(args):
     t_seed = time.perf_counter() - t_seed
     N = pos.shape[0]
     dt = 1.0 / 480.0
-    scene = fe.Scene((n, n, n), solver=fe.APIC, max_cfl=1.0, cg_rel_tol=1e-8, cg_max_it=4000, max_refine=24)
+    scene = fe.Scene((n, n, n), solver=fe.APIC, max_cfl=1.0, cg_rel_tol=1e-8, cg_max_it=4000, max_refine=24,
+                     pressure_solver={"auto": fe.AUTO, "mgpcg": fe.MGPCG, "cg": fe.CG}[args.pressure_solver])
     stream = torch.cuda.Stream()
     scene.set_stream(stream.cuda_stream)
     scene.set_particles(pos, vel)
@@ -218,7 +243,8 @@ def run_pool(args):
     fluid = np.array([s["fluid_cells"] for s in stats], dtype=np.float64)
     its = np.array([s["cg_iterations"] for s in stats], dtype=np.float64)
     refs = np.array([s["refinements"] for s in stats], dtype=np.float64)
-    alg_bytes = fluid * (its * 41.0 + (refs + 1.0) * 45.0)
+    multigrid = uses_multigrid(n, args.pressure_solver)
+    alg_bytes = solver_alg_bytes(fluid, its, refs, n, multigrid)
     peak, peak_kind = peaks()
     achieved = alg_bytes.sum() / (cg_ms.sum() / 1e3) / 1e9
     phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
@@ -231,7 +257,7 @@ def run_pool(args):
                                "rel 1e-8" % n, "grid": [n, n, n], "particles": N, "solver": "APIC",
                    "substeps_timed": args.steps, "warmup": args.warmup, "seeding_s": t_seed,
                    "l2": "working set > 126 MB L2 (particles alone %.0f MB); no flush" % (N * 60 / 1e6)},
-        "roofline": {"bound": "hbm", "kernel": "k_cg (persistent FP32 CG + FP64 refinement, one launch/substep)",
+        "roofline": {"bound": "hbm", "kernel": "k_mgcg" if multigrid else "k_cg",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": float(alg_bytes.mean())},
         "phases": {"share": {"pre_solve": phase_share[0], "cg_solve": phase_share[1], "post_solve": phase_share[2]},
@@ -407,6 +433,9 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=1, help="substeps of the CPU reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
+    ap.add_argument("--pressure-solver", default="auto", choices=["auto", "mgpcg", "cg"],
+                    help="inner pressure solver: auto (multigrid-preconditioned CG from 2^20 cells, plain CG below), "
+                         "mgpcg or cg")
     ap.add_argument("--workload", default="single", choices=["single", "batched", "served", "pool256"])
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
     # served: 20 jobs/s as the served configuration, over 6 s instead of 10 min and with resolutions <= 128 so
@@ -448,7 +477,7 @@ def main():
     pos, vel = fe.seed_regions([dict(kind=0, lo=BOX[:3], hi=BOX[3:])], (n, n, n), (0, 0, 0), (1, 1, 1), 0)
     N = pos.shape[0]
     scene = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_inner_tol=args.cg_inner_tol,
-                     device=local)
+                     device=local, pressure_solver={"auto": fe.AUTO, "mgpcg": fe.MGPCG, "cg": fe.CG}[args.pressure_solver])
     stream = torch.cuda.Stream()
     scene.set_stream(stream.cuda_stream)
     scene.set_particles(pos, vel)
@@ -478,10 +507,11 @@ def main():
     fluid = np.array([s["fluid_cells"] for s in stats], dtype=np.float64)
     its = np.array([s["cg_iterations"] for s in stats], dtype=np.float64)
     refs = np.array([s["refinements"] for s in stats], dtype=np.float64)
-    alg_bytes = fluid * (its * 41.0 + (refs + 1.0) * 45.0)  # per launch: inner iterations + FP64 residual passes
+    multigrid = uses_multigrid(n, args.pressure_solver)
+    alg_bytes = solver_alg_bytes(fluid, its, refs, n, multigrid)  # per launch
     peak, peak_kind = peaks()
     achieved = alg_bytes.sum() / (cg_ms.sum() / 1e3) / 1e9
-    per_unit = profile_traffic()
+    per_unit = profile_traffic(multigrid)
     units = fluid * (its + refs + 1.0)
     traffic = float(per_unit * units.mean()) if per_unit else None
     phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
@@ -521,12 +551,19 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded analytic scene)",
             "config": workload_config(n, args.steps, args.warmup, world, N),
-            "roofline": {"bound": "hbm", "kernel": "k_cg (persistent FP32 CG + FP64 refinement, one launch/substep)",
+            "roofline": {"bound": "hbm",
+                         "kernel": ("k_mgcg (persistent multigrid-preconditioned FP32 CG + FP64 refinement, one "
+                                    "launch/substep)" if multigrid else
+                                    "k_cg (persistent FP32 CG + FP64 refinement, one launch/substep)"),
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": float(alg_bytes.mean()),
-                         "note": "algorithmic bytes = fluid cells x (41 B x inner iterations + 45 B x FP64 residual "
-                                 "passes); at 128^3 the CG working set is L2-resident"},
+                         "note": ("algorithmic bytes = FLUID cells x (68 B x inner iterations + 45 B x FP64 residual "
+                                  "passes) + 30 B x coarse-level cells x inner iterations; the solve is bound by its "
+                                  "grid barriers (about 14 per inner iteration), not by bandwidth: its working set "
+                                  "is L2-resident at 128^3" if multigrid else
+                                  "algorithmic bytes = fluid cells x (41 B x inner iterations + 45 B x FP64 residual "
+                                  "passes); at 128^3 the CG working set is L2-resident")},
             "phases": {"share": {"pre_solve": phase_share[0], "cg_solve": phase_share[1], "post_solve": phase_share[2]},
                        "ms_per_substep": (phase_ms.mean(axis=0)).tolist()},
             "solver": {"cg_iterations_mean": float(its.mean()), "refinements_mean": float(refs.mean()),

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(PKG, "libfluide_b200.so")
 FE_OK = 0
 FE_ERR_CUDA, FE_ERR_BAD_ARG, FE_ERR_OOM, FE_ERR_NOT_CONVERGED, FE_ERR_TIMEOUT, FE_ERR_STATE, FE_ERR_NO_DEVICE = range(1, 8)
 PIC, FLIP, APIC = 0, 1, 2
+AUTO, MGPCG, CG = 0, 1, 2  # fe_pressure_solver
 AIR, FLUID, BOUNDRY = 0, 1, 2
 (STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P, STAGE_MOVE) = range(8)
 
@@ -44,7 +45,7 @@ class SceneDesc(ctypes.Structure):
                 ("solver", ctypes.c_int32), ("flip_blend", ctypes.c_double), ("gravity", ctypes.c_double * 3),
                 ("max_cfl", ctypes.c_double), ("cg_rel_tol", ctypes.c_double), ("cg_max_it", ctypes.c_int32),
                 ("cg_inner_tol", ctypes.c_double), ("max_refine", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("max_particles", ctypes.c_uint64)]
+                ("max_particles", ctypes.c_uint64), ("pressure_solver", ctypes.c_int32)]
 
 
 class StepStats(ctypes.Structure):

@@ -23,182 +23,30 @@
 // solve surfaces as a status instead of a hung device.  Dot products travel with the barrier: blocks
 // add their partials into a rotating totals slot before arriving and read the totals once after it, so
 // all blocks take identical branch decisions.
-#include "fe_internal.cuh"
-
-#include <cuda/atomic>
+#include "fe_solver_common.cuh"
+#include "fe_mg_body.cuh"
 
 namespace fe {
 namespace {
 
 constexpr int kCgThreads = 1024;
 constexpr int kMultiThreads = 256;
-constexpr int kListCache = 8192;  // FLUID-list entries cached in shared memory per block (32 KB)
-constexpr unsigned long long kSpinLimit = 1ull << 26;
-
-struct CgParams {
-    double rel_tol, inner_tol;
-    int max_it, max_refine;
-    fe_step_stats* stats_ring;
-    unsigned* stats_counter;
-    unsigned stats_cap;
-};
-
-// Barrier generations count modulo 65535 (a multiple of 3), so the three rotating totals slots keep their
-// order across the wrap.
-__device__ __forceinline__ unsigned next_gen(unsigned g) { return g + 1u == 65535u ? 0u : g + 1u; }
-
-// Grid-wide barrier on two words in different 128-byte lines: bar[0] counts arrivals (one acq_rel
-// fetch_add per block), bar[32] holds the generation.  The last arriver resets the count, zeroes the totals
-// slot of the next generation and bumps the generation with a release store; the others poll the
-// generation (bounded) with acquire loads, away from the line the arrivals hit.  The release/acquire pair at
-// device scope, with the __syncthreads on either side, orders every thread's memory traffic of the block
-// across the barrier.  `gen` is the generation this barrier started in (tracked by thread 0).  Returns
-// false when the wait gave up.
-__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals, unsigned gen)
-{
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
-    const unsigned old = count.fetch_add(1u, cuda::memory_order_acq_rel);
-    if (old == nblocks - 1) {
-        double* next = totals + 4 * (next_gen(gen) % 3u);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) next[k] = 0.0;
-        count.store(0u, cuda::memory_order_relaxed);
-        genw.store(next_gen(gen), cuda::memory_order_release);
-        return true;
-    }
-    cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
-    unsigned long long spins = 0;
-    while (genw.load(cuda::memory_order_acquire) == gen) {
-        if (++spins > kSpinLimit) {
-            e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
-            return false;
-        }
-        if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) return false;
-    }
-    return true;
-}
-
-__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        bar_arrive_wait(w.bar, w.err, (unsigned)nblk, w.partial, gen);
-        gen = next_gen(gen);
-    }
-    __syncthreads();
-    return *(volatile int*)w.err == 0;
-}
-
-// Grid-wide sum of N doubles fused with the barrier.  Each block reduces to warp 0, whose lane 0 adds
-// the block partials into the totals slot of this barrier (FP64 red.add, ordered before the arrival by
-// its release) and arrives; after the barrier it reads the totals once.  Three total slots rotate: the
-// last arriver of barrier k zeroes slot k+1 before releasing it, and slot k is read only until the
-// readers arrive at barrier k+1.  All blocks read the same final totals, so their branch decisions
-// agree (the summation order, and hence the last bits, can vary from run to run).  (Per-block slots summed
-// by the last arriver avoid the floating-point atomics but put one more L2 round trip on the critical
-// path, which measured slower.)
-template <int N>
-__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w, unsigned& gen,
-                                            int nblk)
-{
-    static_assert(N <= 4, "at most 4 sums per reduction");
-    // warp partials use sh[0, 32 N), the totals sh[128, 128 + N): disjoint, so a warp that races ahead into
-    // the next reduction cannot overwrite totals another warp has not read yet
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < N; ++k)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < N; ++k) sh[wid * N + k] = v[k];
-    __syncthreads();
-    if (wid == 0) {
-        const int nw = blockDim.x >> 5;
-        double part[N];
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            double s = lane < nw ? sh[lane * N + k] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            part[k] = s;
-        }
-        if (lane == 0) {
-            // slot of this barrier: generation modulo 3; thread 0 tracks the generation itself (it takes
-            // part in every barrier), which saves a load round trip per barrier
-            double* totals = w.partial;  // [3][4]
-            double* slot = totals + 4 * (gen % 3u);  // zeroed by the release of this generation
-#pragma unroll
-            for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
-            const bool ok = bar_arrive_wait(w.bar, w.err, (unsigned)nblk, totals, gen);
-            gen = next_gen(gen);
-            if (ok)
-#pragma unroll
-                for (int k = 0; k < N; ++k) sh[128 + k] = __ldcg(slot + k);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < N; ++k) v[k] = sh[128 + k];
-    return *(volatile int*)w.err == 0;
-}
-
-// Block-wide sum of one double, valid in all threads (setup only).
-__device__ __forceinline__ double block_sum1(double x, double* sh)
-{
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    __syncthreads();
-    if (lane == 0) sh[wid] = x;
-    __syncthreads();
-    double s = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sh[k];
-    __syncthreads();
-    return s;
-}
-
-enum : uint32_t { kXm = 1, kXp = 2, kYm = 4, kYp = 8, kZm = 16, kZp = 32 };
-
-struct Stencil7 {
-    int sx;
-    int sxy;
-    float ih2[3];
-};
-
-// (A v)_c for the FLUID row c with in-domain mask m, non-FLUID entries of v being 0.
-template <class F>
-__device__ __forceinline__ float apply_row(const Stencil7& st, int c, uint32_t m, F val)
-{
-    const float vc = val(c);
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    if (m & kXm) ax += vc - val(c - 1);
-    if (m & kXp) ax += vc - val(c + 1);
-    if (m & kYm) ay += vc - val(c - st.sx);
-    if (m & kYp) ay += vc - val(c + st.sx);
-    if (m & kZm) az += vc - val(c - st.sxy);
-    if (m & kZp) az += vc - val(c + st.sxy);
-    return st.ih2[0] * ax + st.ih2[1] * ay + st.ih2[2] * az;
-}
 
 // The solver body, run by `nblk` blocks of which this is block `blk` (a whole grid for one scene, or a
 // block range of a multi-scene launch, see k_multi_cg); every barrier and reduction spans those blocks.
-__device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, const CgParams& prm, const int blk,
-                                        const int nblk, int* out_its = nullptr, int* out_fluid = nullptr)
+__device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, const CgWork& w, const CgParams& prm,
+                                        const int blk, const int nblk, int* out_its = nullptr, int* out_fluid = nullptr)
 {
-    __shared__ double sh[32 * 4 + 4];
-    __shared__ uint32_t s_warp[32];
+    double* sh = smem.sh;
+    uint32_t* s_warp = smem.s_warp;
     // the FLUID list does not change during a solve: each thread keeps its first list entries in shared
     // memory (entry k of thread t at s_list[k * blockDim.x + t]), which takes one dependent L2 round trip
     // out of every pass
-    __shared__ uint32_t s_list[kListCache];
-    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    uint32_t* s_list = smem.s_list;
+    const int nx = v.g.nx, ny = v.g.ny;
     const int sxy = nx * ny;
-    const int nc = sxy * nz;
     const int T = nblk * blockDim.x;
     const int tid = blk * blockDim.x + threadIdx.x;
-    const uint8_t* __restrict__ marks = v.marks;
     const double ih2d[3] = {v.inv_h[0] * v.inv_h[0], v.inv_h[1] * v.inv_h[1], v.inv_h[2] * v.inv_h[2]};
     Stencil7 st;
     st.sx = nx;
@@ -215,69 +63,11 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
     float* __restrict__ X = w.x;
     uint32_t* __restrict__ list = w.list;
 
-    // barrier generation as of this launch (thread 0 keeps it from here on)
     unsigned gen = 0;
-    if (threadIdx.x == 0) gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[32]).load(cuda::memory_order_relaxed);
-
-    // ---- setup: zero non-FLUID entries, ||b||^2, per-block FLUID counts over the block's cell range
-    const int chunk = (nc + nblk - 1) / nblk;
-    const int cb = min(nc, blk * chunk), ce = min(nc, cb + chunk);
-    double acc[2] = {0.0, 0.0};
-    for (int c = cb + threadIdx.x; c < ce; c += blockDim.x) {
-        if (marks[c] == FE_CELL_FLUID) {
-            acc[0] += b[c] * b[c];
-            acc[1] += 1.0;
-        } else {
-            p64[c] = 0.0;
-            R[0][c] = 0.f;
-            R[1][c] = 0.f;
-            W[0][c] = 0.f;
-            W[1][c] = 0.f;
-            S[0][c] = 0.f;
-            S[1][c] = 0.f;
-        }
-    }
-    // block offset = FLUID count of all earlier blocks (fixed order), total = all blocks
-    const double mine = block_sum1(acc[1], sh);
-    if (threadIdx.x == 0) w.partial[16 + blk] = mine;
-    double tot[2] = {acc[0], acc[1]};
-    if (!grid_reduce<2>(tot, sh, w, gen, nblk)) return;
-    const double bnorm = sqrt(tot[0]);
-    const int F = (int)tot[1];
-    double before = 0.0;
-    for (int bb = threadIdx.x; bb < blk; bb += blockDim.x) before += __ldcg(w.partial + 16 + bb);
-    before = block_sum1(before, sh);
-    // ordered compaction of this block's FLUID cells with their in-domain masks
-    uint32_t base = (uint32_t)before;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int c0 = cb; c0 < ce; c0 += blockDim.x) {
-        const int c = c0 + threadIdx.x;
-        const bool fl = c < ce && marks[c] == FE_CELL_FLUID;
-        const unsigned bal = __ballot_sync(0xffffffffu, fl);
-        if (lane == 0) s_warp[wid] = __popc(bal);
-        __syncthreads();
-        uint32_t off = 0, total = 0;
-        for (int k = 0; k < nwarp; ++k) {
-            const uint32_t x = s_warp[k];
-            off += k < wid ? x : 0u;
-            total += x;
-        }
-        if (fl) {
-            const int i = c % nx, j = (c / nx) % ny, k = c / sxy;
-            uint32_t m = (i > 0 ? kXm : 0u) | (i + 1 < nx ? kXp : 0u) | (j > 0 ? kYm : 0u) | (j + 1 < ny ? kYp : 0u) |
-                         (k > 0 ? kZm : 0u) | (k + 1 < nz ? kZp : 0u);
-            const uint32_t slot = base + off + __popc(bal & ((1u << lane) - 1u));
-            list[slot] = ((uint32_t)c << 6) | m;
-        }
-        base += total;
-        __syncthreads();
-    }
-    if (!grid_sync(w, gen, nblk)) return;
-    const int kc = kListCache / (int)blockDim.x;
-    {
-        int k = 0;
-        for (int e = tid; e < F && k < kc; e += T, ++k) s_list[k * blockDim.x + threadIdx.x] = __ldcg(list + e);
-    }
+    SolverSetup su;
+    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su)) return;
+    const int F = su.F, kc = su.kc;
+    const double bnorm = su.bnorm;
     auto entry = [&](int k, int e) -> uint32_t { return k < kc ? s_list[k * blockDim.x + threadIdx.x] : list[e]; };
     const double target = prm.rel_tol * bnorm;
     if (bnorm == 0.0) {
@@ -409,11 +199,22 @@ __device__ __forceinline__ void cg_body(const SceneView& v, const CgWork& w, con
 
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgParams prm)
 {
-    cg_body(v, w, prm, blockIdx.x, gridDim.x);
+    __shared__ SolverSmem smem;
+    cg_body(smem, v, w, prm, blockIdx.x, gridDim.x);
+}
+
+// The same solve with the multigrid-preconditioned inner loop (fe_mg_body.cuh).
+__global__ void __launch_bounds__(kCgThreads, 1) k_mgcg(SceneView v, CgWork w, MgWork mg, CgParams prm)
+{
+    __shared__ SolverSmem smem;
+    mg_body(smem, v, w, mg, prm, blockIdx.x, gridDim.x);
 }
 
 // Many scenes in one cooperative launch: blocks [start[s], start[s+1]) solve scene s with their own barrier
-// and reductions, so scenes iterate independently and concurrently.
+// and reductions, so scenes iterate independently and concurrently.  Every scene uses the plain CG body
+// here: its one barrier per iteration overlaps with the other scenes' barriers, and the multigrid body would
+// more than double this kernel's registers (fewer co-resident blocks for every scene of the batch).  A
+// scene's own multigrid setting applies when it steps alone.
 __global__ void __launch_bounds__(kMultiThreads) k_multi_cg(MultiCgScene* __restrict__ scenes, int S)
 {
     int sc = 0;
@@ -429,7 +230,8 @@ __global__ void __launch_bounds__(kMultiThreads) k_multi_cg(MultiCgScene* __rest
     prm.stats_cap = 1u << 16;
     int its = 0, fluid = 0;
     const int blk = (int)blockIdx.x - m.block_start;
-    cg_body(m.view, m.work, prm, blk, m.block_count, &its, &fluid);
+    __shared__ SolverSmem smem;
+    cg_body(smem, m.view, m.work, prm, blk, m.block_count, &its, &fluid);
     if (blk == 0 && threadIdx.x == 0) {  // read by the next solve's k_multi_partition
         m.last_its = its;
         m.last_fluid = fluid;
@@ -520,9 +322,68 @@ cudaError_t cg_prepare(CgWork& w, int device)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg, kCgThreads, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgcg, kCgThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
     w.blocks = sms;  // one persistent block per SM
     w.threads = kCgThreads;
     return cudaSuccess;
+}
+
+int mg_plan(int nx, int ny, int nz, const double h[3], MgLevel* out)
+{
+    int n[3] = {nx, ny, nz};
+    double hh[3] = {h[0], h[1], h[2]};
+    int levels = 0;
+    while (true) {
+        MgLevel& L = out[levels];
+        L = MgLevel{};
+        L.nx = n[0];
+        L.ny = n[1];
+        L.nz = n[2];
+        for (int a = 0; a < 3; ++a) L.ih2[a] = (float)(1.0 / (hh[a] * hh[a]));
+        ++levels;
+        if (std::max(n[0], std::max(n[1], n[2])) <= 8 || levels == kMaxMgLevels) break;
+        for (int a = 0; a < 3; ++a) {
+            n[a] = (n[a] + 1) / 2;
+            hh[a] *= 2.0;
+        }
+    }
+    // the last level is solved in one block's shared memory: it must have at most 512 cells
+    if (levels < 2 || out[levels - 1].nx * out[levels - 1].ny * out[levels - 1].nz > kCoarseMaxCells) return 1;
+    return levels;
+}
+
+int mg_block_from(const MgLevel* lv, int levels)
+{
+    int b = levels - 1;
+    while (b > 1 && (size_t)lv[b - 1].nx * lv[b - 1].ny * lv[b - 1].nz <= (size_t)kBlockLevelCells) --b;
+    return b;
+}
+
+cudaError_t launch_mgcg(const SceneView& v, const CgWork& w, const MgWork& mg, double rel_tol, double inner_tol,
+                        int max_it, int max_refine, cudaStream_t st)
+{
+    CgParams prm;
+    prm.rel_tol = rel_tol;
+    prm.inner_tol = inner_tol;
+    prm.max_it = max_it;
+    prm.max_refine = max_refine;
+    prm.stats_ring = w.stats;
+    prm.stats_counter = (unsigned*)(w.bar + 2);
+    prm.stats_cap = 1u << 16;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)w.blocks);
+    cfg.blockDim = dim3((unsigned)w.threads);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_mgcg, v, w, mg, prm);
+    count_launch();
+    return e;
 }
 
 cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, double inner_tol, int max_it,

@@ -180,6 +180,32 @@ struct CgWork {
 };
 cudaError_t cg_prepare(CgWork& w, int device);
 
+// Multigrid hierarchy of the MG-preconditioned solver (fe_mg_body.cuh): level 0 is the scene grid, whose
+// vectors are the solver's own (CgWork); level l >= 1 halves every axis of level l-1 (rounding up) until
+// the largest axis is <= 8, and that last level is solved by one block.
+constexpr int kMaxMgLevels = 12;
+// FE_PRESSURE_AUTO picks the multigrid solver from this many grid cells on: measured on B200, the plain CG
+// is faster at 32^3 and 64^3 (fewer, cheaper barriers in total), the multigrid one from about 90^3 on.
+constexpr size_t kMgAutoCells = (size_t)1 << 20;
+struct MgLevel {
+    int nx, ny, nz;
+    float ih2[3];      // 1 / h_l^2 per axis, h_l = 2^l h
+    uint8_t* mask;     // l >= 1: 1 where some child cell holds fluid
+    float* r;          // l >= 1: restricted residual
+    float* z;          // l >= 1: correction
+    float* t;          // l >= 1: scratch: the level's residual going down, its pre-smoothed correction going up
+};
+struct MgWork {
+    int levels;        // levels in use (0 or 1: no hierarchy, the plain CG solves)
+    int block_from;    // levels >= block_from (at most 4096 cells each) are processed by one block alone
+    MgLevel lv[kMaxMgLevels];
+};
+// Level dimensions for an nx x ny x nz grid with spacing h (host); returns the number of levels (>= 2), or 1
+// when the grid is too small for a hierarchy.
+int mg_plan(int nx, int ny, int nz, const double h[3], MgLevel* out);
+// First level (>= 1) small enough to be processed by one block without grid barriers.
+int mg_block_from(const MgLevel* lv, int levels);
+
 // One scene of a multi-scene pressure solve (fe_cg.cu k_multi_cg): the scene's grid view and solver
 // buffers, its solver settings and the block range [block_start, block_start + block_count) that solves it.
 struct MultiCgScene {
@@ -196,5 +222,7 @@ cudaError_t multi_cg_capacity(int device, int* max_blocks, int* threads);
 cudaError_t launch_multi_cg(MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st);
 cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, double inner_tol, int max_it, int max_refine,
                       cudaStream_t st);
+cudaError_t launch_mgcg(const SceneView& v, const CgWork& w, const MgWork& mg, double rel_tol, double inner_tol,
+                        int max_it, int max_refine, cudaStream_t st);
 
 }  // namespace fe

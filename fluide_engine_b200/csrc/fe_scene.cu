@@ -109,6 +109,7 @@ struct fe_scene {
     void* scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
     CgWork cg{};
+    MgWork mg{};                       // multigrid levels (levels >= 2) when the pressure solver is FE_PRESSURE_MGPCG
     double* d_scalar = nullptr;        // CFL / divergence result
     float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
     uint32_t* staging_u32 = nullptr;
@@ -263,6 +264,29 @@ fe_status alloc_grid(fe_scene* s)
     w.r0 = vec; w.r1 = vec + nc; w.w0 = vec + 2 * nc; w.w1 = vec + 3 * nc;
     w.s0 = vec + 4 * nc; w.s1 = vec + 5 * nc; w.pv = vec + 6 * nc; w.x = vec + 7 * nc;
     FE_CUDA(dalloc(L, &w.list, nc, dev, st));
+    // multigrid levels 1 .. L-1 (dense; level 0 is the grid above)
+    s->mg.levels = 0;
+    const bool want_mg = s->desc.pressure_solver == FE_PRESSURE_MGPCG ||
+                         (s->desc.pressure_solver == FE_PRESSURE_AUTO && nc >= kMgAutoCells);
+    if (want_mg) {
+        const int levels = mg_plan(nx, ny, nz, v.h, s->mg.lv);
+        if (levels >= 2) {
+            for (int l = 1; l < levels; ++l) {
+                MgLevel& M = s->mg.lv[l];
+                const size_t cells = (size_t)M.nx * M.ny * M.nz;
+                FE_CUDA(dalloc(L, &M.mask, cells, dev, st));
+                FE_CUDA(dalloc(L, &M.r, cells, dev, st));
+                FE_CUDA(dalloc(L, &M.z, cells, dev, st));
+                FE_CUDA(dalloc(L, &M.t, cells, dev, st));
+                FE_CUDA(cudaMemsetAsync(M.mask, 0, cells, st));
+                FE_CUDA(cudaMemsetAsync(M.r, 0, cells * sizeof(float), st));
+                FE_CUDA(cudaMemsetAsync(M.z, 0, cells * sizeof(float), st));
+                FE_CUDA(cudaMemsetAsync(M.t, 0, cells * sizeof(float), st));
+            }
+            s->mg.levels = levels;
+            s->mg.block_from = mg_block_from(s->mg.lv, levels);
+        }
+    }
     FE_CUDA(cg_prepare(w, s->device));
     // 3 rotating totals slots (12 doubles) + per-block FLUID counts of up to kMaxCgBlocks solver blocks
     FE_CUDA(dalloc(L, &w.partial, cg_partial_doubles(kMaxCgBlocks), dev, st));
@@ -410,8 +434,12 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last)
             FE_CUDA(launch_rhs(v, st));
             break;
         case kStepCg:
-            FE_CUDA(launch_cg(v, s->cg, s->desc.cg_rel_tol, s->desc.cg_inner_tol, s->desc.cg_max_it,
-                              s->desc.max_refine, st));
+            if (s->mg.levels >= 2)
+                FE_CUDA(launch_mgcg(v, s->cg, s->mg, s->desc.cg_rel_tol, s->desc.cg_inner_tol, s->desc.cg_max_it,
+                                    s->desc.max_refine, st));
+            else
+                FE_CUDA(launch_cg(v, s->cg, s->desc.cg_rel_tol, s->desc.cg_inner_tol, s->desc.cg_max_it,
+                                  s->desc.max_refine, st));
             break;
         case kStepApply:
             FE_CUDA(ensure_grid(s, pressure_buffer(s)));
@@ -565,6 +593,7 @@ fe_status fe_scene_desc_default(fe_scene_desc* d)
     d->cg_inner_tol = 1e-4;
     d->max_refine = kMaxRefineDefault;
     d->device = 0;
+    d->pressure_solver = FE_PRESSURE_AUTO;
     return FE_OK;
 }
 
@@ -583,6 +612,9 @@ fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
     if (desc->solver < FE_SOLVER_PIC || desc->solver > FE_SOLVER_APIC) return set_error(FE_ERR_BAD_ARG, "bad solver");
     if (!(desc->max_cfl > 0.0) || desc->max_cfl > 64.0) return set_error(FE_ERR_BAD_ARG, "max_cfl must be in (0, 64]");
     if (!(desc->cg_rel_tol > 0.0) || desc->cg_max_it < 1) return set_error(FE_ERR_BAD_ARG, "bad CG settings");
+    if (desc->pressure_solver != FE_PRESSURE_AUTO && desc->pressure_solver != FE_PRESSURE_MGPCG &&
+        desc->pressure_solver != FE_PRESSURE_CG)
+        return set_error(FE_ERR_BAD_ARG, "bad pressure solver %d", desc->pressure_solver);
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) return set_error(FE_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
@@ -1048,7 +1080,7 @@ uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[
 
 const char* fe_last_error(void) { return g_err; }
 
-int32_t fe_abi_version(void) { return 10000; }
+int32_t fe_abi_version(void) { return 10100; }
 
 }  // extern "C"
 

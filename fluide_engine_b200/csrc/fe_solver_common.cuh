@@ -1,0 +1,273 @@
+// fe_solver_common.cuh -- device pieces shared by the persistent pressure solvers (fe_cg.cu, fe_mgcg.cu):
+// the bounded grid barrier, grid-wide FP64 sums fused with it, the 7-point FLUID-row stencil and the setup
+// that compacts the FLUID cells into the solver's list.  Internal linkage: each solver file gets its own copy.
+#pragma once
+
+#include <cuda/atomic>
+
+#include "fe_internal.cuh"
+
+namespace fe {
+namespace {
+
+constexpr int kListCache = 8192;  // FLUID-list entries cached in shared memory per block (32 KB)
+constexpr unsigned long long kSpinLimit = 1ull << 26;
+
+struct CgParams {
+    double rel_tol, inner_tol;
+    int max_it, max_refine;
+    fe_step_stats* stats_ring;
+    unsigned* stats_counter;
+    unsigned stats_cap;
+};
+
+// Barrier generations count modulo 65535 (a multiple of 3), so the three rotating totals slots keep their
+// order across the wrap.
+__device__ __forceinline__ unsigned next_gen(unsigned g) { return g + 1u == 65535u ? 0u : g + 1u; }
+
+// Grid-wide barrier on two words in different 128-byte lines: bar[0] counts arrivals (one acq_rel
+// fetch_add per block), bar[32] holds the generation.  The last arriver resets the count, zeroes the totals
+// slot of the next generation and bumps the generation with a release store; the others poll the
+// generation (bounded) with acquire loads, away from the line the arrivals hit.  The release/acquire pair at
+// device scope, with the __syncthreads on either side, orders every thread's memory traffic of the block
+// across the barrier.  `gen` is the generation this barrier started in (tracked by thread 0).  Returns
+// false when the wait gave up.
+__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals, unsigned gen)
+{
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
+    const unsigned old = count.fetch_add(1u, cuda::memory_order_acq_rel);
+    if (old == nblocks - 1) {
+        double* next = totals + 4 * (next_gen(gen) % 3u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) next[k] = 0.0;
+        count.store(0u, cuda::memory_order_relaxed);
+        genw.store(next_gen(gen), cuda::memory_order_release);
+        return true;
+    }
+    cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
+    unsigned long long spins = 0;
+    while (genw.load(cuda::memory_order_acquire) == gen) {
+        if (++spins > kSpinLimit) {
+            e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
+            return false;
+        }
+        if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bar_arrive_wait(w.bar, w.err, (unsigned)nblk, w.partial, gen);
+        gen = next_gen(gen);
+    }
+    __syncthreads();
+    return *(volatile int*)w.err == 0;
+}
+
+// Grid-wide sum of N doubles fused with the barrier.  Each block reduces to warp 0, whose lane 0 adds
+// the block partials into the totals slot of this barrier (FP64 red.add, ordered before the arrival by
+// its release) and arrives; after the barrier it reads the totals once.  Three total slots rotate: the
+// last arriver of barrier k zeroes slot k+1 before releasing it, and slot k is read only until the
+// readers arrive at barrier k+1.  All blocks read the same final totals, so their branch decisions
+// agree (the summation order, and hence the last bits, can vary from run to run).  (Per-block slots summed
+// by the last arriver avoid the floating-point atomics but put one more L2 round trip on the critical
+// path, which measured slower.)
+template <int N>
+__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w, unsigned& gen,
+                                            int nblk)
+{
+    static_assert(N <= 4, "at most 4 sums per reduction");
+    // warp partials use sh[0, 32 N), the totals sh[128, 128 + N): disjoint, so a warp that races ahead into
+    // the next reduction cannot overwrite totals another warp has not read yet
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < N; ++k) sh[wid * N + k] = v[k];
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        double part[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            double s = lane < nw ? sh[lane * N + k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            part[k] = s;
+        }
+        if (lane == 0) {
+            // slot of this barrier: generation modulo 3; thread 0 tracks the generation itself (it takes
+            // part in every barrier), which saves a load round trip per barrier
+            double* totals = w.partial;  // [3][4]
+            double* slot = totals + 4 * (gen % 3u);  // zeroed by the release of this generation
+#pragma unroll
+            for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
+            const bool ok = bar_arrive_wait(w.bar, w.err, (unsigned)nblk, totals, gen);
+            gen = next_gen(gen);
+            if (ok)
+#pragma unroll
+                for (int k = 0; k < N; ++k) sh[128 + k] = __ldcg(slot + k);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = sh[128 + k];
+    return *(volatile int*)w.err == 0;
+}
+
+// Block-wide sum of one double, valid in all threads (setup only).
+__device__ __forceinline__ double block_sum1(double x, double* sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sh[k];
+    __syncthreads();
+    return s;
+}
+
+enum : uint32_t { kXm = 1, kXp = 2, kYm = 4, kYp = 8, kZm = 16, kZp = 32 };
+
+struct Stencil7 {
+    int sx;
+    int sxy;
+    float ih2[3];
+};
+
+// (A v)_c for the FLUID row c with in-domain mask m, non-FLUID entries of v being 0.
+template <class F>
+__device__ __forceinline__ float apply_row(const Stencil7& st, int c, uint32_t m, F val)
+{
+    const float vc = val(c);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (m & kXm) ax += vc - val(c - 1);
+    if (m & kXp) ax += vc - val(c + 1);
+    if (m & kYm) ay += vc - val(c - st.sx);
+    if (m & kYp) ay += vc - val(c + st.sx);
+    if (m & kZm) az += vc - val(c - st.sxy);
+    if (m & kZp) az += vc - val(c + st.sxy);
+    return st.ih2[0] * ax + st.ih2[1] * ay + st.ih2[2] * az;
+}
+
+// Shared memory of one solver block, declared once per kernel and handed to whichever solver body runs.
+constexpr int kCoarseMaxCells = 512;  // the multigrid solver's coarsest level lives in shared memory
+struct SolverSmem {
+    double sh[32 * 4 + 4];                 // block reductions
+    uint32_t s_warp[32];                   // compaction counts
+    uint32_t s_list[kListCache];           // cached FLUID-list entries
+    float cz[2][kCoarseMaxCells];          // multigrid: coarsest-level correction (ping-pong)
+    float cr[kCoarseMaxCells];             // multigrid: coarsest-level right-hand side
+    float cw[kCoarseMaxCells];             // multigrid: coarsest-level omega / diagonal (0 outside the mask)
+    uint8_t cb[kCoarseMaxCells];           // multigrid: coarsest-level in-domain neighbour bits
+};
+
+// Solver setup shared by the persistent solvers, run by `nblk` blocks of which this is block `blk`: zeroes
+// the non-FLUID entries of the pressure and of the FP32 solver vectors (so stencils over them need no branch
+// on the cell type), sums ||b||^2, compacts the FLUID cells in cell order into w.list with their
+// in-domain-neighbour masks (per-block counts -> grid reduction -> block offsets -> ordered compaction), and
+// caches each thread's first list entries in s_list.  Returns false when a grid wait gave up.
+struct SolverSetup {
+    int F;          // FLUID cells
+    double bnorm;   // ||b||_2
+    int kc;         // list entries cached per thread
+};
+
+__device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w, const int blk, const int nblk,
+                                             unsigned& gen, double* sh, uint32_t* s_warp, uint32_t* s_list,
+                                             SolverSetup& out)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const int sxy = nx * ny;
+    const int nc = sxy * nz;
+    const int T = nblk * blockDim.x;
+    const int tid = blk * blockDim.x + threadIdx.x;
+    const uint8_t* __restrict__ marks = v.marks;
+    double* __restrict__ p64 = v.p;
+    const double* __restrict__ b = v.b;
+    float* __restrict__ R[2] = {w.r0, w.r1};
+    float* __restrict__ W[2] = {w.w0, w.w1};
+    float* __restrict__ S[2] = {w.s0, w.s1};
+    uint32_t* __restrict__ list = w.list;
+    // barrier generation as of this launch (thread 0 keeps it from here on)
+    gen = 0;
+    if (threadIdx.x == 0) gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[32]).load(cuda::memory_order_relaxed);
+
+    // ---- setup: zero non-FLUID entries, ||b||^2, per-block FLUID counts over the block's cell range
+    const int chunk = (nc + nblk - 1) / nblk;
+    const int cb = min(nc, blk * chunk), ce = min(nc, cb + chunk);
+    double acc[2] = {0.0, 0.0};
+    for (int c = cb + threadIdx.x; c < ce; c += blockDim.x) {
+        if (marks[c] == FE_CELL_FLUID) {
+            acc[0] += b[c] * b[c];
+            acc[1] += 1.0;
+        } else {
+            p64[c] = 0.0;
+            R[0][c] = 0.f;
+            R[1][c] = 0.f;
+            W[0][c] = 0.f;
+            W[1][c] = 0.f;
+            S[0][c] = 0.f;
+            S[1][c] = 0.f;
+            w.pv[c] = 0.f;
+        }
+    }
+    // block offset = FLUID count of all earlier blocks (fixed order), total = all blocks
+    const double mine = block_sum1(acc[1], sh);
+    if (threadIdx.x == 0) w.partial[16 + blk] = mine;
+    double tot[2] = {acc[0], acc[1]};
+    if (!grid_reduce<2>(tot, sh, w, gen, nblk)) return false;
+    const double bnorm = sqrt(tot[0]);
+    const int F = (int)tot[1];
+    double before = 0.0;
+    for (int bb = threadIdx.x; bb < blk; bb += blockDim.x) before += __ldcg(w.partial + 16 + bb);
+    before = block_sum1(before, sh);
+    // ordered compaction of this block's FLUID cells with their in-domain masks
+    uint32_t base = (uint32_t)before;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int c0 = cb; c0 < ce; c0 += blockDim.x) {
+        const int c = c0 + threadIdx.x;
+        const bool fl = c < ce && marks[c] == FE_CELL_FLUID;
+        const unsigned bal = __ballot_sync(0xffffffffu, fl);
+        if (lane == 0) s_warp[wid] = __popc(bal);
+        __syncthreads();
+        uint32_t off = 0, total = 0;
+        for (int k = 0; k < nwarp; ++k) {
+            const uint32_t x = s_warp[k];
+            off += k < wid ? x : 0u;
+            total += x;
+        }
+        if (fl) {
+            const int i = c % nx, j = (c / nx) % ny, k = c / sxy;
+            uint32_t m = (i > 0 ? kXm : 0u) | (i + 1 < nx ? kXp : 0u) | (j > 0 ? kYm : 0u) | (j + 1 < ny ? kYp : 0u) |
+                         (k > 0 ? kZm : 0u) | (k + 1 < nz ? kZp : 0u);
+            const uint32_t slot = base + off + __popc(bal & ((1u << lane) - 1u));
+            list[slot] = ((uint32_t)c << 6) | m;
+        }
+        base += total;
+        __syncthreads();
+    }
+    if (!grid_sync(w, gen, nblk)) return false;
+    const int kc = kListCache / (int)blockDim.x;
+    {
+        int k = 0;
+        for (int e = tid; e < F && k < kc; e += T, ++k) s_list[k * blockDim.x + threadIdx.x] = __ldcg(list + e);
+    }
+    out.F = F;
+    out.bnorm = bnorm;
+    out.kc = kc;
+    return true;
+}
+
+}  // namespace
+}  // namespace fe

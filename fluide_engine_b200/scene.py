@@ -18,7 +18,7 @@ class Scene:
 
     def __init__(self, n, solver=_abi.FLIP, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), flip_blend=0.05,
                  gravity=(0.0, -9.81, 0.0), max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-4,
-                 max_refine=12, device=0, max_particles=0):
+                 max_refine=12, device=0, max_particles=0, pressure_solver=_abi.AUTO):
         L = _abi.lib()
         d = _abi.SceneDesc()
         check(L.fe_scene_desc_default(ctypes.byref(d)))
@@ -29,7 +29,7 @@ class Scene:
             d.gravity[a] = gravity[a]
         d.solver, d.flip_blend, d.max_cfl = solver, flip_blend, max_cfl
         d.cg_rel_tol, d.cg_max_it, d.cg_inner_tol, d.max_refine = cg_rel_tol, cg_max_it, cg_inner_tol, max_refine
-        d.device, d.max_particles = device, max_particles
+        d.device, d.max_particles, d.pressure_solver = device, max_particles, pressure_solver
         h = ctypes.c_void_p()
         check(L.fe_scene_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h

@@ -54,7 +54,18 @@ typedef struct {
     int32_t max_refine;      /* cap on FP64 outer refinement steps per pressure solve */
     int32_t device;          /* CUDA device ordinal */
     uint64_t max_particles;  /* capacity; 0 = sized by the first fe_scene_set_particles */
+    int32_t pressure_solver; /* fe_pressure_solver: how the inner FP32 solve runs (same system, same FP64 test) */
 } fe_scene_desc;
+
+/* Inner solver of the pressure projection.  Both solve the reference's system
+ * (single_phase_pressure_solver.cpp:99-164) to the same FP64 relative-residual target inside the same FP64
+ * refinement; they differ in how many inner iterations that takes.  The reference uses unpreconditioned CG
+ * (linear_system/conjugate_gradient_solver.cpp:14-55). */
+typedef enum {
+    FE_PRESSURE_AUTO = 0,    /* default: MGPCG for grids of 2^20 cells (about 101^3) or more, CG below (faster there) */
+    FE_PRESSURE_MGPCG = 1,   /* CG preconditioned by one multigrid V-cycle: 10-25 inner iterations, 4 L - 2 barriers each */
+    FE_PRESSURE_CG = 2       /* unpreconditioned CG: one grid barrier per iteration, 130-1100 iterations */
+} fe_pressure_solver;
 
 /* Per-substep statistics. */
 typedef struct {

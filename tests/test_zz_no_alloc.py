@@ -32,7 +32,8 @@ def test_noalloc_projection_matches_scene_pressure_stage():
     dt = 1.0 / 240.0
     pos, _ = fe.seed_regions([dict(kind=0, lo=(0.0, 0.0, 0.0), hi=(0.4, 0.6, 1.0))], n)
     vel = (np.random.default_rng(3).standard_normal(pos.shape) * 0.5).astype(np.float32)
-    scene = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=2000)
+    # fe_project_noalloc runs the plain CG solver: compare with the scene path configured the same way
+    scene = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=2000, pressure_solver=fe.CG)
     scene.set_particles(pos, vel)
     scene.run_stages(dt, fe.STAGE_SORT, fe.STAGE_PRE)
     u0, v0, w0, p0, marks = scene.grid()  # exactly what the pressure stage consumes
