@@ -78,7 +78,7 @@ def mg_coarse_cells(n):
 
 
 def uses_multigrid(n, pressure_solver):
-    return pressure_solver == "mgpcg" or (pressure_solver == "auto" and n ** 3 >= (1 << 20))
+    return pressure_solver == "mgpcg" or (pressure_solver == "auto" and n ** 3 >= (1 << 22))
 
 
 def solver_alg_bytes(fluid, its, refs, n, multigrid):
@@ -434,7 +434,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
     ap.add_argument("--pressure-solver", default="auto", choices=["auto", "mgpcg", "cg"],
-                    help="inner pressure solver: auto (multigrid-preconditioned CG from 2^20 cells, plain CG below), "
+                    help="inner pressure solver: auto (multigrid-preconditioned CG from 2^22 cells, plain CG below), "
                          "mgpcg or cg")
     ap.add_argument("--workload", default="single", choices=["single", "batched", "served", "pool256"])
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")

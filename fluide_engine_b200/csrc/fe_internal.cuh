@@ -184,9 +184,11 @@ cudaError_t cg_prepare(CgWork& w, int device);
 // vectors are the solver's own (CgWork); level l >= 1 halves every axis of level l-1 (rounding up) until
 // the largest axis is <= 8, and that last level is solved by one block.
 constexpr int kMaxMgLevels = 12;
-// FE_PRESSURE_AUTO picks the multigrid solver from this many grid cells on: measured on B200, the plain CG
-// is faster at 32^3 and 64^3 (fewer, cheaper barriers in total), the multigrid one from about 90^3 on.
-constexpr size_t kMgAutoCells = (size_t)1 << 20;
+// FE_PRESSURE_AUTO picks the multigrid solver from this many grid cells on.  Measured on B200 over whole
+// runs: the plain CG is faster at 32^3, 64^3 and 128^3 (at 128^3 its 380 one-barrier iterations cost about
+// what the multigrid solver's 27 iterations of 14 barriers do), the multigrid one by 6x at 256^3, where the
+// plain CG streams its vectors from HBM about 1,000 times per solve.
+constexpr size_t kMgAutoCells = (size_t)1 << 22;
 struct MgLevel {
     int nx, ny, nz;
     float ih2[3];      // 1 / h_l^2 per axis, h_l = 2^l h

@@ -80,6 +80,7 @@ PYBIND11_MODULE(PyFluidEngine, m)
         .def("GetDensity", &HybridSimulator::GetDensity)
         .def("SetParticlesPerBlock", &HybridSimulator::SetParticlesPerBlock)
         .def("SetPressureSolverTolerance", &HybridSimulator::SetPressureSolverTolerance)
+        .def("SetPressureSolverKind", [](HybridSimulator& s, int kind) { s.SetPressureSolverKind((fe_pressure_solver)kind); })
         // extensions: deterministic seeding and numpy particle access
         .def("InitializeFromRegions",
              [](HybridSimulator& s, const py::list& regions, uint64_t seed) {

@@ -157,9 +157,12 @@ class HybridSimulator:
             return self._scene.num_particles()
         return 0 if self._pending is None else self._pending[0].shape[0]
 
-    def SetPressureSolverSettings(self, cg_rel_tol=None, cg_max_it=None, cg_inner_tol=None, max_refine=None):
+    def SetPressureSolverSettings(self, cg_rel_tol=None, cg_max_it=None, cg_inner_tol=None, max_refine=None,
+                                  pressure_solver=None):
+        """Solver settings (the reference swaps LinearSystemSolver objects, pic_simulator.cpp:56-59);
+        pressure_solver: fluide_engine_b200.AUTO / MGPCG / CG."""
         upd = {k: v for k, v in dict(cg_rel_tol=cg_rel_tol, cg_max_it=cg_max_it, cg_inner_tol=cg_inner_tol,
-                                     max_refine=max_refine).items() if v is not None}
+                                     max_refine=max_refine, pressure_solver=pressure_solver).items() if v is not None}
         self._rebuild(lambda: self._cg.update(upd))
 
     # forces / scene contents ----------------------------------------------------------------------

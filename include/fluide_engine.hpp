@@ -186,6 +186,8 @@ class HybridSimulator : public PhysicsAnimation {
     {
         Reconfigure([&] { _desc.cg_rel_tol = relTol; _desc.cg_max_it = maxIterations; });
     }
+    // Inner solver of the projection: FE_PRESSURE_AUTO (default), FE_PRESSURE_MGPCG or FE_PRESSURE_CG.
+    void SetPressureSolverKind(fe_pressure_solver kind) { Reconfigure([&] { _desc.pressure_solver = kind; }); }
 
     // Particle seeding and access (the reference seeds only through InitializeParticles' std::rand).
     size_t InitializeFromRegions(const std::vector<fe_region_desc>& regions, uint64_t seed = 0);
