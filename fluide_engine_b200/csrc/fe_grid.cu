@@ -29,18 +29,43 @@ struct FaceArrays {
 
 enum { kModePlain = 0, kModePre = 1, kModePost = 2 };
 
+// 3D launch over the three face arrays: blocks of 32 x 8 threads tile (i, j); blockIdx.z runs over the z
+// layers of u (nz), then v (nz), then w (nz + 1), so every thread gets its face coordinates without integer
+// division and a warp's 32 threads read consecutive faces.
+constexpr int kTileX = 32, kTileY = 8;
+struct FaceCoord {
+    int c, i, j, k, sx, sy, sz;
+    size_t f;
+};
+dim3 face_grid(int nx, int ny, int nz)
+{
+    return dim3((unsigned)((nx + 1 + kTileX - 1) / kTileX), (unsigned)((ny + 1 + kTileY - 1) / kTileY),
+                (unsigned)(3 * nz + 1));
+}
+dim3 cell_grid(int nx, int ny, int nz)
+{
+    return dim3((unsigned)((nx + kTileX - 1) / kTileX), (unsigned)((ny + kTileY - 1) / kTileY), (unsigned)nz);
+}
+__device__ __forceinline__ bool face_coord(int nx, int ny, int nz, FaceCoord& fc)
+{
+    const int z = (int)blockIdx.z;
+    if (z < nz) { fc.c = 0; fc.k = z; fc.sx = nx + 1; fc.sy = ny; fc.sz = nz; }
+    else if (z < 2 * nz) { fc.c = 1; fc.k = z - nz; fc.sx = nx; fc.sy = ny + 1; fc.sz = nz; }
+    else { fc.c = 2; fc.k = z - 2 * nz; fc.sx = nx; fc.sy = ny; fc.sz = nz + 1; }
+    fc.i = (int)(blockIdx.x * kTileX + threadIdx.x);
+    fc.j = (int)(blockIdx.y * kTileY + threadIdx.y);
+    if (fc.i >= fc.sx || fc.j >= fc.sy) return false;
+    fc.f = (size_t)fc.i + (size_t)fc.sx * ((size_t)fc.j + (size_t)fc.sy * (size_t)fc.k);
+    return true;
+}
+
 template <int MODE>
 __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid, float gx, float gy, float gz)
 {
-    const size_t nu = (size_t)(nx + 1) * ny * nz, nv = (size_t)nx * (ny + 1) * nz, nw = (size_t)nx * ny * (nz + 1);
-    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t >= nu + nv + nw) return;
-    int c, sx, sy, sz;
-    size_t f;
-    if (t < nu) { c = 0; f = t; sx = nx + 1; sy = ny; sz = nz; }
-    else if (t < nu + nv) { c = 1; f = t - nu; sx = nx; sy = ny + 1; sz = nz; }
-    else { c = 2; f = t - nu - nv; sx = nx; sy = ny; sz = nz + 1; }
-    const int i = (int)(f % sx), j = (int)((f / sx) % sy), k = (int)(f / ((size_t)sx * sy));
+    FaceCoord fc;
+    if (!face_coord(nx, ny, nz, fc)) return;
+    const int c = fc.c, i = fc.i, j = fc.j, k = fc.k, sx = fc.sx, sy = fc.sy, sz = fc.sz;
+    const size_t f = fc.f;
     // select by value (a runtime index into the parameter arrays would spill them to local memory)
     const float* in = c == 0 ? fa.in[0] : (c == 1 ? fa.in[1] : fa.in[2]);
     const uint8_t* vin = c == 0 ? fa.vin[0] : (c == 1 ? fa.vin[1] : fa.vin[2]);
@@ -74,13 +99,13 @@ __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid
 __global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
                       const float* __restrict__ w)
 {
-    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
-    const size_t nc = (size_t)nx * ny * nz;
-    size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (c >= nc) return;
+    const int nx = v.g.nx, ny = v.g.ny;
+    const int i = (int)(blockIdx.x * kTileX + threadIdx.x), j = (int)(blockIdx.y * kTileY + threadIdx.y);
+    const int k = (int)blockIdx.z;
+    if (i >= nx || j >= ny) return;
+    const size_t c = idx3(i, j, k, nx, ny);
     double b = 0.0;
     if (v.marks[c] == FE_CELL_FLUID) {
-        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
         const double left = u[idx3(i, j, k, nx + 1, ny)], right = u[idx3(i + 1, j, k, nx + 1, ny)];
         const double down = vv[idx3(i, j, k, nx, ny + 1)], up = vv[idx3(i, j + 1, k, nx, ny + 1)];
         const double back = w[idx3(i, j, k, nx, ny)], front = w[idx3(i, j, k + 1, nx, ny)];
@@ -92,30 +117,25 @@ __global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __r
 __global__ void k_apply(SceneView v, float* u, float* vv, float* w)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
-    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz, nww = (size_t)nx * ny * (nz + 1);
-    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t >= nu + nvv + nww) return;
+    FaceCoord fc;
+    if (!face_coord(nx, ny, nz, fc)) return;
     const double* p = v.p;
-    if (t < nu) {
-        const int i = (int)(t % (nx + 1)), j = (int)((t / (nx + 1)) % ny), k = (int)(t / ((size_t)(nx + 1) * ny));
+    const int i = fc.i, j = fc.j, k = fc.k;
+    if (fc.c == 0) {
         if (i < 1 || i > nx - 1) return;
         const size_t cm = idx3(i - 1, j, k, nx, ny);
         if (v.marks[cm] != FE_CELL_FLUID) return;
-        u[t] = (float)((double)u[t] + v.inv_h[0] * (p[cm + 1] - p[cm]));
-    } else if (t < nu + nvv) {
-        const size_t f = t - nu;
-        const int i = (int)(f % nx), j = (int)((f / nx) % (ny + 1)), k = (int)(f / ((size_t)nx * (ny + 1)));
+        u[fc.f] = (float)((double)u[fc.f] + v.inv_h[0] * (p[cm + 1] - p[cm]));
+    } else if (fc.c == 1) {
         if (j < 1 || j > ny - 1) return;
         const size_t cm = idx3(i, j - 1, k, nx, ny);
         if (v.marks[cm] != FE_CELL_FLUID) return;
-        vv[f] = (float)((double)vv[f] + v.inv_h[1] * (p[cm + nx] - p[cm]));
+        vv[fc.f] = (float)((double)vv[fc.f] + v.inv_h[1] * (p[cm + nx] - p[cm]));
     } else {
-        const size_t f = t - nu - nvv;
-        const int i = (int)(f % nx), j = (int)((f / nx) % ny), k = (int)(f / ((size_t)nx * ny));
         if (k < 1 || k > nz - 1) return;
         const size_t cm = idx3(i, j, k - 1, nx, ny);
         if (v.marks[cm] != FE_CELL_FLUID) return;
-        w[f] = (float)((double)w[f] + v.inv_h[2] * (p[cm + (size_t)nx * ny] - p[cm]));
+        w[fc.f] = (float)((double)w[fc.f] + v.inv_h[2] * (p[cm + (size_t)nx * ny] - p[cm]));
     }
 }
 
@@ -182,7 +202,6 @@ cudaError_t run_extrap_group(const SceneView& v, float* const src[3], float* con
                              int depth, float gx, float gy, float gz, cudaStream_t st)
 {
     const size_t total = faces_total(v);
-    const unsigned nb = (unsigned)((total + 255) / 256);
     const float* in[3] = {src[0], src[1], src[2]};
     const uint8_t* vin[3] = {v.mu, v.mv, v.mw};
     // validity buffers alternate between two scratch sets laid out inside mu2 (size 2 * faces)
@@ -200,8 +219,9 @@ cudaError_t run_extrap_group(const SceneView& v, float* const src[3], float* con
             fa.vin[c] = vin[c];
             fa.vout[c] = vset[pass & 1][c];
         }
-        if (last) k_extrap<MODE><<<nb, 256, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, false, gx, gy, gz);
-        else k_extrap<kModePlain><<<nb, 256, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, true, 0.f, 0.f, 0.f);
+        const dim3 grid = face_grid(v.g.nx, v.g.ny, v.g.nz), block(kTileX, kTileY);
+        if (last) k_extrap<MODE><<<grid, block, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, false, gx, gy, gz);
+        else k_extrap<kModePlain><<<grid, block, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, true, 0.f, 0.f, 0.f);
         count_launch();
         for (int c = 0; c < 3; ++c) {
             in[c] = out[c];
@@ -214,16 +234,11 @@ cudaError_t run_extrap_group(const SceneView& v, float* const src[3], float* con
 __global__ void k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g, float gx, float gy,
                             float gz)
 {
-    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz, nww = (size_t)nx * ny * (nz + 1);
-    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t >= nu + nvv + nww) return;
-    int c, sx, sy, sz;
-    size_t f;
-    float* a;
-    if (t < nu) { c = 0; f = t; sx = nx + 1; sy = ny; sz = nz; a = u; }
-    else if (t < nu + nvv) { c = 1; f = t - nu; sx = nx; sy = ny + 1; sz = nz; a = vv; }
-    else { c = 2; f = t - nu - nvv; sx = nx; sy = ny; sz = nz + 1; a = w; }
-    const int i = (int)(f % sx), j = (int)((f / sx) % sy), k = (int)(f / ((size_t)sx * sy));
+    FaceCoord fc;
+    if (!face_coord(nx, ny, nz, fc)) return;
+    const int c = fc.c, i = fc.i, j = fc.j, k = fc.k, sx = fc.sx, sy = fc.sy, sz = fc.sz;
+    const size_t f = fc.f;
+    float* a = c == 0 ? u : (c == 1 ? vv : w);
     const bool wall = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1)) ||
                       (c == 2 && (k == 0 || k == sz - 1));
     if (wall) a[f] = 0.f;
@@ -241,8 +256,8 @@ cudaError_t launch_pre(const SceneView& v, double dt, cudaStream_t st)
     float* B[3] = {v.u2, v.v2, v.w2};
     const int d = v.extrap_depth;
     if (d <= 0) {
-        const size_t total = faces_total(v);
-        k_wall_tail<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny, v.g.nz, true, gx, gy, gz);
+        k_wall_tail<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny,
+                                                                                      v.g.nz, true, gx, gy, gz);
         count_launch();
         return cudaGetLastError();
     }
@@ -256,8 +271,8 @@ cudaError_t launch_post(const SceneView& v, cudaStream_t st)
     float* B[3] = {v.u2, v.v2, v.w2};
     const int d = v.extrap_depth;
     if (d <= 0) {
-        const size_t total = faces_total(v);
-        k_wall_tail<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny, v.g.nz, false, 0, 0, 0);
+        k_wall_tail<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny,
+                                                                                      v.g.nz, false, 0, 0, 0);
         count_launch();
         return cudaGetLastError();
     }
@@ -279,8 +294,7 @@ cudaError_t launch_rhs(const SceneView& v, cudaStream_t st)
 {
     const float *u, *vv, *w;
     pressure_buffers(v, u, vv, w);
-    const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
-    k_rhs<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(v, u, vv, w);
+    k_rhs<<<cell_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v, u, vv, w);
     count_launch();
     return cudaGetLastError();
 }
@@ -289,8 +303,7 @@ cudaError_t launch_apply(const SceneView& v, cudaStream_t st)
 {
     const float *u, *vv, *w;
     pressure_buffers(v, u, vv, w);
-    const size_t total = faces_total(v);
-    k_apply<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(v, (float*)u, (float*)vv, (float*)w);
+    k_apply<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v, (float*)u, (float*)vv, (float*)w);
     count_launch();
     return cudaGetLastError();
 }
