@@ -72,15 +72,26 @@ __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid
     float val = in[f];
     uint8_t valid = vin[f];
     if (!valid) {
+        const size_t sxy = (size_t)sx * sy;
+        // the six neighbours (order i+1, i-1, j+1, j-1, k+1, k-1): every validity byte and value is loaded
+        // before any is used, so they are in flight together instead of validity-then-value round trips
+        const bool in_dom[6] = {i + 1 < sx, i > 0, j + 1 < sy, j > 0, k + 1 < sz, k > 0};
+        const long long off[6] = {1, -1, (long long)sx, -(long long)sx, (long long)sxy, -(long long)sxy};
+        uint8_t nvalid[6];
+        float nval[6];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            nvalid[n] = in_dom[n] ? vin[(long long)f + off[n]] : (uint8_t)0;
+            nval[n] = in_dom[n] ? in[(long long)f + off[n]] : 0.f;
+        }
         float sum = 0.f;
         unsigned count = 0;
-        const size_t sxy = (size_t)sx * sy;
-        if (i + 1 < sx && vin[f + 1]) { sum += in[f + 1]; ++count; }
-        if (i > 0 && vin[f - 1]) { sum += in[f - 1]; ++count; }
-        if (j + 1 < sy && vin[f + sx]) { sum += in[f + sx]; ++count; }
-        if (j > 0 && vin[f - sx]) { sum += in[f - sx]; ++count; }
-        if (k + 1 < sz && vin[f + sxy]) { sum += in[f + sxy]; ++count; }
-        if (k > 0 && vin[f - sxy]) { sum += in[f - sxy]; ++count; }
+#pragma unroll
+        for (int n = 0; n < 6; ++n)
+            if (nvalid[n]) {
+                sum += nval[n];
+                ++count;
+            }
         if (count > 0) {
             val = sum / (float)count;
             valid = 1;
