@@ -37,7 +37,8 @@ def build_oracle(force=False):
 class _Desc(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int * 3), ("origin", ctypes.c_double * 3), ("size", ctypes.c_double * 3),
                 ("solver", ctypes.c_int), ("blend", ctypes.c_double), ("gravity", ctypes.c_double * 3),
-                ("max_cfl", ctypes.c_double), ("cg_rel_tol", ctypes.c_double), ("cg_max_it", ctypes.c_int)]
+                ("max_cfl", ctypes.c_double), ("cg_rel_tol", ctypes.c_double), ("cg_max_it", ctypes.c_int),
+                ("viscosity", ctypes.c_double)]
 
 
 class Region(ctypes.Structure):
@@ -67,10 +68,14 @@ def lib():
         U8 = ctypes.POINTER(ctypes.c_uint8)
         L.or_get_marks.argtypes = [P, U8]
         L.or_get_face_markers.argtypes = [P, U8, U8, U8]
+        L.or_get_diffusion_markers.argtypes = [P, U8, U8, U8]
+        L.or_diffusion_iterations.restype = ctypes.c_int
+        L.or_diffusion_iterations.argtypes = [P, ctypes.c_int]
         for name in ("or_stage_p2g", "or_stage_sdf", "or_stage_extrapolate", "or_stage_bc", "or_stage_g2p",
                      "or_build_markers"):
             getattr(L, name).argtypes = [P]
-        for name in ("or_stage_forces", "or_stage_pressure", "or_stage_advection", "or_stage_move", "or_substep"):
+        for name in ("or_stage_forces", "or_stage_diffusion", "or_stage_pressure", "or_stage_advection",
+                     "or_stage_move", "or_substep"):
             getattr(L, name).argtypes = [P, ctypes.c_double]
         L.or_cfl.restype = ctypes.c_double
         L.or_cfl.argtypes = [P, ctypes.c_double]
@@ -168,7 +173,7 @@ class OracleSim:
     """FP64 restatement of one simulator (PIC/FLIP/APIC) over the C oracle."""
 
     def __init__(self, n, solver, origin=(0, 0, 0), size=(1, 1, 1), blend=0.05, gravity=(0, -9.81, 0), max_cfl=1.0,
-                 cg_rel_tol=1e-6, cg_max_it=500):
+                 cg_rel_tol=1e-6, cg_max_it=500, viscosity=0.0):
         L = lib()
         d = _Desc()
         for a in range(3):
@@ -177,6 +182,7 @@ class OracleSim:
             d.size[a] = size[a]
             d.gravity[a] = gravity[a]
         d.solver, d.blend, d.max_cfl, d.cg_rel_tol, d.cg_max_it = solver, blend, max_cfl, cg_rel_tol, cg_max_it
+        d.viscosity = viscosity
         self.n, self.solver = tuple(n), solver
         self.h = L.or_create(ctypes.byref(d))
         if not self.h:
@@ -221,6 +227,15 @@ class OracleSim:
         a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
         self.L.or_get_face_markers(self.h, u8ptr(a), u8ptr(b), u8ptr(c))
         return a, b, c
+
+    def diffusion_markers(self):
+        su, sv, sw = face_shapes(self.n)
+        a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
+        self.L.or_get_diffusion_markers(self.h, u8ptr(a), u8ptr(b), u8ptr(c))
+        return a, b, c
+
+    def diffusion_iterations(self):
+        return tuple(self.L.or_diffusion_iterations(self.h, c) for c in range(3))
 
     def _cells(self, dtype):
         nx, ny, nz = self.n
@@ -309,8 +324,8 @@ def ref_lib(variant="serial"):
         L.ref_get_face_markers.argtypes = [P, U8, U8, U8]
         for name in ("ref_stage_p2g", "ref_stage_sdf"):
             getattr(L, name).argtypes = [P]
-        for name in ("ref_stage_begin", "ref_stage_forces", "ref_stage_pressure", "ref_stage_advection", "ref_substep",
-                     "ref_advance_frame"):
+        for name in ("ref_stage_begin", "ref_stage_forces", "ref_stage_diffusion", "ref_stage_pressure",
+                     "ref_stage_advection", "ref_substep", "ref_advance_frame", "ref_set_viscosity"):
             getattr(L, name).argtypes = [P, ctypes.c_double]
         L.ref_cfl.restype = ctypes.c_double
         L.ref_cfl.argtypes = [P, ctypes.c_double]
@@ -322,13 +337,15 @@ class RefSim:
     """The reference's own CPU simulator (serial or threaded build) behind oracle/ref_harness.cpp."""
 
     def __init__(self, n, solver, origin=(0, 0, 0), size=(1, 1, 1), blend=0.05, gravity=(0, -9.81, 0), max_cfl=1.0,
-                 cg_rel_tol=1e-6, cg_max_it=500, variant="serial"):
+                 cg_rel_tol=1e-6, cg_max_it=500, variant="serial", viscosity=0.0):
         self.L = ref_lib(variant)
         o = np.array(origin, dtype=np.float64); s = np.array(size, dtype=np.float64)
         g = np.array(gravity, dtype=np.float64)
         self.n, self.solver = tuple(n), solver
         self.h = self.L.ref_create(solver, n[0], n[1], n[2], dptr(o), dptr(s), blend, dptr(g), max_cfl, cg_rel_tol,
                                    cg_max_it)
+        if viscosity > 0:
+            self.L.ref_set_viscosity(self.h, viscosity)
 
     def __del__(self):
         if getattr(self, "h", None):

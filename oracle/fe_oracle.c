@@ -45,6 +45,8 @@ struct or_sim {
     double* b;               /* LinearSystem::b */
     int cg_it;
     double cg_res;
+    uint8_t *dmu, *dmv, *dmw; /* diffusion face markers (BackwardEulerDiffusionSolver::_fluidMarkers) */
+    int diff_it[3];           /* Jacobi iterations of the last diffusion solve, per component */
 };
 
 /* ---------------------------------------------------------------- math_utils.hpp restatements */
@@ -298,6 +300,9 @@ or_sim* or_create(const or_desc* d)
     s->marks = (uint8_t*)xcalloc(nc, 1);
     s->p = (double*)xcalloc(nc, sizeof(double));
     s->b = (double*)xcalloc(nc, sizeof(double));
+    s->dmu = (uint8_t*)xcalloc(cnt3(s->du), 1);
+    s->dmv = (uint8_t*)xcalloc(cnt3(s->dv), 1);
+    s->dmw = (uint8_t*)xcalloc(cnt3(s->dw), 1);
     return s;
 }
 
@@ -309,6 +314,7 @@ void or_destroy(or_sim* s)
     free(s->su); free(s->sv); free(s->sw);
     free(s->mu); free(s->mv); free(s->mw);
     free(s->sdf); free(s->marks); free(s->p); free(s->b);
+    free(s->dmu); free(s->dmv); free(s->dmw);
     free(s);
 }
 
@@ -804,6 +810,125 @@ void or_stage_pressure(or_sim* s, double dt)
     or_stage_bc(s);
 }
 
+/* ---------------------------------------------------------------- diffusion (viscosity) */
+
+/* JacobiIterationSolver::Solve (linear_system/jacobi_iteration_solver.cpp:14-37) with its Relax (:39-76) and
+ * CalculateTolerance (:79-83 = sqrt(BLAS::Dot(r, r)) of BLAS::Residual).  The reference's default diffusion
+ * solver, CudaJacobiIterationSolver(1000, 5, 1e-14) (fluid_solvers/backward_euler_diffusion_solver.cpp:10),
+ * relaxes with the same expression (linear_system/cuda_jacobi_iteration_solver.cu:5-24) on the same check
+ * schedule (:49-61); only its residual norm sums in another order.  Returns the iterations run; the result is
+ * left in x. */
+static int jacobi_solve(const row4* A, const double* b, double* x, dim3i n, int max_it, int check, double tol)
+{
+    size_t N = cnt3(n);
+    double* xt = (double*)xcalloc(N, sizeof(double));
+    double* res = (double*)xcalloc(N, sizeof(double));
+    double* cur = x; /* system->x */
+    double* nxt = xt; /* _xTemp */
+    int done = max_it;
+    for (int it = 0; it < max_it; ++it) {
+        for (int i = 0; i < n.x; ++i)
+            for (int j = 0; j < n.y; ++j)
+                for (int k = 0; k < n.z; ++k) {
+                    size_t c = ix3(n, i, j, k);
+                    double r = ((i > 0) ? A[ix3(n, i - 1, j, k)].r * cur[ix3(n, i - 1, j, k)] : 0.0) +
+                               ((i + 1 < n.x) ? A[c].r * cur[ix3(n, i + 1, j, k)] : 0.0) +
+                               ((j > 0) ? A[ix3(n, i, j - 1, k)].u * cur[ix3(n, i, j - 1, k)] : 0.0) +
+                               ((j + 1 < n.y) ? A[c].u * cur[ix3(n, i, j + 1, k)] : 0.0) +
+                               ((k > 0) ? A[ix3(n, i, j, k - 1)].f * cur[ix3(n, i, j, k - 1)] : 0.0) +
+                               ((k + 1 < n.z) ? A[c].f * cur[ix3(n, i, j, k + 1)] : 0.0);
+                    nxt[c] = (b[c] - r) / A[c].c;
+                }
+        double* t = cur; /* system->x.Swap(_xTemp) */
+        cur = nxt;
+        nxt = t;
+        if (it != 0 && it % check == 0) {
+            blas_residual(A, cur, b, res, n);
+            if (sqrt(blas_dot(res, res, n)) < tol) {
+                done = it + 1;
+                break;
+            }
+        }
+    }
+    if (cur != x) memcpy(x, cur, N * sizeof(double));
+    free(xt);
+    free(res);
+    return done;
+}
+
+/* One component of BackwardEulerDiffusionSolver::Solve (fluid_solvers/backward_euler_diffusion_solver.cpp:
+ * 20-49): markers from the fluid SDF sampled at the face positions of the copy-constructed velocity grid,
+ * whose data origins include the domain origin (face_centered_grid3d.cpp:11-17,303-316; the collider SDF is
+ * positive, so BOUNDRY never occurs), BuildMatrix (:136-198), BuildVectors (:200-242), then the Jacobi solve. */
+static int diffuse_component(or_sim* s, double* arr, dim3i sz, const double org[3], const double c[3],
+                             uint8_t* mk)
+{
+    size_t N = cnt3(sz);
+    for (int i = 0; i < sz.x; ++i)
+        for (int j = 0; j < sz.y; ++j)
+            for (int k = 0; k < sz.z; ++k) {
+                double pos[3] = {org[0] + s->h[0] * (double)i, org[1] + s->h[1] * (double)j,
+                                 org[2] + s->h[2] * (double)k};
+                mk[ix3(sz, i, j, k)] = sample3(s->sdf, s->n, s->sdf_origin, s->h, pos) < 0 ? OR_FLUID : OR_AIR;
+            }
+    row4* A = (row4*)malloc((N ? N : 1) * sizeof(row4));
+    double* b = (double*)xcalloc(N, sizeof(double));
+    for (int i = 0; i < sz.x; ++i)
+        for (int j = 0; j < sz.y; ++j)
+            for (int k = 0; k < sz.z; ++k) {
+                size_t f = ix3(sz, i, j, k);
+                row4* row = &A[f];
+                row->c = 1.0;
+                row->u = row->f = row->r = 0.0;
+                b[f] = arr[f]; /* b = x = arr; BOUNDRY neighbours would add c * arr */
+                if (mk[f] != OR_FLUID) continue;
+                if (i + 1 < sz.x) {
+                    if (mk[ix3(sz, i + 1, j, k)] != OR_AIR) row->c += c[0];
+                    if (mk[ix3(sz, i + 1, j, k)] == OR_FLUID) row->r -= c[0];
+                }
+                if (i > 0 && mk[ix3(sz, i - 1, j, k)] != OR_AIR) row->c += c[0];
+                if (j + 1 < sz.y) {
+                    if (mk[ix3(sz, i, j + 1, k)] != OR_AIR) row->c += c[1];
+                    if (mk[ix3(sz, i, j + 1, k)] == OR_FLUID) row->u -= c[1];
+                }
+                if (j > 0 && mk[ix3(sz, i, j - 1, k)] != OR_AIR) row->c += c[1];
+                if (k + 1 < sz.z) {
+                    if (mk[ix3(sz, i, j, k + 1)] != OR_AIR) row->c += c[2];
+                    if (mk[ix3(sz, i, j, k + 1)] == OR_FLUID) row->f -= c[2];
+                }
+                if (k > 0 && mk[ix3(sz, i, j, k - 1)] != OR_AIR) row->c += c[2];
+            }
+    int its = jacobi_solve(A, b, arr, sz, 1000, 5, 0.00000000000001);
+    free(A);
+    free(b);
+    return its;
+}
+
+/* PICSimulator::ComputeDiffusion (pic_simulator.cpp:214-222).  The call passes dt and viscosity swapped
+ * into DiffusionSolver::Solve; c = (timeInterval * viscosity) / (h * h) is the same product either way. */
+void or_stage_diffusion(or_sim* s, double dt)
+{
+    if (!(s->d.viscosity > 0.0)) return;
+    double c[3];
+    for (int a = 0; a < 3; ++a) c[a] = (s->d.viscosity * dt) / (s->h[a] * s->h[a]);
+    s->diff_it[0] = diffuse_component(s, s->u, s->du, s->rxo, c, s->dmu);
+    s->diff_it[1] = diffuse_component(s, s->v, s->dv, s->ryo, c, s->dmv);
+    s->diff_it[2] = diffuse_component(s, s->w, s->dw, s->rzo, c, s->dmw);
+    or_stage_bc(s);
+}
+
+int or_diffusion_iterations(const or_sim* s, int component)
+{
+    return (component >= 0 && component < 3) ? s->diff_it[component] : -1;
+}
+
+void or_get_diffusion_markers(const or_sim* s, uint8_t* mu, uint8_t* mv, uint8_t* mw)
+{
+    if (mu) memcpy(mu, s->dmu, cnt3(s->du));
+    if (mv) memcpy(mv, s->dmv, cnt3(s->dv));
+    if (mw) memcpy(mw, s->dmw, cnt3(s->dw));
+}
+
 double or_divergence_l2(const or_sim* s)
 {
     double acc = 0;
@@ -939,6 +1064,7 @@ void or_substep(or_sim* s, double dt)
     or_stage_extrapolate(s);
     or_stage_bc(s);
     or_stage_forces(s, dt);
+    or_stage_diffusion(s, dt);
     or_stage_pressure(s, dt);
     or_stage_advection(s, dt);
 }

@@ -11,7 +11,7 @@
  * against the reference compiled from its own sources, and by the reference's known-answer tests
  * restated in tests/test_oracle_known_answers.py).
  *
- * Scope: the no-collider, no-emitter, zero-viscosity scenes of the benchmark configurations.  With
+ * Scope: the no-collider, no-emitter scenes of the benchmark configurations, with or without viscosity.  With
  * no colliders the collider SDF is 1.7976931348623157e30 everywhere (3d/collider_collection.cpp:3,38),
  * which makes the collider branches of BlockedBoundryConditionSolver::ConstrainVelocity, the
  * BOUNDRY marker and ExtrapolateIntoCollider provable no-ops; they are restated as such.
@@ -39,6 +39,7 @@ typedef struct {
     double max_cfl;      /* HybridSimulator::_maxCfl */
     double cg_rel_tol;   /* CG stops when r.r <= (rel * ||b||_2)^2 */
     int cg_max_it;       /* ConjugateGradientSolver::_maxNumberOfIterations */
+    double viscosity;    /* Fluid3::viscosity (HybridSimulator::SetViscosity); 0 skips ComputeDiffusion */
 } or_desc;
 
 typedef struct or_sim or_sim;
@@ -72,6 +73,7 @@ void or_stage_advection(or_sim* s, double dt);      /* ComputeAdvection (extrap,
 void or_stage_g2p(or_sim* s);                       /* TransferGrid2Particles only */
 void or_stage_move(or_sim* s, double dt);           /* MoveParticles only */
 void or_build_markers(or_sim* s);                   /* SinglePhasePressureSolver::BuildMarkers only */
+void or_stage_diffusion(or_sim* s, double dt);      /* ComputeDiffusion (3 Jacobi solves + BC; no-op at viscosity 0) */
 
 void or_substep(or_sim* s, double dt);              /* PICSimulator::OnAdvanceTimeStep */
 double or_cfl(const or_sim* s, double dt);          /* PICSimulator::Cfl */
@@ -79,6 +81,9 @@ unsigned or_number_of_substeps(const or_sim* s, double dt); /* PICSimulator::Num
 int or_advance_time(or_sim* s, double frame_dt);    /* PhysicsAnimation::AdvanceTimeStep; returns substeps */
 
 int or_cg_iterations(const or_sim* s);              /* iterations of the last solve */
+int or_diffusion_iterations(const or_sim* s, int component); /* Jacobi iterations of the last diffusion solve */
+/* Face markers of the last diffusion solve (BackwardEulerDiffusionSolver::_fluidMarkers per component). */
+void or_get_diffusion_markers(const or_sim* s, uint8_t* mu, uint8_t* mv, uint8_t* mw);
 double or_cg_rel_residual(const or_sim* s);         /* true ||b - A p|| / ||b|| after the last solve */
 double or_divergence_l2(const or_sim* s);           /* ||div u||_2 over FLUID cells of the current grid */
 

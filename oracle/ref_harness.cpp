@@ -18,6 +18,8 @@
 #include "linear_system/conjugate_gradient_solver.hpp"
 #include "linear_system/blas.hpp"
 #include "linear_system/cuda_jacobi_iteration_solver.hpp"
+#include "linear_system/jacobi_iteration_solver.hpp"
+#include "fluid_solvers/backward_euler_diffusion_solver.hpp"
 #include "forces/directional_field.hpp"
 #undef private
 #undef protected
@@ -109,6 +111,19 @@ void* ref_create(int solver, int nx, int ny, int nz, const double* origin, const
 }
 
 void ref_destroy(void* p) { delete (Handle*)p; }
+
+// HybridSimulator::SetViscosity (hybrid_simulator.cpp:97-100).  The diffusion solver's default linear solver is
+// CudaJacobiIterationSolver(1000, 5, 1e-14) (fluid_solvers/backward_euler_diffusion_solver.cpp:10); on the CPU
+// the reference's own JacobiIterationSolver with the same settings takes its place (same relaxation and check
+// schedule, linear_system/jacobi_iteration_solver.cpp:14-76).
+void ref_set_viscosity(void* p, double viscosity)
+{
+    Handle* h = (Handle*)p;
+    auto diffusion = std::make_shared<BackwardEulerDiffusionSolver>();
+    diffusion->_systemSolver = std::make_shared<JacobiIterationSolver>(1000, 5, 0.00000000000001);
+    h->sim->SetDiffusionSolver(diffusion);
+    h->sim->SetViscosity(viscosity);
+}
 
 void ref_set_particles(void* p, size_t n, const double* pos, const double* vel, const double* C)
 {
@@ -228,6 +243,7 @@ void ref_stage_p2g(void* p) { Handle* h = (Handle*)p; quiet(h, true); h->sim->Tr
 void ref_stage_sdf(void* p) { Handle* h = (Handle*)p; quiet(h, true); h->sim->BuildSignedDistanceField(); quiet(h, false); }
 void ref_stage_begin(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->BeginAdvanceTimeStep(dt); quiet(h, false); }
 void ref_stage_forces(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeExternalForces(dt); quiet(h, false); }
+void ref_stage_diffusion(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeDiffusion(dt); quiet(h, false); }
 void ref_stage_pressure(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputePressure(dt); quiet(h, false); }
 void ref_stage_advection(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeAdvection(dt); quiet(h, false); }
 void ref_substep(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->OnAdvanceTimeStep(dt); quiet(h, false); }

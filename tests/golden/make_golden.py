@@ -4,7 +4,8 @@ Run from the repository root with the reference built (python oracle/build_ref.p
 
     python tests/golden/make_golden.py
 
-Each fixture is one substep of a small seeded scene (dam-break block, 8 particles per cell) run by
+It writes the fixtures that are missing (--force rewrites all of them).  Each fixture is one substep of a
+small seeded scene (dam-break block, 8 particles per cell) run by
 the serial build of the reference (PICSimulator / FLIPSimulator / APICSimulator::OnAdvanceTimeStep
 behind oracle/ref_harness.cpp): the inputs (FP32 positions widened to FP64, velocities, APIC C,
 warm-start pressure) and the outputs after P2G, after the particle SDF, and after the whole substep.
@@ -28,6 +29,11 @@ CASES = [
     ("pic_12x10x8", (12, 10, 8), oracle.PIC, (0.0, 0.0, 0.0, 0.5, 0.5, 0.7), 1, 2.0, (0.0, 0.0, 0.0)),
     ("apic_10", (10, 10, 10), oracle.APIC, (0.2, 0.0, 0.1, 0.7, 0.5, 0.9), 2, 1.0, (0.0, 0.0, 0.0)),
     ("flip_16_cfl3", (16, 16, 16), oracle.FLIP, (0.0, 0.0, 0.0, 0.4, 0.6, 1.0), 3, 3.0, (0.0, 0.0, 0.0)),
+    # viscous scenes (BackwardEulerDiffusionSolver with the CPU Jacobi solver): c = nu dt / h^2 of 0.006 (the
+    # Jacobi solve stops at its first checks), 0.6 (about 80 iterations) and 12.5 (the 1000-iteration cap)
+    ("flip_12_visc", (12, 12, 12), oracle.FLIP, (0.0, 0.0, 0.0, 0.4, 0.6, 1.0), 4, 1.0, (0.0, 0.0, 0.0), 0.01),
+    ("apic_12x10x9_visc", (12, 10, 9), oracle.APIC, (0.1, 0.0, 0.0, 0.6, 0.5, 0.8), 5, 1.0, (0.0, 0.0, 0.0), 1.0),
+    ("pic_10_visc_cap", (10, 10, 10), oracle.PIC, (0.0, 0.0, 0.2, 0.5, 0.6, 0.9), 6, 2.0, (0.0, 0.0, 0.0), 30.0),
 ]
 
 
@@ -42,9 +48,9 @@ def scene(n, region, seed, origin):
     return pos.astype(np.float64), vel.astype(np.float64), C.astype(np.float64), p0
 
 
-def make(name, n, solver, region, seed, max_cfl, origin, dt=1.0 / 240.0):
+def make(name, n, solver, region, seed, max_cfl, origin, viscosity=0.0, dt=1.0 / 240.0):
     pos, vel, C, p0 = scene(n, region, seed, origin)
-    kw = dict(origin=origin, max_cfl=max_cfl, cg_rel_tol=1e-6, cg_max_it=500)
+    kw = dict(origin=origin, max_cfl=max_cfl, cg_rel_tol=1e-6, cg_max_it=500, viscosity=viscosity)
     r = oracle.RefSim(n, solver, **kw)
     r.set_particles(pos, vel, C)
     r.set_pressure(p0)
@@ -59,7 +65,7 @@ def make(name, n, solver, region, seed, max_cfl, origin, dt=1.0 / 240.0):
     u, v, w = r.grid()
     P, V, CC = r.particles()
     np.savez_compressed(
-        os.path.join(OUT, name + ".npz"), n=np.array(n), solver=solver, max_cfl=max_cfl, dt=dt,
+        os.path.join(OUT, name + ".npz"), n=np.array(n), solver=solver, max_cfl=max_cfl, dt=dt, viscosity=viscosity,
         origin=np.array(origin), pos=pos, vel=vel, C=C, p0=p0, p2g_u=p2g[0], p2g_v=p2g[1], p2g_w=p2g[2], sdf=sdf,
         out_u=u, out_v=v, out_w=w, out_p=r.pressure(), out_marks=r.marks(), out_pos=P, out_vel=V, out_C=CC)
 
@@ -67,6 +73,9 @@ def make(name, n, solver, region, seed, max_cfl, origin, dt=1.0 / 240.0):
 if __name__ == "__main__":
     if not oracle.ref_available("serial"):
         sys.exit("build the reference first: python oracle/build_ref.py")
+    force = "--force" in sys.argv
     for c in CASES:
+        if not force and os.path.exists(os.path.join(OUT, c[0] + ".npz")):
+            continue
         make(*c)
         print("wrote", c[0])
