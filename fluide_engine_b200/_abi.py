@@ -16,7 +16,8 @@ FE_ERR_CUDA, FE_ERR_BAD_ARG, FE_ERR_OOM, FE_ERR_NOT_CONVERGED, FE_ERR_TIMEOUT, F
 PIC, FLIP, APIC = 0, 1, 2
 AUTO, MGPCG, CG = 0, 1, 2  # fe_pressure_solver
 AIR, FLUID, BOUNDRY = 0, 1, 2
-(STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P, STAGE_MOVE) = range(8)
+(STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_DIFFUSE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P,
+ STAGE_MOVE) = range(9)
 
 STATUS_NAMES = {0: "FE_OK", 1: "FE_ERR_CUDA", 2: "FE_ERR_BAD_ARG", 3: "FE_ERR_OOM", 4: "FE_ERR_NOT_CONVERGED",
                 5: "FE_ERR_TIMEOUT", 6: "FE_ERR_STATE", 7: "FE_ERR_NO_DEVICE"}
@@ -27,7 +28,8 @@ EXPORTS = [
     "fe_scene_get_particles",
     "fe_scene_num_particles", "fe_scene_step", "fe_scene_step_profiled", "fe_scene_advance_frame", "fe_scene_cfl", "fe_scene_run_stages",
     "fe_scene_get_grid", "fe_scene_set_grid", "fe_scene_set_pressure", "fe_scene_get_face_markers",
-    "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_get_sort", "fe_scene_divergence",
+    "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_set_viscosity",
+    "fe_scene_get_diffusion", "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
     "fe_abi_version",
@@ -45,7 +47,7 @@ class SceneDesc(ctypes.Structure):
                 ("solver", ctypes.c_int32), ("flip_blend", ctypes.c_double), ("gravity", ctypes.c_double * 3),
                 ("max_cfl", ctypes.c_double), ("cg_rel_tol", ctypes.c_double), ("cg_max_it", ctypes.c_int32),
                 ("cg_inner_tol", ctypes.c_double), ("max_refine", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("max_particles", ctypes.c_uint64), ("pressure_solver", ctypes.c_int32)]
+                ("max_particles", ctypes.c_uint64), ("pressure_solver", ctypes.c_int32), ("viscosity", ctypes.c_double)]
 
 
 class StepStats(ctypes.Structure):
@@ -101,6 +103,8 @@ def lib():
     L.fe_scene_get_snapshot.argtypes = [P, P, P, P]
     L.fe_scene_get_rhs.argtypes = [P, P]
     L.fe_scene_get_fluid_sdf.argtypes = [P, P]
+    L.fe_scene_set_viscosity.argtypes = [P, ctypes.c_double]
+    L.fe_scene_get_diffusion.argtypes = [P, P, P, P, P]
     L.fe_scene_get_sort.argtypes = [P, P, P, ctypes.c_uint64]
     L.fe_scene_divergence.argtypes = [P, D]
     L.fe_scene_set_stream.argtypes = [P, P]

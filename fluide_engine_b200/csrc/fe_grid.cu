@@ -29,35 +29,6 @@ struct FaceArrays {
 
 enum { kModePlain = 0, kModePre = 1, kModePost = 2 };
 
-// 3D launch over the three face arrays: blocks of 32 x 8 threads tile (i, j); blockIdx.z runs over the z
-// layers of u (nz), then v (nz), then w (nz + 1), so every thread gets its face coordinates without integer
-// division and a warp's 32 threads read consecutive faces.
-constexpr int kTileX = 32, kTileY = 8;
-struct FaceCoord {
-    int c, i, j, k, sx, sy, sz;
-    size_t f;
-};
-dim3 face_grid(int nx, int ny, int nz)
-{
-    return dim3((unsigned)((nx + 1 + kTileX - 1) / kTileX), (unsigned)((ny + 1 + kTileY - 1) / kTileY),
-                (unsigned)(3 * nz + 1));
-}
-dim3 cell_grid(int nx, int ny, int nz)
-{
-    return dim3((unsigned)((nx + kTileX - 1) / kTileX), (unsigned)((ny + kTileY - 1) / kTileY), (unsigned)nz);
-}
-__device__ __forceinline__ bool face_coord(int nx, int ny, int nz, FaceCoord& fc)
-{
-    const int z = (int)blockIdx.z;
-    if (z < nz) { fc.c = 0; fc.k = z; fc.sx = nx + 1; fc.sy = ny; fc.sz = nz; }
-    else if (z < 2 * nz) { fc.c = 1; fc.k = z - nz; fc.sx = nx; fc.sy = ny + 1; fc.sz = nz; }
-    else { fc.c = 2; fc.k = z - 2 * nz; fc.sx = nx; fc.sy = ny; fc.sz = nz + 1; }
-    fc.i = (int)(blockIdx.x * kTileX + threadIdx.x);
-    fc.j = (int)(blockIdx.y * kTileY + threadIdx.y);
-    if (fc.i >= fc.sx || fc.j >= fc.sy) return false;
-    fc.f = (size_t)fc.i + (size_t)fc.sx * ((size_t)fc.j + (size_t)fc.sy * (size_t)fc.k);
-    return true;
-}
 
 template <int MODE>
 __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid, float gx, float gy, float gz)

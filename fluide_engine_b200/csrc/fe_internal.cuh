@@ -152,6 +152,51 @@ __device__ __forceinline__ float sample_face(const float* __restrict__ a, float 
     return sample_st(a, s, sx, sy);
 }
 
+// 3D launch over the three face arrays: blocks of 32 x 8 threads tile (i, j); blockIdx.z runs over the z
+// layers of u (nz), then v (nz), then w (nz + 1), so every thread gets its face coordinates without integer
+// division and a warp's 32 threads read consecutive faces.
+constexpr int kTileX = 32, kTileY = 8;
+struct FaceCoord {
+    int c, i, j, k, sx, sy, sz;
+    size_t f;
+};
+inline dim3 face_grid(int nx, int ny, int nz)
+{
+    return dim3((unsigned)((nx + 1 + kTileX - 1) / kTileX), (unsigned)((ny + 1 + kTileY - 1) / kTileY),
+                (unsigned)(3 * nz + 1));
+}
+inline dim3 cell_grid(int nx, int ny, int nz)
+{
+    return dim3((unsigned)((nx + kTileX - 1) / kTileX), (unsigned)((ny + kTileY - 1) / kTileY), (unsigned)nz);
+}
+__device__ __forceinline__ bool face_coord(int nx, int ny, int nz, FaceCoord& fc)
+{
+    const int z = (int)blockIdx.z;
+    if (z < nz) { fc.c = 0; fc.k = z; fc.sx = nx + 1; fc.sy = ny; fc.sz = nz; }
+    else if (z < 2 * nz) { fc.c = 1; fc.k = z - nz; fc.sx = nx; fc.sy = ny + 1; fc.sz = nz; }
+    else { fc.c = 2; fc.k = z - 2 * nz; fc.sx = nx; fc.sy = ny; fc.sz = nz + 1; }
+    fc.i = (int)(blockIdx.x * kTileX + threadIdx.x);
+    fc.j = (int)(blockIdx.y * kTileY + threadIdx.y);
+    if (fc.i >= fc.sx || fc.j >= fc.sy) return false;
+    fc.f = (size_t)fc.i + (size_t)fc.sx * ((size_t)fc.j + (size_t)fc.sy * (size_t)fc.k);
+    return true;
+}
+
+// Viscosity (fe_diffuse.cu): buffers of the implicit diffusion solve, allocated when a scene's viscosity is > 0.
+// Face arrays are the three components concatenated (u | v | w) like the velocity buffers.
+struct DiffWork {
+    unsigned long long* node_dist;  // nx*ny*nz: bits of the smallest particle distance per SDF node (all ones: none)
+    uint8_t* mark;                  // faces: FE_CELL_FLUID / FE_CELL_AIR (BackwardEulerDiffusionSolver::_fluidMarkers)
+    unsigned long long* list;       // FLUID faces: (face << 9) | (wall << 8) | (component << 6) | FLUID-neighbour mask
+    double* x[2];                   // faces: Jacobi iterates (only FLUID entries are used)
+    unsigned* count;                // [0]: list length
+    int* its;                       // [3]: Jacobi iterations of the last solve, per component
+    int* tab_i0;                    // [component][axis][index]: GetBarycentric index of each face coordinate
+    double* tab_f;                  // same layout: GetBarycentric fraction
+    int tab_stride;                 // max(nx, ny, nz) + 1 entries per (component, axis)
+    int blocks;                     // blocks of the persistent Jacobi kernel (all co-resident)
+};
+
 // Kernel launchers (one per .cu file).
 cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, size_t scan_tmp_bytes);
 size_t sort_scan_tmp_bytes(uint32_t n);
@@ -159,6 +204,8 @@ cudaError_t launch_gather(const SceneView& v, const SceneView& dst, cudaStream_t
 cudaError_t launch_p2g(const SceneView& v, cudaStream_t st);
 cudaError_t launch_mark(const SceneView& v, cudaStream_t st);
 cudaError_t launch_fluid_sdf(const SceneView& v, double* out, cudaStream_t st);
+// Distance bits of the band SDF per node by a particle scatter, then the diffusion face markers (fe_mark.cu).
+cudaError_t launch_face_fluid_marks(const SceneView& v, const DiffWork& d, cudaStream_t st);
 cudaError_t launch_pre(const SceneView& v, double dt, cudaStream_t st);
 cudaError_t launch_post(const SceneView& v, cudaStream_t st);
 cudaError_t launch_rhs(const SceneView& v, cudaStream_t st);
@@ -226,5 +273,11 @@ cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, doubl
                       cudaStream_t st);
 cudaError_t launch_mgcg(const SceneView& v, const CgWork& w, const MgWork& mg, double rel_tol, double inner_tol,
                         int max_it, int max_refine, cudaStream_t st);
+
+// Viscosity (fe_diffuse.cu): ComputeDiffusion on the velocity buffers u, vv, ww (face markers, FLUID-face list,
+// persistent Jacobi solve, wall layers zeroed).  Uses the scene's solver barrier and error words (CgWork).
+cudaError_t launch_diffuse(const SceneView& v, const DiffWork& d, const CgWork& w, float* u, float* vv, float* ww,
+                           double dt, double viscosity, cudaStream_t st);
+cudaError_t diffuse_prepare(DiffWork& d, int device);
 
 }  // namespace fe

@@ -167,6 +167,76 @@ __global__ void k_fluid_sdf(SceneView v, double R2, double* out)
     }
 }
 
+
+// One thread per particle: every SDF node within the band 2r of the particle that the reference's hash search
+// would visit from that node and whose squared distance is <= (2r)^2 takes the minimum of the distance.  The
+// distances are non-negative doubles, whose bit patterns order like their values, so a 64-bit atomicMin on the
+// bits builds the same per-node minimum as the gather of node_sdf (the node's value is min(2r, that) - r).
+// Particles sorted by cell hit the same nodes as their neighbours; a plain read of the current minimum first
+// (it only ever decreases, so a stale value is still an upper bound) skips most atomics.
+__global__ void __launch_bounds__(256) k_sdf_scatter(SceneView v, unsigned long long* __restrict__ node, double R2)
+{
+    uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (p >= v.np) return;
+    const double X[3] = {(double)v.px[p], (double)v.py[p], (double)v.pz[p]};
+    const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
+    const double inv_bucket = 1.0 / v.bucket;
+    int lo[3], hi[3], pb[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        // nodes i with |q_i - x| <= 2r, widened by 1e-6 h (the exact test below decides)
+        const double t = (X[a] - v.sdf_origin[a]) * v.inv_h[a];
+        const double rr = v.band * v.inv_h[a] + 1e-6;
+        lo[a] = max((int)floor(t - rr) + 1, 0);
+        hi[a] = min((int)floor(t + rr), n[a] - 1);
+        pb[a] = bucket_fast(X[a], v.bucket, inv_bucket);
+    }
+    for (int k = lo[2]; k <= hi[2]; ++k) {
+        if (pb[2] != v.q_b0[2][k] && pb[2] != v.q_b1[2][k]) continue;
+        for (int j = lo[1]; j <= hi[1]; ++j) {
+            if (pb[1] != v.q_b0[1][j] && pb[1] != v.q_b1[1][j]) continue;
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+                if (pb[0] != v.q_b0[0][i] && pb[0] != v.q_b1[0][i]) continue;
+                const double d2 = dist2_ref(X[0], X[1], X[2], v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]);
+                if (!(d2 <= R2)) continue;
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(__dsqrt_rn(d2));
+                unsigned long long* cell = node + idx3(i, j, k, n[0], n[1]);
+                if (bits < __ldcg(cell)) atomicMin(cell, bits);
+            }
+        }
+    }
+}
+
+// BackwardEulerDiffusionSolver::BuildX/Y/ZMarkers (fluid_solvers/backward_euler_diffusion_solver.cpp:71-128):
+// a face is FLUID iff ScalarGrid3D::Sample (3d/scalar_grid3d.cpp:33-65) of the fluid SDF at the face centre is
+// < 0.  The face centres are those of the copied velocity grid (data origins include the domain origin,
+// grid_systems/face_centered_grid3d.cpp:11-17,303-316); their GetBarycentric index and fraction per axis come
+// from host tables computed in FP64 with the reference's expressions.
+__global__ void k_face_mark(SceneView v, DiffWork d)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    FaceCoord fc;
+    if (!face_coord(nx, ny, nz, fc)) return;
+    const int base = fc.c * 3 * d.tab_stride;
+    const int i0 = d.tab_i0[base + fc.i], j0 = d.tab_i0[base + d.tab_stride + fc.j];
+    const int k0 = d.tab_i0[base + 2 * d.tab_stride + fc.k];
+    const double fx = d.tab_f[base + fc.i], fy = d.tab_f[base + d.tab_stride + fc.j];
+    const double fz = d.tab_f[base + 2 * d.tab_stride + fc.k];
+    const int ip = min(i0 + 1, nx - 1), jp = min(j0 + 1, ny - 1), kp = min(k0 + 1, nz - 1);
+    const unsigned long long band = (unsigned long long)__double_as_longlong(v.band);
+    const unsigned long long* __restrict__ node = d.node_dist;
+    auto val = [&](int i, int j, int k) {
+        const unsigned long long b = min(__ldg(node + idx3(i, j, k, nx, ny)), band);
+        return __dsub_rn(__longlong_as_double((long long)b), v.radius);
+    };
+    const double c000 = val(i0, j0, k0), c100 = val(ip, j0, k0), c010 = val(i0, jp, k0), c110 = val(ip, jp, k0);
+    const double c001 = val(i0, j0, kp), c101 = val(ip, j0, kp), c011 = val(i0, jp, kp), c111 = val(ip, jp, kp);
+    const double b0 = lerp_ref(lerp_ref(c000, c100, fx), lerp_ref(c010, c110, fx), fy);
+    const double b1 = lerp_ref(lerp_ref(c001, c101, fx), lerp_ref(c011, c111, fx), fy);
+    const size_t off = fc.c == 0 ? 0 : (fc.c == 1 ? (size_t)(nx + 1) * ny * nz
+                                                   : (size_t)(nx + 1) * ny * nz + (size_t)nx * (ny + 1) * nz);
+    d.mark[off + fc.f] = lerp_ref(b0, b1, fz) < 0.0 ? FE_CELL_FLUID : FE_CELL_AIR;
+}
 }  // namespace
 
 cudaError_t launch_mark(const SceneView& v, cudaStream_t st)
@@ -196,5 +266,20 @@ cudaError_t launch_fluid_sdf(const SceneView& v, double* out, cudaStream_t st)
     count_launch();
     return cudaGetLastError();
 }
+
+cudaError_t launch_face_fluid_marks(const SceneView& v, const DiffWork& d, cudaStream_t st)
+{
+    const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
+    cudaError_t e = cudaMemsetAsync(d.node_dist, 0xff, nc * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    if (v.np > 0) {
+        k_sdf_scatter<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, d.node_dist, v.band * v.band);
+        count_launch();
+    }
+    k_face_mark<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v, d);
+    count_launch();
+    return cudaGetLastError();
+}
+
 
 }  // namespace fe

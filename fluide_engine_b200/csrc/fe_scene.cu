@@ -110,6 +110,9 @@ struct fe_scene {
     size_t scan_tmp_bytes = 0;
     CgWork cg{};
     MgWork mg{};                       // multigrid levels (levels >= 2) when the pressure solver is FE_PRESSURE_MGPCG
+    DiffWork diff{};                   // viscosity buffers (allocated once the viscosity is > 0)
+    bool diff_ready = false;
+    uint64_t epoch = 0;                // bumped when the substep's kernel sequence changes (batches re-capture)
     double* d_scalar = nullptr;        // CFL / divergence result
     float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
     uint32_t* staging_u32 = nullptr;
@@ -210,6 +213,54 @@ void bary_host(double x, int iHigh, int* i, double* f)
     else if (ii > iHigh - 1) { ii = iHigh - 1; *f = 1; }
     else *f = x - sfl;
     *i = ii;
+}
+
+// Buffers of the viscosity solve (fe_diffuse.cu) and the GetBarycentric tables of the face centres of the copied
+// velocity grid (data origins with the domain origin, grid_systems/face_centered_grid3d.cpp:11-17,303-316) in the
+// fluid SDF grid (ScalarGrid3D::Sample, 3d/scalar_grid3d.cpp:33-65), computed in FP64 as the reference does.
+fe_status alloc_diffusion(fe_scene* s)
+{
+    if (s->diff_ready) return FE_OK;
+    const SceneView& v = s->base;
+    const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
+    const size_t nc = (size_t)n[0] * n[1] * n[2];
+    const size_t nf = (size_t)(n[0] + 1) * n[1] * n[2] + (size_t)n[0] * (n[1] + 1) * n[2] +
+                      (size_t)n[0] * n[1] * (n[2] + 1);
+    auto& L = s->allocs;
+    const int dev = s->device;
+    cudaStream_t st = s->own_stream;
+    DiffWork d{};
+    FE_CUDA(dalloc(L, &d.node_dist, nc, dev, st));
+    FE_CUDA(dalloc(L, &d.mark, nf, dev, st));
+    FE_CUDA(cudaMemsetAsync(d.mark, 0, nf, st));
+    FE_CUDA(dalloc(L, &d.list, nf, dev, st));
+    FE_CUDA(dalloc(L, &d.x[0], nf, dev, st));
+    FE_CUDA(dalloc(L, &d.x[1], nf, dev, st));
+    FE_CUDA(dalloc(L, &d.count, 1, dev, st));
+    FE_CUDA(cudaMemsetAsync(d.count, 0, sizeof(unsigned), st));
+    FE_CUDA(dalloc(L, &d.its, 3, dev, st));
+    FE_CUDA(cudaMemsetAsync(d.its, 0, 3 * sizeof(int), st));
+    d.tab_stride = std::max(n[0], std::max(n[1], n[2])) + 1;
+    std::vector<int> ti0((size_t)9 * d.tab_stride, 0);
+    std::vector<double> tf((size_t)9 * d.tab_stride, 0.0);
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a) {
+            const double org = v.origin[a] + v.h[a] * (a == c ? 0.0 : 0.5);  // CalculateDataOrigins
+            const size_t base = (size_t)(3 * c + a) * d.tab_stride;
+            for (int i = 0; i < n[a] + (a == c ? 1 : 0); ++i) {
+                const double pos = org + v.h[a] * (double)i;                   // GetXPos / GetYPos / GetZPos
+                bary_host((pos - v.sdf_origin[a]) / v.h[a], n[a] - 1, &ti0[base + i], &tf[base + i]);
+            }
+        }
+    FE_CUDA(dalloc(L, &d.tab_i0, ti0.size(), dev, st));
+    FE_CUDA(dalloc(L, &d.tab_f, tf.size(), dev, st));
+    FE_CUDA(cudaMemcpyAsync(d.tab_i0, ti0.data(), ti0.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    FE_CUDA(cudaMemcpyAsync(d.tab_f, tf.data(), tf.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    FE_CUDA(diffuse_prepare(d, dev));
+    FE_CUDA(cudaStreamSynchronize(st));  // host tables are freed on return; the buffers are ready for any stream
+    s->diff = d;
+    s->diff_ready = true;
+    return FE_OK;
 }
 
 fe_status alloc_grid(fe_scene* s)
@@ -338,6 +389,10 @@ fe_status alloc_grid(fe_scene* s)
         FE_CUDA(dalloc(L, &v.crit_count, 1, dev, st));
         FE_CUDA(dalloc(L, &v.crit_flag, (nc + 3) & ~(size_t)3, dev, st));
     }
+    if (s->desc.viscosity > 0.0) {
+        fe_status ds = alloc_diffusion(s);
+        if (ds != FE_OK) return ds;
+    }
     // everything above is complete before any other stream touches the scene
     FE_CUDA(cudaStreamSynchronize(st));
     return FE_OK;
@@ -374,7 +429,7 @@ fe_status alloc_particles(fe_scene* s, uint64_t cap)
 }
 
 // Makes the velocity live in buffer `want` (0 = A, 1 = B); only stage-by-stage runs ever need the copy.
-cudaError_t ensure_grid(fe_scene* s, int want)
+cudaError_t ensure_grid(fe_scene* s, int want, cudaStream_t st = nullptr)
 {
     if (s->grid_cur == want) return cudaSuccess;
     const SceneView& v = s->base;
@@ -383,30 +438,33 @@ cudaError_t ensure_grid(fe_scene* s, int want)
     float* src = s->grid_cur ? v.u2 : v.u;
     float* dst = want ? v.u2 : v.u;
     s->grid_cur = want;
-    return cudaMemcpyAsync(dst, src, nf * sizeof(float), cudaMemcpyDeviceToDevice, s->stream);
+    return cudaMemcpyAsync(dst, src, nf * sizeof(float), cudaMemcpyDeviceToDevice, st ? st : s->stream);
 }
 
 int pressure_buffer(const fe_scene* s) { return (s->base.extrap_depth > 0 && (s->base.extrap_depth & 1)) ? 1 : 0; }
 
 // Internal steps of one substep; the public fe_stage ids map onto ranges of them.
-enum { kStepSort, kStepP2g, kStepMark, kStepPre, kStepRhs, kStepCg, kStepApply, kStepPost, kStepG2p, kStepMove,
-       kStepCount };
+enum { kStepSort, kStepP2g, kStepMark, kStepPre, kStepDiffuse, kStepRhs, kStepCg, kStepApply, kStepPost, kStepG2p,
+       kStepMove, kStepCount };
 
 int first_step(int stage)
 {
-    static const int m[FE_STAGE_COUNT] = {kStepSort, kStepP2g, kStepMark, kStepPre, kStepRhs, kStepPost, kStepG2p, kStepMove};
+    static const int m[FE_STAGE_COUNT] = {kStepSort, kStepP2g, kStepMark, kStepPre, kStepDiffuse, kStepRhs, kStepPost,
+                                          kStepG2p, kStepMove};
     return m[stage];
 }
 int last_step(int stage)
 {
-    static const int m[FE_STAGE_COUNT] = {kStepSort, kStepP2g, kStepMark, kStepPre, kStepApply, kStepPost, kStepG2p, kStepMove};
+    static const int m[FE_STAGE_COUNT] = {kStepSort, kStepP2g, kStepMark, kStepPre, kStepDiffuse, kStepApply, kStepPost,
+                                          kStepG2p, kStepMove};
     return m[stage];
 }
 
 // Enqueues internal steps [first, last] of one substep on s->stream.
-fe_status enqueue_steps(fe_scene* s, double dt, int first, int last)
+// `stream` overrides the scene's stream (a batch runs the pre-solve steps of viscous scenes on its own stream).
+fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_t stream = nullptr)
 {
-    cudaStream_t st = s->stream;
+    cudaStream_t st = stream ? stream : s->stream;
     for (int step = first; step <= last; ++step) {
         SceneView v = view_of(s, s->parity);
         switch (step) {
@@ -425,12 +483,20 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last)
             FE_CUDA(launch_mark(v, st));
             break;
         case kStepPre:
-            FE_CUDA(ensure_grid(s, 0));
+            FE_CUDA(ensure_grid(s, 0, st));
             FE_CUDA(launch_pre(v, dt, st));
             s->grid_cur = pressure_buffer(s);
             break;
+        case kStepDiffuse:
+            if (s->desc.viscosity > 0.0) {
+                const int pb = pressure_buffer(s);
+                FE_CUDA(ensure_grid(s, pb, st));
+                FE_CUDA(launch_diffuse(v, s->diff, s->cg, pb ? v.u2 : v.u, pb ? v.v2 : v.v, pb ? v.w2 : v.w, dt,
+                                       s->desc.viscosity, st));
+            }
+            break;
         case kStepRhs:
-            FE_CUDA(ensure_grid(s, pressure_buffer(s)));
+            FE_CUDA(ensure_grid(s, pressure_buffer(s), st));
             FE_CUDA(launch_rhs(v, st));
             break;
         case kStepCg:
@@ -442,16 +508,16 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last)
                                   s->desc.max_refine, st));
             break;
         case kStepApply:
-            FE_CUDA(ensure_grid(s, pressure_buffer(s)));
+            FE_CUDA(ensure_grid(s, pressure_buffer(s), st));
             FE_CUDA(launch_apply(v, st));
             break;
         case kStepPost:
-            FE_CUDA(ensure_grid(s, pressure_buffer(s)));
+            FE_CUDA(ensure_grid(s, pressure_buffer(s), st));
             FE_CUDA(launch_post(v, st));
             s->grid_cur = 0;
             break;
         case kStepG2p:
-            FE_CUDA(ensure_grid(s, 0));
+            FE_CUDA(ensure_grid(s, 0, st));
             if (last >= kStepMove) {
                 FE_CUDA(launch_g2p(v, dt, true, true, st));
                 step = kStepMove;
@@ -460,7 +526,7 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last)
             }
             break;
         case kStepMove:
-            FE_CUDA(ensure_grid(s, 0));
+            FE_CUDA(ensure_grid(s, 0, st));
             FE_CUDA(launch_g2p(v, dt, false, true, st));
             break;
         default:
@@ -615,6 +681,8 @@ fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
     if (desc->pressure_solver != FE_PRESSURE_AUTO && desc->pressure_solver != FE_PRESSURE_MGPCG &&
         desc->pressure_solver != FE_PRESSURE_CG)
         return set_error(FE_ERR_BAD_ARG, "bad pressure solver %d", desc->pressure_solver);
+    if (!(desc->viscosity >= 0.0) || !std::isfinite(desc->viscosity))
+        return set_error(FE_ERR_BAD_ARG, "viscosity must be finite and >= 0");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) return set_error(FE_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
@@ -1011,6 +1079,42 @@ fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf)
     return FE_OK;
 }
 
+fe_status fe_scene_set_viscosity(fe_scene* s, double viscosity)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    if (!(viscosity >= 0.0) || !std::isfinite(viscosity))
+        return set_error(FE_ERR_BAD_ARG, "viscosity must be finite and >= 0");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    if (viscosity > 0.0 && !s->diff_ready) {
+        FE_CUDA(cudaStreamSynchronize(s->stream));
+        fe_status st = alloc_diffusion(s);
+        if (st != FE_OK) return st;
+    }
+    if ((viscosity > 0.0) != (s->desc.viscosity > 0.0) || viscosity != s->desc.viscosity) {
+        drop_graphs(s);  // the captured substeps hold the old sequence / coefficients
+        ++s->epoch;
+    }
+    s->desc.viscosity = viscosity;
+    return FE_OK;
+}
+
+fe_status fe_scene_get_diffusion(fe_scene* s, int32_t* iterations, uint8_t* mu, uint8_t* mv, uint8_t* mw)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    if (!s->diff_ready) return set_error(FE_ERR_STATE, "the scene has never had a viscosity > 0");
+    const int nx = s->base.g.nx, ny = s->base.g.ny, nz = s->base.g.nz;
+    const size_t nu = (size_t)(nx + 1) * ny * nz, nv = (size_t)nx * (ny + 1) * nz, nw = (size_t)nx * ny * (nz + 1);
+    if (iterations) FE_CUDA(cudaMemcpyAsync(iterations, s->diff.its, 3 * sizeof(int32_t), cudaMemcpyDefault, s->stream));
+    if (mu) FE_CUDA(cudaMemcpyAsync(mu, s->diff.mark, nu, cudaMemcpyDefault, s->stream));
+    if (mv) FE_CUDA(cudaMemcpyAsync(mv, s->diff.mark + nu, nv, cudaMemcpyDefault, s->stream));
+    if (mw) FE_CUDA(cudaMemcpyAsync(mw, s->diff.mark + nu + nv, nw, cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
 fe_status fe_scene_get_sort(fe_scene* s, uint32_t* keys, uint32_t* perm, uint64_t n)
 {
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
@@ -1080,7 +1184,7 @@ uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[
 
 const char* fe_last_error(void) { return g_err; }
 
-int32_t fe_abi_version(void) { return 10100; }
+int32_t fe_abi_version(void) { return 10200; }
 
 }  // extern "C"
 
@@ -1103,6 +1207,7 @@ struct fe_batch {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_kernels[2] = {0, 0};
     double graph_dt = -1.0;
+    uint64_t graph_epoch = 0;  // sum of the scenes' epochs when the graphs were captured
     int parity = 0;
     int64_t steps_done = 0;   // substeps since creation: a young batch replays per-scene graphs
 };
@@ -1124,20 +1229,35 @@ void batch_drop_graphs(fe_batch* b)
     b->graph_dt = -1.0;
 }
 
+// The pre-solve steps of a scene with viscosity run on the batch's stream, one scene after another, so that no
+// two cooperative Jacobi kernels (fe_diffuse.cu) are ever in flight together; the other scenes' pre-solve steps
+// run concurrently on their own streams.
+cudaStream_t pre_stream(const fe_batch* b, const fe_scene* s) { return s->desc.viscosity > 0.0 ? b->stream : s->stream; }
+
 // Enqueues one batch substep on b->stream with fork/join over the scenes' streams.
 fe_status batch_enqueue(fe_batch* b, double dt)
 {
     const int S = (int)b->scenes.size();
     cudaEvent_t fork0 = b->events[2 * S], fork1 = b->events[2 * S + 1];
     FE_CUDA(cudaEventRecord(fork0, b->stream));
-    for (int i = 0; i < S; ++i) {
-        fe_scene* s = b->scenes[i];
-        FE_CUDA(cudaStreamWaitEvent(s->stream, fork0, 0));
-        fe_status st = enqueue_steps(s, dt, kStepSort, kStepRhs);
-        if (st != FE_OK) return st;
-        FE_CUDA(cudaEventRecord(b->events[2 * i], s->stream));
-        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
-    }
+    // forked scenes first, then the viscous ones on the batch stream, then the joins (a join enqueued before a
+    // viscous scene's steps would make them wait for the forked scene)
+    for (int pass = 0; pass < 3; ++pass)
+        for (int i = 0; i < S; ++i) {
+            fe_scene* s = b->scenes[i];
+            const cudaStream_t ps = pre_stream(b, s);
+            if (pass == 0 && ps != b->stream) {
+                FE_CUDA(cudaStreamWaitEvent(ps, fork0, 0));
+                fe_status st = enqueue_steps(s, dt, kStepSort, kStepRhs, ps);
+                if (st != FE_OK) return st;
+                FE_CUDA(cudaEventRecord(b->events[2 * i], ps));
+            } else if (pass == 1 && ps == b->stream) {
+                fe_status st = enqueue_steps(s, dt, kStepSort, kStepRhs, ps);
+                if (st != FE_OK) return st;
+            } else if (pass == 2 && ps != b->stream) {
+                FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
+            }
+        }
     FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
     FE_CUDA(cudaEventRecord(fork1, b->stream));
     for (int i = 0; i < S; ++i) {
@@ -1169,14 +1289,19 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = null
     cudaEvent_t fork0 = b->events[2 * S], fork1 = b->events[2 * S + 1];
     if (ev) FE_CUDA(cudaEventRecord(ev[0], b->stream));
     FE_CUDA(cudaEventRecord(fork0, b->stream));
-    for (int i = 0; i < S; ++i) {
-        fe_scene* s = b->scenes[i];
-        FE_CUDA(cudaStreamWaitEvent(s->stream, fork0, 0));
-        FE_CUDA(cudaGraphLaunch(s->graph[s->parity][0], s->stream));
-        g_launches += s->graph_kernels[s->parity][0];
-        FE_CUDA(cudaEventRecord(b->events[2 * i], s->stream));
-        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
-    }
+    for (int pass = 0; pass < 3; ++pass)  // forked scenes, viscous scenes on the batch stream, joins
+        for (int i = 0; i < S; ++i) {
+            fe_scene* s = b->scenes[i];
+            const cudaStream_t ps = pre_stream(b, s);
+            if ((pass == 0 && ps != b->stream) || (pass == 1 && ps == b->stream)) {
+                if (pass == 0) FE_CUDA(cudaStreamWaitEvent(ps, fork0, 0));
+                FE_CUDA(cudaGraphLaunch(s->graph[s->parity][0], ps));
+                g_launches += s->graph_kernels[s->parity][0];
+                if (pass == 0) FE_CUDA(cudaEventRecord(b->events[2 * i], ps));
+            } else if (pass == 2 && ps != b->stream) {
+                FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
+            }
+        }
     if (ev) FE_CUDA(cudaEventRecord(ev[1], b->stream));
     FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
     if (ev) FE_CUDA(cudaEventRecord(ev[2], b->stream));
@@ -1427,9 +1552,12 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
             ++b->steps_done;
             continue;
         }
-        if (b->graph_dt != dt) {
+        uint64_t epoch = 0;
+        for (const fe_scene* s : b->scenes) epoch += s->epoch;
+        if (b->graph_dt != dt || b->graph_epoch != epoch) {
             batch_drop_graphs(b);
             b->graph_dt = dt;
+            b->graph_epoch = epoch;
         }
         const int par = b->parity;
         if (!b->graph[par]) {

@@ -18,7 +18,7 @@ class Scene:
 
     def __init__(self, n, solver=_abi.FLIP, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), flip_blend=0.05,
                  gravity=(0.0, -9.81, 0.0), max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-4,
-                 max_refine=12, device=0, max_particles=0, pressure_solver=_abi.AUTO):
+                 max_refine=12, device=0, max_particles=0, pressure_solver=_abi.AUTO, viscosity=0.0):
         L = _abi.lib()
         d = _abi.SceneDesc()
         check(L.fe_scene_desc_default(ctypes.byref(d)))
@@ -30,6 +30,7 @@ class Scene:
         d.solver, d.flip_blend, d.max_cfl = solver, flip_blend, max_cfl
         d.cg_rel_tol, d.cg_max_it, d.cg_inner_tol, d.max_refine = cg_rel_tol, cg_max_it, cg_inner_tol, max_refine
         d.device, d.max_particles, d.pressure_solver = device, max_particles, pressure_solver
+        d.viscosity = viscosity
         h = ctypes.c_void_p()
         check(L.fe_scene_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
@@ -154,6 +155,18 @@ class Scene:
         s = np.zeros((nz, ny, nx), dtype=np.float64)
         check(self._L.fe_scene_get_fluid_sdf(self._h, ptr(s)))
         return s
+
+    def set_viscosity(self, viscosity):
+        check(self._L.fe_scene_set_viscosity(self._h, float(viscosity)))
+        self.desc.viscosity = float(viscosity)
+
+    def diffusion(self):
+        """(Jacobi iterations per component, (mu, mv, mw) FLUID face markers) of the last viscosity solve."""
+        its = np.zeros(3, dtype=np.int32)
+        su, sv, sw = face_shapes(self.n)
+        a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
+        check(self._L.fe_scene_get_diffusion(self._h, ptr(its), ptr(a), ptr(b), ptr(c)))
+        return tuple(int(x) for x in its), (a, b, c)
 
     def sort_result(self):
         N = self.num_particles()

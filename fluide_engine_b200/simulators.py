@@ -5,7 +5,7 @@ Same class and method names as the reference's pybind11 module PyFluidEngine
 bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp) and C++ classes (pic_simulator.hpp:27-43,
 hybrid_simulator.hpp:10-41, physics_animation.hpp:8-19, flip_simulator.hpp:9-16), backed by one
 device-resident Scene.  Only what the substep needs is implemented; entry points of components outside
-it (mesh initialisation, colliders, emitters, viscosity, surface extraction) raise NotImplementedError
+it (mesh initialisation, colliders, emitters, surface extraction) raise NotImplementedError
 with the reason instead of silently doing something else.
 """
 import numpy as np
@@ -127,9 +127,14 @@ class HybridSimulator:
         return self._viscosity
 
     def SetViscosity(self, viscosity):
-        if viscosity != 0.0:
-            raise NotImplementedError("viscosity (BackwardEulerDiffusionSolver) is outside the substep path")
-        self._viscosity = 0.0
+        """HybridSimulator::SetViscosity (hybrid_simulator.cpp:97-100): > 0 runs ComputeDiffusion every substep
+        (pic_simulator.cpp:214-222) with the reference's BackwardEulerDiffusionSolver settings."""
+        viscosity = float(viscosity)
+        if not viscosity >= 0.0:
+            raise ValueError("viscosity must be >= 0")
+        self._viscosity = viscosity
+        if self._scene is not None:
+            self._scene.set_viscosity(viscosity)
 
     def GetDensity(self):
         return self._density
@@ -248,7 +253,7 @@ class HybridSimulator:
         if self._scene is None:
             self._scene = Scene(self._n, solver=self._solver, origin=self._origin, size=self._size,
                                 flip_blend=self._blend, gravity=self._gravity(), max_cfl=self._maxCfl,
-                                device=self._device, **self._cg)
+                                device=self._device, viscosity=self._viscosity, **self._cg)
             if self._pending is not None:
                 p, v, c = self._pending
                 self._scene.set_particles(p, v, c)

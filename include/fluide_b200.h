@@ -55,6 +55,7 @@ typedef struct {
     int32_t device;          /* CUDA device ordinal */
     uint64_t max_particles;  /* capacity; 0 = sized by the first fe_scene_set_particles */
     int32_t pressure_solver; /* fe_pressure_solver: how the inner FP32 solve runs (same system, same FP64 test) */
+    double viscosity;        /* kinematic viscosity (HybridSimulator::SetViscosity); 0 = none, the reference default */
 } fe_scene_desc;
 
 /* Inner solver of the pressure projection.  Both solve the reference's system
@@ -85,11 +86,12 @@ typedef enum {
     FE_STAGE_P2G = 1,        /* TransferParticles2Grid (pic :356-437, flip :25-119, apic :15-118) */
     FE_STAGE_MARK = 2,       /* BuildSignedDistanceField + BuildMarkers (pic :452-475, single_phase :30-48) */
     FE_STAGE_PRE = 3,        /* ExtrapolateVelocityToAir + BC + gravity + BC (pic :186-212) */
-    FE_STAGE_PRESSURE = 4,   /* BuildSystem + CG + ApplyPressure + BC (pic :224-229) */
-    FE_STAGE_POST = 5,       /* ExtrapolateVelocityToAir + BC (pic :233-234) */
-    FE_STAGE_G2P = 6,        /* TransferGrid2Particles (pic :439-450, flip :121-161, apic :120-176) */
-    FE_STAGE_MOVE = 7,       /* MoveParticles (pic :239-312) */
-    FE_STAGE_COUNT = 8
+    FE_STAGE_DIFFUSE = 4,    /* ComputeDiffusion: backward Euler viscosity + BC (pic :214-222); no-op at viscosity 0 */
+    FE_STAGE_PRESSURE = 5,   /* BuildSystem + CG + ApplyPressure + BC (pic :224-229) */
+    FE_STAGE_POST = 6,       /* ExtrapolateVelocityToAir + BC (pic :233-234) */
+    FE_STAGE_G2P = 7,        /* TransferGrid2Particles (pic :439-450, flip :121-161, apic :120-176) */
+    FE_STAGE_MOVE = 8,       /* MoveParticles (pic :239-312) */
+    FE_STAGE_COUNT = 9
 } fe_stage;
 
 /* Fills *d with the reference defaults (maxCfl 3 from hybrid_simulator.cpp:21, blend 0.05 from
@@ -159,6 +161,18 @@ fe_status fe_scene_get_rhs(fe_scene* s, double* b);
 /* Band-limited particle SDF on the cell-centred grid (HybridSimulator::GetFluidSdf, hybrid_simulator.cpp:82-85,
  * as built by PICSimulator::BuildSignedDistanceField, pic_simulator.cpp:452-475), FP64. */
 fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf);
+/* Viscosity (HybridSimulator::SetViscosity, hybrid_simulator.cpp:97-100), settable at any time.  When it is > 0
+ * every substep runs ComputeDiffusion (pic_simulator.cpp:214-222) after the external forces: the reference's
+ * BackwardEulerDiffusionSolver (fluid_solvers/backward_euler_diffusion_solver.cpp:20-242) -- per component, faces
+ * whose fluid-SDF sample is < 0 are FLUID and (1 + sum c) u' - c sum u'_nbr = u with c = viscosity dt / h^2 is
+ * relaxed by the Jacobi iteration of CudaJacobiIterationSolver(1000, 5, 1e-14) -- in FP64 with the reference's
+ * operation order, then the wall layers are zeroed.  The first call with a viscosity > 0 allocates the solve's
+ * buffers (about 48 bytes per cell). */
+fe_status fe_scene_set_viscosity(fe_scene* s, double viscosity);
+/* Last viscosity solve: Jacobi iterations per component (3 int32, 1000 = the cap) and the FLUID face markers
+ * of each component (BackwardEulerDiffusionSolver::_fluidMarkers, face-array layout).  Any pointer may be
+ * NULL; FE_ERR_STATE if the scene never had a viscosity > 0. */
+fe_status fe_scene_get_diffusion(fe_scene* s, int32_t* iterations, uint8_t* mu, uint8_t* mv, uint8_t* mw);
 /* Sorted cell keys and the permutation of the last sort (slot -> particle id), n entries each. */
 fe_status fe_scene_get_sort(fe_scene* s, uint32_t* keys, uint32_t* perm, uint64_t n);
 /* Post-projection ||div u||_2 over FLUID cells of the current grid (FP64). */

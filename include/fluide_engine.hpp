@@ -7,7 +7,7 @@
 // DirectionalField (forces/directional_field.hpp) and Vector3 (common/vector3.hpp), with the same names
 // and argument meaning.  State lives on the GPU in one fe_scene (include/fluide_b200.h), created on the
 // first step after particles exist.  Entry points of components outside the substep (mesh seeding,
-// colliders, emitters, viscosity, surface extraction) throw std::logic_error saying so; errors of the
+// colliders, emitters, surface extraction) throw std::logic_error saying so; errors of the
 // library throw fluide::Error carrying the fe_status.  Header-only; link with libfluide_b200.so.
 #ifndef FLUIDE_ENGINE_HPP
 #define FLUIDE_ENGINE_HPP
@@ -156,7 +156,7 @@ class HybridSimulator : public PhysicsAnimation {
         return c;
     }
     double MaxCfl() const { return _desc.max_cfl; }
-    double GetViscosity() const { return 0.0; }
+    double GetViscosity() const { return _desc.viscosity; }
     double GetDensity() const { return _density; }
     size_t GetParticlesPerBlock() const { return _particlesPerBlok; }
     Vector3<double> GetOrigin() const { return _domain.GetOrigin(); }
@@ -174,9 +174,13 @@ class HybridSimulator : public PhysicsAnimation {
         return (size_t)n;
     }
     void SetMaxClf(double maxCfl) { Reconfigure([&] { _desc.max_cfl = maxCfl; }); }
+    // HybridSimulator::SetViscosity (hybrid_simulator.cpp:97-100): > 0 adds ComputeDiffusion to every substep
+    // (pic_simulator.cpp:214-222), the reference's BackwardEulerDiffusionSolver with its Jacobi settings.
     void SetViscosity(double viscosity)
     {
-        if (viscosity != 0.0) throw std::logic_error("viscosity (BackwardEulerDiffusionSolver) is outside the substep path");
+        if (_scene) fluide::check(fe_scene_set_viscosity(_scene, viscosity));
+        else if (!(viscosity >= 0.0) || !std::isfinite(viscosity)) throw std::invalid_argument("viscosity must be >= 0");
+        _desc.viscosity = viscosity;
     }
     void SetDensity(double density) { _density = density; }  // unused by the projection, as in the reference
     void SetParticlesPerBlock(size_t n) { _particlesPerBlok = n; }

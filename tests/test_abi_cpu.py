@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_string():
     L = fe.lib()
-    assert L.fe_abi_version() == 10100
+    assert L.fe_abi_version() == 10200
     assert isinstance(L.fe_last_error(), bytes)
 
 
@@ -79,5 +79,7 @@ def test_python_mirror_api_without_device():
     assert tuple(sim.GetGridSpacing()) == (1 / 16, 1 / 16, 1 / 16)
     with pytest.raises(NotImplementedError):
         sim.AddCollider(object())
-    with pytest.raises(NotImplementedError):
-        sim.SetViscosity(0.1)
+    sim.SetViscosity(0.1)  # kept until the scene exists (no device here)
+    assert sim.GetViscosity() == 0.1
+    with pytest.raises(ValueError):
+        sim.SetViscosity(-1.0)

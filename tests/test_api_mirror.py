@@ -54,8 +54,10 @@ def test_reference_construction_sequence_without_device():
     assert sim.InitializeFromRegions([dict(kind=0, lo=(0, 0, 0), hi=(0.4, 0.6, 1.0))]) == 13 * 19 * 32
     g = sim.GetGridSpacing()
     assert (g.x, g.y, g.z) == (1 / 16, 1 / 16, 1 / 16)
-    with pytest.raises(RuntimeError):
-        sim.SetViscosity(0.5)
+    sim.SetViscosity(0.5)  # HybridSimulator::SetViscosity; the scene is created on the first step
+    assert sim.GetViscosity() == 0.5
+    with pytest.raises((ValueError, RuntimeError)):
+        sim.SetViscosity(-0.5)
     with pytest.raises(RuntimeError):
         sim.AddCollider(None)
 
