@@ -189,8 +189,9 @@ struct DiffWork {
     uint8_t* mark;                  // faces: FE_CELL_FLUID / FE_CELL_AIR (BackwardEulerDiffusionSolver::_fluidMarkers)
     unsigned long long* list;       // FLUID faces: (face << 9) | (wall << 8) | (component << 6) | FLUID-neighbour mask
     double* x[2];                   // faces: Jacobi iterates (only FLUID entries are used)
+    double* snap;                   // faces: an earlier iterate, for the exact early exit
     unsigned* count;                // [0]: list length
-    int* its;                       // [3]: Jacobi iterations of the last solve, per component
+    int* its;                       // [4]: Jacobi iterations of the last solve per component, relaxation passes run
     int* tab_i0;                    // [component][axis][index]: GetBarycentric index of each face coordinate
     double* tab_f;                  // same layout: GetBarycentric fraction
     int tab_stride;                 // max(nx, ny, nz) + 1 entries per (component, axis)

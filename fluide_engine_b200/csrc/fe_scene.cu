@@ -236,10 +236,11 @@ fe_status alloc_diffusion(fe_scene* s)
     FE_CUDA(dalloc(L, &d.list, nf, dev, st));
     FE_CUDA(dalloc(L, &d.x[0], nf, dev, st));
     FE_CUDA(dalloc(L, &d.x[1], nf, dev, st));
+    FE_CUDA(dalloc(L, &d.snap, nf, dev, st));
     FE_CUDA(dalloc(L, &d.count, 1, dev, st));
     FE_CUDA(cudaMemsetAsync(d.count, 0, sizeof(unsigned), st));
-    FE_CUDA(dalloc(L, &d.its, 3, dev, st));
-    FE_CUDA(cudaMemsetAsync(d.its, 0, 3 * sizeof(int), st));
+    FE_CUDA(dalloc(L, &d.its, 4, dev, st));
+    FE_CUDA(cudaMemsetAsync(d.its, 0, 4 * sizeof(int), st));
     d.tab_stride = std::max(n[0], std::max(n[1], n[2])) + 1;
     std::vector<int> ti0((size_t)9 * d.tab_stride, 0);
     std::vector<double> tf((size_t)9 * d.tab_stride, 0.0);
@@ -1107,7 +1108,7 @@ fe_status fe_scene_get_diffusion(fe_scene* s, int32_t* iterations, uint8_t* mu, 
     if (!s->diff_ready) return set_error(FE_ERR_STATE, "the scene has never had a viscosity > 0");
     const int nx = s->base.g.nx, ny = s->base.g.ny, nz = s->base.g.nz;
     const size_t nu = (size_t)(nx + 1) * ny * nz, nv = (size_t)nx * (ny + 1) * nz, nw = (size_t)nx * ny * (nz + 1);
-    if (iterations) FE_CUDA(cudaMemcpyAsync(iterations, s->diff.its, 3 * sizeof(int32_t), cudaMemcpyDefault, s->stream));
+    if (iterations) FE_CUDA(cudaMemcpyAsync(iterations, s->diff.its, 4 * sizeof(int32_t), cudaMemcpyDefault, s->stream));
     if (mu) FE_CUDA(cudaMemcpyAsync(mu, s->diff.mark, nu, cudaMemcpyDefault, s->stream));
     if (mv) FE_CUDA(cudaMemcpyAsync(mv, s->diff.mark + nu, nv, cudaMemcpyDefault, s->stream));
     if (mw) FE_CUDA(cudaMemcpyAsync(mw, s->diff.mark + nu + nv, nw, cudaMemcpyDefault, s->stream));

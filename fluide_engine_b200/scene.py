@@ -162,11 +162,15 @@ class Scene:
 
     def diffusion(self):
         """(Jacobi iterations per component, (mu, mv, mw) FLUID face markers) of the last viscosity solve."""
-        its = np.zeros(3, dtype=np.int32)
+        return self.diffusion_info()[:2]
+
+    def diffusion_info(self):
+        """As diffusion(), plus the relaxation passes the GPU ran."""
+        its = np.zeros(4, dtype=np.int32)
         su, sv, sw = face_shapes(self.n)
         a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
         check(self._L.fe_scene_get_diffusion(self._h, ptr(its), ptr(a), ptr(b), ptr(c)))
-        return tuple(int(x) for x in its), (a, b, c)
+        return tuple(int(x) for x in its[:3]), (a, b, c), int(its[3])
 
     def sort_result(self):
         N = self.num_particles()

@@ -169,9 +169,11 @@ fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf);
  * operation order, then the wall layers are zeroed.  The first call with a viscosity > 0 allocates the solve's
  * buffers (about 48 bytes per cell). */
 fe_status fe_scene_set_viscosity(fe_scene* s, double viscosity);
-/* Last viscosity solve: Jacobi iterations per component (3 int32, 1000 = the cap) and the FLUID face markers
- * of each component (BackwardEulerDiffusionSolver::_fluidMarkers, face-array layout).  Any pointer may be
- * NULL; FE_ERR_STATE if the scene never had a viscosity > 0. */
+/* Last viscosity solve: iterations[0..2] = the reference's Jacobi iterations per component (1000 = the cap),
+ * iterations[3] = relaxation passes the GPU ran (fewer than 1000 when every component's iterates became
+ * periodic, after which iterate 1000 is known without running to it); and the FLUID face markers of each
+ * component (BackwardEulerDiffusionSolver::_fluidMarkers, face-array layout).  Any pointer may be NULL;
+ * FE_ERR_STATE if the scene never had a viscosity > 0. */
 fe_status fe_scene_get_diffusion(fe_scene* s, int32_t* iterations, uint8_t* mu, uint8_t* mv, uint8_t* mw);
 /* Sorted cell keys and the permutation of the last sort (slot -> particle id), n entries each. */
 fe_status fe_scene_get_sort(fe_scene* s, uint32_t* keys, uint32_t* perm, uint64_t n);
