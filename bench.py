@@ -31,14 +31,18 @@ BOX = (0.0, 0.0, 0.0, 0.4, 0.6, 1.0)
 DT = 1.0 / 240.0
 
 
-def workload_config(n, steps, warmup, n_gpus, np_):
-    return {
+def workload_config(n, steps, warmup, n_gpus, np_, viscosity=0.0):
+    cfg = {
         "workload": "FLIP dam break %d^3, box [0,0.4]x[0,0.6]x[0,1], 8 particles/cell (seed 0), dt=1/240, "
-                    "FP32 CG in FP64 refinement to rel 1e-6" % n,
+                    "FP32 CG in FP64 refinement to rel 1e-6" % n + (", viscosity %g (backward Euler, Jacobi "
+                                                                    "1000/5/1e-14)" % viscosity if viscosity else ""),
         "grid": [n, n, n], "particles": np_, "solver": "FLIP 0.95", "dt": DT, "cg_rel_tol": 1e-6, "max_cfl": 1.0,
         "substeps_timed": steps, "warmup": warmup, "parallelism": "replicas x%d" % n_gpus,
         "l2": "working set > 126 MB L2 (particles alone %.0f MB); no flush" % (np_ * 24 / 1e6),
     }
+    if viscosity:
+        cfg["viscosity"] = viscosity
+    return cfg
 
 
 def max_over_ranks(x, device):
@@ -153,7 +157,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def reference_sample(n, steps, cores_hint=None):
+def reference_sample(n, steps, cores_hint=None, viscosity=0.0):
     """Times the reference's own threaded CPU simulator on the workload; returns (value, info)."""
     import numpy as np
     import oracle
@@ -162,11 +166,13 @@ def reference_sample(n, steps, cores_hint=None):
     pos, vel = oracle.seed_regions([dict(kind=0, lo=BOX[:3], hi=BOX[3:])], (n, n, n), (0, 0, 0), (1, 1, 1), 0)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     if variant:
-        sim = oracle.RefSim((n, n, n), oracle.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=500, variant=variant)
+        sim = oracle.RefSim((n, n, n), oracle.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=500, variant=variant,
+                            viscosity=viscosity)
         kind = "reference"
         threads = os.cpu_count()  # std::thread::hardware_concurrency() threads per parallel loop
     else:
-        sim = oracle.OracleSim((n, n, n), oracle.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=500)
+        sim = oracle.OracleSim((n, n, n), oracle.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=500,
+                               viscosity=viscosity)
         kind = "port"
         threads = 1
     sim.set_particles(pos.astype(np.float64), vel.astype(np.float64))
@@ -178,9 +184,45 @@ def reference_sample(n, steps, cores_hint=None):
     total = sum(times)
     value = pos.shape[0] * steps / total
     info = {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
-            "sample": "%d substep(s) of the %d^3 FLIP dam break from rest (%d particles), %.1f s; host has %d cores"
-                      % (steps, n, pos.shape[0], total, cores)}
+            "sample": "%d substep(s) of the %d^3 FLIP dam break from rest (%d particles)%s, %.1f s; host has %d cores"
+                      % (steps, n, pos.shape[0], ", viscosity %g" % viscosity if viscosity else "", total, cores)}
     return value, total / steps * 1e3, info
+
+
+# Algorithmic bytes of one Jacobi relaxation per FLUID face (k_jacobi): list entry 8 B + right-hand side 4 B +
+# iterate read 8 B (each neighbour value is read by its 6 neighbours, once per face algorithmically) + write 8 B.
+JACOBI_BYTES_PER_FACE = 28
+
+
+def diffusion_report(scene, stream, peak, peak_kind, reps=5):
+    """The viscosity stage on the scene's current state, timed alone (FE_STAGE_DIFFUSE: band-SDF scatter, face
+    markers, FLUID-face list, persistent Jacobi kernel), with the Jacobi kernel's relaxation count and an
+    algorithmic-bandwidth figure for it.  Runs after the timed region; the state it leaves is not used."""
+    import torch
+
+    import fluide_engine_b200 as fe
+
+    scene.run_stages(DT, fe.STAGE_SORT, fe.STAGE_PRE)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times, passes = [], []
+    for _ in range(reps):
+        ev0.record(stream)
+        scene.run_stages(DT, fe.STAGE_DIFFUSE, fe.STAGE_DIFFUSE)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+        its, marks, npass = scene.diffusion_info()
+        passes.append(npass)
+    faces = int(sum(int(m.sum()) for m in marks))
+    ms = sorted(times)[len(times) // 2]
+    npass = passes[times.index(ms)]
+    achieved = faces * npass * JACOBI_BYTES_PER_FACE / (ms / 1e3) / 1e9
+    return {"stage_ms": ms, "stage_ms_all": times, "jacobi_iterations": list(its), "relaxation_passes": npass,
+            "fluid_faces": faces,
+            "roofline": {"bound": "latency (one grid barrier per relaxation)", "kernel": "k_jacobi",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "note": "algorithmic bytes = FLUID faces x passes x %d B; the "
+                         "stage time includes the SDF scatter, face markers and list build" % JACOBI_BYTES_PER_FACE}}
 
 
 def run_reference_arm(args):
@@ -189,12 +231,12 @@ def run_reference_arm(args):
         return 0
     n_gpus = args.gpus
     steps = max(1, min(args.steps, args.ref_steps))
-    value, ms, info = reference_sample(args.n, steps)
+    value, ms, info = reference_sample(args.n, steps, viscosity=args.viscosity)
     particles = int(round(value * ms / 1e3))
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": n_gpus, "steps": steps, "warmup": 0,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded analytic scene)", "impl": "reference",
-            "config": workload_config(args.n, steps, 0, 1, particles), "cpu_baseline": info,
+            "config": workload_config(args.n, steps, 0, 1, particles, args.viscosity), "cpu_baseline": info,
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -437,6 +479,8 @@ def main():
                     help="inner pressure solver: auto (multigrid-preconditioned CG from 2^22 cells, plain CG below), "
                          "mgpcg or cg")
     ap.add_argument("--workload", default="single", choices=["single", "batched", "served", "pool256"])
+    ap.add_argument("--viscosity", type=float, default=0.0,
+                    help="single workload / reference arm: kinematic viscosity (0 = none, as the benchmark scenes)")
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
     # served: 20 jobs/s as the served configuration, over 6 s instead of 10 min and with resolutions <= 128 so
     # that a run takes tens of seconds; the work still exceeds the arrival window several times (saturated)
@@ -477,7 +521,8 @@ def main():
     pos, vel = fe.seed_regions([dict(kind=0, lo=BOX[:3], hi=BOX[3:])], (n, n, n), (0, 0, 0), (1, 1, 1), 0)
     N = pos.shape[0]
     scene = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_inner_tol=args.cg_inner_tol,
-                     device=local, pressure_solver={"auto": fe.AUTO, "mgpcg": fe.MGPCG, "cg": fe.CG}[args.pressure_solver])
+                     device=local, pressure_solver={"auto": fe.AUTO, "mgpcg": fe.MGPCG, "cg": fe.CG}[args.pressure_solver],
+                     viscosity=args.viscosity)
     stream = torch.cuda.Stream()
     scene.set_stream(stream.cuda_stream)
     scene.set_particles(pos, vel)
@@ -515,6 +560,7 @@ def main():
     units = fluid * (its + refs + 1.0)
     traffic = float(per_unit * units.mean()) if per_unit else None
     phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
+    diffusion = diffusion_report(scene, stream, peak, peak_kind) if args.viscosity > 0 else None
 
     # end to end through the public API with host buffers: H2D particles, one substep, D2H particles
     pin_pos = torch.from_numpy(pos).pin_memory()
@@ -541,7 +587,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            _, _, cpu = reference_sample(n, args.ref_steps)
+            _, _, cpu = reference_sample(n, args.ref_steps, viscosity=args.viscosity)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": METRIC, "cores": None, "kind": "unavailable", "sample": str(ex)[:200]}
 
@@ -550,7 +596,7 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded analytic scene)",
-            "config": workload_config(n, args.steps, args.warmup, world, N),
+            "config": workload_config(n, args.steps, args.warmup, world, N, args.viscosity),
             "roofline": {"bound": "hbm",
                          "kernel": ("k_mgcg (persistent multigrid-preconditioned FP32 CG + FP64 refinement, one "
                                     "launch/substep)" if multigrid else
@@ -577,6 +623,8 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        if diffusion:
+            line["diffusion"] = diffusion
         print(json.dumps(line), flush=True)
     scene.close()
     if world > 1:

@@ -18,6 +18,8 @@
 // node value is within ~1e-15 r of zero; such "critical" cells are listed and re-evaluated with the full
 // band SDF and the reference's trilinear sample by k_mark_fixup.  The result is byte-identical to the
 // reference in every case.
+#include <cmath>
+
 #include "fe_internal.cuh"
 
 namespace fe {
@@ -169,11 +171,15 @@ __global__ void k_fluid_sdf(SceneView v, double R2, double* out)
 
 
 // One thread per particle: every SDF node within the band 2r of the particle that the reference's hash search
-// would visit from that node and whose squared distance is <= (2r)^2 takes the minimum of the distance.  The
-// distances are non-negative doubles, whose bit patterns order like their values, so a 64-bit atomicMin on the
-// bits builds the same per-node minimum as the gather of node_sdf (the node's value is min(2r, that) - r).
-// Particles sorted by cell hit the same nodes as their neighbours; a plain read of the current minimum first
-// (it only ever decreases, so a stale value is still an upper bound) skips most atomics.
+// would visit from that node and whose squared distance is <= (2r)^2 takes the minimum of that squared distance.
+// The node's reference value is min(2r, min over those particles of |p - c|) - r; correctly rounded sqrt is
+// monotonic, so min |p - c| = sqrt(min |p - c|^2) exactly, and the square root is taken once per node when the
+// markers are sampled.  Squared distances are non-negative doubles, whose bit patterns order like their values,
+// so a 64-bit atomicMin on the bits takes the minimum.  Each squared distance is summed in the reference's order,
+// (dx^2 + dy^2) + dz^2; a row whose dy^2 + dz^2 already exceeds (2r)^2 is skipped (rounding is monotonic, so the
+// full sum would exceed it too), and the bucket test runs once per axis.  Particles sorted by cell hit the same
+// nodes as their neighbours; a plain read of the current minimum first (it only decreases, so a stale value is
+// still an upper bound) skips most atomics.
 __global__ void __launch_bounds__(256) k_sdf_scatter(SceneView v, unsigned long long* __restrict__ node, double R2)
 {
     uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -181,25 +187,37 @@ __global__ void __launch_bounds__(256) k_sdf_scatter(SceneView v, unsigned long 
     const double X[3] = {(double)v.px[p], (double)v.py[p], (double)v.pz[p]};
     const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
     const double inv_bucket = 1.0 / v.bucket;
-    int lo[3], hi[3], pb[3];
+    int lo[3], hi[3];
+    unsigned long long pass[3];  // bit u: candidate node lo + u is in a bucket the node's search visits
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         // nodes i with |q_i - x| <= 2r, widened by 1e-6 h (the exact test below decides)
         const double t = (X[a] - v.sdf_origin[a]) * v.inv_h[a];
         const double rr = v.band * v.inv_h[a] + 1e-6;
         lo[a] = max((int)floor(t - rr) + 1, 0);
-        hi[a] = min((int)floor(t + rr), n[a] - 1);
-        pb[a] = bucket_fast(X[a], v.bucket, inv_bucket);
+        hi[a] = min(min((int)floor(t + rr), n[a] - 1), lo[a] + 63);  // 2r spans at most 64 nodes per axis
+        const int pb = bucket_fast(X[a], v.bucket, inv_bucket);
+        pass[a] = 0ull;
+        for (int i = lo[a]; i <= hi[a]; ++i)
+            if (pb == v.q_b0[a][i] || pb == v.q_b1[a][i]) pass[a] |= 1ull << (i - lo[a]);
     }
+    const double* qx = v.q_pos[0];
     for (int k = lo[2]; k <= hi[2]; ++k) {
-        if (pb[2] != v.q_b0[2][k] && pb[2] != v.q_b1[2][k]) continue;
+        if (!((pass[2] >> (k - lo[2])) & 1ull)) continue;
+        const double dz = __dsub_rn(X[2], v.q_pos[2][k]);
+        const double dz2 = __dmul_rn(dz, dz);
+        if (!(dz2 <= R2)) continue;
         for (int j = lo[1]; j <= hi[1]; ++j) {
-            if (pb[1] != v.q_b0[1][j] && pb[1] != v.q_b1[1][j]) continue;
+            if (!((pass[1] >> (j - lo[1])) & 1ull)) continue;
+            const double dy = __dsub_rn(X[1], v.q_pos[1][j]);
+            const double dy2 = __dmul_rn(dy, dy);
+            if (!(__dadd_rn(dy2, dz2) <= R2)) continue;
             for (int i = lo[0]; i <= hi[0]; ++i) {
-                if (pb[0] != v.q_b0[0][i] && pb[0] != v.q_b1[0][i]) continue;
-                const double d2 = dist2_ref(X[0], X[1], X[2], v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]);
+                if (!((pass[0] >> (i - lo[0])) & 1ull)) continue;
+                const double dx = __dsub_rn(X[0], qx[i]);
+                const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), dy2), dz2);  // dist2_ref's order
                 if (!(d2 <= R2)) continue;
-                const unsigned long long bits = (unsigned long long)__double_as_longlong(__dsqrt_rn(d2));
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
                 unsigned long long* cell = node + idx3(i, j, k, n[0], n[1]);
                 if (bits < __ldcg(cell)) atomicMin(cell, bits);
             }
@@ -223,11 +241,16 @@ __global__ void k_face_mark(SceneView v, DiffWork d)
     const double fx = d.tab_f[base + fc.i], fy = d.tab_f[base + d.tab_stride + fc.j];
     const double fz = d.tab_f[base + 2 * d.tab_stride + fc.k];
     const int ip = min(i0 + 1, nx - 1), jp = min(j0 + 1, ny - 1), kp = min(k0 + 1, nz - 1);
-    const unsigned long long band = (unsigned long long)__double_as_longlong(v.band);
     const unsigned long long* __restrict__ node = d.node_dist;
+    // node value min(2r, sqrt(smallest squared distance)) - r (all ones: no particle within the band)
     auto val = [&](int i, int j, int k) {
-        const unsigned long long b = min(__ldg(node + idx3(i, j, k, nx, ny)), band);
-        return __dsub_rn(__longlong_as_double((long long)b), v.radius);
+        const unsigned long long raw = __ldg(node + idx3(i, j, k, nx, ny));
+        double m = v.band;
+        if (raw != ~0ull) {
+            const double dm = __dsqrt_rn(__longlong_as_double((long long)raw));
+            if (dm < m) m = dm;
+        }
+        return __dsub_rn(m, v.radius);
     };
     const double c000 = val(i0, j0, k0), c100 = val(ip, j0, k0), c010 = val(i0, jp, k0), c110 = val(ip, jp, k0);
     const double c001 = val(i0, j0, kp), c101 = val(ip, j0, kp), c011 = val(i0, jp, kp), c111 = val(ip, jp, kp);

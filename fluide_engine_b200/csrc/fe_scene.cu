@@ -222,6 +222,9 @@ fe_status alloc_diffusion(fe_scene* s)
 {
     if (s->diff_ready) return FE_OK;
     const SceneView& v = s->base;
+    for (int a = 0; a < 3; ++a)  // k_sdf_scatter keeps the candidate nodes of one axis in a 64-bit mask
+        if (2.0 * v.band * v.inv_h[a] + 2.0 > 64.0)
+            return set_error(FE_ERR_BAD_ARG, "cells too anisotropic for the viscosity solve (max(h) / h > 18)");
     const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
     const size_t nc = (size_t)n[0] * n[1] * n[2];
     const size_t nf = (size_t)(n[0] + 1) * n[1] * n[2] + (size_t)n[0] * (n[1] + 1) * n[2] +
