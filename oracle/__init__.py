@@ -25,7 +25,8 @@ def build_oracle(force=False):
     """Compiles fe_oracle.c into liboracle.so (FP64, no FMA contraction)."""
     srcs = [os.path.join(HERE, "fe_oracle.c"), os.path.join(HERE, "fe_oracle.h"),
             os.path.join(HERE, "..", "fluide_engine_b200", "csrc", "fe_keys.h"),
-            os.path.join(HERE, "..", "fluide_engine_b200", "csrc", "fe_seed.h")]
+            os.path.join(HERE, "..", "fluide_engine_b200", "csrc", "fe_seed.h"),
+            os.path.join(HERE, "..", "fluide_engine_b200", "csrc", "fe_mc_tables.h")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(s) for s in srcs):
         return LIB
     cmd = ["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fPIC", "-shared", "-o", LIB,
@@ -103,6 +104,12 @@ def lib():
         F = ctypes.POINTER(ctypes.c_float)
         U32 = ctypes.POINTER(ctypes.c_uint32)
         L.or_sort_keys.argtypes = [F, ctypes.c_size_t, I3, F, F, U32, U32]
+        I64 = ctypes.POINTER(ctypes.c_int64)
+        SZ = ctypes.POINTER(ctypes.c_size_t)
+        L.or_build_surface.restype = ctypes.c_int
+        L.or_build_surface.argtypes = [D, I3, D, D, D, D, I64, ctypes.c_size_t, ctypes.c_size_t, SZ, SZ]
+        L.or_write_obj.restype = ctypes.c_int
+        L.or_write_obj.argtypes = [ctypes.c_char_p, ctypes.c_char_p, D, D, ctypes.c_size_t, I64, ctypes.c_size_t]
         L.or_seed_regions.restype = ctypes.c_size_t
         L.or_seed_regions.argtypes = [ctypes.c_void_p, ctypes.c_int, I3, D, D, ctypes.c_uint64, F, F, ctypes.c_size_t]
         _lib = L
@@ -279,6 +286,32 @@ class OracleSim:
         return self.L.or_divergence_l2(self.h)
 
 
+def build_surface(sdf, n, origin, h):
+    """MarchingCubesSolver::BuildSurface on a node grid (numpy (nz, ny, nx)); returns (vertices (V,3), normals (V,3),
+    triangles (T,4) int64: vertex ids and normal id)."""
+    L = lib()
+    sdf = np.ascontiguousarray(sdf, dtype=np.float64)
+    n3 = np.array(n, dtype=np.int32)
+    o = np.array(origin, dtype=np.float64)
+    hh = np.array(h, dtype=np.float64)
+    nv, nt = ctypes.c_size_t(), ctypes.c_size_t()
+    I64 = ctypes.POINTER(ctypes.c_int64)
+    assert L.or_build_surface(dptr(sdf), iptr(n3), dptr(o), dptr(hh), None, None, None, 0, 0, ctypes.byref(nv),
+                              ctypes.byref(nt)) == 0
+    V = np.zeros((nv.value, 3)); N = np.zeros((nv.value, 3)); T = np.zeros((nt.value, 4), dtype=np.int64)
+    assert L.or_build_surface(dptr(sdf), iptr(n3), dptr(o), dptr(hh), dptr(V), dptr(N), T.ctypes.data_as(I64),
+                              nv.value, nt.value, ctypes.byref(nv), ctypes.byref(nt)) == 0
+    return V, N, T
+
+
+def write_obj(path, name, V, N, T):
+    """OBJManager::Save of a mesh from build_surface."""
+    V, N = (np.ascontiguousarray(a, dtype=np.float64) for a in (V, N))
+    T = np.ascontiguousarray(T, dtype=np.int64)
+    assert lib().or_write_obj(path.encode(), name.encode(), dptr(V), dptr(N), V.shape[0],
+                              T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), T.shape[0]) == 0
+
+
 def project(n, h, marks, u, v, w, p, rel_tol=1e-6, max_it=500):
     """Standalone pressure projection (SinglePhasePressureSolver::Solve with CG); returns (its, rel residual)."""
     L = lib()
@@ -329,6 +362,11 @@ def ref_lib(variant="serial"):
             getattr(L, name).argtypes = [P, ctypes.c_double]
         L.ref_cfl.restype = ctypes.c_double
         L.ref_cfl.argtypes = [P, ctypes.c_double]
+        L.ref_set_sdf.argtypes = [P, D]
+        I64 = ctypes.POINTER(ctypes.c_int64)
+        SZ = ctypes.POINTER(ctypes.c_size_t)
+        L.ref_get_surface.argtypes = [P, D, D, I64, ctypes.c_size_t, ctypes.c_size_t, SZ, SZ]
+        L.ref_save_obj.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
         _ref_libs[variant] = L
     return _ref_libs[variant]
 
@@ -407,3 +445,20 @@ class RefSim:
 
     def advance_frame(self, dt):
         self.L.ref_advance_frame(self.h, dt)
+
+    def set_sdf(self, sdf):
+        sdf = np.ascontiguousarray(sdf, dtype=np.float64); self.L.ref_set_sdf(self.h, dptr(sdf))
+
+    def surface(self):
+        """PICSimulator::GetSurface into a fresh TriangleMesh: (vertices, normals, triangles (T,4) int64)."""
+        nv, nt = ctypes.c_size_t(), ctypes.c_size_t()
+        I64 = ctypes.POINTER(ctypes.c_int64)
+        self.L.ref_get_surface(self.h, None, None, None, 0, 0, ctypes.byref(nv), ctypes.byref(nt))
+        V = np.zeros((nv.value, 3)); N = np.zeros((nv.value, 3)); T = np.zeros((nt.value, 4), dtype=np.int64)
+        self.L.ref_get_surface(self.h, dptr(V), dptr(N), T.ctypes.data_as(I64), nv.value, nt.value, ctypes.byref(nv),
+                               ctypes.byref(nt))
+        return V, N, T
+
+    def save_obj(self, path, name):
+        """OBJManager::Save of the last surface()."""
+        self.L.ref_save_obj(self.h, path.encode(), name.encode())

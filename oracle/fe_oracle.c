@@ -10,6 +10,7 @@
 #include "fe_oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1139,4 +1140,263 @@ size_t or_seed_regions(const void* regions, int nreg, const int n[3], const doub
                        uint64_t seed, float* pos, float* vel, size_t cap)
 {
     return fe_seed_regions_host((const fe_region*)regions, nreg, n, origin, h, seed, pos, vel, cap);
+}
+
+/* ---------------------------------------------------------------- surface (marching cubes + OBJ) */
+
+#include "../fluide_engine_b200/csrc/fe_mc_tables.h"
+
+static const unsigned long long or_mc3d[256] = FE_MC_CASES_3D;
+static const unsigned long long or_mc2d[16] = FE_MC_CASES_2D;
+static const int or_mc_edge[12][2] = FE_MC_EDGE_CORNERS;
+
+typedef struct {
+    double *v, *n;    /* 3 per vertex */
+    int64_t* t;       /* 4 per triangle: vertices, normal index */
+    size_t nv, nt, cap_v, cap_t;
+    int64_t* map;     /* vertex map (MarchingCubeVertexMap): key -> vertex id, -1 = absent */
+    size_t map_size;
+} or_mesh;
+
+static void mesh_add_vertex(or_mesh* m, const double p[3], const double nrm[3])
+{
+    if (m->nv < m->cap_v) {
+        memcpy(m->v + 3 * m->nv, p, 3 * sizeof(double));
+        memcpy(m->n + 3 * m->nv, nrm, 3 * sizeof(double));
+    }
+    ++m->nv;
+}
+
+static void mesh_add_triangle(or_mesh* m, const int64_t f[3])
+{
+    if (m->nt < m->cap_t) {
+        int64_t* t = m->t + 4 * m->nt;
+        t[0] = f[0]; t[1] = f[1]; t[2] = f[2];
+        t[3] = (int64_t)m->nv - 1; /* mesh->GetNormals().size() - 1 */
+    }
+    ++m->nt;
+}
+
+/* MarchingCubesSolver::GlobalVertexId / GlobalEdgeId (marching_cubes_solver.cpp:157-181): keys on the doubled grid. */
+static size_t mc_key(int i, int j, int k, const int n[3], int ox, int oy, int oz)
+{
+    return ((size_t)(2 * k + oz) * 2 * (size_t)n[1] + (size_t)(2 * j + oy)) * 2 * (size_t)n[0] + (size_t)(2 * i + ox);
+}
+static const int mc_vertex_off[8][3] = {{0, 0, 0}, {2, 0, 0}, {2, 0, 2}, {0, 0, 2}, {0, 2, 0}, {2, 2, 0}, {2, 2, 2}, {0, 2, 2}};
+static const int mc_edge_off[12][3] = {{1, 0, 0}, {2, 0, 1}, {1, 0, 2}, {0, 0, 1}, {1, 2, 0}, {2, 2, 1},
+                                       {1, 2, 2}, {0, 2, 1}, {0, 1, 0}, {2, 1, 0}, {2, 1, 2}, {0, 1, 2}};
+
+static double sdfv(const double* s, const int n[3], int i, int j, int k) { return s[(size_t)i + (size_t)n[0] * ((size_t)j + (size_t)n[1] * (size_t)k)]; }
+
+/* MarchingCubesSolver::Gradient (marching_cubes_solver.cpp:116-155). */
+static void mc_gradient(const double* s, const int n[3], const double h[3], int i, int j, int k, double g[3])
+{
+    int ip = i + 1, im = i - 1, jp = j + 1, jm = j - 1, kp = k + 1, km = k - 1;
+    if (i > n[0] - 2) ip = i; else if (i == 0) im = 0;
+    if (j > n[1] - 2) jp = j; else if (j == 0) jm = 0;
+    if (k > n[2] - 2) kp = k; else if (k == 0) km = 0;
+    const double ih[3] = {1.0 / h[0], 1.0 / h[1], 1.0 / h[2]};
+    g[0] = 0.5 * ih[0] * (sdfv(s, n, ip, j, k) - sdfv(s, n, im, j, k));
+    g[1] = 0.5 * ih[1] * (sdfv(s, n, i, jp, k) - sdfv(s, n, i, jm, k));
+    g[2] = 0.5 * ih[2] * (sdfv(s, n, i, j, kp) - sdfv(s, n, i, j, km));
+}
+
+/* Grid3D::GridIndexToPosition (common/grid3d.hpp:20-23). */
+static void grid_pos(const double o[3], const double h[3], int i, int j, int k, double p[3])
+{
+    p[0] = o[0] + i * h[0];
+    p[1] = o[1] + j * h[1];
+    p[2] = o[2] + k * h[2];
+}
+
+static int64_t map_get(or_mesh* m, size_t key) { return key < m->map_size ? m->map[key] : -1; }
+static void map_put(or_mesh* m, size_t key, int64_t id) { if (key < m->map_size) m->map[key] = id; }
+
+/* SolveSingleCube (marching_cubes_solver.cpp:183-316), iso value 0. */
+static void mc_cube(const double* s, const int n[3], const double o[3], const double h[3], int i, int j, int k, or_mesh* m)
+{
+    static const int cof[8][3] = FE_MC_CORNER_OFFSETS;
+    double data[8], nrm[8][3];
+    for (int c = 0; c < 8; ++c) {
+        data[c] = sdfv(s, n, i + cof[c][0], j + cof[c][1], k + cof[c][2]);
+        mc_gradient(s, n, h, i + cof[c][0], j + cof[c][1], k + cof[c][2], nrm[c]);
+    }
+    int cfg = 0;
+    for (int c = 0; c < 8; ++c)
+        if (data[c] <= 0.0) cfg |= 1 << c;
+    if (cfg == 0 || cfg == 255) return;
+    /* BoundingBox3D with origin GridIndexToPosition(i, j, k) and size h; Corner (3d/bounding_box_3d.cpp:23-31) */
+    double bo[3];
+    grid_pos(o, h, i, j, k, bo);
+    static const int index_map[8] = {0, 1, 5, 4, 2, 3, 7, 6};
+    double e[12][3], en[12][3];
+    for (int ed = 0; ed < 12; ++ed) {
+        const int a = or_mc_edge[ed][0], b = or_mc_edge[ed][1];
+        if (((cfg >> a) & 1) == ((cfg >> b) & 1)) continue;
+        double p0[3], p1[3];
+        for (int d = 0; d < 3; ++d) {
+            const int ca = index_map[a], cb = index_map[b];
+            const double offa = ((ca >> d) & 1) ? 0.5 : -0.5, offb = ((cb >> d) & 1) ? 0.5 : -0.5;
+            p0[d] = (h[d] * offa + bo[d]) + 0.5 * h[d];
+            p1[d] = (h[d] * offb + bo[d]) + 0.5 * h[d];
+        }
+        const double phi0 = data[a] - 0.0, phi1 = data[b] - 0.0;
+        double alpha = (fabs(phi0) + fabs(phi1) > 0.000000001) ? fabs(phi0) / (fabs(phi0) + fabs(phi1)) : 0.5;
+        if (alpha < 0.000001) alpha = 0.000001;
+        if (alpha > 0.999999) alpha = 0.999999;
+        for (int d = 0; d < 3; ++d) {
+            e[ed][d] = (1.0 - alpha) * p0[d] + alpha * p1[d];
+            en[ed][d] = (1.0 - alpha) * nrm[a][d] + alpha * nrm[b][d];
+        }
+    }
+    const unsigned long long cs = or_mc3d[cfg];
+    const int ntri = (int)(cs >> 60);
+    for (int t = 0; t < ntri; ++t) {
+        int64_t f[3];
+        for (int q = 0; q < 3; ++q) {
+            const int ed = (int)((cs >> (4 * (3 * t + q))) & 15);
+            const size_t key = mc_key(i, j, k, n, mc_edge_off[ed][0], mc_edge_off[ed][1], mc_edge_off[ed][2]);
+            int64_t id = map_get(m, key);
+            if (id < 0) {
+                /* SafeNormalize: n / |n| when |n|^2 > 0 (Vector3::Normalize, common/vector3.hpp:149-152) */
+                double nn[3] = {en[ed][0], en[ed][1], en[ed][2]};
+                const double len = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+                if (len * len > 0.0) {
+                    const double l2 = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+                    nn[0] /= l2; nn[1] /= l2; nn[2] /= l2;
+                }
+                id = (int64_t)m->nv;
+                mesh_add_vertex(m, e[ed], nn);
+                map_put(m, key, id);
+            }
+            f[q] = id;
+        }
+        mesh_add_triangle(m, f);
+    }
+}
+
+/* SolveSingleSquare (marching_cubes_solver.cpp:497-583): data, keys (4 corners then 4 edges), corners, normal. */
+static void mc_square(const double data[4], const size_t keys[8], const double nrm[3], const double corners[4][3], or_mesh* m)
+{
+    int cfg = 0;
+    for (int c = 0; c < 4; ++c)
+        if (data[c] <= 0.0) cfg |= 1 << c;
+    if (cfg == 0) return;
+    double e[4][3];
+    for (int ed = 0; ed < 4; ++ed) {
+        const int a = ed, b = (ed + 1) & 3;
+        if (((cfg >> a) & 1) == ((cfg >> b) & 1)) continue;
+        const double phi0 = data[a] - 0.0, phi1 = data[b] - 0.0;
+        double alpha = (fabs(phi0) + fabs(phi1) > 1e-12) ? fabs(phi0) / (fabs(phi0) + fabs(phi1)) : (double)0.5f;
+        if (alpha < (double)0.000001f) alpha = (double)0.000001f;
+        if (alpha > (double)0.999999f) alpha = (double)0.999999f;
+        for (int d = 0; d < 3; ++d) e[ed][d] = (1.0 - alpha) * corners[a][d] + alpha * corners[b][d];
+    }
+    const unsigned long long cs = or_mc2d[cfg];
+    const int ntri = (int)(cs >> 60);
+    for (int t = 0; t < ntri; ++t) {
+        int64_t f[3];
+        for (int q = 0; q < 3; ++q) {
+            const int iv = (int)((cs >> (4 * (3 * t + q))) & 15);
+            const size_t key = keys[iv];
+            int64_t id = map_get(m, key);
+            if (id < 0) {
+                id = (int64_t)m->nv;
+                mesh_add_vertex(m, iv < 4 ? corners[iv] : e[iv - 4], nrm);
+                map_put(m, key, id);
+            }
+            f[q] = id;
+        }
+        mesh_add_triangle(m, f);
+    }
+}
+
+/* One cap square of the domain face `side` (0 back z-, 1 front z+, 2 left x-, 3 right x+, 4 down y-, 5 up y+) at
+ * cube (i, j, k): SolveXY / SolveYZ / SolveXZ (marching_cubes_solver.cpp:318-495) list its corners and keys. */
+static void mc_cap(const double* s, const int n[3], const double o[3], const double h[3], int side, int i, int j, int k,
+                   or_mesh* m)
+{
+    /* corner node offsets per side, in the square's corner order; vertex ids (mc_vertex_off) and edge ids */
+    static const int corner_off[6][4][3] = {
+        {{1, 0, 0}, {0, 0, 0}, {0, 1, 0}, {1, 1, 0}}, {{0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}},
+        {{0, 0, 0}, {0, 0, 1}, {0, 1, 1}, {0, 1, 0}}, {{1, 0, 1}, {1, 0, 0}, {1, 1, 0}, {1, 1, 1}},
+        {{0, 0, 0}, {1, 0, 0}, {1, 0, 1}, {0, 0, 1}}, {{1, 1, 0}, {0, 1, 0}, {0, 1, 1}, {1, 1, 1}}};
+    static const int vid[6][4] = {{1, 0, 4, 5}, {3, 2, 6, 7}, {0, 3, 7, 4}, {2, 1, 5, 6}, {0, 1, 2, 3}, {5, 4, 7, 6}};
+    static const int eid[6][4] = {{0, 8, 4, 9}, {2, 10, 6, 11}, {3, 11, 7, 8}, {1, 9, 5, 10}, {0, 1, 2, 3}, {4, 7, 6, 5}};
+    static const double normal[6][3] = {{0, 0, -1}, {0, 0, 1}, {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}};
+    double data[4], corners[4][3];
+    size_t keys[8];
+    for (int c = 0; c < 4; ++c) {
+        const int a = i + corner_off[side][c][0], b = j + corner_off[side][c][1], d = k + corner_off[side][c][2];
+        data[c] = sdfv(s, n, a, b, d);
+        grid_pos(o, h, a, b, d, corners[c]);
+        keys[c] = mc_key(i, j, k, n, mc_vertex_off[vid[side][c]][0], mc_vertex_off[vid[side][c]][1], mc_vertex_off[vid[side][c]][2]);
+        keys[4 + c] = mc_key(i, j, k, n, mc_edge_off[eid[side][c]][0], mc_edge_off[eid[side][c]][1], mc_edge_off[eid[side][c]][2]);
+    }
+    mc_square(data, keys, normal[side], corners, m);
+}
+
+int or_build_surface(const double* sdf, const int n[3], const double origin[3], const double h[3], double* vertices,
+                     double* normals, int64_t* tris, size_t cap_v, size_t cap_t, size_t* nv, size_t* nt)
+{
+    if (n[0] < 2 || n[1] < 2 || n[2] < 2) return -1;
+    or_mesh m = {vertices, normals, tris, 0, 0, vertices ? cap_v : 0, tris ? cap_t : 0, NULL, 0};
+    m.map_size = 8 * (size_t)n[0] * (size_t)n[1] * (size_t)n[2];
+    m.map = (int64_t*)malloc(m.map_size * sizeof(int64_t));
+    int64_t* map2 = (int64_t*)malloc(m.map_size * sizeof(int64_t));
+    if (!m.map || !map2) { free(m.map); free(map2); return -1; }
+#define OR_MAP_RESET(p) for (size_t q_ = 0; q_ < m.map_size; ++q_) (p)[q_] = -1
+    /* CalculateXYZMeshPart: i, j, k nested, one vertex map */
+    OR_MAP_RESET(m.map);
+    for (int i = 0; i < n[0] - 1; ++i)
+        for (int j = 0; j < n[1] - 1; ++j)
+            for (int k = 0; k < n[2] - 1; ++k) mc_cube(sdf, n, origin, h, i, j, k, &m);
+    /* the three cap parts, each with one vertex map per side; a part's two sides alternate per square */
+    int64_t* maps[2] = {m.map, map2};
+    for (int part = 0; part < 3; ++part) {
+        OR_MAP_RESET(maps[0]);
+        OR_MAP_RESET(maps[1]);
+        const int outer = part == 0 ? n[1] - 1 : n[2] - 1;          /* XY: j, YZ: k, XZ: k */
+        const int inner = part == 1 ? n[1] - 1 : n[0] - 1;          /* XY: i, YZ: j, XZ: i */
+        for (int a = 0; a < outer; ++a)
+            for (int b = 0; b < inner; ++b)
+                for (int sd = 0; sd < 2; ++sd) {
+                    int i, j, k;
+                    if (part == 0) { i = b; j = a; k = sd ? n[2] - 2 : 0; }
+                    else if (part == 1) { i = sd ? n[0] - 2 : 0; j = b; k = a; }
+                    else { i = b; j = sd ? n[1] - 2 : 0; k = a; }
+                    m.map = maps[sd];
+                    mc_cap(sdf, n, origin, h, 2 * part + sd, i, j, k, &m);
+                }
+    }
+#undef OR_MAP_RESET
+    free(maps[0]);
+    free(maps[1]);
+    *nv = m.nv;
+    *nt = m.nt;
+    return 0;
+}
+
+/* OBJManager::OnSave (3d/obj_manager.cpp:14-90): std::to_string is printf "%f"; indices are 1-based, the
+ * normal index of a triangle is written as size_t (so -1 prints as 0). */
+int or_write_obj(const char* path, const char* name, const double* v, const double* vn, size_t nv, const int64_t* t,
+                 size_t nt)
+{
+    FILE* f = fopen(path, "wb");
+    if (!f) return -1;
+    fprintf(f, "mtllib test.mtl\n");
+    fprintf(f, "o %s\n\n", name ? name : "");
+    for (size_t i = 0; i < nv; ++i) fprintf(f, "v %f %f %f\n", v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    fprintf(f, "\n");
+    for (size_t i = 0; i < nv; ++i) fprintf(f, "vn %f %f %f\n", vn[3 * i], vn[3 * i + 1], vn[3 * i + 2]);
+    fprintf(f, "\n");
+    fprintf(f, "s off\n\n");
+    for (size_t i = 0; i < nt; ++i) {
+        const uint64_t nidx = (uint64_t)t[4 * i + 3] + 1u;
+        fprintf(f, "f %llu//%llu %llu//%llu %llu//%llu\n", (unsigned long long)t[4 * i] + 1, (unsigned long long)nidx,
+                (unsigned long long)t[4 * i + 1] + 1, (unsigned long long)nidx, (unsigned long long)t[4 * i + 2] + 1,
+                (unsigned long long)nidx);
+    }
+    fprintf(f, "\n");
+    return fclose(f) == 0 ? 0 : -1;
 }

@@ -100,6 +100,16 @@ double or_scalar_sample(const double* arr, const int size[3], const double origi
 int or_project(const int n[3], const double h[3], const uint8_t* marks, double* u, double* v, double* w,
                double* p, double rel_tol, int max_it, double* rel_residual);
 
+/* MarchingCubesSolver::BuildSurface (3d/marching_cubes_solver.cpp:25-50) with iso value 0 and no colliders, on a
+ * node grid of n[0]*n[1]*n[2] values (x-fastest) with the given origin and spacing.  Fills up to cap_v vertices and
+ * normals (3 doubles each) and cap_t triangles (4 int64 each: vertex ids, normal id) in the reference's order and
+ * returns the full counts in *nv, *nt (call with NULL buffers to size them). */
+int or_build_surface(const double* sdf, const int n[3], const double origin[3], const double h[3], double* vertices,
+                     double* normals, int64_t* tris, size_t cap_v, size_t cap_t, size_t* nv, size_t* nt);
+/* OBJManager::Save of such a mesh (3d/obj_manager.cpp:14-90). */
+int or_write_obj(const char* path, const char* name, const double* v, const double* vn, size_t nv, const int64_t* t,
+                 size_t nt);
+
 /* Stable counting sort of FP32 particle positions by fe_keys.h cell key; writes keys and perm. */
 void or_sort_keys(const float* pos, size_t n, const int dims[3], const float origin[3], const float inv_h[3],
                   uint32_t* keys_sorted, uint32_t* perm);

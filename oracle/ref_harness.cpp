@@ -9,6 +9,13 @@
 // protected substep stages so single stages can be compared.
 //
 // Private members are reached with the usual test-only access trick; layout is unchanged.
+// The mesh writer is used through its public interface; its standard-library headers must not see the access
+// trick below, so it comes first.
+#include <fstream>
+#include <sstream>
+#include "3d/obj_manager.hpp"
+#include "3d/triangle_mesh.hpp"
+
 #define private public
 #define protected public
 #include "pic_simulator.hpp"
@@ -59,6 +66,7 @@ struct RelTolCG : public LinearSystemSolver {
 };
 
 struct Handle {
+    TriangleMesh mesh;  // the last GetSurface result
     int solver;
     std::shared_ptr<PICSimulator> sim;
     std::shared_ptr<SinglePhasePressureSolver> pressure;
@@ -243,6 +251,48 @@ void ref_stage_p2g(void* p) { Handle* h = (Handle*)p; quiet(h, true); h->sim->Tr
 void ref_stage_sdf(void* p) { Handle* h = (Handle*)p; quiet(h, true); h->sim->BuildSignedDistanceField(); quiet(h, false); }
 void ref_stage_begin(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->BeginAdvanceTimeStep(dt); quiet(h, false); }
 void ref_stage_forces(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeExternalForces(dt); quiet(h, false); }
+// Overwrites Fluid3::sdf (x-fastest node values), the input of GetSurface.
+void ref_set_sdf(void* p, const double* values)
+{
+    Handle* h = (Handle*)p;
+    auto& sdf = h->sim->_fluid.sdf;
+    each3(sdf, [&](size_t i, size_t j, size_t k, size_t c) { sdf(i, j, k) = values[c]; });
+}
+
+// PICSimulator::GetSurface (pic_simulator.cpp:71-78) into a fresh mesh; copies up to the given capacities.
+void ref_get_surface(void* p, double* v, double* n, int64_t* t, size_t cap_v, size_t cap_t, size_t* nv, size_t* nt)
+{
+    Handle* h = (Handle*)p;
+    quiet(h, true);
+    h->mesh.Clear();
+    h->sim->GetSurface(h->mesh);
+    quiet(h, false);
+    const auto& V = h->mesh.GetVerticies();
+    const auto& N = h->mesh.GetNormals();
+    const auto& T = h->mesh.GetTriangles();
+    *nv = V.size();
+    *nt = T.size();
+    for (size_t i = 0; v && i < V.size() && i < cap_v; ++i) {
+        v[3 * i] = V[i].x; v[3 * i + 1] = V[i].y; v[3 * i + 2] = V[i].z;
+        n[3 * i] = N[i].x; n[3 * i + 1] = N[i].y; n[3 * i + 2] = N[i].z;
+    }
+    for (size_t i = 0; t && i < T.size() && i < cap_t; ++i) {
+        t[4 * i] = (int64_t)T[i].point1Idx; t[4 * i + 1] = (int64_t)T[i].point2Idx;
+        t[4 * i + 2] = (int64_t)T[i].point3Idx; t[4 * i + 3] = (int64_t)T[i].normalIdx;
+    }
+}
+
+// OBJManager::Save of the last GetSurface mesh under the given object name.
+void ref_save_obj(void* p, const char* path, const char* name)
+{
+    Handle* h = (Handle*)p;
+    h->mesh.SetObjectName(name);
+    OBJManager obj;
+    quiet(h, true);
+    obj.Save(path, h->mesh);
+    quiet(h, false);
+}
+
 void ref_stage_diffusion(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeDiffusion(dt); quiet(h, false); }
 void ref_stage_pressure(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputePressure(dt); quiet(h, false); }
 void ref_stage_advection(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeAdvection(dt); quiet(h, false); }

@@ -70,6 +70,25 @@ def make(name, n, solver, region, seed, max_cfl, origin, viscosity=0.0, dt=1.0 /
         out_u=u, out_v=v, out_w=w, out_p=r.pressure(), out_marks=r.marks(), out_pos=P, out_vel=V, out_C=CC)
 
 
+SURFACE_CASES = [
+    # name, n, region, seed, origin: the reference's GetSurface (marching cubes + caps) of the particle SDF
+    ("surface_16", (16, 16, 16), (0.0, 0.0, 0.0, 0.4, 0.6, 1.0), 0, (0.0, 0.0, 0.0)),
+    ("surface_12x20x9", (12, 20, 9), (0.1, 0.0, 0.2, 0.7, 0.5, 0.8), 1, (0.0, 0.0, 0.0)),
+]
+
+
+def make_surface(name, n, region, seed, origin):
+    lo = tuple(origin[a] + region[a] for a in range(3))
+    hi = tuple(origin[a] + region[3 + a] for a in range(3))
+    pos, _ = oracle.seed_regions([dict(kind=0, lo=lo, hi=hi)], n, origin, (1, 1, 1), seed)
+    r = oracle.RefSim(n, oracle.FLIP, origin=origin)
+    r.set_particles(pos.astype(np.float64))
+    r.stage("sdf")
+    V, N, T = r.surface()
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), n=np.array(n), origin=np.array(origin), sdf=r.sdf(), V=V, N=N,
+                        T=T)
+
+
 if __name__ == "__main__":
     if not oracle.ref_available("serial"):
         sys.exit("build the reference first: python oracle/build_ref.py")
@@ -78,4 +97,9 @@ if __name__ == "__main__":
         if not force and os.path.exists(os.path.join(OUT, c[0] + ".npz")):
             continue
         make(*c)
+        print("wrote", c[0])
+    for c in SURFACE_CASES:
+        if not force and os.path.exists(os.path.join(OUT, c[0] + ".npz")):
+            continue
+        make_surface(*c)
         print("wrote", c[0])
