@@ -29,7 +29,8 @@ EXPORTS = [
     "fe_scene_num_particles", "fe_scene_step", "fe_scene_step_profiled", "fe_scene_advance_frame", "fe_scene_cfl", "fe_scene_run_stages",
     "fe_scene_get_grid", "fe_scene_set_grid", "fe_scene_set_pressure", "fe_scene_get_face_markers",
     "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_set_viscosity",
-    "fe_scene_get_diffusion", "fe_scene_get_sort", "fe_scene_divergence",
+    "fe_scene_get_diffusion", "fe_scene_build_surface", "fe_scene_get_surface", "fe_scene_write_surface_obj",
+    "fe_write_obj", "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
     "fe_abi_version",
@@ -105,6 +106,10 @@ def lib():
     L.fe_scene_get_fluid_sdf.argtypes = [P, P]
     L.fe_scene_set_viscosity.argtypes = [P, ctypes.c_double]
     L.fe_scene_get_diffusion.argtypes = [P, P, P, P, P]
+    L.fe_scene_build_surface.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.fe_scene_get_surface.argtypes = [P, P, P, P]
+    L.fe_scene_write_surface_obj.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
+    L.fe_write_obj.argtypes = [ctypes.c_char_p, ctypes.c_char_p, P, P, ctypes.c_uint64, P, ctypes.c_uint64]
     L.fe_scene_get_sort.argtypes = [P, P, P, ctypes.c_uint64]
     L.fe_scene_divergence.argtypes = [P, D]
     L.fe_scene_set_stream.argtypes = [P, P]

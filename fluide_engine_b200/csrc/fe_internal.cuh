@@ -201,12 +201,18 @@ struct DiffWork {
 // Kernel launchers (one per .cu file).
 cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, size_t scan_tmp_bytes);
 size_t sort_scan_tmp_bytes(uint32_t n);
+// Exclusive prefix sum of n counts into out[0..n] (out[n] = total); tmp holds sort_scan_tmp_bytes(n).
+cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t n, uint32_t* out, void* tmp, size_t tmp_bytes,
+                                  cudaStream_t st);
 cudaError_t launch_gather(const SceneView& v, const SceneView& dst, cudaStream_t st);
 cudaError_t launch_p2g(const SceneView& v, cudaStream_t st);
 cudaError_t launch_mark(const SceneView& v, cudaStream_t st);
 cudaError_t launch_fluid_sdf(const SceneView& v, double* out, cudaStream_t st);
 // Distance bits of the band SDF per node by a particle scatter, then the diffusion face markers (fe_mark.cu).
 cudaError_t launch_face_fluid_marks(const SceneView& v, const DiffWork& d, cudaStream_t st);
+// The band SDF of v's particles at every node (BuildSignedDistanceField's values, FP64) by the same scatter;
+// node_scratch holds nx*ny*nz u64 (fe_mark.cu).
+cudaError_t launch_node_sdf(const SceneView& v, unsigned long long* node_scratch, double* sdf, cudaStream_t st);
 cudaError_t launch_pre(const SceneView& v, double dt, cudaStream_t st);
 cudaError_t launch_post(const SceneView& v, cudaStream_t st);
 cudaError_t launch_rhs(const SceneView& v, cudaStream_t st);
@@ -274,6 +280,14 @@ cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, doubl
                       cudaStream_t st);
 cudaError_t launch_mgcg(const SceneView& v, const CgWork& w, const MgWork& mg, double rel_tol, double inner_tol,
                         int max_it, int max_refine, cudaStream_t st);
+
+// Surface extraction (fe_surface.cu): items = the node grid's cubes, then its XY, YZ and XZ cap squares (two faces
+// each); counts per item, then the mesh from the scanned counts.
+size_t mc_items(int nx, int ny, int nz);
+cudaError_t launch_mc_count(const SceneView& v, const double* sdf, uint8_t* cfg, uint32_t* nvert, uint32_t* ntri,
+                            cudaStream_t st);
+cudaError_t launch_mc_emit(const SceneView& v, const double* sdf, const uint8_t* cfg, const uint32_t* vbase,
+                           const uint32_t* tbase, double* V, double* N, int64_t* T, cudaStream_t st);
 
 // Viscosity (fe_diffuse.cu): ComputeDiffusion on the velocity buffers u, vv, ww (face markers, FLUID-face list,
 // persistent Jacobi solve, wall layers zeroed).  Uses the scene's solver barrier and error words (CgWork).

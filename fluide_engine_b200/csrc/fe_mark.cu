@@ -225,6 +225,24 @@ __global__ void __launch_bounds__(256) k_sdf_scatter(SceneView v, unsigned long 
     }
 }
 
+// Node values of BuildSignedDistanceField (pic_simulator.cpp:452-475): min(2r, sqrt(smallest squared distance)) - r.
+__device__ __forceinline__ double node_value(unsigned long long raw, double band, double radius)
+{
+    double m = band;
+    if (raw != ~0ull) {
+        const double dm = __dsqrt_rn(__longlong_as_double((long long)raw));
+        if (dm < m) m = dm;
+    }
+    return __dsub_rn(m, radius);
+}
+
+__global__ void k_node_values(const unsigned long long* __restrict__ node, size_t nc, double band, double radius,
+                              double* __restrict__ sdf)
+{
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x)
+        sdf[c] = node_value(node[c], band, radius);
+}
+
 // BackwardEulerDiffusionSolver::BuildX/Y/ZMarkers (fluid_solvers/backward_euler_diffusion_solver.cpp:71-128):
 // a face is FLUID iff ScalarGrid3D::Sample (3d/scalar_grid3d.cpp:33-65) of the fluid SDF at the face centre is
 // < 0.  The face centres are those of the copied velocity grid (data origins include the domain origin,
@@ -243,15 +261,7 @@ __global__ void k_face_mark(SceneView v, DiffWork d)
     const int ip = min(i0 + 1, nx - 1), jp = min(j0 + 1, ny - 1), kp = min(k0 + 1, nz - 1);
     const unsigned long long* __restrict__ node = d.node_dist;
     // node value min(2r, sqrt(smallest squared distance)) - r (all ones: no particle within the band)
-    auto val = [&](int i, int j, int k) {
-        const unsigned long long raw = __ldg(node + idx3(i, j, k, nx, ny));
-        double m = v.band;
-        if (raw != ~0ull) {
-            const double dm = __dsqrt_rn(__longlong_as_double((long long)raw));
-            if (dm < m) m = dm;
-        }
-        return __dsub_rn(m, v.radius);
-    };
+    auto val = [&](int i, int j, int k) { return node_value(__ldg(node + idx3(i, j, k, nx, ny)), v.band, v.radius); };
     const double c000 = val(i0, j0, k0), c100 = val(ip, j0, k0), c010 = val(i0, jp, k0), c110 = val(ip, jp, k0);
     const double c001 = val(i0, j0, kp), c101 = val(ip, j0, kp), c011 = val(i0, jp, kp), c111 = val(ip, jp, kp);
     const double b0 = lerp_ref(lerp_ref(c000, c100, fx), lerp_ref(c010, c110, fx), fy);
@@ -286,6 +296,20 @@ cudaError_t launch_mark(const SceneView& v, cudaStream_t st)
 cudaError_t launch_fluid_sdf(const SceneView& v, double* out, cudaStream_t st)
 {
     k_fluid_sdf<<<148 * 8, 128, 0, st>>>(v, v.band * v.band, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_node_sdf(const SceneView& v, unsigned long long* node, double* sdf, cudaStream_t st)
+{
+    const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
+    cudaError_t e = cudaMemsetAsync(node, 0xff, nc * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    if (v.np > 0) {
+        k_sdf_scatter<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, node, v.band * v.band);
+        count_launch();
+    }
+    k_node_values<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(node, nc, v.band, v.radius, sdf);
     count_launch();
     return cudaGetLastError();
 }

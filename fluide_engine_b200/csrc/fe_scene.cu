@@ -112,6 +112,24 @@ struct fe_scene {
     MgWork mg{};                       // multigrid levels (levels >= 2) when the pressure solver is FE_PRESSURE_MGPCG
     DiffWork diff{};                   // viscosity buffers (allocated once the viscosity is > 0)
     bool diff_ready = false;
+    // Surface extraction (fe_surface.cu), allocated on first use: node distances and SDF values, per-item case
+    // bytes, counts and their scans, scan scratch, and the last mesh (grown on demand).
+    struct {
+        unsigned long long* node = nullptr;
+        double* sdf = nullptr;
+        uint8_t* cfg = nullptr;
+        uint32_t *nvert = nullptr, *ntri = nullptr, *vbase = nullptr, *tbase = nullptr;
+        void* tmp = nullptr;
+        size_t tmp_bytes = 0, items = 0;
+        double *V = nullptr, *N = nullptr;
+        int64_t* T = nullptr;
+        uint64_t cap_v = 0, cap_t = 0, nv = 0, nt = 0;
+        bool built = false;
+        std::vector<void*> mesh_allocs;
+    } surf;
+    // true once a substep's sort has run since the particles were set: the other particle set then holds the
+    // positions at the start of the last substep, from which the reference's Fluid3::sdf was built
+    bool prev_valid = false;
     uint64_t epoch = 0;                // bumped when the substep's kernel sequence changes (batches re-capture)
     double* d_scalar = nullptr;        // CFL / divergence result
     float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
@@ -477,6 +495,7 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             SceneView dst = view_of(s, s->parity ^ 1);
             FE_CUDA(launch_gather(v, dst, st));
             s->parity ^= 1;
+            s->prev_valid = true;
             break;
         }
         case kStepP2g:
@@ -640,7 +659,40 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
     }
     if (ev) FE_CUDA(cudaEventRecord(ev[3], s->stream));
     s->parity ^= 1;  // the sort inside the first graph flipped the buffer sets
+    s->prev_valid = true;
     s->grid_cur = 0;
+    return FE_OK;
+}
+
+// The band SDF from which the reference's last Fluid3::sdf was built: the positions at the start of the last
+// substep (the other particle set, once a substep has run), else the current particles.  Allocates the surface
+// buffers on first use.
+fe_status surface_sdf(fe_scene* s)
+{
+    auto& w = s->surf;
+    const SceneView& b = s->base;
+    const size_t nc = (size_t)b.g.nx * b.g.ny * b.g.nz;
+    if (!w.sdf) {
+        cudaStream_t st = s->own_stream;
+        FE_CUDA(cudaStreamSynchronize(s->stream));
+        w.items = mc_items(b.g.nx, b.g.ny, b.g.nz);
+        if (w.items + 1 >= (1ull << 32)) return set_error(FE_ERR_BAD_ARG, "grid too large for surface extraction");
+        w.tmp_bytes = sort_scan_tmp_bytes((uint32_t)w.items);
+        auto& L = s->allocs;
+        FE_CUDA(dalloc(L, &w.node, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.sdf, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.cfg, w.items, s->device, st));
+        FE_CUDA(dalloc(L, &w.nvert, w.items, s->device, st));
+        FE_CUDA(dalloc(L, &w.ntri, w.items, s->device, st));
+        FE_CUDA(dalloc(L, &w.vbase, w.items + 1, s->device, st));
+        FE_CUDA(dalloc(L, &w.tbase, w.items + 1, s->device, st));
+        uint8_t* tmp;
+        FE_CUDA(dalloc(L, &tmp, w.tmp_bytes, s->device, st));
+        w.tmp = tmp;
+        FE_CUDA(cudaStreamSynchronize(st));
+    }
+    const SceneView v = view_of(s, s->prev_valid ? (s->parity ^ 1) : s->parity);
+    FE_CUDA(launch_node_sdf(v, w.node, w.sdf, s->stream));
     return FE_OK;
 }
 
@@ -767,6 +819,7 @@ fe_status fe_scene_destroy(fe_scene* s)
     // back to the pool in the own stream's order (the scene's work on any stream is complete here)
     free_list(s->allocs, s->own_stream);
     free_list(s->particle_allocs, s->own_stream);
+    free_list(s->surf.mesh_allocs, s->own_stream);
     cudaStreamDestroy(s->own_stream);  // its pending frees still run
     delete s;
     return FE_OK;
@@ -806,6 +859,7 @@ fe_status fe_scene_set_particles(fe_scene* s, const float* pos, const float* vel
     }
     FE_CUDA(cudaStreamSynchronize(s->stream));
     s->have_particles = true;
+    s->prev_valid = false;
     return FE_OK;
 }
 
@@ -835,6 +889,7 @@ fe_status fe_scene_reset(fe_scene* s)
     FE_CUDA(cudaMemsetAsync(s->cg.err, 0, sizeof(int), st));
     FE_CUDA(cudaStreamSynchronize(st));
     s->grid_cur = 0;
+    s->prev_valid = false;
     return FE_OK;
 }
 
@@ -1069,18 +1124,79 @@ fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf)
     if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles first");
     std::lock_guard<std::mutex> lk(s->mu);
     FE_CUDA(cudaSetDevice(s->device));
-    // the band SDF gathers through cell ranges, so sort the current particles first
-    fe_status st = enqueue_stages(s, 1.0, FE_STAGE_SORT, FE_STAGE_SORT);
+    fe_status st = surface_sdf(s);
     if (st != FE_OK) return st;
     const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
-    double* tmp = nullptr;
-    FE_CUDA(cudaMallocAsync((void**)&tmp, nc * sizeof(double), s->stream));
-    cudaError_t e = launch_fluid_sdf(view_of(s, s->parity), tmp, s->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sdf, tmp, nc * 8, cudaMemcpyDefault, s->stream);
-    cudaFreeAsync(tmp, s->stream);
-    FE_CUDA(e);
+    FE_CUDA(cudaMemcpyAsync(sdf, s->surf.sdf, nc * sizeof(double), cudaMemcpyDefault, s->stream));
     FE_CUDA(cudaStreamSynchronize(s->stream));
     return FE_OK;
+}
+
+fe_status fe_scene_build_surface(fe_scene* s, uint64_t* n_vertices, uint64_t* n_triangles)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles first");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    fe_status st = surface_sdf(s);
+    if (st != FE_OK) return st;
+    auto& w = s->surf;
+    const SceneView& v = s->base;
+    cudaStream_t stream = s->stream;
+    FE_CUDA(launch_mc_count(v, w.sdf, w.cfg, w.nvert, w.ntri, stream));
+    FE_CUDA(launch_exclusive_scan(w.nvert, (uint32_t)w.items, w.vbase, w.tmp, w.tmp_bytes, stream));
+    FE_CUDA(launch_exclusive_scan(w.ntri, (uint32_t)w.items, w.tbase, w.tmp, w.tmp_bytes, stream));
+    uint32_t tot[2] = {0, 0};
+    FE_CUDA(cudaMemcpyAsync(&tot[0], w.vbase + w.items, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaMemcpyAsync(&tot[1], w.tbase + w.items, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    if (tot[0] > w.cap_v || tot[1] > w.cap_t) {
+        free_list(w.mesh_allocs, stream);
+        w.cap_v = std::max<uint64_t>(tot[0], 1) * 5 / 4;
+        w.cap_t = std::max<uint64_t>(tot[1], 1) * 5 / 4;
+        FE_CUDA(dalloc(w.mesh_allocs, &w.V, 3 * w.cap_v, s->device, stream));
+        FE_CUDA(dalloc(w.mesh_allocs, &w.N, 3 * w.cap_v, s->device, stream));
+        FE_CUDA(dalloc(w.mesh_allocs, &w.T, 4 * w.cap_t, s->device, stream));
+    }
+    FE_CUDA(launch_mc_emit(v, w.sdf, w.cfg, w.vbase, w.tbase, w.V, w.N, w.T, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    w.nv = tot[0];
+    w.nt = tot[1];
+    w.built = true;
+    if (n_vertices) *n_vertices = w.nv;
+    if (n_triangles) *n_triangles = w.nt;
+    return FE_OK;
+}
+
+fe_status fe_scene_get_surface(fe_scene* s, double* vertices, double* normals, int64_t* triangles)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->surf.built) return set_error(FE_ERR_STATE, "build the surface first (fe_scene_build_surface)");
+    FE_CUDA(cudaSetDevice(s->device));
+    auto& w = s->surf;
+    if (vertices && w.nv) FE_CUDA(cudaMemcpyAsync(vertices, w.V, 3 * w.nv * sizeof(double), cudaMemcpyDefault, s->stream));
+    if (normals && w.nv) FE_CUDA(cudaMemcpyAsync(normals, w.N, 3 * w.nv * sizeof(double), cudaMemcpyDefault, s->stream));
+    if (triangles && w.nt) FE_CUDA(cudaMemcpyAsync(triangles, w.T, 4 * w.nt * sizeof(int64_t), cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_write_surface_obj(fe_scene* s, const char* path, const char* object_name)
+{
+    if (!s || !path) return set_error(FE_ERR_BAD_ARG, "null argument");
+    uint64_t nv = 0, nt = 0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (!s->surf.built) return set_error(FE_ERR_STATE, "build the surface first (fe_scene_build_surface)");
+        nv = s->surf.nv;
+        nt = s->surf.nt;
+    }
+    std::vector<double> V(3 * nv), N(3 * nv);
+    std::vector<int64_t> T(4 * nt);
+    fe_status st = fe_scene_get_surface(s, V.data(), N.data(), T.data());
+    if (st != FE_OK) return st;
+    return fe_write_obj(path, object_name, V.data(), N.data(), nv, T.data(), nt);
 }
 
 fe_status fe_scene_set_viscosity(fe_scene* s, double viscosity)
@@ -1318,6 +1434,7 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = null
         FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
         FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
         s->parity ^= 1;  // the pre-solve graph's sort flipped the particle buffer sets
+        s->prev_valid = true;
         s->grid_cur = 0;
     }
     if (ev) FE_CUDA(cudaEventRecord(ev[3], b->stream));
@@ -1574,6 +1691,7 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
         b->parity ^= 1;
         for (fe_scene* s : b->scenes) {
             s->parity ^= 1;
+            s->prev_valid = true;
             s->grid_cur = 0;
         }
     }

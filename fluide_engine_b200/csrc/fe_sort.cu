@@ -220,6 +220,20 @@ __global__ void k_gather(SceneView src, SceneView dst, int ncomp)
 // block sums (nb words), one spare, and the long-run counter
 size_t sort_scan_tmp_bytes(uint32_t n) { return ((n + kScanTile - 1) / kScanTile + 2) * sizeof(uint32_t); }
 
+cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t n, uint32_t* out, void* tmp, size_t tmp_bytes,
+                                  cudaStream_t st)
+{
+    if (n == 0) return cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
+    const uint32_t nb = (n + kScanTile - 1) / kScanTile;
+    if (sort_scan_tmp_bytes(n) > tmp_bytes) return cudaErrorInvalidValue;
+    uint32_t* sums = (uint32_t*)tmp;
+    k_scan_partials<<<nb, kScanThreads, 0, st>>>(in, n, sums);
+    k_scan_block_sums<<<1, kScanThreads, 0, st>>>(sums, nb);
+    k_scan_final<<<nb, kScanThreads, 0, st>>>(in, n, sums, out);
+    count_launch(3);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, size_t scan_tmp_bytes)
 {
     const uint32_t K = v.g.key_space;

@@ -156,6 +156,19 @@ class Scene:
         check(self._L.fe_scene_get_fluid_sdf(self._h, ptr(s)))
         return s
 
+    def surface(self):
+        """GetSurface: (vertices (V,3) f64, normals (V,3) f64, triangles (T,4) int64: vertex ids, normal id)."""
+        nv, nt = ctypes.c_uint64(), ctypes.c_uint64()
+        check(self._L.fe_scene_build_surface(self._h, ctypes.byref(nv), ctypes.byref(nt)))
+        V = np.zeros((nv.value, 3)); N = np.zeros((nv.value, 3)); T = np.zeros((nt.value, 4), dtype=np.int64)
+        check(self._L.fe_scene_get_surface(self._h, ptr(V), ptr(N), ptr(T)))
+        return V, N, T
+
+    def write_surface_obj(self, path, name=""):
+        """Builds the surface and writes it as OBJManager::Save does."""
+        check(self._L.fe_scene_build_surface(self._h, None, None))
+        check(self._L.fe_scene_write_surface_obj(self._h, str(path).encode(), name.encode()))
+
     def set_viscosity(self, viscosity):
         check(self._L.fe_scene_set_viscosity(self._h, float(viscosity)))
         self.desc.viscosity = float(viscosity)

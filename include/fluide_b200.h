@@ -159,8 +159,24 @@ fe_status fe_scene_get_snapshot(fe_scene* s, float* u, float* v, float* w);
 /* Right-hand side b = div u of the last pressure solve (SinglePhasePressureSolver::BuildSystem b). */
 fe_status fe_scene_get_rhs(fe_scene* s, double* b);
 /* Band-limited particle SDF on the cell-centred grid (HybridSimulator::GetFluidSdf, hybrid_simulator.cpp:82-85,
- * as built by PICSimulator::BuildSignedDistanceField, pic_simulator.cpp:452-475), FP64. */
+ * as built by PICSimulator::BuildSignedDistanceField, pic_simulator.cpp:452-475), FP64: the one built at the
+ * start of the last substep (from the current particles before any substep). */
 fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf);
+/* Fluid surface (PICSimulator::GetSurface, pic_simulator.cpp:71-78: MarchingCubesSolver::BuildSurface,
+ * 3d/marching_cubes_solver.cpp:25-583, iso value 0, no colliders) of the band particle SDF the reference holds in
+ * Fluid3::sdf: the one built at the start of the last substep (from the current particles before any substep).
+ * The mesh equals the reference's: vertices and normals in its creation order (FP64), triangles as 4 int64 each
+ * (three vertex ids, then the normal id the reference stores: the last vertex created so far).  Built on the
+ * device; fe_scene_build_surface returns the counts, fe_scene_get_surface copies the mesh out (host or device
+ * pointers; any may be NULL), fe_scene_write_surface_obj writes it as OBJManager::Save does. */
+fe_status fe_scene_build_surface(fe_scene* s, uint64_t* n_vertices, uint64_t* n_triangles);
+fe_status fe_scene_get_surface(fe_scene* s, double* vertices, double* normals, int64_t* triangles);
+fe_status fe_scene_write_surface_obj(fe_scene* s, const char* path, const char* object_name);
+/* OBJManager::Save (3d/obj_manager.cpp:14-90, 3d/mesh_file_manager.cpp) of a mesh in the layout above (host
+ * pointers): the reference's header, "v" / "vn" lines in "%f" format, "s off", "f a//n b//n c//n" lines. */
+fe_status fe_write_obj(const char* path, const char* object_name, const double* vertices, const double* normals,
+                       uint64_t n_vertices, const int64_t* triangles, uint64_t n_triangles);
+
 /* Viscosity (HybridSimulator::SetViscosity, hybrid_simulator.cpp:97-100), settable at any time.  When it is > 0
  * every substep runs ComputeDiffusion (pic_simulator.cpp:214-222) after the external forces: the reference's
  * BackwardEulerDiffusionSolver (fluid_solvers/backward_euler_diffusion_solver.cpp:20-242) -- per component, faces
