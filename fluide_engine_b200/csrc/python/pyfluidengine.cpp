@@ -2,7 +2,8 @@
 //
 // Same module name, class names and method names as the reference's binding
 // (python_wrapper/main.cpp:20-33, simulators_wrapper.cu:36-85, vector3_wrapper.cpp, frame_wrapper.cpp,
-// bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp) for the substep path, so
+// bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp, triangle_mesh_wrapper.cpp, obj_manager_wrapper.cpp)
+// for the substep path and its surface output, so
 // `import PyFluidEngine as pyf` keeps working for a caller of the simulators.  The GIL is released while
 // a frame or a batch of substeps runs.  Extensions for seeding and reading particles take and return
 // numpy arrays.
@@ -54,6 +55,42 @@ PYBIND11_MODULE(PyFluidEngine, m)
         .def("GetIndex", &Frame::GetIndex)
         .def("GetTimeIntervalInSeconds", &Frame::GetTimeIntervalInSeconds)
         .def("GetTimeInSeconds", &Frame::GetTimeInSeconds);
+    // TriangleMesh / OBJManager (triangle_mesh_wrapper.cpp, obj_manager_wrapper.cpp); the mesh's arrays are also
+    // readable as numpy (vertices (V,3), normals (V,3), triangles (T,4): vertex ids, normal id).
+    py::class_<TriangleMesh>(m, "TriangleMesh")
+        .def(py::init<>())
+        .def("Clear", &TriangleMesh::Clear)
+        .def("GetObjectName", &TriangleMesh::GetObjectName)
+        .def("SetObjectName", &TriangleMesh::SetObjectName)
+        .def("GetVertices", [](const TriangleMesh& mesh) {
+            const auto& V = mesh.GetVerticies();
+            py::array_t<double> out({(py::ssize_t)V.size(), (py::ssize_t)3});
+            for (size_t i = 0; i < V.size(); ++i) {
+                out.mutable_at(i, 0) = V[i].x; out.mutable_at(i, 1) = V[i].y; out.mutable_at(i, 2) = V[i].z;
+            }
+            return out;
+        })
+        .def("GetNormals", [](const TriangleMesh& mesh) {
+            const auto& N = mesh.GetNormals();
+            py::array_t<double> out({(py::ssize_t)N.size(), (py::ssize_t)3});
+            for (size_t i = 0; i < N.size(); ++i) {
+                out.mutable_at(i, 0) = N[i].x; out.mutable_at(i, 1) = N[i].y; out.mutable_at(i, 2) = N[i].z;
+            }
+            return out;
+        })
+        .def("GetTriangles", [](const TriangleMesh& mesh) {
+            const auto& T = mesh.GetTriangles();
+            py::array_t<int64_t> out({(py::ssize_t)T.size(), (py::ssize_t)4});
+            for (size_t i = 0; i < T.size(); ++i) {
+                out.mutable_at(i, 0) = (int64_t)T[i].point1Idx; out.mutable_at(i, 1) = (int64_t)T[i].point2Idx;
+                out.mutable_at(i, 2) = (int64_t)T[i].point3Idx; out.mutable_at(i, 3) = (int64_t)T[i].normalIdx;
+            }
+            return out;
+        });
+    py::class_<OBJManager>(m, "OBJManager")
+        .def(py::init<>())
+        .def("Save", &OBJManager::Save)
+        .def("Load", &OBJManager::Load);
     py::class_<BoundingBox3D>(m, "BoundingBox3D")
         .def(py::init<Vector3<double>, Vector3<double>>())
         .def("GetOrigin", &BoundingBox3D::GetOrigin)
@@ -148,7 +185,7 @@ PYBIND11_MODULE(PyFluidEngine, m)
         .def("SetCurrentFrame", &PICSimulator::SetCurrentFrame)
         .def("SetViscosity", &PICSimulator::SetViscosity)
         .def("SetMaxClf", &PICSimulator::SetMaxClf)
-        .def("GetSurface", [](PICSimulator& s, py::object) { s.GetSurface(*(TriangleMesh*)nullptr); });
+        .def("GetSurface", &PICSimulator::GetSurface, py::call_guard<py::gil_scoped_release>());
     py::class_<APICSimulator, std::shared_ptr<APICSimulator>, PICSimulator>(m, "APICSimulator")
         .def(py::init<Vector3<size_t>, BoundingBox3D>());
     py::class_<FLIPSimulator, std::shared_ptr<FLIPSimulator>, PICSimulator>(m, "FLIPSimulator")

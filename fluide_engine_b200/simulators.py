@@ -5,7 +5,7 @@ Same class and method names as the reference's pybind11 module PyFluidEngine
 bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp) and C++ classes (pic_simulator.hpp:27-43,
 hybrid_simulator.hpp:10-41, physics_animation.hpp:8-19, flip_simulator.hpp:9-16), backed by one
 device-resident Scene.  Only what the substep needs is implemented; entry points of components outside
-it (mesh initialisation, colliders, emitters, surface extraction) raise NotImplementedError
+it (mesh initialisation, colliders, emitters) raise NotImplementedError
 with the reason instead of silently doing something else.
 """
 import numpy as np
@@ -86,6 +86,44 @@ class DirectionalField(ExternalForce):
 
     def SetStrength(self, strength):
         self._strength = Vector3D(*strength)
+
+
+class TriangleMesh:
+    """TriangleMesh (3d/triangle_mesh.hpp): vertices (V,3), normals (V,3) and triangles (T,4: three vertex ids and
+    the normal id) as numpy arrays, appended to by GetSurface."""
+
+    def __init__(self):
+        self.Clear()
+        self._name = ""
+
+    def Clear(self):
+        self.vertices = np.zeros((0, 3))
+        self.normals = np.zeros((0, 3))
+        self.triangles = np.zeros((0, 4), dtype=np.int64)
+
+    def GetObjectName(self):
+        return self._name
+
+    def SetObjectName(self, name):
+        self._name = str(name)
+
+    def _append(self, V, N, T):
+        base = self.vertices.shape[0]
+        self.vertices = np.concatenate([self.vertices, V])
+        self.normals = np.concatenate([self.normals, N])
+        self.triangles = np.concatenate([self.triangles, T + base])
+
+
+class OBJManager:
+    """OBJManager::Save (3d/obj_manager.cpp:14-90) through the library's writer."""
+
+    def Save(self, name, obj):
+        V = np.ascontiguousarray(obj.vertices, dtype=np.float64)
+        N = np.ascontiguousarray(obj.normals, dtype=np.float64)
+        T = np.ascontiguousarray(obj.triangles, dtype=np.int64)
+        L = _abi.lib()
+        _abi.check(L.fe_write_obj(str(name).encode(), obj.GetObjectName().encode(), _abi.ptr(V), _abi.ptr(N),
+                                  V.shape[0], _abi.ptr(T), T.shape[0]))
 
 
 class HybridSimulator:
@@ -186,7 +224,10 @@ class HybridSimulator:
         raise NotImplementedError("mesh seeding (Mesh2SDF) is outside the substep path; use InitializeFromRegions")
 
     def GetSurface(self, mesh):
-        raise NotImplementedError("surface extraction (marching cubes) is outside the substep path")
+        """PICSimulator::GetSurface (pic_simulator.cpp:71-78): appends the marching-cubes surface of the SDF built at
+        the start of the last substep to mesh (a TriangleMesh), as the reference's surface tracker does."""
+        V, N, T = self._ensure_scene().surface()
+        mesh._append(V, N, T)
 
     def InitializeFromRegions(self, regions, seed=0):
         """Seeds boxes / spheres with the deterministic subcell rule (8 particles per cell)."""

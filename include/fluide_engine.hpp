@@ -7,12 +7,13 @@
 // DirectionalField (forces/directional_field.hpp) and Vector3 (common/vector3.hpp), with the same names
 // and argument meaning.  State lives on the GPU in one fe_scene (include/fluide_b200.h), created on the
 // first step after particles exist.  Entry points of components outside the substep (mesh seeding,
-// colliders, emitters, surface extraction) throw std::logic_error saying so; errors of the
+// colliders, emitters) throw std::logic_error saying so; errors of the
 // library throw fluide::Error carrying the fe_status.  Header-only; link with libfluide_b200.so.
 #ifndef FLUIDE_ENGINE_HPP
 #define FLUIDE_ENGINE_HPP
 
 #include <cmath>
+#include <cstdio>
 #include <cstddef>
 #include <cstdint>
 #include <memory>
@@ -95,7 +96,106 @@ struct fe_region_desc {
     double vel[3];    // initial velocity
 };
 
-class TriangleMesh;
+// Triangle3D (3d/triangle_3d.hpp): vertex indices and the normal index, 0-based.
+struct Triangle3D {
+    size_t point1Idx, point2Idx, point3Idx, normalIdx;
+    Triangle3D(size_t p1 = 0, size_t p2 = 1, size_t p3 = 2, size_t normIdx = 0)
+        : point1Idx(p1), point2Idx(p2), point3Idx(p3), normalIdx(normIdx) {}
+};
+typedef Triangle3D Triangle3D_t;
+
+// TriangleMesh (3d/triangle_mesh.hpp): vertices, normals and triangles as the surface tracker appends them.
+class TriangleMesh {
+  public:
+    void Clear() { _vertices.clear(); _normals.clear(); _triangles.clear(); }
+    void AddVertex(const Vector3<double>& v) { _vertices.push_back(v); }
+    void AddNormal(const Vector3<double>& n) { _normals.push_back(n); }
+    void AddTriangle(const Triangle3D_t& t) { _triangles.push_back(t); }
+    const std::vector<Vector3<double>>& GetVerticies() const { return _vertices; }
+    const std::vector<Vector3<double>>& GetNormals() const { return _normals; }
+    const std::vector<Triangle3D_t>& GetTriangles() const { return _triangles; }
+    std::vector<Vector3<double>>& GetVerticies() { return _vertices; }
+    std::vector<Vector3<double>>& GetNormals() { return _normals; }
+    std::vector<Triangle3D_t>& GetTriangles() { return _triangles; }
+    std::string GetObjectName() const { return _objectName; }
+    void SetObjectName(std::string name) { _objectName = std::move(name); }
+
+  private:
+    std::string _objectName;
+    std::vector<Vector3<double>> _vertices, _normals;
+    std::vector<Triangle3D_t> _triangles;
+};
+
+// OBJManager (3d/obj_manager.cpp): Save writes the reference's OBJ text (fe_write_obj); Load reads "o", "v", "vn"
+// and three-vertex "f" lines as OBJManager::ParseLine does (:92-161).
+class OBJManager {
+  public:
+    void Save(std::string name, const TriangleMesh& obj)
+    {
+        const auto& V = obj.GetVerticies();
+        const auto& N = obj.GetNormals();
+        const auto& T = obj.GetTriangles();
+        std::vector<double> v(3 * V.size()), n(3 * N.size());
+        std::vector<int64_t> t(4 * T.size());
+        for (size_t i = 0; i < V.size(); ++i) { v[3 * i] = V[i].x; v[3 * i + 1] = V[i].y; v[3 * i + 2] = V[i].z; }
+        for (size_t i = 0; i < N.size(); ++i) { n[3 * i] = N[i].x; n[3 * i + 1] = N[i].y; n[3 * i + 2] = N[i].z; }
+        for (size_t i = 0; i < T.size(); ++i) {
+            t[4 * i] = (int64_t)T[i].point1Idx; t[4 * i + 1] = (int64_t)T[i].point2Idx;
+            t[4 * i + 2] = (int64_t)T[i].point3Idx; t[4 * i + 3] = (int64_t)T[i].normalIdx;
+        }
+        if (V.size() != N.size()) throw std::invalid_argument("OBJManager::Save: one normal per vertex expected");
+        fluide::check(fe_write_obj(name.c_str(), obj.GetObjectName().c_str(), v.data(), n.data(), V.size(), t.data(),
+                                   T.size()));
+    }
+    void Load(std::string name, TriangleMesh& obj)
+    {
+        FILE* f = std::fopen(name.c_str(), "rb");
+        if (!f) return;  // the reference reports the error on stdout and leaves the mesh unchanged
+        std::string line;
+        for (int c = std::fgetc(f);; c = std::fgetc(f)) {
+            if (c == '\n' || c == EOF) {
+                ParseLine(line, obj);
+                line.clear();
+                if (c == EOF) break;
+            } else {
+                line.push_back((char)c);
+            }
+        }
+        std::fclose(f);
+    }
+
+  private:
+    static std::vector<std::string> Split(const std::string& s, char d)
+    {
+        std::vector<std::string> out;  // std::getline semantics: empty fields kept, no trailing empty field
+        size_t b = 0;
+        while (b < s.size()) {
+            size_t e = s.find(d, b);
+            if (e == std::string::npos) e = s.size();
+            out.push_back(s.substr(b, e - b));
+            b = e + 1;
+        }
+        return out;
+    }
+    static void ParseLine(const std::string& line, TriangleMesh& obj)
+    {
+        const std::vector<std::string> w = Split(line, ' ');
+        if (w.empty()) return;
+        if (w[0] == "o" && w.size() > 1) obj.SetObjectName(w[1]);
+        else if (w[0] == "v" && w.size() > 3) obj.AddVertex(Vector3<double>(std::stod(w[1]), std::stod(w[2]), std::stod(w[3])));
+        else if (w[0] == "vn" && w.size() > 3) obj.AddNormal(Vector3<double>(std::stod(w[1]), std::stod(w[2]), std::stod(w[3])));
+        else if (w[0] == "f" && w.size() == 4) {
+            std::vector<size_t> vs;
+            std::vector<std::string> fv;
+            for (size_t i = 1; i < w.size(); ++i) {
+                fv = Split(w[i], '/');
+                if (fv.size() > 1) vs.push_back(std::stoul(fv[0]));
+            }
+            obj.AddTriangle(Triangle3D_t(vs[0] - 1, vs[1] - 1, vs[2] - 1, std::stoul(fv[fv.size() - 1]) - 1));
+        }
+    }
+};
+
 class Collider;
 class Emitter;
 
@@ -239,7 +339,24 @@ class HybridSimulator : public PhysicsAnimation {
     {
         throw std::logic_error("mesh seeding (Mesh2SDF) is outside the substep path; use InitializeFromRegions");
     }
-    void GetSurface(TriangleMesh&) { throw std::logic_error("surface extraction is outside the substep path"); }
+    // PICSimulator::GetSurface (pic_simulator.cpp:71-78): appends the marching-cubes surface of Fluid3::sdf (the
+    // SDF built at the start of the last substep) to mesh, exactly as the reference's surface tracker does.
+    void GetSurface(TriangleMesh& mesh)
+    {
+        uint64_t nv = 0, nt = 0;
+        fluide::check(fe_scene_build_surface(Scene(), &nv, &nt));
+        std::vector<double> v(3 * nv), n(3 * nv);
+        std::vector<int64_t> t(4 * nt);
+        fluide::check(fe_scene_get_surface(Scene(), v.data(), n.data(), t.data()));
+        const size_t base = mesh.GetVerticies().size();  // ids continue after what the mesh holds
+        for (uint64_t i = 0; i < nv; ++i) {
+            mesh.AddNormal(Vector3<double>(n[3 * i], n[3 * i + 1], n[3 * i + 2]));
+            mesh.AddVertex(Vector3<double>(v[3 * i], v[3 * i + 1], v[3 * i + 2]));
+        }
+        for (uint64_t i = 0; i < nt; ++i)
+            mesh.AddTriangle(Triangle3D_t(base + (size_t)t[4 * i], base + (size_t)t[4 * i + 1], base + (size_t)t[4 * i + 2],
+                                          base + (size_t)t[4 * i + 3]));
+    }
 
     fe_scene* Scene()
     {

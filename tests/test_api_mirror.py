@@ -42,6 +42,8 @@ def test_module_names_match_reference():
         for name in REFERENCE_SIMULATOR_METHODS + REFERENCE_HYBRID_METHODS:
             assert hasattr(getattr(m, cls), name), (cls, name)
     assert hasattr(m.FLIPSimulator, "SetBlendingFactor")
+    # triangle_mesh_wrapper.cpp / obj_manager_wrapper.cpp
+    assert hasattr(m.TriangleMesh, "Clear") and hasattr(m.OBJManager, "Save") and hasattr(m.OBJManager, "Load")
 
 
 def test_reference_construction_sequence_without_device():
@@ -103,9 +105,46 @@ def test_pyfluidengine_frames_match_oracle():
 
 
 @pytest.mark.gpu
-def test_cpp_api_binary_runs():
-    out = subprocess.run([build_cpp_api_binary()], capture_output=True, text=True, check=True).stdout
+def test_cpp_api_binary_runs(tmp_path):
+    obj = tmp_path / "frame.obj"
+    out = subprocess.run([build_cpp_api_binary(), str(obj)], capture_output=True, text=True, check=True).stdout
     fields = dict(kv.split("=") for kv in out.split())
     assert fields["frames"] == "3" and int(fields["particles"]) == 13 * 19 * 32
     assert int(fields["substeps"]) >= 3
     assert 0.0 < float(fields["mean_y"]) < 0.3  # the block's centre (0.3) falls under gravity
+    nv, nt = int(fields["surface_v"]), int(fields["surface_t"])
+    assert nv > 0 and nt > 0
+    text = obj.read_text().splitlines()
+    assert text[:2] == ["mtllib test.mtl", "o fluid"]
+    assert sum(l.startswith("v ") for l in text) == nv and sum(l.startswith("f ") for l in text) == nt
+
+
+@pytest.mark.gpu
+def test_pyfluidengine_surface_obj_round_trip(tmp_path):
+    """The SimulationRunner sequence through PyFluidEngine: AdvanceSingleFrame, GetSurface into a TriangleMesh,
+    OBJManager.Save; OBJManager.Load reads the file back (to the file's 6 decimals)."""
+    m = pyf()
+    sim = m.APICSimulator(m.Vector3S(16, 16, 16), m.BoundingBox3D(m.Vector3D(0.0, 0.0, 0.0), m.Vector3D(1.0, 1.0, 1.0)))
+    sim.AddExternalForce(m.DirectionalField(m.Vector3D(0.0, -9.81, 0.0)))
+    sim.SetMaxClf(1.0)
+    sim.SetViscosity(0.01)
+    sim.InitializeFromRegions([dict(kind=0, lo=(0, 0, 0), hi=(0.4, 0.6, 1.0))])
+    sim.SetCurrentFrame(m.Frame(1.0 / 60.0))
+    sim.AdvanceSingleFrame()
+    mesh = m.TriangleMesh()
+    sim.GetSurface(mesh)
+    mesh.SetObjectName("fluid")
+    V, N, T = mesh.GetVertices(), mesh.GetNormals(), mesh.GetTriangles()
+    assert V.shape[0] > 0 and T.shape[0] > 0 and N.shape == V.shape
+    path = str(tmp_path / "f.obj")
+    m.OBJManager().Save(path, mesh)
+    back = m.TriangleMesh()
+    m.OBJManager().Load(path, back)
+    assert back.GetObjectName() == "fluid"
+    np.testing.assert_allclose(back.GetVertices(), V, atol=5e-7)
+    np.testing.assert_allclose(back.GetNormals(), N, atol=5e-7)
+    assert np.array_equal(back.GetTriangles(), T)
+    # GetSurface appends: a second call doubles the mesh, ids continuing after the first copy
+    sim.GetSurface(mesh)
+    T2 = mesh.GetTriangles()
+    assert T2.shape[0] == 2 * T.shape[0] and np.array_equal(T2[T.shape[0]:], T + V.shape[0])
