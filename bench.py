@@ -225,6 +225,53 @@ def diffusion_report(scene, stream, peak, peak_kind, reps=5):
                          "stage time includes the SDF scatter, face markers and list build" % JACOBI_BYTES_PER_FACE}}
 
 
+def surface_report(scene, n, reps=5, reference=True):
+    """GetSurface per frame: the band SDF of the last substep's particles and the marching-cubes mesh built on the
+    device (fe_scene_build_surface, wall time of the synchronous call), the OBJ write of that mesh, and the
+    reference's own CPU GetSurface (MarchingCubesSolver on its SDF of the same particles) for comparison."""
+    import ctypes
+    import tempfile
+
+    import numpy as np
+
+    import fluide_engine_b200 as fe
+
+    L = fe.lib()
+    nv, nt = ctypes.c_uint64(), ctypes.c_uint64()
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fe._abi.check(L.fe_scene_build_surface(scene.handle, ctypes.byref(nv), ctypes.byref(nt)))
+        times.append((time.perf_counter() - t0) * 1e3)
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        fe._abi.check(L.fe_scene_write_surface_obj(scene.handle, os.path.join(d, "f.obj").encode(), b"fluid"))
+        obj_ms = (time.perf_counter() - t0) * 1e3
+        obj_bytes = os.path.getsize(os.path.join(d, "f.obj"))
+    out = {"build_ms": sorted(times)[len(times) // 2], "build_ms_all": times, "vertices": int(nv.value),
+           "triangles": int(nt.value), "obj_write_ms": obj_ms, "obj_bytes": obj_bytes,
+           "path": "fe_scene_build_surface (device: SDF scatter, cube/cap counts, 2 scans, emit) + "
+                   "fe_scene_write_surface_obj (host: OBJManager::Save format)"}
+    if reference:
+        try:
+            import oracle
+
+            variant = "threaded" if oracle.ref_available("threaded") else ("serial" if oracle.ref_available("serial") else None)
+            if variant:
+                P = scene.particles()[0].astype(np.float64)
+                r = oracle.RefSim((n, n, n), oracle.FLIP, variant=variant)
+                r.set_particles(P)
+                r.stage("sdf")
+                t0 = time.perf_counter()
+                V, _, T = r.surface()
+                out["reference_ms"] = (time.perf_counter() - t0) * 1e3
+                out["reference_mesh"] = [int(V.shape[0]), int(T.shape[0])]
+        except Exception as ex:  # reported, never required
+            out["reference_ms"] = None
+            out["reference_error"] = str(ex)[:200]
+    return out
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -479,6 +526,8 @@ def main():
                     help="inner pressure solver: auto (multigrid-preconditioned CG from 2^22 cells, plain CG below), "
                          "mgpcg or cg")
     ap.add_argument("--workload", default="single", choices=["single", "batched", "served", "pool256"])
+    ap.add_argument("--surface", action="store_true",
+                    help="single workload: also time GetSurface (device mesh + OBJ write) after the timed region")
     ap.add_argument("--viscosity", type=float, default=0.0,
                     help="single workload / reference arm: kinematic viscosity (0 = none, as the benchmark scenes)")
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
@@ -561,6 +610,7 @@ def main():
     traffic = float(per_unit * units.mean()) if per_unit else None
     phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
     diffusion = diffusion_report(scene, stream, peak, peak_kind) if args.viscosity > 0 else None
+    surface = surface_report(scene, n, reference=not args.no_cpu_baseline) if args.surface and rank == 0 else None
 
     # end to end through the public API with host buffers: H2D particles, one substep, D2H particles
     pin_pos = torch.from_numpy(pos).pin_memory()
@@ -625,6 +675,8 @@ def main():
         }
         if diffusion:
             line["diffusion"] = diffusion
+        if surface:
+            line["surface"] = surface
         print(json.dumps(line), flush=True)
     scene.close()
     if world > 1:

@@ -8,6 +8,7 @@ from ._abi import (APIC, FLIP, PIC, AIR, FLUID, AUTO, CG, MGPCG, FluideError, ke
                    STAGE_MOVE)
 from .scene import Batch, Scene, face_shapes  # noqa: F401
 from .simulators import (APICSimulator, BoundingBox3D, DirectionalField, FLIPSimulator, Frame,  # noqa: F401
-                         HybridSimulator, OBJManager, PICSimulator, TriangleMesh, Vector3D, Vector3S)
+                         HybridSimulator, OBJManager, PICSimulator, SimulationRunner, SimulationStats, TriangleMesh,
+                         Vector3D, Vector3S)
 
 __version__ = "0.1.0"

@@ -19,8 +19,11 @@
 //               that item's case byte.
 // The arithmetic is the reference's, operation by operation in FP64 with explicit round-to-nearest intrinsics (no
 // fused multiply-add), so vertices, normals and triangles are identical to the reference's mesh.
+#include <algorithm>
 #include <cinttypes>
 #include <cstdio>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "fe_internal.cuh"
@@ -405,7 +408,38 @@ cudaError_t launch_mc_emit(const SceneView& v, const double* sdf, const uint8_t*
 
 // OBJManager::OnSave (3d/obj_manager.cpp:14-90): header, object name, "v" lines, "vn" lines, "s off", and "f a//n
 // b//n c//n" with 1-based indices; numbers as std::to_string prints them ("%f"); the normal index is written as
-// an unsigned value (a -1 prints as 0).
+// an unsigned value (a -1 prints as 0).  The lines are formatted by several host threads into per-range
+// buffers and written in order, so the file is the same bytes as a serial writer's.
+namespace {
+
+template <class F>
+void format_ranges(uint64_t n, F line, std::vector<std::string>& parts)
+{
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = (unsigned)std::min<uint64_t>(std::min(hw, 32u), (n + 16383) / 16384);
+    parts.assign(std::max(nt, 1u), std::string());
+    auto work = [&](unsigned t) {
+        const uint64_t b = n * t / std::max(nt, 1u), e = n * (t + 1) / std::max(nt, 1u);
+        std::string& out = parts[t];
+        out.reserve((size_t)(e - b) * 40);
+        char buf[160];
+        for (uint64_t i = b; i < e; ++i) {
+            const int len = line(i, buf, sizeof(buf));
+            out.append(buf, (size_t)len);
+        }
+    };
+    if (nt <= 1) {
+        work(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+}
+
+}  // namespace
+
 extern "C" fe_status fe_write_obj(const char* path, const char* object_name, const double* vertices,
                                   const double* normals, uint64_t n_vertices, const int64_t* triangles,
                                   uint64_t n_triangles)
@@ -414,22 +448,27 @@ extern "C" fe_status fe_write_obj(const char* path, const char* object_name, con
         return fe::set_error(FE_ERR_BAD_ARG, "null argument");
     FILE* f = std::fopen(path, "wb");
     if (!f) return fe::set_error(FE_ERR_BAD_ARG, "cannot open %s for writing", path);
-    std::vector<char> buf((size_t)1 << 20);
-    std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+    std::vector<std::string> parts;
+    auto put = [&](const std::string& str) { std::fwrite(str.data(), 1, str.size(), f); };
     std::fprintf(f, "mtllib test.mtl\no %s\n\n", object_name ? object_name : "");
-    for (uint64_t i = 0; i < n_vertices; ++i)
-        std::fprintf(f, "v %f %f %f\n", vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+    format_ranges(n_vertices, [&](uint64_t i, char* b, size_t cap) {
+        return std::snprintf(b, cap, "v %f %f %f\n", vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+    }, parts);
+    for (const auto& p : parts) put(p);
     std::fputs("\n", f);
-    for (uint64_t i = 0; i < n_vertices; ++i)
-        std::fprintf(f, "vn %f %f %f\n", normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]);
+    format_ranges(n_vertices, [&](uint64_t i, char* b, size_t cap) {
+        return std::snprintf(b, cap, "vn %f %f %f\n", normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]);
+    }, parts);
+    for (const auto& p : parts) put(p);
     std::fputs("\n", f);
     std::fputs("s off\n\n", f);
-    for (uint64_t i = 0; i < n_triangles; ++i) {
+    format_ranges(n_triangles, [&](uint64_t i, char* b, size_t cap) {
         const int64_t* t = triangles + 4 * i;
         const uint64_t nn = (uint64_t)t[3] + 1u;
-        std::fprintf(f, "f %" PRIu64 "//%" PRIu64 " %" PRIu64 "//%" PRIu64 " %" PRIu64 "//%" PRIu64 "\n",
-                     (uint64_t)t[0] + 1u, nn, (uint64_t)t[1] + 1u, nn, (uint64_t)t[2] + 1u, nn);
-    }
+        return std::snprintf(b, cap, "f %" PRIu64 "//%" PRIu64 " %" PRIu64 "//%" PRIu64 " %" PRIu64 "//%" PRIu64 "\n",
+                             (uint64_t)t[0] + 1u, nn, (uint64_t)t[1] + 1u, nn, (uint64_t)t[2] + 1u, nn);
+    }, parts);
+    for (const auto& p : parts) put(p);
     std::fputs("\n", f);
     const bool ok = std::ferror(f) == 0;
     if (std::fclose(f) != 0 || !ok) return fe::set_error(FE_ERR_BAD_ARG, "write to %s failed", path);

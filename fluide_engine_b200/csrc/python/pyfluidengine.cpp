@@ -175,6 +175,24 @@ PYBIND11_MODULE(PyFluidEngine, m)
                  return out;
              });
 
+    // SimulationStats / SimulationRunner (simulator_runner_wrapper.cpp)
+    py::class_<SimulationStats>(m, "SimulationStats")
+        .def(py::init<>())
+        .def("PrintStats", [](const SimulationStats& st) { st.PrintStats(); })
+        .def("Clear", &SimulationStats::Clear)
+        .def_readwrite("simulatorType", &SimulationStats::simulatorType)
+        .def_readwrite("numberOfIterations", &SimulationStats::numberOfIterations)
+        .def_readwrite("gridSize", &SimulationStats::gridSize)
+        .def_readwrite("numberOfParticles", &SimulationStats::numberOfParticles)
+        .def_readwrite("timeIntervalInSeconds", &SimulationStats::timeIntervalInSeconds)
+        .def_readwrite("simulationTimeInSeconds", &SimulationStats::simulationTimeInSeconds)
+        .def_readwrite("iterationTimeInSeconds", &SimulationStats::iterationTimeInSeconds)
+        .def_readwrite("cflPerIteration", &SimulationStats::cflPerIteration);
+    py::class_<SimulationRunner>(m, "SimulationRunner")
+        .def(py::init<>())
+        .def("RunSimulation", &SimulationRunner::RunSimulation, py::call_guard<py::gil_scoped_release>())
+        .def("GetStats", &SimulationRunner::GetStats);
+
     py::class_<PICSimulator, std::shared_ptr<PICSimulator>, HybridSimulator> pic(m, "PICSimulator");
     pic.def(py::init<Vector3<size_t>, BoundingBox3D>())
         .def("AdvanceSingleFrame", &PICSimulator::AdvanceSingleFrame, py::call_guard<py::gil_scoped_release>())

@@ -331,3 +331,101 @@ class FLIPSimulator(HybridSimulator):
 
 class APICSimulator(HybridSimulator):
     _solver = _abi.APIC
+
+
+class SimulationStats:
+    """SimulationStats (simulation_stats.hpp): per-run statistics of SimulationRunner."""
+
+    def __init__(self):
+        self.Clear()
+
+    def Clear(self):
+        self.simulatorType = ""
+        self.numberOfIterations = 0
+        self.gridSize = Vector3S(0, 0, 0)
+        self.numberOfParticles = 0
+        self.timeIntervalInSeconds = 0.0
+        self.simulationTimeInSeconds = 0.0
+        self.iterationTimeInSeconds = []
+        self.cflPerIteration = []
+
+    @staticmethod
+    def _median(v):
+        return float(np.median(v)) if len(v) else float("nan")
+
+    def PrintStats(self, out=None):
+        import sys
+
+        out = out or sys.stdout
+        mean = lambda v: float(np.mean(v)) if len(v) else 0.0  # noqa: E731
+        g = self.gridSize
+        out.write("================ SIMULATION STATS ================\n")
+        out.write("Simulator type: %s\n" % self.simulatorType)
+        out.write("Grid resolution: %d x %d x %d\n" % (g.x, g.y, g.z))
+        out.write("Number of particles: %d\n" % self.numberOfParticles)
+        out.write("Number of Iterations: %d\n" % self.numberOfIterations)
+        out.write("Time interval: %g [s]\n" % self.timeIntervalInSeconds)
+        out.write("Median CFL: %g\n" % mean(self.cflPerIteration))  # the reference's labels (simulation_stats.cpp:27-28)
+        out.write("Mean CFL: %g\n" % self._median(self.cflPerIteration))
+        out.write("Median frame: %g [s]\n" % self._median(self.iterationTimeInSeconds))
+        out.write("Mean frame: %g [s]\n" % mean(self.iterationTimeInSeconds))
+        out.write("Simulation time: %g [s]\n" % self.simulationTimeInSeconds)
+        out.write("==================================================\n")
+
+
+class SimulationRunner:
+    """SimulationRunner (simulation_runner.cpp:16-56): AdvanceSingleFrame, GetSurface and OBJ output per
+    iteration into <cache>/simulated_frames/<name>_<i>.obj, log in <cache>/log.txt.  Frame i's OBJ is written on a
+    host thread while the GPU advances frame i + 1."""
+
+    def __init__(self):
+        self._stats = SimulationStats()
+
+    def RunSimulation(self, simulator, timeIntervalInSeconds, numberOfIterations, simulationOutputName, cacheFolderPath):
+        import os
+        import threading
+        import time
+
+        simulator.SetCurrentFrame(Frame(timeIntervalInSeconds))
+        os.makedirs(os.path.join(cacheFolderPath, "simulated_frames"), exist_ok=True)
+        writer, errors = None, []
+
+        def write(path, mesh):
+            try:
+                OBJManager().Save(path, mesh)
+            except Exception as ex:  # re-raised on the calling thread
+                errors.append(ex)
+
+        with open(os.path.join(cacheFolderPath, "log.txt"), "w") as log:
+            for i in range(int(numberOfIterations)):
+                log.write("Iteration: %d\n" % i)
+                t0 = time.perf_counter()
+                simulator.AdvanceSingleFrame()
+                mesh = TriangleMesh()
+                simulator.GetSurface(mesh)
+                path = os.path.join(cacheFolderPath, "simulated_frames", "%s_%d.obj" % (simulationOutputName, i))
+                if writer is not None:
+                    writer.join()
+                if errors:
+                    raise errors[0]
+                writer = threading.Thread(target=write, args=(path, mesh))
+                writer.start()
+                dt = time.perf_counter() - t0
+                self._stats.simulationTimeInSeconds += dt
+                self._stats.iterationTimeInSeconds.append(dt)
+                self._stats.cflPerIteration.append(simulator.Cfl(timeIntervalInSeconds))
+                log.write("\n")
+            if writer is not None:
+                writer.join()
+            if errors:
+                raise errors[0]
+            self._stats.numberOfIterations = int(numberOfIterations)
+            self._stats.timeIntervalInSeconds = timeIntervalInSeconds
+            self._stats.simulatorType = type(simulator).__name__
+            self._stats.numberOfParticles = simulator.GetNumberOfParticles()
+            self._stats.gridSize = simulator.GetResolution()
+            self._stats.PrintStats(log)
+
+    def GetStats(self):
+        return self._stats
+

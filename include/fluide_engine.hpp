@@ -12,9 +12,16 @@
 #ifndef FLUIDE_ENGINE_HPP
 #define FLUIDE_ENGINE_HPP
 
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstddef>
+#include <filesystem>
+#include <limits>
+#include <numeric>
+#include <thread>
+#include <typeinfo>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -437,6 +444,107 @@ class APICSimulator : public PICSimulator {
   public:
     APICSimulator(const Vector3<size_t>& gridSize, const BoundingBox3D& domain)
         : PICSimulator(gridSize, domain, FE_SOLVER_APIC) {}
+};
+
+// SimulationStats (simulation_stats.hpp / .cpp), printed in the reference's format (including its swapped
+// "Median CFL" / "Mean CFL" labels, simulation_stats.cpp:27-28).
+class SimulationStats {
+  public:
+    void PrintStats(std::FILE* out = stdout) const
+    {
+        std::fprintf(out, "================ SIMULATION STATS ================\n");
+        std::fprintf(out, "Simulator type: %s\n", simulatorType.c_str());
+        std::fprintf(out, "Grid resolution: %zu x %zu x %zu\n", gridSize.x, gridSize.y, gridSize.z);
+        std::fprintf(out, "Number of particles: %zu\n", numberOfParticles);
+        std::fprintf(out, "Number of Iterations: %zu\n", numberOfIterations);
+        std::fprintf(out, "Time interval: %g [s]\n", timeIntervalInSeconds);
+        std::fprintf(out, "Median CFL: %g\n", Mean(cflPerIteration));
+        std::fprintf(out, "Mean CFL: %g\n", Median(cflPerIteration));
+        std::fprintf(out, "Median frame: %g [s]\n", Median(iterationTimeInSeconds));
+        std::fprintf(out, "Mean frame: %g [s]\n", Mean(iterationTimeInSeconds));
+        std::fprintf(out, "Simulation time: %g [s]\n", simulationTimeInSeconds);
+        std::fprintf(out, "==================================================\n");
+    }
+    void Clear() { *this = SimulationStats(); }
+    static double Median(std::vector<double> v)
+    {
+        if (v.empty()) return std::numeric_limits<double>::signaling_NaN();
+        auto i1 = v.begin() + (v.size() - 1) / 2, i2 = v.begin() + v.size() / 2;
+        std::nth_element(v.begin(), i1, v.end());
+        std::nth_element(i1, i2, v.end());
+        return 0.5 * (*i1 + *i2);
+    }
+    static double Mean(const std::vector<double>& v)
+    {
+        return v.empty() ? 0.0 : std::accumulate(v.begin(), v.end(), 0.0) / v.size();
+    }
+
+    std::string simulatorType;
+    size_t numberOfIterations = 0;
+    Vector3<size_t> gridSize = Vector3<size_t>(0);
+    size_t numberOfParticles = 0;
+    double timeIntervalInSeconds = 0;
+    double simulationTimeInSeconds = 0;
+    std::vector<double> iterationTimeInSeconds;
+    std::vector<double> cflPerIteration;
+};
+
+// SimulationRunner (simulation_runner.cpp:16-56): for each iteration, AdvanceSingleFrame, GetSurface and
+// OBJManager::Save to <cache>/simulated_frames/<name>_<i>.obj, with the log (iterations, stats) in <cache>/log.txt.
+// The OBJ of frame i is written by a host thread while the GPU advances frame i + 1 (the mesh is copied to the
+// host first); the per-iteration time therefore covers the frame and its surface, and the last write is waited
+// for before RunSimulation returns.
+class SimulationRunner {
+  public:
+    void RunSimulation(const std::shared_ptr<HybridSimulator> simulator, double timeIntervalInSeconds,
+                       size_t numberOfIterations, std::string simulationOutputName, std::string cacheFolderPath)
+    {
+        simulator->SetCurrentFrame(Frame(timeIntervalInSeconds));
+        std::filesystem::create_directories(cacheFolderPath);
+        std::filesystem::create_directories(cacheFolderPath + "/simulated_frames");
+        std::FILE* log = std::fopen((cacheFolderPath + "/log.txt").c_str(), "w");
+        std::thread writer;
+        std::exception_ptr write_error;
+        for (size_t i = 0; i < numberOfIterations; ++i) {
+            if (log) std::fprintf(log, "Iteration: %zu\n", i);
+            const auto start = std::chrono::steady_clock::now();
+            simulator->AdvanceSingleFrame();
+            auto surface = std::make_shared<TriangleMesh>();
+            simulator->GetSurface(*surface);
+            const std::string path = cacheFolderPath + "/simulated_frames/" + simulationOutputName + "_" +
+                                     std::to_string(i) + ".obj";
+            if (writer.joinable()) writer.join();
+            if (write_error) std::rethrow_exception(write_error);
+            writer = std::thread([surface, path, &write_error] {
+                try {
+                    OBJManager().Save(path, *surface);
+                } catch (...) {
+                    write_error = std::current_exception();
+                }
+            });
+            const auto end = std::chrono::steady_clock::now();
+            const double duration = std::chrono::duration_cast<std::chrono::nanoseconds>(end - start).count() / 1e9;
+            _stats.simulationTimeInSeconds += duration;
+            _stats.iterationTimeInSeconds.push_back(duration);
+            _stats.cflPerIteration.push_back(simulator->Cfl(timeIntervalInSeconds));
+            if (log) std::fprintf(log, "\n");
+        }
+        if (writer.joinable()) writer.join();
+        if (write_error) std::rethrow_exception(write_error);
+        _stats.numberOfIterations = numberOfIterations;
+        _stats.timeIntervalInSeconds = timeIntervalInSeconds;
+        _stats.simulatorType = typeid(*simulator.get()).name();
+        _stats.numberOfParticles = simulator->GetNumberOfParticles();
+        _stats.gridSize = simulator->GetResolution();
+        if (log) {
+            _stats.PrintStats(log);
+            std::fclose(log);
+        }
+    }
+    SimulationStats GetStats() const { return _stats; }
+
+  private:
+    SimulationStats _stats;
 };
 
 #endif  // FLUIDE_ENGINE_HPP

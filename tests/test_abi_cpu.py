@@ -83,3 +83,24 @@ def test_python_mirror_api_without_device():
     assert sim.GetViscosity() == 0.1
     with pytest.raises(ValueError):
         sim.SetViscosity(-1.0)
+
+
+def test_write_obj_matches_oracle_writer(tmp_path):
+    """fe_write_obj (host code, formatted by several threads) writes the same bytes as the oracle's serial restatement
+    of OBJManager::Save, which is pinned to the reference; no device needed."""
+    import numpy as np
+
+    import oracle
+    from fluide_engine_b200 import _abi
+
+    rng = np.random.default_rng(3)
+    nv, nt = 70001, 120003  # several formatting threads, uneven ranges
+    V = rng.standard_normal((nv, 3)) * 10.0
+    V[5] = [-0.0, 1e-7, -5e-7]  # signed zero and values that round to zero in "%f"
+    N = rng.standard_normal((nv, 3))
+    T = rng.integers(0, nv, (nt, 4)).astype(np.int64)
+    T[0, 3] = -1  # the reference's size_t(-1) normal index prints as 0
+    L = _abi.lib()
+    _abi.check(L.fe_write_obj(str(tmp_path / "a.obj").encode(), b"fluid", _abi.ptr(V), _abi.ptr(N), nv, _abi.ptr(T), nt))
+    oracle.write_obj(str(tmp_path / "b.obj"), "fluid", V, N, T)
+    assert (tmp_path / "a.obj").read_bytes() == (tmp_path / "b.obj").read_bytes()
