@@ -110,6 +110,13 @@ def lib():
         L.or_build_surface.argtypes = [D, I3, D, D, D, D, I64, ctypes.c_size_t, ctypes.c_size_t, SZ, SZ]
         L.or_write_obj.restype = ctypes.c_int
         L.or_write_obj.argtypes = [ctypes.c_char_p, ctypes.c_char_p, D, D, ctypes.c_size_t, I64, ctypes.c_size_t]
+        L.or_mesh_to_sdf.argtypes = [D, ctypes.c_size_t, I64, ctypes.c_size_t, I3, D, D, D]
+        L.or_distance_to_triangle.restype = ctypes.c_double
+        L.or_distance_to_triangle.argtypes = [D, D, D, D]
+        L.or_mesh_is_inside.restype = ctypes.c_int
+        L.or_mesh_is_inside.argtypes = [D, I64, ctypes.c_size_t, D]
+        L.or_seed_cells.argtypes = [P, U8]
+        L.or_set_sdf.argtypes = [P, D]
         L.or_seed_regions.restype = ctypes.c_size_t
         L.or_seed_regions.argtypes = [ctypes.c_void_p, ctypes.c_int, I3, D, D, ctypes.c_uint64, F, F, ctypes.c_size_t]
         _lib = L
@@ -235,6 +242,13 @@ class OracleSim:
         self.L.or_get_face_markers(self.h, u8ptr(a), u8ptr(b), u8ptr(c))
         return a, b, c
 
+    def seed_cells(self):
+        """InitializeParticles' cell mask (1: the cell receives particles) from the current fluid SDF."""
+        m = self._cells(np.uint8); self.L.or_seed_cells(self.h, u8ptr(m)); return m
+
+    def set_sdf(self, sdf):
+        sdf = np.ascontiguousarray(sdf, dtype=np.float64); self.L.or_set_sdf(self.h, dptr(sdf))
+
     def diffusion_markers(self):
         su, sv, sw = face_shapes(self.n)
         a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
@@ -304,6 +318,20 @@ def build_surface(sdf, n, origin, h):
     return V, N, T
 
 
+def mesh_to_sdf(V, T, n, origin, h):
+    """Mesh2SDF::Build of a mesh (V (nv,3), T (nt,4) int64) onto a node grid; returns (nz, ny, nx) values."""
+    L = lib()
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    T = np.ascontiguousarray(T, dtype=np.int64)
+    n3 = np.array(n, dtype=np.int32)
+    o = np.array(origin, dtype=np.float64)
+    hh = np.array(h, dtype=np.float64)
+    out = np.zeros((n[2], n[1], n[0]))
+    L.or_mesh_to_sdf(dptr(V), V.shape[0], T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), T.shape[0], iptr(n3), dptr(o),
+                     dptr(hh), dptr(out))
+    return out
+
+
 def write_obj(path, name, V, N, T):
     """OBJManager::Save of a mesh from build_surface."""
     V, N = (np.ascontiguousarray(a, dtype=np.float64) for a in (V, N))
@@ -324,6 +352,20 @@ def project(n, h, marks, u, v, w, p, rel_tol=1e-6, max_it=500):
 
 
 # ---------------------------------------------------------------------------------------- reference
+
+
+def ref_mesh_to_sdf(V, T, n, origin, h, variant="serial"):
+    """The reference's own Mesh2SDF::Build."""
+    L = ref_lib(variant)
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    T = np.ascontiguousarray(T, dtype=np.int64)
+    n3 = (ctypes.c_int * 3)(*n)
+    o = np.array(origin, dtype=np.float64)
+    hh = np.array(h, dtype=np.float64)
+    out = np.zeros((n[2], n[1], n[0]))
+    L.ref_mesh_to_sdf(dptr(V), V.shape[0], T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), T.shape[0], n3, dptr(o),
+                      dptr(hh), dptr(out))
+    return out
 
 
 def ref_available(variant="serial"):
@@ -367,6 +409,8 @@ def ref_lib(variant="serial"):
         SZ = ctypes.POINTER(ctypes.c_size_t)
         L.ref_get_surface.argtypes = [P, D, D, I64, ctypes.c_size_t, ctypes.c_size_t, SZ, SZ]
         L.ref_save_obj.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
+        L.ref_mesh_to_sdf.argtypes = [D, ctypes.c_size_t, I64, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), D, D, D]
+        L.ref_init_from_mesh.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t]
         _ref_libs[variant] = L
     return _ref_libs[variant]
 
@@ -458,6 +502,13 @@ class RefSim:
         self.L.ref_get_surface(self.h, dptr(V), dptr(N), T.ctypes.data_as(I64), nv.value, nt.value, ctypes.byref(nv),
                                ctypes.byref(nt))
         return V, N, T
+
+    def init_from_mesh(self, V, T):
+        """PICSimulator::InitializeFromTriangleMesh (Mesh2SDF into Fluid3::sdf, then InitializeParticles)."""
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.int64)
+        self.L.ref_init_from_mesh(self.h, dptr(V), V.shape[0], T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                  T.shape[0])
 
     def save_obj(self, path, name):
         """OBJManager::Save of the last surface()."""

@@ -10,7 +10,7 @@ libraries under oracle/_ref/ (git-ignored):
 * libfe_ref_threaded.so -- the loops as written (one std::thread per hardware thread); this is the
                            timed CPU baseline.
 
-The reference does not compile with g++ as written (it targets MSVC).  Four mechanical adjustments
+The reference does not compile with g++ as written (it targets MSVC).  Five mechanical adjustments
 are applied without touching the reference tree:
   1. two headers (common/parallel_utils.hpp, common/array3.hpp) bind rvalue lambdas to non-const
      references; sed-patched copies that take forwarding references are generated into
@@ -18,7 +18,11 @@ are applied without touching the reference tree:
      the originals into no-ops;
   2./3. extra member qualifications (grid_systems/face_centered_grid3d.hpp:30,
      emmiter/volume_emmiter.hpp:22) are accepted with -fpermissive;
-  4. <concurrent_vector.h> (MSVC PPL) resolves to oracle/shim/concurrent_vector.h.
+  4. <concurrent_vector.h> (MSVC PPL) resolves to oracle/shim/concurrent_vector.h;
+  5. TriangleMesh::IsInside (3d/triangle_mesh.cpp:151) calls an unqualified abs on a double, which MSVC
+     resolves to abs(double) but g++ to the C library's int abs(int) (truncating the winding sum, so no
+     point would ever be inside); a force-included header brings std::abs into the global namespace, giving
+     the MSVC meaning.  It is the reference's only unqualified abs.
 The generated headers are build intermediates and are deleted after the build.
 """
 import os
@@ -66,6 +70,8 @@ def _gen_headers(gen_dir, threaded):
     a3 = a3.replace('#include "parallel_utils.hpp"', '#include "%s"' % os.path.join(gen_dir, "parallel_utils.hpp"))
     with open(os.path.join(gen_dir, "array3.hpp"), "w") as f:
         f.write(a3)
+    with open(os.path.join(gen_dir, "msvc_abs.hpp"), "w") as f:
+        f.write("#include <cmath>\n#include <cstdlib>\nusing std::abs;\n")
 
 
 def _build_variant(name, threaded):
@@ -74,7 +80,8 @@ def _build_variant(name, threaded):
     os.makedirs(objdir, exist_ok=True)
     _gen_headers(gen, threaded)
     inc = ["-I", os.path.join(HERE, "shim"), "-I", REF, "-I", "/usr/local/cuda/include",
-           "-include", os.path.join(gen, "parallel_utils.hpp"), "-include", os.path.join(gen, "array3.hpp")]
+           "-include", os.path.join(gen, "parallel_utils.hpp"), "-include", os.path.join(gen, "array3.hpp"),
+           "-include", os.path.join(gen, "msvc_abs.hpp")]
     srcs = _sources() + [os.path.join(HERE, "ref_harness.cpp")]
 
     def compile_one(src):

@@ -1400,3 +1400,181 @@ int or_write_obj(const char* path, const char* name, const double* v, const doub
     fprintf(f, "\n");
     return fclose(f) == 0 ? 0 : -1;
 }
+
+/* ---------------------------------------------------------------- mesh -> SDF, mesh seeding */
+
+static double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static double len3(const double a[3]) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+
+/* Collisions::ClossestPointOnTriangle (3d/collisions.cpp:21-212): the region-based closest point of a triangle
+ * (Eberly, "Distance Between Point and Triangle in 3D"), in the reference's operation order. */
+static void closest_on_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3], double out[3])
+{
+    double diff[3], e0[3], e1[3];
+    for (int d = 0; d < 3; ++d) { diff[d] = p0[d] - pt[d]; e0[d] = p1[d] - p0[d]; e1[d] = p2[d] - p0[d]; }
+    const double a00 = dot3(e0, e0), a01 = dot3(e0, e1), a11 = dot3(e1, e1);
+    const double b0 = dot3(diff, e0), b1 = dot3(diff, e1);
+    const double dd = a00 * a11 - a01 * a01;
+    const double det = dd > 0.0 ? dd : 0.0; /* std::max(x, 0.0) */
+    double s = a01 * b1 - a11 * b0;
+    double t = a01 * b0 - a00 * b1;
+    if (s + t <= det) {
+        if (s < 0) {
+            if (t < 0) { /* region 4 */
+                if (b0 < 0) {
+                    t = 0;
+                    if (-b0 >= a00) s = 1; else s = -b0 / a00;
+                } else {
+                    s = 0;
+                    if (b1 >= 0) t = 0; else if (-b1 >= a11) t = 1; else t = -b1 / a11;
+                }
+            } else { /* region 3 */
+                s = 0;
+                if (b1 >= 0) t = 0; else if (-b1 >= a11) t = 1; else t = -b1 / a11;
+            }
+        } else if (t < 0) { /* region 5 */
+            t = 0;
+            if (b0 >= 0) s = 0; else if (-b0 >= a00) s = 1; else s = -b0 / a00;
+        } else { /* region 0 */
+            s /= det;
+            t /= det;
+        }
+    } else {
+        double tmp0, tmp1, numer, denom;
+        if (s < 0) { /* region 2 */
+            tmp0 = a01 + b0;
+            tmp1 = a11 + b1;
+            if (tmp1 > tmp0) {
+                numer = tmp1 - tmp0;
+                denom = a00 - 2 * a01 + a11;
+                if (numer >= denom) { s = 1; t = 0; } else { s = numer / denom; t = 1 - s; }
+            } else {
+                s = 0;
+                if (tmp1 <= 0) t = 1; else if (b1 >= 0) t = 0; else t = -b1 / a11;
+            }
+        } else if (t < 0) { /* region 6 */
+            tmp0 = a01 + b1;
+            tmp1 = a00 + b0;
+            if (tmp1 > tmp0) {
+                numer = tmp1 - tmp0;
+                denom = a00 - 2 * a01 + a11;
+                if (numer >= denom) { t = 1; s = 0; } else { t = numer / denom; s = 1 - t; }
+            } else {
+                t = 0;
+                if (tmp1 <= 0) s = 1; else if (b0 >= 0) s = 0; else s = -b0 / a00;
+            }
+        } else { /* region 1 */
+            numer = a11 + b1 - a01 - b0;
+            if (numer <= 0) { s = 0; t = 1; }
+            else {
+                denom = a00 - 2 * a01 + a11;
+                if (numer >= denom) { s = 1; t = 0; } else { s = numer / denom; t = 1 - s; }
+            }
+        }
+    }
+    for (int d = 0; d < 3; ++d) out[d] = (p0[d] + s * e0[d]) + t * e1[d];
+}
+
+/* Collisions::DistanceToTriangle (3d/collisions.cpp:214-217). */
+double or_distance_to_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3])
+{
+    double c[3], d[3];
+    closest_on_triangle(pt, p0, p1, p2, c);
+    for (int a = 0; a < 3; ++a) d[a] = c[a] - pt[a];
+    return len3(d);
+}
+
+/* TriangleMesh::IsInside (3d/triangle_mesh.cpp:120-163): the winding sum of atan2(det, k) over the triangles
+ * (half solid angles), inside when |sum| >= 2 pi - 0.001, with abs on the double (its meaning on MSVC, the
+ * reference's platform). */
+int or_mesh_is_inside(const double* V, const int64_t* T, size_t nt, const double pt[3])
+{
+    const double PI_ = 3.14159265358979323846;
+    double ret = 0;
+    for (size_t i = 0; i < nt; ++i) {
+        double A[3], B[3], C[3];
+        for (int d = 0; d < 3; ++d) {
+            A[d] = V[3 * T[4 * i] + d] - pt[d];
+            B[d] = V[3 * T[4 * i + 1] + d] - pt[d];
+            C[d] = V[3 * T[4 * i + 2] + d] - pt[d];
+        }
+        double omega = A[0] * B[1] * C[2];
+        omega += B[0] * C[1] * A[2];
+        omega += C[0] * A[1] * B[2];
+        omega -= C[0] * B[1] * A[2];
+        omega -= B[0] * A[1] * C[2];
+        omega -= A[0] * C[1] * B[2];
+        const double na = len3(A), nb = len3(B), nc = len3(C);
+        double k = na * nb * nc;
+        k += nc * ((A[0] * B[0] + A[1] * B[1]) + A[2] * B[2]);
+        k += na * ((B[0] * C[0] + B[1] * C[1]) + B[2] * C[2]);
+        k += nb * ((C[0] * A[0] + C[1] * A[1]) + C[2] * A[2]);
+        ret += atan2(omega, k);
+    }
+    return fabs(ret) >= 2.0 * PI_ - 0.001;
+}
+
+static int clampi(int v, int maxv, int minv) { return v < minv ? minv : (v > maxv ? maxv : v); }
+
+/* Mesh2SDF::Build (3d/mesh_2_sdf.cpp:14-82): ComputeExactBandDistanceField with bandwidth 1 (the fill value
+ * max(h) * (nx + ny + nz); per triangle, the nodes of its index box -- vertex coordinates times 1 / h_x on every
+ * axis, truncated, widened by the band and clamped -- take min(distance to the triangle)), then ComputeSigns. */
+void or_mesh_to_sdf(const double* V, size_t nv, const int64_t* T, size_t nt, const int n[3], const double origin[3],
+                    const double h[3], double* sdf)
+{
+    const size_t nc = (size_t)n[0] * n[1] * n[2];
+    double hmax = h[2];
+    if (h[0] >= h[1] && h[0] >= h[2]) hmax = h[0]; else if (h[1] >= h[0] && h[1] >= h[2]) hmax = h[1];
+    const double fill = hmax * (double)((size_t)n[0] + (size_t)n[1] + (size_t)n[2]);
+    for (size_t c = 0; c < nc; ++c) sdf[c] = fill;
+    if (nv == 0) return;
+    const int band = 1;
+    const double inv = 1.0 / h[0];
+    for (size_t t = 0; t < nt; ++t) {
+        const double* p = V + 3 * T[4 * t];
+        const double* q = V + 3 * T[4 * t + 1];
+        const double* r = V + 3 * T[4 * t + 2];
+        double f[3][3];
+        for (int d = 0; d < 3; ++d) { f[0][d] = p[d] * inv; f[1][d] = q[d] * inv; f[2][d] = r[d] * inv; }
+        int lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = clampi((int)fmin(f[0][d], fmin(f[1][d], f[2][d])) - band, n[d] - 1, 0);
+            hi[d] = clampi((int)fmax(f[0][d], fmax(f[1][d], f[2][d])) + band + 1, n[d] - 1, 0);
+        }
+        for (int k = lo[2]; k <= hi[2]; ++k)
+            for (int j = lo[1]; j <= hi[1]; ++j)
+                for (int i = lo[0]; i <= hi[0]; ++i) {
+                    double pt[3];
+                    grid_pos(origin, h, i, j, k, pt);
+                    const double dist = or_distance_to_triangle(pt, p, q, r);
+                    size_t c = (size_t)i + (size_t)n[0] * ((size_t)j + (size_t)n[1] * (size_t)k);
+                    if (dist < sdf[c]) sdf[c] = dist;
+                }
+    }
+    for (int k = 0; k < n[2]; ++k)
+        for (int j = 0; j < n[1]; ++j)
+            for (int i = 0; i < n[0]; ++i) {
+                double pt[3];
+                grid_pos(origin, h, i, j, k, pt);
+                if (or_mesh_is_inside(V, T, nt, pt)) {
+                    size_t c = (size_t)i + (size_t)n[0] * ((size_t)j + (size_t)n[1] * (size_t)k);
+                    sdf[c] = sdf[c] * -1.0;
+                }
+            }
+}
+
+/* PICSimulator::InitializeParticles (pic_simulator.cpp:521-548): the cells (i, j, k) of the velocity grid whose
+ * GridIndexToPosition (its origin, the domain origin, + h * index) has a fluid-SDF sample < 0 receive
+ * particlesPerBlock particles in [position, position + h).  Writes 1 / 0 per cell. */
+void or_seed_cells(const or_sim* s, uint8_t* mask)
+{
+    for (int k = 0; k < s->n.z; ++k)
+        for (int j = 0; j < s->n.y; ++j)
+            for (int i = 0; i < s->n.x; ++i) {
+                double pt[3];
+                grid_pos(s->d.origin, s->h, i, j, k, pt);
+                mask[ix3(s->n, i, j, k)] = sample3(s->sdf, s->n, s->sdf_origin, s->h, pt) < 0 ? 1 : 0;
+            }
+}
+
+void or_set_sdf(or_sim* s, const double* sdf) { memcpy(s->sdf, sdf, cnt3(s->n) * sizeof(double)); }

@@ -110,6 +110,16 @@ int or_build_surface(const double* sdf, const int n[3], const double origin[3], 
 int or_write_obj(const char* path, const char* name, const double* v, const double* vn, size_t nv, const int64_t* t,
                  size_t nt);
 
+/* Mesh2SDF::Build (3d/mesh_2_sdf.cpp:14-82) of a triangle mesh (V: 3 doubles per vertex, T: 4 int64 per triangle,
+ * the last unused) onto a node grid n[3] with origin and spacing; sdf receives n[0]*n[1]*n[2] values, x-fastest. */
+void or_mesh_to_sdf(const double* V, size_t nv, const int64_t* T, size_t nt, const int n[3], const double origin[3],
+                    const double h[3], double* sdf);
+double or_distance_to_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3]);
+int or_mesh_is_inside(const double* V, const int64_t* T, size_t nt, const double pt[3]);
+/* InitializeParticles' cell test on the simulator's current fluid SDF (1 where particles would be seeded). */
+void or_seed_cells(const or_sim* s, uint8_t* mask);
+void or_set_sdf(or_sim* s, const double* sdf);
+
 /* Stable counting sort of FP32 particle positions by fe_keys.h cell key; writes keys and perm. */
 void or_sort_keys(const float* pos, size_t n, const int dims[3], const float origin[3], const float inv_h[3],
                   uint32_t* keys_sorted, uint32_t* perm);

@@ -26,6 +26,7 @@
 #include "linear_system/blas.hpp"
 #include "linear_system/cuda_jacobi_iteration_solver.hpp"
 #include "linear_system/jacobi_iteration_solver.hpp"
+#include "3d/mesh_2_sdf.hpp"
 #include "fluid_solvers/backward_euler_diffusion_solver.hpp"
 #include "forces/directional_field.hpp"
 #undef private
@@ -280,6 +281,36 @@ void ref_get_surface(void* p, double* v, double* n, int64_t* t, size_t cap_v, si
         t[4 * i] = (int64_t)T[i].point1Idx; t[4 * i + 1] = (int64_t)T[i].point2Idx;
         t[4 * i + 2] = (int64_t)T[i].point3Idx; t[4 * i + 3] = (int64_t)T[i].normalIdx;
     }
+}
+
+static TriangleMesh make_mesh(const double* v, size_t nv, const int64_t* t, size_t nt)
+{
+    TriangleMesh mesh;
+    for (size_t i = 0; i < nv; ++i) mesh.AddVertex(Vector3<double>(v[3 * i], v[3 * i + 1], v[3 * i + 2]));
+    for (size_t i = 0; i < nt; ++i)
+        mesh.AddTriangle(Triangle3D_t((size_t)t[4 * i], (size_t)t[4 * i + 1], (size_t)t[4 * i + 2], (size_t)t[4 * i + 3]));
+    return mesh;
+}
+
+// Mesh2SDF::Build (3d/mesh_2_sdf.cpp:14-18) onto a ScalarGrid3D of the given size, origin and spacing.
+void ref_mesh_to_sdf(const double* v, size_t nv, const int64_t* t, size_t nt, const int* n, const double* origin,
+                     const double* h, double* out)
+{
+    TriangleMesh mesh = make_mesh(v, nv, t, nt);
+    ScalarGrid3D sdf(Vector3<size_t>(n[0], n[1], n[2]), 0.0, Vector3<double>(origin[0], origin[1], origin[2]),
+                     Vector3<double>(h[0], h[1], h[2]));
+    Mesh2SDF().Build(mesh, sdf);
+    each3(sdf, [&](size_t i, size_t j, size_t k, size_t c) { out[c] = sdf(i, j, k); });
+}
+
+// PICSimulator::InitializeFromTriangleMesh (pic_simulator.cpp:33-39).
+void ref_init_from_mesh(void* p, const double* v, size_t nv, const int64_t* t, size_t nt)
+{
+    Handle* h = (Handle*)p;
+    TriangleMesh mesh = make_mesh(v, nv, t, nt);
+    quiet(h, true);
+    h->sim->InitializeFromTriangleMesh(mesh);
+    quiet(h, false);
 }
 
 // OBJManager::Save of the last GetSurface mesh under the given object name.
