@@ -3,7 +3,8 @@
 The compute path is the sm_100a library libfluide_b200.so (CUDA kernels + C ABI, include/fluide_b200.h);
 this package binds it with ctypes and mirrors the reference's simulator API.
 """
-from ._abi import (APIC, FLIP, PIC, AIR, FLUID, AUTO, CG, MGPCG, FluideError, kernel_launch_count, lib, seed_regions,  # noqa: F401
+from ._abi import (APIC, FLIP, PIC, AIR, FLUID, AUTO, CG, MGPCG, FluideError, kernel_launch_count, lib,  # noqa: F401
+                   mesh_to_sdf, seed_regions,
                    STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_DIFFUSE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P,
                    STAGE_MOVE)
 from .scene import Batch, Scene, face_shapes  # noqa: F401

@@ -30,7 +30,8 @@ EXPORTS = [
     "fe_scene_get_grid", "fe_scene_set_grid", "fe_scene_set_pressure", "fe_scene_get_face_markers",
     "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_set_viscosity",
     "fe_scene_get_diffusion", "fe_scene_build_surface", "fe_scene_get_surface", "fe_scene_write_surface_obj",
-    "fe_write_obj", "fe_scene_get_sort", "fe_scene_divergence",
+    "fe_write_obj", "fe_mesh_to_sdf", "fe_scene_init_from_mesh", "fe_scene_add_volume_emitter", "fe_scene_clear_emitters",
+    "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
     "fe_abi_version",
@@ -110,6 +111,11 @@ def lib():
     L.fe_scene_get_surface.argtypes = [P, P, P, P]
     L.fe_scene_write_surface_obj.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
     L.fe_write_obj.argtypes = [ctypes.c_char_p, ctypes.c_char_p, P, P, ctypes.c_uint64, P, ctypes.c_uint64]
+    L.fe_mesh_to_sdf.argtypes = [P, ctypes.c_uint64, P, ctypes.c_uint64, P, P, P, P, ctypes.c_int32]
+    L.fe_scene_init_from_mesh.argtypes = [P, P, ctypes.c_uint64, P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
+    L.fe_scene_add_volume_emitter.argtypes = [P, P, ctypes.c_uint64, P, ctypes.c_uint64, P, P, P, ctypes.c_uint32, P,
+                                              ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]
+    L.fe_scene_clear_emitters.argtypes = [P]
     L.fe_scene_get_sort.argtypes = [P, P, P, ctypes.c_uint64]
     L.fe_scene_divergence.argtypes = [P, D]
     L.fe_scene_set_stream.argtypes = [P, P]
@@ -180,3 +186,18 @@ def seed_regions(regions, n, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), seed=
     vel = np.zeros((cnt, 3), dtype=np.float32)
     L.fe_seed_regions(ctypes.cast(arr, ctypes.c_void_p), len(regions), n3, o, s, seed, ptr(pos), ptr(vel), cnt)
     return pos, vel
+
+
+def mesh_to_sdf(vertices, triangles, n, origin, spacing, device=0):
+    """Mesh2SDF::Build on the GPU (fe_mesh_to_sdf): node values (nz, ny, nx) float64."""
+    L = lib()
+    V = np.ascontiguousarray(vertices, dtype=np.float64)
+    T = np.ascontiguousarray(triangles, dtype=np.int64)
+    if T.ndim == 2 and T.shape[1] == 3:
+        T = np.ascontiguousarray(np.concatenate([T, np.zeros((T.shape[0], 1), np.int64)], axis=1))
+    out = np.zeros((n[2], n[1], n[0]))
+    n3 = (ctypes.c_int32 * 3)(*n)
+    o = (ctypes.c_double * 3)(*origin)
+    h = (ctypes.c_double * 3)(*spacing)
+    check(L.fe_mesh_to_sdf(ptr(V), V.shape[0], ptr(T), T.shape[0], n3, o, h, ptr(out), device))
+    return out

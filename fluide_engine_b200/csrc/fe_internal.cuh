@@ -289,6 +289,20 @@ cudaError_t launch_mc_count(const SceneView& v, const double* sdf, uint8_t* cfg,
 cudaError_t launch_mc_emit(const SceneView& v, const double* sdf, const uint8_t* cfg, const uint32_t* vbase,
                            const uint32_t* tbase, double* V, double* N, int64_t* T, cudaStream_t st);
 
+// Scene initialisation from meshes (fe_mesh.cu).  Mesh2SDF onto a node grid (scratch: one u64 per node); the
+// InitializeParticles and VolumeEmitter counts per node (particles per block where the rule holds); spawning the
+// counted particles at node position + h * U[0,1]^3 into v's arrays from index `base` on.
+cudaError_t launch_mesh_to_sdf(const double* V, uint64_t nv, const int64_t* T, uint64_t nt, const int n[3],
+                               const double o[3], const double h[3], unsigned long long* scratch, double* sdf,
+                               cudaStream_t st);
+cudaError_t launch_seed_count(const double* fluid_sdf, const int n[3], const double sdf_o[3], const double h[3],
+                              const double vel_o[3], uint32_t ppb, uint32_t* count, cudaStream_t st);
+cudaError_t launch_emit_count(const double* emitter_sdf, const int en[3], const double* fluid_sdf, int fnx, int fny,
+                              uint32_t ppb, uint32_t* count, cudaStream_t st);
+cudaError_t launch_spawn(const int n[3], const double o[3], const double h[3], const uint32_t* count,
+                         const uint32_t* offset, uint64_t seed, const SceneView& v, uint64_t base, const float vel[3],
+                         cudaStream_t st);
+
 // Viscosity (fe_diffuse.cu): ComputeDiffusion on the velocity buffers u, vv, ww (face markers, FLUID-face list,
 // persistent Jacobi solve, wall layers zeroed).  Uses the scene's solver barrier and error words (CgWork).
 cudaError_t launch_diffuse(const SceneView& v, const DiffWork& d, const CgWork& w, float* u, float* vv, float* ww,

@@ -130,6 +130,23 @@ struct fe_scene {
     // true once a substep's sort has run since the particles were set: the other particle set then holds the
     // positions at the start of the last substep, from which the reference's Fluid3::sdf was built
     bool prev_valid = false;
+    // Fluid3::sdf holds the mesh SDF of fe_scene_init_from_mesh (in surf.sdf) until the next substep
+    bool mesh_sdf = false;
+    // VolumeEmitters (fe_mesh.cu): each emits at the start of every substep
+    struct Emitter {
+        int n[3];
+        double o[3], h[3];
+        double* sdf = nullptr;
+        uint32_t* count = nullptr;
+        uint32_t* offset = nullptr;
+        void* tmp = nullptr;
+        size_t tmp_bytes = 0;
+        uint32_t ppb = 8;
+        float vel[3] = {0, 0, 0};
+        uint64_t seed = 0, calls = 0;
+        std::vector<void*> allocs;
+    };
+    std::vector<Emitter> emitters;
     uint64_t epoch = 0;                // bumped when the substep's kernel sequence changes (batches re-capture)
     double* d_scalar = nullptr;        // CFL / divergence result
     float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
@@ -420,10 +437,14 @@ fe_status alloc_grid(fe_scene* s)
     return FE_OK;
 }
 
-fe_status alloc_particles(fe_scene* s, uint64_t cap)
+// Allocates both particle sets and the per-particle scratch for `cap` particles; the first `keep` particles of
+// the current set are copied into set 0 (which becomes current) before the old buffers are released.
+fe_status alloc_particles(fe_scene* s, uint64_t cap, uint64_t keep = 0)
 {
     drop_graphs(s);
-    free_list(s->particle_allocs, s->stream);
+    std::vector<void*> old = std::move(s->particle_allocs);
+    s->particle_allocs.clear();
+    const ParticleSet src = s->set[s->parity];
     auto& L = s->particle_allocs;
     const bool apic = s->desc.solver == FE_SOLVER_APIC;
     for (int k = 0; k < 2; ++k) {
@@ -446,6 +467,21 @@ fe_status alloc_particles(fe_scene* s, uint64_t cap)
     FE_CUDA(dalloc(L, &v.perm, cap, s->device, s->stream));
     FE_CUDA(dalloc(L, &s->staging, cap * 9, s->device, s->stream));
     FE_CUDA(dalloc(L, &s->staging_u32, cap, s->device, s->stream));
+    if (keep) {
+        const ParticleSet& dst = s->set[0];
+        auto cp = [&](void* d, const void* sp, size_t bytes) {
+            return cudaMemcpyAsync(d, sp, bytes, cudaMemcpyDeviceToDevice, s->stream);
+        };
+        const size_t fb = keep * sizeof(float);
+        FE_CUDA(cp(dst.px, src.px, fb)); FE_CUDA(cp(dst.py, src.py, fb)); FE_CUDA(cp(dst.pz, src.pz, fb));
+        FE_CUDA(cp(dst.vx, src.vx, fb)); FE_CUDA(cp(dst.vy, src.vy, fb)); FE_CUDA(cp(dst.vz, src.vz, fb));
+        FE_CUDA(cp(dst.pid, src.pid, keep * sizeof(uint32_t)));
+        for (int a = 0; a < 9; ++a)
+            if (dst.c[a] && src.c[a]) FE_CUDA(cp(dst.c[a], src.c[a], fb));
+        s->parity = 0;
+        s->prev_valid = false;  // the other set no longer holds the last substep's start
+    }
+    free_list(old, s->stream);  // stream order: after the copies
     s->cap = cap;
     return FE_OK;
 }
@@ -496,6 +532,7 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             FE_CUDA(launch_gather(v, dst, st));
             s->parity ^= 1;
             s->prev_valid = true;
+            s->mesh_sdf = false;
             break;
         }
         case kStepP2g:
@@ -624,8 +661,22 @@ fe_status capture_graphs(fe_scene* s, int parity, double dt)
 
 // One substep: the three phase graphs of the current parity (captured on first use for this dt); when
 // `ev` is non-null, events ev[0..3] are recorded before, between and after the phases.
+fe_status emit_particles(fe_scene* s);
+
 fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
 {
+    if (!s->emitters.empty()) {
+        // emitters change the particle count every substep: direct launches, no graphs
+        fe_status st = emit_particles(s);
+        if (st != FE_OK) return st;
+        for (int ph = 0; ph < 3; ++ph) {
+            if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
+            st = enqueue_steps(s, dt, kPhaseFirst[ph], kPhaseLast[ph]);
+            if (st != FE_OK) return st;
+        }
+        if (ev) FE_CUDA(cudaEventRecord(ev[3], s->stream));
+        return FE_OK;
+    }
     if (!s->graphs_disabled) {
         if (s->graph_dt != dt) {
             drop_graphs(s);
@@ -660,6 +711,7 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
     if (ev) FE_CUDA(cudaEventRecord(ev[3], s->stream));
     s->parity ^= 1;  // the sort inside the first graph flipped the buffer sets
     s->prev_valid = true;
+    s->mesh_sdf = false;
     s->grid_cur = 0;
     return FE_OK;
 }
@@ -667,7 +719,7 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
 // The band SDF from which the reference's last Fluid3::sdf was built: the positions at the start of the last
 // substep (the other particle set, once a substep has run), else the current particles.  Allocates the surface
 // buffers on first use.
-fe_status surface_sdf(fe_scene* s)
+fe_status surf_alloc(fe_scene* s)
 {
     auto& w = s->surf;
     const SceneView& b = s->base;
@@ -691,8 +743,57 @@ fe_status surface_sdf(fe_scene* s)
         w.tmp = tmp;
         FE_CUDA(cudaStreamSynchronize(st));
     }
+    return FE_OK;
+}
+
+// Fluid3::sdf as the reference holds it now, into surf.sdf: the mesh SDF of fe_scene_init_from_mesh until the next
+// substep; else the band SDF of the particles at the start of the last substep (or of the current particles before
+// any substep).
+fe_status surface_sdf(fe_scene* s)
+{
+    fe_status st = surf_alloc(s);
+    if (st != FE_OK) return st;
+    if (!s->prev_valid && s->mesh_sdf) return FE_OK;
     const SceneView v = view_of(s, s->prev_valid ? (s->parity ^ 1) : s->parity);
-    FE_CUDA(launch_node_sdf(v, w.node, w.sdf, s->stream));
+    FE_CUDA(launch_node_sdf(v, s->surf.node, s->surf.sdf, s->stream));
+    return FE_OK;
+}
+
+// PICSimulator::OnBeginAdvanceTimeStep's emitter loop (pic_simulator.cpp:160-163): every VolumeEmitter adds its
+// particles to the current set before the substep, reading the fluid SDF the previous substep built (zero -- the
+// initial value of Fluid3::sdf -- before any substep and without a mesh initialisation).  The counts are read back
+// to size the particle arrays, so a substep with emitters runs without graphs.
+fe_status emit_particles(fe_scene* s)
+{
+    if (s->emitters.empty()) return FE_OK;
+    cudaStream_t st = s->stream;
+    const double* fluid = nullptr;
+    if (s->prev_valid || s->mesh_sdf) {
+        fe_status e = surface_sdf(s);
+        if (e != FE_OK) return e;
+        fluid = s->surf.sdf;
+    }
+    const SceneView& b = s->base;
+    for (auto& em : s->emitters) {
+        const size_t nc = (size_t)em.n[0] * em.n[1] * em.n[2];
+        FE_CUDA(launch_emit_count(em.sdf, em.n, fluid, b.g.nx, b.g.ny, em.ppb, em.count, st));
+        FE_CUDA(launch_exclusive_scan(em.count, (uint32_t)nc, em.offset, em.tmp, em.tmp_bytes, st));
+        uint32_t total = 0;
+        FE_CUDA(cudaMemcpyAsync(&total, em.offset + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        FE_CUDA(cudaStreamSynchronize(st));
+        const uint64_t np = s->base.np;
+        if (!total) continue;
+        if (np + total >= (1ull << 32)) return set_error(FE_ERR_BAD_ARG, "too many particles (2^32)");
+        if (np + total > s->cap || !s->set[0].px) {
+            fe_status e = alloc_particles(s, std::max<uint64_t>((np + total) * 5 / 4, 1024), np);
+            if (e != FE_OK) return e;
+        }
+        FE_CUDA(launch_spawn(em.n, em.o, em.h, em.count, em.offset, em.seed + 0x9E3779B97F4A7C15ull * ++em.calls,
+                             view_of(s, s->parity), np, em.vel, st));
+        s->base.np = np + total;
+        s->have_particles = true;
+        drop_graphs(s);  // graphs are sized by the particle count
+    }
     return FE_OK;
 }
 
@@ -820,6 +921,7 @@ fe_status fe_scene_destroy(fe_scene* s)
     free_list(s->allocs, s->own_stream);
     free_list(s->particle_allocs, s->own_stream);
     free_list(s->surf.mesh_allocs, s->own_stream);
+    for (auto& e : s->emitters) free_list(e.allocs, s->own_stream);
     cudaStreamDestroy(s->own_stream);  // its pending frees still run
     delete s;
     return FE_OK;
@@ -890,6 +992,9 @@ fe_status fe_scene_reset(fe_scene* s)
     FE_CUDA(cudaStreamSynchronize(st));
     s->grid_cur = 0;
     s->prev_valid = false;
+    s->mesh_sdf = false;
+    for (auto& e : s->emitters) free_list(e.allocs, s->stream);
+    s->emitters.clear();
     return FE_OK;
 }
 
@@ -1129,6 +1234,203 @@ fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf)
     const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
     FE_CUDA(cudaMemcpyAsync(sdf, s->surf.sdf, nc * sizeof(double), cudaMemcpyDefault, s->stream));
     FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+}  // extern "C"
+
+namespace fe {
+namespace {
+
+// Copies a mesh (host or device pointers) into pool memory on `st`; the caller frees `list` in stream order.
+fe_status upload_mesh(const double* V, uint64_t nv, const int64_t* T, uint64_t nt, int device, cudaStream_t st,
+                      std::vector<void*>& list, double** dV, int64_t** dT)
+{
+    if ((nv && !V) || (nt && !T)) return set_error(FE_ERR_BAD_ARG, "null mesh arrays");
+    std::vector<int64_t> check;
+    FE_CUDA(dalloc(list, dV, std::max<uint64_t>(3 * nv, 1), device, st));
+    FE_CUDA(dalloc(list, dT, std::max<uint64_t>(4 * nt, 1), device, st));
+    if (nv) FE_CUDA(cudaMemcpyAsync(*dV, V, 3 * nv * sizeof(double), cudaMemcpyDefault, st));
+    if (nt) {
+        FE_CUDA(cudaMemcpyAsync(*dT, T, 4 * nt * sizeof(int64_t), cudaMemcpyDefault, st));
+        // vertex ids are validated on the host (a device kernel must never read outside the vertex array)
+        check.resize(4 * nt);
+        FE_CUDA(cudaMemcpyAsync(check.data(), *dT, 4 * nt * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        FE_CUDA(cudaStreamSynchronize(st));
+        for (uint64_t t = 0; t < nt; ++t)
+            for (int q = 0; q < 3; ++q)
+                if (check[4 * t + q] < 0 || (uint64_t)check[4 * t + q] >= nv)
+                    return set_error(FE_ERR_BAD_ARG, "triangle %llu references vertex %lld of %llu", (unsigned long long)t,
+                                     (long long)check[4 * t + q], (unsigned long long)nv);
+    }
+    return FE_OK;
+}
+
+// Counted particles (count per node, scanned into offset) appended to the scene's current particles.
+fe_status append_counted(fe_scene* s, const int n[3], const double o[3], const double h[3], const uint32_t* count,
+                         uint32_t* offset, void* tmp, size_t tmp_bytes, uint64_t seed, const float vel[3])
+{
+    cudaStream_t st = s->stream;
+    const size_t nc = (size_t)n[0] * n[1] * n[2];
+    FE_CUDA(launch_exclusive_scan(count, (uint32_t)nc, offset, tmp, tmp_bytes, st));
+    uint32_t total = 0;
+    FE_CUDA(cudaMemcpyAsync(&total, offset + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    FE_CUDA(cudaStreamSynchronize(st));
+    if (!total) return FE_OK;
+    const uint64_t np = s->have_particles ? s->base.np : 0;
+    if (np + total >= (1ull << 32)) return set_error(FE_ERR_BAD_ARG, "too many particles (2^32)");
+    if (np + total > s->cap || !s->set[0].px) {
+        fe_status e = alloc_particles(s, std::max<uint64_t>(np + total, 1), np);
+        if (e != FE_OK) return e;
+    }
+    FE_CUDA(launch_spawn(n, o, h, count, offset, seed, view_of(s, s->parity), np, vel, st));
+    FE_CUDA(cudaStreamSynchronize(st));
+    s->base.np = np + total;
+    s->have_particles = true;
+    drop_graphs(s);
+    return FE_OK;
+}
+
+}  // namespace
+}  // namespace fe
+
+extern "C" {
+
+fe_status fe_mesh_to_sdf(const double* vertices, uint64_t n_vertices, const int64_t* triangles, uint64_t n_triangles,
+                         const int32_t n[3], const double origin[3], const double spacing[3], double* sdf, int32_t device)
+{
+    if (!n || !origin || !spacing || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
+    for (int a = 0; a < 3; ++a)
+        if (n[a] < 1 || !(spacing[a] > 0.0)) return set_error(FE_ERR_BAD_ARG, "bad grid");
+    FE_CUDA(cudaSetDevice(device));
+    cudaStream_t st;
+    FE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    std::vector<void*> list;
+    double* dV = nullptr;
+    int64_t* dT = nullptr;
+    const size_t nc = (size_t)n[0] * n[1] * n[2];
+    unsigned long long* scratch = nullptr;
+    double* dsdf = nullptr;
+    const int nn[3] = {n[0], n[1], n[2]};
+    fe_status r = upload_mesh(vertices, n_vertices, triangles, n_triangles, device, st, list, &dV, &dT);
+    cudaError_t e = cudaSuccess;
+    if (r == FE_OK) e = dalloc(list, &scratch, nc, device, st);
+    if (r == FE_OK && e == cudaSuccess) e = dalloc(list, &dsdf, nc, device, st);
+    if (r == FE_OK && e == cudaSuccess) e = launch_mesh_to_sdf(dV, n_vertices, dT, n_triangles, nn, origin, spacing, scratch, dsdf, st);
+    if (r == FE_OK && e == cudaSuccess) e = cudaMemcpyAsync(sdf, dsdf, nc * sizeof(double), cudaMemcpyDefault, st);
+    if (r == FE_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    free_list(list, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (r != FE_OK) return r;
+    return cuda_check(e, "mesh to sdf");
+}
+
+fe_status fe_scene_init_from_mesh(fe_scene* s, const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                  uint64_t n_triangles, uint32_t particles_per_cell, uint64_t seed)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    fe_status r = surf_alloc(s);
+    if (r != FE_OK) return r;
+    const SceneView& b = s->base;
+    const int n[3] = {b.g.nx, b.g.ny, b.g.nz};
+    const size_t nc = (size_t)n[0] * n[1] * n[2];
+    cudaStream_t st = s->stream;
+    std::vector<void*> list;
+    double* dV = nullptr;
+    int64_t* dT = nullptr;
+    r = upload_mesh(vertices, n_vertices, triangles, n_triangles, s->device, st, list, &dV, &dT);
+    uint32_t *count = nullptr, *offset = nullptr;
+    uint8_t* tmp = nullptr;
+    const size_t tmp_bytes = sort_scan_tmp_bytes((uint32_t)nc);
+    cudaError_t e = cudaSuccess;
+    if (r == FE_OK) e = dalloc(list, &count, nc, s->device, st);
+    if (r == FE_OK && e == cudaSuccess) e = dalloc(list, &offset, nc + 1, s->device, st);
+    if (r == FE_OK && e == cudaSuccess) e = dalloc(list, &tmp, tmp_bytes, s->device, st);
+    // Mesh2SDF into Fluid3::sdf, then InitializeParticles on it
+    if (r == FE_OK && e == cudaSuccess)
+        e = launch_mesh_to_sdf(dV, n_vertices, dT, n_triangles, n, b.sdf_origin, b.h, s->surf.node, s->surf.sdf, st);
+    if (r == FE_OK && e == cudaSuccess) {
+        s->mesh_sdf = true;
+        s->prev_valid = false;
+        e = launch_seed_count(s->surf.sdf, n, b.sdf_origin, b.h, b.origin, particles_per_cell ? particles_per_cell : 16u,
+                              count, st);
+    }
+    if (r == FE_OK && e == cudaSuccess) {
+        const float zero[3] = {0.f, 0.f, 0.f};
+        r = append_counted(s, n, b.origin, b.h, count, offset, tmp, tmp_bytes, seed, zero);
+    }
+    free_list(list, st);
+    cudaStreamSynchronize(st);
+    if (r != FE_OK) return r;
+    return cuda_check(e, "init from mesh");
+}
+
+fe_status fe_scene_add_volume_emitter(fe_scene* s, const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                      uint64_t n_triangles, const int32_t resolution[3], const double domain_origin[3],
+                                      const double domain_size[3], uint32_t particles_per_block, const double velocity[3],
+                                      uint64_t seed, int32_t* id)
+{
+    if (!s || !resolution || !domain_origin || !domain_size || !velocity) return set_error(FE_ERR_BAD_ARG, "null argument");
+    const SceneView& b = s->base;
+    const int gn[3] = {b.g.nx, b.g.ny, b.g.nz};
+    for (int a = 0; a < 3; ++a) {
+        if (resolution[a] < 1 || resolution[a] > gn[a])
+            return set_error(FE_ERR_BAD_ARG, "emitter resolution must be within the scene's grid (it indexes the fluid SDF)");
+        if (!(domain_size[a] > 0.0)) return set_error(FE_ERR_BAD_ARG, "bad emitter domain");
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    fe_scene::Emitter em;
+    for (int a = 0; a < 3; ++a) {
+        em.n[a] = resolution[a];
+        em.o[a] = domain_origin[a];
+        em.h[a] = domain_size[a] / resolution[a];  // volume_emmiter.cpp:12
+        em.vel[a] = (float)velocity[a];
+    }
+    em.ppb = particles_per_block;
+    em.seed = seed;
+    const size_t nc = (size_t)em.n[0] * em.n[1] * em.n[2];
+    em.tmp_bytes = sort_scan_tmp_bytes((uint32_t)nc);
+    cudaStream_t st = s->stream;
+    uint8_t* tmp = nullptr;
+    FE_CUDA(dalloc(em.allocs, &em.sdf, nc, s->device, st));
+    FE_CUDA(dalloc(em.allocs, &em.count, nc, s->device, st));
+    FE_CUDA(dalloc(em.allocs, &em.offset, nc + 1, s->device, st));
+    FE_CUDA(dalloc(em.allocs, &tmp, em.tmp_bytes, s->device, st));
+    em.tmp = tmp;
+    s->emitters.push_back(std::move(em));
+    const int32_t idx = (int32_t)s->emitters.size() - 1;
+    if (id) *id = idx;
+    // VolumeEmitter::InitializeFromTriangleMesh: Mesh2SDF onto the emitter's grid
+    auto& e2 = s->emitters.back();
+    std::vector<void*> list;
+    double* dV = nullptr;
+    int64_t* dT = nullptr;
+    fe_status r = upload_mesh(vertices, n_vertices, triangles, n_triangles, s->device, st, list, &dV, &dT);
+    unsigned long long* scratch = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (r == FE_OK) e = dalloc(list, &scratch, nc, s->device, st);
+    if (r == FE_OK && e == cudaSuccess) e = launch_mesh_to_sdf(dV, n_vertices, dT, n_triangles, e2.n, e2.o, e2.h, scratch, e2.sdf, st);
+    free_list(list, st);
+    cudaStreamSynchronize(st);
+    if (r == FE_OK && e != cudaSuccess) r = cuda_check(e, "emitter sdf");
+    if (r != FE_OK) {
+        free_list(s->emitters.back().allocs, st);
+        s->emitters.pop_back();
+    }
+    return r;
+}
+
+fe_status fe_scene_clear_emitters(fe_scene* s)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    for (auto& e : s->emitters) free_list(e.allocs, s->stream);
+    s->emitters.clear();
     return FE_OK;
 }
 
@@ -1435,6 +1737,7 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = null
         FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
         s->parity ^= 1;  // the pre-solve graph's sort flipped the particle buffer sets
         s->prev_valid = true;
+        s->mesh_sdf = false;
         s->grid_cur = 0;
     }
     if (ev) FE_CUDA(cudaEventRecord(ev[3], b->stream));
@@ -1451,6 +1754,8 @@ fe_status batch_check_scenes(fe_scene* const* scenes, int32_t count)
         if (scenes[i]->device != scenes[0]->device)
             return set_error(FE_ERR_BAD_ARG, "all scenes of a batch must share a device");
         if (!scenes[i]->have_particles) return set_error(FE_ERR_STATE, "scene %d has no particles", i);
+        if (!scenes[i]->emitters.empty())
+            return set_error(FE_ERR_BAD_ARG, "scene %d has emitters (its particle count changes every substep): step it alone", i);
         for (int j = 0; j < i; ++j)
             if (scenes[j] == scenes[i]) return set_error(FE_ERR_BAD_ARG, "scene %d appears twice", i);
     }
@@ -1692,6 +1997,7 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
         for (fe_scene* s : b->scenes) {
             s->parity ^= 1;
             s->prev_valid = true;
+            s->mesh_sdf = false;
             s->grid_cur = 0;
         }
     }

@@ -7,6 +7,14 @@ from . import _abi
 from ._abi import check, ptr
 
 
+def _tri4(triangles):
+    """Triangles as (T, 4) int64 (three vertex ids and an unused normal id), from (T, 3) or (T, 4)."""
+    T = np.asarray(triangles, dtype=np.int64)
+    if T.ndim == 2 and T.shape[1] == 3:
+        T = np.concatenate([T, np.zeros((T.shape[0], 1), np.int64)], axis=1)
+    return np.ascontiguousarray(T)
+
+
 def face_shapes(n):
     """numpy shapes (z, y, x) of the u, v, w face arrays; memory is x-fastest like the reference's Array3."""
     nx, ny, nz = n
@@ -155,6 +163,27 @@ class Scene:
         s = np.zeros((nz, ny, nx), dtype=np.float64)
         check(self._L.fe_scene_get_fluid_sdf(self._h, ptr(s)))
         return s
+
+    def init_from_mesh(self, vertices, triangles, particles_per_cell=0, seed=0):
+        """InitializeFromTriangleMesh: mesh SDF as the fluid SDF, particles appended in the cells inside it."""
+        V = np.ascontiguousarray(vertices, dtype=np.float64)
+        T = _tri4(triangles)
+        check(self._L.fe_scene_init_from_mesh(self._h, ptr(V), V.shape[0], ptr(T), T.shape[0], particles_per_cell, seed))
+
+    def add_volume_emitter(self, vertices, triangles, resolution, domain_origin, domain_size, particles_per_block=8,
+                           velocity=(0.0, 0.0, 0.0), seed=0):
+        """VolumeEmitter: emits at the start of every substep; returns its id."""
+        V = np.ascontiguousarray(vertices, dtype=np.float64)
+        T = _tri4(triangles)
+        eid = ctypes.c_int32()
+        check(self._L.fe_scene_add_volume_emitter(
+            self._h, ptr(V), V.shape[0], ptr(T), T.shape[0], (ctypes.c_int32 * 3)(*resolution),
+            (ctypes.c_double * 3)(*domain_origin), (ctypes.c_double * 3)(*domain_size), particles_per_block,
+            (ctypes.c_double * 3)(*velocity), seed, ctypes.byref(eid)))
+        return eid.value
+
+    def clear_emitters(self):
+        check(self._L.fe_scene_clear_emitters(self._h))
 
     def surface(self):
         """GetSurface: (vertices (V,3) f64, normals (V,3) f64, triangles (T,4) int64: vertex ids, normal id)."""

@@ -177,6 +177,39 @@ fe_status fe_scene_write_surface_obj(fe_scene* s, const char* path, const char* 
 fe_status fe_write_obj(const char* path, const char* object_name, const double* vertices, const double* normals,
                        uint64_t n_vertices, const int64_t* triangles, uint64_t n_triangles);
 
+/* Scene initialisation from triangle meshes.  Meshes are given as vertices (3 doubles each) and triangles (4 int64
+ * each: three vertex ids, then a normal id that is not used), host or device pointers.
+ *
+ * fe_mesh_to_sdf: Mesh2SDF::Build (3d/mesh_2_sdf.cpp:14-82) onto a node grid of n[0]*n[1]*n[2] values (x-fastest)
+ * with the given origin and spacing: exact distances within the band of every triangle's index box (box from the
+ * vertex coordinates times 1 / spacing[0], without the origin, as the reference computes it), the fill value
+ * max(spacing) * (n[0] + n[1] + n[2]) elsewhere, negated inside the mesh (winding number, TriangleMesh::IsInside
+ * with abs on the double as on the reference's platform).  Distances equal the reference's bit for bit.
+ *
+ * fe_scene_init_from_mesh: PICSimulator::InitializeFromTriangleMesh (pic_simulator.cpp:33-39): the mesh SDF
+ * becomes the scene's Fluid3::sdf (returned by fe_scene_get_fluid_sdf and used by the surface until the next
+ * substep), and every cell whose velocity-grid position (domain origin + h * index) samples it below 0 receives
+ * particles_per_cell particles (0: the reference default 16) at position + h * U[0,1]^3, velocity 0, appended to
+ * the scene's particles.  The reference draws the offsets from the unseeded std::rand() in a parallel loop; here
+ * they come from a counter-based generator started at `seed`, so the cells and counts equal the reference's and
+ * the positions are reproducible.
+ *
+ * fe_scene_add_volume_emitter: VolumeEmitter (emmiter/volume_emmiter.cpp:8-86) with the mesh SDF on its own grid
+ * (resolution, domain; resolution within the scene's grid): at the start of every substep each emitter node
+ * with SDF <= 0 whose fluid SDF value (same index; the SDF of the previous substep) is >= 0 receives
+ * particles_per_block particles at position + h * U[0,1]^3 with `velocity` (PICSimulator::OnBeginAdvanceTimeStep,
+ * pic_simulator.cpp:160-163).  A scene with emitters steps without graphs (its particle count changes) and cannot
+ * join a batch.  fe_scene_clear_emitters removes them (fe_scene_reset does too). */
+fe_status fe_mesh_to_sdf(const double* vertices, uint64_t n_vertices, const int64_t* triangles, uint64_t n_triangles,
+                         const int32_t n[3], const double origin[3], const double spacing[3], double* sdf, int32_t device);
+fe_status fe_scene_init_from_mesh(fe_scene* s, const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                  uint64_t n_triangles, uint32_t particles_per_cell, uint64_t seed);
+fe_status fe_scene_add_volume_emitter(fe_scene* s, const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                      uint64_t n_triangles, const int32_t resolution[3], const double domain_origin[3],
+                                      const double domain_size[3], uint32_t particles_per_block, const double velocity[3],
+                                      uint64_t seed, int32_t* emitter_id);
+fe_status fe_scene_clear_emitters(fe_scene* s);
+
 /* Viscosity (HybridSimulator::SetViscosity, hybrid_simulator.cpp:97-100), settable at any time.  When it is > 0
  * every substep runs ComputeDiffusion (pic_simulator.cpp:214-222) after the external forces: the reference's
  * BackwardEulerDiffusionSolver (fluid_solvers/backward_euler_diffusion_solver.cpp:20-242) -- per component, faces

@@ -1415,7 +1415,7 @@ static void closest_on_triangle(const double pt[3], const double p0[3], const do
     const double a00 = dot3(e0, e0), a01 = dot3(e0, e1), a11 = dot3(e1, e1);
     const double b0 = dot3(diff, e0), b1 = dot3(diff, e1);
     const double dd = a00 * a11 - a01 * a01;
-    const double det = dd > 0.0 ? dd : 0.0; /* std::max(x, 0.0) */
+    const double det = (dd < 0.0) ? 0.0 : dd; /* std::max(x, 0.0) = (x < 0.0) ? 0.0 : x (keeps -0.0 and NaN) */
     double s = a01 * b1 - a11 * b0;
     double t = a01 * b0 - a00 * b1;
     if (s + t <= det) {
