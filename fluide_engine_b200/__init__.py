@@ -8,8 +8,8 @@ from ._abi import (APIC, FLIP, PIC, AIR, FLUID, AUTO, CG, MGPCG, FluideError, ke
                    STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_DIFFUSE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P,
                    STAGE_MOVE)
 from .scene import Batch, Scene, face_shapes  # noqa: F401
-from .simulators import (APICSimulator, BoundingBox3D, DirectionalField, FLIPSimulator, Frame,  # noqa: F401
-                         HybridSimulator, OBJManager, PICSimulator, SimulationRunner, SimulationStats, TriangleMesh,
-                         Vector3D, Vector3S)
+from .simulators import (APICSimulator, BoundingBox3D, DirectionalField, Emitter, FLIPSimulator, Frame,  # noqa: F401
+                         HybridSimulator, OBJManager, PICSimulator, ScalarGrid3D, SimulationRunner, SimulationStats,
+                         TriangleMesh, Vector3D, Vector3S, VolumeEmitter)
 
 __version__ = "0.1.0"

@@ -31,6 +31,7 @@ EXPORTS = [
     "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_set_viscosity",
     "fe_scene_get_diffusion", "fe_scene_build_surface", "fe_scene_get_surface", "fe_scene_write_surface_obj",
     "fe_write_obj", "fe_mesh_to_sdf", "fe_scene_init_from_mesh", "fe_scene_add_volume_emitter", "fe_scene_clear_emitters",
+    "fe_scene_set_emitter_sdf", "fe_scene_set_fluid_sdf",
     "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
@@ -116,6 +117,8 @@ def lib():
     L.fe_scene_add_volume_emitter.argtypes = [P, P, ctypes.c_uint64, P, ctypes.c_uint64, P, P, P, ctypes.c_uint32, P,
                                               ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]
     L.fe_scene_clear_emitters.argtypes = [P]
+    L.fe_scene_set_emitter_sdf.argtypes = [P, ctypes.c_int32, P]
+    L.fe_scene_set_fluid_sdf.argtypes = [P, P]
     L.fe_scene_get_sort.argtypes = [P, P, P, ctypes.c_uint64]
     L.fe_scene_divergence.argtypes = [P, D]
     L.fe_scene_set_stream.argtypes = [P, P]

@@ -157,6 +157,7 @@ struct fe_scene {
     uint64_t graph_kernels[2][3] = {{0, 0, 0}, {0, 0, 0}};
     double graph_dt = -1.0;
     bool graphs_disabled = false;
+    bool last_substep_empty = false;  // the last run_substep had no particles (an emitter scene before emission)
     std::mutex mu;
 };
 
@@ -665,10 +666,20 @@ fe_status emit_particles(fe_scene* s);
 
 fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
 {
+    s->last_substep_empty = false;
     if (!s->emitters.empty()) {
         // emitters change the particle count every substep: direct launches, no graphs
         fe_status st = emit_particles(s);
         if (st != FE_OK) return st;
+        if (!s->have_particles || s->base.np == 0) {
+            // Nothing emitted yet: the reference's substep would only build an all-air grid and the all-positive
+            // SDF of no particles, which emits like the initial 0 SDF, so skipping it leaves the same state.
+            s->last_substep_empty = true;
+            for (int q = 0; q < 4; ++q)
+                if (ev) FE_CUDA(cudaEventRecord(ev[q], s->stream));
+            return FE_OK;
+        }
+        s->last_substep_empty = false;
         for (int ph = 0; ph < 3; ++ph) {
             if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
             st = enqueue_steps(s, dt, kPhaseFirst[ph], kPhaseLast[ph]);
@@ -1036,13 +1047,36 @@ fe_status fe_scene_step(fe_scene* s, double dt, int32_t nsub, fe_step_stats* sta
 {
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
     if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
-    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles before stepping");
+    if (!s->have_particles && s->emitters.empty()) return set_error(FE_ERR_STATE, "set particles before stepping");
     std::lock_guard<std::mutex> lk(s->mu);
     FE_CUDA(cudaSetDevice(s->device));
     if (stats) FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), s->stream));
+    std::vector<uint8_t> skipped;  // substeps an emitter scene ran without particles (no solve, no stats entry)
     for (int i = 0; i < nsub; ++i) {
         fe_status st = run_substep(s, dt, nullptr);
         if (st != FE_OK) return st;
+        if (s->last_substep_empty) {
+            skipped.resize(nsub, 0);
+            skipped[i] = 1;
+        }
+    }
+    if (stats && nsub > 0 && !skipped.empty()) {
+        // the ring holds the solved substeps in order; a skipped substep reports a converged empty solve
+        int solved = 0;
+        for (int i = 0; i < nsub; ++i) solved += !skipped[i];
+        std::vector<fe_step_stats> ring((size_t)std::min(solved, 1 << 16));
+        if (!ring.empty())
+            FE_CUDA(cudaMemcpyAsync(ring.data(), s->stats_ring, ring.size() * sizeof(fe_step_stats), cudaMemcpyDeviceToHost,
+                                    s->stream));
+        fe_status st = check_device_error(s);
+        if (st != FE_OK) return st;
+        size_t k = 0;
+        for (int i = 0; i < std::min(nsub, 1 << 16); ++i) {
+            fe_step_stats e{};
+            e.converged = 1;
+            stats[i] = skipped[i] ? e : ring[k++ % std::max<size_t>(ring.size(), 1)];
+        }
+        return FE_OK;
     }
     if (stats && nsub > 0) {
         const int cnt = std::min(nsub, 1 << 16);
@@ -1086,6 +1120,10 @@ fe_status fe_scene_cfl(fe_scene* s, double dt, double* cfl)
     if (!s || !cfl) return set_error(FE_ERR_BAD_ARG, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
     FE_CUDA(cudaSetDevice(s->device));
+    if (!s->have_particles || s->base.np == 0) {  // no particles (an emitter scene before emission): speed 0
+        *cfl = 0.0;
+        return FE_OK;
+    }
     FE_CUDA(ensure_grid(s, 0));
     FE_CUDA(launch_cfl(s->base, dt, s->d_scalar, s->stream));
     double m = 0;
@@ -1100,7 +1138,7 @@ fe_status fe_scene_advance_frame(fe_scene* s, double frame_dt, int32_t* substeps
 {
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
     if (!(frame_dt > 0.0)) return set_error(FE_ERR_BAD_ARG, "frame_dt must be > 0");
-    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles before stepping");
+    if (!s->have_particles && s->emitters.empty()) return set_error(FE_ERR_STATE, "set particles before stepping");
     double remaining = frame_dt;
     int count = 0;
     while (remaining > 0.0000000001) {  // physics_animation.cpp:76
@@ -1113,8 +1151,13 @@ fe_status fe_scene_advance_frame(fe_scene* s, double frame_dt, int32_t* substeps
         {
             std::lock_guard<std::mutex> lk(s->mu);
             FE_CUDA(cudaSetDevice(s->device));
-            st = enqueue_stages(s, sub, FE_STAGE_SORT, FE_STAGE_MOVE);
+            // OnBeginAdvanceTimeStep emits after the substep count was taken from the particles before emission
+            st = emit_particles(s);
             if (st != FE_OK) return st;
+            if (s->have_particles && s->base.np > 0) {
+                st = enqueue_stages(s, sub, FE_STAGE_SORT, FE_STAGE_MOVE);
+                if (st != FE_OK) return st;
+            }
         }
         remaining -= sub;
         ++count;
@@ -1226,7 +1269,7 @@ fe_status fe_scene_get_rhs(fe_scene* s, double* b)
 fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf)
 {
     if (!s || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
-    if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles first");
+    if (!s->have_particles && !s->mesh_sdf) return set_error(FE_ERR_STATE, "set particles first");
     std::lock_guard<std::mutex> lk(s->mu);
     FE_CUDA(cudaSetDevice(s->device));
     fe_status st = surface_sdf(s);
@@ -1234,6 +1277,21 @@ fe_status fe_scene_get_fluid_sdf(fe_scene* s, double* sdf)
     const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
     FE_CUDA(cudaMemcpyAsync(sdf, s->surf.sdf, nc * sizeof(double), cudaMemcpyDefault, s->stream));
     FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
+fe_status fe_scene_set_fluid_sdf(fe_scene* s, const double* sdf)
+{
+    if (!s || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    fe_status st = surf_alloc(s);
+    if (st != FE_OK) return st;
+    const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+    FE_CUDA(cudaMemcpyAsync(s->surf.sdf, sdf, nc * sizeof(double), cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    s->mesh_sdf = true;  // held until the next substep builds the particles' SDF
+    s->prev_valid = false;
     return FE_OK;
 }
 
@@ -1424,6 +1482,19 @@ fe_status fe_scene_add_volume_emitter(fe_scene* s, const double* vertices, uint6
     return r;
 }
 
+fe_status fe_scene_set_emitter_sdf(fe_scene* s, int32_t id, const double* sdf)
+{
+    if (!s || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (id < 0 || (size_t)id >= s->emitters.size()) return set_error(FE_ERR_BAD_ARG, "no emitter %d", id);
+    FE_CUDA(cudaSetDevice(s->device));
+    const auto& em = s->emitters[(size_t)id];
+    const size_t nc = (size_t)em.n[0] * em.n[1] * em.n[2];
+    FE_CUDA(cudaMemcpyAsync(em.sdf, sdf, nc * sizeof(double), cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
 fe_status fe_scene_clear_emitters(fe_scene* s)
 {
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
@@ -1606,7 +1677,7 @@ uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[
 
 const char* fe_last_error(void) { return g_err; }
 
-int32_t fe_abi_version(void) { return 10200; }
+int32_t fe_abi_version(void) { return 10300; }
 
 }  // extern "C"
 

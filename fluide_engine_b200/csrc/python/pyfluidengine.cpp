@@ -2,8 +2,9 @@
 //
 // Same module name, class names and method names as the reference's binding
 // (python_wrapper/main.cpp:20-33, simulators_wrapper.cu:36-85, vector3_wrapper.cpp, frame_wrapper.cpp,
-// bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp, triangle_mesh_wrapper.cpp, obj_manager_wrapper.cpp)
-// for the substep path and its surface output, so
+// bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp, triangle_mesh_wrapper.cpp, obj_manager_wrapper.cpp,
+// scalar_grid_3d_wrapper.cpp, emitters_wrapper.cpp) for the substep path, its surface output and scene
+// initialisation, so
 // `import PyFluidEngine as pyf` keeps working for a caller of the simulators.  The GIL is released while
 // a frame or a batch of substeps runs.  Extensions for seeding and reading particles take and return
 // numpy arrays.
@@ -188,6 +189,16 @@ PYBIND11_MODULE(PyFluidEngine, m)
         .def_readwrite("simulationTimeInSeconds", &SimulationStats::simulationTimeInSeconds)
         .def_readwrite("iterationTimeInSeconds", &SimulationStats::iterationTimeInSeconds)
         .def_readwrite("cflPerIteration", &SimulationStats::cflPerIteration);
+    py::class_<ScalarGrid3D>(m, "ScalarGrid3D")
+        .def(py::init<const Vector3<size_t>&, const double&, Vector3<double>, Vector3<double>>())
+        .def("GetElement", [](const ScalarGrid3D& g, size_t i, size_t j, size_t k) { return g.GetElement(i, j, k); })
+        .def("SetElement", &ScalarGrid3D::SetElement);
+    py::class_<Emitter, std::shared_ptr<Emitter>>(m, "Emitter");
+    py::class_<VolumeEmitter, std::shared_ptr<VolumeEmitter>, Emitter>(m, "VolumeEmitter")
+        .def(py::init<const TriangleMesh&, Vector3<size_t>, BoundingBox3D, const size_t&, const Vector3<double>&,
+                      const Vector3<double>&>())
+        .def("InitializeFromTriangleMesh", &VolumeEmitter::InitializeFromTriangleMesh)
+        .def("InitializeFromSdf", &VolumeEmitter::InitializeFromSdf);
     py::class_<SimulationRunner>(m, "SimulationRunner")
         .def(py::init<>())
         .def("RunSimulation", &SimulationRunner::RunSimulation, py::call_guard<py::gil_scoped_release>())
@@ -196,10 +207,10 @@ PYBIND11_MODULE(PyFluidEngine, m)
     py::class_<PICSimulator, std::shared_ptr<PICSimulator>, HybridSimulator> pic(m, "PICSimulator");
     pic.def(py::init<Vector3<size_t>, BoundingBox3D>())
         .def("AdvanceSingleFrame", &PICSimulator::AdvanceSingleFrame, py::call_guard<py::gil_scoped_release>())
-        .def("InitializeFromTriangleMesh", [](PICSimulator& s, py::object) { s.InitializeFromTriangleMesh(*(TriangleMesh*)nullptr); })
+        .def("InitializeFromTriangleMesh", &PICSimulator::InitializeFromTriangleMesh)
         .def("AddExternalForce", [](PICSimulator& s, std::shared_ptr<DirectionalField> f) { s.AddExternalForce(f); })
         .def("AddCollider", [](PICSimulator& s, py::object) { s.AddCollider(nullptr); })
-        .def("AddEmitter", [](PICSimulator& s, py::object) { s.AddEmitter(nullptr); })
+        .def("AddEmitter", &PICSimulator::AddEmitter)
         .def("SetCurrentFrame", &PICSimulator::SetCurrentFrame)
         .def("SetViscosity", &PICSimulator::SetViscosity)
         .def("SetMaxClf", &PICSimulator::SetMaxClf)

@@ -182,6 +182,16 @@ class Scene:
             (ctypes.c_double * 3)(*velocity), seed, ctypes.byref(eid)))
         return eid.value
 
+    def set_emitter_sdf(self, emitter_id, sdf):
+        """VolumeEmitter::InitializeFromSdf: node values on the emitter's grid, shape (nz, ny, nx)."""
+        S = np.ascontiguousarray(sdf, dtype=np.float64)
+        check(self._L.fe_scene_set_emitter_sdf(self._h, emitter_id, ptr(S)))
+
+    def set_fluid_sdf(self, sdf):
+        """Fluid3::sdf until the next substep (as after init_from_mesh), shape (nz, ny, nx)."""
+        S = np.ascontiguousarray(sdf, dtype=np.float64)
+        check(self._L.fe_scene_set_fluid_sdf(self._h, ptr(S)))
+
     def clear_emitters(self):
         check(self._L.fe_scene_clear_emitters(self._h))
 

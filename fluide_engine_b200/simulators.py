@@ -115,7 +115,35 @@ class TriangleMesh:
 
 
 class OBJManager:
-    """OBJManager::Save (3d/obj_manager.cpp:14-90) through the library's writer."""
+    """OBJManager::Save (3d/obj_manager.cpp:14-90) through the library's writer; Load reads "o", "v", "vn" and
+    three-vertex "f" lines as OBJManager::ParseLine does (:92-161)."""
+
+    def Load(self, name, obj):
+        try:
+            f = open(name, "rb")
+        except OSError:
+            return  # the reference reports the error on stdout and leaves the mesh unchanged
+        V, N, T = [], [], []
+        with f:
+            for raw in f.read().decode().split("\n"):
+                w = raw.split(" ")
+                if w[-1] == "" and len(w) > 1:
+                    w = w[:-1]  # std::getline keeps no trailing empty field
+                if not w or w == [""]:
+                    continue
+                if w[0] == "o" and len(w) > 1:
+                    obj.SetObjectName(w[1])
+                elif w[0] == "v" and len(w) > 3:
+                    V.append([float(w[1]), float(w[2]), float(w[3])])
+                elif w[0] == "vn" and len(w) > 3:
+                    N.append([float(w[1]), float(w[2]), float(w[3])])
+                elif w[0] == "f" and len(w) == 4:
+                    fv = [x.split("/") for x in w[1:]]
+                    vs = [int(x[0]) for x in fv if len(x) > 1]
+                    T.append([vs[0] - 1, vs[1] - 1, vs[2] - 1, int(fv[-1][-1]) - 1])
+        obj.vertices = np.concatenate([obj.vertices, np.asarray(V, dtype=np.float64).reshape(-1, 3)])
+        obj.normals = np.concatenate([obj.normals, np.asarray(N, dtype=np.float64).reshape(-1, 3)])
+        obj.triangles = np.concatenate([obj.triangles, np.asarray(T, dtype=np.int64).reshape(-1, 4)])
 
     def Save(self, name, obj):
         V = np.ascontiguousarray(obj.vertices, dtype=np.float64)
@@ -124,6 +152,75 @@ class OBJManager:
         L = _abi.lib()
         _abi.check(L.fe_write_obj(str(name).encode(), obj.GetObjectName().encode(), _abi.ptr(V), _abi.ptr(N),
                                   V.shape[0], _abi.ptr(T), T.shape[0]))
+
+
+class ScalarGrid3D:
+    """ScalarGrid3D (3d/scalar_grid3d.hpp), the node-value subset: element (i, j, k) at i + nx * (j + ny * k)."""
+
+    def __init__(self, size=None, initialValue=0.0, origin=None, gridSpacing=None):
+        size = Vector3S(1) if size is None else size
+        self._size = (int(size.x), int(size.y), int(size.z))
+        self._origin = Vector3D(0.0) if origin is None else origin
+        self._spacing = Vector3D(1.0) if gridSpacing is None else gridSpacing
+        self.values = np.full((self._size[2], self._size[1], self._size[0]), float(initialValue))
+
+    def GetSize(self):
+        return Vector3S(*self._size)
+
+    def GetOrigin(self):
+        return self._origin
+
+    def GetGridSpacing(self):
+        return self._spacing
+
+    def GetElement(self, i, j, k):
+        return float(self.values[k, j, i])
+
+    def SetElement(self, i, j, k, value):
+        self.values[k, j, i] = value
+
+
+class Emitter:
+    """Emitter (emmiter/emmiter.hpp)."""
+
+
+class VolumeEmitter(Emitter):
+    """VolumeEmitter (emmiter/volume_emmiter.cpp:8-86): at the start of every substep each node of its grid with
+    SDF <= 0 where the previous substep's fluid SDF is >= 0 receives particlesPerBlock particles (node + spacing *
+    U[0,1]^3) with `velocity`; the SDF is the mesh's (built on the GPU at registration) or InitializeFromSdf's.
+    velocityVariance is kept and unused, as in the reference.  Changes after AddEmitter apply at the next step."""
+
+    def __init__(self, mesh, resolution, domain, particlesPerBlock, velocity, velocityVariance):
+        self._res = (int(resolution.x), int(resolution.y), int(resolution.z))
+        o, sz = domain.GetOrigin(), domain.GetSize()
+        self._origin = (o.x, o.y, o.z)
+        self._size = (sz.x, sz.y, sz.z)
+        self._ppb = int(particlesPerBlock)
+        self._velocity = (velocity.x, velocity.y, velocity.z)
+        self._velocityVariance = velocityVariance
+        self._version = 0
+        self.InitializeFromTriangleMesh(mesh)
+
+    def InitializeFromTriangleMesh(self, mesh):
+        self._V = np.array(mesh.vertices, dtype=np.float64)
+        self._T = np.array(mesh.triangles, dtype=np.int64)
+        self._sdf = None
+        self._version += 1
+
+    def InitializeFromSdf(self, sdf):
+        """VolumeEmitter::InitializeFromSdf (:50-56): the emitter's node (i, j, k) takes sdf(i, j, k)."""
+        nx, ny, nz = self._res
+        if sdf.values.shape[0] < nz or sdf.values.shape[1] < ny or sdf.values.shape[2] < nx:
+            raise ValueError("InitializeFromSdf: the grid must cover the emitter's resolution")
+        self._sdf = np.ascontiguousarray(sdf.values[:nz, :ny, :nx], dtype=np.float64)
+        self._version += 1
+
+    def _add_to(self, scene, seed):
+        eid = scene.add_volume_emitter(self._V, self._T, self._res, self._origin, self._size,
+                                       particles_per_block=self._ppb, velocity=self._velocity, seed=seed)
+        if self._sdf is not None:
+            scene.set_emitter_sdf(eid, self._sdf)
+        return eid
 
 
 class HybridSimulator:
@@ -144,6 +241,10 @@ class HybridSimulator:
         self._density = 1.0
         self._blend = 0.05
         self._forces = []
+        self._emitters = []
+        self._registered = None         # (scene, emitter versions) the scene's emitters were built from
+        self._meshSeed = 0
+        self._meshSdfLive = False       # InitializeFromTriangleMesh ran and no substep since
         self._device = device
         self._scene = None
         self._pending = None            # (pos, vel, C) until the scene exists
@@ -218,10 +319,18 @@ class HybridSimulator:
         raise NotImplementedError("colliders are outside the substep path (no benchmark scene has one)")
 
     def AddEmitter(self, emitter):
-        raise NotImplementedError("emitters are outside the substep path (no benchmark scene has one)")
+        """PICSimulator::AddEmitter (pic_simulator.cpp:46-49); registered with the scene at the next step."""
+        if not isinstance(emitter, VolumeEmitter):
+            raise TypeError("AddEmitter: a VolumeEmitter is expected")
+        self._emitters.append(emitter)
 
     def InitializeFromTriangleMesh(self, mesh):
-        raise NotImplementedError("mesh seeding (Mesh2SDF) is outside the substep path; use InitializeFromRegions")
+        """PICSimulator::InitializeFromTriangleMesh (pic_simulator.cpp:33-39): the mesh SDF becomes the fluid SDF and
+        every cell inside it receives GetParticlesPerBlock() particles, appended to those already set.  The fluid SDF
+        stays the mesh's until the first substep, also across settings changes that rebuild the scene."""
+        self._ensure_scene().init_from_mesh(mesh.vertices, mesh.triangles, self._particlesPerBlok, self._meshSeed)
+        self._meshSeed += 1
+        self._meshSdfLive = True
 
     def GetSurface(self, mesh):
         """PICSimulator::GetSurface (pic_simulator.cpp:71-78): appends the marching-cubes surface of the SDF built at
@@ -269,7 +378,8 @@ class HybridSimulator:
 
     def AdvanceSingleFrame(self):
         """PhysicsAnimation::AdvanceSingleFrame (physics_animation.cpp:17-21, 48-61, 64-92)."""
-        scene = self._ensure_scene()
+        scene = self._sync_emitters()
+        self._meshSdfLive = False
         self._currentTime = self._currentFrame.GetTimeInSeconds()
         dt = self._currentFrame.GetTimeIntervalInSeconds()
         n = scene.advance_frame(dt)
@@ -279,7 +389,9 @@ class HybridSimulator:
 
     def AdvanceFixedSubsteps(self, dt, nsub, stats=True):
         """nsub substeps of exactly dt (the benchmark configurations' fixed-dt mode)."""
-        self.last_stats = self._ensure_scene().step(dt, nsub, stats=stats) or []
+        scene = self._sync_emitters()
+        self._meshSdfLive = False
+        self.last_stats = scene.step(dt, nsub, stats=stats) or []
         return self.last_stats
 
     # internals ------------------------------------------------------------------------------------
@@ -301,6 +413,17 @@ class HybridSimulator:
                 self._pending = None
         return self._scene
 
+    def _sync_emitters(self):
+        """(Re-)registers the emitters when the scene is new or an emitter changed since its registration."""
+        scene = self._ensure_scene()
+        key = (id(scene), tuple((id(e), e._version) for e in self._emitters))
+        if self._registered != key:
+            scene.clear_emitters()
+            for i, e in enumerate(self._emitters):
+                e._add_to(scene, 0x5EED0000 + i)
+            self._registered = key
+        return scene
+
     def _rebuild(self, change):
         """Applies a settings change; a live scene is rebuilt with its particles and pressure kept."""
         if self._scene is None:
@@ -308,11 +431,16 @@ class HybridSimulator:
             return
         pos, vel, C = self._scene.particles()
         p = self._scene.grid()[3]
+        sdf = self._scene.fluid_sdf() if self._meshSdfLive else None
         self._scene.close()
         self._scene = None
+        self._registered = None
         change()
         self._pending = (pos, vel, C if self._solver == _abi.APIC else None)
-        self._ensure_scene().set_pressure(p)
+        scene = self._ensure_scene()
+        scene.set_pressure(p)
+        if sdf is not None:
+            scene.set_fluid_sdf(sdf)
 
 
 class PICSimulator(HybridSimulator):

@@ -199,7 +199,9 @@ fe_status fe_write_obj(const char* path, const char* object_name, const double* 
  * with SDF <= 0 whose fluid SDF value (same index; the SDF of the previous substep) is >= 0 receives
  * particles_per_block particles at position + h * U[0,1]^3 with `velocity` (PICSimulator::OnBeginAdvanceTimeStep,
  * pic_simulator.cpp:160-163).  A scene with emitters steps without graphs (its particle count changes) and cannot
- * join a batch.  fe_scene_clear_emitters removes them (fe_scene_reset does too). */
+ * join a batch; it may start without particles (fe_scene_step and fe_scene_advance_frame then emit first; a
+ * substep that still has none is skipped and reports a converged empty solve).  fe_scene_clear_emitters removes
+ * them (fe_scene_reset does too). */
 fe_status fe_mesh_to_sdf(const double* vertices, uint64_t n_vertices, const int64_t* triangles, uint64_t n_triangles,
                          const int32_t n[3], const double origin[3], const double spacing[3], double* sdf, int32_t device);
 fe_status fe_scene_init_from_mesh(fe_scene* s, const double* vertices, uint64_t n_vertices, const int64_t* triangles,
@@ -209,6 +211,14 @@ fe_status fe_scene_add_volume_emitter(fe_scene* s, const double* vertices, uint6
                                       const double domain_size[3], uint32_t particles_per_block, const double velocity[3],
                                       uint64_t seed, int32_t* emitter_id);
 fe_status fe_scene_clear_emitters(fe_scene* s);
+/* VolumeEmitter::InitializeFromSdf (emmiter/volume_emmiter.cpp:50-56): replaces emitter `id`'s SDF with node values
+ * on its grid (resolution[0] * resolution[1] * resolution[2] doubles, x-fastest; host or device pointer). */
+fe_status fe_scene_set_emitter_sdf(fe_scene* s, int32_t id, const double* sdf);
+/* Fluid3::sdf (fluid3.hpp:22, a public member of the reference's fluid) set to node values on the scene's SDF grid
+ * (n[0] * n[1] * n[2] doubles, x-fastest, host or device pointer); held, like the mesh SDF of
+ * fe_scene_init_from_mesh, until the next substep builds the particles' SDF.  Lets a caller that rebuilds a scene
+ * between seeding and the first substep (e.g. to change its settings) carry the fluid SDF over. */
+fe_status fe_scene_set_fluid_sdf(fe_scene* s, const double* sdf);
 
 /* Viscosity (HybridSimulator::SetViscosity, hybrid_simulator.cpp:97-100), settable at any time.  When it is > 0
  * every substep runs ComputeDiffusion (pic_simulator.cpp:214-222) after the external forces: the reference's

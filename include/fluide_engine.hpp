@@ -4,11 +4,12 @@
 // substep: PhysicsAnimation (physics_animation.hpp:8-29), HybridSimulator (hybrid_simulator.hpp:10-41),
 // PICSimulator (pic_simulator.hpp:27-43), FLIPSimulator (flip_simulator.hpp:9-16), APICSimulator
 // (apic_simulator.hpp:9-15), Frame (common/frame.hpp), BoundingBox3D (3d/bounding_box_3d.hpp),
-// DirectionalField (forces/directional_field.hpp) and Vector3 (common/vector3.hpp), with the same names
-// and argument meaning.  State lives on the GPU in one fe_scene (include/fluide_b200.h), created on the
-// first step after particles exist.  Entry points of components outside the substep (mesh seeding,
-// colliders, emitters) throw std::logic_error saying so; errors of the
-// library throw fluide::Error carrying the fe_status.  Header-only; link with libfluide_b200.so.
+// DirectionalField (forces/directional_field.hpp), Vector3 (common/vector3.hpp), TriangleMesh, OBJManager,
+// ScalarGrid3D (the node-value subset), VolumeEmitter (emmiter/volume_emmiter.hpp), SimulationStats and
+// SimulationRunner, with the same names and argument meaning.  State lives on the GPU in one fe_scene
+// (include/fluide_b200.h), created on first use.  Colliders are outside the GPU path: AddCollider throws
+// std::logic_error saying so; errors of the library throw fluide::Error carrying the fe_status.
+// Header-only; link with libfluide_b200.so.
 #ifndef FLUIDE_ENGINE_HPP
 #define FLUIDE_ENGINE_HPP
 
@@ -203,8 +204,124 @@ class OBJManager {
     }
 };
 
+// ScalarGrid3D (3d/scalar_grid3d.hpp): node values with origin and spacing, index i + nx * (j + ny * k) as
+// Array3::GetElement (common/array3.hpp:65-74).  The subset a caller needs to hand an SDF to an emitter.
+class ScalarGrid3D {
+  public:
+    ScalarGrid3D(const Vector3<size_t>& size = Vector3<size_t>(1), const double& initialValue = 0,
+                 Vector3<double> origin = Vector3<double>(0), Vector3<double> gridSpacing = Vector3<double>(1))
+        : _size(size), _origin(origin), _spacing(gridSpacing), _data(size.x * size.y * size.z, initialValue) {}
+    Vector3<size_t> GetSize() const { return _size; }
+    Vector3<double> GetOrigin() const { return _origin; }
+    Vector3<double> GetGridSpacing() const { return _spacing; }
+    Vector3<double> GridIndexToPosition(size_t i, size_t j, size_t k) const
+    {
+        return Vector3<double>(_origin.x + i * _spacing.x, _origin.y + j * _spacing.y, _origin.z + k * _spacing.z);
+    }
+    const double& GetElement(size_t i, size_t j, size_t k) const { return _data.at(i + _size.x * (j + _size.y * k)); }
+    double& GetElement(size_t i, size_t j, size_t k) { return _data.at(i + _size.x * (j + _size.y * k)); }
+    void SetElement(size_t i, size_t j, size_t k, double value) { GetElement(i, j, k) = value; }
+    const double& operator()(size_t i, size_t j, size_t k) const { return GetElement(i, j, k); }
+    double& operator()(size_t i, size_t j, size_t k) { return GetElement(i, j, k); }
+    const std::vector<double>& GetRawData() const { return _data; }
+
+  private:
+    Vector3<size_t> _size;
+    Vector3<double> _origin, _spacing;
+    std::vector<double> _data;
+};
+
+namespace fluide {
+// A TriangleMesh as the C ABI takes it: 3 doubles per vertex, 4 int64 per triangle (vertex ids, normal id).
+inline void flatten_mesh(const TriangleMesh& mesh, std::vector<double>& V, std::vector<int64_t>& T)
+{
+    V.clear();
+    T.clear();
+    for (const auto& v : mesh.GetVerticies()) {
+        V.push_back(v.x);
+        V.push_back(v.y);
+        V.push_back(v.z);
+    }
+    for (const auto& t : mesh.GetTriangles()) {
+        T.push_back((int64_t)t.point1Idx);
+        T.push_back((int64_t)t.point2Idx);
+        T.push_back((int64_t)t.point3Idx);
+        T.push_back((int64_t)t.normalIdx);
+    }
+}
+}  // namespace fluide
+
 class Collider;
-class Emitter;
+
+// Emitter (emmiter/emmiter.hpp): the base the simulators take in AddEmitter.
+class Emitter {
+  public:
+    virtual ~Emitter() = default;
+};
+
+// VolumeEmitter (emmiter/volume_emmiter.cpp:8-86): at the start of every substep, each node of its grid
+// (`resolution` nodes over `domain`) whose SDF is <= 0 and where the fluid SDF of the previous substep is >= 0
+// receives particlesPerBlock particles at node + spacing * U[0,1]^3 with `velocity`.  The SDF comes from the mesh
+// (Mesh2SDF, built on the GPU when the emitter is registered with a scene) or from InitializeFromSdf.
+// velocityVariance is kept and unused, as in the reference.  The resolution must be within the simulator's grid
+// (the emitter indexes the fluid SDF with its own node indices).  Changing the emitter after AddEmitter takes
+// effect at the simulator's next step.
+class VolumeEmitter : public Emitter {
+  public:
+    VolumeEmitter(const TriangleMesh& mesh, Vector3<size_t> resolution, BoundingBox3D domain, const size_t& particlesPerBlock,
+                  const Vector3<double>& velocity, const Vector3<double>& velocityVariance)
+        : _resolution(resolution), _domain(domain), _particlesPerBlock(particlesPerBlock), _velocity(velocity),
+          _velocityVariance(velocityVariance)
+    {
+        InitializeFromTriangleMesh(mesh);
+    }
+    void InitializeFromTriangleMesh(const TriangleMesh& mesh)
+    {
+        fluide::flatten_mesh(mesh, _V, _T);
+        _sdf.clear();
+        ++_version;
+    }
+    // VolumeEmitter::InitializeFromSdf (:50-56): the emitter's node (i, j, k) takes sdf(i, j, k).
+    void InitializeFromSdf(const ScalarGrid3D& sdf)
+    {
+        const Vector3<size_t> n = sdf.GetSize();
+        if (n.x < _resolution.x || n.y < _resolution.y || n.z < _resolution.z)
+            throw std::invalid_argument("InitializeFromSdf: the grid must cover the emitter's resolution");
+        std::vector<double> v(_resolution.x * _resolution.y * _resolution.z);
+        for (size_t k = 0; k < _resolution.z; ++k)
+            for (size_t j = 0; j < _resolution.y; ++j)
+                for (size_t i = 0; i < _resolution.x; ++i) v[i + _resolution.x * (j + _resolution.y * k)] = sdf(i, j, k);
+        _sdf = std::move(v);
+        ++_version;
+    }
+    Vector3<double> GetVelocity() const { return _velocity; }
+    Vector3<double> GetVelocityVariance() const { return _velocityVariance; }
+    size_t GetParticlesPerBlock() const { return _particlesPerBlock; }
+    uint64_t Version() const { return _version; }
+
+    // Registers the emitter with a scene (fe_scene_add_volume_emitter, then fe_scene_set_emitter_sdf for an SDF).
+    int32_t AddTo(fe_scene* scene, uint64_t seed) const
+    {
+        const int32_t res[3] = {(int32_t)_resolution.x, (int32_t)_resolution.y, (int32_t)_resolution.z};
+        const Vector3<double> o = _domain.GetOrigin(), sz = _domain.GetSize();
+        const double origin[3] = {o.x, o.y, o.z}, size[3] = {sz.x, sz.y, sz.z};
+        const double vel[3] = {_velocity.x, _velocity.y, _velocity.z};
+        int32_t id = -1;
+        fluide::check(fe_scene_add_volume_emitter(scene, _V.data(), _V.size() / 3, _T.data(), _T.size() / 4, res, origin,
+                                                  size, (uint32_t)_particlesPerBlock, vel, seed, &id));
+        if (!_sdf.empty()) fluide::check(fe_scene_set_emitter_sdf(scene, id, _sdf.data()));
+        return id;
+    }
+
+  private:
+    Vector3<size_t> _resolution;
+    BoundingBox3D _domain;
+    size_t _particlesPerBlock;
+    Vector3<double> _velocity, _velocityVariance;
+    std::vector<double> _V, _sdf;
+    std::vector<int64_t> _T;
+    uint64_t _version = 0;
+};
 
 class PhysicsAnimation {
   public:
@@ -327,6 +444,8 @@ class HybridSimulator : public PhysicsAnimation {
     // Fixed-dt substeps (the benchmark configurations' mode); stats may be null.
     void AdvanceFixedSubsteps(double dt, int nsub, fe_step_stats* stats = nullptr)
     {
+        SyncEmitters();
+        _meshSdfLive = false;
         fluide::check(fe_scene_step(Scene(), dt, nsub, stats));
     }
 
@@ -341,10 +460,24 @@ class HybridSimulator : public PhysicsAnimation {
         _forces.push_back(newForce);
     }
     void AddCollider(std::shared_ptr<Collider>) { throw std::logic_error("colliders are outside the substep path"); }
-    void AddEmitter(std::shared_ptr<Emitter>) { throw std::logic_error("emitters are outside the substep path"); }
-    void InitializeFromTriangleMesh(const TriangleMesh&)
+    // PICSimulator::AddEmitter (pic_simulator.cpp:46-49); emitters are registered with the scene at the next step.
+    void AddEmitter(std::shared_ptr<Emitter> emitter)
     {
-        throw std::logic_error("mesh seeding (Mesh2SDF) is outside the substep path; use InitializeFromRegions");
+        auto v = std::dynamic_pointer_cast<VolumeEmitter>(emitter);
+        if (!v) throw std::invalid_argument("AddEmitter: a VolumeEmitter is expected");
+        _emitters.push_back(v);
+    }
+    // PICSimulator::InitializeFromTriangleMesh (pic_simulator.cpp:33-39): the mesh SDF becomes the fluid SDF and
+    // every cell inside it receives GetParticlesPerBlock() particles (appended to the particles already set).
+    // The fluid SDF stays the mesh's until the first substep, also across settings changes that rebuild the scene.
+    void InitializeFromTriangleMesh(const TriangleMesh& mesh)
+    {
+        std::vector<double> V;
+        std::vector<int64_t> T;
+        fluide::flatten_mesh(mesh, V, T);
+        fluide::check(fe_scene_init_from_mesh(Scene(), V.data(), V.size() / 3, T.data(), T.size() / 4,
+                                              (uint32_t)_particlesPerBlok, _meshSeed++));
+        _meshSdfLive = true;
     }
     // PICSimulator::GetSurface (pic_simulator.cpp:71-78): appends the marching-cubes surface of Fluid3::sdf (the
     // SDF built at the start of the last substep) to mesh, exactly as the reference's surface tracker does.
@@ -369,7 +502,10 @@ class HybridSimulator : public PhysicsAnimation {
     {
         if (!_scene) {
             fluide::check(fe_scene_create(&_desc, &_scene));
+            ++_sceneGeneration;
             Upload();
+            if (_meshSdfLive && !_sdf.empty()) fluide::check(fe_scene_set_fluid_sdf(_scene, _sdf.data()));
+            _sdf.clear();
         }
         return _scene;
     }
@@ -377,6 +513,8 @@ class HybridSimulator : public PhysicsAnimation {
   protected:
     unsigned AdvanceTimeStep(double timeIntervalInSeconds) override
     {
+        SyncEmitters();
+        _meshSdfLive = false;
         int32_t n = 0;
         fluide::check(fe_scene_advance_frame(Scene(), timeIntervalInSeconds, &n));
         return (unsigned)n;
@@ -384,12 +522,31 @@ class HybridSimulator : public PhysicsAnimation {
     template <class F>
     void Reconfigure(F change)
     {
-        if (_scene) {  // keep the particles: read them back, rebuild with the new settings
+        if (_scene) {  // keep the particles (and a mesh-initialised fluid SDF): read back, rebuild with the new settings
             GetParticles(_pos, _vel, _kind == FE_SOLVER_APIC ? &_C : nullptr);
+            if (_meshSdfLive) {
+                _sdf.resize((size_t)_n.x * _n.y * _n.z);
+                fluide::check(fe_scene_get_fluid_sdf(_scene, _sdf.data()));
+            }
             fe_scene_destroy(_scene);
             _scene = nullptr;
         }
         change();
+    }
+    // (Re-)registers the emitters when the scene is new or an emitter changed since its registration.
+    void SyncEmitters()
+    {
+        fe_scene* s = Scene();
+        bool stale = _emitterGeneration != _sceneGeneration || _emitterVersions.size() != _emitters.size();
+        for (size_t i = 0; !stale && i < _emitters.size(); ++i) stale = _emitterVersions[i] != _emitters[i]->Version();
+        if (!stale) return;
+        fluide::check(fe_scene_clear_emitters(s));
+        _emitterVersions.clear();
+        for (size_t i = 0; i < _emitters.size(); ++i) {
+            _emitters[i]->AddTo(s, 0x5EED0000ull + i);
+            _emitterVersions.push_back(_emitters[i]->Version());
+        }
+        _emitterGeneration = _sceneGeneration;
     }
     void Upload()
     {
@@ -407,6 +564,11 @@ class HybridSimulator : public PhysicsAnimation {
     size_t _particlesPerBlok = 16;  // hybrid_simulator.cpp:22
     std::vector<float> _pos, _vel, _C;
     std::vector<std::shared_ptr<ExternalForce>> _forces;
+    std::vector<std::shared_ptr<VolumeEmitter>> _emitters;
+    std::vector<uint64_t> _emitterVersions;
+    uint64_t _sceneGeneration = 0, _emitterGeneration = 0, _meshSeed = 0;
+    bool _meshSdfLive = false;  // InitializeFromTriangleMesh ran and no substep since
+    std::vector<double> _sdf;   // its SDF while the scene is rebuilt
 };
 
 inline size_t HybridSimulator::InitializeFromRegions(const std::vector<fe_region_desc>& regions, uint64_t seed)

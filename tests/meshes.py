@@ -40,3 +40,11 @@ def icosphere(center, radius, subdiv=2):
     V = np.array(V) * radius + np.asarray(center, float)
     T = np.array([(a, b, c, 0) for a, b, c in F], dtype=np.int64)
     return V, T
+
+
+def write_obj(path, V, T, name="mesh"):
+    """A mesh as OBJ text that OBJManager::Load reads ("v" lines, "f a//n b//n c//n" faces with 1-based ids)."""
+    lines = [f"o {name}"] + [f"v {x:.17g} {y:.17g} {z:.17g}" for x, y, z in V] + ["vn 0 0 1"]
+    lines += [f"f {a + 1}//1 {b + 1}//1 {c + 1}//1" for a, b, c, *_ in T]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

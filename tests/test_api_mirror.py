@@ -44,6 +44,11 @@ def test_module_names_match_reference():
     assert hasattr(m.FLIPSimulator, "SetBlendingFactor")
     # triangle_mesh_wrapper.cpp / obj_manager_wrapper.cpp
     assert hasattr(m.TriangleMesh, "Clear") and hasattr(m.OBJManager, "Save") and hasattr(m.OBJManager, "Load")
+    # emitters_wrapper.cpp / scalar_grid_3d_wrapper.cpp
+    assert hasattr(m, "Emitter") and issubclass(m.VolumeEmitter, m.Emitter)
+    for name in ("InitializeFromTriangleMesh", "InitializeFromSdf"):
+        assert hasattr(m.VolumeEmitter, name)
+    assert hasattr(m.ScalarGrid3D, "GetElement") and hasattr(m.ScalarGrid3D, "SetElement")
 
 
 def test_reference_construction_sequence_without_device():
@@ -62,14 +67,46 @@ def test_reference_construction_sequence_without_device():
         sim.SetViscosity(-0.5)
     with pytest.raises(RuntimeError):
         sim.AddCollider(None)
+    # emitters are kept until the first step registers them with the scene
+    em = m.VolumeEmitter(m.TriangleMesh(), m.Vector3S(16, 16, 16), domain, 8, m.Vector3D(0.0, 6.0, 0.0), m.Vector3D(0.0))
+    grid = m.ScalarGrid3D(m.Vector3S(16, 16, 16), 1.0, m.Vector3D(0.0), m.Vector3D(1.0 / 16))
+    grid.SetElement(3, 4, 5, -2.0)
+    assert grid.GetElement(3, 4, 5) == -2.0 and grid.GetElement(4, 4, 5) == 1.0
+    em.InitializeFromSdf(grid)
+    sim.AddEmitter(em)
+    with pytest.raises(TypeError):
+        sim.AddEmitter(grid)
 
 
-def build_cpp_api_binary():
+def test_python_mirror_obj_load_and_emitter_without_device(tmp_path):
+    import fluide_engine_b200 as m
+    from meshes import box, write_obj
+
+    V, T = box((0.1, 0.2, 0.3), (0.4, 0.5, 0.6))
+    write_obj(tmp_path / "b.obj", V, T, name="emitter")
+    mesh = m.TriangleMesh()
+    m.OBJManager().Load(str(tmp_path / "b.obj"), mesh)
+    assert mesh.GetObjectName() == "emitter"
+    assert np.array_equal(mesh.vertices, V) and np.array_equal(mesh.triangles[:, :3], T[:, :3])
+    m.OBJManager().Load(str(tmp_path / "missing.obj"), mesh)  # reported, mesh unchanged
+    assert mesh.vertices.shape[0] == 8
+    domain = m.BoundingBox3D(m.Vector3D(0.0), m.Vector3D(1.0))
+    em = m.VolumeEmitter(mesh, m.Vector3S(8, 8, 8), domain, 4, m.Vector3D(0.0, 1.0, 0.0), m.Vector3D(0.0))
+    grid = m.ScalarGrid3D(m.Vector3S(4, 4, 4), 1.0)
+    with pytest.raises(ValueError):
+        em.InitializeFromSdf(grid)  # smaller than the emitter's grid
+    sim = m.FLIPSimulator(m.Vector3S(8, 8, 8), domain)
+    sim.AddEmitter(em)
+    with pytest.raises(TypeError):
+        sim.AddEmitter(grid)
+
+
+def build_cpp_api_binary(name="api_dam_break"):
     from fluide_engine_b200 import build
 
     build.build()
-    out = os.path.join(PKG, "_build", "api_dam_break")
-    src = os.path.join(ROOT, "tests", "cpp", "api_dam_break.cpp")
+    out = os.path.join(PKG, "_build", name)
+    src = os.path.join(ROOT, "tests", "cpp", name + ".cpp")
     cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), src, "-o", out, "-L", PKG,
            "-l:libfluide_b200.so", "-Wl,-rpath," + PKG]
     subprocess.run(cmd, check=True)
@@ -78,6 +115,82 @@ def build_cpp_api_binary():
 
 def test_cpp_api_compiles_and_links():
     assert os.path.exists(build_cpp_api_binary())
+    assert os.path.exists(build_cpp_api_binary("api_emitter"))
+
+
+def mesh_scene_expectations(Vf, Tf, Ve, Te, n, size, ppc=16, ppb=12):
+    """Oracle counts for InitializeFromTriangleMesh (ppc per seeded cell) and the first emission (ppb per emitter
+    node with SDF <= 0 where the fluid SDF, the mesh's, is >= 0) on an n-cell domain [0, size]^3."""
+    import oracle
+
+    h = [size / n[a] for a in range(3)]
+    sdf = oracle.mesh_to_sdf(Vf, Tf, n, [h[a] / 2.0 for a in range(3)], h)
+    o = oracle.OracleSim(n, oracle.FLIP, size=(size,) * 3)
+    o.set_sdf(sdf)
+    init = ppc * int(o.seed_cells().sum())
+    esdf = oracle.mesh_to_sdf(Ve, Te, n, (0.0, 0.0, 0.0), h)
+    return init, ppb * int(((esdf <= 0) & (sdf >= 0)).sum()), ppb * int((esdf <= 0).sum())
+
+
+@pytest.mark.gpu
+def test_cpp_api_emitter_scene(tmp_path):
+    """The reference's main.cpp sequence (fluid mesh, VolumeEmitter, viscosity, SetMaxClf, frames) through the C++
+    API: seeded and emitted counts equal the oracle's."""
+    from meshes import box, write_obj
+
+    Vf, Tf = box((0.2, 0.2, 0.2), (2.6, 2.0, 5.8))
+    Ve, Te = box((1.9, 1.5, 1.9), (3.1, 2.5, 3.1))  # overlaps the fluid: nodes inside it do not emit
+    write_obj(tmp_path / "emitter.obj", Ve, Te)
+    write_obj(tmp_path / "fluid.obj", Vf, Tf)
+    out = subprocess.run([build_cpp_api_binary("api_emitter"), str(tmp_path / "emitter.obj"), str(tmp_path / "fluid.obj")],
+                         capture_output=True, text=True, check=True).stdout
+    fields = {k: int(v) for k, v in (kv.split("=") for kv in out.split())}
+    init, first_emit, all_emit = mesh_scene_expectations(Vf, Tf, Ve, Te, (30, 30, 30), 6.0)
+    assert init > 0 and 0 < first_emit < all_emit
+    assert fields["init"] == init
+    assert fields["first"] == init + first_emit  # the mesh's fluid SDF survived SetMaxClf's scene rebuild
+    assert fields["frames"] == 3 and fields["final"] >= fields["first"]
+    assert fields["emit_only_frame"] == all_emit  # no particles: one substep of the whole frame, emitting first
+    assert fields["sdf_emitter"] == 5 * 3 * 2 * 4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["pybind", "python"])
+def test_mesh_init_and_emitter_through_mirrors(tmp_path, which):
+    from meshes import box, write_obj
+
+    if which == "pybind":
+        m = pyf()
+    else:
+        import fluide_engine_b200 as m
+    Vf, Tf = box((0.05, 0.05, 0.05), (0.45, 0.5, 0.95))
+    Ve, Te = box((0.35, 0.4, 0.35), (0.65, 0.7, 0.65))
+    write_obj(tmp_path / "fluid.obj", Vf, Tf)
+    write_obj(tmp_path / "emitter.obj", Ve, Te)
+    fluid, emitter = m.TriangleMesh(), m.TriangleMesh()
+    m.OBJManager().Load(str(tmp_path / "fluid.obj"), fluid)
+    m.OBJManager().Load(str(tmp_path / "emitter.obj"), emitter)
+    n = 16
+    domain = m.BoundingBox3D(m.Vector3D(0.0, 0.0, 0.0), m.Vector3D(1.0, 1.0, 1.0))
+    sim = m.FLIPSimulator(m.Vector3S(n, n, n), domain)
+    sim.AddExternalForce(m.DirectionalField(m.Vector3D(0.0, -9.81, 0.0)))
+    sim.InitializeFromTriangleMesh(fluid)
+    init, first_emit, all_emit = mesh_scene_expectations(Vf, Tf, Ve, Te, (n, n, n), 1.0)
+    assert sim.GetNumberOfParticles() == init > 0
+    em = m.VolumeEmitter(emitter, m.Vector3S(n, n, n), domain, 12, m.Vector3D(0.0, 6.0, 0.0), m.Vector3D(0.0))
+    sim.AddEmitter(em)
+    sim.SetMaxClf(1.0)  # rebuilds the scene, keeping the particles and the mesh's fluid SDF
+    sim.AdvanceFixedSubsteps(1.0 / 240.0, 1)
+    assert 0 < first_emit < all_emit
+    assert sim.GetNumberOfParticles() == init + first_emit
+    # an emitter changed after AddEmitter is re-registered at the next step: an all-positive SDF emits nothing
+    em.InitializeFromSdf(m.ScalarGrid3D(m.Vector3S(n, n, n), 1.0, m.Vector3D(0.0), m.Vector3D(1.0 / n)))
+    before = sim.GetNumberOfParticles()
+    sim.AdvanceFixedSubsteps(1.0 / 240.0, 2)
+    assert sim.GetNumberOfParticles() == before
+    sim.SetCurrentFrame(m.Frame(1.0 / 60.0))
+    sim.AdvanceSingleFrame()
+    assert sim.GetNumberOfParticles() == before
 
 
 @pytest.mark.gpu

@@ -92,3 +92,69 @@ def test_volume_emitter_counts_per_substep():
     np2 = g.num_particles()
     g.step(1 / 240, 1)
     assert g.num_particles() == np2
+
+
+def test_emitter_scene_without_particles():
+    """A scene with an emitter and no particles steps (the reference's main.cpp scene): the first substep emits
+    first; an emitter that never emits leaves every substep empty (skipped, reported as converged empty solves)."""
+    n = (16, 16, 16)
+    h = 1.0 / 16
+    V, T = box((0.3, 0.6, 0.3), (0.7, 0.9, 0.7))
+    esdf = oracle.mesh_to_sdf(V, T, n, (0, 0, 0), (h, h, h))
+    g = fe.Scene(n, solver=fe.APIC, max_cfl=1.0)
+    g.add_volume_emitter(V, T, n, (0, 0, 0), (1, 1, 1), particles_per_block=3, velocity=(0.0, -1.0, 0.0), seed=1)
+    assert g.num_particles() == 0
+    assert g.advance_frame(1 / 60) == 1  # CFL of no particles: one substep of the whole frame
+    assert g.num_particles() == 3 * int((esdf <= 0).sum())
+    P, Vel, _ = g.particles()
+    assert np.isfinite(P).all() and (Vel[:, 1] < 0).mean() > 0.5
+    # an emitter outside the grid's nodes never emits
+    e = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0)
+    Vo, To = box((3.0, 3.0, 3.0), (3.5, 3.5, 3.5))
+    e.add_volume_emitter(Vo, To, n, (0, 0, 0), (1, 1, 1), particles_per_block=4)
+    stats = e.step(1 / 240, 3)
+    assert e.num_particles() == 0
+    assert [s["converged"] for s in stats] == [1, 1, 1] and all(s["fluid_cells"] == 0 for s in stats)
+    assert e.advance_frame(1 / 60) == 1 and e.num_particles() == 0
+    # without particles or emitters a scene still refuses to step
+    with pytest.raises(fe.FluideError):
+        fe.Scene(n, solver=fe.FLIP).step(1 / 240, 1)
+
+
+def test_emitter_sdf_and_fluid_sdf_setters():
+    n = (12, 10, 8)
+    h = (1.0 / 12, 1.0 / 10, 1.0 / 8)
+    V, T = box((0.2, 0.2, 0.2), (0.8, 0.8, 0.8))
+    g = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0)
+    eid = g.add_volume_emitter(V, T, (6, 5, 4), (0, 0, 0), (0.5, 0.5, 0.5), particles_per_block=2)
+    sdf = np.ones((4, 5, 6))
+    sdf[1:3, 2, 1:5] = -1.0  # 2 * 1 * 4 nodes (VolumeEmitter::InitializeFromSdf)
+    g.set_emitter_sdf(eid, sdf)
+    # Fluid3::sdf set by the caller: negative (fluid) at one of those nodes, so it does not emit
+    fluid = np.full((n[2], n[1], n[0]), 0.5)
+    fluid[1, 2, 1] = -0.5
+    g.set_fluid_sdf(fluid)
+    assert np.array_equal(g.fluid_sdf(), fluid)
+    g.step(1 / 240, 1)
+    assert g.num_particles() == 2 * (8 - 1)
+    P = g.particles()[0].astype(np.float64)
+    assert (P >= 0).all() and (P[:, 0] < 5 * 0.5 / 6 + 0.05).all()
+    with pytest.raises(fe.FluideError):
+        g.set_emitter_sdf(eid + 1, sdf)
+
+
+def test_advance_frame_emits_every_substep():
+    """PhysicsAnimation::AdvanceTimeStep takes each substep's count from the particles before the emitter runs
+    (physics_animation.cpp:76-86, pic_simulator.cpp:160-163); every substep of the frame emits."""
+    n = (16, 16, 16)
+    h = 1.0 / 16
+    V, T = box((0.3, 0.6, 0.3), (0.7, 0.9, 0.7))
+    esdf = oracle.mesh_to_sdf(V, T, n, (0, 0, 0), (h, h, h))
+    g = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0)
+    pos, _ = fe.seed_regions([dict(kind=0, lo=(0, 0, 0), hi=(1.0, 0.2, 1.0))], n)
+    g.set_particles(pos)
+    g.add_volume_emitter(V, T, n, (0, 0, 0), (1, 1, 1), particles_per_block=2, velocity=(0.0, 3.0, 0.0))
+    np0 = g.num_particles()
+    nsub = g.advance_frame(1 / 60)
+    assert nsub >= 1
+    assert g.num_particles() - np0 >= 2 * int((esdf <= 0).sum())
