@@ -4,12 +4,13 @@ The compute path is the sm_100a library libfluide_b200.so (CUDA kernels + C ABI,
 this package binds it with ctypes and mirrors the reference's simulator API.
 """
 from ._abi import (APIC, FLIP, PIC, AIR, FLUID, AUTO, CG, MGPCG, FluideError, kernel_launch_count, lib,  # noqa: F401
-                   mesh_to_sdf, seed_regions,
+                   mesh_to_sdf, seed_regions, volume_field_vectors,
                    STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_DIFFUSE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P,
                    STAGE_MOVE)
 from .scene import Batch, Scene, face_shapes  # noqa: F401
-from .simulators import (APICSimulator, BoundingBox3D, DirectionalField, Emitter, FLIPSimulator, Frame,  # noqa: F401
-                         HybridSimulator, OBJManager, PICSimulator, ScalarGrid3D, SimulationRunner, SimulationStats,
-                         TriangleMesh, Vector3D, Vector3S, VolumeEmitter)
+from .simulators import (APICSimulator, BoundingBox3D, DirectionalField, Emitter, ExternalForce,  # noqa: F401
+                         FLIPSimulator, Frame, HybridSimulator, OBJManager, PICSimulator, PointField, ScalarGrid3D,
+                         SimulationRunner, SimulationStats, SwirlField, TriangleMesh, Vector3D, Vector3S,
+                         VolumeEmitter, VolumeField)
 
 __version__ = "0.1.0"

@@ -31,7 +31,8 @@ EXPORTS = [
     "fe_scene_get_snapshot", "fe_scene_get_rhs", "fe_scene_get_fluid_sdf", "fe_scene_set_viscosity",
     "fe_scene_get_diffusion", "fe_scene_build_surface", "fe_scene_get_surface", "fe_scene_write_surface_obj",
     "fe_write_obj", "fe_mesh_to_sdf", "fe_scene_init_from_mesh", "fe_scene_add_volume_emitter", "fe_scene_clear_emitters",
-    "fe_scene_set_emitter_sdf", "fe_scene_set_fluid_sdf",
+    "fe_scene_set_emitter_sdf", "fe_scene_set_fluid_sdf", "fe_scene_add_force", "fe_scene_clear_forces",
+    "fe_volume_field_vectors",
     "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
@@ -59,6 +60,18 @@ class StepStats(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+FORCE_POINT, FORCE_SWIRL, FORCE_VOLUME = 1, 2, 3
+
+
+class ForceDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("origin", ctypes.c_double * 3), ("axis", ctypes.c_double * 3),
+                ("strength", ctypes.c_double), ("falloff", ctypes.c_double),
+                ("vertices", ctypes.c_void_p), ("n_vertices", ctypes.c_uint64),
+                ("triangles", ctypes.c_void_p), ("n_triangles", ctypes.c_uint64),
+                ("resolution", ctypes.c_int32 * 3), ("domain_origin", ctypes.c_double * 3),
+                ("domain_size", ctypes.c_double * 3), ("field", ctypes.c_void_p)]
 
 
 class Region(ctypes.Structure):
@@ -119,6 +132,9 @@ def lib():
     L.fe_scene_clear_emitters.argtypes = [P]
     L.fe_scene_set_emitter_sdf.argtypes = [P, ctypes.c_int32, P]
     L.fe_scene_set_fluid_sdf.argtypes = [P, P]
+    L.fe_scene_add_force.argtypes = [P, ctypes.POINTER(ForceDesc), ctypes.POINTER(ctypes.c_int32)]
+    L.fe_scene_clear_forces.argtypes = [P]
+    L.fe_volume_field_vectors.argtypes = [P, ctypes.c_uint64, P, ctypes.c_uint64, P, P, P, P, ctypes.c_int32]
     L.fe_scene_get_sort.argtypes = [P, P, P, ctypes.c_uint64]
     L.fe_scene_divergence.argtypes = [P, D]
     L.fe_scene_set_stream.argtypes = [P, P]
@@ -189,6 +205,49 @@ def seed_regions(regions, n, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), seed=
     vel = np.zeros((cnt, 3), dtype=np.float32)
     L.fe_seed_regions(ctypes.cast(arr, ctypes.c_void_p), len(regions), n3, o, s, seed, ptr(pos), ptr(vel), cnt)
     return pos, vel
+
+
+def volume_field_vectors(vertices, triangles, n, origin, spacing, device=0):
+    """VolumeField::Initialize's closest-point vectors on the GPU (fe_volume_field_vectors): (nz, ny, nx, 3)."""
+    L = lib()
+    V = np.ascontiguousarray(vertices, dtype=np.float64)
+    T = np.ascontiguousarray(triangles, dtype=np.int64)
+    if T.ndim == 2 and T.shape[1] == 3:
+        T = np.ascontiguousarray(np.concatenate([T, np.zeros((T.shape[0], 1), np.int64)], axis=1))
+    out = np.zeros((n[2], n[1], n[0], 3))
+    check(L.fe_volume_field_vectors(ptr(V), V.shape[0], ptr(T), T.shape[0], (ctypes.c_int32 * 3)(*n),
+                                    (ctypes.c_double * 3)(*origin), (ctypes.c_double * 3)(*spacing), ptr(out), device))
+    return out
+
+
+def force_desc(kind, origin=(0.0, 0.0, 0.0), axis=(0.0, 1.0, 0.0), strength=0.0, falloff=1.0, vertices=None,
+               triangles=None, resolution=(1, 1, 1), domain_origin=(0.0, 0.0, 0.0), domain_size=(1.0, 1.0, 1.0),
+               field=None):
+    """An fe_force_desc; the arrays it points to are returned alongside and must outlive the call."""
+    d = ForceDesc()
+    d.kind = kind
+    d.origin[:] = origin
+    d.axis[:] = axis
+    d.strength = strength
+    d.falloff = falloff
+    keep = []
+    if vertices is not None:
+        V = np.ascontiguousarray(vertices, dtype=np.float64)
+        T = np.asarray(triangles, dtype=np.int64)
+        if T.ndim == 2 and T.shape[1] == 3:
+            T = np.concatenate([T, np.zeros((T.shape[0], 1), np.int64)], axis=1)
+        T = np.ascontiguousarray(T)
+        keep += [V, T]
+        d.vertices, d.n_vertices = V.ctypes.data, V.shape[0]
+        d.triangles, d.n_triangles = T.ctypes.data, T.shape[0]
+    d.resolution[:] = resolution
+    d.domain_origin[:] = domain_origin
+    d.domain_size[:] = domain_size
+    if field is not None:
+        F = np.ascontiguousarray(field, dtype=np.float64)
+        keep.append(F)
+        d.field = F.ctypes.data
+    return d, keep
 
 
 def mesh_to_sdf(vertices, triangles, n, origin, spacing, device=0):

@@ -303,6 +303,29 @@ cudaError_t launch_spawn(const int n[3], const double o[3], const double h[3], c
                          const uint32_t* offset, uint64_t seed, const SceneView& v, uint64_t base, const float vel[3],
                          cudaStream_t st);
 
+// VolumeField's closest-point vectors on a node grid (fe_mesh.cu): 3 doubles per node, x-fastest.
+cudaError_t launch_volume_vectors(const double* V, uint64_t nv, const int64_t* T, uint64_t nt, const int n[3],
+                                  const double o[3], const double h[3], double* out, cudaStream_t st);
+
+// Position-dependent external forces (fe_forces.cu), applied after the pre-solve pass (which adds gravity).
+constexpr int kMaxForces = 8;
+struct ForceDev {
+    int kind;                   // FE_FORCE_POINT / SWIRL / VOLUME
+    int n[3];                   // volume: node grid
+    double origin[3], axis[3];  // point / swirl origin; swirl axis (normalised)
+    double strength;
+    double cos_a, sin_a;        // swirl: cos / sin of RotatePointAroundAxis's angle, evaluated on the host
+    double o[3], h[3];          // volume: grid origin and spacing
+    const double* field;        // volume: closest-point vectors, 3 per node
+};
+struct ForceList {
+    int count;
+    ForceDev f[kMaxForces];
+};
+// u, vv, ww: the velocity buffers the pre-solve pass wrote; faces at the velocity grid's data origins.
+cudaError_t launch_forces(const SceneView& v, const ForceList& fl, float* u, float* vv, float* ww, double dt,
+                          cudaStream_t st);
+
 // Viscosity (fe_diffuse.cu): ComputeDiffusion on the velocity buffers u, vv, ww (face markers, FLUID-face list,
 // persistent Jacobi solve, wall layers zeroed).  Uses the scene's solver barrier and error words (CgWork).
 cudaError_t launch_diffuse(const SceneView& v, const DiffWork& d, const CgWork& w, float* u, float* vv, float* ww,

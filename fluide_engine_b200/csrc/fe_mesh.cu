@@ -37,8 +37,9 @@ __device__ __forceinline__ double dd(double a, double b) { return __ddiv_rn(a, b
 __device__ __forceinline__ double dot3(const double a[3], const double b[3]) { return da(da(dm(a[0], b[0]), dm(a[1], b[1])), dm(a[2], b[2])); }
 __device__ __forceinline__ double len3(const double a[3]) { return __dsqrt_rn(dot3(a, a)); }
 
-// Collisions::ClossestPointOnTriangle (3d/collisions.cpp:21-212), region by region, then DistanceToPoint.
-__device__ double distance_to_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3])
+// Collisions::ClossestPointOnTriangle (3d/collisions.cpp:21-212), region by region.
+__device__ void closest_on_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3],
+                                    double out[3])
 {
     double diff[3], e0[3], e1[3];
 #pragma unroll
@@ -99,9 +100,17 @@ __device__ double distance_to_triangle(const double pt[3], const double p0[3], c
             else { s = dd(numer, denom); t = ds(1.0, s); }
         }
     }
-    double c[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) c[d] = ds(da(da(p0[d], dm(s, e0[d])), dm(t, e1[d])), pt[d]);
+    for (int d = 0; d < 3; ++d) out[d] = da(da(p0[d], dm(s, e0[d])), dm(t, e1[d]));
+}
+
+// Collisions::DistanceToTriangle (3d/collisions.cpp:214-217): DistanceToPoint(point, closest point).
+__device__ double distance_to_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3])
+{
+    double c[3];
+    closest_on_triangle(pt, p0, p1, p2, c);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c[d] = ds(c[d], pt[d]);
     return len3(c);
 }
 
@@ -280,6 +289,40 @@ __global__ void k_spawn(NodeGrid g, const uint32_t* __restrict__ count, const ui
     }
 }
 
+// VolumeField::Initialize (forces/volume_field.cpp:72-89): at every node of the field's grid, the closest point on
+// the first nearest triangle (Collisions::ClosestTriangleIdx, 3d/collisions.cpp:249-265: strict < from
+// 1.7976931348623157e30) minus the node position, 3 doubles per node.  One thread per node over all triangles.
+__global__ void __launch_bounds__(256) k_volume_vectors(MeshView m, NodeGrid g, double* __restrict__ out)
+{
+    const size_t nc = (size_t)g.n[0] * g.n[1] * g.n[2];
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % g.n[0]), j = (int)((c / g.n[0]) % g.n[1]), k = (int)(c / ((size_t)g.n[0] * g.n[1]));
+        const double gp[3] = {grid_pos(g, 0, i), grid_pos(g, 1, j), grid_pos(g, 2, k)};
+        double best = 1.7976931348623157e30;
+        uint64_t idx = 0;
+        double A[3], B[3], C[3];
+        for (uint64_t t = 0; t < m.nt; ++t) {
+            load_vertex(m, __ldg(m.T + 4 * t), A);
+            load_vertex(m, __ldg(m.T + 4 * t + 1), B);
+            load_vertex(m, __ldg(m.T + 4 * t + 2), C);
+            const double d = distance_to_triangle(gp, A, B, C);
+            if (d < best) {
+                best = d;
+                idx = t;
+            }
+        }
+        double cp[3] = {0.0, 0.0, 0.0};
+        if (m.nt) {
+            load_vertex(m, m.T[4 * idx], A);
+            load_vertex(m, m.T[4 * idx + 1], B);
+            load_vertex(m, m.T[4 * idx + 2], C);
+            closest_on_triangle(gp, A, B, C, cp);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) out[3 * c + a] = ds(cp[a], gp[a]);
+    }
+}
+
 NodeGrid node_grid(const int n[3], const double o[3], const double h[3])
 {
     NodeGrid g;
@@ -308,6 +351,21 @@ cudaError_t launch_mesh_to_sdf(const double* V, uint64_t nv, const int64_t* T, u
     }
     if (nv == 0) m.nt = 0;  // no vertices: no distances and no triangle to wind around (the fill stays positive)
     k_mesh_sign<<<(unsigned)std::min<size_t>((nc + 255) / 256, 148 * 32), 256, 0, st>>>(m, g, scratch, sdf);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_volume_vectors(const double* V, uint64_t nv, const int64_t* T, uint64_t nt, const int n[3],
+                                  const double o[3], const double h[3], double* out, cudaStream_t st)
+{
+    MeshView m;
+    m.V = V;
+    m.T = T;
+    m.nv = nv;
+    m.nt = nv ? nt : 0;
+    const NodeGrid g = node_grid(n, o, h);
+    const size_t nc = (size_t)n[0] * n[1] * n[2];
+    k_volume_vectors<<<(unsigned)std::min<size_t>((nc + 255) / 256, 148 * 32), 256, 0, st>>>(m, g, out);
     count_launch();
     return cudaGetLastError();
 }

@@ -147,6 +147,9 @@ struct fe_scene {
         std::vector<void*> allocs;
     };
     std::vector<Emitter> emitters;
+    // position-dependent external forces (fe_forces.cu), applied after the pre-solve pass
+    std::vector<std::vector<void*>> force_allocs;
+    ForceList forces{};
     uint64_t epoch = 0;                // bumped when the substep's kernel sequence changes (batches re-capture)
     double* d_scalar = nullptr;        // CFL / divergence result
     float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
@@ -547,6 +550,10 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             FE_CUDA(ensure_grid(s, 0, st));
             FE_CUDA(launch_pre(v, dt, st));
             s->grid_cur = pressure_buffer(s);
+            if (s->forces.count > 0) {
+                const int pb = pressure_buffer(s);
+                FE_CUDA(launch_forces(v, s->forces, pb ? v.u2 : v.u, pb ? v.v2 : v.v, pb ? v.w2 : v.w, dt, st));
+            }
             break;
         case kStepDiffuse:
             if (s->desc.viscosity > 0.0) {
@@ -933,6 +940,7 @@ fe_status fe_scene_destroy(fe_scene* s)
     free_list(s->particle_allocs, s->own_stream);
     free_list(s->surf.mesh_allocs, s->own_stream);
     for (auto& e : s->emitters) free_list(e.allocs, s->own_stream);
+    for (auto& l : s->force_allocs) free_list(l, s->own_stream);
     cudaStreamDestroy(s->own_stream);  // its pending frees still run
     delete s;
     return FE_OK;
@@ -1482,6 +1490,109 @@ fe_status fe_scene_add_volume_emitter(fe_scene* s, const double* vertices, uint6
     return r;
 }
 
+fe_status fe_scene_add_force(fe_scene* s, const fe_force_desc* f, int32_t* id)
+{
+    if (!s || !f) return set_error(FE_ERR_BAD_ARG, "null argument");
+    if (f->kind != FE_FORCE_POINT && f->kind != FE_FORCE_SWIRL && f->kind != FE_FORCE_VOLUME)
+        return set_error(FE_ERR_BAD_ARG, "unknown force kind %d", (int)f->kind);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->forces.count >= kMaxForces) return set_error(FE_ERR_BAD_ARG, "at most %d position-dependent forces", kMaxForces);
+    FE_CUDA(cudaSetDevice(s->device));
+    ForceDev d{};
+    d.kind = f->kind;
+    d.strength = f->strength;
+    for (int a = 0; a < 3; ++a) d.origin[a] = f->origin[a];
+    std::vector<void*> allocs;
+    if (f->kind == FE_FORCE_SWIRL) {
+        // SwirlField stores GetNormalized() of its axis; Sample rotates by 0.0001 degrees (PI, math_utils.hpp:11)
+        const double al = std::sqrt(f->axis[0] * f->axis[0] + f->axis[1] * f->axis[1] + f->axis[2] * f->axis[2]);
+        for (int a = 0; a < 3; ++a) d.axis[a] = f->axis[a] / al;
+        const double angle = 0.0001 * 3.14159265358979323846 / 180;
+        d.cos_a = std::cos(angle);
+        d.sin_a = std::sin(angle);
+    } else if (f->kind == FE_FORCE_VOLUME) {
+        for (int a = 0; a < 3; ++a) {
+            if (f->resolution[a] < 1 || !(f->domain_size[a] > 0.0)) return set_error(FE_ERR_BAD_ARG, "bad volume field grid");
+            d.n[a] = f->resolution[a];
+            d.o[a] = f->domain_origin[a];
+            d.h[a] = f->domain_size[a] / f->resolution[a];  // volume_field.cpp:8
+        }
+        const size_t nc = (size_t)d.n[0] * d.n[1] * d.n[2];
+        cudaStream_t st = s->stream;
+        double* field = nullptr;
+        FE_CUDA(dalloc(allocs, &field, 3 * nc, s->device, st));
+        fe_status r = FE_OK;
+        cudaError_t e = cudaSuccess;
+        if (f->field) {
+            e = cudaMemcpyAsync(field, f->field, 3 * nc * sizeof(double), cudaMemcpyDefault, st);
+        } else {
+            std::vector<void*> list;
+            double* dV = nullptr;
+            int64_t* dT = nullptr;
+            r = upload_mesh(f->vertices, f->n_vertices, f->triangles, f->n_triangles, s->device, st, list, &dV, &dT);
+            if (r == FE_OK) e = launch_volume_vectors(dV, f->n_vertices, dT, f->n_triangles, d.n, d.o, d.h, field, st);
+            free_list(list, st);
+        }
+        if (r == FE_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (r == FE_OK && e != cudaSuccess) r = cuda_check(e, "volume field");
+        if (r != FE_OK) {
+            free_list(allocs, st);
+            return r;
+        }
+        d.field = field;
+    }
+    drop_graphs(s);  // the captured substeps hold the old force list
+    ++s->epoch;
+    if (id) *id = s->forces.count;
+    s->forces.f[s->forces.count++] = d;
+    s->force_allocs.push_back(std::move(allocs));
+    return FE_OK;
+}
+
+fe_status fe_scene_clear_forces(fe_scene* s)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    if (s->forces.count) {
+        drop_graphs(s);
+        ++s->epoch;
+    }
+    for (auto& l : s->force_allocs) free_list(l, s->stream);
+    s->force_allocs.clear();
+    s->forces.count = 0;
+    return FE_OK;
+}
+
+fe_status fe_volume_field_vectors(const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                  uint64_t n_triangles, const int32_t n[3], const double origin[3],
+                                  const double spacing[3], double* out, int32_t device)
+{
+    if (!n || !origin || !spacing || !out) return set_error(FE_ERR_BAD_ARG, "null argument");
+    for (int a = 0; a < 3; ++a)
+        if (n[a] < 1 || !(spacing[a] > 0.0)) return set_error(FE_ERR_BAD_ARG, "bad grid");
+    FE_CUDA(cudaSetDevice(device));
+    cudaStream_t st;
+    FE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    std::vector<void*> list;
+    double* dV = nullptr;
+    int64_t* dT = nullptr;
+    double* dout = nullptr;
+    const size_t nc = (size_t)n[0] * n[1] * n[2];
+    const int nn[3] = {n[0], n[1], n[2]};
+    fe_status r = upload_mesh(vertices, n_vertices, triangles, n_triangles, device, st, list, &dV, &dT);
+    cudaError_t e = cudaSuccess;
+    if (r == FE_OK) e = dalloc(list, &dout, 3 * nc, device, st);
+    if (r == FE_OK && e == cudaSuccess) e = launch_volume_vectors(dV, n_vertices, dT, n_triangles, nn, origin, spacing, dout, st);
+    if (r == FE_OK && e == cudaSuccess) e = cudaMemcpyAsync(out, dout, 3 * nc * sizeof(double), cudaMemcpyDefault, st);
+    if (r == FE_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    free_list(list, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (r != FE_OK) return r;
+    return cuda_check(e, "volume field vectors");
+}
+
 fe_status fe_scene_set_emitter_sdf(fe_scene* s, int32_t id, const double* sdf)
 {
     if (!s || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
@@ -1677,7 +1788,7 @@ uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[
 
 const char* fe_last_error(void) { return g_err; }
 
-int32_t fe_abi_version(void) { return 10300; }
+int32_t fe_abi_version(void) { return 10400; }
 
 }  // extern "C"
 

@@ -101,6 +101,21 @@ PYBIND11_MODULE(PyFluidEngine, m)
         .def(py::init<Vector3<double>>())
         .def("Sample", &DirectionalField::Sample)
         .def("SetStrength", &DirectionalField::SetStrength);
+    py::class_<PointField, std::shared_ptr<PointField>, ExternalForce>(m, "PointField")
+        .def(py::init<Vector3<double>, double, double>())
+        .def("Sample", &PointField::Sample)
+        .def("GetStrength", &PointField::GetStrength)
+        .def("SetStrength", &PointField::SetStrength);
+    py::class_<SwirlField, std::shared_ptr<SwirlField>, ExternalForce>(m, "SwirlField")
+        .def(py::init<Vector3<double>, Vector3<double>, double, double>())
+        .def("Sample", &SwirlField::Sample)
+        .def("GetStrength", &SwirlField::GetStrength)
+        .def("SetStrength", &SwirlField::SetStrength);
+    py::class_<VolumeField, std::shared_ptr<VolumeField>, ExternalForce>(m, "VolumeField")
+        .def(py::init<const TriangleMesh&, Vector3<size_t>, BoundingBox3D, double>())
+        .def("Sample", &VolumeField::Sample)
+        .def("GetStrength", &VolumeField::GetStrength)
+        .def("SetStrength", &VolumeField::SetStrength);
 
     py::class_<HybridSimulator, std::shared_ptr<HybridSimulator>>(m, "HybridSimulator")
         .def("MaxCfl", &HybridSimulator::MaxCfl)
@@ -208,7 +223,7 @@ PYBIND11_MODULE(PyFluidEngine, m)
     pic.def(py::init<Vector3<size_t>, BoundingBox3D>())
         .def("AdvanceSingleFrame", &PICSimulator::AdvanceSingleFrame, py::call_guard<py::gil_scoped_release>())
         .def("InitializeFromTriangleMesh", &PICSimulator::InitializeFromTriangleMesh)
-        .def("AddExternalForce", [](PICSimulator& s, std::shared_ptr<DirectionalField> f) { s.AddExternalForce(f); })
+        .def("AddExternalForce", [](PICSimulator& s, std::shared_ptr<ExternalForce> f) { s.AddExternalForce(f); })
         .def("AddCollider", [](PICSimulator& s, py::object) { s.AddCollider(nullptr); })
         .def("AddEmitter", &PICSimulator::AddEmitter)
         .def("SetCurrentFrame", &PICSimulator::SetCurrentFrame)

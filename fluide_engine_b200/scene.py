@@ -187,6 +187,30 @@ class Scene:
         S = np.ascontiguousarray(sdf, dtype=np.float64)
         check(self._L.fe_scene_set_emitter_sdf(self._h, emitter_id, ptr(S)))
 
+    def add_point_field(self, origin, strength, falloff=1.0):
+        """PointField after gravity in the force list (fe_scene_add_force); returns its index."""
+        return self._add_force(_abi.force_desc(_abi.FORCE_POINT, origin=origin, strength=strength, falloff=falloff))
+
+    def add_swirl_field(self, origin, axis, strength, falloff=1.0):
+        """SwirlField (the axis is normalised as the reference's constructor does)."""
+        return self._add_force(_abi.force_desc(_abi.FORCE_SWIRL, origin=origin, axis=axis, strength=strength,
+                                               falloff=falloff))
+
+    def add_volume_field(self, vertices, triangles, resolution, domain_origin, domain_size, strength, field=None):
+        """VolumeField of a mesh on its own node grid (vectors computed on the GPU unless `field` is given)."""
+        return self._add_force(_abi.force_desc(_abi.FORCE_VOLUME, strength=strength, vertices=vertices,
+                                               triangles=triangles, resolution=resolution,
+                                               domain_origin=domain_origin, domain_size=domain_size, field=field))
+
+    def _add_force(self, desc_keep):
+        desc, _keep = desc_keep
+        fid = ctypes.c_int32()
+        check(self._L.fe_scene_add_force(self._h, ctypes.byref(desc), ctypes.byref(fid)))
+        return fid.value
+
+    def clear_forces(self):
+        check(self._L.fe_scene_clear_forces(self._h))
+
     def set_fluid_sdf(self, sdf):
         """Fluid3::sdf until the next substep (as after init_from_mesh), shape (nz, ny, nx)."""
         S = np.ascontiguousarray(sdf, dtype=np.float64)

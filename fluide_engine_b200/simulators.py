@@ -88,6 +88,79 @@ class DirectionalField(ExternalForce):
         self._strength = Vector3D(*strength)
 
 
+class PointField(ExternalForce):
+    """PointField (forces/point_field.cpp:3-56): strength / max(|p - origin|, 1) toward the origin; applied on the
+    GPU after gravity."""
+
+    def __init__(self, origin=Vector3D(0.0), strength=0.0, strengthFallOff=1.0):
+        self._origin, self._strength, self._falloff = Vector3D(*origin), float(strength), float(strengthFallOff)
+
+    def GetOrigin(self):
+        return self._origin
+
+    def GetStrength(self):
+        return self._strength
+
+    def SetStrength(self, strength):
+        self._strength = float(strength)
+
+    def _add_to(self, scene):
+        scene.add_point_field(tuple(self._origin), self._strength, self._falloff)
+
+
+class SwirlField(ExternalForce):
+    """SwirlField (forces/swirlf_field.cpp:5-23); the axis is normalised as the reference's constructor does."""
+
+    def __init__(self, origin=Vector3D(0.0), axisDirection=Vector3D(0.0, 1.0, 0.0), strength=0.0,
+                 strengthFallOff=1.0):
+        a = np.array(tuple(axisDirection), dtype=np.float64)
+        l = np.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2])
+        self._origin, self._axis, self._axisGiven = Vector3D(*origin), Vector3D(*(a / l)), tuple(a)
+        self._strength, self._falloff = float(strength), float(strengthFallOff)
+
+    def GetOrigin(self):
+        return self._origin
+
+    def GetAxisDirection(self):
+        return self._axis
+
+    def GetStrength(self):
+        return self._strength
+
+    def SetStrength(self, strength):
+        self._strength = float(strength)
+
+    def _add_to(self, scene):
+        scene.add_swirl_field(tuple(self._origin), self._axisGiven, self._strength, self._falloff)  # normalised there
+
+
+class VolumeField(ExternalForce):
+    """VolumeField (forces/volume_field.cpp:5-89) of a TriangleMesh on its own node grid; the closest-point
+    vectors are computed on the GPU the first time the field is registered with a scene."""
+
+    def __init__(self, mesh, resolution, domain, strength):
+        self._V = np.array(mesh.vertices, dtype=np.float64)
+        self._T = np.array(mesh.triangles, dtype=np.int64)
+        self._res = (int(resolution.x), int(resolution.y), int(resolution.z))
+        o, sz = domain.GetOrigin(), domain.GetSize()
+        self._origin, self._size = (o.x, o.y, o.z), (sz.x, sz.y, sz.z)
+        self._strength = float(strength)
+        self._field = None
+
+    def GetStrength(self):
+        return self._strength
+
+    def SetStrength(self, strength):
+        self._strength = float(strength)
+
+    def _add_to(self, scene):
+        if self._field is None:
+            h = tuple(self._size[a] / self._res[a] for a in range(3))
+            self._field = _abi.volume_field_vectors(self._V, self._T, self._res, self._origin, h)
+        scene.add_volume_field(self._V, self._T, self._res, self._origin, self._size, self._strength,
+                               field=self._field)
+
+
 class TriangleMesh:
     """TriangleMesh (3d/triangle_mesh.hpp): vertices (V,3), normals (V,3) and triangles (T,4: three vertex ids and
     the normal id) as numpy arrays, appended to by GetSurface."""
@@ -241,6 +314,7 @@ class HybridSimulator:
         self._density = 1.0
         self._blend = 0.05
         self._forces = []
+        self._fieldForces = []
         self._emitters = []
         self._registered = None         # (scene, emitter versions) the scene's emitters were built from
         self._meshSeed = 0
@@ -311,8 +385,15 @@ class HybridSimulator:
 
     # forces / scene contents ----------------------------------------------------------------------
     def AddExternalForce(self, force):
+        """PICSimulator::AddExternalForce (pic_simulator.cpp:41-44): DirectionalFields add up to gravity; PointField,
+        SwirlField and VolumeField are applied after it on the GPU, in the order added."""
+        if isinstance(force, (PointField, SwirlField, VolumeField)):
+            self._fieldForces.append(force)
+            if self._scene is not None:
+                force._add_to(self._scene)
+            return
         if not isinstance(force, DirectionalField):
-            raise NotImplementedError("only DirectionalField forces are on the substep path")
+            raise TypeError("AddExternalForce: DirectionalField, PointField, SwirlField or VolumeField expected")
         self._rebuild(lambda: self._forces.append(force))
 
     def AddCollider(self, collider):
@@ -407,6 +488,8 @@ class HybridSimulator:
             self._scene = Scene(self._n, solver=self._solver, origin=self._origin, size=self._size,
                                 flip_blend=self._blend, gravity=self._gravity(), max_cfl=self._maxCfl,
                                 device=self._device, viscosity=self._viscosity, **self._cg)
+            for f in self._fieldForces:
+                f._add_to(self._scene)
             if self._pending is not None:
                 p, v, c = self._pending
                 self._scene.set_particles(p, v, c)

@@ -220,6 +220,42 @@ fe_status fe_scene_set_emitter_sdf(fe_scene* s, int32_t id, const double* sdf);
  * between seeding and the first substep (e.g. to change its settings) carry the fluid SDF over. */
 fe_status fe_scene_set_fluid_sdf(fe_scene* s, const double* sdf);
 
+/* Position-dependent external forces (PICSimulator::AddExternalForce, pic_simulator.cpp:41-44, of a PointField,
+ * SwirlField or VolumeField; a DirectionalField is fe_scene_desc::gravity).  Every substep, after gravity,
+ * ComputeExternalForces (pic_simulator.cpp:203-212) adds dt * each force's component at every face position
+ * (ExternalForce::ApplyExternalForce, forces/external_force.cpp:3-29) in the order added, then re-zeroes the
+ * walls.  At most 8 per scene; kept by fe_scene_reset, removed by fe_scene_clear_forces.
+ *   FE_FORCE_POINT  PointField(origin, strength, falloff) (forces/point_field.cpp:3-56)
+ *   FE_FORCE_SWIRL  SwirlField(origin, axis, strength, falloff) (forces/swirlf_field.cpp:5-23; the axis is
+ *                   normalised as its constructor does)
+ *   FE_FORCE_VOLUME VolumeField(mesh, resolution, domain, strength) (forces/volume_field.cpp:5-89): node vectors
+ *                   from `field` (3 doubles per node, x-fastest, host or device) when non-null, else computed
+ *                   from the mesh (closest point on the first nearest triangle minus the node, on the GPU)
+ * falloff is stored by the reference and unused by its samples. */
+typedef enum { FE_FORCE_POINT = 1, FE_FORCE_SWIRL = 2, FE_FORCE_VOLUME = 3 } fe_force_kind;
+typedef struct fe_force_desc {
+    int32_t kind;
+    double origin[3];
+    double axis[3];
+    double strength;
+    double falloff;
+    const double* vertices;   /* volume: mesh, 3 doubles per vertex */
+    uint64_t n_vertices;
+    const int64_t* triangles; /* volume: 4 int64 per triangle (vertex ids, unused normal id) */
+    uint64_t n_triangles;
+    int32_t resolution[3];    /* volume: nodes per axis */
+    double domain_origin[3];  /* volume: grid origin; spacing = domain_size / resolution */
+    double domain_size[3];
+    const double* field;      /* volume: precomputed node vectors, or NULL */
+} fe_force_desc;
+fe_status fe_scene_add_force(fe_scene* s, const fe_force_desc* force, int32_t* id);
+fe_status fe_scene_clear_forces(fe_scene* s);
+/* VolumeField::Initialize's node vectors (forces/volume_field.cpp:72-89) on a grid of n nodes with the given
+ * origin and spacing: 3 doubles per node, x-fastest, written to `out` (host or device). */
+fe_status fe_volume_field_vectors(const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                  uint64_t n_triangles, const int32_t n[3], const double origin[3],
+                                  const double spacing[3], double* out, int32_t device);
+
 /* Viscosity (HybridSimulator::SetViscosity, hybrid_simulator.cpp:97-100), settable at any time.  When it is > 0
  * every substep runs ComputeDiffusion (pic_simulator.cpp:214-222) after the external forces: the reference's
  * BackwardEulerDiffusionSolver (fluid_solvers/backward_euler_diffusion_solver.cpp:20-242) -- per component, faces

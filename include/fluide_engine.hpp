@@ -4,7 +4,7 @@
 // substep: PhysicsAnimation (physics_animation.hpp:8-29), HybridSimulator (hybrid_simulator.hpp:10-41),
 // PICSimulator (pic_simulator.hpp:27-43), FLIPSimulator (flip_simulator.hpp:9-16), APICSimulator
 // (apic_simulator.hpp:9-15), Frame (common/frame.hpp), BoundingBox3D (3d/bounding_box_3d.hpp),
-// DirectionalField (forces/directional_field.hpp), Vector3 (common/vector3.hpp), TriangleMesh, OBJManager,
+// DirectionalField, PointField, SwirlField, VolumeField (forces/), Vector3 (common/vector3.hpp), TriangleMesh, OBJManager,
 // ScalarGrid3D (the node-value subset), VolumeEmitter (emmiter/volume_emmiter.hpp), SimulationStats and
 // SimulationRunner, with the same names and argument meaning.  State lives on the GPU in one fe_scene
 // (include/fluide_b200.h), created on first use.  Colliders are outside the GPU path: AddCollider throws
@@ -94,6 +94,107 @@ class DirectionalField : public ExternalForce {
 
   private:
     Vector3<double> _strength;
+};
+
+namespace fluide {
+inline double length3(double x, double y, double z) { return std::sqrt(x * x + y * y + z * z); }  // Vector3::GetLength
+// A position-dependent force the GPU substep applies (PointField, SwirlField, VolumeField): its C-ABI record.
+class FieldForce : public ExternalForce {
+  public:
+    virtual fe_force_desc Desc() const = 0;
+};
+}  // namespace fluide
+
+// PointField (forces/point_field.cpp:3-56): strength / max(|p - origin|, 1) toward the origin.
+class PointField : public fluide::FieldForce {
+  public:
+    PointField(Vector3<double> origin = Vector3<double>(0), double strength = 0, double strengthFallOff = 1)
+        : _origin(origin), _strength(strength), _strengthFallOff(strengthFallOff) {}
+    Vector3<double> Sample(const Vector3<double>& p) const override
+    {
+        const double len = fluide::length3(p.x - _origin.x, p.y - _origin.y, p.z - _origin.z);
+        const double dist = len >= 1.0 ? len : 1.0;
+        const double ex = _origin.x - p.x, ey = _origin.y - p.y, ez = _origin.z - p.z;
+        const double el = fluide::length3(ex, ey, ez);
+        const double sc = _strength * (1.0 / dist);
+        return Vector3<double>(sc * (ex / el), sc * (ey / el), sc * (ez / el));
+    }
+    void SetPosition(Vector3<double> origin) { _origin = origin; }
+    void SetStrength(double strength) { _strength = strength; }
+    void SetStrengthFallOff(double f) { _strengthFallOff = f; }
+    Vector3<double> GetOrigin() const { return _origin; }
+    double GetStrength() const { return _strength; }
+    double GetStrengthFallOff() const { return _strengthFallOff; }
+    fe_force_desc Desc() const override
+    {
+        fe_force_desc d{};
+        d.kind = FE_FORCE_POINT;
+        d.origin[0] = _origin.x; d.origin[1] = _origin.y; d.origin[2] = _origin.z;
+        d.strength = _strength;
+        d.falloff = _strengthFallOff;
+        return d;
+    }
+
+  private:
+    Vector3<double> _origin;
+    double _strength, _strengthFallOff;
+};
+
+// SwirlField (forces/swirlf_field.cpp:5-23): strength / max(d, 1)^2 along the displacement of a small rotation about
+// the axis (Collisions::RotatePointAroundAxis / DistanceToAxis, 3d/collisions.cpp:219-246).
+class SwirlField : public fluide::FieldForce {
+  public:
+    SwirlField(Vector3<double> origin = Vector3<double>(0), Vector3<double> axisDirection = Vector3<double>(0, 1, 0),
+               double strength = 0, double strengthFallOff = 1)
+        : _origin(origin), _axisGiven(axisDirection), _strength(strength), _strengthFallOff(strengthFallOff)
+    {
+        const double l = fluide::length3(axisDirection.x, axisDirection.y, axisDirection.z);
+        _axis = Vector3<double>(axisDirection.x / l, axisDirection.y / l, axisDirection.z / l);
+    }
+    Vector3<double> Sample(const Vector3<double>& p) const override
+    {
+        const Vector3<double>& o = _origin;
+        const Vector3<double>& ax = _axis;
+        const double d0 = fluide::length3(o.x - ax.x, o.y - ax.y, o.z - ax.z);
+        const double dx = (ax.x - o.x) / d0, dy = (ax.y - o.y) / d0, dz = (ax.z - o.z) / d0;
+        const double t = (p.x - o.x) * dx + (p.y - o.y) * dy + (p.z - o.z) * dz;
+        double dist = fluide::length3(p.x - (o.x + t * dx), p.y - (o.y + t * dy), p.z - (o.z + t * dz));
+        dist = dist >= 1.0 ? dist : 1.0;
+        const double angle = 0.0001 * 3.14159265358979323846 / 180, cA = std::cos(angle), sA = std::sin(angle);
+        const double al = fluide::length3(ax.x, ax.y, ax.z);
+        const double u = ax.x / al, v = ax.y / al, w = ax.z / al, x = p.x, y = p.y, z = p.z, a = o.x, b = o.y, c = o.z;
+        const double rx = (a * (v * v + w * w) - u * (b * v + c * w - u * x - v * y - w * z)) * (1 - cA) + x * cA +
+                          ((-1.0 * c) * v + b * w - w * y + v * z) * sA;
+        const double ry = (b * (u * u + w * w) - v * (a * u + c * w - u * x - v * y - w * z)) * (1 - cA) + y * cA +
+                          (c * u - a * w + w * x - u * z) * sA;
+        const double rz = (c * (u * u + v * v) - w * (a * u + b * v - u * x - v * y - w * z)) * (1 - cA) + z * cA +
+                          ((-1.0 * b) * u + a * v - v * x + u * y) * sA;
+        const double fx = x - rx, fy = y - ry, fz = z - rz, fl = fluide::length3(fx, fy, fz);
+        const double sc = _strength * (1 / (dist * dist));
+        return Vector3<double>(sc * (fx / fl), sc * (fy / fl), sc * (fz / fl));
+    }
+    void SetOrigin(Vector3<double> origin) { _origin = origin; }
+    void SetAxisDirection(Vector3<double>) {}  // the reference's setter assigns its parameter to itself (swirlf_field.cpp:36-39)
+    void SetStrength(double strength) { _strength = strength; }
+    void SetStrengthFallOff(double f) { _strengthFallOff = f; }
+    Vector3<double> GetOrigin() const { return _origin; }
+    Vector3<double> GetAxisDirection() const { return _axis; }
+    double GetStrength() const { return _strength; }
+    double GetStrengthFallOff() const { return _strengthFallOff; }
+    fe_force_desc Desc() const override
+    {
+        fe_force_desc d{};
+        d.kind = FE_FORCE_SWIRL;
+        d.origin[0] = _origin.x; d.origin[1] = _origin.y; d.origin[2] = _origin.z;
+        d.axis[0] = _axisGiven.x; d.axis[1] = _axisGiven.y; d.axis[2] = _axisGiven.z;  // the library normalises it
+        d.strength = _strength;
+        d.falloff = _strengthFallOff;
+        return d;
+    }
+
+  private:
+    Vector3<double> _origin, _axisGiven, _axis;
+    double _strength, _strengthFallOff;
 };
 
 // Region description for InitializeFromRegions (layout of the C ABI's fe_seed_regions records).
@@ -250,6 +351,90 @@ inline void flatten_mesh(const TriangleMesh& mesh, std::vector<double>& V, std::
     }
 }
 }  // namespace fluide
+
+// VolumeField (forces/volume_field.cpp:5-89): at every node of its grid (`resolution` nodes over `domain`) the
+// vector from the node to the closest point of the mesh; Sample interpolates it trilinearly and pushes along its
+// negation with strength / max(|vector|, 1)^2.  The vectors are computed on the GPU (fe_volume_field_vectors) on
+// first use; the simulators apply the force on the GPU.
+class VolumeField : public fluide::FieldForce {
+  public:
+    VolumeField(const TriangleMesh& mesh, Vector3<size_t> resolution, BoundingBox3D domain, double strength)
+        : _resolution(resolution), _strength(strength)
+    {
+        const Vector3<double> s = domain.GetSize();
+        _domainSize = s;
+        _origin = domain.GetOrigin();
+        _gridSpacing = Vector3<double>(s.x / resolution.x, s.y / resolution.y, s.z / resolution.z);
+        fluide::flatten_mesh(mesh, _V, _T);
+    }
+    Vector3<double> Sample(const Vector3<double>& p) const override
+    {
+        const std::vector<double>& f = Vectors();
+        const size_t n[3] = {_resolution.x, _resolution.y, _resolution.z};
+        const double x[3] = {(p.x - _origin.x) / _gridSpacing.x, (p.y - _origin.y) / _gridSpacing.y,
+                             (p.z - _origin.z) / _gridSpacing.z};
+        size_t i0[3], i1[3];
+        double fr[3];
+        for (int a = 0; a < 3; ++a) {  // GetBarycentric (common/math_utils.hpp:48-73), iLow 0, iHigh n - 1
+            const int hi = (int)n[a] - 1;
+            const double fl = std::floor(x[a]);
+            int ii = (int)fl;
+            if (hi == 0 || ii < 0) { ii = 0; fr[a] = 0.0; }
+            else if (ii > hi - 1) { ii = hi - 1; fr[a] = 1.0; }
+            else fr[a] = x[a] - fl;
+            i0[a] = (size_t)ii;
+            i1[a] = std::min((size_t)ii + 1, n[a] - 1);
+        }
+        auto at = [&](size_t i, size_t j, size_t k, int c) { return f[3 * (i + n[0] * (j + n[1] * k)) + c]; };
+        auto lerp = [](double a, double b, double t) { return (1 - t) * a + t * b; };
+        double q[3];
+        for (int c = 0; c < 3; ++c) {
+            const double b0 = lerp(lerp(at(i0[0], i0[1], i0[2], c), at(i1[0], i0[1], i0[2], c), fr[0]),
+                                   lerp(at(i0[0], i1[1], i0[2], c), at(i1[0], i1[1], i0[2], c), fr[0]), fr[1]);
+            const double b1 = lerp(lerp(at(i0[0], i0[1], i1[2], c), at(i1[0], i0[1], i1[2], c), fr[0]),
+                                   lerp(at(i0[0], i1[1], i1[2], c), at(i1[0], i1[1], i1[2], c), fr[0]), fr[1]);
+            q[c] = lerp(b0, b1, fr[2]);
+        }
+        const double len = fluide::length3(q[0], q[1], q[2]);
+        const double dist = len >= 1.0 ? len : 1.0;
+        const double sc = _strength * (1 / (dist * dist));
+        return Vector3<double>(sc * ((q[0] / len) * -1.0), sc * ((q[1] / len) * -1.0), sc * ((q[2] / len) * -1.0));
+    }
+    void SetStrength(double strength) { _strength = strength; }
+    double GetStrength() const { return _strength; }
+    // The node vectors (3 per node, x-fastest), computed on the GPU the first time they are needed.
+    const std::vector<double>& Vectors() const
+    {
+        if (_field.empty()) {
+            std::vector<double> f(3 * _resolution.x * _resolution.y * _resolution.z);
+            const int32_t n[3] = {(int32_t)_resolution.x, (int32_t)_resolution.y, (int32_t)_resolution.z};
+            const double o[3] = {_origin.x, _origin.y, _origin.z}, h[3] = {_gridSpacing.x, _gridSpacing.y, _gridSpacing.z};
+            fluide::check(fe_volume_field_vectors(_V.data(), _V.size() / 3, _T.data(), _T.size() / 4, n, o, h, f.data(), 0));
+            _field = std::move(f);
+        }
+        return _field;
+    }
+    fe_force_desc Desc() const override
+    {
+        fe_force_desc d{};
+        d.kind = FE_FORCE_VOLUME;
+        d.strength = _strength;
+        d.resolution[0] = (int32_t)_resolution.x; d.resolution[1] = (int32_t)_resolution.y;
+        d.resolution[2] = (int32_t)_resolution.z;
+        d.domain_origin[0] = _origin.x; d.domain_origin[1] = _origin.y; d.domain_origin[2] = _origin.z;
+        d.domain_size[0] = _domainSize.x; d.domain_size[1] = _domainSize.y; d.domain_size[2] = _domainSize.z;
+        d.field = Vectors().data();
+        return d;
+    }
+
+  private:
+    Vector3<size_t> _resolution;
+    Vector3<double> _origin, _gridSpacing, _domainSize;
+    double _strength;
+    std::vector<double> _V;
+    std::vector<int64_t> _T;
+    mutable std::vector<double> _field;
+};
 
 class Collider;
 
@@ -449,8 +634,19 @@ class HybridSimulator : public PhysicsAnimation {
         fluide::check(fe_scene_step(Scene(), dt, nsub, stats));
     }
 
+    // PICSimulator::AddExternalForce (pic_simulator.cpp:41-44).  DirectionalFields add up to the scene's gravity;
+    // PointField, SwirlField and VolumeField are applied after it on the GPU, in the order added.
     void AddExternalForce(const std::shared_ptr<ExternalForce> newForce)
     {
+        if (auto field = std::dynamic_pointer_cast<fluide::FieldForce>(newForce)) {
+            const fe_force_desc d = field->Desc();
+            if (_scene) fluide::check(fe_scene_add_force(_scene, &d, nullptr));
+            _fieldForces.push_back(field);
+            _forces.push_back(newForce);
+            return;
+        }
+        if (!std::dynamic_pointer_cast<DirectionalField>(newForce))
+            throw std::invalid_argument("AddExternalForce: DirectionalField, PointField, SwirlField or VolumeField expected");
         Reconfigure([&] {
             const Vector3<double> g = newForce->Sample(Vector3<double>(0));
             _desc.gravity[0] += g.x;
@@ -503,6 +699,10 @@ class HybridSimulator : public PhysicsAnimation {
         if (!_scene) {
             fluide::check(fe_scene_create(&_desc, &_scene));
             ++_sceneGeneration;
+            for (const auto& f : _fieldForces) {
+                const fe_force_desc d = f->Desc();
+                fluide::check(fe_scene_add_force(_scene, &d, nullptr));
+            }
             Upload();
             if (_meshSdfLive && !_sdf.empty()) fluide::check(fe_scene_set_fluid_sdf(_scene, _sdf.data()));
             _sdf.clear();
@@ -564,6 +764,7 @@ class HybridSimulator : public PhysicsAnimation {
     size_t _particlesPerBlok = 16;  // hybrid_simulator.cpp:22
     std::vector<float> _pos, _vel, _C;
     std::vector<std::shared_ptr<ExternalForce>> _forces;
+    std::vector<std::shared_ptr<fluide::FieldForce>> _fieldForces;
     std::vector<std::shared_ptr<VolumeEmitter>> _emitters;
     std::vector<uint64_t> _emitterVersions;
     uint64_t _sceneGeneration = 0, _emitterGeneration = 0, _meshSeed = 0;

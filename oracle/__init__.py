@@ -119,6 +119,12 @@ def lib():
         L.or_set_sdf.argtypes = [P, D]
         L.or_seed_regions.restype = ctypes.c_size_t
         L.or_seed_regions.argtypes = [ctypes.c_void_p, ctypes.c_int, I3, D, D, ctypes.c_uint64, F, F, ctypes.c_size_t]
+        for name in ("or_add_point_field", "or_add_swirl_field", "or_add_volume_field"):
+            getattr(L, name).restype = ctypes.c_int
+        L.or_add_point_field.argtypes = [P, D, ctypes.c_double]
+        L.or_add_swirl_field.argtypes = [P, D, D, ctypes.c_double]
+        L.or_add_volume_field.argtypes = [P, D, I64, ctypes.c_size_t, I3, D, D, ctypes.c_double]
+        L.or_volume_field_vectors.argtypes = [D, I64, ctypes.c_size_t, I3, D, D, D]
         _lib = L
     return _lib
 
@@ -277,6 +283,24 @@ class OracleSim:
     def rhs(self):
         b = self._cells(np.float64); self.L.or_get_rhs(self.h, dptr(b)); return b
 
+    def add_point_field(self, origin, strength):
+        """PointField (forces/point_field.cpp) after gravity in the force list."""
+        assert self.L.or_add_point_field(self.h, dptr(np.array(origin, dtype=np.float64)), strength) == 0
+
+    def add_swirl_field(self, origin, axis, strength):
+        """SwirlField (forces/swirlf_field.cpp)."""
+        assert self.L.or_add_swirl_field(self.h, dptr(np.array(origin, dtype=np.float64)),
+                                         dptr(np.array(axis, dtype=np.float64)), strength) == 0
+
+    def add_volume_field(self, V, T, n, domain_origin, domain_size, strength):
+        """VolumeField (forces/volume_field.cpp) of a mesh (V (nv,3), T (nt,4) int64)."""
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.int64)
+        assert self.L.or_add_volume_field(self.h, dptr(V), T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), T.shape[0],
+                                          iptr(np.array(n, dtype=np.int32)),
+                                          dptr(np.array(domain_origin, dtype=np.float64)),
+                                          dptr(np.array(domain_size, dtype=np.float64)), strength) == 0
+
     def stage(self, name, dt=None):
         fn = getattr(self.L, "or_stage_" + name) if name != "markers" else self.L.or_build_markers
         return fn(self.h) if dt is None else fn(self.h, dt)
@@ -316,6 +340,18 @@ def build_surface(sdf, n, origin, h):
     assert L.or_build_surface(dptr(sdf), iptr(n3), dptr(o), dptr(hh), dptr(V), dptr(N), T.ctypes.data_as(I64),
                               nv.value, nt.value, ctypes.byref(nv), ctypes.byref(nt)) == 0
     return V, N, T
+
+
+def volume_field_vectors(V, T, n, origin, h):
+    """VolumeField::Initialize's closest-point vectors: (nz, ny, nx, 3)."""
+    L = lib()
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    T = np.ascontiguousarray(T, dtype=np.int64)
+    out = np.zeros((n[2], n[1], n[0], 3))
+    L.or_volume_field_vectors(dptr(V), T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), T.shape[0],
+                              iptr(np.array(n, dtype=np.int32)), dptr(np.array(origin, dtype=np.float64)),
+                              dptr(np.array(h, dtype=np.float64)), dptr(out))
+    return out
 
 
 def mesh_to_sdf(V, T, n, origin, h):
@@ -411,6 +447,10 @@ def ref_lib(variant="serial"):
         L.ref_save_obj.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
         L.ref_mesh_to_sdf.argtypes = [D, ctypes.c_size_t, I64, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), D, D, D]
         L.ref_init_from_mesh.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t]
+        L.ref_add_point_field.argtypes = [P, D, ctypes.c_double, ctypes.c_double]
+        L.ref_add_swirl_field.argtypes = [P, D, D, ctypes.c_double, ctypes.c_double]
+        L.ref_add_volume_field.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), D,
+                                           D, ctypes.c_double]
         _ref_libs[variant] = L
     return _ref_libs[variant]
 
@@ -476,6 +516,20 @@ class RefSim:
         a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
         self.L.ref_get_face_markers(self.h, u8ptr(a), u8ptr(b), u8ptr(c))
         return a, b, c
+
+    def add_point_field(self, origin, strength, falloff=1.0):
+        self.L.ref_add_point_field(self.h, dptr(np.array(origin, dtype=np.float64)), strength, falloff)
+
+    def add_swirl_field(self, origin, axis, strength, falloff=1.0):
+        self.L.ref_add_swirl_field(self.h, dptr(np.array(origin, dtype=np.float64)),
+                                   dptr(np.array(axis, dtype=np.float64)), strength, falloff)
+
+    def add_volume_field(self, V, T, n, domain_origin, domain_size, strength):
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.int64)
+        self.L.ref_add_volume_field(self.h, dptr(V), V.shape[0], T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                    T.shape[0], (ctypes.c_int * 3)(*n), dptr(np.array(domain_origin, dtype=np.float64)),
+                                    dptr(np.array(domain_size, dtype=np.float64)), strength)
 
     def stage(self, name, dt=None):
         fn = getattr(self.L, "ref_stage_" + name)

@@ -27,6 +27,19 @@ typedef struct {
 static inline size_t ix3(dim3i d, int i, int j, int k) { return (size_t)i + (size_t)d.x * ((size_t)j + (size_t)d.y * (size_t)k); }
 static inline size_t cnt3(dim3i d) { return (size_t)d.x * (size_t)d.y * (size_t)d.z; }
 
+/* A position-dependent external force (PointField, SwirlField, VolumeField), after the DirectionalField of
+ * or_desc::gravity in PICSimulator::_externalForces. */
+typedef struct {
+    int kind;                    /* OR_FORCE_POINT / SWIRL / VOLUME */
+    double origin[3], axis[3];   /* point / swirl origin; swirl axis (normalised, as the SwirlField constructor) */
+    double strength;
+    double cos_a, sin_a;         /* RotatePointAroundAxis's cos / sin of its 0.0001-degree angle */
+    int n[3];                    /* volume field: node grid and its closest-point vectors (3 per node) */
+    double o[3], h[3];
+    double* field;
+} or_force;
+#define OR_MAX_FORCES 8
+
 struct or_sim {
     or_desc d;
     dim3i n;                 /* cells */
@@ -48,6 +61,8 @@ struct or_sim {
     double cg_res;
     uint8_t *dmu, *dmv, *dmw; /* diffusion face markers (BackwardEulerDiffusionSolver::_fluidMarkers) */
     int diff_it[3];           /* Jacobi iterations of the last diffusion solve, per component */
+    or_force forces[OR_MAX_FORCES];
+    int nforces;
 };
 
 /* ---------------------------------------------------------------- math_utils.hpp restatements */
@@ -316,6 +331,7 @@ void or_destroy(or_sim* s)
     free(s->mu); free(s->mv); free(s->mw);
     free(s->sdf); free(s->marks); free(s->p); free(s->b);
     free(s->dmu); free(s->dmv); free(s->dmw);
+    for (int f = 0; f < s->nforces; ++f) free(s->forces[f].field);
     free(s);
 }
 
@@ -607,12 +623,15 @@ void or_stage_bc(or_sim* s)
 
 /* PICSimulator::ComputeExternalForces (pic_simulator.cpp:203-212) with one DirectionalField
  * (forces/external_force.cpp:4-29, forces/directional_field.cpp:13-16). */
+static void apply_position_forces(or_sim* s, double dt);
+
 void or_stage_forces(or_sim* s, double dt)
 {
     size_t nu = cnt3(s->du), nv = cnt3(s->dv), nw = cnt3(s->dw);
     for (size_t f = 0; f < nu; ++f) s->u[f] += dt * s->d.gravity[0];
     for (size_t f = 0; f < nv; ++f) s->v[f] += dt * s->d.gravity[1];
     for (size_t f = 0; f < nw; ++f) s->w[f] += dt * s->d.gravity[2];
+    apply_position_forces(s, dt);
     or_stage_bc(s);
 }
 
@@ -1578,3 +1597,194 @@ void or_seed_cells(const or_sim* s, uint8_t* mask)
 }
 
 void or_set_sdf(or_sim* s, const double* sdf) { memcpy(s->sdf, sdf, cnt3(s->n) * sizeof(double)); }
+
+/* ---------------------------------------------------------------- position-dependent external forces */
+
+static double vlen(double x, double y, double z) { return sqrt(x * x + y * y + z * z); } /* Vector3::GetLength */
+
+/* PointField::Sample (forces/point_field.cpp:16-19, GetDistance :46-49, GetDirection :51-56). */
+static void point_sample(const or_force* f, const double p[3], double out[3])
+{
+    const double len = vlen(p[0] - f->origin[0], p[1] - f->origin[1], p[2] - f->origin[2]);
+    const double dist = len >= 1.0 ? len : 1.0;
+    double e[3] = {f->origin[0] - p[0], f->origin[1] - p[1], f->origin[2] - p[2]};
+    const double el = vlen(e[0], e[1], e[2]); /* Normalize = Divide(length) */
+    for (int a = 0; a < 3; ++a) e[a] /= el;
+    const double sc = f->strength * (1.0 / dist);
+    for (int a = 0; a < 3; ++a) out[a] = sc * e[a];
+}
+
+/* Collisions::RotatePointAroundAxis (3d/collisions.cpp:219-237): rotation of p about the line through
+ * (a, b, c) with direction (u, v, w), the closed form of the rotation matrix about an arbitrary axis. */
+static void rotate_about_axis(const double o[3], const double axis[3], const double p[3], double cA, double sA,
+                              double out[3])
+{
+    const double al = vlen(axis[0], axis[1], axis[2]); /* GetNormalized */
+    const double u = axis[0] / al, v = axis[1] / al, w = axis[2] / al;
+    const double x = p[0], y = p[1], z = p[2];
+    const double a = o[0], b = o[1], c = o[2];
+    out[0] = (a * (v * v + w * w) - u * (b * v + c * w - u * x - v * y - w * z)) * (1 - cA) + x * cA +
+             ((-1.0 * c) * v + b * w - w * y + v * z) * sA;
+    out[1] = (b * (u * u + w * w) - v * (a * u + c * w - u * x - v * y - w * z)) * (1 - cA) + y * cA +
+             (c * u - a * w + w * x - u * z) * sA;
+    out[2] = (c * (u * u + v * v) - w * (a * u + b * v - u * x - v * y - w * z)) * (1 - cA) + z * cA +
+             ((-1.0 * b) * u + a * v - v * x + u * y) * sA;
+}
+
+/* SwirlField::Sample (forces/swirlf_field.cpp:16-23) with Collisions::DistanceToAxis (3d/collisions.cpp:239-246),
+ * which takes the axis direction as a second point on the axis. */
+static void swirl_sample(const or_force* f, const double p[3], double out[3])
+{
+    const double* o = f->origin;
+    const double* ax = f->axis;
+    const double d0 = vlen(o[0] - ax[0], o[1] - ax[1], o[2] - ax[2]); /* DistanceToPoint(axisDirection, axisOrigin) */
+    double dir[3], vv[3], cl[3];
+    for (int a = 0; a < 3; ++a) dir[a] = (ax[a] - o[a]) / d0;
+    for (int a = 0; a < 3; ++a) vv[a] = p[a] - o[a];
+    const double t = vv[0] * dir[0] + vv[1] * dir[1] + vv[2] * dir[2];
+    for (int a = 0; a < 3; ++a) cl[a] = o[a] + t * dir[a];
+    double dist = vlen(p[0] - cl[0], p[1] - cl[1], p[2] - cl[2]);
+    dist = dist >= 1.0 ? dist : 1.0;
+    double r[3], fd[3];
+    rotate_about_axis(o, ax, p, f->cos_a, f->sin_a, r);
+    for (int a = 0; a < 3; ++a) fd[a] = p[a] - r[a];
+    const double fl = vlen(fd[0], fd[1], fd[2]);
+    for (int a = 0; a < 3; ++a) fd[a] = fd[a] / fl;
+    const double sc = f->strength * (1 / (dist * dist));
+    for (int a = 0; a < 3; ++a) out[a] = sc * fd[a];
+}
+
+/* VolumeField::Sample (forces/volume_field.cpp:20-58): trilinear closest-point vector, force along its negation
+ * with strength / max(|vector|, 1)^2. */
+static void volume_sample(const or_force* f, const double p[3], double out[3])
+{
+    int id[3], ip[3];
+    double fr[3];
+    for (int a = 0; a < 3; ++a) {
+        barycentric((p[a] - f->o[a]) / f->h[a], f->n[a] - 1, &id[a], &fr[a]);
+        ip[a] = id[a] + 1 < f->n[a] - 1 ? id[a] + 1 : f->n[a] - 1;
+    }
+    double sv[3];
+    for (int c = 0; c < 3; ++c) {
+#define FV(i, j, k) f->field[3 * ((size_t)(i) + (size_t)f->n[0] * ((size_t)(j) + (size_t)f->n[1] * (size_t)(k))) + c]
+        const double q[8] = {FV(id[0], id[1], id[2]), FV(ip[0], id[1], id[2]), FV(id[0], ip[1], id[2]),
+                             FV(ip[0], ip[1], id[2]), FV(id[0], id[1], ip[2]), FV(ip[0], id[1], ip[2]),
+                             FV(id[0], ip[1], ip[2]), FV(ip[0], ip[1], ip[2])};
+#undef FV
+        sv[c] = or_trilerp(q, fr[0], fr[1], fr[2]);
+    }
+    const double len = vlen(sv[0], sv[1], sv[2]);
+    double fd[3];
+    for (int a = 0; a < 3; ++a) fd[a] = (sv[a] / len) * (-1.0);
+    const double dist = len >= 1.0 ? len : 1.0;
+    const double sc = f->strength * (1 / (dist * dist));
+    for (int a = 0; a < 3; ++a) out[a] = sc * fd[a];
+}
+
+static void force_sample(const or_force* f, const double p[3], double out[3])
+{
+    if (f->kind == OR_FORCE_POINT) point_sample(f, p, out);
+    else if (f->kind == OR_FORCE_SWIRL) swirl_sample(f, p, out);
+    else volume_sample(f, p, out);
+}
+
+/* ExternalForce::ApplyExternalForce (forces/external_force.cpp:3-29) of every position-dependent force, in the
+ * order added: each face += dt * the force's component at the face position (FaceCenteredGrid3D::GetXPos, ...). */
+static void apply_position_forces(or_sim* s, double dt)
+{
+    const double* org[3] = {s->xo, s->yo, s->zo};
+    double* arr[3] = {s->u, s->v, s->w};
+    const dim3i dims[3] = {s->du, s->dv, s->dw};
+    for (int f = 0; f < s->nforces; ++f)
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < dims[c].z; ++k)
+                for (int j = 0; j < dims[c].y; ++j)
+                    for (int i = 0; i < dims[c].x; ++i) {
+                        const double p[3] = {org[c][0] + s->h[0] * (double)i, org[c][1] + s->h[1] * (double)j,
+                                             org[c][2] + s->h[2] * (double)k};
+                        double fv[3];
+                        force_sample(&s->forces[f], p, fv);
+                        arr[c][ix3(dims[c], i, j, k)] += dt * fv[c];
+                    }
+}
+
+static or_force* new_force(or_sim* s, int kind, double strength)
+{
+    if (s->nforces >= OR_MAX_FORCES) return NULL;
+    or_force* f = &s->forces[s->nforces++];
+    memset(f, 0, sizeof(*f));
+    f->kind = kind;
+    f->strength = strength;
+    return f;
+}
+
+/* PointField(origin, strength, strengthFallOff) (forces/point_field.cpp:3-5); the fall-off is unused by Sample. */
+int or_add_point_field(or_sim* s, const double origin[3], double strength)
+{
+    or_force* f = new_force(s, OR_FORCE_POINT, strength);
+    if (!f) return -1;
+    for (int a = 0; a < 3; ++a) f->origin[a] = origin[a];
+    return 0;
+}
+
+/* SwirlField(origin, axisDirection, strength, strengthFallOff) (forces/swirlf_field.cpp:5-8): the axis is stored
+ * normalised; the rotation angle of Sample is 0.0001 degrees (PI from common/math_utils.hpp:11). */
+int or_add_swirl_field(or_sim* s, const double origin[3], const double axis[3], double strength)
+{
+    or_force* f = new_force(s, OR_FORCE_SWIRL, strength);
+    if (!f) return -1;
+    const double al = vlen(axis[0], axis[1], axis[2]);
+    for (int a = 0; a < 3; ++a) {
+        f->origin[a] = origin[a];
+        f->axis[a] = axis[a] / al;
+    }
+    const double ang = 0.0001 * 3.14159265358979323846 / 180;
+    f->cos_a = cos(ang);
+    f->sin_a = sin(ang);
+    return 0;
+}
+
+/* The closest-point vectors of VolumeField::Initialize (forces/volume_field.cpp:72-89): at every node of the
+ * field's grid, closest point on the first nearest triangle (Collisions::ClosestTriangleIdx, 3d/collisions.cpp:
+ * 249-265, strict < from 1.7976931348623157e30) minus the node position.  (Initialize also builds a Mesh2SDF
+ * that Sample never reads.) */
+void or_volume_field_vectors(const double* V, const int64_t* T, size_t nt, const int n[3], const double o[3],
+                             const double h[3], double* out)
+{
+    for (int k = 0; k < n[2]; ++k)
+        for (int j = 0; j < n[1]; ++j)
+            for (int i = 0; i < n[0]; ++i) {
+                const double gp[3] = {o[0] + i * h[0], o[1] + j * h[1], o[2] + k * h[2]};
+                double best = 1.7976931348623157E+30;
+                size_t idx = 0;
+                for (size_t t = 0; t < nt; ++t) {
+                    const double d = or_distance_to_triangle(gp, V + 3 * T[4 * t], V + 3 * T[4 * t + 1], V + 3 * T[4 * t + 2]);
+                    if (d < best) {
+                        best = d;
+                        idx = t;
+                    }
+                }
+                double cp[3] = {0, 0, 0};
+                if (nt) closest_on_triangle(gp, V + 3 * T[4 * idx], V + 3 * T[4 * idx + 1], V + 3 * T[4 * idx + 2], cp);
+                double* dst = out + 3 * ((size_t)i + (size_t)n[0] * ((size_t)j + (size_t)n[1] * (size_t)k));
+                for (int a = 0; a < 3; ++a) dst[a] = cp[a] - gp[a];
+            }
+}
+
+/* VolumeField(mesh, resolution, domain, strength) (forces/volume_field.cpp:5-13): spacing = domain size /
+ * resolution, origin = domain origin. */
+int or_add_volume_field(or_sim* s, const double* V, const int64_t* T, size_t nt, const int n[3],
+                        const double domain_origin[3], const double domain_size[3], double strength)
+{
+    if (n[0] < 1 || n[1] < 1 || n[2] < 1) return -1;
+    or_force* f = new_force(s, OR_FORCE_VOLUME, strength);
+    if (!f) return -1;
+    for (int a = 0; a < 3; ++a) {
+        f->n[a] = n[a];
+        f->o[a] = domain_origin[a];
+        f->h[a] = domain_size[a] / n[a];
+    }
+    f->field = (double*)xcalloc(3 * (size_t)n[0] * n[1] * n[2], sizeof(double));
+    or_volume_field_vectors(V, T, nt, f->n, f->o, f->h, f->field);
+    return 0;
+}

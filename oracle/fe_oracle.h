@@ -75,6 +75,18 @@ void or_stage_move(or_sim* s, double dt);           /* MoveParticles only */
 void or_build_markers(or_sim* s);                   /* SinglePhasePressureSolver::BuildMarkers only */
 void or_stage_diffusion(or_sim* s, double dt);      /* ComputeDiffusion (3 Jacobi solves + BC; no-op at viscosity 0) */
 
+/* Position-dependent external forces, applied by or_stage_forces after the DirectionalField of or_desc::gravity
+ * in the order added (at most 8); 0 on success.  PointField (forces/point_field.cpp), SwirlField
+ * (forces/swirlf_field.cpp), VolumeField (forces/volume_field.cpp, mesh as in or_mesh_to_sdf). */
+enum { OR_FORCE_POINT = 1, OR_FORCE_SWIRL = 2, OR_FORCE_VOLUME = 3 };
+int or_add_point_field(or_sim* s, const double origin[3], double strength);
+int or_add_swirl_field(or_sim* s, const double origin[3], const double axis[3], double strength);
+int or_add_volume_field(or_sim* s, const double* V, const int64_t* T, size_t nt, const int n[3],
+                        const double domain_origin[3], const double domain_size[3], double strength);
+/* VolumeField::Initialize's closest-point vectors on a node grid (3 doubles per node, x-fastest). */
+void or_volume_field_vectors(const double* V, const int64_t* T, size_t nt, const int n[3], const double o[3],
+                             const double h[3], double* out);
+
 void or_substep(or_sim* s, double dt);              /* PICSimulator::OnAdvanceTimeStep */
 double or_cfl(const or_sim* s, double dt);          /* PICSimulator::Cfl */
 unsigned or_number_of_substeps(const or_sim* s, double dt); /* PICSimulator::NumberOfSubTimeSteps */

@@ -29,6 +29,9 @@
 #include "3d/mesh_2_sdf.hpp"
 #include "fluid_solvers/backward_euler_diffusion_solver.hpp"
 #include "forces/directional_field.hpp"
+#include "forces/point_field.hpp"
+#include "forces/swirl_field.hpp"
+#include "forces/volume_field.hpp"
 #undef private
 #undef protected
 
@@ -321,6 +324,33 @@ void ref_save_obj(void* p, const char* path, const char* name)
     OBJManager obj;
     quiet(h, true);
     obj.Save(path, h->mesh);
+    quiet(h, false);
+}
+
+// PICSimulator::AddExternalForce (pic_simulator.cpp:41-44) of the reference's position-dependent fields, after the
+// DirectionalField that ref_create adds.
+void ref_add_point_field(void* p, const double* origin, double strength, double falloff)
+{
+    Handle* h = (Handle*)p;
+    h->sim->AddExternalForce(std::make_shared<PointField>(Vector3<double>(origin[0], origin[1], origin[2]), strength, falloff));
+}
+
+void ref_add_swirl_field(void* p, const double* origin, const double* axis, double strength, double falloff)
+{
+    Handle* h = (Handle*)p;
+    h->sim->AddExternalForce(std::make_shared<SwirlField>(Vector3<double>(origin[0], origin[1], origin[2]),
+                                                          Vector3<double>(axis[0], axis[1], axis[2]), strength, falloff));
+}
+
+void ref_add_volume_field(void* p, const double* v, size_t nv, const int64_t* t, size_t nt, const int* n,
+                          const double* domain_origin, const double* domain_size, double strength)
+{
+    Handle* h = (Handle*)p;
+    TriangleMesh mesh = make_mesh(v, nv, t, nt);
+    BoundingBox3D domain(Vector3<double>(domain_origin[0], domain_origin[1], domain_origin[2]),
+                         Vector3<double>(domain_size[0], domain_size[1], domain_size[2]));
+    quiet(h, true);
+    h->sim->AddExternalForce(std::make_shared<VolumeField>(mesh, Vector3<size_t>(n[0], n[1], n[2]), domain, strength));
     quiet(h, false);
 }
 
