@@ -132,6 +132,9 @@ struct fe_scene {
     bool prev_valid = false;
     // Fluid3::sdf holds the mesh SDF of fe_scene_init_from_mesh (in surf.sdf) until the next substep
     bool mesh_sdf = false;
+    // BuildCollider has run (at the start of some substep): until then the collider SDF is its initial 0
+    // (ColliderCollection's ScalarGrid3D, 3d/collider_collection.cpp:5-8), which no emitter node passes (> 0)
+    bool collider_built = false;
     // VolumeEmitters (fe_mesh.cu): each emits at the start of every substep
     struct Emitter {
         int n[3];
@@ -537,6 +540,7 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             s->parity ^= 1;
             s->prev_valid = true;
             s->mesh_sdf = false;
+            s->collider_built = true;
             break;
         }
         case kStepP2g:
@@ -682,6 +686,8 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
             // Nothing emitted yet: the reference's substep would only build an all-air grid and the all-positive
             // SDF of no particles, which emits like the initial 0 SDF, so skipping it leaves the same state.
             s->last_substep_empty = true;
+            s->collider_built = true;
+            s->mesh_sdf = false;  // the substep's SDF of no particles is positive everywhere (emits like the initial 0)
             for (int q = 0; q < 4; ++q)
                 if (ev) FE_CUDA(cudaEventRecord(ev[q], s->stream));
             return FE_OK;
@@ -730,6 +736,7 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
     s->parity ^= 1;  // the sort inside the first graph flipped the buffer sets
     s->prev_valid = true;
     s->mesh_sdf = false;
+    s->collider_built = true;
     s->grid_cur = 0;
     return FE_OK;
 }
@@ -779,11 +786,13 @@ fe_status surface_sdf(fe_scene* s)
 
 // PICSimulator::OnBeginAdvanceTimeStep's emitter loop (pic_simulator.cpp:160-163): every VolumeEmitter adds its
 // particles to the current set before the substep, reading the fluid SDF the previous substep built (zero -- the
-// initial value of Fluid3::sdf -- before any substep and without a mesh initialisation).  The counts are read back
+// initial value of Fluid3::sdf -- before any substep and without a mesh initialisation).  The emitter also needs
+// the collider SDF > 0 at the node, and the collider SDF is built right after the emitters, so in a scene's first
+// substep it still holds its initial 0 and nothing is emitted.  The counts are read back
 // to size the particle arrays, so a substep with emitters runs without graphs.
 fe_status emit_particles(fe_scene* s)
 {
-    if (s->emitters.empty()) return FE_OK;
+    if (s->emitters.empty() || !s->collider_built) return FE_OK;  // colliderSdf(i, j, k) > 0 fails on the initial 0
     cudaStream_t st = s->stream;
     const double* fluid = nullptr;
     if (s->prev_valid || s->mesh_sdf) {
@@ -1012,6 +1021,7 @@ fe_status fe_scene_reset(fe_scene* s)
     s->grid_cur = 0;
     s->prev_valid = false;
     s->mesh_sdf = false;
+    s->collider_built = false;
     for (auto& e : s->emitters) free_list(e.allocs, s->stream);
     s->emitters.clear();
     return FE_OK;
@@ -1165,7 +1175,10 @@ fe_status fe_scene_advance_frame(fe_scene* s, double frame_dt, int32_t* substeps
             if (s->have_particles && s->base.np > 0) {
                 st = enqueue_stages(s, sub, FE_STAGE_SORT, FE_STAGE_MOVE);
                 if (st != FE_OK) return st;
+            } else {
+                s->mesh_sdf = false;  // as in run_substep's skipped substep
             }
+            s->collider_built = true;
         }
         remaining -= sub;
         ++count;
@@ -1920,6 +1933,7 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = null
         s->parity ^= 1;  // the pre-solve graph's sort flipped the particle buffer sets
         s->prev_valid = true;
         s->mesh_sdf = false;
+        s->collider_built = true;
         s->grid_cur = 0;
     }
     if (ev) FE_CUDA(cudaEventRecord(ev[3], b->stream));
@@ -2180,6 +2194,7 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
             s->parity ^= 1;
             s->prev_valid = true;
             s->mesh_sdf = false;
+            s->collider_built = true;
             s->grid_cur = 0;
         }
     }

@@ -170,6 +170,14 @@ PYBIND11_MODULE(PyFluidEngine, m)
                  if (c.size() != p.size() * 3) c.assign(p.size() * 3, 0.f);
                  return py::make_tuple(to_arr(p, 3), to_arr(v, 3), to_arr(c, 9));
              })
+        .def("GetFluidSdf",
+             [](HybridSimulator& s) {
+                 const ScalarGrid3D g = s.GetFluidSdf();
+                 const Vector3<size_t> n = g.GetSize();
+                 py::array_t<double> out({(py::ssize_t)n.z, (py::ssize_t)n.y, (py::ssize_t)n.x});
+                 std::copy(g.GetRawData().begin(), g.GetRawData().end(), out.mutable_data());
+                 return out;
+             })
         .def("AdvanceFixedSubsteps",
              [](HybridSimulator& s, double dt, int nsub) {
                  std::vector<fe_step_stats> st((size_t)std::max(nsub, 1));

@@ -198,7 +198,9 @@ fe_status fe_write_obj(const char* path, const char* object_name, const double* 
  * (resolution, domain; resolution within the scene's grid): at the start of every substep each emitter node
  * with SDF <= 0 whose fluid SDF value (same index; the SDF of the previous substep) is >= 0 receives
  * particles_per_block particles at position + h * U[0,1]^3 with `velocity` (PICSimulator::OnBeginAdvanceTimeStep,
- * pic_simulator.cpp:160-163).  A scene with emitters steps without graphs (its particle count changes) and cannot
+ * pic_simulator.cpp:160-163), except in the scene's first substep: the reference's emitters also require the
+ * collider SDF > 0 and run before the first BuildCollider, while that SDF still holds its initial 0, so the first
+ * substep emits nothing (fe_scene_reset starts over).  A scene with emitters steps without graphs (its particle count changes) and cannot
  * join a batch; it may start without particles (fe_scene_step and fe_scene_advance_frame then emit first; a
  * substep that still has none is skipped and reports a converged empty solve).  fe_scene_clear_emitters removes
  * them (fe_scene_reset does too). */

@@ -675,6 +675,19 @@ class HybridSimulator : public PhysicsAnimation {
                                               (uint32_t)_particlesPerBlok, _meshSeed++));
         _meshSdfLive = true;
     }
+    // HybridSimulator::GetFluidSdf (hybrid_simulator.hpp:35): Fluid3::sdf, the SDF built at the start of the last
+    // substep (or the mesh SDF of InitializeFromTriangleMesh before any), on the nodes at origin + h / 2.
+    ScalarGrid3D GetFluidSdf()
+    {
+        const Vector3<double> h = GetGridSpacing(), o = GetOrigin();
+        ScalarGrid3D g(_n, 0.0, Vector3<double>(o.x + h.x / 2.0, o.y + h.y / 2.0, o.z + h.z / 2.0), h);
+        std::vector<double> v(_n.x * _n.y * _n.z);
+        fluide::check(fe_scene_get_fluid_sdf(Scene(), v.data()));
+        for (size_t k = 0; k < _n.z; ++k)
+            for (size_t j = 0; j < _n.y; ++j)
+                for (size_t i = 0; i < _n.x; ++i) g(i, j, k) = v[i + _n.x * (j + _n.y * k)];
+        return g;
+    }
     // PICSimulator::GetSurface (pic_simulator.cpp:71-78): appends the marching-cubes surface of Fluid3::sdf (the
     // SDF built at the start of the last substep) to mesh, exactly as the reference's surface tracker does.
     void GetSurface(TriangleMesh& mesh)

@@ -3,7 +3,8 @@
 // InitializeFromTriangleMesh(fluid mesh), a VolumeEmitter (12 particles per node, velocity (0, 6, 0)),
 // SetViscosity(0.01), SetMaxClf(5), frames of 1/60 s.  A second simulator starts from the emitter alone, a third
 // takes its emitter SDF from a ScalarGrid3D (InitializeFromSdf).
-// argv[1] = emitter OBJ, argv[2] = fluid OBJ.  Prints "init=<n> first=<n> frames=<n> final=<n>
+// argv[1] = emitter OBJ, argv[2] = fluid OBJ, argv[3] = where to write the fluid SDF after the first substep
+// (doubles, x-fastest).  Prints "init=<n> none=<n> first=<n> frames=<n> final=<n> emit_only_first=<n>
 // emit_only_frame=<n> sdf_emitter=<n>" for the test to check.
 #include <cstdio>
 #include <memory>
@@ -27,9 +28,16 @@ int main(int argc, char** argv)
     const size_t init = sim.GetNumberOfParticles();
     sim.AddEmitter(std::make_shared<VolumeEmitter>(emitterObject, size, domain, 12, Vector3<double>(0.0, 6.0, 0.0), 0.0));
     sim.SetViscosity(0.01);
+    const ScalarGrid3D meshSdf = sim.GetFluidSdf();
     sim.SetMaxClf(5);  // rebuilds the scene: the particles and the mesh's fluid SDF are carried over
+    const ScalarGrid3D kept = sim.GetFluidSdf();
+    int sdfKept = kept.GetRawData() == meshSdf.GetRawData() ? 1 : 0;
+    sim.AdvanceFixedSubsteps(1.0 / 240.0, 1);  // the first substep emits nothing (collider SDF still 0)
+    const size_t none = sim.GetNumberOfParticles();
+    const ScalarGrid3D fluidSdf = sim.GetFluidSdf();  // built in that substep; the next one emits where it is >= 0
     sim.AdvanceFixedSubsteps(1.0 / 240.0, 1);
     const size_t first = sim.GetNumberOfParticles();
+
     sim.SetCurrentFrame(Frame(1.0 / 60.0));
     for (int f = 0; f < 3; ++f) sim.AdvanceSingleFrame();
     const size_t fin = sim.GetNumberOfParticles();
@@ -39,7 +47,9 @@ int main(int argc, char** argv)
     only.AddEmitter(std::make_shared<VolumeEmitter>(emitterObject, size, domain, 12, Vector3<double>(0.0, 6.0, 0.0), 0.0));
     only.SetMaxClf(5);
     only.SetCurrentFrame(Frame(1.0 / 60.0));
-    only.AdvanceSingleFrame();  // starts without particles: the first substep emits
+    only.AdvanceSingleFrame();  // starts without particles: its one substep emits nothing
+    const size_t emitOnlyFirst = only.GetNumberOfParticles();
+    only.AdvanceSingleFrame();  // now every node inside the emitter emits
     const size_t emitOnlyFrame = only.GetNumberOfParticles();
 
     // an emitter SDF negative on the nodes 10..12 x 20..21 x 10..13: 3 * 2 * 4 nodes emit 5 particles each
@@ -51,10 +61,22 @@ int main(int argc, char** argv)
     fromSdf->InitializeFromSdf(grid);
     PICSimulator third(size, domain);
     third.AddEmitter(fromSdf);
-    third.AdvanceFixedSubsteps(1.0 / 240.0, 1);
+    third.AdvanceFixedSubsteps(1.0 / 240.0, 2);
     const size_t sdfEmitter = third.GetNumberOfParticles();
 
-    std::printf("init=%zu first=%zu frames=%lu final=%zu emit_only_frame=%zu sdf_emitter=%zu\n", init, first,
-                sim.GetCurrentFrame().GetIndex(), fin, emitOnlyFrame, sdfEmitter);
+    // the fluid SDF the second substep's emission read, written for the test's own count
+    if (argc > 3) {
+        FILE* f = std::fopen(argv[3], "wb");
+        if (!f) return 3;
+        for (size_t k = 0; k < size.z; ++k)
+            for (size_t j = 0; j < size.y; ++j)
+                for (size_t i = 0; i < size.x; ++i) {
+                    const double v = fluidSdf(i, j, k);
+                    std::fwrite(&v, sizeof(double), 1, f);
+                }
+        std::fclose(f);
+    }
+    std::printf("sdf_kept=%d init=%zu none=%zu first=%zu frames=%lu final=%zu emit_only_first=%zu emit_only_frame=%zu sdf_emitter=%zu\n",
+                sdfKept, init, none, first, sim.GetCurrentFrame().GetIndex(), fin, emitOnlyFirst, emitOnlyFrame, sdfEmitter);
     return 0;
 }

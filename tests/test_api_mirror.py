@@ -118,9 +118,9 @@ def test_cpp_api_compiles_and_links():
     assert os.path.exists(build_cpp_api_binary("api_emitter"))
 
 
-def mesh_scene_expectations(Vf, Tf, Ve, Te, n, size, ppc=16, ppb=12):
-    """Oracle counts for InitializeFromTriangleMesh (ppc per seeded cell) and the first emission (ppb per emitter
-    node with SDF <= 0 where the fluid SDF, the mesh's, is >= 0) on an n-cell domain [0, size]^3."""
+def mesh_scene_expectations(Vf, Tf, Ve, Te, n, size, ppc=16):
+    """Oracle values for InitializeFromTriangleMesh on an n-cell domain [0, size]^3: the particle count (ppc per
+    seeded cell), the fluid mesh's SDF and the emitter mesh's SDF on the emitter grid."""
     import oracle
 
     h = [size / n[a] for a in range(3)]
@@ -129,7 +129,7 @@ def mesh_scene_expectations(Vf, Tf, Ve, Te, n, size, ppc=16, ppb=12):
     o.set_sdf(sdf)
     init = ppc * int(o.seed_cells().sum())
     esdf = oracle.mesh_to_sdf(Ve, Te, n, (0.0, 0.0, 0.0), h)
-    return init, ppb * int(((esdf <= 0) & (sdf >= 0)).sum()), ppb * int((esdf <= 0).sum())
+    return init, sdf, esdf
 
 
 @pytest.mark.gpu
@@ -142,15 +142,21 @@ def test_cpp_api_emitter_scene(tmp_path):
     Ve, Te = box((1.9, 1.5, 1.9), (3.1, 2.5, 3.1))  # overlaps the fluid: nodes inside it do not emit
     write_obj(tmp_path / "emitter.obj", Ve, Te)
     write_obj(tmp_path / "fluid.obj", Vf, Tf)
-    out = subprocess.run([build_cpp_api_binary("api_emitter"), str(tmp_path / "emitter.obj"), str(tmp_path / "fluid.obj")],
-                         capture_output=True, text=True, check=True).stdout
+    sdf_path = tmp_path / "fluid_sdf.bin"
+    out = subprocess.run([build_cpp_api_binary("api_emitter"), str(tmp_path / "emitter.obj"), str(tmp_path / "fluid.obj"),
+                          str(sdf_path)], capture_output=True, text=True, check=True).stdout
     fields = {k: int(v) for k, v in (kv.split("=") for kv in out.split())}
-    init, first_emit, all_emit = mesh_scene_expectations(Vf, Tf, Ve, Te, (30, 30, 30), 6.0)
-    assert init > 0 and 0 < first_emit < all_emit
-    assert fields["init"] == init
-    assert fields["first"] == init + first_emit  # the mesh's fluid SDF survived SetMaxClf's scene rebuild
+    init, _, esdf = mesh_scene_expectations(Vf, Tf, Ve, Te, (30, 30, 30), 6.0)
+    fluid = np.fromfile(sdf_path, dtype=np.float64).reshape(30, 30, 30)  # after the first substep
+    emit = 12 * int(((esdf <= 0) & (fluid >= 0)).sum())
+    assert fields["sdf_kept"] == 1  # the mesh's fluid SDF survived SetMaxClf's scene rebuild
+    assert fields["init"] == init > 0
+    assert fields["none"] == init  # the first substep emits nothing: the collider SDF is still its initial 0
+    assert 0 < emit < 12 * int((esdf <= 0).sum())  # the emitter overlaps the fluid: nodes inside it do not emit
+    assert fields["first"] == init + emit
     assert fields["frames"] == 3 and fields["final"] >= fields["first"]
-    assert fields["emit_only_frame"] == all_emit  # no particles: one substep of the whole frame, emitting first
+    assert fields["emit_only_first"] == 0  # no particles: one substep of the whole frame, emitting nothing
+    assert fields["emit_only_frame"] == 12 * int((esdf <= 0).sum())
     assert fields["sdf_emitter"] == 5 * 3 * 2 * 4
 
 
@@ -175,14 +181,19 @@ def test_mesh_init_and_emitter_through_mirrors(tmp_path, which):
     sim = m.FLIPSimulator(m.Vector3S(n, n, n), domain)
     sim.AddExternalForce(m.DirectionalField(m.Vector3D(0.0, -9.81, 0.0)))
     sim.InitializeFromTriangleMesh(fluid)
-    init, first_emit, all_emit = mesh_scene_expectations(Vf, Tf, Ve, Te, (n, n, n), 1.0)
+    init, mesh_sdf, esdf = mesh_scene_expectations(Vf, Tf, Ve, Te, (n, n, n), 1.0)
     assert sim.GetNumberOfParticles() == init > 0
     em = m.VolumeEmitter(emitter, m.Vector3S(n, n, n), domain, 12, m.Vector3D(0.0, 6.0, 0.0), m.Vector3D(0.0))
     sim.AddEmitter(em)
     sim.SetMaxClf(1.0)  # rebuilds the scene, keeping the particles and the mesh's fluid SDF
+    assert np.array_equal(sim.GetFluidSdf(), mesh_sdf)
     sim.AdvanceFixedSubsteps(1.0 / 240.0, 1)
-    assert 0 < first_emit < all_emit
-    assert sim.GetNumberOfParticles() == init + first_emit
+    assert sim.GetNumberOfParticles() == init  # the scene's first substep emits nothing
+    fl = sim.GetFluidSdf()
+    sim.AdvanceFixedSubsteps(1.0 / 240.0, 1)
+    emit = 12 * int(((esdf <= 0) & (fl >= 0)).sum())
+    assert 0 < emit < 12 * int((esdf <= 0).sum())
+    assert sim.GetNumberOfParticles() == init + emit
     # an emitter changed after AddEmitter is re-registered at the next step: an all-positive SDF emits nothing
     em.InitializeFromSdf(m.ScalarGrid3D(m.Vector3S(n, n, n), 1.0, m.Vector3D(0.0), m.Vector3D(1.0 / n)))
     before = sim.GetNumberOfParticles()

@@ -72,11 +72,15 @@ def test_volume_emitter_counts_per_substep():
     eid = g.add_volume_emitter(V, T, n, (0, 0, 0), (1, 1, 1), particles_per_block=8, velocity=(0.0, 6.0, 0.0), seed=3)
     assert eid == 0
     esdf = oracle.mesh_to_sdf(V, T, n, (0, 0, 0), (h, h, h))
-    # first substep: Fluid3::sdf is still its initial 0 everywhere, so every emitter node with sdf <= 0 emits
+    # first substep: the collider SDF still holds its initial 0, which fails the emitter's > 0 test everywhere
     np0 = g.num_particles()
     g.step(1 / 240, 1)
+    assert g.num_particles() == np0
+    # second substep: every node inside the emitter where the first substep's fluid SDF is >= 0 emits
+    fluid = g.fluid_sdf()
+    g.step(1 / 240, 1)
     np1 = g.num_particles()
-    assert np1 - np0 == 8 * int((esdf <= 0).sum()) > 0
+    assert np1 - np0 == 8 * int(((esdf <= 0) & (fluid >= 0)).sum()) > 0
     P, Vel, _ = g.particles()
     new_p = P[np0:].astype(np.float64)
     # emitted inside the emitter's nodes (box [0.3, 0.7] x [0.6, 0.9] x [0.3, 0.7] plus one cell of node extent),
@@ -84,7 +88,7 @@ def test_volume_emitter_counts_per_substep():
     lo, hi = np.array([0.3, 0.6, 0.3]) - 2 * h, np.array([0.7, 0.9, 0.7]) + 2 * h
     assert ((new_p >= lo) & (new_p <= hi)).all()
     assert Vel[np0:, 1].mean() > 1.0  # they start at (0, 6, 0)
-    # second substep: emission where the fluid SDF of the previous substep is >= 0
+    # third substep: where the emitted particles now make the fluid SDF negative, nothing more is emitted
     fluid = g.fluid_sdf()
     g.step(1 / 240, 1)
     assert g.num_particles() - np1 == 8 * int(((esdf <= 0) & (fluid >= 0)).sum())
@@ -104,7 +108,9 @@ def test_emitter_scene_without_particles():
     g = fe.Scene(n, solver=fe.APIC, max_cfl=1.0)
     g.add_volume_emitter(V, T, n, (0, 0, 0), (1, 1, 1), particles_per_block=3, velocity=(0.0, -1.0, 0.0), seed=1)
     assert g.num_particles() == 0
-    assert g.advance_frame(1 / 60) == 1  # CFL of no particles: one substep of the whole frame
+    assert g.advance_frame(1 / 60) == 1  # CFL of no particles: one substep of the whole frame, emitting nothing
+    assert g.num_particles() == 0
+    assert g.advance_frame(1 / 60) == 1  # the collider SDF is built now: every node inside the emitter emits
     assert g.num_particles() == 3 * int((esdf <= 0).sum())
     P, Vel, _ = g.particles()
     assert np.isfinite(P).all() and (Vel[:, 1] < 0).mean() > 0.5
@@ -130,6 +136,8 @@ def test_emitter_sdf_and_fluid_sdf_setters():
     sdf = np.ones((4, 5, 6))
     sdf[1:3, 2, 1:5] = -1.0  # 2 * 1 * 4 nodes (VolumeEmitter::InitializeFromSdf)
     g.set_emitter_sdf(eid, sdf)
+    g.step(1 / 240, 1)  # the first substep emits nothing (and, without particles, is skipped)
+    assert g.num_particles() == 0
     # Fluid3::sdf set by the caller: negative (fluid) at one of those nodes, so it does not emit
     fluid = np.full((n[2], n[1], n[0]), 0.5)
     fluid[1, 2, 1] = -0.5
@@ -155,6 +163,10 @@ def test_advance_frame_emits_every_substep():
     g.set_particles(pos)
     g.add_volume_emitter(V, T, n, (0, 0, 0), (1, 1, 1), particles_per_block=2, velocity=(0.0, 3.0, 0.0))
     np0 = g.num_particles()
-    nsub = g.advance_frame(1 / 60)
+    assert g.advance_frame(1 / 60) == 1  # particles at rest: CFL 0, one substep, the scene's first: no emission
+    assert g.num_particles() == np0
+    fluid = g.fluid_sdf()
+    nsub = g.advance_frame(1 / 60)  # its first substep emits where the previous substep's fluid SDF is >= 0
     assert nsub >= 1
-    assert g.num_particles() - np0 >= 2 * int((esdf <= 0).sum())
+    first = 2 * int(((esdf <= 0) & (fluid >= 0)).sum())
+    assert first > 0 and g.num_particles() - np0 >= first
