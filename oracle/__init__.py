@@ -125,6 +125,10 @@ def lib():
         L.or_add_swirl_field.argtypes = [P, D, D, ctypes.c_double]
         L.or_add_volume_field.argtypes = [P, D, I64, ctypes.c_size_t, I3, D, D, ctypes.c_double]
         L.or_volume_field_vectors.argtypes = [D, I64, ctypes.c_size_t, I3, D, D, D]
+        L.or_add_mesh_collider.restype = ctypes.c_int
+        L.or_add_mesh_collider.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t, D, ctypes.c_size_t, I3, D, D]
+        L.or_build_collider.argtypes = [P]
+        L.or_get_collider_sdf.argtypes = [P, D]
         _lib = L
     return _lib
 
@@ -282,6 +286,24 @@ class OracleSim:
 
     def rhs(self):
         b = self._cells(np.float64); self.L.or_get_rhs(self.h, dptr(b)); return b
+
+    def add_mesh_collider(self, V, T, N, n, origin, h):
+        """TriangleMeshCollider of a mesh (V (nv,3), T (nt,4) int64 with normal ids into N (nn,3)) on its own grid."""
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.int64)
+        N = np.ascontiguousarray(N, dtype=np.float64)
+        assert self.L.or_add_mesh_collider(self.h, dptr(V), V.shape[0], T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                           T.shape[0], dptr(N), N.shape[0], iptr(np.array(n, dtype=np.int32)),
+                                           dptr(np.array(origin, dtype=np.float64)),
+                                           dptr(np.array(h, dtype=np.float64))) == 0
+
+    def build_collider(self):
+        self.L.or_build_collider(self.h)
+
+    def collider_sdf(self):
+        out = np.zeros((self.n[2], self.n[1], self.n[0]))
+        self.L.or_get_collider_sdf(self.h, dptr(out))
+        return out
 
     def add_point_field(self, origin, strength):
         """PointField (forces/point_field.cpp) after gravity in the force list."""
@@ -448,6 +470,9 @@ def ref_lib(variant="serial"):
         L.ref_mesh_to_sdf.argtypes = [D, ctypes.c_size_t, I64, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), D, D, D]
         L.ref_init_from_mesh.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t]
         L.ref_add_point_field.argtypes = [P, D, ctypes.c_double, ctypes.c_double]
+        L.ref_add_mesh_collider.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t, D, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_int), D, D]
+        L.ref_get_collider_sdf.argtypes = [P, D]
         L.ref_add_swirl_field.argtypes = [P, D, D, ctypes.c_double, ctypes.c_double]
         L.ref_add_volume_field.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), D,
                                            D, ctypes.c_double]
@@ -516,6 +541,19 @@ class RefSim:
         a, b, c = (np.zeros(s, dtype=np.uint8) for s in (su, sv, sw))
         self.L.ref_get_face_markers(self.h, u8ptr(a), u8ptr(b), u8ptr(c))
         return a, b, c
+
+    def add_mesh_collider(self, V, T, N, n, origin, h):
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.int64)
+        N = np.ascontiguousarray(N, dtype=np.float64)
+        self.L.ref_add_mesh_collider(self.h, dptr(V), V.shape[0], T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                     T.shape[0], dptr(N), N.shape[0], (ctypes.c_int * 3)(*n),
+                                     dptr(np.array(origin, dtype=np.float64)), dptr(np.array(h, dtype=np.float64)))
+
+    def collider_sdf(self):
+        out = np.zeros((self.n[2], self.n[1], self.n[0]))
+        self.L.ref_get_collider_sdf(self.h, dptr(out))
+        return out
 
     def add_point_field(self, origin, strength, falloff=1.0):
         self.L.ref_add_point_field(self.h, dptr(np.array(origin, dtype=np.float64)), strength, falloff)

@@ -40,6 +40,19 @@ typedef struct {
 } or_force;
 #define OR_MAX_FORCES 8
 
+/* A TriangleMeshCollider (3d/triangle_mesh_collider.cpp:4-8): the mesh and its Mesh2SDF on the collider's own node
+ * grid. */
+typedef struct {
+    int n[3];
+    double o[3], h[3];
+    double* sdf;
+    double* V;
+    int64_t* T;
+    double* N;     /* mesh normals; triangle t's normal is N[T[4t + 3]] */
+    size_t nv, nt, nn;
+} or_collider;
+#define OR_MAX_COLLIDERS 8
+
 struct or_sim {
     or_desc d;
     dim3i n;                 /* cells */
@@ -63,6 +76,9 @@ struct or_sim {
     int diff_it[3];           /* Jacobi iterations of the last diffusion solve, per component */
     or_force forces[OR_MAX_FORCES];
     int nforces;
+    or_collider colliders[OR_MAX_COLLIDERS];
+    int ncolliders;
+    double* csdf;             /* ColliderCollection::_sdf on the n nodes at the domain origin; initially 0 */
 };
 
 /* ---------------------------------------------------------------- math_utils.hpp restatements */
@@ -319,6 +335,7 @@ or_sim* or_create(const or_desc* d)
     s->dmu = (uint8_t*)xcalloc(cnt3(s->du), 1);
     s->dmv = (uint8_t*)xcalloc(cnt3(s->dv), 1);
     s->dmw = (uint8_t*)xcalloc(cnt3(s->dw), 1);
+    s->csdf = (double*)xcalloc(cnt3(s->n), sizeof(double));
     return s;
 }
 
@@ -332,6 +349,10 @@ void or_destroy(or_sim* s)
     free(s->sdf); free(s->marks); free(s->p); free(s->b);
     free(s->dmu); free(s->dmv); free(s->dmw);
     for (int f = 0; f < s->nforces; ++f) free(s->forces[f].field);
+    for (int c = 0; c < s->ncolliders; ++c) {
+        free(s->colliders[c].sdf); free(s->colliders[c].V); free(s->colliders[c].T); free(s->colliders[c].N);
+    }
+    free(s->csdf);
     free(s);
 }
 
@@ -514,6 +535,9 @@ static inline size_t hash_key(int bx, int by, int bz)
 /* PICSimulator::BuildSignedDistanceField (pic_simulator.cpp:452-475) with HashGridParticleSearcher::Build and
  * ForEachNearbyPoint (hash_grid_particle_searcher.cpp:14-32, 97-126, 154-204).  ExtrapolateIntoCollider
  * (pic_simulator.cpp:497-519) is the identity with no colliders: every node is valid. */
+static void extrapolate_into_collider(or_sim* s);
+static double collider_sample(const or_sim* s, const double pos[3]);
+
 void or_stage_sdf(or_sim* s)
 {
     double maxH = s->h[0] > (s->h[1] > s->h[2] ? s->h[1] : s->h[2]) ? s->h[0] : (s->h[1] > s->h[2] ? s->h[1] : s->h[2]);
@@ -565,10 +589,11 @@ void or_stage_sdf(or_sim* s)
                 s->sdf[ix3(s->n, i, j, k)] = minDistance - radious;
             }
     free(start); free(list); free(key); free(fill);
+    if (s->ncolliders > 0) extrapolate_into_collider(s);
 }
 
-/* SinglePhasePressureSolver::BuildMarkers (fluid_solvers/single_phase_pressure_solver.cpp:30-48).  The collider
- * SDF is positive everywhere, so the BOUNDRY branch is never taken. */
+/* SinglePhasePressureSolver::BuildMarkers (fluid_solvers/single_phase_pressure_solver.cpp:30-48).  Without
+ * colliders the collider SDF is positive everywhere, so the BOUNDRY branch is never taken. */
 void or_build_markers(or_sim* s)
 {
     for (int i = 0; i < s->n.x; ++i)
@@ -579,7 +604,8 @@ void or_build_markers(or_sim* s)
                                (s->d.origin[1] + 0.5 * s->h[1]) + s->h[1] * j,
                                (s->d.origin[2] + 0.5 * s->h[2]) + s->h[2] * k};
                 double v = sample3(s->sdf, s->n, s->sdf_origin, s->h, c);
-                s->marks[ix3(s->n, i, j, k)] = v < 0 ? OR_FLUID : OR_AIR;
+                s->marks[ix3(s->n, i, j, k)] =
+                    v < 0 ? OR_FLUID : ((s->ncolliders > 0 && collider_sample(s, c) < 0) ? OR_BOUNDRY : OR_AIR);
             }
 }
 
@@ -600,10 +626,16 @@ void or_stage_extrapolate(or_sim* s)
     free(prev);
 }
 
+static void constrain_with_colliders(or_sim* s);
+
 /* BlockedBoundryConditionSolver::ConstrainVelocity (fluid_solvers/blocked_boundry_condition_solver.cpp:18-291).
  * Without colliders only the wall-layer zeroing (:198-244) changes the grid. */
 void or_stage_bc(or_sim* s)
 {
+    if (s->ncolliders > 0) {
+        constrain_with_colliders(s);
+        return;
+    }
     for (int k = 0; k < s->du.z; ++k)
         for (int j = 0; j < s->du.y; ++j) {
             s->u[ix3(s->du, 0, j, k)] = 0;
@@ -1038,8 +1070,12 @@ void or_stage_g2p(or_sim* s)
     }
 }
 
-/* PICSimulator::MoveParticles (pic_simulator.cpp:239-312).  The collider response never fires: the
- * collider SDF is positive everywhere. */
+static void resolve_collision(const or_collider* c, const double prev[3], double* pos, double* vel);
+
+/* PICSimulator::MoveParticles (pic_simulator.cpp:239-312).  Without colliders the collider response never fires
+ * (the collider SDF is positive everywhere).  With colliders, a particle that ends inside the collider SDF makes
+ * every collider c resolve particle number c (the loop variable of :300-302 shadows the particle index), from this
+ * particle's start position. */
 void or_stage_move(or_sim* s, double dt)
 {
     unsigned nsub = (unsigned)(s->d.max_cfl > 1.0 ? s->d.max_cfl : 1.0);
@@ -1050,6 +1086,7 @@ void or_stage_move(or_sim* s, double dt)
         double* x = s->pos + 3 * pi;
         double* vel = s->vel + 3 * pi;
         double pt0[3] = {x[0], x[1], x[2]}, pt1[3] = {x[0], x[1], x[2]};
+        const double pt0s[3] = {x[0], x[1], x[2]}; /* startParticlePosition */
         for (unsigned t = 0; t < nsub; ++t) {
             double v0[3], mid[3], mv[3];
             sample_velocity(s, s->u, s->v, s->w, s->xo, s->yo, s->zo, pt0, v0);
@@ -1063,6 +1100,11 @@ void or_stage_move(or_sim* s, double dt)
             if (pt1[a] >= O[a] + S[a]) { pt1[a] = O[a] + S[a]; vel[a] = 0.0; }
         }
         x[0] = pt1[0]; x[1] = pt1[1]; x[2] = pt1[2];
+        if (s->ncolliders > 0 && collider_sample(s, x) < 0) {
+            const double start[3] = {pt0s[0], pt0s[1], pt0s[2]};
+            for (int c = 0; c < s->ncolliders; ++c)
+                if ((size_t)c < s->np) resolve_collision(&s->colliders[c], start, s->pos + 3 * c, s->vel + 3 * c);
+        }
     }
 }
 
@@ -1079,6 +1121,7 @@ void or_stage_advection(or_sim* s, double dt)
  * No emitters; BuildCollider leaves the collider SDF at its constant; viscosity 0 skips diffusion. */
 void or_substep(or_sim* s, double dt)
 {
+    or_build_collider(s);
     or_stage_p2g(s);
     or_stage_sdf(s);
     or_stage_extrapolate(s);
@@ -1787,4 +1830,269 @@ int or_add_volume_field(or_sim* s, const double* V, const int64_t* T, size_t nt,
     f->field = (double*)xcalloc(3 * (size_t)n[0] * n[1] * n[2], sizeof(double));
     or_volume_field_vectors(V, T, nt, f->n, f->o, f->h, f->field);
     return 0;
+}
+
+/* ---------------------------------------------------------------- colliders */
+
+/* ScalarGrid3D::Sample of the collider SDF (ColliderCollection::_sdf: the n nodes at the velocity grid's origin,
+ * the domain origin, spacing h; pic_simulator.cpp:24). */
+static double collider_sample(const or_sim* s, const double pos[3])
+{
+    return sample3(s->csdf, s->n, s->d.origin, s->h, pos);
+}
+
+/* TriangleMeshCollider(gridSize, gridOrigin, gridSpacing, mesh) (3d/triangle_mesh_collider.cpp:4-8): Mesh2SDF of
+ * the mesh on the collider's own node grid.  N holds the mesh normals (3 doubles each), indexed by the triangles'
+ * normal ids as ResolveCollision reads them.  Returns 0 on success. */
+int or_add_mesh_collider(or_sim* s, const double* V, size_t nv, const int64_t* T, size_t nt, const double* N,
+                         size_t nn, const int n[3], const double origin[3], const double h[3])
+{
+    if (s->ncolliders >= OR_MAX_COLLIDERS || n[0] < 1 || n[1] < 1 || n[2] < 1) return -1;
+    for (size_t t = 0; t < nt; ++t)
+        if (T[4 * t + 3] < 0 || (size_t)T[4 * t + 3] >= nn) return -1;
+    or_collider* c = &s->colliders[s->ncolliders++];
+    memset(c, 0, sizeof(*c));
+    for (int a = 0; a < 3; ++a) {
+        c->n[a] = n[a];
+        c->o[a] = origin[a];
+        c->h[a] = h[a];
+    }
+    c->sdf = (double*)xcalloc((size_t)n[0] * n[1] * n[2], sizeof(double));
+    or_mesh_to_sdf(V, nv, T, nt, n, origin, h, c->sdf);
+    c->V = (double*)xcalloc(3 * nv, sizeof(double));
+    c->T = (int64_t*)xcalloc(4 * nt, sizeof(int64_t));
+    c->N = (double*)xcalloc(3 * nn, sizeof(double));
+    if (nv) memcpy(c->V, V, 3 * nv * sizeof(double));
+    if (nt) memcpy(c->T, T, 4 * nt * sizeof(int64_t));
+    if (nn) memcpy(c->N, N, 3 * nn * sizeof(double));
+    c->nv = nv;
+    c->nt = nt;
+    c->nn = nn;
+    return 0;
+}
+
+/* BoundryConditionSolver::BuildCollider -> ColliderCollection::BuildSdf (3d/collider_collection.cpp:33-50): every
+ * node takes the smallest GetClosestDistanceAt (TriangleMeshCollider: its SDF sampled at the node) over the
+ * colliders, from 1.7976931348623157e30. */
+void or_build_collider(or_sim* s)
+{
+    for (int k = 0; k < s->n.z; ++k)
+        for (int j = 0; j < s->n.y; ++j)
+            for (int i = 0; i < s->n.x; ++i) {
+                const double p[3] = {s->d.origin[0] + i * s->h[0], s->d.origin[1] + j * s->h[1],
+                                     s->d.origin[2] + k * s->h[2]};
+                double m = OR_MAX_DISTANCE;
+                for (int c = 0; c < s->ncolliders; ++c) {
+                    const or_collider* cl = &s->colliders[c];
+                    const dim3i d = {cl->n[0], cl->n[1], cl->n[2]};
+                    const double v = sample3(cl->sdf, d, cl->o, cl->h, p);
+                    if (v < m) m = v;
+                }
+                s->csdf[ix3(s->n, i, j, k)] = m;
+            }
+}
+
+void or_get_collider_sdf(const or_sim* s, double* out) { memcpy(out, s->csdf, cnt3(s->n) * sizeof(double)); }
+
+/* PICSimulator::ExtrapolateIntoCollider (pic_simulator.cpp:497-519): fluid SDF nodes where the collider SDF
+ * (sampled at the node) is < 0 take ceil(maxCfl) rounds of ExtrapolateToRegion. */
+static void extrapolate_into_collider(or_sim* s)
+{
+    const size_t nc = cnt3(s->n);
+    uint8_t* valid = (uint8_t*)xcalloc(nc, 1);
+    double* prev = (double*)xcalloc(nc, sizeof(double));
+    for (int i = 0; i < s->n.x; ++i)
+        for (int j = 0; j < s->n.y; ++j)
+            for (int k = 0; k < s->n.z; ++k) {
+                const double p[3] = {s->sdf_origin[0] + i * s->h[0], s->sdf_origin[1] + j * s->h[1],
+                                     s->sdf_origin[2] + k * s->h[2]};
+                valid[ix3(s->n, i, j, k)] = collider_sample(s, p) < 0 ? 0 : 1;
+            }
+    memcpy(prev, s->sdf, nc * sizeof(double));
+    extrapolate_to_region(prev, valid, s->n, (size_t)ceil(s->d.max_cfl), s->sdf);
+    free(valid);
+    free(prev);
+}
+
+/* BlockedBoundryConditionSolver::FractionInsideSdf (fluid_solvers/blocked_boundry_condition_solver.cpp:304-322). */
+static double fraction_inside(double phi0, double phi1)
+{
+    if (phi0 < 0.0 && phi1 < 0.0) return 1;
+    if (phi0 < 0.0 && !(phi1 < 0.0)) return phi0 / (phi0 - phi1);
+    if (!(phi0 < 0.0) && phi1 < 0.0) return phi1 / (phi1 - phi0);
+    return 0;
+}
+
+/* ScalarGrid3D::Gradient (3d/scalar_grid3d.cpp:67-90) of the collider SDF: the interpolation weights of the eight
+ * surrounding nodes times their clamped central differences. */
+static void collider_gradient(const or_sim* s, const double pos[3], double g[3])
+{
+    idx8 id;
+    double w[8];
+    coords_weights(s->n, s->d.origin, s->h, pos, &id, w);
+    g[0] = g[1] = g[2] = 0.0;
+    for (int t = 0; t < 8; ++t) {
+        const int i = id.i[t], j = id.j[t], k = id.k[t];
+        const double left = s->csdf[ix3(s->n, i > 0 ? i - 1 : i, j, k)];
+        const double right = s->csdf[ix3(s->n, i + 1 < s->n.x ? i + 1 : i, j, k)];
+        const double down = s->csdf[ix3(s->n, i, j > 0 ? j - 1 : j, k)];
+        const double up = s->csdf[ix3(s->n, i, j + 1 < s->n.y ? j + 1 : j, k)];
+        const double back = s->csdf[ix3(s->n, i, j, k > 0 ? k - 1 : k)];
+        const double front = s->csdf[ix3(s->n, i, j, k + 1 < s->n.z ? k + 1 : k)];
+        const double wt = w[t] * 0.5;
+        g[0] += (wt * (right - left)) / s->h[0];
+        g[1] += (wt * (up - down)) / s->h[1];
+        g[2] += (wt * (front - back)) / s->h[2];
+    }
+}
+
+/* ConstrainVelocity with colliders (fluid_solvers/blocked_boundry_condition_solver.cpp:18-291): faces whose
+ * half-cell segment lies inside the collider SDF (FractionInsideSdf of the samples h/2 either side, 1 - clamped
+ * fraction not > 0) are zeroed and refilled by ceil(maxCfl) rounds of ExtrapolateToRegion; faces inside the
+ * collider then take the tangential part of the sampled velocity (ApplyFriction with coefficient 0: v - n (v . n),
+ * n the normalised SDF gradient; 0 where the gradient vanishes); the wall layers are zeroed; and faces between a
+ * cell whose collider-SDF node is < 0 and one whose node is not are zeroed. */
+static void constrain_with_colliders(or_sim* s)
+{
+    double* arr[3] = {s->u, s->v, s->w};
+    const dim3i dims[3] = {s->du, s->dv, s->dw};
+    const double* org[3] = {s->xo, s->yo, s->zo};
+    const size_t depth = (size_t)ceil(s->d.max_cfl);
+    uint8_t* mk[3];
+    double* tmp[3];
+    for (int c = 0; c < 3; ++c) {
+        const size_t nf = cnt3(dims[c]);
+        mk[c] = (uint8_t*)xcalloc(nf, 1);
+        tmp[c] = (double*)xcalloc(nf, sizeof(double));
+        for (int k = 0; k < dims[c].z; ++k)
+            for (int j = 0; j < dims[c].y; ++j)
+                for (int i = 0; i < dims[c].x; ++i) {
+                    const double p[3] = {org[c][0] + s->h[0] * (double)i, org[c][1] + s->h[1] * (double)j,
+                                         org[c][2] + s->h[2] * (double)k};
+                    double p0[3] = {p[0], p[1], p[2]}, p1[3] = {p[0], p[1], p[2]};
+                    const double off[3] = {c == 0 ? 0.5 * s->h[0] : 0.0, c == 1 ? 0.5 * s->h[1] : 0.0,
+                                           c == 2 ? 0.5 * s->h[2] : 0.0};
+                    for (int a = 0; a < 3; ++a) {
+                        p0[a] = p[a] - off[a];
+                        p1[a] = p[a] + off[a];
+                    }
+                    double frac = fraction_inside(collider_sample(s, p0), collider_sample(s, p1));
+                    frac = 1 - clampd(frac, 1.0, 0.0);
+                    const size_t f = ix3(dims[c], i, j, k);
+                    if (frac > 0.0) {
+                        mk[c][f] = 1;
+                    } else {
+                        arr[c][f] = 0.0;
+                        mk[c][f] = 0;
+                    }
+                }
+    }
+    for (int c = 0; c < 3; ++c) {
+        const size_t nf = cnt3(dims[c]);
+        double* prev = (double*)xcalloc(nf, sizeof(double));
+        memcpy(prev, arr[c], nf * sizeof(double));
+        extrapolate_to_region(prev, mk[c], dims[c], depth, arr[c]);
+        free(prev);
+    }
+    for (int c = 0; c < 3; ++c)
+        for (int k = 0; k < dims[c].z; ++k)
+            for (int j = 0; j < dims[c].y; ++j)
+                for (int i = 0; i < dims[c].x; ++i) {
+                    const double p[3] = {org[c][0] + s->h[0] * (double)i, org[c][1] + s->h[1] * (double)j,
+                                         org[c][2] + s->h[2] * (double)k};
+                    const size_t f = ix3(dims[c], i, j, k);
+                    if (collider_sample(s, p) < 0) {
+                        double vel[3], g[3];
+                        sample_velocity(s, s->u, s->v, s->w, s->xo, s->yo, s->zo, p, vel);
+                        collider_gradient(s, p, g);
+                        const double gl = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+                        if (gl * gl > 0.0) {
+                            const double gv = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+                            const double nrm[3] = {g[0] / gv, g[1] / gv, g[2] / gv};
+                            const double vr[3] = {vel[0] - 0.0, vel[1] - 0.0, vel[2] - 0.0};
+                            const double d = vr[0] * nrm[0] + vr[1] * nrm[1] + vr[2] * nrm[2];
+                            tmp[c][f] = (vr[c] - nrm[c] * d) + 0.0;
+                        } else {
+                            tmp[c][f] = 0.0;
+                        }
+                    } else {
+                        tmp[c][f] = arr[c][f];
+                    }
+                }
+    for (int c = 0; c < 3; ++c) {
+        memcpy(arr[c], tmp[c], cnt3(dims[c]) * sizeof(double));
+        free(tmp[c]);
+        free(mk[c]);
+    }
+    /* the wall layers (:198-244) */
+    for (int k = 0; k < s->du.z; ++k)
+        for (int j = 0; j < s->du.y; ++j) {
+            s->u[ix3(s->du, 0, j, k)] = 0;
+            s->u[ix3(s->du, s->du.x - 1, j, k)] = 0;
+        }
+    for (int k = 0; k < s->dv.z; ++k)
+        for (int i = 0; i < s->dv.x; ++i) {
+            s->v[ix3(s->dv, i, 0, k)] = 0;
+            s->v[ix3(s->dv, i, s->dv.y - 1, k)] = 0;
+        }
+    for (int j = 0; j < s->dw.y; ++j)
+        for (int i = 0; i < s->dw.x; ++i) {
+            s->w[ix3(s->dw, i, j, 0)] = 0;
+            s->w[ix3(s->dw, i, j, s->dw.z - 1)] = 0;
+        }
+    /* faces between BOUNDRY and FLUID cells of the node-value markers (:246-290) */
+    const dim3i n = s->n;
+    for (int k = 0; k < n.z; ++k)
+        for (int j = 0; j < n.y; ++j)
+            for (int i = 0; i < n.x; ++i) {
+#define CB(a, b, c) (s->csdf[ix3(n, (a), (b), (c))] < 0)
+                if (!CB(i, j, k)) continue;
+                if (i > 0 && !CB(i - 1, j, k)) s->u[ix3(s->du, i, j, k)] = 0;
+                if (i < n.x - 1 && !CB(i + 1, j, k)) s->u[ix3(s->du, i + 1, j, k)] = 0;
+                if (j > 0 && !CB(i, j - 1, k)) s->v[ix3(s->dv, i, j, k)] = 0;
+                if (j < n.y - 1 && !CB(i, j + 1, k)) s->v[ix3(s->dv, i, j + 1, k)] = 0;
+                if (k > 0 && !CB(i, j, k - 1)) s->w[ix3(s->dw, i, j, k)] = 0;
+                if (k < n.z - 1 && !CB(i, j, k + 1)) s->w[ix3(s->dw, i, j, k + 1)] = 0;
+#undef CB
+            }
+}
+
+/* TriangleMeshCollider::ResolveCollision (3d/triangle_mesh_collider.cpp:65-100) with radius and restitution 0 and
+ * friction 0: the closest point on the first nearest triangle to `prev` (Collisions::ClosestTriangleIdx,
+ * ClossestPointOnTriangle) becomes the position; when the position was inside the mesh
+ * (TriangleMesh::IsInside), the velocity's normal part toward the triangle's normal is scaled by -0. */
+static void resolve_collision(const or_collider* c, const double prev[3], double* pos, double* vel)
+{
+    double best = OR_MAX_DISTANCE;
+    size_t idx = 0;
+    for (size_t t = 0; t < c->nt; ++t) {
+        const double d = or_distance_to_triangle(prev, c->V + 3 * c->T[4 * t], c->V + 3 * c->T[4 * t + 1],
+                                                 c->V + 3 * c->T[4 * t + 2]);
+        if (d < best) {
+            best = d;
+            idx = t;
+        }
+    }
+    double cp[3];
+    closest_on_triangle(prev, c->V + 3 * c->T[4 * idx], c->V + 3 * c->T[4 * idx + 1], c->V + 3 * c->T[4 * idx + 2], cp);
+    const double* nrm = c->N + 3 * c->T[4 * idx + 3];
+    if (or_mesh_is_inside(c->V, c->T, c->nt, pos)) {
+        const double rv[3] = {vel[0] - 0.0, vel[1] - 0.0, vel[2] - 0.0};
+        const double nd = nrm[0] * rv[0] + nrm[1] * rv[1] + nrm[2] * rv[2];
+        double rn[3] = {nd * nrm[0], nd * nrm[1], nd * nrm[2]};
+        double rt[3] = {rv[0] - rn[0], rv[1] - rn[1], rv[2] - rn[2]};
+        if (nd < 0.0) {
+            const double drn[3] = {(-0.0 - 1.0) * rn[0], (-0.0 - 1.0) * rn[1], (-0.0 - 1.0) * rn[2]};
+            for (int a = 0; a < 3; ++a) rn[a] *= -0.0;
+            if (rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] > 0.0) {
+                const double lt = sqrt(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2]);
+                const double ln = sqrt(drn[0] * drn[0] + drn[1] * drn[1] + drn[2] * drn[2]);
+                const double q = 1.0 - 0.0 * ln / lt;
+                const double fs = (q < 0.0) ? 0.0 : q; /* std::max(q, 0.0) */
+                for (int a = 0; a < 3; ++a) rt[a] *= fs;
+            }
+        }
+        for (int a = 0; a < 3; ++a) vel[a] = (rn[a] + rt[a]) + 0.0;
+    }
+    for (int a = 0; a < 3; ++a) pos[a] = cp[a];
 }

@@ -83,6 +83,16 @@ int or_add_point_field(or_sim* s, const double origin[3], double strength);
 int or_add_swirl_field(or_sim* s, const double origin[3], const double axis[3], double strength);
 int or_add_volume_field(or_sim* s, const double* V, const int64_t* T, size_t nt, const int n[3],
                         const double domain_origin[3], const double domain_size[3], double strength);
+/* Colliders (at most 8): TriangleMeshCollider(gridSize, gridOrigin, gridSpacing, mesh) (3d/triangle_mesh_collider.cpp)
+ * with its mesh normals N (3 doubles each; triangle t's normal id is T[4t + 3]); 0 on success.  With colliders the
+ * stages run the reference's collider branches: BuildCollider (or_build_collider, first in or_substep),
+ * ExtrapolateIntoCollider (in or_stage_sdf), BOUNDRY markers, ConstrainVelocity's blocking, extrapolation and
+ * friction projection (or_stage_bc), and ResolveCollision in MoveParticles. */
+int or_add_mesh_collider(or_sim* s, const double* V, size_t nv, const int64_t* T, size_t nt, const double* N,
+                         size_t nn, const int n[3], const double origin[3], const double h[3]);
+void or_build_collider(or_sim* s);                  /* ColliderCollection::BuildSdf */
+void or_get_collider_sdf(const or_sim* s, double* out); /* the collider SDF on the n nodes at the domain origin */
+
 /* VolumeField::Initialize's closest-point vectors on a node grid (3 doubles per node, x-fastest). */
 void or_volume_field_vectors(const double* V, const int64_t* T, size_t nt, const int n[3], const double o[3],
                              const double h[3], double* out);

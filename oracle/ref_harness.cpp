@@ -32,6 +32,7 @@
 #include "forces/point_field.hpp"
 #include "forces/swirl_field.hpp"
 #include "forces/volume_field.hpp"
+#include "3d/triangle_mesh_collider.hpp"
 #undef private
 #undef protected
 
@@ -352,6 +353,28 @@ void ref_add_volume_field(void* p, const double* v, size_t nv, const int64_t* t,
     quiet(h, true);
     h->sim->AddExternalForce(std::make_shared<VolumeField>(mesh, Vector3<size_t>(n[0], n[1], n[2]), domain, strength));
     quiet(h, false);
+}
+
+// PICSimulator::AddCollider (pic_simulator.cpp:66-69) of a TriangleMeshCollider on its own node grid; the mesh
+// carries normals n (3 doubles each), indexed by the triangles' normal ids.
+void ref_add_mesh_collider(void* p, const double* v, size_t nv, const int64_t* t, size_t nt, const double* nrm,
+                           size_t nn, const int* n, const double* origin, const double* h)
+{
+    Handle* hd = (Handle*)p;
+    TriangleMesh mesh = make_mesh(v, nv, t, nt);
+    for (size_t i = 0; i < nn; ++i) mesh.AddNormal(Vector3<double>(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]));
+    quiet(hd, true);
+    hd->sim->AddCollider(std::make_shared<TriangleMeshCollider>(Vector3<size_t>(n[0], n[1], n[2]),
+                                                                Vector3<double>(origin[0], origin[1], origin[2]),
+                                                                Vector3<double>(h[0], h[1], h[2]), mesh));
+    quiet(hd, false);
+}
+
+void ref_get_collider_sdf(void* p, double* out)
+{
+    Handle* hd = (Handle*)p;
+    const ScalarGrid3D& g = hd->sim->_boundryConditionSolver->GetColliderSdf();
+    each3(g, [&](size_t i, size_t j, size_t k, size_t c) { out[c] = g(i, j, k); });
 }
 
 void ref_stage_diffusion(void* p, double dt) { Handle* h = (Handle*)p; quiet(h, true); h->sim->ComputeDiffusion(dt); quiet(h, false); }

@@ -48,3 +48,14 @@ def write_obj(path, V, T, name="mesh"):
     lines += [f"f {a + 1}//1 {b + 1}//1 {c + 1}//1" for a, b, c, *_ in T]
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
+
+
+def with_face_normals(V, T):
+    """(V, T, N): each triangle's normal id set to its own index into N, the unit face normals (b - a) x (c - a)."""
+    V = np.asarray(V, float)
+    T = np.array(T, dtype=np.int64)
+    a, b, c = V[T[:, 0]], V[T[:, 1]], V[T[:, 2]]
+    N = np.cross(b - a, c - a)
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    T[:, 3] = np.arange(T.shape[0])
+    return V, T, N
