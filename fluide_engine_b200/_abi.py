@@ -32,7 +32,7 @@ EXPORTS = [
     "fe_scene_get_diffusion", "fe_scene_build_surface", "fe_scene_get_surface", "fe_scene_write_surface_obj",
     "fe_write_obj", "fe_mesh_to_sdf", "fe_scene_init_from_mesh", "fe_scene_add_volume_emitter", "fe_scene_clear_emitters",
     "fe_scene_set_emitter_sdf", "fe_scene_set_fluid_sdf", "fe_scene_add_force", "fe_scene_clear_forces",
-    "fe_volume_field_vectors",
+    "fe_volume_field_vectors", "fe_scene_add_mesh_collider", "fe_scene_clear_colliders", "fe_scene_get_collider_sdf",
     "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
@@ -134,6 +134,10 @@ def lib():
     L.fe_scene_set_fluid_sdf.argtypes = [P, P]
     L.fe_scene_add_force.argtypes = [P, ctypes.POINTER(ForceDesc), ctypes.POINTER(ctypes.c_int32)]
     L.fe_scene_clear_forces.argtypes = [P]
+    L.fe_scene_add_mesh_collider.argtypes = [P, P, ctypes.c_uint64, P, ctypes.c_uint64, P, ctypes.c_uint64, P, P, P,
+                                             ctypes.POINTER(ctypes.c_int32)]
+    L.fe_scene_clear_colliders.argtypes = [P]
+    L.fe_scene_get_collider_sdf.argtypes = [P, P]
     L.fe_volume_field_vectors.argtypes = [P, ctypes.c_uint64, P, ctypes.c_uint64, P, P, P, P, ctypes.c_int32]
     L.fe_scene_get_sort.argtypes = [P, P, P, ctypes.c_uint64]
     L.fe_scene_divergence.argtypes = [P, D]

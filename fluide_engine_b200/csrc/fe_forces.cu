@@ -120,7 +120,7 @@ __device__ __forceinline__ void volume_sample(const ForceDev& f, const double p[
 __global__ void __launch_bounds__(kTileX * kTileY) k_forces(float* __restrict__ u, float* __restrict__ v,
                                                             float* __restrict__ w, int nx, int ny, int nz,
                                                             const ForceList fl, double hx, double hy, double hz,
-                                                            double dt)
+                                                            double dt, bool zero_walls)
 {
     FaceCoord fc;
     if (!face_coord(nx, ny, nz, fc)) return;
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_forces(float* __restrict__ 
     float* arr = c == 0 ? u : (c == 1 ? v : w);
     const bool wall = (c == 0 && (fc.i == 0 || fc.i == fc.sx - 1)) || (c == 1 && (fc.j == 0 || fc.j == fc.sy - 1)) ||
                       (c == 2 && (fc.k == 0 || fc.k == fc.sz - 1));
-    if (wall) {  // ApplyBoundryCondition re-zeroes the normal component on the six wall layers
+    if (wall && zero_walls) {  // ApplyBoundryCondition re-zeroes the normal component on the six wall layers
         arr[fc.f] = 0.f;
         return;
     }
@@ -152,11 +152,11 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_forces(float* __restrict__ 
 }  // namespace
 
 cudaError_t launch_forces(const SceneView& v, const ForceList& fl, float* u, float* vv, float* ww, double dt,
-                          cudaStream_t st)
+                          cudaStream_t st, bool zero_walls)
 {
     if (fl.count <= 0) return cudaSuccess;
     k_forces<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(u, vv, ww, v.g.nx, v.g.ny, v.g.nz, fl,
-                                                                               v.h[0], v.h[1], v.h[2], dt);
+                                                                               v.h[0], v.h[1], v.h[2], dt, zero_walls);
     count_launch();
     return cudaGetLastError();
 }

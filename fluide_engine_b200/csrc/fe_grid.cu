@@ -12,8 +12,8 @@
 //              (fluid_solvers/blocked_boundry_condition_solver.cpp:198-244).
 //   K_rhs      b = div u on FLUID cells (DivergenceAtCallCenter, grid_systems/face_centered_grid3d.cpp:
 //              157-166, evaluated in FP64 from the FP32 faces), 0 elsewhere.
-//   K_apply    u_{i+1} += (p_{i+1} - p_i) / h for FLUID cells i toward +x/+y/+z only
-//              (fluid_solvers/single_phase_pressure_solver.cpp:56-92); wall faces are never touched.
+//   K_apply    u_{i+1} += (p_{i+1} - p_i) / h for FLUID cells i toward +x/+y/+z only, except toward BOUNDRY
+//              cells (fluid_solvers/single_phase_pressure_solver.cpp:56-92); wall faces are never touched.
 //   K_cfl      max over cells of |u_cc| + dt*(0,-9.8,0) component-wise (pic_simulator.cpp:80-97).
 #include "fe_internal.cuh"
 
@@ -106,17 +106,17 @@ __global__ void k_apply(SceneView v, float* u, float* vv, float* w)
     if (fc.c == 0) {
         if (i < 1 || i > nx - 1) return;
         const size_t cm = idx3(i - 1, j, k, nx, ny);
-        if (v.marks[cm] != FE_CELL_FLUID) return;
+        if (v.marks[cm] != FE_CELL_FLUID || v.marks[cm + 1] == FE_CELL_BOUNDRY) return;
         u[fc.f] = (float)((double)u[fc.f] + v.inv_h[0] * (p[cm + 1] - p[cm]));
     } else if (fc.c == 1) {
         if (j < 1 || j > ny - 1) return;
         const size_t cm = idx3(i, j - 1, k, nx, ny);
-        if (v.marks[cm] != FE_CELL_FLUID) return;
+        if (v.marks[cm] != FE_CELL_FLUID || v.marks[cm + nx] == FE_CELL_BOUNDRY) return;
         vv[fc.f] = (float)((double)vv[fc.f] + v.inv_h[1] * (p[cm + nx] - p[cm]));
     } else {
         if (k < 1 || k > nz - 1) return;
         const size_t cm = idx3(i, j, k - 1, nx, ny);
-        if (v.marks[cm] != FE_CELL_FLUID) return;
+        if (v.marks[cm] != FE_CELL_FLUID || v.marks[cm + (size_t)nx * ny] == FE_CELL_BOUNDRY) return;
         w[fc.f] = (float)((double)w[fc.f] + v.inv_h[2] * (p[cm + (size_t)nx * ny] - p[cm]));
     }
 }
@@ -212,6 +212,44 @@ cudaError_t run_extrap_group(const SceneView& v, float* const src[3], float* con
     }
     return cudaGetLastError();
 }
+
+}  // namespace
+
+// `depth` plain passes of ExtrapolateToRegion (no wall tail) from `src` with the read-only validity `valid0`, the
+// last pass writing `dst_final` (which must differ from src); intermediate results alternate between `other` and
+// src, the validity between the two face-sized halves of `vscratch`.
+cudaError_t launch_extrap_faces(const SceneView& v, float* const src[3], float* const dst_final[3],
+                                float* const other[3], const uint8_t* const valid0[3], uint8_t* vscratch, int depth,
+                                cudaStream_t st)
+{
+    const size_t total = faces_total(v);
+    const size_t nu = (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz, nvv = (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz;
+    const float* in[3] = {src[0], src[1], src[2]};
+    const uint8_t* vin[3] = {valid0[0], valid0[1], valid0[2]};
+    uint8_t* vset[2][3] = {{vscratch, vscratch + nu, vscratch + nu + nvv},
+                           {vscratch + total, vscratch + total + nu, vscratch + total + nu + nvv}};
+    for (int pass = 0; pass < depth; ++pass) {
+        const bool last = pass == depth - 1;
+        FaceArrays fa;
+        float* const* out = last ? dst_final : ((pass & 1) ? src : other);
+        for (int c = 0; c < 3; ++c) {
+            fa.in[c] = in[c];
+            fa.out[c] = out[c];
+            fa.vin[c] = vin[c];
+            fa.vout[c] = vset[pass & 1][c];
+        }
+        k_extrap<kModePlain><<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(
+            fa, v.g.nx, v.g.ny, v.g.nz, !last, 0.f, 0.f, 0.f);
+        count_launch();
+        for (int c = 0; c < 3; ++c) {
+            in[c] = out[c];
+            vin[c] = vset[pass & 1][c];
+        }
+    }
+    return cudaGetLastError();
+}
+
+namespace {
 
 __global__ void k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g, float gx, float gy,
                             float gz)

@@ -298,7 +298,7 @@ cudaError_t launch_mesh_to_sdf(const double* V, uint64_t nv, const int64_t* T, u
 cudaError_t launch_seed_count(const double* fluid_sdf, const int n[3], const double sdf_o[3], const double h[3],
                               const double vel_o[3], uint32_t ppb, uint32_t* count, cudaStream_t st);
 cudaError_t launch_emit_count(const double* emitter_sdf, const int en[3], const double* fluid_sdf, int fnx, int fny,
-                              uint32_t ppb, uint32_t* count, cudaStream_t st);
+                              uint32_t ppb, uint32_t* count, cudaStream_t st, const double* collider_sdf = nullptr);
 cudaError_t launch_spawn(const int n[3], const double o[3], const double h[3], const uint32_t* count,
                          const uint32_t* offset, uint64_t seed, const SceneView& v, uint64_t base, const float vel[3],
                          cudaStream_t st);
@@ -306,6 +306,68 @@ cudaError_t launch_spawn(const int n[3], const double o[3], const double h[3], c
 // VolumeField's closest-point vectors on a node grid (fe_mesh.cu): 3 doubles per node, x-fastest.
 cudaError_t launch_volume_vectors(const double* V, uint64_t nv, const int64_t* T, uint64_t nt, const int n[3],
                                   const double o[3], const double h[3], double* out, cudaStream_t st);
+
+// Solid colliders (fe_collide.cu).  A TriangleMeshCollider: its Mesh2SDF on its own node grid and its mesh.
+constexpr int kMaxColliders = 8;
+struct ColliderDev {
+    int n[3];
+    double o[3], h[3];
+    const double* sdf;
+    const double* V;   // 3 per vertex
+    const int64_t* T;  // 4 per triangle: vertex ids, normal id into N
+    const double* N;   // 3 per normal
+    uint64_t nv, nt;
+};
+struct CollideSet {
+    int count;
+    ColliderDev c[kMaxColliders];
+};
+enum : uint8_t { kFaceInside = 1, kFaceZero = 2 };
+// Per-scene collider buffers: the collider SDF and its fixed classification, and per-substep scratch.
+struct CollideWork {
+    double* csdf;            // n^3 nodes at the domain origin
+    uint8_t* node_valid;     // n^3: ExtrapolateIntoCollider's valid nodes
+    uint8_t* cell_boundry;   // n^3: BuildMarkers' BOUNDRY cells (when not FLUID)
+    uint8_t* face_open;      // faces (u | v | w): not blocked by the collider
+    uint8_t* face_cls;       // faces: kFaceInside / kFaceZero
+    uint8_t* vscratch;       // 2 x faces: extrapolation validity ping-pong
+    uint8_t* node_vscratch;  // 2 x n^3
+    float *ftmp0, *ftmp1;    // faces: extrapolation copies
+    float* fric;             // faces: projected velocities of the inside faces
+    double *sdf_a, *sdf_b;   // n^3: fluid SDF ping-pong
+    // collision response (sized by the particle capacity)
+    float* start;            // 3 per slot: position before the move
+    float* startv;           // 3 per slot: velocity before the move (after the grid-to-particle transfer)
+    float* spos;             // 3 per original index: start positions of the flagged particles
+    uint32_t* flag;          // cap + 1
+    uint32_t* offs;          // cap + 1
+    uint32_t* list;          // cap
+    double *cp, *nrm;        // 3 per (listed particle, collider)
+    uint8_t* ins;            // 1 per (listed particle, collider)
+    uint32_t* slot_of;       // kMaxColliders
+    void* scan_tmp;
+    size_t scan_tmp_bytes;
+};
+// The move parameters of k_g2p (MoveParticles' RK2 sub-steps and domain clamp) and its final velocity buffers.
+struct CollideMove {
+    float dt_sub;
+    int nsub;
+    float lo[3], hi[3];
+    const float *u, *v, *w;
+};
+cudaError_t launch_collider_setup(const SceneView& v, const CollideSet& cs, CollideWork& w, cudaStream_t st);
+cudaError_t launch_collider_bc(const SceneView& v, const CollideWork& w, float* const buf[3], cudaStream_t st);
+cudaError_t launch_collider_marks(const SceneView& v, const CollideWork& w, unsigned long long* node_scratch,
+                                  double** fluid_sdf, cudaStream_t st);
+cudaError_t launch_collider_keep_start(const SceneView& v, const CollideWork& w, cudaStream_t st);
+cudaError_t launch_collider_resolve(const SceneView& v, const CollideSet& cs, const CollideWork& w,
+                                    const CollideMove& g, cudaStream_t st);
+cudaError_t launch_surface_with_colliders(const double* fluid, const double* csdf, size_t n, double* out,
+                                          cudaStream_t st);
+cudaError_t launch_add_gravity(const SceneView& v, float* const buf[3], double dt, cudaStream_t st);
+cudaError_t launch_extrap_faces(const SceneView& v, float* const src[3], float* const dst_final[3],
+                                float* const other[3], const uint8_t* const valid0[3], uint8_t* vscratch, int depth,
+                                cudaStream_t st);
 
 // Position-dependent external forces (fe_forces.cu), applied after the pre-solve pass (which adds gravity).
 constexpr int kMaxForces = 8;
@@ -324,7 +386,7 @@ struct ForceList {
 };
 // u, vv, ww: the velocity buffers the pre-solve pass wrote; faces at the velocity grid's data origins.
 cudaError_t launch_forces(const SceneView& v, const ForceList& fl, float* u, float* vv, float* ww, double dt,
-                          cudaStream_t st);
+                          cudaStream_t st, bool zero_walls = true);
 
 // Viscosity (fe_diffuse.cu): ComputeDiffusion on the velocity buffers u, vv, ww (face markers, FLUID-face list,
 // persistent Jacobi solve, wall layers zeroed).  Uses the scene's solver barrier and error words (CgWork).

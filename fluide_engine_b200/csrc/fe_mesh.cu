@@ -25,112 +25,10 @@
 #include <cinttypes>
 #include <cstring>
 
-#include "fe_internal.cuh"
+#include "fe_geom.cuh"
 
 namespace fe {
 namespace {
-
-__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double dd(double a, double b) { return __ddiv_rn(a, b); }
-__device__ __forceinline__ double dot3(const double a[3], const double b[3]) { return da(da(dm(a[0], b[0]), dm(a[1], b[1])), dm(a[2], b[2])); }
-__device__ __forceinline__ double len3(const double a[3]) { return __dsqrt_rn(dot3(a, a)); }
-
-// Collisions::ClossestPointOnTriangle (3d/collisions.cpp:21-212), region by region.
-__device__ void closest_on_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3],
-                                    double out[3])
-{
-    double diff[3], e0[3], e1[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) { diff[d] = ds(p0[d], pt[d]); e0[d] = ds(p1[d], p0[d]); e1[d] = ds(p2[d], p0[d]); }
-    const double a00 = dot3(e0, e0), a01 = dot3(e0, e1), a11 = dot3(e1, e1);
-    const double b0 = dot3(diff, e0), b1 = dot3(diff, e1);
-    const double dt = ds(dm(a00, a11), dm(a01, a01));
-    const double det = dt < 0.0 ? 0.0 : dt;  // std::max(x, 0.0)
-    double s = ds(dm(a01, b1), dm(a11, b0));
-    double t = ds(dm(a01, b0), dm(a00, b1));
-    if (da(s, t) <= det) {
-        if (s < 0) {
-            if (t < 0) {  // region 4
-                if (b0 < 0) {
-                    t = 0;
-                    s = (-b0 >= a00) ? 1.0 : dd(-b0, a00);
-                } else {
-                    s = 0;
-                    t = (b1 >= 0) ? 0.0 : ((-b1 >= a11) ? 1.0 : dd(-b1, a11));
-                }
-            } else {  // region 3
-                s = 0;
-                t = (b1 >= 0) ? 0.0 : ((-b1 >= a11) ? 1.0 : dd(-b1, a11));
-            }
-        } else if (t < 0) {  // region 5
-            t = 0;
-            s = (b0 >= 0) ? 0.0 : ((-b0 >= a00) ? 1.0 : dd(-b0, a00));
-        } else {  // region 0
-            s = dd(s, det);
-            t = dd(t, det);
-        }
-    } else {
-        const double denom = da(ds(a00, dm(2.0, a01)), a11);
-        if (s < 0) {  // region 2
-            const double tmp0 = da(a01, b0), tmp1 = da(a11, b1);
-            if (tmp1 > tmp0) {
-                const double numer = ds(tmp1, tmp0);
-                if (numer >= denom) { s = 1; t = 0; }
-                else { s = dd(numer, denom); t = ds(1.0, s); }
-            } else {
-                s = 0;
-                t = (tmp1 <= 0) ? 1.0 : ((b1 >= 0) ? 0.0 : dd(-b1, a11));
-            }
-        } else if (t < 0) {  // region 6
-            const double tmp0 = da(a01, b1), tmp1 = da(a00, b0);
-            if (tmp1 > tmp0) {
-                const double numer = ds(tmp1, tmp0);
-                if (numer >= denom) { t = 1; s = 0; }
-                else { t = dd(numer, denom); s = ds(1.0, t); }
-            } else {
-                t = 0;
-                s = (tmp1 <= 0) ? 1.0 : ((b0 >= 0) ? 0.0 : dd(-b0, a00));
-            }
-        } else {  // region 1
-            const double numer = ds(ds(da(a11, b1), a01), b0);
-            if (numer <= 0) { s = 0; t = 1; }
-            else if (numer >= denom) { s = 1; t = 0; }
-            else { s = dd(numer, denom); t = ds(1.0, s); }
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) out[d] = da(da(p0[d], dm(s, e0[d])), dm(t, e1[d]));
-}
-
-// Collisions::DistanceToTriangle (3d/collisions.cpp:214-217): DistanceToPoint(point, closest point).
-__device__ double distance_to_triangle(const double pt[3], const double p0[3], const double p1[3], const double p2[3])
-{
-    double c[3];
-    closest_on_triangle(pt, p0, p1, p2, c);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) c[d] = ds(c[d], pt[d]);
-    return len3(c);
-}
-
-struct MeshView {
-    const double* V;   // 3 per vertex
-    const int64_t* T;  // 4 per triangle (three vertex ids, unused normal id)
-    uint64_t nv, nt;
-};
-
-struct NodeGrid {
-    int n[3];
-    double o[3], h[3];
-};
-
-__device__ __forceinline__ double grid_pos(const NodeGrid& g, int a, int idx) { return da(g.o[a], dm((double)idx, g.h[a])); }
-
-__device__ __forceinline__ void load_vertex(const MeshView& m, int64_t id, double out[3])
-{
-    out[0] = m.V[3 * id]; out[1] = m.V[3 * id + 1]; out[2] = m.V[3 * id + 2];
-}
 
 // One CTA per triangle (grid-stride): the nodes of its index box take the minimum distance.
 __global__ void __launch_bounds__(256) k_mesh_band(MeshView m, NodeGrid g, unsigned long long* __restrict__ bits)
@@ -170,29 +68,8 @@ __global__ void __launch_bounds__(256) k_mesh_sign(MeshView m, NodeGrid g, const
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
         const int i = (int)(c % g.n[0]), j = (int)((c / g.n[0]) % g.n[1]), k = (int)(c / ((size_t)g.n[0] * g.n[1]));
         const double pt[3] = {grid_pos(g, 0, i), grid_pos(g, 1, j), grid_pos(g, 2, k)};
-        double ret = 0.0;
-        for (uint64_t t = 0; t < m.nt; ++t) {
-            double A[3], B[3], C[3];
-            load_vertex(m, __ldg(m.T + 4 * t), A);
-            load_vertex(m, __ldg(m.T + 4 * t + 1), B);
-            load_vertex(m, __ldg(m.T + 4 * t + 2), C);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) { A[d] = ds(A[d], pt[d]); B[d] = ds(B[d], pt[d]); C[d] = ds(C[d], pt[d]); }
-            double omega = dm(dm(A[0], B[1]), C[2]);
-            omega = da(omega, dm(dm(B[0], C[1]), A[2]));
-            omega = da(omega, dm(dm(C[0], A[1]), B[2]));
-            omega = ds(omega, dm(dm(C[0], B[1]), A[2]));
-            omega = ds(omega, dm(dm(B[0], A[1]), C[2]));
-            omega = ds(omega, dm(dm(A[0], C[1]), B[2]));
-            const double na = len3(A), nb = len3(B), nc3 = len3(C);
-            double kk = dm(dm(na, nb), nc3);
-            kk = da(kk, dm(nc3, dot3(A, B)));
-            kk = da(kk, dm(na, dot3(B, C)));
-            kk = da(kk, dm(nb, dot3(C, A)));
-            ret = da(ret, atan2(omega, kk));
-        }
         const double d = __longlong_as_double((long long)bits[c]);
-        sdf[c] = fabs(ret) >= two_pi_tol ? dm(d, -1.0) : d;
+        sdf[c] = fabs(winding_sum(m, pt)) >= two_pi_tol ? dm(d, -1.0) : d;
     }
 }
 
@@ -210,34 +87,6 @@ __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t counter)
     return (double)(z >> 11) * (1.0 / 9007199254740992.0);
 }
 
-// ScalarGrid3D::Sample (3d/scalar_grid3d.cpp:33-65) of a node grid at a position, with GetBarycentric clamping.
-__device__ double sample_nodes(const double* __restrict__ f, const NodeGrid& g, const double pos[3])
-{
-    int i0[3];
-    double fr[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double x = dd(ds(pos[a], g.o[a]), g.h[a]);
-        const int hiI = g.n[a] - 1;
-        const double fl = floor(x);
-        int ii = (int)fl;
-        double ff;
-        if (hiI == 0 || ii < 0) { ii = 0; ff = 0.0; }
-        else if (ii > hiI - 1) { ii = hiI - 1; ff = 1.0; }
-        else ff = ds(x, fl);
-        i0[a] = ii;
-        fr[a] = ff;
-    }
-    const int ip = min(i0[0] + 1, g.n[0] - 1), jp = min(i0[1] + 1, g.n[1] - 1), kp = min(i0[2] + 1, g.n[2] - 1);
-    auto at = [&](int i, int j, int k) { return f[idx3(i, j, k, g.n[0], g.n[1])]; };
-    auto lerp = [](double a, double b, double t) { return da(dm(ds(1.0, t), a), dm(t, b)); };
-    const double b0 = lerp(lerp(at(i0[0], i0[1], i0[2]), at(ip, i0[1], i0[2]), fr[0]),
-                           lerp(at(i0[0], jp, i0[2]), at(ip, jp, i0[2]), fr[0]), fr[1]);
-    const double b1 = lerp(lerp(at(i0[0], i0[1], kp), at(ip, i0[1], kp), fr[0]),
-                           lerp(at(i0[0], jp, kp), at(ip, jp, kp), fr[0]), fr[1]);
-    return lerp(b0, b1, fr[2]);
-}
-
 // InitializeParticles' cell test: 1 where the velocity-grid position samples the fluid SDF below 0.
 __global__ void k_seed_count(const double* __restrict__ fluid_sdf, NodeGrid sdf_grid, NodeGrid vel_grid, uint32_t ppb,
                              uint32_t* __restrict__ count)
@@ -253,13 +102,16 @@ __global__ void k_seed_count(const double* __restrict__ fluid_sdf, NodeGrid sdf_
 
 // VolumeEmitter::Emitt's node test: emitter SDF <= 0 and the fluid SDF at the same index >= 0.
 __global__ void k_emit_count(const double* __restrict__ emitter_sdf, NodeGrid eg, const double* __restrict__ fluid_sdf,
-                             int fnx, int fny, uint32_t ppb, uint32_t* __restrict__ count)
+                             int fnx, int fny, uint32_t ppb, uint32_t* __restrict__ count,
+                             const double* __restrict__ collider_sdf)
 {
     const size_t nc = (size_t)eg.n[0] * eg.n[1] * eg.n[2];
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
         const int i = (int)(c % eg.n[0]), j = (int)((c / eg.n[0]) % eg.n[1]), k = (int)(c / ((size_t)eg.n[0] * eg.n[1]));
         const double fv = fluid_sdf ? fluid_sdf[idx3(i, j, k, fnx, fny)] : 0.0;
-        count[c] = (emitter_sdf[c] <= 0.0 && fv >= 0.0) ? ppb : 0u;
+        // colliderSdf(i, j, k) > 0: with no collider every node holds 1.7976931348623157e30
+        const bool free_node = collider_sdf ? collider_sdf[idx3(i, j, k, fnx, fny)] > 0.0 : true;
+        count[c] = (emitter_sdf[c] <= 0.0 && fv >= 0.0 && free_node) ? ppb : 0u;
     }
 }
 
@@ -381,13 +233,13 @@ cudaError_t launch_seed_count(const double* fluid_sdf, const int n[3], const dou
 }
 
 cudaError_t launch_emit_count(const double* emitter_sdf, const int en[3], const double* fluid_sdf, int fnx, int fny,
-                              uint32_t ppb, uint32_t* count, cudaStream_t st)
+                              uint32_t ppb, uint32_t* count, cudaStream_t st, const double* collider_sdf)
 {
     const double z[3] = {0, 0, 0};
     const NodeGrid eg = node_grid(en, z, z);
     const size_t nc = (size_t)en[0] * en[1] * en[2];
     k_emit_count<<<(unsigned)std::min<size_t>((nc + 255) / 256, 148 * 32), 256, 0, st>>>(emitter_sdf, eg, fluid_sdf, fnx,
-                                                                                        fny, ppb, count);
+                                                                                        fny, ppb, count, collider_sdf);
     count_launch();
     return cudaGetLastError();
 }

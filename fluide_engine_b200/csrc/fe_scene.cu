@@ -153,6 +153,13 @@ struct fe_scene {
     // position-dependent external forces (fe_forces.cu), applied after the pre-solve pass
     std::vector<std::vector<void*>> force_allocs;
     ForceList forces{};
+    // solid colliders (fe_collide.cu): the meshes and their SDFs, the collider SDF with its classification, scratch
+    CollideSet colliders{};
+    std::vector<std::vector<void*>> collider_allocs;
+    CollideWork cw{};
+    std::vector<void*> cw_grid_allocs, cw_particle_allocs;
+    uint64_t cw_cap = 0;
+    double* collider_fluid_sdf = nullptr;  // Fluid3::sdf of the last collider substep (after ExtrapolateIntoCollider)
     uint64_t epoch = 0;                // bumped when the substep's kernel sequence changes (batches re-capture)
     double* d_scalar = nullptr;        // CFL / divergence result
     float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
@@ -446,6 +453,32 @@ fe_status alloc_grid(fe_scene* s)
 
 // Allocates both particle sets and the per-particle scratch for `cap` particles; the first `keep` particles of
 // the current set are copied into set 0 (which becomes current) before the old buffers are released.
+// The collision response's buffers, sized by the particle capacity and the collider count.
+fe_status collide_particle_buffers(fe_scene* s)
+{
+    if (s->cw_cap == s->cap && s->cw.ins && s->cw.cp) return FE_OK;
+    free_list(s->cw_particle_allocs, s->stream);
+    auto& L = s->cw_particle_allocs;
+    auto& w = s->cw;
+    const uint64_t cap = std::max<uint64_t>(s->cap, 1);
+    FE_CUDA(dalloc(L, &w.start, 3 * cap, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.startv, 3 * cap, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.spos, 3 * cap, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.flag, cap + 1, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.offs, cap + 1, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.list, cap, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.cp, 3 * cap * kMaxColliders, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.nrm, 3 * cap * kMaxColliders, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.ins, cap * kMaxColliders, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.slot_of, kMaxColliders, s->device, s->stream));
+    w.scan_tmp_bytes = sort_scan_tmp_bytes((uint32_t)(cap + 1));
+    uint8_t* tmp = nullptr;
+    FE_CUDA(dalloc(L, &tmp, w.scan_tmp_bytes, s->device, s->stream));
+    w.scan_tmp = tmp;
+    s->cw_cap = s->cap;
+    return FE_OK;
+}
+
 fe_status alloc_particles(fe_scene* s, uint64_t cap, uint64_t keep = 0)
 {
     drop_graphs(s);
@@ -490,6 +523,7 @@ fe_status alloc_particles(fe_scene* s, uint64_t cap, uint64_t keep = 0)
     }
     free_list(old, s->stream);  // stream order: after the copies
     s->cap = cap;
+    if (s->colliders.count > 0) return collide_particle_buffers(s);
     return FE_OK;
 }
 
@@ -525,6 +559,22 @@ int last_step(int stage)
     return m[stage];
 }
 
+// MoveParticles' parameters as k_g2p uses them, for the collision response's replayed moves.
+CollideMove collide_move(const SceneView& v, double dt)
+{
+    CollideMove g;
+    g.nsub = v.rk_substeps;
+    g.dt_sub = (float)(dt / g.nsub);
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = (float)v.origin[a];
+        g.hi[a] = (float)(v.origin[a] + v.size[a]);
+    }
+    g.u = v.u;
+    g.v = v.v;
+    g.w = v.w;
+    return g;
+}
+
 // Enqueues internal steps [first, last] of one substep on s->stream.
 // `stream` overrides the scene's stream (a batch runs the pre-solve steps of viscous scenes on its own stream).
 fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_t stream = nullptr)
@@ -548,10 +598,25 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             s->grid_cur = 0;
             break;
         case kStepMark:
-            FE_CUDA(launch_mark(v, st));
+            if (s->colliders.count > 0) FE_CUDA(launch_collider_marks(v, s->cw, s->surf.node, &s->collider_fluid_sdf, st));
+            else FE_CUDA(launch_mark(v, st));
             break;
         case kStepPre:
             FE_CUDA(ensure_grid(s, 0, st));
+            if (s->colliders.count > 0) {
+                // ExtrapolateVelocityToAir, ConstrainVelocity, forces, ConstrainVelocity (pic_simulator.cpp:186-211)
+                float* A[3] = {v.u, v.v, v.w};
+                float* B[3] = {v.u2, v.v2, v.w2};
+                float* const* fin = (v.extrap_depth & 1) ? B : A;
+                const uint8_t* mk[3] = {v.mu, v.mv, v.mw};
+                if (v.extrap_depth > 0) FE_CUDA(launch_extrap_faces(v, A, fin, B, mk, v.mu2, v.extrap_depth, st));
+                FE_CUDA(launch_collider_bc(v, s->cw, fin, st));
+                FE_CUDA(launch_add_gravity(v, fin, dt, st));
+                if (s->forces.count > 0) FE_CUDA(launch_forces(v, s->forces, fin[0], fin[1], fin[2], dt, st, false));
+                FE_CUDA(launch_collider_bc(v, s->cw, fin, st));
+                s->grid_cur = pressure_buffer(s);
+                break;
+            }
             FE_CUDA(launch_pre(v, dt, st));
             s->grid_cur = pressure_buffer(s);
             if (s->forces.count > 0) {
@@ -572,7 +637,7 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             FE_CUDA(launch_rhs(v, st));
             break;
         case kStepCg:
-            if (s->mg.levels >= 2)
+            if (s->mg.levels >= 2 && s->colliders.count == 0)
                 FE_CUDA(launch_mgcg(v, s->cg, s->mg, s->desc.cg_rel_tol, s->desc.cg_inner_tol, s->desc.cg_max_it,
                                     s->desc.max_refine, st));
             else
@@ -582,15 +647,36 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
         case kStepApply:
             FE_CUDA(ensure_grid(s, pressure_buffer(s), st));
             FE_CUDA(launch_apply(v, st));
+            if (s->colliders.count > 0) {  // ComputePressure ends with ApplyBoundryCondition (pic_simulator.cpp:228)
+                const int pb = pressure_buffer(s);
+                float* P[3] = {pb ? v.u2 : v.u, pb ? v.v2 : v.v, pb ? v.w2 : v.w};
+                FE_CUDA(launch_collider_bc(v, s->cw, P, st));
+            }
             break;
         case kStepPost:
             FE_CUDA(ensure_grid(s, pressure_buffer(s), st));
-            FE_CUDA(launch_post(v, st));
+            if (s->colliders.count > 0) {  // ExtrapolateVelocityToAir, ConstrainVelocity (pic_simulator.cpp:233-234)
+                float* A[3] = {v.u, v.v, v.w};
+                float* B[3] = {v.u2, v.v2, v.w2};
+                const int d = v.extrap_depth;
+                const uint8_t* mk[3] = {v.mu, v.mv, v.mw};
+                if (d > 0) FE_CUDA(launch_extrap_faces(v, (d & 1) ? B : A, A, (d & 1) ? A : B, mk, v.mu2, d, st));
+                FE_CUDA(launch_collider_bc(v, s->cw, A, st));
+            } else {
+                FE_CUDA(launch_post(v, st));
+            }
             s->grid_cur = 0;
             break;
         case kStepG2p:
             FE_CUDA(ensure_grid(s, 0, st));
-            if (last >= kStepMove) {
+            if (last >= kStepMove && s->colliders.count > 0) {
+                // the collision response needs the state between the transfer and the move: no fusion
+                FE_CUDA(launch_g2p(v, dt, true, false, st));
+                FE_CUDA(launch_collider_keep_start(v, s->cw, st));
+                FE_CUDA(launch_g2p(v, dt, false, true, st));
+                FE_CUDA(launch_collider_resolve(v, s->colliders, s->cw, collide_move(v, dt), st));
+                step = kStepMove;
+            } else if (last >= kStepMove) {
                 FE_CUDA(launch_g2p(v, dt, true, true, st));
                 step = kStepMove;
             } else {
@@ -599,7 +685,9 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             break;
         case kStepMove:
             FE_CUDA(ensure_grid(s, 0, st));
+            if (s->colliders.count > 0) FE_CUDA(launch_collider_keep_start(v, s->cw, st));
             FE_CUDA(launch_g2p(v, dt, false, true, st));
+            if (s->colliders.count > 0) FE_CUDA(launch_collider_resolve(v, s->colliders, s->cw, collide_move(v, dt), st));
             break;
         default:
             return set_error(FE_ERR_BAD_ARG, "unknown step %d", step);
@@ -779,6 +867,12 @@ fe_status surface_sdf(fe_scene* s)
     fe_status st = surf_alloc(s);
     if (st != FE_OK) return st;
     if (!s->prev_valid && s->mesh_sdf) return FE_OK;
+    if (s->prev_valid && s->colliders.count > 0 && s->collider_fluid_sdf) {  // after ExtrapolateIntoCollider
+        const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+        FE_CUDA(cudaMemcpyAsync(s->surf.sdf, s->collider_fluid_sdf, nc * sizeof(double), cudaMemcpyDeviceToDevice,
+                                s->stream));
+        return FE_OK;
+    }
     const SceneView v = view_of(s, s->prev_valid ? (s->parity ^ 1) : s->parity);
     FE_CUDA(launch_node_sdf(v, s->surf.node, s->surf.sdf, s->stream));
     return FE_OK;
@@ -803,7 +897,8 @@ fe_status emit_particles(fe_scene* s)
     const SceneView& b = s->base;
     for (auto& em : s->emitters) {
         const size_t nc = (size_t)em.n[0] * em.n[1] * em.n[2];
-        FE_CUDA(launch_emit_count(em.sdf, em.n, fluid, b.g.nx, b.g.ny, em.ppb, em.count, st));
+        FE_CUDA(launch_emit_count(em.sdf, em.n, fluid, b.g.nx, b.g.ny, em.ppb, em.count, st,
+                                  s->colliders.count > 0 ? s->cw.csdf : nullptr));
         FE_CUDA(launch_exclusive_scan(em.count, (uint32_t)nc, em.offset, em.tmp, em.tmp_bytes, st));
         uint32_t total = 0;
         FE_CUDA(cudaMemcpyAsync(&total, em.offset + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -950,6 +1045,9 @@ fe_status fe_scene_destroy(fe_scene* s)
     free_list(s->surf.mesh_allocs, s->own_stream);
     for (auto& e : s->emitters) free_list(e.allocs, s->own_stream);
     for (auto& l : s->force_allocs) free_list(l, s->own_stream);
+    for (auto& l : s->collider_allocs) free_list(l, s->own_stream);
+    free_list(s->cw_grid_allocs, s->own_stream);
+    free_list(s->cw_particle_allocs, s->own_stream);
     cudaStreamDestroy(s->own_stream);  // its pending frees still run
     delete s;
     return FE_OK;
@@ -1022,6 +1120,7 @@ fe_status fe_scene_reset(fe_scene* s)
     s->prev_valid = false;
     s->mesh_sdf = false;
     s->collider_built = false;
+    s->collider_fluid_sdf = nullptr;
     for (auto& e : s->emitters) free_list(e.allocs, s->stream);
     s->emitters.clear();
     return FE_OK;
@@ -1606,6 +1705,139 @@ fe_status fe_volume_field_vectors(const double* vertices, uint64_t n_vertices, c
     return cuda_check(e, "volume field vectors");
 }
 
+fe_status fe_scene_add_mesh_collider(fe_scene* s, const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                     uint64_t n_triangles, const double* normals, uint64_t n_normals,
+                                     const int32_t resolution[3], const double grid_origin[3],
+                                     const double grid_spacing[3], int32_t* id)
+{
+    if (!s || !resolution || !grid_origin || !grid_spacing) return set_error(FE_ERR_BAD_ARG, "null argument");
+    if (n_triangles == 0 || n_vertices == 0 || !vertices || !triangles || !normals)
+        return set_error(FE_ERR_BAD_ARG, "a collider mesh needs vertices, triangles and normals");
+    for (int a = 0; a < 3; ++a)
+        if (resolution[a] < 1 || !(grid_spacing[a] > 0.0)) return set_error(FE_ERR_BAD_ARG, "bad collider grid");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->colliders.count >= kMaxColliders) return set_error(FE_ERR_BAD_ARG, "at most %d colliders", kMaxColliders);
+    if (s->desc.viscosity > 0.0)
+        return set_error(FE_ERR_BAD_ARG, "colliders with viscosity are not supported (BackwardEulerDiffusionSolver's "
+                                         "BOUNDRY faces); set the viscosity to 0 first");
+    FE_CUDA(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    // normal ids are validated on the host: ResolveCollision reads normals[triangle.normalIdx]
+    std::vector<int64_t> tri(4 * n_triangles);
+    FE_CUDA(cudaMemcpy(tri.data(), triangles, tri.size() * sizeof(int64_t), cudaMemcpyDefault));
+    for (uint64_t t = 0; t < n_triangles; ++t)
+        if (tri[4 * t + 3] < 0 || (uint64_t)tri[4 * t + 3] >= n_normals)
+            return set_error(FE_ERR_BAD_ARG, "triangle %llu has normal id %lld of %llu", (unsigned long long)t,
+                             (long long)tri[4 * t + 3], (unsigned long long)n_normals);
+    fe_status r = surf_alloc(s);  // its node scratch serves the band SDF of the collider marks
+    if (r != FE_OK) return r;
+    std::vector<void*> allocs;
+    double* dV = nullptr;
+    int64_t* dT = nullptr;
+    r = upload_mesh(vertices, n_vertices, triangles, n_triangles, s->device, st, allocs, &dV, &dT);
+    if (r != FE_OK) {
+        free_list(allocs, st);
+        return r;
+    }
+    ColliderDev c{};
+    for (int a = 0; a < 3; ++a) {
+        c.n[a] = resolution[a];
+        c.o[a] = grid_origin[a];
+        c.h[a] = grid_spacing[a];
+    }
+    const size_t cn = (size_t)c.n[0] * c.n[1] * c.n[2];
+    double *dN = nullptr, *dsdf = nullptr;
+    unsigned long long* scratch = nullptr;
+    cudaError_t e = dalloc(allocs, &dN, 3 * n_normals, s->device, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dN, normals, 3 * n_normals * sizeof(double), cudaMemcpyDefault, st);
+    if (e == cudaSuccess) e = dalloc(allocs, &dsdf, cn, s->device, st);
+    std::vector<void*> tmp_list;
+    if (e == cudaSuccess) e = dalloc(tmp_list, &scratch, cn, s->device, st);
+    // TriangleMeshCollider's constructor: Mesh2SDF of the mesh on its own grid
+    if (e == cudaSuccess) e = launch_mesh_to_sdf(dV, n_vertices, dT, n_triangles, c.n, c.o, c.h, scratch, dsdf, st);
+    free_list(tmp_list, st);
+    if (e != cudaSuccess) {
+        free_list(allocs, st);
+        return cuda_check(e, "collider");
+    }
+    c.sdf = dsdf;
+    c.V = dV;
+    c.T = dT;
+    c.N = dN;
+    c.nv = n_vertices;
+    c.nt = n_triangles;
+    // grid-sized buffers on the first collider
+    auto& w = s->cw;
+    const SceneView& b = s->base;
+    if (s->colliders.count == 0) {
+        const size_t nc = (size_t)b.g.nx * b.g.ny * b.g.nz;
+        const size_t nf = (size_t)(b.g.nx + 1) * b.g.ny * b.g.nz + (size_t)b.g.nx * (b.g.ny + 1) * b.g.nz +
+                          (size_t)b.g.nx * b.g.ny * (b.g.nz + 1);
+        auto& L = s->cw_grid_allocs;
+        FE_CUDA(dalloc(L, &w.csdf, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.node_valid, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.cell_boundry, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.face_open, nf, s->device, st));
+        FE_CUDA(dalloc(L, &w.face_cls, nf, s->device, st));
+        FE_CUDA(dalloc(L, &w.vscratch, 2 * nf, s->device, st));
+        FE_CUDA(dalloc(L, &w.node_vscratch, 2 * nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.ftmp0, nf, s->device, st));
+        FE_CUDA(dalloc(L, &w.ftmp1, nf, s->device, st));
+        FE_CUDA(dalloc(L, &w.fric, nf, s->device, st));
+        FE_CUDA(dalloc(L, &w.sdf_a, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.sdf_b, nc, s->device, st));
+    }
+    s->colliders.c[s->colliders.count] = c;
+    if (id) *id = s->colliders.count;
+    s->colliders.count += 1;
+    s->collider_allocs.push_back(std::move(allocs));
+    // ColliderCollection::BuildSdf gives the same SDF every substep (static colliders): build and classify now
+    FE_CUDA(launch_collider_setup(b, s->colliders, w, st));
+    r = collide_particle_buffers(s);
+    if (r != FE_OK) return r;
+    FE_CUDA(cudaStreamSynchronize(st));
+    s->collider_fluid_sdf = nullptr;
+    drop_graphs(s);
+    ++s->epoch;
+    return FE_OK;
+}
+
+fe_status fe_scene_clear_colliders(fe_scene* s)
+{
+    if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    if (s->colliders.count == 0) return FE_OK;
+    for (auto& l : s->collider_allocs) free_list(l, s->stream);
+    s->collider_allocs.clear();
+    free_list(s->cw_grid_allocs, s->stream);
+    free_list(s->cw_particle_allocs, s->stream);
+    s->cw = CollideWork{};
+    s->cw_cap = 0;
+    s->colliders.count = 0;
+    s->collider_fluid_sdf = nullptr;
+    drop_graphs(s);
+    ++s->epoch;
+    return FE_OK;
+}
+
+fe_status fe_scene_get_collider_sdf(fe_scene* s, double* sdf)
+{
+    if (!s || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+    if (s->colliders.count == 0 || !s->collider_built) {
+        // ColliderCollection's SDF starts at 0 and is 1.7976931348623157e30 everywhere once built without colliders
+        const std::vector<double> c(nc, s->collider_built ? 1.7976931348623157e30 : 0.0);
+        FE_CUDA(cudaMemcpy(sdf, c.data(), nc * sizeof(double), cudaMemcpyDefault));
+        return FE_OK;
+    }
+    FE_CUDA(cudaMemcpyAsync(sdf, s->cw.csdf, nc * sizeof(double), cudaMemcpyDefault, s->stream));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    return FE_OK;
+}
+
 fe_status fe_scene_set_emitter_sdf(fe_scene* s, int32_t id, const double* sdf)
 {
     if (!s || !sdf) return set_error(FE_ERR_BAD_ARG, "null argument");
@@ -1640,7 +1872,13 @@ fe_status fe_scene_build_surface(fe_scene* s, uint64_t* n_vertices, uint64_t* n_
     auto& w = s->surf;
     const SceneView& v = s->base;
     cudaStream_t stream = s->stream;
-    FE_CUDA(launch_mc_count(v, w.sdf, w.cfg, w.nvert, w.ntri, stream));
+    const double* msdf = w.sdf;
+    if (s->colliders.count > 0 && s->collider_built) {  // MarchingCubesSolver::BuildSurface's collider step
+        double* mod = reinterpret_cast<double*>(w.node);
+        FE_CUDA(launch_surface_with_colliders(w.sdf, s->cw.csdf, (size_t)v.g.nx * v.g.ny * v.g.nz, mod, stream));
+        msdf = mod;
+    }
+    FE_CUDA(launch_mc_count(v, msdf, w.cfg, w.nvert, w.ntri, stream));
     FE_CUDA(launch_exclusive_scan(w.nvert, (uint32_t)w.items, w.vbase, w.tmp, w.tmp_bytes, stream));
     FE_CUDA(launch_exclusive_scan(w.ntri, (uint32_t)w.items, w.tbase, w.tmp, w.tmp_bytes, stream));
     uint32_t tot[2] = {0, 0};
@@ -1655,7 +1893,7 @@ fe_status fe_scene_build_surface(fe_scene* s, uint64_t* n_vertices, uint64_t* n_
         FE_CUDA(dalloc(w.mesh_allocs, &w.N, 3 * w.cap_v, s->device, stream));
         FE_CUDA(dalloc(w.mesh_allocs, &w.T, 4 * w.cap_t, s->device, stream));
     }
-    FE_CUDA(launch_mc_emit(v, w.sdf, w.cfg, w.vbase, w.tbase, w.V, w.N, w.T, stream));
+    FE_CUDA(launch_mc_emit(v, msdf, w.cfg, w.vbase, w.tbase, w.V, w.N, w.T, stream));
     FE_CUDA(cudaStreamSynchronize(stream));
     w.nv = tot[0];
     w.nt = tot[1];
@@ -1702,6 +1940,9 @@ fe_status fe_scene_set_viscosity(fe_scene* s, double viscosity)
     if (!(viscosity >= 0.0) || !std::isfinite(viscosity))
         return set_error(FE_ERR_BAD_ARG, "viscosity must be finite and >= 0");
     std::lock_guard<std::mutex> lk(s->mu);
+    if (viscosity > 0.0 && s->colliders.count > 0)
+        return set_error(FE_ERR_BAD_ARG, "viscosity with colliders is not supported (BackwardEulerDiffusionSolver's "
+                                         "BOUNDRY faces); clear the colliders first");
     FE_CUDA(cudaSetDevice(s->device));
     if (viscosity > 0.0 && !s->diff_ready) {
         FE_CUDA(cudaStreamSynchronize(s->stream));
@@ -1801,7 +2042,7 @@ uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[
 
 const char* fe_last_error(void) { return g_err; }
 
-int32_t fe_abi_version(void) { return 10400; }
+int32_t fe_abi_version(void) { return 10500; }
 
 }  // extern "C"
 
@@ -1952,6 +2193,8 @@ fe_status batch_check_scenes(fe_scene* const* scenes, int32_t count)
         if (!scenes[i]->have_particles) return set_error(FE_ERR_STATE, "scene %d has no particles", i);
         if (!scenes[i]->emitters.empty())
             return set_error(FE_ERR_BAD_ARG, "scene %d has emitters (its particle count changes every substep): step it alone", i);
+        if (scenes[i]->colliders.count > 0)
+            return set_error(FE_ERR_BAD_ARG, "scene %d has colliders: step it alone", i);
         for (int j = 0; j < i; ++j)
             if (scenes[j] == scenes[i]) return set_error(FE_ERR_BAD_ARG, "scene %d appears twice", i);
     }

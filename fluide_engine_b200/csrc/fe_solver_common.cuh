@@ -249,8 +249,14 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
         }
         if (fl) {
             const int i = c % nx, j = (c / nx) % ny, k = c / sxy;
-            uint32_t m = (i > 0 ? kXm : 0u) | (i + 1 < nx ? kXp : 0u) | (j > 0 ? kYm : 0u) | (j + 1 < ny ? kYp : 0u) |
-                         (k > 0 ? kZm : 0u) | (k + 1 < nz ? kZp : 0u);
+            // in-domain neighbours that are not BOUNDRY (single_phase_pressure_solver.cpp:117-150)
+            const size_t sxy1 = (size_t)nx * ny;
+            uint32_t m = (i > 0 && marks[c - 1] != FE_CELL_BOUNDRY ? kXm : 0u) |
+                         (i + 1 < nx && marks[c + 1] != FE_CELL_BOUNDRY ? kXp : 0u) |
+                         (j > 0 && marks[c - nx] != FE_CELL_BOUNDRY ? kYm : 0u) |
+                         (j + 1 < ny && marks[c + nx] != FE_CELL_BOUNDRY ? kYp : 0u) |
+                         (k > 0 && marks[c - sxy1] != FE_CELL_BOUNDRY ? kZm : 0u) |
+                         (k + 1 < nz && marks[c + sxy1] != FE_CELL_BOUNDRY ? kZp : 0u);
             const uint32_t slot = base + off + __popc(bal & ((1u << lane) - 1u));
             list[slot] = ((uint32_t)c << 6) | m;
         }

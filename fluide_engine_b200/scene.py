@@ -208,6 +208,26 @@ class Scene:
         check(self._L.fe_scene_add_force(self._h, ctypes.byref(desc), ctypes.byref(fid)))
         return fid.value
 
+    def add_mesh_collider(self, vertices, triangles, normals, resolution, grid_origin, grid_spacing):
+        """TriangleMeshCollider on its own node grid (triangles (T, 4): vertex ids and a normal id into normals)."""
+        V = np.ascontiguousarray(vertices, dtype=np.float64)
+        T = np.ascontiguousarray(triangles, dtype=np.int64)
+        N = np.ascontiguousarray(normals, dtype=np.float64)
+        cid = ctypes.c_int32()
+        check(self._L.fe_scene_add_mesh_collider(self._h, ptr(V), V.shape[0], ptr(T), T.shape[0], ptr(N), N.shape[0],
+                                                 (ctypes.c_int32 * 3)(*resolution), (ctypes.c_double * 3)(*grid_origin),
+                                                 (ctypes.c_double * 3)(*grid_spacing), ctypes.byref(cid)))
+        return cid.value
+
+    def clear_colliders(self):
+        check(self._L.fe_scene_clear_colliders(self._h))
+
+    def collider_sdf(self):
+        nx, ny, nz = self.n
+        out = np.zeros((nz, ny, nx))
+        check(self._L.fe_scene_get_collider_sdf(self._h, ptr(out)))
+        return out
+
     def clear_forces(self):
         check(self._L.fe_scene_clear_forces(self._h))
 

@@ -258,6 +258,24 @@ fe_status fe_volume_field_vectors(const double* vertices, uint64_t n_vertices, c
                                   uint64_t n_triangles, const int32_t n[3], const double origin[3],
                                   const double spacing[3], double* out, int32_t device);
 
+/* Solid colliders: PICSimulator::AddCollider (pic_simulator.cpp:66-69) of a TriangleMeshCollider(gridSize,
+ * gridOrigin, gridSpacing, mesh) (3d/triangle_mesh_collider.cpp:4-100): the mesh's Mesh2SDF on the collider's own
+ * node grid (resolution, grid_origin, grid_spacing), and the mesh itself with normals (3 doubles each; each
+ * triangle's 4th id indexes them) for the collision response.  With colliders every substep runs the reference's
+ * collider branches: the collider SDF (ColliderCollection::BuildSdf on the scene's n nodes at the domain origin),
+ * ExtrapolateIntoCollider of the fluid SDF, BOUNDRY cells in the pressure system, BlockedBoundryConditionSolver's
+ * blocking, extrapolation and tangential projection at every ApplyBoundryCondition, and ResolveCollision in
+ * MoveParticles with the reference's indexing (a particle ending inside the collider SDF moves particle number c
+ * onto collider c's surface; pic_simulator.cpp:296-305).  At most 8; kept by fe_scene_reset.  A scene with
+ * colliders uses the plain CG pressure solver, cannot join a batch and cannot have a viscosity > 0.
+ * fe_scene_get_collider_sdf returns the collider SDF as the reference holds it (0 before the first substep). */
+fe_status fe_scene_add_mesh_collider(fe_scene* s, const double* vertices, uint64_t n_vertices, const int64_t* triangles,
+                                     uint64_t n_triangles, const double* normals, uint64_t n_normals,
+                                     const int32_t resolution[3], const double grid_origin[3],
+                                     const double grid_spacing[3], int32_t* id);
+fe_status fe_scene_clear_colliders(fe_scene* s);
+fe_status fe_scene_get_collider_sdf(fe_scene* s, double* sdf);
+
 /* Viscosity (HybridSimulator::SetViscosity, hybrid_simulator.cpp:97-100), settable at any time.  When it is > 0
  * every substep runs ComputeDiffusion (pic_simulator.cpp:214-222) after the external forces: the reference's
  * BackwardEulerDiffusionSolver (fluid_solvers/backward_euler_diffusion_solver.cpp:20-242) -- per component, faces
