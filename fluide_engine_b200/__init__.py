@@ -8,7 +8,8 @@ from ._abi import (APIC, FLIP, PIC, AIR, FLUID, AUTO, CG, MGPCG, FluideError, ke
                    STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_DIFFUSE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P,
                    STAGE_MOVE)
 from .scene import Batch, Scene, face_shapes  # noqa: F401
-from .simulators import (APICSimulator, BoundingBox3D, DirectionalField, Emitter, ExternalForce,  # noqa: F401
+from .simulators import (APICSimulator, BoundingBox3D, Collider, ColliderCollection, DirectionalField,  # noqa: F401
+                         Emitter, ExternalForce, TriangleMeshCollider,
                          FLIPSimulator, Frame, HybridSimulator, OBJManager, PICSimulator, PointField, ScalarGrid3D,
                          SimulationRunner, SimulationStats, SwirlField, TriangleMesh, Vector3D, Vector3S,
                          VolumeEmitter, VolumeField)

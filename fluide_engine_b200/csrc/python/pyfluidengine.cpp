@@ -216,6 +216,16 @@ PYBIND11_MODULE(PyFluidEngine, m)
         .def(py::init<const Vector3<size_t>&, const double&, Vector3<double>, Vector3<double>>())
         .def("GetElement", [](const ScalarGrid3D& g, size_t i, size_t j, size_t k) { return g.GetElement(i, j, k); })
         .def("SetElement", &ScalarGrid3D::SetElement);
+    // colliders_wrapper.cpp
+    py::class_<Collider, std::shared_ptr<Collider>>(m, "Collider")
+        .def("IsInside", &Collider::IsInside)
+        .def("GetClosestDistanceAt", &Collider::GetClosestDistanceAt);
+    py::class_<TriangleMeshCollider, std::shared_ptr<TriangleMeshCollider>, Collider>(m, "TriangleMeshCollider")
+        .def(py::init<const Vector3<size_t>&, const Vector3<double>&, const Vector3<double>&, const TriangleMesh&>());
+    py::class_<ColliderCollection, std::shared_ptr<ColliderCollection>>(m, "ColliderCollection")
+        .def(py::init<const Vector3<size_t>&, const Vector3<double>&, const Vector3<double>&>())
+        .def("AddCollider", &ColliderCollection::AddCollider)
+        .def("IsInside", &ColliderCollection::IsInside);
     py::class_<Emitter, std::shared_ptr<Emitter>>(m, "Emitter");
     py::class_<VolumeEmitter, std::shared_ptr<VolumeEmitter>, Emitter>(m, "VolumeEmitter")
         .def(py::init<const TriangleMesh&, Vector3<size_t>, BoundingBox3D, const size_t&, const Vector3<double>&,
@@ -232,7 +242,8 @@ PYBIND11_MODULE(PyFluidEngine, m)
         .def("AdvanceSingleFrame", &PICSimulator::AdvanceSingleFrame, py::call_guard<py::gil_scoped_release>())
         .def("InitializeFromTriangleMesh", &PICSimulator::InitializeFromTriangleMesh)
         .def("AddExternalForce", [](PICSimulator& s, std::shared_ptr<ExternalForce> f) { s.AddExternalForce(f); })
-        .def("AddCollider", [](PICSimulator& s, py::object) { s.AddCollider(nullptr); })
+        .def("AddCollider", &PICSimulator::AddCollider)
+        .def("SetColliders", &PICSimulator::SetColliders)
         .def("AddEmitter", &PICSimulator::AddEmitter)
         .def("SetCurrentFrame", &PICSimulator::SetCurrentFrame)
         .def("SetViscosity", &PICSimulator::SetViscosity)

@@ -253,6 +253,75 @@ class ScalarGrid3D:
         self.values[k, j, i] = value
 
 
+class Collider:
+    """Collider (3d/collider.hpp)."""
+
+
+class TriangleMeshCollider(Collider):
+    """TriangleMeshCollider (3d/triangle_mesh_collider.cpp:4-100) of a TriangleMesh with normals on its own node grid;
+    the simulators run its boundary condition and collision response on the GPU."""
+
+    def __init__(self, gridSize, gridOrigin, gridSpacing, mesh):
+        self._n = (int(gridSize.x), int(gridSize.y), int(gridSize.z))
+        self._origin = (gridOrigin.x, gridOrigin.y, gridOrigin.z)
+        self._spacing = (gridSpacing.x, gridSpacing.y, gridSpacing.z)
+        self._V = np.array(mesh.vertices, dtype=np.float64)
+        self._T = np.array(mesh.triangles, dtype=np.int64)
+        self._N = np.array(mesh.normals, dtype=np.float64)
+        self._sdf = None
+
+    def GetClosestDistanceAt(self, position):
+        """ScalarGrid3D::Sample of the collider's SDF (computed on the GPU the first time)."""
+        if self._sdf is None:
+            self._sdf = _abi.mesh_to_sdf(self._V, self._T, self._n, self._origin, self._spacing)
+        p = np.array(tuple(position), dtype=np.float64)
+        n = self._n
+        i0, i1, fr = [], [], []
+        for a in range(3):
+            x = (p[a] - self._origin[a]) / self._spacing[a]
+            hi = n[a] - 1
+            fl = np.floor(x)
+            ii = int(fl)
+            if hi == 0 or ii < 0:
+                ii, f = 0, 0.0
+            elif ii > hi - 1:
+                ii, f = hi - 1, 1.0
+            else:
+                f = x - fl
+            i0.append(ii)
+            i1.append(min(ii + 1, n[a] - 1))
+            fr.append(f)
+        at = lambda i, j, k: self._sdf[k, j, i]  # noqa: E731
+        lerp = lambda a, b, t: (1 - t) * a + t * b  # noqa: E731
+        b0 = lerp(lerp(at(i0[0], i0[1], i0[2]), at(i1[0], i0[1], i0[2]), fr[0]),
+                  lerp(at(i0[0], i1[1], i0[2]), at(i1[0], i1[1], i0[2]), fr[0]), fr[1])
+        b1 = lerp(lerp(at(i0[0], i0[1], i1[2]), at(i1[0], i0[1], i1[2]), fr[0]),
+                  lerp(at(i0[0], i1[1], i1[2]), at(i1[0], i1[1], i1[2]), fr[0]), fr[1])
+        return float(lerp(b0, b1, fr[2]))
+
+    def IsInside(self, position):
+        return self.GetClosestDistanceAt(position) < 0
+
+    def _add_to(self, scene):
+        scene.add_mesh_collider(self._V, self._T, self._N, self._n, self._origin, self._spacing)
+
+
+class ColliderCollection:
+    """ColliderCollection (3d/collider_collection.hpp): the colliders of SetColliders."""
+
+    def __init__(self, size=None, gridSpacing=None, origin=None):
+        self._colliders = []
+
+    def AddCollider(self, collider):
+        self._colliders.append(collider)
+
+    def GetColliders(self):
+        return self._colliders
+
+    def IsInside(self, position):
+        return any(c.IsInside(position) for c in self._colliders)
+
+
 class Emitter:
     """Emitter (emmiter/emmiter.hpp)."""
 
@@ -315,6 +384,7 @@ class HybridSimulator:
         self._blend = 0.05
         self._forces = []
         self._fieldForces = []
+        self._colliders = []
         self._emitters = []
         self._registered = None         # (scene, emitter versions) the scene's emitters were built from
         self._meshSeed = 0
@@ -324,6 +394,7 @@ class HybridSimulator:
         self._pending = None            # (pos, vel, C) until the scene exists
         self._currentFrame = Frame()
         self._currentTime = 0.0
+        self._numberOfTimeSteps = 0
         self._cg = dict(cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-4, max_refine=12)
         self.last_stats = []
 
@@ -345,9 +416,9 @@ class HybridSimulator:
         viscosity = float(viscosity)
         if not viscosity >= 0.0:
             raise ValueError("viscosity must be >= 0")
-        self._viscosity = viscosity
         if self._scene is not None:
             self._scene.set_viscosity(viscosity)
+        self._viscosity = viscosity
 
     def GetDensity(self):
         return self._density
@@ -397,7 +468,23 @@ class HybridSimulator:
         self._rebuild(lambda: self._forces.append(force))
 
     def AddCollider(self, collider):
-        raise NotImplementedError("colliders are outside the substep path (no benchmark scene has one)")
+        """PICSimulator::AddCollider (pic_simulator.cpp:66-69): a TriangleMeshCollider, applied on the GPU."""
+        if not isinstance(collider, TriangleMeshCollider):
+            raise TypeError("AddCollider: a TriangleMeshCollider is expected")
+        if self._scene is not None:
+            collider._add_to(self._scene)
+        self._colliders.append(collider)
+
+    def SetColliders(self, colliders):
+        """PICSimulator::SetColliders (pic_simulator.cpp:61-64): replaces the colliders with a ColliderCollection's."""
+        cs = list(colliders.GetColliders())
+        if not all(isinstance(c, TriangleMeshCollider) for c in cs):
+            raise TypeError("SetColliders: TriangleMeshColliders are expected")
+        if self._scene is not None:
+            self._scene.clear_colliders()
+            for c in cs:
+                c._add_to(self._scene)
+        self._colliders = cs
 
     def AddEmitter(self, emitter):
         """PICSimulator::AddEmitter (pic_simulator.cpp:46-49); registered with the scene at the next step."""
@@ -464,9 +551,14 @@ class HybridSimulator:
         self._currentTime = self._currentFrame.GetTimeInSeconds()
         dt = self._currentFrame.GetTimeIntervalInSeconds()
         n = scene.advance_frame(dt)
+        self._numberOfTimeSteps = n
         self._currentTime += dt
         self._currentFrame.Advance()
         return n
+
+    def GetNumberOfSubTimeSteps(self):
+        """PhysicsAnimation::GetNumberOfSubTimeSteps (physics_animation.cpp:43-46): substeps of the last frame."""
+        return self._numberOfTimeSteps
 
     def AdvanceFixedSubsteps(self, dt, nsub, stats=True):
         """nsub substeps of exactly dt (the benchmark configurations' fixed-dt mode)."""
@@ -490,6 +582,8 @@ class HybridSimulator:
                                 device=self._device, viscosity=self._viscosity, **self._cg)
             for f in self._fieldForces:
                 f._add_to(self._scene)
+            for c in self._colliders:
+                c._add_to(self._scene)
             if self._pending is not None:
                 p, v, c = self._pending
                 self._scene.set_particles(p, v, c)

@@ -5,11 +5,10 @@
 // PICSimulator (pic_simulator.hpp:27-43), FLIPSimulator (flip_simulator.hpp:9-16), APICSimulator
 // (apic_simulator.hpp:9-15), Frame (common/frame.hpp), BoundingBox3D (3d/bounding_box_3d.hpp),
 // DirectionalField, PointField, SwirlField, VolumeField (forces/), Vector3 (common/vector3.hpp), TriangleMesh, OBJManager,
-// ScalarGrid3D (the node-value subset), VolumeEmitter (emmiter/volume_emmiter.hpp), SimulationStats and
-// SimulationRunner, with the same names and argument meaning.  State lives on the GPU in one fe_scene
-// (include/fluide_b200.h), created on first use.  Colliders are outside the GPU path: AddCollider throws
-// std::logic_error saying so; errors of the library throw fluide::Error carrying the fe_status.
-// Header-only; link with libfluide_b200.so.
+// ScalarGrid3D (the node-value subset), VolumeEmitter (emmiter/volume_emmiter.hpp), SimulationStats,
+// SimulationRunner, Collider, TriangleMeshCollider and ColliderCollection (3d/), with the same names and argument
+// meaning.  State lives on the GPU in one fe_scene (include/fluide_b200.h), created on first use; errors of the
+// library throw fluide::Error carrying the fe_status.  Header-only; link with libfluide_b200.so.
 #ifndef FLUIDE_ENGINE_HPP
 #define FLUIDE_ENGINE_HPP
 
@@ -436,7 +435,103 @@ class VolumeField : public fluide::FieldForce {
     mutable std::vector<double> _field;
 };
 
-class Collider;
+// Collider (3d/collider.hpp): the base the simulators take in AddCollider.
+class Collider {
+  public:
+    virtual ~Collider() = default;
+    virtual bool IsInside(const Vector3<double>& position) = 0;
+    virtual double GetClosestDistanceAt(const Vector3<double>& position) = 0;
+    virtual Vector3<double> GetVelocityAt(const Vector3<double>& position) = 0;
+};
+
+// TriangleMeshCollider (3d/triangle_mesh_collider.cpp:4-100): a static solid given by a mesh with normals and the
+// node grid its Mesh2SDF lives on.  The simulators run its boundary condition and collision response on the GPU;
+// the distance queries here sample the same SDF (computed on the GPU, fe_mesh_to_sdf, the first time one is asked).
+class TriangleMeshCollider : public Collider {
+  public:
+    TriangleMeshCollider(const Vector3<size_t>& gridSize, const Vector3<double>& gridOrigin,
+                         const Vector3<double>& gridSpacing, const TriangleMesh& mesh)
+        : _n(gridSize), _origin(gridOrigin), _spacing(gridSpacing)
+    {
+        fluide::flatten_mesh(mesh, _V, _T);
+        for (const auto& nrm : mesh.GetNormals()) {
+            _N.push_back(nrm.x);
+            _N.push_back(nrm.y);
+            _N.push_back(nrm.z);
+        }
+    }
+    bool IsInside(const Vector3<double>& position) override { return GetClosestDistanceAt(position) < 0; }
+    // ScalarGrid3D::Sample of the collider's SDF (3d/scalar_grid3d.cpp:33-65)
+    double GetClosestDistanceAt(const Vector3<double>& p) override
+    {
+        const std::vector<double>& f = Sdf();
+        const size_t n[3] = {_n.x, _n.y, _n.z};
+        const double x[3] = {(p.x - _origin.x) / _spacing.x, (p.y - _origin.y) / _spacing.y, (p.z - _origin.z) / _spacing.z};
+        size_t i0[3], i1[3];
+        double fr[3];
+        for (int a = 0; a < 3; ++a) {
+            const int hi = (int)n[a] - 1;
+            const double fl = std::floor(x[a]);
+            int ii = (int)fl;
+            if (hi == 0 || ii < 0) { ii = 0; fr[a] = 0.0; }
+            else if (ii > hi - 1) { ii = hi - 1; fr[a] = 1.0; }
+            else fr[a] = x[a] - fl;
+            i0[a] = (size_t)ii;
+            i1[a] = std::min((size_t)ii + 1, n[a] - 1);
+        }
+        auto at = [&](size_t i, size_t j, size_t k) { return f[i + n[0] * (j + n[1] * k)]; };
+        auto lerp = [](double a, double b, double t) { return (1 - t) * a + t * b; };
+        const double b0 = lerp(lerp(at(i0[0], i0[1], i0[2]), at(i1[0], i0[1], i0[2]), fr[0]),
+                               lerp(at(i0[0], i1[1], i0[2]), at(i1[0], i1[1], i0[2]), fr[0]), fr[1]);
+        const double b1 = lerp(lerp(at(i0[0], i0[1], i1[2]), at(i1[0], i0[1], i1[2]), fr[0]),
+                               lerp(at(i0[0], i1[1], i1[2]), at(i1[0], i1[1], i1[2]), fr[0]), fr[1]);
+        return lerp(b0, b1, fr[2]);
+    }
+    Vector3<double> GetVelocityAt(const Vector3<double>&) override { return Vector3<double>(0.0); }  // returns 0
+    // Registers the collider with a scene (fe_scene_add_mesh_collider).
+    void AddTo(fe_scene* scene) const
+    {
+        const int32_t res[3] = {(int32_t)_n.x, (int32_t)_n.y, (int32_t)_n.z};
+        const double o[3] = {_origin.x, _origin.y, _origin.z}, h[3] = {_spacing.x, _spacing.y, _spacing.z};
+        fluide::check(fe_scene_add_mesh_collider(scene, _V.data(), _V.size() / 3, _T.data(), _T.size() / 4, _N.data(),
+                                                 _N.size() / 3, res, o, h, nullptr));
+    }
+
+  private:
+    const std::vector<double>& Sdf()
+    {
+        if (_sdf.empty()) {
+            std::vector<double> f(_n.x * _n.y * _n.z);
+            const int32_t n[3] = {(int32_t)_n.x, (int32_t)_n.y, (int32_t)_n.z};
+            const double o[3] = {_origin.x, _origin.y, _origin.z}, h[3] = {_spacing.x, _spacing.y, _spacing.z};
+            fluide::check(fe_mesh_to_sdf(_V.data(), _V.size() / 3, _T.data(), _T.size() / 4, n, o, h, f.data(), 0));
+            _sdf = std::move(f);
+        }
+        return _sdf;
+    }
+    Vector3<size_t> _n;
+    Vector3<double> _origin, _spacing;
+    std::vector<double> _V, _N, _sdf;
+    std::vector<int64_t> _T;
+};
+
+// ColliderCollection (3d/collider_collection.hpp): the colliders of PICSimulator::SetColliders.
+class ColliderCollection {
+  public:
+    ColliderCollection(const Vector3<size_t>& = Vector3<size_t>(1), const Vector3<double>& = Vector3<double>(1),
+                       const Vector3<double>& = Vector3<double>(0)) {}
+    void AddCollider(std::shared_ptr<Collider> collider) { _colliders.push_back(collider); }
+    std::vector<std::shared_ptr<Collider>>& GetColliders() { return _colliders; }
+    bool IsInside(const Vector3<double>& position)
+    {
+        for (auto& c : _colliders)
+            if (c->IsInside(position)) return true;
+        return false;
+    }
+
+  private:
+    std::vector<std::shared_ptr<Collider>> _colliders;
+};
 
 // Emitter (emmiter/emmiter.hpp): the base the simulators take in AddEmitter.
 class Emitter {
@@ -655,7 +750,28 @@ class HybridSimulator : public PhysicsAnimation {
         });
         _forces.push_back(newForce);
     }
-    void AddCollider(std::shared_ptr<Collider>) { throw std::logic_error("colliders are outside the substep path"); }
+    // PICSimulator::AddCollider / SetColliders (pic_simulator.cpp:61-69): TriangleMeshColliders, applied on the GPU
+    // (boundary condition, BOUNDRY cells, collision response).  A simulator with colliders cannot have a viscosity.
+    void AddCollider(std::shared_ptr<Collider> collider)
+    {
+        auto m = std::dynamic_pointer_cast<TriangleMeshCollider>(collider);
+        if (!m) throw std::invalid_argument("AddCollider: a TriangleMeshCollider is expected");
+        if (_scene) m->AddTo(_scene);
+        _colliders.push_back(m);
+    }
+    void SetColliders(std::shared_ptr<ColliderCollection> colliders)
+    {
+        std::vector<std::shared_ptr<TriangleMeshCollider>> list;
+        for (auto& c : colliders->GetColliders()) {
+            auto m = std::dynamic_pointer_cast<TriangleMeshCollider>(c);
+            if (!m) throw std::invalid_argument("SetColliders: TriangleMeshColliders are expected");
+            list.push_back(m);
+        }
+        if (_scene) fluide::check(fe_scene_clear_colliders(_scene));
+        _colliders = list;
+        if (_scene)
+            for (auto& m : _colliders) m->AddTo(_scene);
+    }
     // PICSimulator::AddEmitter (pic_simulator.cpp:46-49); emitters are registered with the scene at the next step.
     void AddEmitter(std::shared_ptr<Emitter> emitter)
     {
@@ -716,6 +832,7 @@ class HybridSimulator : public PhysicsAnimation {
                 const fe_force_desc d = f->Desc();
                 fluide::check(fe_scene_add_force(_scene, &d, nullptr));
             }
+            for (const auto& c : _colliders) c->AddTo(_scene);
             Upload();
             if (_meshSdfLive && !_sdf.empty()) fluide::check(fe_scene_set_fluid_sdf(_scene, _sdf.data()));
             _sdf.clear();
@@ -778,6 +895,7 @@ class HybridSimulator : public PhysicsAnimation {
     std::vector<float> _pos, _vel, _C;
     std::vector<std::shared_ptr<ExternalForce>> _forces;
     std::vector<std::shared_ptr<fluide::FieldForce>> _fieldForces;
+    std::vector<std::shared_ptr<TriangleMeshCollider>> _colliders;
     std::vector<std::shared_ptr<VolumeEmitter>> _emitters;
     std::vector<uint64_t> _emitterVersions;
     uint64_t _sceneGeneration = 0, _emitterGeneration = 0, _meshSeed = 0;

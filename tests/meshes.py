@@ -42,10 +42,16 @@ def icosphere(center, radius, subdiv=2):
     return V, T
 
 
-def write_obj(path, V, T, name="mesh"):
-    """A mesh as OBJ text that OBJManager::Load reads ("v" lines, "f a//n b//n c//n" faces with 1-based ids)."""
-    lines = [f"o {name}"] + [f"v {x:.17g} {y:.17g} {z:.17g}" for x, y, z in V] + ["vn 0 0 1"]
-    lines += [f"f {a + 1}//1 {b + 1}//1 {c + 1}//1" for a, b, c, *_ in T]
+def write_obj(path, V, T, name="mesh", N=None):
+    """A mesh as OBJ text that OBJManager::Load reads ("v" and "vn" lines, "f a//n b//n c//n" faces with 1-based ids;
+    with normals N, each face's normal is N[T[:, 3]], else one normal (0, 0, 1) for all)."""
+    lines = [f"o {name}"] + [f"v {x:.17g} {y:.17g} {z:.17g}" for x, y, z in V]
+    if N is None:
+        lines += ["vn 0 0 1"]
+        lines += [f"f {a + 1}//1 {b + 1}//1 {c + 1}//1" for a, b, c, *_ in T]
+    else:
+        lines += [f"vn {x:.17g} {y:.17g} {z:.17g}" for x, y, z in N]
+        lines += [f"f {a + 1}//{n + 1} {b + 1}//{n + 1} {c + 1}//{n + 1}" for a, b, c, n in T]
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
 

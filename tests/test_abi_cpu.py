@@ -77,8 +77,8 @@ def test_python_mirror_api_without_device():
     n = sim.InitializeFromRegions([dict(kind=0, lo=(0, 0, 0), hi=(0.4, 0.6, 1.0))])
     assert sim.GetNumberOfParticles() == n == 13 * 19 * 32
     assert tuple(sim.GetGridSpacing()) == (1 / 16, 1 / 16, 1 / 16)
-    with pytest.raises(NotImplementedError):
-        sim.AddCollider(object())
+    with pytest.raises(TypeError):
+        sim.AddCollider(object())  # a TriangleMeshCollider is expected
     sim.SetViscosity(0.1)  # kept until the scene exists (no device here)
     assert sim.GetViscosity() == 0.1
     with pytest.raises(ValueError):

@@ -65,7 +65,7 @@ def test_reference_construction_sequence_without_device():
     assert sim.GetViscosity() == 0.5
     with pytest.raises((ValueError, RuntimeError)):
         sim.SetViscosity(-0.5)
-    with pytest.raises(RuntimeError):
+    with pytest.raises((ValueError, TypeError, RuntimeError)):
         sim.AddCollider(None)
     # emitters are kept until the first step registers them with the scene
     em = m.VolumeEmitter(m.TriangleMesh(), m.Vector3S(16, 16, 16), domain, 8, m.Vector3D(0.0, 6.0, 0.0), m.Vector3D(0.0))
@@ -116,6 +116,7 @@ def build_cpp_api_binary(name="api_dam_break"):
 def test_cpp_api_compiles_and_links():
     assert os.path.exists(build_cpp_api_binary())
     assert os.path.exists(build_cpp_api_binary("api_emitter"))
+    assert os.path.exists(build_cpp_api_binary("api_collider"))
 
 
 def mesh_scene_expectations(Vf, Tf, Ve, Te, n, size, ppc=16):
@@ -348,3 +349,84 @@ def test_field_forces_through_mirrors_match_oracle(tmp_path, which):
     Po, Vo, _ = o.particles()
     assert np.linalg.norm(P - Po) / np.linalg.norm(Po) < 1e-4
     assert np.linalg.norm(Vel - Vo) / np.linalg.norm(Vo) < 1e-3
+
+
+def collider_scene_meshes(tmp_path):
+    from meshes import box, with_face_normals, write_obj
+
+    Vf, Tf = box((0.05, 0.05, 0.05), (0.45, 0.6, 0.95))
+    Vc, Tc, Nc = with_face_normals(*box((0.5, 0.0, 0.3), (0.75, 0.4, 0.7)))
+    write_obj(tmp_path / "fluid.obj", Vf, Tf)
+    write_obj(tmp_path / "collider.obj", Vc, Tc, N=Nc)
+    return (Vf, Tf), (Vc, Tc, Nc)
+
+
+def oracle_frames_with_collider(pos, vel, coll, frames, max_cfl):
+    import oracle
+
+    o = oracle.OracleSim((16, 16, 16), oracle.PIC, max_cfl=max_cfl, cg_rel_tol=1e-10, cg_max_it=5000)
+    o.add_mesh_collider(*coll, (16, 16, 16), (0.0, 0.0, 0.0), (1 / 16,) * 3)
+    o.set_particles(pos.astype(np.float64), vel.astype(np.float64))
+    subs = [o.advance_time(1 / 60) for _ in range(frames)]
+    return o, subs
+
+
+@pytest.mark.gpu
+def test_cpp_api_collider_scene(tmp_path):
+    """test/pic_simulator_test.cpp's collider sequence through the C++ API tracks the oracle over two frames."""
+    _, coll = collider_scene_meshes(tmp_path)
+    a, b = tmp_path / "init.bin", tmp_path / "final.bin"
+    out = subprocess.run([build_cpp_api_binary("api_collider"), str(tmp_path / "fluid.obj"),
+                          str(tmp_path / "collider.obj"), str(a), str(b)], capture_output=True, text=True,
+                         check=True).stdout
+    fields = {k: int(v) for k, v in (kv.split("=") for kv in out.split())}
+    init = np.fromfile(a, dtype=np.float32).reshape(-1, 6)
+    final = np.fromfile(b, dtype=np.float32).reshape(-1, 6)
+    assert fields["particles"] == init.shape[0] == final.shape[0] > 0 and fields["inside"] == 1
+    o, subs = oracle_frames_with_collider(init[:, :3], init[:, 3:], coll, 2, 2.0)
+    assert fields["substeps"] == sum(subs)
+    Po, Vo, _ = o.particles()
+    assert np.linalg.norm(final[:, :3] - Po) / np.linalg.norm(Po) < 1e-4
+    assert np.linalg.norm(final[1:, 3:] - Vo[1:]) / np.linalg.norm(Vo[1:]) < 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["pybind", "python"])
+def test_colliders_through_mirrors_track_oracle(tmp_path, which):
+    _, coll = collider_scene_meshes(tmp_path)
+    if which == "pybind":
+        m = pyf()
+    else:
+        import fluide_engine_b200 as m
+    fluid, cmesh = m.TriangleMesh(), m.TriangleMesh()
+    m.OBJManager().Load(str(tmp_path / "fluid.obj"), fluid)
+    m.OBJManager().Load(str(tmp_path / "collider.obj"), cmesh)
+    domain = m.BoundingBox3D(m.Vector3D(0.0, 0.0, 0.0), m.Vector3D(1.0, 1.0, 1.0))
+    sim = m.PICSimulator(m.Vector3S(16, 16, 16), domain)
+    sim.AddExternalForce(m.DirectionalField(m.Vector3D(0.0, -9.81, 0.0)))
+    sim.InitializeFromTriangleMesh(fluid)
+    col = m.TriangleMeshCollider(m.Vector3S(16, 16, 16), m.Vector3D(0.0, 0.0, 0.0), m.Vector3D(1 / 16, 1 / 16, 1 / 16),
+                                 cmesh)
+    assert col.IsInside(m.Vector3D(0.6, 0.2, 0.5)) and not col.IsInside(m.Vector3D(0.2, 0.2, 0.5))
+    collection = m.ColliderCollection(m.Vector3S(16, 16, 16), m.Vector3D(1 / 16, 1 / 16, 1 / 16), m.Vector3D(0.0, 0.0, 0.0))
+    collection.AddCollider(col)
+    sim.SetColliders(collection)
+    sim.SetMaxClf(2.0)
+    if which == "pybind":
+        sim.SetPressureSolverTolerance(1e-8, 4000)
+    else:
+        sim.SetPressureSolverSettings(cg_rel_tol=1e-8, cg_max_it=4000)
+    P0, V0, _ = sim.GetParticles()
+    o, subs = oracle_frames_with_collider(P0, V0, coll, 2, 2.0)
+    sim.SetCurrentFrame(m.Frame(1.0 / 60.0))
+    n = 0
+    for _ in range(2):
+        sim.AdvanceSingleFrame()
+        n += sim.GetNumberOfSubTimeSteps()
+    assert n == sum(subs)
+    P, V, _ = sim.GetParticles()
+    Po, Vo, _ = o.particles()
+    assert np.linalg.norm(P - Po) / np.linalg.norm(Po) < 1e-4
+    assert np.linalg.norm(V[1:] - Vo[1:]) / np.linalg.norm(Vo[1:]) < 1e-3
+    with pytest.raises((ValueError, TypeError, RuntimeError, m.FluideError if hasattr(m, "FluideError") else RuntimeError)):
+        sim.SetViscosity(0.1)  # colliders with viscosity are not on this path
