@@ -31,17 +31,71 @@ BOX = (0.0, 0.0, 0.0, 0.4, 0.6, 1.0)
 DT = 1.0 / 240.0
 
 
-def workload_config(n, steps, warmup, n_gpus, np_, viscosity=0.0):
+# The --collider obstacle: a box in the dam break's path (TriangleMeshCollider on the scene's grid).
+COLLIDER_BOX = (0.55, 0.0, 0.35, 0.8, 0.3, 0.65)
+
+
+def box_mesh(b):
+    """A closed box as (V (8,3), T (12,4): vertex ids and a normal id, N (12,3) unit face normals)."""
+    import numpy as np
+
+    lo, hi = np.array(b[:3], float), np.array(b[3:], float)
+    V = np.array([[lo[0] if (c & 1) == 0 else hi[0], lo[1] if (c & 2) == 0 else hi[1], lo[2] if (c & 4) == 0 else hi[2]]
+                  for c in range(8)])
+    tri = []
+    for a, b_, c, d in [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]:
+        tri += [(a, b_, c), (a, c, d)]
+    T = np.array([[a, b_, c, t] for t, (a, b_, c) in enumerate(tri)], dtype=np.int64)
+    N = np.cross(V[T[:, 1]] - V[T[:, 0]], V[T[:, 2]] - V[T[:, 0]])
+    return V, T, N / np.linalg.norm(N, axis=1, keepdims=True)
+
+
+def sphere_mesh(center, radius, subdiv=1):
+    """An icosphere as (V, T (T,4)) for the --mesh-init report."""
+    import numpy as np
+
+    t = (1.0 + 5 ** 0.5) / 2.0
+    V = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7),
+         (9, 8, 1)]
+    V = [np.array(v, float) / np.linalg.norm(v) for v in V]
+    for _ in range(subdiv):
+        cache, F2 = {}, []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = V[a] + V[b]
+                V.append(m / np.linalg.norm(m))
+                cache[key] = len(V) - 1
+            return cache[key]
+
+        for a, b, c in F:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            F2 += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        F = F2
+    V = np.array(V) * radius + np.asarray(center, float)
+    return V, np.array([[a, b, c, 0] for a, b, c in F], dtype=np.int64)
+
+
+def workload_config(n, steps, warmup, n_gpus, np_, viscosity=0.0, collider=False):
     cfg = {
         "workload": "FLIP dam break %d^3, box [0,0.4]x[0,0.6]x[0,1], 8 particles/cell (seed 0), dt=1/240, "
                     "FP32 CG in FP64 refinement to rel 1e-6" % n + (", viscosity %g (backward Euler, Jacobi "
-                                                                    "1000/5/1e-14)" % viscosity if viscosity else ""),
+                                                                    "1000/5/1e-14)" % viscosity if viscosity else "")
+                    + (", box collider [%g,%g]x[%g,%g]x[%g,%g] (TriangleMeshCollider on the %d^3 grid)"
+                       % (COLLIDER_BOX[0], COLLIDER_BOX[3], COLLIDER_BOX[1], COLLIDER_BOX[4], COLLIDER_BOX[2],
+                          COLLIDER_BOX[5], n) if collider else ""),
         "grid": [n, n, n], "particles": np_, "solver": "FLIP 0.95", "dt": DT, "cg_rel_tol": 1e-6, "max_cfl": 1.0,
         "substeps_timed": steps, "warmup": warmup, "parallelism": "replicas x%d" % n_gpus,
         "l2": "working set > 126 MB L2 (particles alone %.0f MB); no flush" % (np_ * 24 / 1e6),
     }
     if viscosity:
         cfg["viscosity"] = viscosity
+    if collider:
+        cfg["collider"] = list(COLLIDER_BOX)
     return cfg
 
 
@@ -157,7 +211,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def reference_sample(n, steps, cores_hint=None, viscosity=0.0):
+def reference_sample(n, steps, cores_hint=None, viscosity=0.0, collider=False):
     """Times the reference's own threaded CPU simulator on the workload; returns (value, info)."""
     import numpy as np
     import oracle
@@ -175,6 +229,9 @@ def reference_sample(n, steps, cores_hint=None, viscosity=0.0):
                                viscosity=viscosity)
         kind = "port"
         threads = 1
+    if collider:
+        V, T, Nrm = box_mesh(COLLIDER_BOX)
+        sim.add_mesh_collider(V, T, Nrm, (n, n, n), (0.0, 0.0, 0.0), (1.0 / n,) * 3)
     sim.set_particles(pos.astype(np.float64), vel.astype(np.float64))
     times = []
     for _ in range(steps):
@@ -184,8 +241,9 @@ def reference_sample(n, steps, cores_hint=None, viscosity=0.0):
     total = sum(times)
     value = pos.shape[0] * steps / total
     info = {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
-            "sample": "%d substep(s) of the %d^3 FLIP dam break from rest (%d particles)%s, %.1f s; host has %d cores"
-                      % (steps, n, pos.shape[0], ", viscosity %g" % viscosity if viscosity else "", total, cores)}
+            "sample": "%d substep(s) of the %d^3 FLIP dam break from rest (%d particles)%s%s, %.1f s; host has %d cores"
+                      % (steps, n, pos.shape[0], ", viscosity %g" % viscosity if viscosity else "",
+                         ", box collider" if collider else "", total, cores)}
     return value, total / steps * 1e3, info
 
 
@@ -272,18 +330,53 @@ def surface_report(scene, n, reps=5, reference=True):
     return out
 
 
+def mesh_init_report(n, device, reference=True, reps=3):
+    """InitializeFromTriangleMesh on the GPU (fe_scene_init_from_mesh: Mesh2SDF band distances and winding signs,
+    cell test, scan, particle writes; wall time of the synchronous call on a fresh scene) for an 80-triangle
+    icosphere, and the reference's own InitializeFromTriangleMesh on the CPU for comparison."""
+    import fluide_engine_b200 as fe
+
+    V, T = sphere_mesh((0.5, 0.45, 0.5), 0.3, 1)
+    times, count = [], 0
+    for _ in range(reps):
+        sc = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, device=device)
+        t0 = time.perf_counter()
+        sc.init_from_mesh(V, T, seed=1)
+        times.append((time.perf_counter() - t0) * 1e3)
+        count = sc.num_particles()
+        sc.close()
+    out = {"gpu_ms": sorted(times)[len(times) // 2], "gpu_ms_all": times, "particles": int(count),
+           "triangles": int(T.shape[0]), "grid": [n, n, n],
+           "path": "fe_scene_init_from_mesh (Mesh2SDF on the device, 16 particles per inside cell)"}
+    if reference:
+        try:
+            import oracle
+
+            variant = "threaded" if oracle.ref_available("threaded") else ("serial" if oracle.ref_available("serial") else None)
+            if variant:
+                r = oracle.RefSim((n, n, n), oracle.FLIP, variant=variant)
+                t0 = time.perf_counter()
+                r.init_from_mesh(V, T)
+                out["reference_ms"] = (time.perf_counter() - t0) * 1e3
+                out["reference_particles"] = int(r.particles()[0].shape[0])
+        except Exception as ex:  # reported, never required
+            out["reference_ms"] = None
+            out["reference_error"] = str(ex)[:200]
+    return out
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     n_gpus = args.gpus
     steps = max(1, min(args.steps, args.ref_steps))
-    value, ms, info = reference_sample(args.n, steps, viscosity=args.viscosity)
+    value, ms, info = reference_sample(args.n, steps, viscosity=args.viscosity, collider=args.collider)
     particles = int(round(value * ms / 1e3))
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": n_gpus, "steps": steps, "warmup": 0,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded analytic scene)", "impl": "reference",
-            "config": workload_config(args.n, steps, 0, 1, particles, args.viscosity), "cpu_baseline": info,
+            "config": workload_config(args.n, steps, 0, 1, particles, args.viscosity, args.collider), "cpu_baseline": info,
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -530,6 +623,10 @@ def main():
                     help="single workload: also time GetSurface (device mesh + OBJ write) after the timed region")
     ap.add_argument("--viscosity", type=float, default=0.0,
                     help="single workload / reference arm: kinematic viscosity (0 = none, as the benchmark scenes)")
+    ap.add_argument("--collider", action="store_true",
+                    help="single workload / reference arm: a box TriangleMeshCollider in the dam break's path")
+    ap.add_argument("--mesh-init", action="store_true",
+                    help="single workload: also time InitializeFromTriangleMesh (GPU and reference CPU)")
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
     # served: 20 jobs/s as the served configuration, over 6 s instead of 10 min and with resolutions <= 128 so
     # that a run takes tens of seconds; the work still exceeds the arrival window several times (saturated)
@@ -572,6 +669,9 @@ def main():
     scene = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, cg_inner_tol=args.cg_inner_tol,
                      device=local, pressure_solver={"auto": fe.AUTO, "mgpcg": fe.MGPCG, "cg": fe.CG}[args.pressure_solver],
                      viscosity=args.viscosity)
+    if args.collider:
+        CV, CT, CN = box_mesh(COLLIDER_BOX)
+        scene.add_mesh_collider(CV, CT, CN, (n, n, n), (0.0, 0.0, 0.0), (1.0 / n,) * 3)
     stream = torch.cuda.Stream()
     scene.set_stream(stream.cuda_stream)
     scene.set_particles(pos, vel)
@@ -601,7 +701,7 @@ def main():
     fluid = np.array([s["fluid_cells"] for s in stats], dtype=np.float64)
     its = np.array([s["cg_iterations"] for s in stats], dtype=np.float64)
     refs = np.array([s["refinements"] for s in stats], dtype=np.float64)
-    multigrid = uses_multigrid(n, args.pressure_solver)
+    multigrid = uses_multigrid(n, args.pressure_solver) and not args.collider  # collider scenes use the plain CG
     alg_bytes = solver_alg_bytes(fluid, its, refs, n, multigrid)  # per launch
     peak, peak_kind = peaks()
     achieved = alg_bytes.sum() / (cg_ms.sum() / 1e3) / 1e9
@@ -611,6 +711,8 @@ def main():
     phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
     diffusion = diffusion_report(scene, stream, peak, peak_kind) if args.viscosity > 0 else None
     surface = surface_report(scene, n, reference=not args.no_cpu_baseline) if args.surface and rank == 0 else None
+    mesh_init = (mesh_init_report(n, local, reference=not args.no_cpu_baseline) if args.mesh_init and rank == 0
+                 else None)
 
     # end to end through the public API with host buffers: H2D particles, one substep, D2H particles
     pin_pos = torch.from_numpy(pos).pin_memory()
@@ -637,7 +739,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            _, _, cpu = reference_sample(n, args.ref_steps, viscosity=args.viscosity)
+            _, _, cpu = reference_sample(n, args.ref_steps, viscosity=args.viscosity, collider=args.collider)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": METRIC, "cores": None, "kind": "unavailable", "sample": str(ex)[:200]}
 
@@ -646,7 +748,7 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded analytic scene)",
-            "config": workload_config(n, args.steps, args.warmup, world, N, args.viscosity),
+            "config": workload_config(n, args.steps, args.warmup, world, N, args.viscosity, args.collider),
             "roofline": {"bound": "hbm",
                          "kernel": ("k_mgcg (persistent multigrid-preconditioned FP32 CG + FP64 refinement, one "
                                     "launch/substep)" if multigrid else
@@ -677,6 +779,8 @@ def main():
             line["diffusion"] = diffusion
         if surface:
             line["surface"] = surface
+        if mesh_init:
+            line["mesh_init"] = mesh_init
         print(json.dumps(line), flush=True)
     scene.close()
     if world > 1:
