@@ -377,6 +377,24 @@ __global__ void k_collide_prep(CollideSet cs, const uint32_t* __restrict__ list,
     }
 }
 
+// Entry k = e * colliders + c reflects particle c iff the previous entry's closest point was inside collider c's
+// mesh (entries e >= 1; the first entry's test uses the particle's own position and is made serially).
+__global__ void k_collide_active(const uint32_t* __restrict__ count, int ncoll, const uint8_t* __restrict__ ins,
+                                 uint32_t* __restrict__ act)
+{
+    const uint64_t total = (uint64_t)(*count) * ncoll;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k <= total; k += (uint64_t)gridDim.x * blockDim.x)
+        act[k] = (k < total && k >= (uint64_t)ncoll && ins[k - ncoll]) ? 1u : 0u;
+}
+
+__global__ void k_collide_active_compact(const uint32_t* __restrict__ count, int ncoll, const uint32_t* __restrict__ act,
+                                         const uint32_t* __restrict__ offs, uint32_t* __restrict__ list)
+{
+    const uint64_t total = (uint64_t)(*count) * ncoll;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x)
+        if (act[k]) list[offs[k]] = (uint32_t)k;
+}
+
 // The velocity part of ResolveCollision for a particle inside the mesh (restitution 0, friction 0).
 __device__ void reflect(double vel[3], const double nrm[3])
 {
@@ -434,7 +452,7 @@ __global__ void k_collide_serial(CollideSet cs, SceneView v, CollideMove g, cons
                                  const float* __restrict__ start, const float* __restrict__ startv,
                                  const uint32_t* __restrict__ slot_of, const uint32_t* __restrict__ count,
                                  const double* __restrict__ cp, const double* __restrict__ nrm,
-                                 const uint8_t* __restrict__ ins)
+                                 const uint32_t* __restrict__ act_offs, const uint32_t* __restrict__ act_list)
 {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     const int nc = (int)min((uint64_t)cs.count, v.np);
@@ -470,16 +488,22 @@ __global__ void k_collide_serial(CollideSet cs, SceneView v, CollideMove g, cons
             }
         }
     }
-    bool cur[kMaxColliders];
-    for (int c = 0; c < nc; ++c) cur[c] = mesh_inside(mesh_of(cs.c[c]), P[c]);
+    // The listed particles' resolutions: particle c reflects at entry e when it was inside the mesh, i.e. at the
+    // first entry by its own position and later by the previous entry's closest point (ins); the entries where
+    // that holds were compacted in order (act_list), and its final position is the last entry's closest point.
     const uint32_t cnt = nc > 0 ? *count : 0u;
-    for (uint32_t e = 0; e < cnt; ++e)
-        for (int c = 0; c < nc; ++c) {
-            const size_t k = (size_t)e * cs.count + c;
-            if (cur[c]) reflect(V[c], nrm + 3 * k);
-            for (int a = 0; a < 3; ++a) P[c][a] = cp[3 * k + a];
-            cur[c] = ins[k] != 0;
+    if (cnt > 0) {
+        for (int c = 0; c < nc; ++c)
+            if (mesh_inside(mesh_of(cs.c[c]), P[c])) reflect(V[c], nrm + 3 * (size_t)c);
+        const uint32_t nact = act_offs[(size_t)cnt * cs.count];
+        for (uint32_t a = 0; a < nact; ++a) {
+            const uint32_t k = act_list[a];
+            const int c = (int)(k % cs.count);
+            if (c < nc) reflect(V[c], nrm + 3 * (size_t)k);
         }
+        for (int c = 0; c < nc; ++c)
+            for (int a = 0; a < 3; ++a) P[c][a] = cp[3 * ((size_t)(cnt - 1) * cs.count + c) + a];
+    }
     for (int c = 0; c < nc; ++c) {
         const uint32_t s = slot_of[c];
         v.px[s] = (float)P[c][0]; v.py[s] = (float)P[c][1]; v.pz[s] = (float)P[c][2];
@@ -508,6 +532,90 @@ __global__ void k_add_gravity(float* u, float* vv, float* w, int nx, int ny, int
 
 unsigned node_blocks(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
+// Connected FLUID components (union-find with atomicMin links; every loop is bounded and reports through err).
+constexpr uint32_t kNoLabel = 0xffffffffu;
+constexpr int kFindLimit = 1 << 24;
+
+__device__ __forceinline__ uint32_t find_root(const uint32_t* label, uint32_t x, int* err)
+{
+    for (int it = 0; it < kFindLimit; ++it) {
+        const uint32_t p = __ldcg(label + x);
+        if (p == x) return x;
+        x = p;
+    }
+    atomicExch(err, FE_ERR_TIMEOUT);
+    return x;
+}
+
+__global__ void k_ccl_init(const uint8_t* __restrict__ marks, size_t nc, uint32_t* __restrict__ label,
+                           uint8_t* __restrict__ open_comp, double* __restrict__ sum, uint32_t* __restrict__ cnt)
+{
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        label[c] = marks[c] == FE_CELL_FLUID ? (uint32_t)c : kNoLabel;
+        open_comp[c] = 0;
+        sum[c] = 0.0;
+        cnt[c] = 0u;
+    }
+}
+
+__global__ void k_ccl_union(const uint8_t* __restrict__ marks, int nx, int ny, int nz, uint32_t* label, int* err)
+{
+    const size_t nc = (size_t)nx * ny * nz, sxy = (size_t)nx * ny;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        if (marks[c] != FE_CELL_FLUID) continue;
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / sxy);
+        const size_t nb[3] = {i > 0 ? c - 1 : c, j > 0 ? c - nx : c, k > 0 ? c - sxy : c};
+        for (int q = 0; q < 3; ++q) {
+            if (nb[q] == c || marks[nb[q]] != FE_CELL_FLUID) continue;
+            uint32_t a = (uint32_t)c, b = (uint32_t)nb[q];
+            for (int it = 0; it < kFindLimit; ++it) {
+                a = find_root(label, a, err);
+                b = find_root(label, b, err);
+                if (a == b) break;
+                if (a > b) { const uint32_t t = a; a = b; b = t; }
+                const uint32_t old = atomicMin(label + b, a);  // link the larger root under the smaller
+                if (old == b) break;
+                b = old;
+                if (it == kFindLimit - 1) atomicExch(err, FE_ERR_TIMEOUT);
+            }
+        }
+    }
+}
+
+// Roots of components with an AIR neighbour (a Dirichlet condition), and the right-hand-side sums of the others.
+__global__ void k_ccl_classify(const uint8_t* __restrict__ marks, const double* __restrict__ b, int nx, int ny, int nz,
+                               uint32_t* label, uint8_t* __restrict__ open_comp, double* __restrict__ sum,
+                               uint32_t* __restrict__ cnt, int* err)
+{
+    const size_t nc = (size_t)nx * ny * nz, sxy = (size_t)nx * ny;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        if (marks[c] != FE_CELL_FLUID) continue;
+        const uint32_t r = find_root(label, (uint32_t)c, err);
+        label[c] = r;
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / sxy);
+        const bool air = (i > 0 && marks[c - 1] == FE_CELL_AIR) || (i + 1 < nx && marks[c + 1] == FE_CELL_AIR) ||
+                         (j > 0 && marks[c - nx] == FE_CELL_AIR) || (j + 1 < ny && marks[c + nx] == FE_CELL_AIR) ||
+                         (k > 0 && marks[c - sxy] == FE_CELL_AIR) || (k + 1 < nz && marks[c + sxy] == FE_CELL_AIR);
+        if (air) open_comp[r] = 1;
+        atomicAdd(sum + r, b[c]);
+        atomicAdd(cnt + r, 1u);
+    }
+}
+
+// A component without AIR neighbours is a pure-Neumann block: its right-hand side loses its mean, which leaves a
+// consistent system unchanged and makes an inconsistent one solvable.
+__global__ void k_ccl_project(const uint8_t* __restrict__ marks, size_t nc, const uint32_t* __restrict__ label,
+                              const uint8_t* __restrict__ open_comp, const double* __restrict__ sum,
+                              const uint32_t* __restrict__ cnt, double* __restrict__ b)
+{
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        if (marks[c] != FE_CELL_FLUID) continue;
+        const uint32_t r = label[c];
+        if (open_comp[r]) continue;
+        b[c] -= sum[r] / (double)cnt[r];
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_collider_setup(const SceneView& v, const CollideSet& cs, CollideWork& w, cudaStream_t st)
@@ -520,6 +628,22 @@ cudaError_t launch_collider_setup(const SceneView& v, const CollideSet& cs, Coll
     count_launch();
     k_collider_faces<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v, w.csdf, w.face_open,
                                                                                           w.face_cls);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_collider_project_rhs(const SceneView& v, const CollideWork& w, int* err, cudaStream_t st)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const size_t nc = (size_t)nx * ny * nz;
+    k_ccl_init<<<node_blocks(nc), 256, 0, st>>>(v.marks, nc, w.label, w.open_comp, w.comp_sum, w.comp_cnt);
+    count_launch();
+    k_ccl_union<<<node_blocks(nc), 256, 0, st>>>(v.marks, nx, ny, nz, w.label, err);
+    count_launch();
+    k_ccl_classify<<<node_blocks(nc), 256, 0, st>>>(v.marks, v.b, nx, ny, nz, w.label, w.open_comp, w.comp_sum,
+                                                   w.comp_cnt, err);
+    count_launch();
+    k_ccl_project<<<node_blocks(nc), 256, 0, st>>>(v.marks, nc, w.label, w.open_comp, w.comp_sum, w.comp_cnt, v.b);
     count_launch();
     return cudaGetLastError();
 }
@@ -600,8 +724,18 @@ cudaError_t launch_collider_resolve(const SceneView& v, const CollideSet& cs, co
     count_launch();
     k_collide_prep<<<148 * 8, 128, 0, st>>>(cs, w.list, w.offs + v.np, w.spos, w.cp, w.nrm, w.ins);
     count_launch();
+    // entries that reflect (in order): flags over (count * colliders + 1) entries, scanned, compacted; the scan
+    // length is the capacity bound because the count lives on the device
+    const uint64_t cap_entries = v.np * (uint64_t)cs.count + 1;
+    k_collide_active<<<node_blocks(cap_entries), 256, 0, st>>>(w.offs + v.np, cs.count, w.ins, w.act);
+    count_launch();
+    e = launch_exclusive_scan(w.act, (uint32_t)cap_entries, w.act_offs, w.act_tmp, w.act_tmp_bytes, st);
+    if (e != cudaSuccess) return e;
+    k_collide_active_compact<<<node_blocks(cap_entries), 256, 0, st>>>(w.offs + v.np, cs.count, w.act, w.act_offs,
+                                                                      w.act_list);
+    count_launch();
     k_collide_serial<<<1, 32, 0, st>>>(cs, v, g, w.csdf, w.start, w.startv, w.slot_of, w.offs + v.np, w.cp, w.nrm,
-                                       w.ins);
+                                       w.act_offs + 0, w.act_list);
     count_launch();
     return cudaGetLastError();
 }

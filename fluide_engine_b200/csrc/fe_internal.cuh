@@ -335,6 +335,10 @@ struct CollideWork {
     float *ftmp0, *ftmp1;    // faces: extrapolation copies
     float* fric;             // faces: projected velocities of the inside faces
     double *sdf_a, *sdf_b;   // n^3: fluid SDF ping-pong
+    uint32_t* label;         // n^3: FLUID component labels (union-find)
+    uint8_t* open_comp;      // n^3 (by root): the component has an AIR neighbour
+    double* comp_sum;        // n^3 (by root): right-hand-side sum of the component
+    uint32_t* comp_cnt;      // n^3 (by root): its cells
     // collision response (sized by the particle capacity)
     float* start;            // 3 per slot: position before the move
     float* startv;           // 3 per slot: velocity before the move (after the grid-to-particle transfer)
@@ -345,6 +349,9 @@ struct CollideWork {
     double *cp, *nrm;        // 3 per (listed particle, collider)
     uint8_t* ins;            // 1 per (listed particle, collider)
     uint32_t* slot_of;       // kMaxColliders
+    uint32_t *act, *act_offs, *act_list;  // (listed particle, collider) entries that reflect, compacted in order
+    void* act_tmp;
+    size_t act_tmp_bytes;
     void* scan_tmp;
     size_t scan_tmp_bytes;
 };
@@ -357,6 +364,8 @@ struct CollideMove {
 };
 cudaError_t launch_collider_setup(const SceneView& v, const CollideSet& cs, CollideWork& w, cudaStream_t st);
 cudaError_t launch_collider_bc(const SceneView& v, const CollideWork& w, float* const buf[3], cudaStream_t st);
+// Enclosed FLUID components (no AIR neighbour: a pure-Neumann block) lose the mean of their right-hand side.
+cudaError_t launch_collider_project_rhs(const SceneView& v, const CollideWork& w, int* err, cudaStream_t st);
 cudaError_t launch_collider_marks(const SceneView& v, const CollideWork& w, unsigned long long* node_scratch,
                                   double** fluid_sdf, cudaStream_t st);
 cudaError_t launch_collider_keep_start(const SceneView& v, const CollideWork& w, cudaStream_t st);

@@ -159,6 +159,7 @@ struct fe_scene {
     CollideWork cw{};
     std::vector<void*> cw_grid_allocs, cw_particle_allocs;
     uint64_t cw_cap = 0;
+    int cw_ncoll = 0;
     double* collider_fluid_sdf = nullptr;  // Fluid3::sdf of the last collider substep (after ExtrapolateIntoCollider)
     uint64_t epoch = 0;                // bumped when the substep's kernel sequence changes (batches re-capture)
     double* d_scalar = nullptr;        // CFL / divergence result
@@ -456,26 +457,36 @@ fe_status alloc_grid(fe_scene* s)
 // The collision response's buffers, sized by the particle capacity and the collider count.
 fe_status collide_particle_buffers(fe_scene* s)
 {
-    if (s->cw_cap == s->cap && s->cw.ins && s->cw.cp) return FE_OK;
+    const int ncoll = std::max(s->colliders.count, 1);
+    if (s->cw_cap == s->cap && s->cw_ncoll == ncoll && s->cw.ins && s->cw.cp) return FE_OK;
     free_list(s->cw_particle_allocs, s->stream);
     auto& L = s->cw_particle_allocs;
     auto& w = s->cw;
     const uint64_t cap = std::max<uint64_t>(s->cap, 1);
+    const uint64_t entries = cap * (uint64_t)ncoll;
     FE_CUDA(dalloc(L, &w.start, 3 * cap, s->device, s->stream));
     FE_CUDA(dalloc(L, &w.startv, 3 * cap, s->device, s->stream));
     FE_CUDA(dalloc(L, &w.spos, 3 * cap, s->device, s->stream));
     FE_CUDA(dalloc(L, &w.flag, cap + 1, s->device, s->stream));
     FE_CUDA(dalloc(L, &w.offs, cap + 1, s->device, s->stream));
     FE_CUDA(dalloc(L, &w.list, cap, s->device, s->stream));
-    FE_CUDA(dalloc(L, &w.cp, 3 * cap * kMaxColliders, s->device, s->stream));
-    FE_CUDA(dalloc(L, &w.nrm, 3 * cap * kMaxColliders, s->device, s->stream));
-    FE_CUDA(dalloc(L, &w.ins, cap * kMaxColliders, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.cp, 3 * entries, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.nrm, 3 * entries, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.ins, entries, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.act, entries + 1, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.act_offs, entries + 1, s->device, s->stream));
+    FE_CUDA(dalloc(L, &w.act_list, entries, s->device, s->stream));
+    w.act_tmp_bytes = sort_scan_tmp_bytes((uint32_t)(entries + 1));
+    uint8_t* atmp = nullptr;
+    FE_CUDA(dalloc(L, &atmp, w.act_tmp_bytes, s->device, s->stream));
+    w.act_tmp = atmp;
     FE_CUDA(dalloc(L, &w.slot_of, kMaxColliders, s->device, s->stream));
     w.scan_tmp_bytes = sort_scan_tmp_bytes((uint32_t)(cap + 1));
     uint8_t* tmp = nullptr;
     FE_CUDA(dalloc(L, &tmp, w.scan_tmp_bytes, s->device, s->stream));
     w.scan_tmp = tmp;
     s->cw_cap = s->cap;
+    s->cw_ncoll = ncoll;
     return FE_OK;
 }
 
@@ -635,6 +646,7 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
         case kStepRhs:
             FE_CUDA(ensure_grid(s, pressure_buffer(s), st));
             FE_CUDA(launch_rhs(v, st));
+            if (s->colliders.count > 0) FE_CUDA(launch_collider_project_rhs(v, s->cw, s->cg.err, st));
             break;
         case kStepCg:
             if (s->mg.levels >= 2 && s->colliders.count == 0)
@@ -1786,6 +1798,10 @@ fe_status fe_scene_add_mesh_collider(fe_scene* s, const double* vertices, uint64
         FE_CUDA(dalloc(L, &w.fric, nf, s->device, st));
         FE_CUDA(dalloc(L, &w.sdf_a, nc, s->device, st));
         FE_CUDA(dalloc(L, &w.sdf_b, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.label, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.open_comp, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.comp_sum, nc, s->device, st));
+        FE_CUDA(dalloc(L, &w.comp_cnt, nc, s->device, st));
     }
     s->colliders.c[s->colliders.count] = c;
     if (id) *id = s->colliders.count;
@@ -1814,6 +1830,7 @@ fe_status fe_scene_clear_colliders(fe_scene* s)
     free_list(s->cw_particle_allocs, s->stream);
     s->cw = CollideWork{};
     s->cw_cap = 0;
+    s->cw_ncoll = 0;
     s->colliders.count = 0;
     s->collider_fluid_sdf = nullptr;
     drop_graphs(s);

@@ -183,6 +183,23 @@ struct SolverSetup {
     int kc;         // list entries cached per thread
 };
 
+// The stencil mask of cell c: in-domain neighbours that are not BOUNDRY (single_phase_pressure_solver.cpp:117-150),
+// 0 for non-FLUID cells.  A FLUID cell enclosed by BOUNDRY cells and walls has an all-zero row in the reference's
+// system: nothing couples to it and its pressure reaches no face (ApplyPressure skips faces toward BOUNDRY), so it
+// is left out of the solve with pressure 0 instead of holding the residual at |b| for every iteration.
+__device__ __forceinline__ uint32_t solve_mask(const uint8_t* __restrict__ marks, int c, int nx, int ny, int nz)
+{
+    if (marks[c] != FE_CELL_FLUID) return 0u;
+    const int i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+    const size_t sxy1 = (size_t)nx * ny;
+    return (i > 0 && marks[c - 1] != FE_CELL_BOUNDRY ? kXm : 0u) |
+           (i + 1 < nx && marks[c + 1] != FE_CELL_BOUNDRY ? kXp : 0u) |
+           (j > 0 && marks[c - nx] != FE_CELL_BOUNDRY ? kYm : 0u) |
+           (j + 1 < ny && marks[c + nx] != FE_CELL_BOUNDRY ? kYp : 0u) |
+           (k > 0 && marks[c - sxy1] != FE_CELL_BOUNDRY ? kZm : 0u) |
+           (k + 1 < nz && marks[c + sxy1] != FE_CELL_BOUNDRY ? kZp : 0u);
+}
+
 __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w, const int blk, const int nblk,
                                              unsigned& gen, double* sh, uint32_t* s_warp, uint32_t* s_list,
                                              SolverSetup& out)
@@ -208,7 +225,7 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
     const int cb = min(nc, blk * chunk), ce = min(nc, cb + chunk);
     double acc[2] = {0.0, 0.0};
     for (int c = cb + threadIdx.x; c < ce; c += blockDim.x) {
-        if (marks[c] == FE_CELL_FLUID) {
+        if (solve_mask(marks, c, nx, ny, nz) != 0u) {
             acc[0] += b[c] * b[c];
             acc[1] += 1.0;
         } else {
@@ -237,7 +254,8 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int c0 = cb; c0 < ce; c0 += blockDim.x) {
         const int c = c0 + threadIdx.x;
-        const bool fl = c < ce && marks[c] == FE_CELL_FLUID;
+        const uint32_t m = c < ce ? solve_mask(marks, c, nx, ny, nz) : 0u;
+        const bool fl = m != 0u;
         const unsigned bal = __ballot_sync(0xffffffffu, fl);
         if (lane == 0) s_warp[wid] = __popc(bal);
         __syncthreads();
@@ -248,15 +266,6 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
             total += x;
         }
         if (fl) {
-            const int i = c % nx, j = (c / nx) % ny, k = c / sxy;
-            // in-domain neighbours that are not BOUNDRY (single_phase_pressure_solver.cpp:117-150)
-            const size_t sxy1 = (size_t)nx * ny;
-            uint32_t m = (i > 0 && marks[c - 1] != FE_CELL_BOUNDRY ? kXm : 0u) |
-                         (i + 1 < nx && marks[c + 1] != FE_CELL_BOUNDRY ? kXp : 0u) |
-                         (j > 0 && marks[c - nx] != FE_CELL_BOUNDRY ? kYm : 0u) |
-                         (j + 1 < ny && marks[c + nx] != FE_CELL_BOUNDRY ? kYp : 0u) |
-                         (k > 0 && marks[c - sxy1] != FE_CELL_BOUNDRY ? kZm : 0u) |
-                         (k + 1 < nz && marks[c + sxy1] != FE_CELL_BOUNDRY ? kZp : 0u);
             const uint32_t slot = base + off + __popc(bal & ((1u << lane) - 1u));
             list[slot] = ((uint32_t)c << 6) | m;
         }
