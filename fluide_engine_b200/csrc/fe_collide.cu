@@ -136,14 +136,29 @@ __global__ void k_collider_faces(SceneView v, const double* __restrict__ csdf, u
     cls[g] = k;
 }
 
-// ConstrainVelocity: blocked faces to 0 before the extrapolation.
-__global__ void k_bc_block(float* u, float* vv, float* w, int nx, int ny, int nz, const uint8_t* __restrict__ open)
+// Faces (u | v | w numbering) as a reference into the three velocity buffers, and their coordinates.
+__device__ __forceinline__ float& face_at(float* u, float* vv, float* w, size_t nu, size_t nvv, uint32_t g)
 {
-    FaceCoord fc;
-    if (!face_coord(nx, ny, nz, fc)) return;
-    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz;
-    const size_t g = (fc.c == 0 ? 0 : (fc.c == 1 ? nu : nu + nvv)) + fc.f;
-    if (!open[g]) (fc.c == 0 ? u : (fc.c == 1 ? vv : w))[fc.f] = 0.f;
+    return g < nu ? u[g] : (g < nu + nvv ? vv[g - nu] : w[g - nu - nvv]);
+}
+__device__ __forceinline__ void face_index_coord(uint32_t g, int nx, int ny, size_t nu, size_t nvv, int& c, int id[3])
+{
+    size_t f = g;
+    int sx = nx, sy = ny;
+    if (g < nu) { c = 0; sx = nx + 1; }
+    else if (g < nu + nvv) { c = 1; f -= nu; sy = ny + 1; }
+    else { c = 2; f -= nu + nvv; }
+    id[0] = (int)(f % sx);
+    id[1] = (int)((f / sx) % sy);
+    id[2] = (int)(f / ((size_t)sx * sy));
+}
+
+// ConstrainVelocity: blocked faces to 0 before the extrapolation (the fixed list of faces that are not open).
+__global__ void k_bc_block(float* u, float* vv, float* w, size_t nu, size_t nvv, const uint32_t* __restrict__ list,
+                           uint32_t n)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+        face_at(u, vv, w, nu, nvv, list[e]) = 0.f;
 }
 
 // ScalarGrid3D::Gradient of the collider SDF at p.
@@ -189,10 +204,16 @@ __device__ void collider_gradient(const double* __restrict__ csdf, const NodeGri
     out[2] = r2;
 }
 
-// ConstrainVelocity's projection of the faces inside the collider, into `tmp` (it samples the whole grid).
-__global__ void k_bc_friction(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
-                              const float* __restrict__ w, const double* __restrict__ csdf,
-                              const uint8_t* __restrict__ cls, float* __restrict__ tmp)
+// A rewritten face's list entry: its face index, with kFinProject set when it is projected onto the collider's
+// tangent plane (inside, not zero, and a non-zero SDF gradient); the other entries are set to 0.
+constexpr uint32_t kFinProject = 0x80000000u;
+
+// The fixed face lists of a static collider classification: the blocked faces, and the faces ConstrainVelocity
+// rewrites with the unit collider normal (FP64) at the projected ones.  With count_only the kernel only counts
+// them into cnt[0] and cnt[1]; list order does not matter (every entry is independent).
+__global__ void k_collider_face_lists(SceneView v, const double* __restrict__ csdf, const uint8_t* __restrict__ open,
+                                      const uint8_t* __restrict__ cls, uint32_t* cnt, uint32_t* __restrict__ blk,
+                                      uint32_t* __restrict__ fin, double* __restrict__ fin_nrm, int count_only)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
     FaceCoord fc;
@@ -200,42 +221,75 @@ __global__ void k_bc_friction(SceneView v, const float* __restrict__ u, const fl
     const int c = fc.c;
     const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz;
     const size_t g = (c == 0 ? 0 : (c == 1 ? nu : nu + nvv)) + fc.f;
-    if (!(cls[g] & kFaceInside)) return;
-    const int id[3] = {fc.i, fc.j, fc.k};
-    double p[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) p[a] = da(a == c ? 0.0 : dm(v.h[a], 0.5), dm(v.h[a], (double)id[a]));
-    const float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
-    const double vel[3] = {sample_face(u, pf[0], pf[1], pf[2], v.xo, v.inv_hf, nx + 1, ny, nz),
-                           sample_face(vv, pf[0], pf[1], pf[2], v.yo, v.inv_hf, nx, ny + 1, nz),
-                           sample_face(w, pf[0], pf[1], pf[2], v.zo, v.inv_hf, nx, ny, nz + 1)};
-    const int n[3] = {nx, ny, nz};
-    const NodeGrid cg = node_grid_of(n, v.origin, v.h);
-    double gr[3];
-    collider_gradient(csdf, cg, p, gr);
-    const double gl = len3(gr);
-    double out = 0.0;
-    if (dm(gl, gl) > 0.0) {
-        const double nrm[3] = {dd(gr[0], gl), dd(gr[1], gl), dd(gr[2], gl)};
-        const double d = dot3(vel, nrm);
-        const double vc = c == 0 ? vel[0] : (c == 1 ? vel[1] : vel[2]);
-        const double nc = c == 0 ? nrm[0] : (c == 1 ? nrm[1] : nrm[2]);
-        out = da(ds(vc, dm(nc, d)), 0.0);
+    if (!open[g]) {
+        const uint32_t e = atomicAdd(cnt, 1u);
+        if (!count_only) blk[e] = (uint32_t)g;
     }
-    tmp[g] = (float)out;
-}
-
-// ConstrainVelocity's write-back: projected inside faces, then the zero bits.
-__global__ void k_bc_finish(float* u, float* vv, float* w, int nx, int ny, int nz, const uint8_t* __restrict__ cls,
-                            const float* __restrict__ tmp)
-{
-    FaceCoord fc;
-    if (!face_coord(nx, ny, nz, fc)) return;
-    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz;
-    const size_t g = (fc.c == 0 ? 0 : (fc.c == 1 ? nu : nu + nvv)) + fc.f;
     const uint8_t k = cls[g];
     if (!(k & (kFaceInside | kFaceZero))) return;
-    (fc.c == 0 ? u : (fc.c == 1 ? vv : w))[fc.f] = (k & kFaceZero) ? 0.f : tmp[g];
+    const uint32_t e = atomicAdd(cnt + 1, 1u);
+    if (count_only) return;
+    uint32_t entry = (uint32_t)g;
+    double nrm[3] = {0.0, 0.0, 0.0};
+    if (!(k & kFaceZero)) {
+        const int id[3] = {fc.i, fc.j, fc.k};
+        double p[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) p[a] = da(a == c ? 0.0 : dm(v.h[a], 0.5), dm(v.h[a], (double)id[a]));
+        const int n[3] = {nx, ny, nz};
+        const NodeGrid cg = node_grid_of(n, v.origin, v.h);
+        double gr[3];
+        collider_gradient(csdf, cg, p, gr);
+        const double gl = len3(gr);
+        if (dm(gl, gl) > 0.0) {
+            nrm[0] = dd(gr[0], gl);
+            nrm[1] = dd(gr[1], gl);
+            nrm[2] = dd(gr[2], gl);
+            entry |= kFinProject;
+        }
+    }
+    fin[e] = entry;
+    fin_nrm[3 * (size_t)e] = nrm[0];
+    fin_nrm[3 * (size_t)e + 1] = nrm[1];
+    fin_nrm[3 * (size_t)e + 2] = nrm[2];
+}
+
+// ConstrainVelocity's projection of the faces inside the collider (it samples the whole grid, so the results go to
+// `tmp`, one per list entry, and are written back by k_bc_finish).
+__global__ void k_bc_friction(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
+                              const float* __restrict__ w, const uint32_t* __restrict__ fin,
+                              const double* __restrict__ fin_nrm, uint32_t n, float* __restrict__ tmp)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const uint32_t entry = fin[e];
+        if (!(entry & kFinProject)) continue;
+        int c, id[3];
+        face_index_coord(entry & ~kFinProject, nx, ny, nu, nvv, c, id);
+        double p[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) p[a] = da(a == c ? 0.0 : dm(v.h[a], 0.5), dm(v.h[a], (double)id[a]));
+        const float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
+        const double vel[3] = {sample_face(u, pf[0], pf[1], pf[2], v.xo, v.inv_hf, nx + 1, ny, nz),
+                               sample_face(vv, pf[0], pf[1], pf[2], v.yo, v.inv_hf, nx, ny + 1, nz),
+                               sample_face(w, pf[0], pf[1], pf[2], v.zo, v.inv_hf, nx, ny, nz + 1)};
+        const double nrm[3] = {fin_nrm[3 * (size_t)e], fin_nrm[3 * (size_t)e + 1], fin_nrm[3 * (size_t)e + 2]};
+        const double d = dot3(vel, nrm);
+        const double vc = c == 0 ? vel[0] : (c == 1 ? vel[1] : vel[2]);
+        const double ncmp = c == 0 ? nrm[0] : (c == 1 ? nrm[1] : nrm[2]);
+        tmp[e] = (float)da(ds(vc, dm(ncmp, d)), 0.0);
+    }
+}
+
+// ConstrainVelocity's write-back: projected inside faces, every other listed face (zero bit, or no normal) to 0.
+__global__ void k_bc_finish(float* u, float* vv, float* w, size_t nu, size_t nvv, const uint32_t* __restrict__ fin,
+                            uint32_t n, const float* __restrict__ tmp)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const uint32_t entry = fin[e];
+        face_at(u, vv, w, nu, nvv, entry & ~kFinProject) = (entry & kFinProject) ? tmp[e] : 0.f;
+    }
 }
 
 // One pass of ExtrapolateToRegion over the fluid-SDF nodes (FP64), neighbour order i+1, i-1, j+1, j-1, k+1, k-1.
@@ -582,10 +636,9 @@ __global__ void k_ccl_union(const uint8_t* __restrict__ marks, int nx, int ny, i
     }
 }
 
-// Roots of components with an AIR neighbour (a Dirichlet condition), and the right-hand-side sums of the others.
-__global__ void k_ccl_classify(const uint8_t* __restrict__ marks, const double* __restrict__ b, int nx, int ny, int nz,
-                               uint32_t* label, uint8_t* __restrict__ open_comp, double* __restrict__ sum,
-                               uint32_t* __restrict__ cnt, int* err)
+// Roots of components with an AIR neighbour (a Dirichlet condition); every FLUID cell's label becomes its root.
+__global__ void k_ccl_classify(const uint8_t* __restrict__ marks, int nx, int ny, int nz, uint32_t* label,
+                               uint8_t* __restrict__ open_comp, int* err)
 {
     const size_t nc = (size_t)nx * ny * nz, sxy = (size_t)nx * ny;
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
@@ -596,7 +649,19 @@ __global__ void k_ccl_classify(const uint8_t* __restrict__ marks, const double* 
         const bool air = (i > 0 && marks[c - 1] == FE_CELL_AIR) || (i + 1 < nx && marks[c + 1] == FE_CELL_AIR) ||
                          (j > 0 && marks[c - nx] == FE_CELL_AIR) || (j + 1 < ny && marks[c + nx] == FE_CELL_AIR) ||
                          (k > 0 && marks[c - sxy] == FE_CELL_AIR) || (k + 1 < nz && marks[c + sxy] == FE_CELL_AIR);
-        if (air) open_comp[r] = 1;
+        if (air && !open_comp[r]) open_comp[r] = 1;
+    }
+}
+
+// Right-hand-side sums of the enclosed components only (the open ones, the bulk of the fluid, need none).
+__global__ void k_ccl_sums(const uint8_t* __restrict__ marks, const double* __restrict__ b, size_t nc,
+                           const uint32_t* __restrict__ label, const uint8_t* __restrict__ open_comp,
+                           double* __restrict__ sum, uint32_t* __restrict__ cnt)
+{
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+        if (marks[c] != FE_CELL_FLUID) continue;
+        const uint32_t r = label[c];
+        if (open_comp[r]) continue;
         atomicAdd(sum + r, b[c]);
         atomicAdd(cnt + r, 1u);
     }
@@ -616,6 +681,9 @@ __global__ void k_ccl_project(const uint8_t* __restrict__ marks, size_t nc, cons
     }
 }
 
+// Blocks for a grid-stride pass over a list of n entries (256 threads), at most 8 per SM.
+unsigned list_blocks(uint32_t n) { return (unsigned)std::max<uint32_t>(1u, std::min<uint32_t>((n + 255u) / 256u, 148u * 8u)); }
+
 }  // namespace
 
 cudaError_t launch_collider_setup(const SceneView& v, const CollideSet& cs, CollideWork& w, cudaStream_t st)
@@ -632,6 +700,16 @@ cudaError_t launch_collider_setup(const SceneView& v, const CollideSet& cs, Coll
     return cudaGetLastError();
 }
 
+cudaError_t launch_collider_face_lists(const SceneView& v, CollideWork& w, bool count_only, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(w.face_cnt, 0, 2 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_collider_face_lists<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(
+        v, w.csdf, w.face_open, w.face_cls, w.face_cnt, w.blk_list, w.fin_list, w.fin_nrm, count_only ? 1 : 0);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_collider_project_rhs(const SceneView& v, const CollideWork& w, int* err, cudaStream_t st)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
@@ -640,8 +718,9 @@ cudaError_t launch_collider_project_rhs(const SceneView& v, const CollideWork& w
     count_launch();
     k_ccl_union<<<node_blocks(nc), 256, 0, st>>>(v.marks, nx, ny, nz, w.label, err);
     count_launch();
-    k_ccl_classify<<<node_blocks(nc), 256, 0, st>>>(v.marks, v.b, nx, ny, nz, w.label, w.open_comp, w.comp_sum,
-                                                   w.comp_cnt, err);
+    k_ccl_classify<<<node_blocks(nc), 256, 0, st>>>(v.marks, nx, ny, nz, w.label, w.open_comp, err);
+    count_launch();
+    k_ccl_sums<<<node_blocks(nc), 256, 0, st>>>(v.marks, v.b, nc, w.label, w.open_comp, w.comp_sum, w.comp_cnt);
     count_launch();
     k_ccl_project<<<node_blocks(nc), 256, 0, st>>>(v.marks, nc, w.label, w.open_comp, w.comp_sum, w.comp_cnt, v.b);
     count_launch();
@@ -651,11 +730,12 @@ cudaError_t launch_collider_project_rhs(const SceneView& v, const CollideWork& w
 cudaError_t launch_collider_bc(const SceneView& v, const CollideWork& w, float* const buf[3], cudaStream_t st)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
-    const dim3 grid = face_grid(nx, ny, nz), block(kTileX, kTileY);
     const size_t nu = (size_t)(nx + 1) * ny * nz, nvv = (size_t)nx * (ny + 1) * nz;
     const size_t total = nu + nvv + (size_t)nx * ny * (nz + 1);
-    k_bc_block<<<grid, block, 0, st>>>(buf[0], buf[1], buf[2], nx, ny, nz, w.face_open);
-    count_launch();
+    if (w.n_blk > 0) {
+        k_bc_block<<<list_blocks(w.n_blk), 256, 0, st>>>(buf[0], buf[1], buf[2], nu, nvv, w.blk_list, w.n_blk);
+        count_launch();
+    }
     if (v.extrap_depth > 0) {
         // copy into scratch 0, extrapolate from there back into buf (scratch 1 is the ping-pong partner)
         float* s0[3] = {w.ftmp0, w.ftmp0 + nu, w.ftmp0 + nu + nvv};
@@ -669,10 +749,13 @@ cudaError_t launch_collider_bc(const SceneView& v, const CollideWork& w, float* 
         cudaError_t e = launch_extrap_faces(v, s0, buf, s1, open, w.vscratch, v.extrap_depth, st);
         if (e != cudaSuccess) return e;
     }
-    k_bc_friction<<<grid, block, 0, st>>>(v, buf[0], buf[1], buf[2], w.csdf, w.face_cls, w.fric);
-    count_launch();
-    k_bc_finish<<<grid, block, 0, st>>>(buf[0], buf[1], buf[2], nx, ny, nz, w.face_cls, w.fric);
-    count_launch();
+    if (w.n_fin > 0) {
+        k_bc_friction<<<list_blocks(w.n_fin), 256, 0, st>>>(v, buf[0], buf[1], buf[2], w.fin_list, w.fin_nrm, w.n_fin,
+                                                            w.fric);
+        count_launch();
+        k_bc_finish<<<list_blocks(w.n_fin), 256, 0, st>>>(buf[0], buf[1], buf[2], nu, nvv, w.fin_list, w.n_fin, w.fric);
+        count_launch();
+    }
     return cudaGetLastError();
 }
 

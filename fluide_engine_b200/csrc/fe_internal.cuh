@@ -333,7 +333,12 @@ struct CollideWork {
     uint8_t* vscratch;       // 2 x faces: extrapolation validity ping-pong
     uint8_t* node_vscratch;  // 2 x n^3
     float *ftmp0, *ftmp1;    // faces: extrapolation copies
-    float* fric;             // faces: projected velocities of the inside faces
+    float* fric;             // faces: projected velocities of the listed faces (one per fin_list entry)
+    uint32_t* face_cnt;      // 2: list lengths found on the device
+    uint32_t* blk_list;      // the faces that are not open (fixed with the collider set)
+    uint32_t* fin_list;      // the faces ConstrainVelocity rewrites, bit 31: projected onto the tangent plane
+    double* fin_nrm;         // 3 per fin_list entry: the unit collider normal at a projected face
+    uint32_t n_blk, n_fin;
     double *sdf_a, *sdf_b;   // n^3: fluid SDF ping-pong
     uint32_t* label;         // n^3: FLUID component labels (union-find)
     uint8_t* open_comp;      // n^3 (by root): the component has an AIR neighbour
@@ -363,6 +368,8 @@ struct CollideMove {
     const float *u, *v, *w;
 };
 cudaError_t launch_collider_setup(const SceneView& v, const CollideSet& cs, CollideWork& w, cudaStream_t st);
+// count_only: the list lengths into face_cnt; otherwise fill lists sized by those counts.
+cudaError_t launch_collider_face_lists(const SceneView& v, CollideWork& w, bool count_only, cudaStream_t st);
 cudaError_t launch_collider_bc(const SceneView& v, const CollideWork& w, float* const buf[3], cudaStream_t st);
 // Enclosed FLUID components (no AIR neighbour: a pure-Neumann block) lose the mean of their right-hand side.
 cudaError_t launch_collider_project_rhs(const SceneView& v, const CollideWork& w, int* err, cudaStream_t st);

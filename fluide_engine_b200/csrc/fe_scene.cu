@@ -157,7 +157,7 @@ struct fe_scene {
     CollideSet colliders{};
     std::vector<std::vector<void*>> collider_allocs;
     CollideWork cw{};
-    std::vector<void*> cw_grid_allocs, cw_particle_allocs;
+    std::vector<void*> cw_grid_allocs, cw_particle_allocs, cw_face_allocs;
     uint64_t cw_cap = 0;
     int cw_ncoll = 0;
     double* collider_fluid_sdf = nullptr;  // Fluid3::sdf of the last collider substep (after ExtrapolateIntoCollider)
@@ -454,6 +454,31 @@ fe_status alloc_grid(fe_scene* s)
 
 // Allocates both particle sets and the per-particle scratch for `cap` particles; the first `keep` particles of
 // the current set are copied into set 0 (which becomes current) before the old buffers are released.
+// The fixed face lists of the collider classification (blocked faces; faces ConstrainVelocity rewrites, with their
+// normals), counted on the device and allocated to size, so the per-substep passes visit only those faces.
+fe_status collider_face_lists(fe_scene* s)
+{
+    auto& w = s->cw;
+    cudaStream_t st = s->stream;
+    const size_t nf = (size_t)(s->base.g.nx + 1) * s->base.g.ny * s->base.g.nz +
+                      (size_t)s->base.g.nx * (s->base.g.ny + 1) * s->base.g.nz +
+                      (size_t)s->base.g.nx * s->base.g.ny * (s->base.g.nz + 1);
+    if (nf >= 0x80000000ull) return set_error(FE_ERR_BAD_ARG, "collider scenes need fewer than 2^31 faces");
+    FE_CUDA(launch_collider_face_lists(s->base, w, true, st));
+    uint32_t cnt[2] = {0, 0};
+    FE_CUDA(cudaMemcpyAsync(cnt, w.face_cnt, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    FE_CUDA(cudaStreamSynchronize(st));
+    free_list(s->cw_face_allocs, st);
+    auto& L = s->cw_face_allocs;
+    FE_CUDA(dalloc(L, &w.blk_list, std::max<size_t>(cnt[0], 1), s->device, st));
+    FE_CUDA(dalloc(L, &w.fin_list, std::max<size_t>(cnt[1], 1), s->device, st));
+    FE_CUDA(dalloc(L, &w.fin_nrm, 3 * std::max<size_t>(cnt[1], 1), s->device, st));
+    w.n_blk = cnt[0];
+    w.n_fin = cnt[1];
+    FE_CUDA(launch_collider_face_lists(s->base, w, false, st));
+    return FE_OK;
+}
+
 // The collision response's buffers, sized by the particle capacity and the collider count.
 fe_status collide_particle_buffers(fe_scene* s)
 {
@@ -1060,6 +1085,7 @@ fe_status fe_scene_destroy(fe_scene* s)
     for (auto& l : s->collider_allocs) free_list(l, s->own_stream);
     free_list(s->cw_grid_allocs, s->own_stream);
     free_list(s->cw_particle_allocs, s->own_stream);
+    free_list(s->cw_face_allocs, s->own_stream);
     cudaStreamDestroy(s->own_stream);  // its pending frees still run
     delete s;
     return FE_OK;
@@ -1796,6 +1822,7 @@ fe_status fe_scene_add_mesh_collider(fe_scene* s, const double* vertices, uint64
         FE_CUDA(dalloc(L, &w.ftmp0, nf, s->device, st));
         FE_CUDA(dalloc(L, &w.ftmp1, nf, s->device, st));
         FE_CUDA(dalloc(L, &w.fric, nf, s->device, st));
+        FE_CUDA(dalloc(L, &w.face_cnt, 2, s->device, st));
         FE_CUDA(dalloc(L, &w.sdf_a, nc, s->device, st));
         FE_CUDA(dalloc(L, &w.sdf_b, nc, s->device, st));
         FE_CUDA(dalloc(L, &w.label, nc, s->device, st));
@@ -1809,6 +1836,8 @@ fe_status fe_scene_add_mesh_collider(fe_scene* s, const double* vertices, uint64
     s->collider_allocs.push_back(std::move(allocs));
     // ColliderCollection::BuildSdf gives the same SDF every substep (static colliders): build and classify now
     FE_CUDA(launch_collider_setup(b, s->colliders, w, st));
+    r = collider_face_lists(s);
+    if (r != FE_OK) return r;
     r = collide_particle_buffers(s);
     if (r != FE_OK) return r;
     FE_CUDA(cudaStreamSynchronize(st));
@@ -1828,6 +1857,7 @@ fe_status fe_scene_clear_colliders(fe_scene* s)
     s->collider_allocs.clear();
     free_list(s->cw_grid_allocs, s->stream);
     free_list(s->cw_particle_allocs, s->stream);
+    free_list(s->cw_face_allocs, s->stream);
     s->cw = CollideWork{};
     s->cw_cap = 0;
     s->cw_ncoll = 0;
