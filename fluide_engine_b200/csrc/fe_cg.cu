@@ -18,6 +18,8 @@
 //              products (r', r') and (w', r'), then ONE grid-wide reduction.  w' = A r' needs the
 //              neighbours' r', which each thread recomputes as r - alpha (w + beta s) from the previous
 //              iteration's neighbour values; r, w and s ping-pong so those stay intact within the pass.
+//              A cell's (r, w, s, p) sit together in one float4, so a neighbour costs one 16-byte load and
+//              the cell's new state one 16-byte store.
 // The grid-wide barrier is a counter + generation word with a bounded spin: if a block waits longer than
 // a few seconds it records FE_ERR_TIMEOUT, every block leaves its loops and the kernel returns, so a stuck
 // solve surfaces as a status instead of a hung device.  Dot products travel with the barrier: blocks
@@ -56,16 +58,14 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
     st.ih2[2] = (float)ih2d[2];
     double* __restrict__ p64 = v.p;
     const double* __restrict__ b = v.b;
-    float* __restrict__ R[2] = {w.r0, w.r1};
-    float* __restrict__ W[2] = {w.w0, w.w1};
-    float* __restrict__ S[2] = {w.s0, w.s1};
-    float* __restrict__ P = w.pv;
-    float* __restrict__ X = w.x;
+    float4* __restrict__ Q[2] = {w.rws0, w.rws1};  // (r, w, s, p) per cell
+    float* __restrict__ R0 = reinterpret_cast<float*>(w.rws0);  // r of cell c at R0[4 c]
+    float* __restrict__ X = w.xcg;
     uint32_t* __restrict__ list = w.list;
 
     unsigned gen = 0;
     SolverSetup su;
-    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su)) return;
+    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su, true)) return;
     const int F = su.F, kc = su.kc;
     const double bnorm = su.bnorm;
     auto entry = [&](int k, int e) -> uint32_t { return k < kc ? s_list[k * blockDim.x + threadIdx.x] : list[e]; };
@@ -94,7 +94,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
             if (m & kZm) az += pc - p64[c - sxy];
             if (m & kZp) az += pc - p64[c + sxy];
             const double rr = b[c] - (ih2d[0] * ax + ih2d[1] * ay + ih2d[2] * az);
-            R[0][c] = (float)rr;
+            R0[4 * (size_t)c] = (float)rr;
             racc[0] += rr * rr;
         }
         cur = 0;
@@ -112,13 +112,10 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
         for (int e = tid, k = 0; e < F; e += T, ++k) {
             const uint32_t ent = entry(k, e);
             const int c = (int)(ent >> 6);
-            const float* __restrict__ r0 = R[0];
-            const float wc = apply_row(st, c, ent & 63u, [&](int q) { return r0[q]; });
-            const float rc = r0[c];
-            W[0][c] = wc;
+            const float wc = apply_row(st, c, ent & 63u, [&](int q) { return R0[4 * (size_t)q]; });
+            const float rc = R0[4 * (size_t)c];
+            Q[0][c] = make_float4(rc, wc, 0.f, 0.f);
             X[c] = 0.f;
-            P[c] = 0.f;
-            S[0][c] = 0.f;
             d0[0] += (double)rc * (double)rc;
             d0[1] += (double)wc * (double)rc;
         }
@@ -140,27 +137,24 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
             if (!(alpha > 0.0) || !isfinite(alpha)) break;  // FP32 breakdown: leave it to the outer loop
             first = false;
             const float af = (float)alpha, bf = (float)beta;
-            const float* __restrict__ r = R[cur];
-            const float* __restrict__ wv = W[cur];
-            const float* __restrict__ s = S[cur];
-            float* __restrict__ rn = R[cur ^ 1];
-            float* __restrict__ wn = W[cur ^ 1];
-            float* __restrict__ sn = S[cur ^ 1];
+            const float4* __restrict__ q0 = Q[cur];
+            float4* __restrict__ q1 = Q[cur ^ 1];
             double dd[2] = {0.0, 0.0};
             for (int e = tid, k = 0; e < F; e += T, ++k) {
                 const uint32_t ent = entry(k, e);
                 const int c = (int)(ent >> 6);
                 // r'(q) = r(q) - alpha (w(q) + beta s(q)) for this cell and its neighbours
-                auto rnew = [&](int q) { return r[q] - af * (wv[q] + bf * s[q]); };
-                const float snew = wv[c] + bf * s[c];
-                const float pnew = r[c] + bf * P[c];
-                const float rc = r[c] - af * snew;
+                auto rnew = [&](int q) {
+                    const float4 t = q0[q];
+                    return t.x - af * (t.y + bf * t.z);
+                };
+                const float4 me = q0[c];
+                const float snew = me.y + bf * me.z;
+                const float pnew = me.x + bf * me.w;
+                const float rc = me.x - af * snew;
                 const float wc = apply_row(st, c, ent & 63u, rnew);
-                P[c] = pnew;
                 X[c] += af * pnew;
-                sn[c] = snew;
-                rn[c] = rc;
-                wn[c] = wc;
+                q1[c] = make_float4(rc, wc, snew, pnew);
                 dd[0] += (double)rc * (double)rc;
                 dd[1] += (double)wc * (double)rc;
             }

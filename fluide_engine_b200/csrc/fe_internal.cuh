@@ -224,7 +224,11 @@ cudaError_t launch_scatter_out(const SceneView& v, float* pos, float* vel, float
 
 // CG solver (fe_cg.cu).
 struct CgWork {
-    float *r0, *r1, *w0, *w1, *s0, *s1, *pv, *x;  // FP32 inner-CG vectors (r, w, s ping-pong)
+    float *r0, *r1, *w0, *w1, *s0, *s1, *pv, *x;  // FP32 vectors of the multigrid solver (8 x cells)
+    // the plain CG's view of the same memory: (r, w, s, p) of a cell in one float4, ping-pong, and its correction
+    // (a 9th run of cells after the 8 above)
+    float4 *rws0, *rws1;
+    float* xcg;
     uint32_t* list;         // compacted FLUID cells: (cell << 6) | in-domain neighbour mask
     double* partial;        // [0, 12) three rotating reduction totals slots, [16, 16 + max blocks) FLUID counts
     unsigned* bar;          // kCgBarWords barrier words

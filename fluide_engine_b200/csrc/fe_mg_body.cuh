@@ -194,7 +194,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
 
     unsigned gen = 0;
     SolverSetup su;
-    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su)) return;
+    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su, false)) return;
     const int F = su.F, kc = su.kc;
     const double bnorm = su.bnorm;
     auto entry = [&](int k, int e) -> uint32_t { return k < kc ? s_list[k * blockDim.x + threadIdx.x] : list[e]; };

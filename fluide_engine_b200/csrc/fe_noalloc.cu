@@ -32,8 +32,8 @@ constexpr int kStatsRing = 4;
 // Byte layout of the scratch array (all offsets multiples of 256).
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kOffB = 0;                                                        // FP64 rhs
-constexpr size_t kOffVec = align256(kOffB + kMaxCells * sizeof(double));          // 8 FP32 CG vectors
-constexpr size_t kOffList = align256(kOffVec + 8 * kMaxCells * sizeof(float));     // compacted FLUID list
+constexpr size_t kOffVec = align256(kOffB + kMaxCells * sizeof(double));          // 9 FP32 CG vectors
+constexpr size_t kOffList = align256(kOffVec + 9 * kMaxCells * sizeof(float));     // compacted FLUID list
 constexpr size_t kOffPartial = align256(kOffList + kMaxCells * sizeof(uint32_t));  // partials + totals
 constexpr size_t kOffBar = align256(kOffPartial + cg_partial_doubles(kMaxBlocks) * sizeof(double));
 constexpr size_t kOffErr = align256(kOffBar + kCgBarWords * sizeof(unsigned));
@@ -64,6 +64,9 @@ fe_status scratch_for(int dev, CgWork* out)
         const size_t n = kMaxCells;
         w.r0 = vec; w.r1 = vec + n; w.w0 = vec + 2 * n; w.w1 = vec + 3 * n;
         w.s0 = vec + 4 * n; w.s1 = vec + 5 * n; w.pv = vec + 6 * n; w.x = vec + 7 * n;
+        w.rws0 = reinterpret_cast<float4*>(vec);
+        w.rws1 = reinterpret_cast<float4*>(vec + 4 * n);
+        w.xcg = vec + 8 * n;
         w.list = (uint32_t*)(base + kOffList);
         w.partial = (double*)(base + kOffPartial);
         w.bar = (unsigned*)(base + kOffBar);

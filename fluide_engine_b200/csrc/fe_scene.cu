@@ -364,10 +364,13 @@ fe_status alloc_grid(fe_scene* s)
     // CG vectors
     CgWork& w = s->cg;
     float* vec;
-    FE_CUDA(dalloc(L, &vec, nc * 8, dev, st));
-    FE_CUDA(cudaMemsetAsync(vec, 0, nc * 8 * sizeof(float), st));
+    FE_CUDA(dalloc(L, &vec, nc * 9, dev, st));
+    FE_CUDA(cudaMemsetAsync(vec, 0, nc * 9 * sizeof(float), st));
     w.r0 = vec; w.r1 = vec + nc; w.w0 = vec + 2 * nc; w.w1 = vec + 3 * nc;
     w.s0 = vec + 4 * nc; w.s1 = vec + 5 * nc; w.pv = vec + 6 * nc; w.x = vec + 7 * nc;
+    w.rws0 = reinterpret_cast<float4*>(vec);
+    w.rws1 = reinterpret_cast<float4*>(vec + 4 * nc);
+    w.xcg = vec + 8 * nc;
     FE_CUDA(dalloc(L, &w.list, nc, dev, st));
     // multigrid levels 1 .. L-1 (dense; level 0 is the grid above)
     s->mg.levels = 0;
@@ -1149,7 +1152,7 @@ fe_status fe_scene_reset(fe_scene* s)
     FE_CUDA(cudaMemsetAsync(v.p, 0, nc * sizeof(double), st));
     FE_CUDA(cudaMemsetAsync(v.b, 0, nc * sizeof(double), st));
     FE_CUDA(cudaMemsetAsync(v.cell_start, 0, ((size_t)v.g.key_space + 1) * sizeof(uint32_t), st));
-    FE_CUDA(cudaMemsetAsync(s->cg.r0, 0, nc * 8 * sizeof(float), st));
+    FE_CUDA(cudaMemsetAsync(s->cg.r0, 0, nc * 9 * sizeof(float), st));
     FE_CUDA(cudaMemsetAsync(s->cg.partial, 0, cg_partial_doubles(kMaxCgBlocks) * sizeof(double), st));
     FE_CUDA(cudaMemsetAsync(s->cg.bar, 0, kCgBarWords * sizeof(unsigned), st));
     FE_CUDA(cudaMemsetAsync(s->cg.err, 0, sizeof(int), st));

@@ -202,7 +202,7 @@ __device__ __forceinline__ uint32_t solve_mask(const uint8_t* __restrict__ marks
 
 __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w, const int blk, const int nblk,
                                              unsigned& gen, double* sh, uint32_t* s_warp, uint32_t* s_list,
-                                             SolverSetup& out)
+                                             SolverSetup& out, bool interleaved)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
     const int sxy = nx * ny;
@@ -230,13 +230,18 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
             acc[1] += 1.0;
         } else {
             p64[c] = 0.0;
-            R[0][c] = 0.f;
-            R[1][c] = 0.f;
-            W[0][c] = 0.f;
-            W[1][c] = 0.f;
-            S[0][c] = 0.f;
-            S[1][c] = 0.f;
-            w.pv[c] = 0.f;
+            if (interleaved) {  // the plain CG's (r, w, s, p) cells
+                w.rws0[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+                w.rws1[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                R[0][c] = 0.f;
+                R[1][c] = 0.f;
+                W[0][c] = 0.f;
+                W[1][c] = 0.f;
+                S[0][c] = 0.f;
+                S[1][c] = 0.f;
+                w.pv[c] = 0.f;
+            }
         }
     }
     // block offset = FLUID count of all earlier blocks (fixed order), total = all blocks

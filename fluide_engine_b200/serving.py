@@ -47,7 +47,7 @@ def scene_bytes(n, particles, solver):
     """Device bytes of one scene (allocation plan of fe_scene.cu): grid, solver vectors and particles."""
     cells = n ** 3
     faces = 3 * (n + 1) * n * n
-    grid = faces * (5 * 4 + 3) + cells * (1 + 8 + 8 + 8 * 4 + 4 + 4 + 4) + (cells // 512 + 1) * 512 * 8
+    grid = faces * (5 * 4 + 3) + cells * (1 + 8 + 8 + 9 * 4 + 4 + 4 + 4) + (cells // 512 + 1) * 512 * 8
     grid += cells * 13 // 7  # multigrid levels: mask + residual + correction + scratch per coarse cell (cells / 7)
     per_particle = 2 * (7 + (9 if solver == _abi.APIC else 0)) * 4 + 3 * 4 + 9 * 4 + 4
     return grid + particles * per_particle
