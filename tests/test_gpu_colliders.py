@@ -154,3 +154,32 @@ def test_collider_scene_rules():
     assert e.num_particles() == expect
     e.clear_colliders()
     e.set_viscosity(0.1)
+
+
+def test_collider_outside_the_domain_tracks_oracle():
+    """A collider with no face inside the domain: its fixed face lists are empty (no boundary-condition passes run)
+    and the substeps still track the oracle."""
+    n = (16, 16, 16)
+    V, T, N = with_face_normals(*box((1.3, 1.2, 1.25), (1.6, 1.7, 1.5)))
+    pos, _ = fe.seed_regions([dict(kind=0, lo=(0.0, 0.0, 0.0), hi=(0.4, 0.6, 1.0))], n, (0, 0, 0), (1, 1, 1), 5)
+    rng = np.random.default_rng(5)
+    vel = (rng.standard_normal(pos.shape) * 0.3).astype(np.float32)
+    C = np.zeros((pos.shape[0], 9), dtype=np.float32)
+    g = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-8)
+    o = oracle.OracleSim(n, fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-10, cg_max_it=20000)
+    h = (1.0 / 16,) * 3
+    g.add_mesh_collider(V, T, N, n, (0.0, 0.0, 0.0), h)
+    o.add_mesh_collider(V, T, N, n, (0.0, 0.0, 0.0), h)
+    g.set_particles(pos, vel, C)
+    o.set_particles(pos.astype(np.float64), vel.astype(np.float64), C.astype(np.float64))
+    dt = 1 / 120
+    for _ in range(3):
+        st = g.step(dt, 1)
+        o.substep(dt)
+        assert st[0]["converged"] == 1
+        assert np.array_equal(g.grid()[4], o.marks())
+    assert (g.collider_sdf() > 0).all()  # nothing of the domain is inside the collider
+    P, V1, _ = g.particles()
+    Po, Vo, _ = o.particles()
+    assert rel_l2(P, Po) < 1e-5
+    assert rel_l2(V1, Vo) < 1e-4
