@@ -36,7 +36,7 @@ EXPORTS = [
     "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
-    "fe_abi_version",
+    "fe_abi_version", "fe_debug_set_barrier_limits",
 ]
 
 
@@ -152,6 +152,7 @@ def lib():
     L.fe_batch_step_profiled.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats),
                                          ctypes.POINTER(ctypes.c_float)]
     L.fe_kernel_launch_count.restype = ctypes.c_uint64
+    L.fe_debug_set_barrier_limits.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
     L.fe_seed_regions.restype = ctypes.c_uint64
     L.fe_seed_regions.argtypes = [P, ctypes.c_int32, P, P, P, ctypes.c_uint64, P, P, ctypes.c_uint64]
     L.fe_last_error.restype = ctypes.c_char_p
@@ -189,6 +190,12 @@ def ptr(a):
 
 def kernel_launch_count():
     return int(lib().fe_kernel_launch_count())
+
+
+def set_barrier_limits(spin_limit=0, extra_arrivals=0):
+    """Failure-detection test hook: the pressure solvers' bounded barrier wait on the current device
+    (fe_debug_set_barrier_limits; spin_limit 0 and extra_arrivals 0 restore normal operation)."""
+    check(lib().fe_debug_set_barrier_limits(int(spin_limit), int(extra_arrivals)))
 
 
 def seed_regions(regions, n, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), seed=0):

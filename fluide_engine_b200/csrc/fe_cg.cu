@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(kMultiThreads) k_multi_cg(MultiCgScene* __rest
     prm.max_refine = m.max_refine;
     prm.stats_ring = m.work.stats;
     prm.stats_counter = m.work.bar + 2;
-    prm.stats_cap = 1u << 16;
+    prm.stats_cap = m.work.stats_cap;
     int its = 0, fluid = 0;
     const int blk = (int)blockIdx.x - m.block_start;
     __shared__ SolverSmem smem;
@@ -276,6 +276,14 @@ __global__ void k_multi_partition(MultiCgScene* __restrict__ scenes, int S, int 
 }
 
 }  // namespace
+
+cudaError_t set_solver_barrier_limits(unsigned long long spin_limit, unsigned extra_arrivals)
+{
+    const unsigned long long lim = spin_limit ? spin_limit : kSpinLimit;
+    cudaError_t e = cudaMemcpyToSymbol(c_spin_limit, &lim, sizeof(lim));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(c_extra_arrivals, &extra_arrivals, sizeof(extra_arrivals));
+}
 
 cudaError_t multi_cg_capacity(int device, int* max_blocks, int* threads)
 {
@@ -365,7 +373,7 @@ cudaError_t launch_mgcg(const SceneView& v, const CgWork& w, const MgWork& mg, d
     prm.max_refine = max_refine;
     prm.stats_ring = w.stats;
     prm.stats_counter = (unsigned*)(w.bar + 2);
-    prm.stats_cap = 1u << 16;
+    prm.stats_cap = w.stats_cap;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)w.blocks);
     cfg.blockDim = dim3((unsigned)w.threads);
@@ -390,7 +398,7 @@ cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, doubl
     prm.max_refine = max_refine;
     prm.stats_ring = w.stats;
     prm.stats_counter = (unsigned*)(w.bar + 2);
-    prm.stats_cap = 1u << 16;
+    prm.stats_cap = w.stats_cap;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)w.blocks);
     cfg.blockDim = dim3((unsigned)w.threads);

@@ -27,6 +27,8 @@ constexpr int kCgBarWords = 64;
 // per-block FLUID counts of the solver's setup.
 constexpr size_t cg_partial_doubles(size_t max_blocks) { return 16 + max_blocks; }
 constexpr int kBatchMaxScenes = 64;
+// Entries of a scene's device ring of solve statistics (one per pressure solve; solves wrap around it).
+constexpr unsigned kStatsRingEntries = 1u << 16;
 
 struct GridDims {
     int nx, ny, nz;
@@ -233,10 +235,14 @@ struct CgWork {
     double* partial;        // [0, 12) three rotating reduction totals slots, [16, 16 + max blocks) FLUID counts
     unsigned* bar;          // kCgBarWords barrier words
     int* err;
-    fe_step_stats* stats;   // device
+    fe_step_stats* stats;   // device ring of solve statistics
+    unsigned stats_cap;     // entries of that ring (solves wrap around it)
     int blocks, threads;
 };
 cudaError_t cg_prepare(CgWork& w, int device);
+// Bounded-wait limits of the pressure solvers' grid barrier on the current device (spin_limit 0: the default;
+// extra_arrivals > 0 makes every barrier wait for blocks that do not exist, so each wait runs out).
+cudaError_t set_solver_barrier_limits(unsigned long long spin_limit, unsigned extra_arrivals);
 
 // Multigrid hierarchy of the MG-preconditioned solver (fe_mg_body.cuh): level 0 is the scene grid, whose
 // vectors are the solver's own (CgWork); level l >= 1 halves every axis of level l-1 (rounding up) until

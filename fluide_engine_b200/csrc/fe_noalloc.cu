@@ -2,21 +2,26 @@
 //
 // Who needs this: code that must not call cudaMalloc / cudaFree (or anything that allocates) on the
 // path where it projects a velocity field -- for example a host application's per-frame callback or
-// a real-time loop where cudaMalloc's implicit device synchronisation would stall the frame, a caller
+// a real-time loop where cudaMalloc's implicit device synchronisation would stall the frame, or a caller
 // whose device memory is owned by another allocator (a framework's caching allocator or a fixed arena)
-// that must not see foreign allocations, or a caller preparing work while a CUDA stream is being
-// captured.  Such callers pass their own device buffers for the inputs and outputs; every scratch byte
-// the solver needs lives in one file-scope __device__ array, sized for at most kMaxCells cells.
+// that must not see foreign allocations.  Such callers pass their own device buffers for the inputs and
+// outputs; every scratch byte the solver needs lives in one file-scope __device__ array, sized for at
+// most kMaxCells cells, which every device that loads the library holds until the process exits.
 //
 // The array is reached from host code only through cudaGetSymbolAddress: its name in host code is a
 // host-side stand-in, not a device address.  The first call on each device (with that device current)
-// resolves the address once and caches it; make that first call before any stream capture begins.
-// All calls on a device share the one array and it keeps the previous call's contents: what must start
-// at zero (barrier words, reduction totals, error flag, statistics counter) is cleared on the caller's stream at the start
-// of every call, and calls whose work overlaps on the GPU (different streams, or host threads issuing
-// concurrently) race on the array -- serialise them on one stream.
+// resolves the address and caches it together with the current context's id; a call that finds a
+// different context (after cudaDeviceReset, say) resolves it again.  Make that first call before any
+// stream capture begins.  Each call ends by reading the solve's status back and synchronising the
+// stream it was given.  All calls on a device share the one array and it keeps the previous call's
+// contents: what must start at zero (barrier words, reduction totals, error flag, statistics counter) is
+// cleared on the caller's stream at the start of every call, and calls whose work overlaps on the GPU
+// (different streams, or host threads issuing concurrently) race on the array -- serialise them on one
+// stream.
 //
 // It runs exactly the kernels of the scene path's pressure stage (K_rhs, the persistent K_cg, K_apply).
+#include <cuda.h>
+
 #include <cstring>
 #include <mutex>
 
@@ -44,14 +49,49 @@ static __device__ __align__(256) unsigned char g_project_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-unsigned char* g_scratch_ptr[kMaxDevices] = {};
-CgWork g_work[kMaxDevices] = {};
+struct ScratchSlot {
+    unsigned long long ctx_id;  // context the address was resolved in (0: not yet)
+    unsigned char* base;
+    CgWork work;
+};
+ScratchSlot g_slot[kMaxDevices] = {};
 
-// Resolves the scratch array's device address for `dev` (current) once; no allocation.
-fe_status scratch_for(int dev, CgWork* out)
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the calling thread's current context (unique for the life of the process), through the driver
+// entry points the runtime hands out; 0 when it cannot be told.
+unsigned long long current_context_id()
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (CtxGetCurrentFn)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)f;
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Set-up for `dev` (current): resolves the scratch array's device address and lays the solver's buffers
+// out in it; done again when the device's context has changed since.  No allocation.
+fe_status scratch_for(int dev, CgWork* out, unsigned char** base_out)
 {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    ScratchSlot& slot = g_slot[dev];
+    if (slot.ctx_id == 0 || ctx == 0 || slot.ctx_id != ctx) {
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_project_scratch);
         if (e != cudaSuccess || !ptr) return cuda_check(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "cudaGetSymbolAddress");
@@ -72,10 +112,13 @@ fe_status scratch_for(int dev, CgWork* out)
         w.bar = (unsigned*)(base + kOffBar);
         w.err = (int*)(base + kOffErr);
         w.stats = (fe_step_stats*)(base + kOffStats);
-        g_work[dev] = w;
-        g_scratch_ptr[dev] = base;
+        w.stats_cap = kStatsRing;
+        slot.work = w;
+        slot.base = base;
+        slot.ctx_id = ctx;
     }
-    *out = g_work[dev];
+    *out = slot.work;
+    *base_out = slot.base;
     return FE_OK;
 }
 
@@ -103,10 +146,10 @@ extern "C" fe_status fe_project_noalloc(const int32_t n[3], const double h[3], c
     FE_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return set_error(FE_ERR_BAD_ARG, "device ordinal %d unsupported", dev);
     CgWork work;
-    fe_status st = scratch_for(dev, &work);
+    unsigned char* base = nullptr;
+    fe_status st = scratch_for(dev, &work, &base);
     if (st != FE_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned char* base = g_scratch_ptr[dev];
 
     SceneView view;
     memset(&view, 0, sizeof(view));

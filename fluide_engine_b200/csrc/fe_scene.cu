@@ -403,8 +403,9 @@ fe_status alloc_grid(fe_scene* s)
     FE_CUDA(cudaMemsetAsync(w.bar, 0, kCgBarWords * sizeof(unsigned), st));
     FE_CUDA(dalloc(L, &w.err, 1, dev, st));
     FE_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
-    FE_CUDA(dalloc(L, &s->stats_ring, (size_t)1 << 16, dev, st));
+    FE_CUDA(dalloc(L, &s->stats_ring, (size_t)kStatsRingEntries, dev, st));
     w.stats = s->stats_ring;
+    w.stats_cap = kStatsRingEntries;
     FE_CUDA(dalloc(L, &s->d_scalar, 4, dev, st));
     // marking tables
     const int n[3] = {nx, ny, nz};
@@ -1222,14 +1223,14 @@ fe_status fe_scene_step(fe_scene* s, double dt, int32_t nsub, fe_step_stats* sta
         // the ring holds the solved substeps in order; a skipped substep reports a converged empty solve
         int solved = 0;
         for (int i = 0; i < nsub; ++i) solved += !skipped[i];
-        std::vector<fe_step_stats> ring((size_t)std::min(solved, 1 << 16));
+        std::vector<fe_step_stats> ring((size_t)std::min(solved, (int)kStatsRingEntries));
         if (!ring.empty())
             FE_CUDA(cudaMemcpyAsync(ring.data(), s->stats_ring, ring.size() * sizeof(fe_step_stats), cudaMemcpyDeviceToHost,
                                     s->stream));
         fe_status st = check_device_error(s);
         if (st != FE_OK) return st;
         size_t k = 0;
-        for (int i = 0; i < std::min(nsub, 1 << 16); ++i) {
+        for (int i = 0; i < std::min(nsub, (int)kStatsRingEntries); ++i) {
             fe_step_stats e{};
             e.converged = 1;
             stats[i] = skipped[i] ? e : ring[k++ % std::max<size_t>(ring.size(), 1)];
@@ -1237,7 +1238,7 @@ fe_status fe_scene_step(fe_scene* s, double dt, int32_t nsub, fe_step_stats* sta
         return FE_OK;
     }
     if (stats && nsub > 0) {
-        const int cnt = std::min(nsub, 1 << 16);
+        const int cnt = std::min(nsub, (int)kStatsRingEntries);
         FE_CUDA(cudaMemcpyAsync(stats, s->stats_ring, cnt * sizeof(fe_step_stats), cudaMemcpyDeviceToHost, s->stream));
         fe_status st = check_device_error(s);
         if (st != FE_OK) return st;
@@ -1267,7 +1268,7 @@ fe_status fe_scene_step_profiled(fe_scene* s, double dt, int32_t nsub, fe_step_s
     for (auto& e : ev) cudaEventDestroy(e);
     if (st != FE_OK) return st;
     if (stats && nsub > 0) {
-        const int cnt = std::min(nsub, 1 << 16);
+        const int cnt = std::min(nsub, (int)kStatsRingEntries);
         FE_CUDA(cudaMemcpyAsync(stats, s->stats_ring, cnt * sizeof(fe_step_stats), cudaMemcpyDeviceToHost, s->stream));
     }
     return check_device_error(s);
@@ -2081,6 +2082,13 @@ fe_status fe_scene_synchronize(fe_scene* s)
 
 uint64_t fe_kernel_launch_count(void) { return g_launches.load(); }
 
+fe_status fe_debug_set_barrier_limits(uint64_t spin_limit, uint32_t extra_arrivals)
+{
+    if (extra_arrivals > 1024u) return set_error(FE_ERR_BAD_ARG, "extra_arrivals must be at most 1024");
+    FE_CUDA(set_solver_barrier_limits((unsigned long long)spin_limit, (unsigned)extra_arrivals));
+    return FE_OK;
+}
+
 uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[3], const double origin[3],
                          const double size[3], uint64_t seed, float* pos, float* vel, uint64_t cap)
 {
@@ -2092,7 +2100,7 @@ uint64_t fe_seed_regions(const void* regions, int32_t nregions, const int32_t n[
 
 const char* fe_last_error(void) { return g_err; }
 
-int32_t fe_abi_version(void) { return 10500; }
+int32_t fe_abi_version(void) { return 10600; }
 
 }  // extern "C"
 
@@ -2441,7 +2449,7 @@ fe_status fe_batch_step_profiled(fe_batch* b, double dt, int32_t nsub, fe_step_s
         if (cst != FE_OK) return cst;
     }
     if (stats && nsub > 0) {
-        const int cnt = std::min(nsub, 1 << 16);
+        const int cnt = std::min(nsub, (int)kStatsRingEntries);
         for (int i = 0; i < S; ++i)
             FE_CUDA(cudaMemcpy(stats + (size_t)i * nsub, b->scenes[i]->stats_ring, cnt * sizeof(fe_step_stats),
                                cudaMemcpyDeviceToHost));
@@ -2497,7 +2505,7 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
         if (st != FE_OK) return st;
     }
     if (stats && nsub > 0) {
-        const int cnt = std::min(nsub, 1 << 16);
+        const int cnt = std::min(nsub, (int)kStatsRingEntries);
         for (int i = 0; i < S; ++i)
             FE_CUDA(cudaMemcpy(stats + (size_t)i * nsub, b->scenes[i]->stats_ring, cnt * sizeof(fe_step_stats),
                                cudaMemcpyDeviceToHost));

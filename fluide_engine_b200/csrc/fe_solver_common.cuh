@@ -13,6 +13,13 @@ namespace {
 constexpr int kListCache = 8192;  // FLUID-list entries cached in shared memory per block (32 KB)
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
+// Limits of the bounded grid-barrier wait, in constant memory (one copy per translation unit that includes this
+// header): the polls a block makes before it gives up with FE_ERR_TIMEOUT, and arrivals the barrier waits for
+// beyond the blocks of the launch.  In normal operation they are kSpinLimit and 0; the failure-detection test
+// hook (fe_debug_set_barrier_limits) sets a short limit and one extra arrival, so every wait runs out.
+__constant__ unsigned long long c_spin_limit = kSpinLimit;
+__constant__ unsigned c_extra_arrivals = 0u;
+
 struct CgParams {
     double rel_tol, inner_tol;
     int max_it, max_refine;
@@ -37,7 +44,7 @@ __device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigne
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
     const unsigned old = count.fetch_add(1u, cuda::memory_order_acq_rel);
-    if (old == nblocks - 1) {
+    if (old == nblocks - 1 + c_extra_arrivals) {
         double* next = totals + 4 * (next_gen(gen) % 3u);
 #pragma unroll
         for (int k = 0; k < 4; ++k) next[k] = 0.0;
@@ -47,8 +54,9 @@ __device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigne
     }
     cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
     unsigned long long spins = 0;
+    const unsigned long long limit = c_spin_limit;
     while (genw.load(cuda::memory_order_acquire) == gen) {
-        if (++spins > kSpinLimit) {
+        if (++spins > limit) {
             e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
             return false;
         }

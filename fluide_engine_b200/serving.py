@@ -41,6 +41,7 @@ class Job:
     frames_done: int = 0
     frame_ms: list = field(default_factory=list)
     seeded: tuple = None        # (pos, vel) once seeded, kept while the job waits for memory
+    cancelled: bool = False     # left before its last frame (Server.cancel); its state is not read back
 
 
 def scene_bytes(n, particles, solver):
@@ -91,9 +92,19 @@ class Server:
         self.timing = collections.defaultdict(float)
         self.rebuilds = 0
         self.reused = 0
+        self.cancelled = []      # jobs that left through cancel(), in the order they left
+        self._cancel = set()     # ids asked to leave, not matched to a job yet
 
     def submit(self, job):
         heapq.heappush(self.waiting, (job.arrival, job.job_id, job))
+
+    def cancel(self, job_id):
+        """Asks job `job_id` to leave; safe from any thread (an on_frame callback included).  A waiting job
+        leaves the queue, a running one leaves at the next frame boundary (no frame of it is cut short: the
+        frame in flight completes for every member), and a job being prepared leaves when it is ready.  Its
+        scene goes back to the pool without a read-back and its memory is released like a finished job's."""
+        with self._lock:
+            self._cancel.add(job_id)
 
     # ---------------------------------------------------------------------------------------- helpers
     def _seed(self, job):
@@ -149,11 +160,11 @@ class Server:
         job.seeded = None
         self.timing["create"] += time.perf_counter() - t
 
-    def _release_job(self, job, now):
+    def _release_job(self, job, now, read_back=True):
         """I/O thread: reads back a finished job and returns its scene to the pool (or frees it)."""
         t = time.perf_counter()
         job.finished_at = now
-        job.final = job.scene.particles()
+        job.final = job.scene.particles() if read_back else None
         scene, job.scene = job.scene, None
         if self.reuse_scenes:
             with self._lock:
@@ -259,7 +270,33 @@ class Server:
                                 self._releasing += 1
                             releases.append(io.submit(self._release_job, j, done_at))
                             self.done.append(j)
-                changed = bool(finished) or bool(ready)
+                with self._lock:
+                    asked = set(self._cancel)
+                gone = []
+                if asked:
+                    # cancelled jobs leave at this frame boundary: waiting ones drop out of the queue, running
+                    # and just-prepared ones release their scenes like finished jobs, without a read-back
+                    keep = [e for e in self.waiting if e[2].job_id not in asked]
+                    gone = [e[2] for e in self.waiting if e[2].job_id in asked]
+                    if gone:
+                        self.waiting = keep
+                        heapq.heapify(self.waiting)
+                    leaving = [j for j in self.running + ready if j.job_id in asked]
+                    if leaving:
+                        self.running = [j for j in self.running if j.job_id not in asked]
+                        ready = [j for j in ready if j.job_id not in asked]
+                        done_at = time.perf_counter() - t0
+                        for j in leaving:
+                            with self._lock:
+                                self._releasing += 1
+                            releases.append(io.submit(self._release_job, j, done_at, False))
+                    gone += leaving
+                    for j in gone:
+                        j.cancelled = True
+                        self.cancelled.append(j)
+                    with self._lock:
+                        self._cancel -= {j.job_id for j in gone}
+                changed = bool(finished) or bool(ready) or bool(gone)
                 self.running.extend(ready)
                 if not self.running:
                     if self.preparing:

@@ -4,9 +4,9 @@ Same class and method names as the reference's pybind11 module PyFluidEngine
 (python_wrapper/simulators_wrapper.cu:36-85, frame_wrapper.cpp, vector3_wrapper.cpp,
 bounding_box_3d_wrapper.cpp, exteranl_forces_wrapper.cpp) and C++ classes (pic_simulator.hpp:27-43,
 hybrid_simulator.hpp:10-41, physics_animation.hpp:8-19, flip_simulator.hpp:9-16), backed by one
-device-resident Scene.  Only what the substep needs is implemented; entry points of components outside
-it (mesh initialisation, colliders, emitters) raise NotImplementedError
-with the reason instead of silently doing something else.
+device-resident Scene: the substep, mesh initialisation, emitters, external forces, triangle-mesh
+colliders, viscosity and the fluid surface.  Invalid arguments raise ValueError / TypeError with the
+reason, and library errors raise FluideError carrying the C ABI status.
 """
 import numpy as np
 

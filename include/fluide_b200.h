@@ -297,15 +297,16 @@ fe_status fe_scene_divergence(fe_scene* s, double* l2);
 
 /* Pressure projection of a caller-owned MAC grid that allocates no device memory.  No counterpart in
  * the reference: it exists for callers that cannot call cudaMalloc/cudaFree on this path (a per-frame or
- * real-time callback where an allocation's implicit device synchronisation would stall, memory owned by
- * another allocator, or setup that runs while a stream is being captured).  All pointers except n, h and
- * stats are device pointers: marks (nx*ny*nz, FE_CELL_*), u/v/w (face arrays, updated in place),
- * p (pressure, warm start in, solution out).  Runs the scene path's pressure stage (rhs, CG in FP64
- * refinement to rel_tol, apply) on `stream` (NULL = legacy default stream) and synchronises it.
- * Scratch lives in one static device array of about 11.6 MB per device, so grids are limited to 2^18
- * cells (e.g. 64^3); larger grids return FE_ERR_BAD_ARG.  The first call on a device resolves the
- * array's address (cudaGetSymbolAddress) and must come before any stream capture.  Calls share the
- * array: calls that overlap on the GPU race, so issue them on one stream.  stats (host) may be NULL. */
+ * real-time callback where an allocation's implicit device synchronisation would stall, or memory owned by
+ * another allocator).  All pointers except n, h and stats are device pointers: marks (nx*ny*nz, FE_CELL_*),
+ * u/v/w (face arrays, updated in place), p (pressure, warm start in, solution out).  Runs the scene path's
+ * pressure stage (rhs, CG in FP64 refinement to rel_tol, apply) on `stream` (NULL = legacy default stream),
+ * then reads the status back and synchronises that stream.  Scratch lives in one static device array of
+ * about 11.6 MB per device (held until the process exits), so grids are limited to 2^18 cells (e.g. 64^3);
+ * larger grids return FE_ERR_BAD_ARG.  The first call on a device (and the first after its context was
+ * replaced, e.g. by cudaDeviceReset) resolves the array's address (cudaGetSymbolAddress); make it before any
+ * stream capture begins.  Calls share the array and it keeps the last call's contents: calls that overlap on
+ * the GPU race, so issue them on one stream.  stats (host) may be NULL. */
 fe_status fe_project_noalloc(const int32_t n[3], const double h[3], const uint8_t* marks, float* u, float* v,
                              float* w, double* p, double rel_tol, int32_t max_it, void* stream,
                              fe_step_stats* stats);
@@ -337,6 +338,15 @@ fe_status fe_batch_step_profiled(fe_batch* b, double dt, int32_t nsub, fe_step_s
 
 /* Number of kernels the library launched since load (counts graph-launched kernels too). */
 uint64_t fe_kernel_launch_count(void);
+
+/* Failure-detection test hook (no reference counterpart: the reference has no error handling).  Sets, for the
+ * current device, the bounded wait of the pressure solvers' grid barrier: spin_limit polls before a block gives
+ * up (0 restores the default, a few seconds of polling), and extra_arrivals, arrivals the barrier waits for
+ * beyond the launched blocks (0 in normal operation).  With extra_arrivals = 1 no barrier can complete: every
+ * waiting block gives up after spin_limit polls, the solve ends, and the step returns FE_ERR_TIMEOUT with the
+ * context usable; the scene's barrier words are reset, so once the limits are restored it steps normally.
+ * Applies to launches (and graph replays) issued after the call. */
+fe_status fe_debug_set_barrier_limits(uint64_t spin_limit, uint32_t extra_arrivals);
 
 /* Deterministic seeding of analytic box / sphere regions (subcell-centre rule).  Region layout:
  * {int32 kind (0 box, 1 sphere); double lo[3]; double hi[3] (sphere: hi[0] = radius); double vel[3]}.

@@ -129,6 +129,7 @@ def lib():
         L.or_add_mesh_collider.argtypes = [P, D, ctypes.c_size_t, I64, ctypes.c_size_t, D, ctypes.c_size_t, I3, D, D]
         L.or_build_collider.argtypes = [P]
         L.or_get_collider_sdf.argtypes = [P, D]
+        L.or_set_enclosed_projection.argtypes = [P, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -286,6 +287,11 @@ class OracleSim:
 
     def rhs(self):
         b = self._cells(np.float64); self.L.or_get_rhs(self.h, dptr(b)); return b
+
+    def set_enclosed_projection(self, on=True):
+        """Not the reference: with colliders, solve enclosed FLUID components the way the GPU does (all-zero
+        rows become identity rows, each component without an AIR neighbour loses its right-hand-side mean)."""
+        self.L.or_set_enclosed_projection(self.h, 1 if on else 0)
 
     def add_mesh_collider(self, V, T, N, n, origin, h):
         """TriangleMeshCollider of a mesh (V (nv,3), T (nt,4) int64 with normal ids into N (nn,3)) on its own grid."""

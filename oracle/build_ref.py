@@ -1,7 +1,8 @@
 """Build recipe for oracle/_ref/ -- TEST INFRASTRUCTURE ONLY.
 
 Compiles the reference's own CPU simulator (AleksanderSiwek/Fluide_Engine, src/) from the sources
-where they lie under /root/reference, together with oracle/ref_harness.cpp, into two shared
+where they lie (the reference checkout named by FE_REFERENCE_SRC, else the `reference_path` entry of the
+repository's BASELINE.json, + "/src"), together with oracle/ref_harness.cpp, into two shared
 libraries under oracle/_ref/ (git-ignored):
 
 * libfe_ref_serial.so   -- parallel_utils loops run on the calling thread (use_threads=false).  The
@@ -33,7 +34,22 @@ import tempfile
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("FE_REFERENCE_SRC", "/root/reference/src")
+def _reference_src():
+    """Reference source tree: $FE_REFERENCE_SRC, else BASELINE.json's reference_path + /src (None if neither)."""
+    env = os.environ.get("FE_REFERENCE_SRC")
+    if env:
+        return env
+    try:
+        import json
+
+        with open(os.path.join(os.path.dirname(HERE), "BASELINE.json")) as f:
+            base = json.load(f).get("reference_path")
+    except (OSError, ValueError):
+        base = None
+    return os.path.join(base, "src") if base else None
+
+
+REF = _reference_src()
 OUT = os.path.join(HERE, "_ref")
 CXX = os.environ.get("FE_REF_CXX", "g++")  # the system g++; a $CXX that links libstdc++ statically breaks loading next to numpy
 FLAGS = ["-std=c++17", "-O3", "-fPIC", "-ffp-contract=off", "-fpermissive", "-w", "-pthread"]
@@ -107,7 +123,7 @@ def _build_variant(name, threaded):
 
 def build(force=False):
     """Builds both variants when the reference sources are present; returns the list of built libraries."""
-    if not os.path.isdir(REF):
+    if not REF or not os.path.isdir(REF):
         return []
     os.makedirs(OUT, exist_ok=True)
     built = []

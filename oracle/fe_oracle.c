@@ -79,6 +79,7 @@ struct or_sim {
     or_collider colliders[OR_MAX_COLLIDERS];
     int ncolliders;
     double* csdf;             /* ColliderCollection::_sdf on the n nodes at the domain origin; initially 0 */
+    int enclosed_projection;  /* restate the GPU's treatment of enclosed FLUID components (off: the reference) */
 };
 
 /* ---------------------------------------------------------------- math_utils.hpp restatements */
@@ -848,6 +849,74 @@ int or_project(const int nn[3], const double h[3], const uint8_t* marks, double*
 
 /* PICSimulator::ComputePressure (pic_simulator.cpp:224-229) -> SinglePhasePressureSolver::Solve
  * (fluid_solvers/single_phase_pressure_solver.cpp:21-28), then ApplyBoundryCondition. */
+/* Not the reference: the GPU's solvable form of a collider scene's system (enabled by
+ * or_set_enclosed_projection; the default follows the reference).  With colliders, FLUID cells can form
+ * components that touch no AIR cell (pure-Neumann blocks walled in by BOUNDRY cells and domain walls),
+ * whose rows the reference leaves singular and, in general, inconsistent, so its CG cannot converge there.
+ * (1) A FLUID cell with no in-domain non-BOUNDRY neighbour has an all-zero row: it becomes an identity row
+ * with b = 0 (pressure 0; ApplyPressure never reads it toward a BOUNDRY or out-of-domain face).
+ * (2) FLUID cells are grouped into 6-connected components; a component without an AIR neighbour loses the
+ * mean of its right-hand side, which leaves a consistent block unchanged and makes an inconsistent one
+ * solvable.  Components are found by a union-find over the FLUID cells in cell order. */
+static size_t uf_find(size_t* parent, size_t x)
+{
+    while (parent[x] != x) {
+        parent[x] = parent[parent[x]];
+        x = parent[x];
+    }
+    return x;
+}
+
+static void project_enclosed(dim3i n, const uint8_t* m, row4* A, double* b, double* p)
+{
+    size_t N = cnt3(n);
+    size_t* parent = (size_t*)malloc(N * sizeof(size_t));
+    uint8_t* open = (uint8_t*)calloc(N, 1);
+    double* sum = (double*)calloc(N, sizeof(double));
+    size_t* cnt = (size_t*)calloc(N, sizeof(size_t));
+    for (size_t c = 0; c < N; ++c) parent[c] = c;
+    for (int i = 0; i < n.x; ++i)
+        for (int j = 0; j < n.y; ++j)
+            for (int k = 0; k < n.z; ++k) {
+                size_t c = ix3(n, i, j, k);
+                if (m[c] != OR_FLUID) continue;
+                if (A[c].c == 0.0) { /* (1) all-zero row */
+                    A[c].c = 1.0;
+                    A[c].r = A[c].u = A[c].f = 0.0;
+                    b[c] = 0.0;
+                    p[c] = 0.0;
+                }
+                size_t nb[3] = {i + 1 < n.x ? ix3(n, i + 1, j, k) : c, j + 1 < n.y ? ix3(n, i, j + 1, k) : c,
+                                k + 1 < n.z ? ix3(n, i, j, k + 1) : c};
+                for (int q = 0; q < 3; ++q) {
+                    if (nb[q] == c || m[nb[q]] != OR_FLUID) continue;
+                    size_t ra = uf_find(parent, c), rb = uf_find(parent, nb[q]);
+                    if (ra != rb) parent[ra > rb ? ra : rb] = ra < rb ? ra : rb;
+                }
+            }
+    for (int i = 0; i < n.x; ++i)
+        for (int j = 0; j < n.y; ++j)
+            for (int k = 0; k < n.z; ++k) {
+                size_t c = ix3(n, i, j, k);
+                if (m[c] != OR_FLUID) continue;
+                size_t r = uf_find(parent, c);
+                if ((i > 0 && m[ix3(n, i - 1, j, k)] == OR_AIR) || (i + 1 < n.x && m[ix3(n, i + 1, j, k)] == OR_AIR) ||
+                    (j > 0 && m[ix3(n, i, j - 1, k)] == OR_AIR) || (j + 1 < n.y && m[ix3(n, i, j + 1, k)] == OR_AIR) ||
+                    (k > 0 && m[ix3(n, i, j, k - 1)] == OR_AIR) || (k + 1 < n.z && m[ix3(n, i, j, k + 1)] == OR_AIR))
+                    open[r] = 1;
+                sum[r] += b[c];
+                cnt[r] += 1;
+            }
+    for (size_t c = 0; c < N; ++c) {
+        if (m[c] != OR_FLUID) continue;
+        size_t r = uf_find(parent, c);
+        if (!open[r]) b[c] -= sum[r] / (double)cnt[r];
+    }
+    free(parent); free(open); free(sum); free(cnt);
+}
+
+void or_set_enclosed_projection(or_sim* s, int on) { s->enclosed_projection = on ? 1 : 0; }
+
 void or_stage_pressure(or_sim* s, double dt)
 {
     (void)dt; /* neither dt nor density enters the solve (single_phase_pressure_solver.cpp:59-60) */
@@ -855,6 +924,7 @@ void or_stage_pressure(or_sim* s, double dt)
     size_t N = cnt3(s->n);
     row4* A = (row4*)malloc(N * sizeof(row4));
     build_system(s->n, s->h, s->marks, s->u, s->v, s->w, A, s->b);
+    if (s->enclosed_projection && s->ncolliders > 0) project_enclosed(s->n, s->marks, A, s->b, s->p);
     s->cg_it = cg_solve(A, s->b, s->p, s->n, s->d.cg_rel_tol, s->d.cg_max_it);
     s->cg_res = true_rel_residual(A, s->b, s->p, s->n);
     apply_pressure(s->n, s->h, s->marks, s->p, s->u, s->v, s->w);

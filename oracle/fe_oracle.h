@@ -56,6 +56,9 @@ void or_get_grid(const or_sim* s, double* u, double* v, double* w);
 void or_set_grid(or_sim* s, const double* u, const double* v, const double* w);
 void or_get_pressure(const or_sim* s, double* p);
 void or_set_pressure(or_sim* s, const double* p);
+/* Not the reference: with colliders, give enclosed FLUID components (no AIR neighbour) a solvable system the
+ * way the GPU does (all-zero rows -> identity, right-hand-side mean removed per enclosed component). */
+void or_set_enclosed_projection(or_sim* s, int on);
 void or_get_marks(const or_sim* s, uint8_t* marks);
 void or_get_sdf(const or_sim* s, double* sdf);
 void or_get_face_markers(const or_sim* s, uint8_t* mu, uint8_t* mv, uint8_t* mw);

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_string():
     L = fe.lib()
-    assert L.fe_abi_version() == 10500
+    assert L.fe_abi_version() == 10600
     assert isinstance(L.fe_last_error(), bytes)
 
 

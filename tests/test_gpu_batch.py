@@ -36,18 +36,30 @@ def test_batch_matches_scenes_alone():
     dt = 1.0 / 240.0
     alone = [make(sp, i) for i, sp in enumerate(SPECS)]
     mixed = [make(sp, i) for i, sp in enumerate(SPECS)]
-    for s in alone:
-        s.step(dt, 4)
     batch = fe.Batch(mixed)
-    stats = batch.step(dt, 4)
+    # first substep: both runs mark cells from identical particles, so the marks are bit-identical
+    for s in alone:
+        s.step(dt, 1)
+    stats1 = batch.step(dt, 1)
+    for a, m in zip(alone, mixed):
+        assert np.array_equal(a.grid()[4], m.grid()[4])
+    for s in alone:
+        s.step(dt, 3)
+    stats = batch.step(dt, 3)
     batch.close()
-    for a, m, st in zip(alone, mixed, stats):
-        assert all(x["converged"] == 1 and x["rel_residual"] <= 1e-6 for x in st), st
+    for a, m, st1, st in zip(alone, mixed, stats1, stats):
+        assert all(x["converged"] == 1 and x["rel_residual"] <= 1e-6 for x in st1 + st), st
         Pa, Va, _ = a.particles()
         Pm, Vm, _ = m.particles()
         assert rel_l2(Pm, Pa) < 1e-5
         assert rel_l2(Vm, Va) < 1e-4
-        assert np.array_equal(a.grid()[4], m.grid()[4]) or rel_l2(m.grid()[0], a.grid()[0]) < 1e-4
+        # later substeps mark from positions that differ in the last bits (the solves' dot products are
+        # summed in a different order with a different block split, and P2G flushes with float atomics), so
+        # a cell whose nearest particle sits within rounding of the marking radius may flip: at most a
+        # handful of cells, never a systematic difference
+        ma, mm = a.grid()[4], m.grid()[4]
+        differ = int((ma != mm).sum())
+        assert differ <= max(2, int(5e-4 * (ma == fe.FLUID).sum())), differ
 
 
 def test_batch_then_single_steps_continue():
@@ -203,3 +215,34 @@ def test_batch_with_multigrid_scenes_matches_alone():
         Pm, Vm, _ = m.particles()
         assert rel_l2(Pm, Pa) < 1e-5
         assert rel_l2(Vm, Va) < 1e-4
+
+
+def test_server_job_cancelled_mid_run_leaves_the_others_unchanged():
+    """A job cancelled while it runs leaves at the next frame boundary; the jobs it ran beside still match the
+    same jobs run alone, and a job cancelled before admission never runs."""
+    regions = [dict(kind=0, lo=(0.0, 0.0, 0.0), hi=(0.4, 0.5, 0.6))]
+    jobs = [serving.Job(job_id=k, n=24 + 8 * (k % 2), solver=(fe.FLIP, fe.APIC, fe.PIC)[k % 3], regions=regions,
+                        frames=5, substeps_per_frame=2, dt=1.0 / 240.0, arrival=0.0 if k < 3 else 30.0, seed=50 + k)
+            for k in range(4)]
+    srv = serving.Server(hbm_budget_bytes=4 << 30, max_batch=4)
+
+    def on_frame(jobs_, ms):
+        if any(j.job_id == 1 and j.frames_done == 2 for j in jobs_):
+            srv.cancel(1)
+            srv.cancel(3)
+
+    for j in jobs:
+        srv.submit(j)
+    srv.run(on_frame=on_frame)
+    assert jobs[1].cancelled and jobs[1].frames_done == 2 and jobs[1].final is None
+    assert jobs[3].cancelled and jobs[3].frames_done == 0
+    for j in (jobs[0], jobs[2]):
+        assert not j.cancelled and j.frames_done == j.frames
+        pos, vel = fe.seed_regions(j.regions, (j.n,) * 3, seed=j.seed)
+        s = fe.Scene((j.n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6)
+        s.set_particles(pos, vel)
+        s.step(j.dt, j.frames * j.substeps_per_frame)
+        P, V, _ = s.particles()
+        assert rel_l2(j.final[0], P) < 1e-5
+        assert rel_l2(j.final[1], V) < 1e-4
+        s.close()

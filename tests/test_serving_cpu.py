@@ -149,3 +149,32 @@ def test_frame_latency_and_arrival_order():
     assert p50 is not None and p99 >= p50 > 0
     admitted = sorted(js, key=lambda j: j.admitted_at)
     assert [j.job_id for j in admitted] == sorted(j.job_id for j in js)
+
+
+def test_cancelled_jobs_leave_and_release_their_memory():
+    """A job cancelled mid-run leaves at the next frame boundary (not read back, scene released); a job cancelled
+    while it waits never runs; the others run all their frames."""
+    js = jobs(6, n=16, frames=6, spacing=0.0)
+    js[5].arrival = 10.0  # still waiting when it is cancelled
+    srv = serving.Server(hbm_budget_bytes=1 << 40, max_batch=4, reuse_scenes=False)
+    frames = []
+
+    def on_frame(jobs_, ms):
+        frames.append({j.job_id for j in jobs_})
+        if any(j.job_id == 1 and j.frames_done == 2 for j in jobs_):
+            srv.cancel(1)   # running: leaves after this frame
+            srv.cancel(5)   # waiting
+
+    for j in js:
+        srv.submit(j)
+    srv.run(on_frame=on_frame)
+    by_id = {j.job_id: j for j in js}
+    assert by_id[1].cancelled and by_id[1].frames_done == 2 and by_id[1].final is None
+    assert by_id[5].cancelled and by_id[5].frames_done == 0 and by_id[5].admitted_at is None
+    assert {j.job_id for j in srv.cancelled} == {1, 5}
+    for i in (0, 2, 3, 4):
+        j = by_id[i]
+        assert not j.cancelled and j.frames_done == j.frames
+        assert np.all(j.final[1] == j.frames * j.substeps_per_frame)
+    assert sum(1 in f for f in frames) == 2
+    assert FakeScene.live == 0 and srv.used == 0
