@@ -211,8 +211,9 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def reference_sample(n, steps, cores_hint=None, viscosity=0.0, collider=False):
-    """Times the reference's own threaded CPU simulator on the workload; returns (value, info)."""
+def reference_sample(n, steps, cores_hint=None, viscosity=0.0, collider=False, warmup=0):
+    """Times the reference's own threaded CPU simulator on the workload: `warmup` untimed substeps from rest, then
+    `steps` timed ones; returns (value, ms per substep, info)."""
     import numpy as np
     import oracle
 
@@ -233,6 +234,10 @@ def reference_sample(n, steps, cores_hint=None, viscosity=0.0, collider=False):
         V, T, Nrm = box_mesh(COLLIDER_BOX)
         sim.add_mesh_collider(V, T, Nrm, (n, n, n), (0.0, 0.0, 0.0), (1.0 / n,) * 3)
     sim.set_particles(pos.astype(np.float64), vel.astype(np.float64))
+    t_warm = time.perf_counter()
+    for _ in range(warmup):
+        sim.substep(DT)
+    t_warm = time.perf_counter() - t_warm
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
@@ -240,10 +245,13 @@ def reference_sample(n, steps, cores_hint=None, viscosity=0.0, collider=False):
         times.append(time.perf_counter() - t0)
     total = sum(times)
     value = pos.shape[0] * steps / total
-    info = {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
-            "sample": "%d substep(s) of the %d^3 FLIP dam break from rest (%d particles)%s%s, %.1f s; host has %d cores"
-                      % (steps, n, pos.shape[0], ", viscosity %g" % viscosity if viscosity else "",
-                         ", box collider" if collider else "", total, cores)}
+    window = ("substep%s %d%s after %d untimed warm-up substep(s) from rest"
+              % ("s" if steps > 1 else "", warmup + 1, "-%d" % (warmup + steps) if steps > 1 else "", warmup)
+              if warmup else "%d substep(s) from rest" % steps)
+    info = {"value": value, "unit": METRIC, "cores": threads, "kind": kind, "window": window,
+            "sample": "%s of the %d^3 FLIP dam break (%d particles)%s%s, %.1f s timed (+%.1f s warm-up); host has %d "
+                      "cores" % (window, n, pos.shape[0], ", viscosity %g" % viscosity if viscosity else "",
+                                 ", box collider" if collider else "", total, t_warm, cores)}
     return value, total / steps * 1e3, info
 
 
@@ -371,12 +379,15 @@ def run_reference_arm(args):
         return 0
     n_gpus = args.gpus
     steps = max(1, min(args.steps, args.ref_steps))
-    value, ms, info = reference_sample(args.n, steps, viscosity=args.viscosity, collider=args.collider)
+    # the same untimed warm-up substeps as the GPU arm, so the timed substep is the first of the GPU arm's window
+    warmup = max(args.warmup, 3)
+    value, ms, info = reference_sample(args.n, steps, viscosity=args.viscosity, collider=args.collider, warmup=warmup)
     particles = int(round(value * ms / 1e3))
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": n_gpus, "steps": steps, "warmup": 0,
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": n_gpus, "steps": steps, "warmup": warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded analytic scene)", "impl": "reference",
-            "config": workload_config(args.n, steps, 0, 1, particles, args.viscosity, args.collider), "cpu_baseline": info,
+            "config": workload_config(args.n, steps, warmup, 1, particles, args.viscosity, args.collider),
+            "window": info["window"], "cpu_baseline": info,
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -455,22 +466,21 @@ def run_pool(args):
     return 0
 
 
-def run_batched(args):
+def batched_measure(n_scenes=48, steps=50, warmup=5, device=0):
     """Batched independent scenes vs the same scenes one at a time on the plain single-scene path.
 
     Scenes: cubic grids drawn from {32,48,64,96,128}, a dam-break block with extents U[0.2,0.6] per axis,
     8 particles per cell, solver drawn from PIC / FLIP(0.95) / APIC (seed 2).  Both arms use the same
-    pressure tolerance (rel 1e-6); times are wall clock around synchronised device work.
+    pressure tolerance (rel 1e-6); times are wall clock around synchronised device work.  Returns a dict.
     """
     import numpy as np
     import torch
 
     import fluide_engine_b200 as fe
 
-    torch.cuda.set_device(0)
     rng = np.random.default_rng(2)
     specs = []
-    for k in range(args.scenes):
+    for k in range(n_scenes):
         n = int(rng.choice([32, 48, 64, 96, 128]))
         ext = rng.uniform(0.2, 0.6, 3)
         solver = int(rng.integers(0, 3))
@@ -480,22 +490,21 @@ def run_batched(args):
         out = []
         for n, solver, ext, k in specs:
             pos, vel = fe.seed_regions([dict(kind=0, lo=(0.0, 0.0, 0.0), hi=ext)], (n, n, n), seed=k)
-            sc = fe.Scene((n, n, n), solver=solver, max_cfl=1.0, cg_rel_tol=1e-6)
+            sc = fe.Scene((n, n, n), solver=solver, max_cfl=1.0, cg_rel_tol=1e-6, device=device)
             sc.set_particles(pos, vel)
             out.append(sc)
         return out
 
-    particles = None
     # one at a time (each scene's own graph-captured substeps, scene after scene)
     scenes = build()
     particles = sum(sc.num_particles() for sc in scenes)
     for sc in scenes:
-        sc.step(DT, args.warmup, stats=False)
+        sc.step(DT, warmup, stats=False)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res_alone = []
     for sc in scenes:
-        st = sc.step(DT, args.steps, stats=True)
+        st = sc.step(DT, steps, stats=True)
         res_alone.append(max(x["rel_residual"] for x in st))
     torch.cuda.synchronize()
     t_alone = time.perf_counter() - t0
@@ -504,11 +513,11 @@ def run_batched(args):
     # batched
     scenes = build()
     batch = fe.Batch(scenes)
-    batch.step(DT, args.warmup, stats=False)
+    batch.step(DT, warmup, stats=False)
     torch.cuda.synchronize()
     launches0 = fe.kernel_launch_count()
     t0 = time.perf_counter()
-    st = batch.step(DT, args.steps, stats=True)
+    st = batch.step(DT, steps, stats=True)
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
     launches = fe.kernel_launch_count() - launches0
@@ -517,38 +526,49 @@ def run_batched(args):
     batch.close()
     for sc in scenes:
         sc.close()
-    v_batch = particles * args.steps / t_batch
-    v_alone = particles * args.steps / t_alone
-    line = {"metric": METRIC, "value": v_batch, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_batch / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 refinement)",
-            "data": "synthetic (seeded analytic scenes)", "workload_kind": "batched",
-            "config": {"workload": "%d batched scenes, n in {32,48,64,96,128}, block extents U[0.2,0.6], "
-                                   "solver U{PIC,FLIP,APIC} (seed 2), dt=1/240, CG rel 1e-6" % len(specs),
-                       "scenes": [[n, ["PIC", "FLIP", "APIC"][sv]] for n, sv, _, _ in specs],
-                       "particles_total": particles, "timing": "wall clock around synchronised device work"},
-            "one_at_a_time": {"value": v_alone, "ms_per_step_all_scenes": t_alone / args.steps * 1e3},
+    v_batch = particles * steps / t_batch
+    v_alone = particles * steps / t_alone
+    return {"value": v_batch, "unit": METRIC, "steps": steps, "warmup": warmup,
+            "ms_per_step": t_batch / steps * 1e3,
+            "workload": "%d batched scenes, n in {32,48,64,96,128}, block extents U[0.2,0.6], solver "
+                        "U{PIC,FLIP,APIC} (seed 2), dt=1/240, CG rel 1e-6, %d substeps after %d warm-up"
+                        % (len(specs), steps, warmup),
+            "scenes": [[n, ["PIC", "FLIP", "APIC"][sv]] for n, sv, _, _ in specs],
+            "particles_total": particles, "timing": "wall clock around synchronised device work",
+            "one_at_a_time": {"value": v_alone, "ms_per_step_all_scenes": t_alone / steps * 1e3},
             "batched_over_one_at_a_time": v_batch / v_alone,
             "accuracy": {"rel_residual_max_batched": max(res_batch), "rel_residual_max_alone": max(res_alone),
                          "converged_all": conv},
             "gpu_launches": int(launches)}
+
+
+def run_batched(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    b = batched_measure(args.scenes, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": b["value"], "unit": METRIC, "n_gpus": 1, "steps": b["steps"],
+            "warmup": b["warmup"], "ms_per_step": b["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 refinement)",
+            "data": "synthetic (seeded analytic scenes)", "workload_kind": "batched",
+            "config": {"workload": b["workload"], "scenes": b["scenes"], "particles_total": b["particles_total"],
+                       "timing": b["timing"]},
+            "one_at_a_time": b["one_at_a_time"], "batched_over_one_at_a_time": b["batched_over_one_at_a_time"],
+            "accuracy": b["accuracy"], "gpu_launches": b["gpu_launches"]}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_served(args):
-    """Served request stream (the served configuration scaled down in duration and resolution; see --trace-*)."""
+def served_measure(rate, seconds, res, fr, budget_gb, max_batch, device=0):
+    """A seeded Poisson trace of APIC pool + sphere jobs served with continuous batching, and the same trace run
+    FIFO one job at a time through the plain single-scene path.  Returns a dict."""
     import numpy as np
-    import torch
 
     import fluide_engine_b200 as fe
     from fluide_engine_b200 import serving
 
-    torch.cuda.set_device(0)
-    res = tuple(int(x) for x in args.trace_res.split(","))
-    fr = tuple(int(x) for x in args.trace_frames.split(","))
-    jobs = serving.poisson_trace(args.trace_rate, args.trace_seconds, 3, resolutions=res, frames=fr)
-    srv = serving.Server(hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), max_batch=args.max_batch)
+    jobs = serving.poisson_trace(rate, seconds, 3, resolutions=res, frames=fr)
+    srv = serving.Server(hbm_budget_bytes=int(budget_gb * 1e9), max_batch=max_batch, device=device)
     for j in jobs:
         srv.submit(j)
     wall, psteps = srv.run()
@@ -564,7 +584,7 @@ def run_served(args):
         t_job = time.perf_counter()
         pos, vel = fe.seed_regions(j.regions, (j.n,) * 3, seed=j.seed)
         t1 = time.perf_counter()
-        sc = fe.Scene((j.n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6)
+        sc = fe.Scene((j.n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6, device=device)
         sc.set_particles(pos, vel)
         t2 = time.perf_counter()
         for _ in range(j.frames):
@@ -583,14 +603,11 @@ def run_served(args):
         alone_split["retire"] += t4 - t3
         clock = start + (time.perf_counter() - t_job)
     t_alone = clock
-    line = {"metric": METRIC, "value": served, "unit": METRIC, "n_gpus": 1, "steps": int(sum(j.frames * j.substeps_per_frame for j in jobs)),
-            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded Poisson trace)", "workload_kind": "served",
-            "config": {"workload": "Poisson %.0f jobs/s for %.0f s (seed 3), APIC pool+sphere, n in %s, %s frames x 4 "
-                                   "substeps, dt=1/480, HBM budget %.0f GB, batch <= %d"
-                                   % (args.trace_rate, args.trace_seconds, list(res), list(fr), args.hbm_budget_gb,
-                                      args.max_batch), "jobs": len(jobs)},
-            "frame_ms": {"p50": p50, "p99": p99},
+    return {"value": served, "unit": METRIC, "substeps_total": int(sum(j.frames * j.substeps_per_frame for j in jobs)),
+            "workload": "Poisson %.0f jobs/s for %.0f s (seed 3), APIC pool+sphere, n in %s, %s frames x 4 substeps, "
+                        "dt=1/480, HBM budget %.0f GB, batch <= %d" % (rate, seconds, list(res), list(fr), budget_gb,
+                                                                         max_batch),
+            "jobs": len(jobs), "frame_ms": {"p50": p50, "p99": p99},
             "one_at_a_time": {"value": ps_alone / t_alone, "makespan_s": t_alone,
                               "frame_ms_p50": float(np.percentile(ms_alone, 50)),
                               "frame_ms_p99": float(np.percentile(ms_alone, 99)),
@@ -600,8 +617,93 @@ def run_served(args):
             "served_over_one_at_a_time": served / (ps_alone / t_alone), "wall_s": wall,
             "server_time_s": dict(srv.timing), "batch_rebuilds": srv.rebuilds, "scenes_reused": srv.reused,
             "device_step_ratio": alone_split["step"] / max(srv.timing["step"], 1e-9)}
+
+
+def run_served(args):
+    """Served request stream (the served configuration scaled down in duration and resolution; see --trace-*)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    res = tuple(int(x) for x in args.trace_res.split(","))
+    fr = tuple(int(x) for x in args.trace_frames.split(","))
+    m = served_measure(args.trace_rate, args.trace_seconds, res, fr, args.hbm_budget_gb, args.max_batch)
+    line = {"metric": METRIC, "value": m["value"], "unit": METRIC, "n_gpus": 1, "steps": m["substeps_total"],
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded Poisson trace)", "workload_kind": "served",
+            "config": {"workload": m["workload"], "jobs": m["jobs"]}}
+    line.update({k: v for k, v in m.items() if k not in ("value", "unit", "substeps_total", "workload", "jobs")})
     print(json.dumps(line), flush=True)
     return 0
+
+
+def divergence_report(scene):
+    """One substep of the scene's current state run stage by stage: ||div u||_2 over FLUID cells before the pressure
+    stage and after it (the reference applies the pressure gradient one-sidedly, only toward +x/+y/+z from FLUID
+    cells, so a FLUID cell with an AIR neighbour on its low side keeps part of its divergence: the post/pre ratio
+    is bounded by that discretisation, not by the solver's residual).  Runs after the timed region."""
+    import fluide_engine_b200 as fe
+
+    scene.run_stages(DT, fe.STAGE_SORT, fe.STAGE_PRE)
+    pre = scene.divergence()
+    scene.run_stages(DT, fe.STAGE_DIFFUSE, fe.STAGE_PRESSURE)
+    post = scene.divergence()
+    scene.run_stages(DT, fe.STAGE_POST, fe.STAGE_MOVE)
+    return {"div_l2_pre": pre, "div_l2_post": post, "div_post_over_pre": post / pre if pre > 0 else None}
+
+
+def oracle_snapshot_report(n=64, later=30, device=0):
+    """Per-substep error against the FP64 oracle on the same scene family at n^3: the GPU runs later-1 substeps,
+    the oracle is seeded with the GPU's particles and pressure (warm start), and both run substep `later`
+    (trajectories diverge chaotically, so errors are compared from an identical snapshot).  The oracle runs its
+    substep stage by stage to report its own divergence before and after the pressure stage."""
+    import numpy as np
+
+    import fluide_engine_b200 as fe
+    import oracle
+
+    def rel(a, b):
+        a = np.asarray(a, np.float64).ravel()
+        b = np.asarray(b, np.float64).ravel()
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    pos, vel = fe.seed_regions([dict(kind=0, lo=BOX[:3], hi=BOX[3:])], (n, n, n), seed=0)
+    g = fe.Scene((n, n, n), solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6, device=device)
+    g.set_particles(pos, vel)
+    g.step(DT, later - 1, stats=False)
+    P0, V0, _ = g.particles()
+    p0 = g.grid()[3]
+    o = oracle.OracleSim((n, n, n), oracle.FLIP, max_cfl=1.0, cg_rel_tol=1e-10, cg_max_it=20000)
+    o.set_particles(P0.astype(np.float64), V0.astype(np.float64))
+    o.set_pressure(p0)
+    t0 = time.perf_counter()
+    o.build_collider()
+    for st_ in ("p2g", "sdf", "extrapolate", "bc"):
+        o.stage(st_)
+    o.stage("forces", DT)
+    o.stage("markers")
+    o_pre = o.divergence_l2()
+    o.stage("pressure", DT)
+    o_post = o.divergence_l2()
+    o_res = o.cg_rel_residual()
+    o.stage("advection", DT)
+    t_oracle = time.perf_counter() - t0
+    stats = g.step(DT, 1)
+    P, V, _ = g.particles()
+    u, v, w, p, m = g.grid()
+    Po, Vo, _ = o.particles()
+    out = {"scene": "FLIP dam break %d^3 (%d particles), substep %d from the GPU's state at substep %d"
+                    % (n, pos.shape[0], later, later - 1),
+           "particle_velocity_rel_l2": rel(V, Vo), "particle_position_rel_l2": rel(P, Po),
+           "pressure_rel_l2": rel(p, o.pressure()),
+           "grid_velocity_rel_l2": rel(np.concatenate([np.ravel(a) for a in (u, v, w)]),
+                                       np.concatenate([np.ravel(a) for a in o.grid()])),
+           "marks_bit_exact": bool(np.array_equal(m, o.marks())),
+           "gpu_rel_residual": stats[0]["rel_residual"], "oracle_rel_residual": o_res,
+           "oracle_div_post_over_pre": o_post / o_pre if o_pre > 0 else None,
+           "oracle_seconds": t_oracle,
+           "tolerances": {"particle_velocity": 1e-4, "grid": 1e-4, "pressure": 1e-3, "marks": "bit-exact"}}
+    g.close()
+    return out
 
 
 def main():
@@ -614,6 +716,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--ref-steps", type=int, default=1, help="substeps of the CPU reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="single workload: skip the accuracy-vs-oracle, batched and served objects of the line")
     ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
     ap.add_argument("--pressure-solver", default="auto", choices=["auto", "mgpcg", "cg"],
                     help="inner pressure solver: auto (multigrid-preconditioned CG from 2^22 cells, plain CG below), "
@@ -710,6 +814,7 @@ def main():
     traffic = float(per_unit * units.mean()) if per_unit else None
     phase_share = (phase_ms.sum(axis=0) / phase_ms.sum()).tolist()
     diffusion = diffusion_report(scene, stream, peak, peak_kind) if args.viscosity > 0 else None
+    divergence = divergence_report(scene)
     surface = surface_report(scene, n, reference=not args.no_cpu_baseline) if args.surface and rank == 0 else None
     mesh_init = (mesh_init_report(n, local, reference=not args.no_cpu_baseline) if args.mesh_init and rank == 0
                  else None)
@@ -737,6 +842,21 @@ def main():
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0, "cuda")
     e2e_value = replica_throughput(world, N, e2e_steps, e2e_s)
+
+    # accuracy beside the result, and the batched / served configurations (one GPU, rank 0 of a single-rank run)
+    extras = rank == 0 and world == 1 and not args.no_extras
+    oracle64 = None
+    if extras and not args.collider and not args.viscosity:
+        try:
+            oracle64 = oracle_snapshot_report(64, 30, local)
+        except Exception as ex:  # reported, never required
+            oracle64 = {"error": str(ex)[:200]}
+    batched = batched_measure(48, 50, 5, local) if extras else None
+    served = None
+    if extras:
+        res = tuple(int(x) for x in args.trace_res.split(","))
+        fr = tuple(int(x) for x in args.trace_frames.split(","))
+        served = served_measure(args.trace_rate, args.trace_seconds, res, fr, args.hbm_budget_gb, args.max_batch, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -770,6 +890,16 @@ def main():
                        "rel_residual_max": float(max(s["rel_residual"] for s in stats)),
                        "converged_all": bool(all(s["converged"] for s in stats)),
                        "fluid_cells_mean": float(fluid.mean())},
+            "accuracy": {"linear_rel_residual_max": float(max(s["rel_residual"] for s in stats)),
+                         "divergence": divergence, "vs_oracle": oracle64,
+                         "note": "linear_rel_residual = ||b - A p|| / ||b|| of every timed solve (FP64); divergence = "
+                                 "||div u|| over FLUID cells after / before the pressure stage of one more substep of "
+                                 "this scene (bounded by the reference's one-sided pressure apply, which the oracle "
+                                 "shares: vs_oracle.oracle_div_post_over_pre); vs_oracle = one substep from an "
+                                 "identical snapshot against the FP64 oracle"},
+            "window": "substeps %d-%d after %d untimed warm-up substeps from rest" % (args.warmup + 1,
+                                                                                   args.warmup + args.steps,
+                                                                                   args.warmup),
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(N * 24),
                     "d2h_bytes_per_step": int(N * 24), "steps": e2e_steps,
                     "path": "fe_scene_set_particles(host) + fe_scene_step(1) + fe_scene_get_particles(host)"},
@@ -777,6 +907,10 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        if batched:
+            line["batched"] = batched
+        if served:
+            line["served"] = served
         if diffusion:
             line["diffusion"] = diffusion
         if surface:

@@ -5,8 +5,8 @@ at 48^3 with the pressure refined to 1e-8 in FP64 (the 256^3 scene's settings).
 Each comparison starts from an identical snapshot: the first substep from the seeded particles, and a later
 substep after the oracle has been re-seeded with the GPU's particles and pressure (the warm start) -- whole
 trajectories diverge chaotically, so per-substep errors are what is compared.  Tolerances (relative L2): particle
-positions 1e-6, particle velocities and APIC matrices 1e-4, grid velocities 1e-4, pressure 1e-3; cell marks
-bit-exact.  The GPU's FP64 relative residual must meet the scene's target.
+positions 1e-6, particle velocities 1e-4, grid velocities 1e-4, pressure 1e-3, APIC matrices 1e-4 of the larger of
+their norm and the gradient scale |v| / h; cell marks bit-exact.  The GPU's FP64 relative residual must meet the scene's target.
 """
 import numpy as np
 import pytest
@@ -37,10 +37,16 @@ def compare_substep(g, o, dt, solver, rel_tol):
     assert np.array_equal(m, o.marks())
     P, V, C = g.particles()
     Po, Vo, Co = o.particles()
-    err = dict(P=rel_l2(P, Po), V=rel_l2(V, Vo), p=rel_l2(p, o.pressure()),
-               grid=max(rel_l2(a, b) for a, b in zip((u, v, w), o.grid())))
+    # the three face arrays as one vector: from rest, u and w hold only rounding noise, so their own relative
+    # norms say nothing
+    ug = np.concatenate([np.ravel(a) for a in (u, v, w)])
+    uo = np.concatenate([np.ravel(a) for a in o.grid()])
+    err = dict(P=rel_l2(P, Po), V=rel_l2(V, Vo), p=rel_l2(p, o.pressure()), grid=rel_l2(ug, uo))
     if solver == fe.APIC:
-        err["C"] = rel_l2(C, Co)
+        # C is a velocity gradient: where the flow is uniform (a falling sphere, a pool at rest) the oracle's C is
+        # FP64 rounding noise, so its error is taken relative to the larger of |C| and the gradient scale |v| / h
+        scale = max(np.linalg.norm(Co), np.linalg.norm(Vo) * max(g.n))
+        err["C"] = float(np.linalg.norm(C.astype(np.float64) - Co) / scale)
     assert err["P"] < 1e-6, err
     assert err["V"] < 1e-4, err
     assert err["grid"] < 1e-4, err
@@ -79,6 +85,7 @@ def test_flip_dam_break_64_tracks_oracle():
 def test_apic_pool_sphere_48_tracks_oracle(psolver):
     """The APIC sphere drop into a pool (pool y < 0.3, sphere r 0.15 at (0.5, 0.7, 0.5) moving at (0, -2, 0),
     seed 1, dt 1/480) at 48^3 with the pressure refined in FP64 to a relative residual of 1e-8: the first substep
-    and substep 30, with the plain and the multigrid-preconditioned inner solver."""
-    first, again = run_scene((48, 48, 48), fe.APIC, POOL, 1, 1.0 / 480.0, 1e-8, 30, pressure_solver=psolver)
+    and substep 80 (the sphere has entered the pool), with the plain and the multigrid-preconditioned inner
+    solver."""
+    first, again = run_scene((48, 48, 48), fe.APIC, POOL, 1, 1.0 / 480.0, 1e-8, 80, pressure_solver=psolver)
     assert first["C"] < 1e-4 and again["C"] < 1e-4
