@@ -7,7 +7,7 @@ from ._abi import (APIC, FLIP, PIC, AIR, FLUID, AUTO, CG, MGPCG, FluideError, ke
                    mesh_to_sdf, seed_regions, volume_field_vectors,
                    STAGE_SORT, STAGE_P2G, STAGE_MARK, STAGE_PRE, STAGE_DIFFUSE, STAGE_PRESSURE, STAGE_POST, STAGE_G2P,
                    STAGE_MOVE)
-from .scene import Batch, Scene, face_shapes  # noqa: F401
+from .scene import Batch, Scene, Snapshot, face_shapes  # noqa: F401
 from .simulators import (APICSimulator, BoundingBox3D, Collider, ColliderCollection, DirectionalField,  # noqa: F401
                          Emitter, ExternalForce, TriangleMeshCollider,
                          FLIPSimulator, Frame, HybridSimulator, OBJManager, PICSimulator, PointField, ScalarGrid3D,

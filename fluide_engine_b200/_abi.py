@@ -36,7 +36,9 @@ EXPORTS = [
     "fe_scene_get_sort", "fe_scene_divergence",
     "fe_scene_set_stream", "fe_scene_synchronize", "fe_project_noalloc", "fe_batch_create", "fe_batch_destroy", "fe_batch_set_scenes",
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
-    "fe_abi_version", "fe_debug_set_barrier_limits",
+    "fe_abi_version", "fe_debug_set_barrier_limits", "fe_scene_set_tuning", "fe_scene_get_tuning",
+    "fe_scene_snapshot", "fe_scene_restore", "fe_snapshot_info", "fe_snapshot_destroy",
+    "fe_scene_autotune", "fe_tuning_store", "fe_tuning_lookup",
 ]
 
 
@@ -52,6 +54,11 @@ class SceneDesc(ctypes.Structure):
                 ("max_cfl", ctypes.c_double), ("cg_rel_tol", ctypes.c_double), ("cg_max_it", ctypes.c_int32),
                 ("cg_inner_tol", ctypes.c_double), ("max_refine", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("max_particles", ctypes.c_uint64), ("pressure_solver", ctypes.c_int32), ("viscosity", ctypes.c_double)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("multigrid", ctypes.c_int32), ("cg_block_threads", ctypes.c_int32),
+                ("mg_block_level_cells", ctypes.c_int32)]
 
 
 class StepStats(ctypes.Structure):
@@ -153,6 +160,16 @@ def lib():
                                          ctypes.POINTER(ctypes.c_float)]
     L.fe_kernel_launch_count.restype = ctypes.c_uint64
     L.fe_debug_set_barrier_limits.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+    L.fe_scene_set_tuning.argtypes = [P, ctypes.POINTER(Tuning)]
+    L.fe_scene_get_tuning.argtypes = [P, ctypes.POINTER(Tuning)]
+    L.fe_scene_snapshot.argtypes = [P, ctypes.POINTER(P)]
+    L.fe_scene_restore.argtypes = [P, P]
+    L.fe_snapshot_info.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.fe_snapshot_destroy.argtypes = [P]
+    L.fe_scene_autotune.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(Tuning),
+                                    ctypes.POINTER(ctypes.c_float)]
+    L.fe_tuning_store.argtypes = [ctypes.c_int32, P, ctypes.c_int32, ctypes.POINTER(Tuning)]
+    L.fe_tuning_lookup.argtypes = [ctypes.c_int32, P, ctypes.c_int32, ctypes.POINTER(Tuning)]
     L.fe_seed_regions.restype = ctypes.c_uint64
     L.fe_seed_regions.argtypes = [P, ctypes.c_int32, P, P, P, ctypes.c_uint64, P, P, ctypes.c_uint64]
     L.fe_last_error.restype = ctypes.c_char_p

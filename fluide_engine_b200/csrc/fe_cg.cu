@@ -25,6 +25,8 @@
 // solve surfaces as a status instead of a hung device.  Dot products travel with the barrier: blocks
 // add their partials into a rotating totals slot before arriving and read the totals once after it, so
 // all blocks take identical branch decisions.
+#include <algorithm>
+
 #include "fe_solver_common.cuh"
 #include "fe_mg_body.cuh"
 
@@ -65,7 +67,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
 
     unsigned gen = 0;
     SolverSetup su;
-    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su, true)) return;
+    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su, kLayoutInterleaved)) return;
     const int F = su.F, kc = su.kc;
     const double bnorm = su.bnorm;
     auto entry = [&](int k, int e) -> uint32_t { return k < kc ? s_list[k * blockDim.x + threadIdx.x] : list[e]; };
@@ -316,19 +318,23 @@ cudaError_t launch_multi_cg(MultiCgScene* scenes, int S, int total_blocks, cudaS
     return e;
 }
 
-cudaError_t cg_prepare(CgWork& w, int device)
+cudaError_t cg_prepare(CgWork& w, int device, int threads)
 {
-    int sms = 0, per_sm = 0;
+    if (threads != 256 && threads != 512 && threads != 1024) return cudaErrorInvalidValue;
+    int sms = 0, per_sm = 0, per_sm_mg = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg, kCgThreads, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg, threads, 0);
     if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgcg, kCgThreads, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_mg, k_mgcg, threads, 0);
     if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
-    w.blocks = sms;  // one persistent block per SM
-    w.threads = kCgThreads;
+    // persistent blocks: as many per SM as fill 1024 threads, all co-resident (a cooperative launch)
+    const int want = kCgThreads / threads;
+    const int per = std::min(want, std::min(per_sm, per_sm_mg));
+    if (per < 1) return cudaErrorCooperativeLaunchTooLarge;
+    if (sms * per > kMaxCgBlocks) return cudaErrorCooperativeLaunchTooLarge;
+    w.blocks = sms * per;
+    w.threads = threads;
     return cudaSuccess;
 }
 
@@ -356,10 +362,10 @@ int mg_plan(int nx, int ny, int nz, const double h[3], MgLevel* out)
     return levels;
 }
 
-int mg_block_from(const MgLevel* lv, int levels)
+int mg_block_from(const MgLevel* lv, int levels, int block_cells)
 {
     int b = levels - 1;
-    while (b > 1 && (size_t)lv[b - 1].nx * lv[b - 1].ny * lv[b - 1].nz <= (size_t)kBlockLevelCells) --b;
+    while (b > 1 && (size_t)lv[b - 1].nx * lv[b - 1].ny * lv[b - 1].nz <= (size_t)block_cells) --b;
     return b;
 }
 

@@ -239,7 +239,9 @@ struct CgWork {
     unsigned stats_cap;     // entries of that ring (solves wrap around it)
     int blocks, threads;
 };
-cudaError_t cg_prepare(CgWork& w, int device);
+// Persistent-solver launch shape: `threads` per block (256, 512 or 1024), as many blocks per SM as make 1024
+// threads, all co-resident.
+cudaError_t cg_prepare(CgWork& w, int device, int threads = 1024);
 // Bounded-wait limits of the pressure solvers' grid barrier on the current device (spin_limit 0: the default;
 // extra_arrivals > 0 makes every barrier wait for blocks that do not exist, so each wait runs out).
 cudaError_t set_solver_barrier_limits(unsigned long long spin_limit, unsigned extra_arrivals);
@@ -269,8 +271,9 @@ struct MgWork {
 // Level dimensions for an nx x ny x nz grid with spacing h (host); returns the number of levels (>= 2), or 1
 // when the grid is too small for a hierarchy.
 int mg_plan(int nx, int ny, int nz, const double h[3], MgLevel* out);
-// First level (>= 1) small enough to be processed by one block without grid barriers.
-int mg_block_from(const MgLevel* lv, int levels);
+// First level (>= 1) from which every level has at most block_cells cells and is processed by one block without
+// grid barriers.
+int mg_block_from(const MgLevel* lv, int levels, int block_cells);
 
 // One scene of a multi-scene pressure solve (fe_cg.cu k_multi_cg): the scene's grid view and solver
 // buffers, its solver settings and the block range [block_start, block_start + block_count) that solves it.

@@ -35,7 +35,6 @@ namespace {
 constexpr float kOmega = 2.0f / 3.0f;
 constexpr float kRestrictScale = 0.1f;
 constexpr int kCoarseSweeps = 30;
-constexpr int kBlockLevelCells = 4096;  // levels this small are processed by one block (no grid barriers)
 
 __device__ __forceinline__ float level_diag(int i, int j, int k, int nx, int ny, int nz, const float* ih2)
 {
@@ -194,7 +193,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
 
     unsigned gen = 0;
     SolverSetup su;
-    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su, false)) return;
+    if (!solver_setup(v, w, blk, nblk, gen, sh, s_warp, s_list, su, kLayoutSeparate)) return;
     const int F = su.F, kc = su.kc;
     const double bnorm = su.bnorm;
     auto entry = [&](int k, int e) -> uint32_t { return k < kc ? s_list[k * blockDim.x + threadIdx.x] : list[e]; };

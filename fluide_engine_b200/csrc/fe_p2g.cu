@@ -7,16 +7,22 @@
 // weight > 0.  PIC and APIC clamp the face index with the CELL count, FLIP with the face count.  APIC
 // adds C_row . (x_face - x_clamped), the particle position clamped by h/2 on the two transverse axes.
 //
-// B200 design: one CTA per 8x8x8-cell tile.  The tile's particles are one contiguous run of the
-// sorted arrays (fe_keys.h), read once with coalesced loads.  Every face they can touch lies in a
-// 10x10x10 box around the tile (one cell of halo on each side covers the clamp quirks), so each CTA
-// accumulates numerator, weight and touched-marker of all three components in 24 KB of shared memory
-// with shared-memory atomics, then flushes the box to global accumulators: box faces touched by the
-// tile get one global red.add each, so a face receives at most 8 global adds (one per neighbouring
-// tile), never one per particle.  A second pass divides numerator by weight and, for FLIP, writes the
-// snapshot (flip_simulator.cpp:107-118).  Particles whose stencil leaves the box (only possible for a
-// domain origin away from zero, where the reference's data origins ignore the origin) fall back to
-// direct global adds, so the kernel stays correct for every input.
+// B200 design: one CTA per 8x8x8-cell tile and one thread per cell of it.  The tile's particles are one
+// contiguous run of the sorted arrays (fe_keys.h) and a cell's particles a contiguous piece of that run, so
+// each thread walks its own cell's particles and sums their contributions in registers.  With the domain origin
+// at zero every face a particle of cell (cx, cy, cz) can touch has indices within one of the cell's (the clamps
+// of GetBarycentric included), so a thread's sums live in 27 slots per component -- (numerator, weight) of the
+// faces (cx + a, cy + b, cz + c), a, b, c in {-1, 0, 1} -- plus a 27-bit touched mask.  Only then does the
+// thread add its touched slots into the tile's 10x10x10 face box in shared memory: one shared atomic per
+// (cell, face) pair instead of one per (particle, face) pair, and the 32 lanes of an atomic instruction hit 32
+// different faces.  Cells with more than kCellCap particles (particles clamped onto a wall pile up in one
+// cell) hand the rest to a warp that spreads them over its lanes and combines the lanes' slots by shuffles.
+// The box is then flushed to global accumulators: box faces touched by the tile get one global red.add each,
+// so a face receives at most 8 global adds (one per neighbouring tile), never one per particle.  A second pass
+// divides numerator by weight and, for FLIP, writes the snapshot (flip_simulator.cpp:107-118).  A particle
+// whose stencil leaves its cell's window (only possible for a domain origin away from zero, where the
+// reference's data origins ignore the origin) takes the direct path instead: shared atomics into the box per
+// face, or global adds for faces outside the box, so the kernel stays correct for every input.
 #include "fe_internal.cuh"
 
 namespace fe {
@@ -24,14 +30,173 @@ namespace {
 
 constexpr int kBox = 10;
 constexpr int kBoxFaces = kBox * kBox * kBox;
-constexpr int kP2gThreads = 256;
+constexpr int kP2gThreads = FE_TILE_CELLS;  // one thread per cell of a tile
+constexpr int kCellCap = 32;                // particles a thread sums for its own cell; the rest go to a warp
+
+// Per-component constants of the transfer (face-array sizes, the clamp sizes the reference passes to
+// GetCooridnatesAndWeights, the data origin, the global accumulators).
+struct P2gComp {
+    int fsx, fsy, fsz;  // face-array sizes
+    int csx, csy, csz;  // clamp sizes: FLIP the face counts, PIC / APIC the cell counts
+    float org[3];       // data origin of the component's face grid
+    float* gnum;
+    float* gden;
+    uint8_t* gmk;
+};
 
 template <int SOLVER>
-__global__ void __launch_bounds__(kP2gThreads) k_p2g(SceneView v)
+__device__ __forceinline__ P2gComp p2g_comp(const SceneView& v, int c)
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const bool flip = SOLVER == FE_SOLVER_FLIP;
+    P2gComp k;
+    k.fsx = nx + (c == 0);
+    k.fsy = ny + (c == 1);
+    k.fsz = nz + (c == 2);
+    k.csx = flip ? k.fsx : nx;
+    k.csy = flip ? k.fsy : ny;
+    k.csz = flip ? k.fsz : nz;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) k.org[a] = c == 0 ? v.xo[a] : (c == 1 ? v.yo[a] : v.zo[a]);
+    k.gnum = c == 0 ? v.nu : (c == 1 ? v.nv : v.nw);
+    k.gden = c == 0 ? v.du : (c == 1 ? v.dv : v.dw);
+    k.gmk = c == 0 ? v.mu : (c == 1 ? v.mv : v.mw);
+    return k;
+}
+
+// A particle's value for component c and its (APIC) clamped position and C row.
+template <int SOLVER>
+struct P2gParticle {
+    float vc;
+    float pc[3];
+    float cr[3];
+};
+
+template <int SOLVER>
+__device__ __forceinline__ P2gParticle<SOLVER> load_particle(const SceneView& v, uint32_t p, int c, float x, float y,
+                                                             float z, const float lo[3], const float hi[3])
+{
+    P2gParticle<SOLVER> q;
+    q.vc = c == 0 ? v.vx[p] : (c == 1 ? v.vy[p] : v.vz[p]);
+    q.pc[0] = x;
+    q.pc[1] = y;
+    q.pc[2] = z;
+    q.cr[0] = q.cr[1] = q.cr[2] = 0.f;
+    if (SOLVER == FE_SOLVER_APIC) {
+        q.cr[0] = v.c[3 * c][p];
+        q.cr[1] = v.c[3 * c + 1][p];
+        q.cr[2] = v.c[3 * c + 2][p];
+        // Clamp(val, max, min) on the two transverse axes (apic_simulator.cpp:55-57,68-70,81-83)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (a != c) q.pc[a] = q.pc[a] < lo[a] ? lo[a] : (q.pc[a] > hi[a] ? hi[a] : q.pc[a]);
+    }
+    return q;
+}
+
+// The particle's 8 faces added one by one: into the box (shared atomics) or, outside it, into the global
+// accumulators.  Used for particles whose stencil leaves their cell's window.
+template <int SOLVER>
+__device__ void splat_direct(const SceneView& v, const P2gComp& k, const Stencil& s, const P2gParticle<SOLVER>& q,
+                             int bx, int by, int bz, float* s_num, float* s_den, uint8_t* s_mk)
+{
+    const float wx[2] = {1.f - s.fx, s.fx}, wy[2] = {1.f - s.fy, s.fy}, wz[2] = {1.f - s.fz, s.fz};
+    const int ii[2] = {s.i, s.ip}, jj[2] = {s.j, s.jp}, kk[2] = {s.k, s.kp};
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int a = t & 1, b = (t >> 1) & 1, d = t >> 2;
+        const float wgt = wx[a] * wy[b] * wz[d];
+        float val = q.vc;
+        if (SOLVER == FE_SOLVER_APIC) {
+            const float gx = k.org[0] + v.hf[0] * (float)ii[a];
+            const float gy = k.org[1] + v.hf[1] * (float)jj[b];
+            const float gz = k.org[2] + v.hf[2] * (float)kk[d];
+            val += q.cr[0] * (gx - q.pc[0]) + q.cr[1] * (gy - q.pc[1]) + q.cr[2] * (gz - q.pc[2]);
+        }
+        const int li = ii[a] - bx, lj = jj[b] - by, lk = kk[d] - bz;
+        if ((unsigned)li < kBox && (unsigned)lj < kBox && (unsigned)lk < kBox) {
+            const int l = li + kBox * (lj + kBox * lk);
+            atomicAdd(&s_num[l], val * wgt);
+            atomicAdd(&s_den[l], wgt);
+            s_mk[l] = 1;
+        } else {
+            const size_t f = idx3(ii[a], jj[b], kk[d], k.fsx, k.fsy);
+            atomicAdd(k.gnum + f, val * wgt);
+            atomicAdd(k.gden + f, wgt);
+            k.gmk[f] = 1;
+        }
+    }
+}
+
+// One particle of cell (cx, cy, cz) into the cell's 27 slots for component c; returns false (and adds nothing)
+// when its stencil leaves the window, in which case the caller takes the direct path.
+template <int SOLVER>
+__device__ __forceinline__ bool splat_slots(const SceneView& v, const P2gComp& k, const Stencil& s,
+                                            const P2gParticle<SOLVER>& q, int cx, int cy, int cz, float (&num)[27],
+                                            float (&den)[27], uint32_t& mask)
+{
+    const int oi = s.i - cx, oip = s.ip - cx, oj = s.j - cy, ojp = s.jp - cy, ok = s.k - cz, okp = s.kp - cz;
+    if (oi < -1 || oip > 1 || oj < -1 || ojp > 1 || ok < -1 || okp > 1) return false;
+    // 1D weights and touched bits on the window offsets -1, 0, 1 (i and ip coincide only on a one-face axis)
+    float wx[3], wy[3], wz[3];
+    uint32_t tx = 0, ty = 0, tz = 0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int o = r - 1;
+        wx[r] = (oi == o ? 1.f - s.fx : 0.f) + (oip == o ? s.fx : 0.f);
+        wy[r] = (oj == o ? 1.f - s.fy : 0.f) + (ojp == o ? s.fy : 0.f);
+        wz[r] = (ok == o ? 1.f - s.fz : 0.f) + (okp == o ? s.fz : 0.f);
+        tx |= (oi == o || oip == o) ? 1u << r : 0u;
+        ty |= (oj == o || ojp == o) ? 1u << r : 0u;
+        tz |= (ok == o || okp == o) ? 1u << r : 0u;
+    }
+#pragma unroll
+    for (int c3 = 0; c3 < 3; ++c3)
+#pragma unroll
+        for (int b3 = 0; b3 < 3; ++b3)
+            if (((ty >> b3) & (tz >> c3)) & 1u) mask |= tx << (3 * b3 + 9 * c3);
+    // APIC: face position minus the clamped particle position per window offset and axis
+    float dx[3], dy[3], dz[3];
+    if (SOLVER == FE_SOLVER_APIC) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            dx[r] = (k.org[0] + v.hf[0] * (float)(cx + r - 1)) - q.pc[0];
+            dy[r] = (k.org[1] + v.hf[1] * (float)(cy + r - 1)) - q.pc[1];
+            dz[r] = (k.org[2] + v.hf[2] * (float)(cz + r - 1)) - q.pc[2];
+        }
+    }
+#pragma unroll
+    for (int c3 = 0; c3 < 3; ++c3)
+#pragma unroll
+        for (int b3 = 0; b3 < 3; ++b3) {
+#pragma unroll
+            for (int a3 = 0; a3 < 3; ++a3) {
+                const int slot = a3 + 3 * b3 + 9 * c3;
+                const float wgt = wx[a3] * wy[b3] * wz[c3];
+                float val = q.vc;
+                if (SOLVER == FE_SOLVER_APIC) val += q.cr[0] * dx[a3] + q.cr[1] * dy[b3] + q.cr[2] * dz[c3];
+                num[slot] += val * wgt;
+                den[slot] += wgt;
+            }
+        }
+    return true;
+}
+
+// Box index of slot `slot` of the cell at tile-local (lx, ly, lz): the box starts one face before the tile.
+__device__ __forceinline__ int slot_box(int lx, int ly, int lz, int slot)
+{
+    const int a = slot % 3, b = (slot / 3) % 3, c = slot / 9;
+    return (lx + a) + kBox * ((ly + b) + kBox * (lz + c));
+}
+
+template <int SOLVER>
+__global__ void __launch_bounds__(kP2gThreads, 1) k_p2g(SceneView v)
 {
     __shared__ float s_num[3][kBoxFaces];
     __shared__ float s_den[3][kBoxFaces];
     __shared__ uint8_t s_mk[3][kBoxFaces];
+    __shared__ uint16_t s_over[FE_TILE_CELLS];  // cells with more than kCellCap particles (tile-local index)
+    __shared__ int s_nover;
 
     const int tile = blockIdx.x;
     const int tx = tile % v.g.tnx, ty = (tile / v.g.tnx) % v.g.tny, tz = tile / (v.g.tnx * v.g.tny);
@@ -45,68 +210,92 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(SceneView v)
         (&s_den[0][0])[t] = 0.f;
         (&s_mk[0][0])[t] = 0;
     }
+    if (threadIdx.x == 0) s_nover = 0;
     __syncthreads();
 
-    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
-    // face-array sizes and the clamp sizes the reference passes to GetCooridnatesAndWeights
-    const int fsx[3] = {nx + 1, nx, nx}, fsy[3] = {ny, ny + 1, ny}, fsz[3] = {nz, nz, nz + 1};
-    const bool flip = SOLVER == FE_SOLVER_FLIP;
-    const int csx[3] = {flip ? nx + 1 : nx, nx, nx}, csy[3] = {ny, flip ? ny + 1 : ny, ny},
-              csz[3] = {nz, nz, flip ? nz + 1 : nz};
-    const float* org[3] = {v.xo, v.yo, v.zo};
-    float* gnum[3] = {v.nu, v.nv, v.nw};
-    float* gden[3] = {v.du, v.dv, v.dw};
-    uint8_t* gmk[3] = {v.mu, v.mv, v.mw};
     const float lo[3] = {v.originf[0] + 0.5f * v.hf[0], v.originf[1] + 0.5f * v.hf[1], v.originf[2] + 0.5f * v.hf[2]};
     const float hi[3] = {v.originf[0] + v.sizef[0] - 0.5f * v.hf[0], v.originf[1] + v.sizef[1] - 0.5f * v.hf[1],
                          v.originf[2] + v.sizef[2] - 0.5f * v.hf[2]};
 
-    // Thread -> particle map that keeps a warp's lanes on different cells: with about 8 particles per
-    // cell, consecutive particles share their 24 face targets, so lane l of warp w takes particle
-    // base + 8 l + w of each 256-particle window and shared-memory atomics rarely collide.
+    // this thread's cell (tile-local index = key & 511 = threadIdx.x)
+    const int lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz = threadIdx.x >> 6;
+    const int cx = tx * FE_TILE + lx, cy = ty * FE_TILE + ly, cz = tz * FE_TILE + lz;
+    uint32_t pb = 0, pe = 0;
+    if (cx < v.g.nx && cy < v.g.ny && cz < v.g.nz) {
+        const uint32_t key = (uint32_t)tile * FE_TILE_CELLS + threadIdx.x;
+        pb = v.cell_start[key];
+        pe = v.cell_start[key + 1];
+    }
+    if (pe - pb > (uint32_t)kCellCap) {
+        s_over[atomicAdd(&s_nover, 1)] = (uint16_t)threadIdx.x;
+        pe = pb + kCellCap;
+    }
+
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+        const P2gComp k = p2g_comp<SOLVER>(v, c);
+        float num[27], den[27];
+#pragma unroll
+        for (int t = 0; t < 27; ++t) num[t] = den[t] = 0.f;
+        uint32_t mask = 0;
+        for (uint32_t p = pb; p < pe; ++p) {
+            const float x = v.px[p], y = v.py[p], z = v.pz[p];
+            const Stencil s = stencil(x, y, z, k.org, v.inv_hf, k.csx, k.csy, k.csz);
+            const P2gParticle<SOLVER> q = load_particle<SOLVER>(v, p, c, x, y, z, lo, hi);
+            if (!splat_slots<SOLVER>(v, k, s, q, cx, cy, cz, num, den, mask))
+                splat_direct<SOLVER>(v, k, s, q, bx, by, bz, s_num[c], s_den[c], s_mk[c]);
+        }
+#pragma unroll
+        for (int t = 0; t < 27; ++t) {
+            if (!((mask >> t) & 1u)) continue;
+            const int l = slot_box(lx, ly, lz, t);
+            atomicAdd(&s_num[c][l], num[t]);
+            atomicAdd(&s_den[c][l], den[t]);
+            s_mk[c][l] = 1;
+        }
+    }
+    __syncthreads();
+
+    // crowded cells: a warp per cell, lanes stride over the particles past kCellCap, slots summed by shuffles
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (uint32_t base = beg; base < end; base += blockDim.x) {
-        const uint32_t p = base + (uint32_t)(lane * nwarps + warp);
-        if (p >= end) continue;
-        const float x = v.px[p], y = v.py[p], z = v.pz[p];
-        const float vel[3] = {v.vx[p], v.vy[p], v.vz[p]};
-#pragma unroll
+    const int nover = s_nover;
+    for (int o = warp; o < nover; o += nwarps) {
+        const int t = s_over[o];
+        const int ox = t & 7, oy = (t >> 3) & 7, oz = t >> 6;
+        const int ocx = tx * FE_TILE + ox, ocy = ty * FE_TILE + oy, ocz = tz * FE_TILE + oz;
+        const uint32_t key = (uint32_t)tile * FE_TILE_CELLS + (uint32_t)t;
+        const uint32_t ob = v.cell_start[key] + kCellCap, oe = v.cell_start[key + 1];
+#pragma unroll 1
         for (int c = 0; c < 3; ++c) {
-            Stencil s = stencil(x, y, z, org[c], v.inv_hf, csx[c], csy[c], csz[c]);
-            float cr[3] = {0.f, 0.f, 0.f}, pc[3] = {x, y, z};
-            if (SOLVER == FE_SOLVER_APIC) {
-                cr[0] = v.c[3 * c][p];
-                cr[1] = v.c[3 * c + 1][p];
-                cr[2] = v.c[3 * c + 2][p];
-                // Clamp(val, max, min) on the two transverse axes (apic_simulator.cpp:55-57,68-70,81-83)
+            const P2gComp k = p2g_comp<SOLVER>(v, c);
+            float num[27], den[27];
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
-                    if (a != c) pc[a] = pc[a] < lo[a] ? lo[a] : (pc[a] > hi[a] ? hi[a] : pc[a]);
+            for (int q = 0; q < 27; ++q) num[q] = den[q] = 0.f;
+            uint32_t mask = 0;
+            for (uint32_t p = ob + lane; p < oe; p += 32) {
+                const float x = v.px[p], y = v.py[p], z = v.pz[p];
+                const Stencil s = stencil(x, y, z, k.org, v.inv_hf, k.csx, k.csy, k.csz);
+                const P2gParticle<SOLVER> q = load_particle<SOLVER>(v, p, c, x, y, z, lo, hi);
+                if (!splat_slots<SOLVER>(v, k, s, q, ocx, ocy, ocz, num, den, mask))
+                    splat_direct<SOLVER>(v, k, s, q, bx, by, bz, s_num[c], s_den[c], s_mk[c]);
             }
-            const float wx[2] = {1.f - s.fx, s.fx}, wy[2] = {1.f - s.fy, s.fy}, wz[2] = {1.f - s.fz, s.fz};
-            const int ii[2] = {s.i, s.ip}, jj[2] = {s.j, s.jp}, kk[2] = {s.k, s.kp};
+            mask = __reduce_or_sync(0xffffffffu, mask);
 #pragma unroll
-            for (int t = 0; t < 8; ++t) {
-                const int a = t & 1, b = (t >> 1) & 1, d = t >> 2;
-                const float wgt = wx[a] * wy[b] * wz[d];
-                float val = vel[c];
-                if (SOLVER == FE_SOLVER_APIC) {
-                    float gx = org[c][0] + v.hf[0] * (float)ii[a];
-                    float gy = org[c][1] + v.hf[1] * (float)jj[b];
-                    float gz = org[c][2] + v.hf[2] * (float)kk[d];
-                    val += cr[0] * (gx - pc[0]) + cr[1] * (gy - pc[1]) + cr[2] * (gz - pc[2]);
+            for (int q = 0; q < 27; ++q) {
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    num[q] += __shfl_xor_sync(0xffffffffu, num[q], off);
+                    den[q] += __shfl_xor_sync(0xffffffffu, den[q], off);
                 }
-                const int li = ii[a] - bx, lj = jj[b] - by, lk = kk[d] - bz;
-                if ((unsigned)li < kBox && (unsigned)lj < kBox && (unsigned)lk < kBox) {
-                    const int l = li + kBox * (lj + kBox * lk);
-                    atomicAdd(&s_num[c][l], val * wgt);
-                    atomicAdd(&s_den[c][l], wgt);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int q = 0; q < 27; ++q) {
+                    if (!((mask >> q) & 1u)) continue;
+                    const int l = slot_box(ox, oy, oz, q);
+                    atomicAdd(&s_num[c][l], num[q]);
+                    atomicAdd(&s_den[c][l], den[q]);
                     s_mk[c][l] = 1;
-                } else {
-                    const size_t f = idx3(ii[a], jj[b], kk[d], fsx[c], fsy[c]);
-                    atomicAdd(gnum[c] + f, val * wgt);
-                    atomicAdd(gden[c] + f, wgt);
-                    gmk[c][f] = 1;
                 }
             }
         }
@@ -115,15 +304,16 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(SceneView v)
 
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+        const P2gComp k = p2g_comp<SOLVER>(v, c);
         for (int l = threadIdx.x; l < kBoxFaces; l += blockDim.x) {
             if (!s_mk[c][l]) continue;
             const int li = l % kBox, lj = (l / kBox) % kBox, lk = l / (kBox * kBox);
             const int gi = bx + li, gj = by + lj, gk = bz + lk;
-            if (gi < 0 || gj < 0 || gk < 0 || gi >= fsx[c] || gj >= fsy[c] || gk >= fsz[c]) continue;
-            const size_t f = idx3(gi, gj, gk, fsx[c], fsy[c]);
-            atomicAdd(gnum[c] + f, s_num[c][l]);
-            atomicAdd(gden[c] + f, s_den[c][l]);
-            gmk[c][f] = 1;
+            if (gi < 0 || gj < 0 || gk < 0 || gi >= k.fsx || gj >= k.fsy || gk >= k.fsz) continue;
+            const size_t f = idx3(gi, gj, gk, k.fsx, k.fsy);
+            atomicAdd(k.gnum + f, s_num[c][l]);
+            atomicAdd(k.gden + f, s_den[c][l]);
+            k.gmk[f] = 1;
         }
     }
 }

@@ -13,8 +13,11 @@
 #include <cstring>
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <new>
+#include <tuple>
 #include <vector>
 
 #include "fe_internal.cuh"
@@ -109,7 +112,9 @@ struct fe_scene {
     void* scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
     CgWork cg{};
-    MgWork mg{};                       // multigrid levels (levels >= 2) when the pressure solver is FE_PRESSURE_MGPCG
+    MgWork mg{};                       // multigrid levels (levels >= 2) once the multigrid solver was wanted
+    bool use_mg = false;               // solve with the multigrid-preconditioned CG (if the grid has a hierarchy)
+    int mg_block_cells = 4096;         // multigrid levels of at most this many cells run in one block
     DiffWork diff{};                   // viscosity buffers (allocated once the viscosity is > 0)
     bool diff_ready = false;
     // Surface extraction (fe_surface.cu), allocated on first use: node distances and SDF values, per-item case
@@ -317,6 +322,36 @@ fe_status alloc_diffusion(fe_scene* s)
     return FE_OK;
 }
 
+// Multigrid hierarchy of the scene's grid (levels 1 .. L-1, dense; level 0 is the grid itself), allocated once;
+// grids too small for a hierarchy keep levels = 0 and solve with the plain CG.
+fe_status ensure_mg(fe_scene* s)
+{
+    if (s->mg.levels >= 2) return FE_OK;
+    SceneView& v = s->base;
+    auto& L = s->allocs;
+    const int dev = s->device;
+    cudaStream_t st = s->own_stream;
+    MgLevel lv[kMaxMgLevels];
+    const int levels = mg_plan(v.g.nx, v.g.ny, v.g.nz, v.h, lv);
+    if (levels < 2) return FE_OK;
+    for (int l = 1; l < levels; ++l) {
+        MgLevel& M = lv[l];
+        const size_t cells = (size_t)M.nx * M.ny * M.nz;
+        FE_CUDA(dalloc(L, &M.mask, cells, dev, st));
+        FE_CUDA(dalloc(L, &M.r, cells, dev, st));
+        FE_CUDA(dalloc(L, &M.z, cells, dev, st));
+        FE_CUDA(dalloc(L, &M.t, cells, dev, st));
+        FE_CUDA(cudaMemsetAsync(M.mask, 0, cells, st));
+        FE_CUDA(cudaMemsetAsync(M.r, 0, cells * sizeof(float), st));
+        FE_CUDA(cudaMemsetAsync(M.z, 0, cells * sizeof(float), st));
+        FE_CUDA(cudaMemsetAsync(M.t, 0, cells * sizeof(float), st));
+    }
+    for (int l = 0; l < levels; ++l) s->mg.lv[l] = lv[l];
+    s->mg.levels = levels;
+    s->mg.block_from = mg_block_from(s->mg.lv, levels, s->mg_block_cells);
+    return FE_OK;
+}
+
 fe_status alloc_grid(fe_scene* s)
 {
     SceneView& v = s->base;
@@ -374,26 +409,11 @@ fe_status alloc_grid(fe_scene* s)
     FE_CUDA(dalloc(L, &w.list, nc, dev, st));
     // multigrid levels 1 .. L-1 (dense; level 0 is the grid above)
     s->mg.levels = 0;
-    const bool want_mg = s->desc.pressure_solver == FE_PRESSURE_MGPCG ||
-                         (s->desc.pressure_solver == FE_PRESSURE_AUTO && nc >= kMgAutoCells);
-    if (want_mg) {
-        const int levels = mg_plan(nx, ny, nz, v.h, s->mg.lv);
-        if (levels >= 2) {
-            for (int l = 1; l < levels; ++l) {
-                MgLevel& M = s->mg.lv[l];
-                const size_t cells = (size_t)M.nx * M.ny * M.nz;
-                FE_CUDA(dalloc(L, &M.mask, cells, dev, st));
-                FE_CUDA(dalloc(L, &M.r, cells, dev, st));
-                FE_CUDA(dalloc(L, &M.z, cells, dev, st));
-                FE_CUDA(dalloc(L, &M.t, cells, dev, st));
-                FE_CUDA(cudaMemsetAsync(M.mask, 0, cells, st));
-                FE_CUDA(cudaMemsetAsync(M.r, 0, cells * sizeof(float), st));
-                FE_CUDA(cudaMemsetAsync(M.z, 0, cells * sizeof(float), st));
-                FE_CUDA(cudaMemsetAsync(M.t, 0, cells * sizeof(float), st));
-            }
-            s->mg.levels = levels;
-            s->mg.block_from = mg_block_from(s->mg.lv, levels);
-        }
+    s->use_mg = s->desc.pressure_solver == FE_PRESSURE_MGPCG ||
+                (s->desc.pressure_solver == FE_PRESSURE_AUTO && nc >= kMgAutoCells);
+    if (s->use_mg) {
+        fe_status mst = ensure_mg(s);
+        if (mst != FE_OK) return mst;
     }
     FE_CUDA(cg_prepare(w, s->device));
     // 3 rotating totals slots (12 doubles) + per-block FLUID counts of up to kMaxCgBlocks solver blocks
@@ -678,7 +698,7 @@ fe_status enqueue_steps(fe_scene* s, double dt, int first, int last, cudaStream_
             if (s->colliders.count > 0) FE_CUDA(launch_collider_project_rhs(v, s->cw, s->cg.err, st));
             break;
         case kStepCg:
-            if (s->mg.levels >= 2 && s->colliders.count == 0)
+            if (s->use_mg && s->mg.levels >= 2 && s->colliders.count == 0)
                 FE_CUDA(launch_mgcg(v, s->cg, s->mg, s->desc.cg_rel_tol, s->desc.cg_inner_tol, s->desc.cg_max_it,
                                     s->desc.max_refine, st));
             else
@@ -983,6 +1003,67 @@ fe_status fe_scene_desc_default(fe_scene_desc* d)
     return FE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Applies the fields of `t` that ask for a change (caller holds the scene's lock or owns the scene alone).
+fe_status apply_tuning(fe_scene* s, const fe_tuning* t)
+{
+    if (t->cg_block_threads > 0 && t->cg_block_threads != 256 && t->cg_block_threads != 512 &&
+        t->cg_block_threads != 1024)
+        return set_error(FE_ERR_BAD_ARG, "cg_block_threads must be 256, 512 or 1024");
+    if (t->multigrid > 1) return set_error(FE_ERR_BAD_ARG, "multigrid is 0 or 1");
+    FE_CUDA(cudaSetDevice(s->device));
+    FE_CUDA(cudaStreamSynchronize(s->stream));
+    if (t->cg_block_threads > 0 && t->cg_block_threads != s->cg.threads) {
+        CgWork w = s->cg;
+        FE_CUDA(cg_prepare(w, s->device, t->cg_block_threads));
+        s->cg.blocks = w.blocks;
+        s->cg.threads = w.threads;
+    }
+    if (t->mg_block_level_cells > 0) {
+        s->mg_block_cells = t->mg_block_level_cells;
+        if (s->mg.levels >= 2) s->mg.block_from = mg_block_from(s->mg.lv, s->mg.levels, s->mg_block_cells);
+    }
+    if (t->multigrid >= 0) {
+        if (t->multigrid == 1) {
+            fe_status st = ensure_mg(s);
+            if (st != FE_OK) return st;
+            FE_CUDA(cudaStreamSynchronize(s->own_stream));
+        }
+        s->use_mg = t->multigrid == 1;
+    }
+    drop_graphs(s);  // the captured substeps hold the old launch shape and solver
+    ++s->epoch;
+    return FE_OK;
+}
+
+// Tuning chosen by fe_scene_autotune (or stored by the caller) per (device, grid, transfer): scenes created with
+// FE_PRESSURE_AUTO start from it.
+struct TuneKey {
+    int device, nx, ny, nz, solver;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::tie(device, nx, ny, nz, solver) < std::tie(o.device, o.nx, o.ny, o.nz, o.solver);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, fe_tuning> g_tune_cache;
+
+bool tuning_lookup(int device, int nx, int ny, int nz, int solver, fe_tuning* out)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(TuneKey{device, nx, ny, nz, solver});
+    if (it == g_tune_cache.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
 fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
 {
     if (!desc || !out) return set_error(FE_ERR_BAD_ARG, "null argument");
@@ -1059,6 +1140,10 @@ fe_status fe_scene_create(const fe_scene_desc* desc, fe_scene** out)
     s->stream = s->own_stream;
     if (st == FE_OK) st = alloc_grid(s);
     if (st == FE_OK && desc->max_particles > 0) st = alloc_particles(s, desc->max_particles);
+    fe_tuning tuned;
+    if (st == FE_OK && desc->pressure_solver == FE_PRESSURE_AUTO &&
+        tuning_lookup(s->device, desc->n[0], desc->n[1], desc->n[2], desc->solver, &tuned))
+        st = apply_tuning(s, &tuned);
     if (st != FE_OK) {
         if (s->own_stream) {
             cudaStreamSynchronize(s->own_stream);
@@ -2061,6 +2146,252 @@ fe_status fe_scene_divergence(fe_scene* s, double* l2)
     FE_CUDA(cudaMemcpyAsync(&acc, s->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     FE_CUDA(cudaStreamSynchronize(s->stream));
     *l2 = std::sqrt(acc);
+    return FE_OK;
+}
+
+}  // extern "C"
+
+// A scene's simulation state at a substep boundary, on the device: the particles in slot order (every channel and
+// the identity permutation), the positions at the start of the last substep (the fluid surface's SDF is built
+// from them), the pressure warm start, the current velocity grid (the next frame's CFL reads it) and the host-side
+// flags and counters that steer the next substeps.
+struct fe_snapshot {
+    int device = 0;
+    int n[3] = {0, 0, 0};
+    int solver = 0;
+    uint64_t np = 0;
+    std::vector<void*> allocs;
+    float* part = nullptr;    // channels x np floats (pos 3, vel 3, C 9 for APIC), then pid (np u32)
+    float* prev = nullptr;    // 3 x np: positions at the start of the last substep (when prev_valid)
+    double* p = nullptr;      // nc
+    float* grid = nullptr;    // nf: the current velocity buffer
+    int channels = 0;
+    bool prev_valid = false, collider_built = false, last_substep_empty = false, have_particles = false;
+    std::vector<uint64_t> emitter_calls;
+    uint64_t bytes = 0;
+};
+
+extern "C" {
+
+fe_status fe_scene_snapshot(fe_scene* s, fe_snapshot** out)
+{
+    if (!s || !out) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    FE_CUDA(cudaSetDevice(s->device));
+    const SceneView& b = s->base;
+    const size_t nc = (size_t)b.g.nx * b.g.ny * b.g.nz;
+    const size_t nf = (size_t)(b.g.nx + 1) * b.g.ny * b.g.nz + (size_t)b.g.nx * (b.g.ny + 1) * b.g.nz +
+                      (size_t)b.g.nx * b.g.ny * (b.g.nz + 1);
+    std::unique_ptr<fe_snapshot> sn(new fe_snapshot);
+    sn->device = s->device;
+    sn->n[0] = b.g.nx;
+    sn->n[1] = b.g.ny;
+    sn->n[2] = b.g.nz;
+    sn->solver = s->desc.solver;
+    sn->np = b.np;
+    sn->channels = 6 + (s->desc.solver == FE_SOLVER_APIC ? 9 : 0);
+    sn->prev_valid = s->prev_valid;
+    sn->collider_built = s->collider_built;
+    sn->last_substep_empty = s->last_substep_empty;
+    sn->have_particles = s->have_particles;
+    for (const auto& e : s->emitters) sn->emitter_calls.push_back(e.calls);
+    cudaStream_t st = s->stream;
+    const int dev = s->device;
+    const size_t np = b.np;
+    FE_CUDA(dalloc(sn->allocs, &sn->p, nc, dev, st));
+    FE_CUDA(dalloc(sn->allocs, &sn->grid, nf, dev, st));
+    FE_CUDA(cudaMemcpyAsync(sn->p, b.p, nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    FE_CUDA(cudaMemcpyAsync(sn->grid, s->grid_cur ? b.u2 : b.u, nf * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    sn->bytes = nc * sizeof(double) + nf * sizeof(float);
+    if (np) {
+        const SceneView v = view_of(s, s->parity);
+        FE_CUDA(dalloc(sn->allocs, &sn->part, np * (sn->channels + 1), dev, st));
+        const float* ch[15] = {v.px, v.py, v.pz, v.vx, v.vy, v.vz};
+        for (int a = 0; a < 9; ++a) ch[6 + a] = v.c[a];
+        for (int k = 0; k < sn->channels; ++k)
+            FE_CUDA(cudaMemcpyAsync(sn->part + k * np, ch[k], np * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        FE_CUDA(cudaMemcpyAsync(sn->part + sn->channels * np, v.pid, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                st));
+        sn->bytes += np * (sn->channels + 1) * sizeof(float);
+        if (s->prev_valid) {
+            const SceneView o = view_of(s, s->parity ^ 1);
+            FE_CUDA(dalloc(sn->allocs, &sn->prev, 3 * np, dev, st));
+            const float* pc[3] = {o.px, o.py, o.pz};
+            for (int k = 0; k < 3; ++k)
+                FE_CUDA(cudaMemcpyAsync(sn->prev + k * np, pc[k], np * sizeof(float), cudaMemcpyDeviceToDevice, st));
+            sn->bytes += 3 * np * sizeof(float);
+        }
+    }
+    FE_CUDA(cudaStreamSynchronize(st));
+    *out = sn.release();
+    return FE_OK;
+}
+
+fe_status fe_scene_restore(fe_scene* s, const fe_snapshot* sn)
+{
+    if (!s || !sn) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const SceneView& b0 = s->base;
+    if (sn->device != s->device || sn->n[0] != b0.g.nx || sn->n[1] != b0.g.ny || sn->n[2] != b0.g.nz ||
+        sn->solver != s->desc.solver)
+        return set_error(FE_ERR_BAD_ARG, "snapshot of another grid, solver or device");
+    if (sn->emitter_calls.size() != s->emitters.size())
+        return set_error(FE_ERR_BAD_ARG, "snapshot taken with %zu emitters, scene has %zu", sn->emitter_calls.size(),
+                         s->emitters.size());
+    FE_CUDA(cudaSetDevice(s->device));
+    const size_t np = sn->np;
+    if (np > s->cap || !s->set[0].px) {
+        FE_CUDA(cudaStreamSynchronize(s->stream));
+        fe_status st = alloc_particles(s, std::max<uint64_t>(np, 1));
+        if (st != FE_OK) return st;
+    }
+    if (np != s->base.np) drop_graphs(s);
+    const SceneView& b = s->base;
+    const size_t nc = (size_t)b.g.nx * b.g.ny * b.g.nz;
+    const size_t nf = (size_t)(b.g.nx + 1) * b.g.ny * b.g.nz + (size_t)b.g.nx * (b.g.ny + 1) * b.g.nz +
+                      (size_t)b.g.nx * b.g.ny * (b.g.nz + 1);
+    cudaStream_t st = s->stream;
+    s->base.np = np;
+    s->parity = 0;
+    s->grid_cur = 0;
+    FE_CUDA(cudaMemcpyAsync(b.p, sn->p, nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    FE_CUDA(cudaMemcpyAsync(b.u, sn->grid, nf * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (np) {
+        const SceneView v = view_of(s, 0);
+        float* ch[15] = {v.px, v.py, v.pz, v.vx, v.vy, v.vz};
+        for (int a = 0; a < 9; ++a) ch[6 + a] = v.c[a];
+        for (int k = 0; k < sn->channels; ++k)
+            FE_CUDA(cudaMemcpyAsync(ch[k], sn->part + k * np, np * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        FE_CUDA(cudaMemcpyAsync(v.pid, sn->part + sn->channels * np, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                st));
+        if (sn->prev) {
+            const SceneView o = view_of(s, 1);
+            float* pc[3] = {o.px, o.py, o.pz};
+            for (int k = 0; k < 3; ++k)
+                FE_CUDA(cudaMemcpyAsync(pc[k], sn->prev + k * np, np * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    FE_CUDA(cudaStreamSynchronize(st));
+    s->prev_valid = sn->prev_valid && sn->prev;
+    s->collider_built = sn->collider_built;
+    s->last_substep_empty = sn->last_substep_empty;
+    s->have_particles = sn->have_particles;
+    s->mesh_sdf = false;
+    for (size_t i = 0; i < s->emitters.size(); ++i) s->emitters[i].calls = sn->emitter_calls[i];
+    return FE_OK;
+}
+
+fe_status fe_snapshot_info(const fe_snapshot* sn, uint64_t* particles, uint64_t* bytes)
+{
+    if (!sn) return set_error(FE_ERR_BAD_ARG, "null snapshot");
+    if (particles) *particles = sn->np;
+    if (bytes) *bytes = sn->bytes;
+    return FE_OK;
+}
+
+fe_status fe_snapshot_destroy(fe_snapshot* sn)
+{
+    if (!sn) return FE_OK;
+    cudaSetDevice(sn->device);
+    for (void* p : sn->allocs) cudaFreeAsync(p, 0);
+    cudaStreamSynchronize(0);
+    delete sn;
+    return FE_OK;
+}
+
+fe_status fe_scene_set_tuning(fe_scene* s, const fe_tuning* t)
+{
+    if (!s || !t) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return apply_tuning(s, t);
+}
+
+fe_status fe_scene_get_tuning(fe_scene* s, fe_tuning* t)
+{
+    if (!s || !t) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    t->multigrid = s->use_mg && s->mg.levels >= 2 && s->colliders.count == 0 ? 1 : 0;
+    t->cg_block_threads = s->cg.threads;
+    t->mg_block_level_cells = s->mg_block_cells;
+    return FE_OK;
+}
+
+fe_status fe_tuning_store(int32_t device, const int32_t n[3], int32_t solver, const fe_tuning* t)
+{
+    if (!n || !t) return set_error(FE_ERR_BAD_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[TuneKey{device, n[0], n[1], n[2], solver}] = *t;
+    return FE_OK;
+}
+
+fe_status fe_tuning_lookup(int32_t device, const int32_t n[3], int32_t solver, fe_tuning* t)
+{
+    if (!n || !t) return set_error(FE_ERR_BAD_ARG, "null argument");
+    if (!tuning_lookup(device, n[0], n[1], n[2], solver, t)) return set_error(FE_ERR_STATE, "no tuning stored");
+    return FE_OK;
+}
+
+fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, fe_tuning* best, float* best_ms)
+{
+    if (!s || !(dt > 0.0) || substeps < 1) return set_error(FE_ERR_BAD_ARG, "bad autotune arguments");
+    if (!s->have_particles || s->base.np == 0) return set_error(FE_ERR_STATE, "autotune needs particles");
+    // candidates: the plain CG at 256 / 512 / 1024 threads per block and, where the grid has a multigrid hierarchy
+    // and no colliders, the multigrid-preconditioned CG at 512 / 1024 threads with one-block levels up to 2048 or
+    // 4096 cells
+    std::vector<fe_tuning> cand;
+    for (int th : {1024, 512, 256}) cand.push_back(fe_tuning{0, th, 4096});
+    MgLevel lv[kMaxMgLevels];
+    const SceneView& b = s->base;
+    if (mg_plan(b.g.nx, b.g.ny, b.g.nz, b.h, lv) >= 2 && s->colliders.count == 0)
+        for (int th : {1024, 512})
+            for (int cells : {4096, 2048}) cand.push_back(fe_tuning{1, th, cells});
+    fe_tuning before;
+    fe_status st = fe_scene_get_tuning(s, &before);
+    if (st != FE_OK) return st;
+    fe_snapshot* snap = nullptr;
+    st = fe_scene_snapshot(s, &snap);
+    if (st != FE_OK) return st;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaSetDevice(s->device);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<fe_step_stats> stats((size_t)substeps);
+    float best_time = -1.f;
+    fe_tuning pick = before;
+    for (const fe_tuning& c : cand) {
+        if ((st = fe_scene_restore(s, snap)) != FE_OK) break;
+        if ((st = fe_scene_set_tuning(s, &c)) != FE_OK) break;
+        if ((st = fe_scene_step(s, dt, 1, nullptr)) != FE_OK) break;  // captures this choice's graphs
+        cudaEventRecord(e0, s->stream);
+        if ((st = fe_scene_step(s, dt, substeps, stats.data())) != FE_OK) break;
+        cudaEventRecord(e1, s->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        bool ok = true;
+        for (const auto& x : stats) ok = ok && x.converged == 1;
+        if (ok && (best_time < 0.f || ms < best_time)) {
+            best_time = ms;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    fe_status st2 = fe_scene_restore(s, snap);
+    fe_snapshot_destroy(snap);
+    if (st == FE_OK) st = st2;
+    if (st == FE_OK) st = fe_scene_set_tuning(s, &pick);
+    if (st != FE_OK) {
+        fe_scene_set_tuning(s, &before);
+        return st;
+    }
+    fe_scene_get_tuning(s, &pick);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[TuneKey{s->device, b.g.nx, b.g.ny, b.g.nz, s->desc.solver}] = pick;
+    }
+    if (best) *best = pick;
+    if (best_ms) *best_ms = best_time / (float)substeps;
     return FE_OK;
 }
 

@@ -37,9 +37,10 @@ __device__ __forceinline__ unsigned next_gen(unsigned g) { return g + 1u == 6553
 // slot of the next generation and bumps the generation with a release store; the others poll the
 // generation (bounded) with acquire loads, away from the line the arrivals hit.  The release/acquire pair at
 // device scope, with the __syncthreads on either side, orders every thread's memory traffic of the block
-// across the barrier.  `gen` is the generation this barrier started in (tracked by thread 0).  Returns
-// false when the wait gave up.
-__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals, unsigned gen)
+// across the barrier.  `gen` is the generation this barrier started in (tracked by thread 0).  The two
+// halves can be used apart (a split-phase barrier: arrive, do work that needs nothing from the others, then
+// wait); bar_arrive returns true for the last arriver, whose barrier is then already complete.
+__device__ __forceinline__ bool bar_arrive(unsigned* bar, unsigned nblocks, double* totals, unsigned gen)
 {
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
@@ -50,8 +51,15 @@ __device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigne
         for (int k = 0; k < 4; ++k) next[k] = 0.0;
         count.store(0u, cuda::memory_order_relaxed);
         genw.store(next_gen(gen), cuda::memory_order_release);
-        return true;
+        return true;  // last arriver: the barrier is complete
     }
+    return false;
+}
+
+// The waiting half: polls the generation until it leaves `gen` (bounded); false when the wait gave up.
+__device__ __forceinline__ bool bar_wait(unsigned* bar, int* err, unsigned gen)
+{
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
     cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
     unsigned long long spins = 0;
     const unsigned long long limit = c_spin_limit;
@@ -63,6 +71,12 @@ __device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigne
         if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) return false;
     }
     return true;
+}
+
+__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals, unsigned gen)
+{
+    if (bar_arrive(bar, nblocks, totals, gen)) return true;
+    return bar_wait(bar, err, gen);
 }
 
 __device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk)
@@ -185,6 +199,10 @@ struct SolverSmem {
 // on the cell type), sums ||b||^2, compacts the FLUID cells in cell order into w.list with their
 // in-domain-neighbour masks (per-block counts -> grid reduction -> block offsets -> ordered compaction), and
 // caches each thread's first list entries in s_list.  Returns false when a grid wait gave up.
+// Vector layouts whose non-FLUID entries the setup zeroes: the multigrid solver's separate arrays, the plain CG's
+// interleaved (r, w, s, p) cells.
+enum { kLayoutSeparate = 0, kLayoutInterleaved = 1 };
+
 struct SolverSetup {
     int F;          // FLUID cells
     double bnorm;   // ||b||_2
@@ -210,7 +228,7 @@ __device__ __forceinline__ uint32_t solve_mask(const uint8_t* __restrict__ marks
 
 __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w, const int blk, const int nblk,
                                              unsigned& gen, double* sh, uint32_t* s_warp, uint32_t* s_list,
-                                             SolverSetup& out, bool interleaved)
+                                             SolverSetup& out, int layout)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
     const int sxy = nx * ny;
@@ -238,7 +256,7 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
             acc[1] += 1.0;
         } else {
             p64[c] = 0.0;
-            if (interleaved) {  // the plain CG's (r, w, s, p) cells
+            if (layout == kLayoutInterleaved) {  // the single-pass CG's (r, w, s, p) cells
                 w.rws0[c] = make_float4(0.f, 0.f, 0.f, 0.f);
                 w.rws1[c] = make_float4(0.f, 0.f, 0.f, 0.f);
             } else {

@@ -102,6 +102,27 @@ class Scene:
         check(self._L.fe_scene_step_profiled(self._h, dt, nsub, arr, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return [arr[i].as_dict() for i in range(nsub)], ms[:nsub]
 
+    def checkpoint(self):
+        """The scene's state at this substep boundary, on the device (fe_scene_snapshot): a Snapshot to restore
+        into this scene or another one of the same grid and solver."""
+        h = ctypes.c_void_p()
+        check(self._L.fe_scene_snapshot(self._h, ctypes.byref(h)))
+        return Snapshot(h, self._L)
+
+    def restore(self, snap):
+        check(self._L.fe_scene_restore(self._h, snap.handle))
+
+    def set_tuning(self, multigrid=-1, cg_block_threads=0, mg_block_level_cells=0):
+        """Launch choices of the pressure solve (fe_scene_set_tuning); -1 / 0 keeps a field's current choice."""
+        t = _abi.Tuning(int(multigrid), int(cg_block_threads), int(mg_block_level_cells))
+        check(self._L.fe_scene_set_tuning(self._h, ctypes.byref(t)))
+
+    def tuning(self):
+        t = _abi.Tuning()
+        check(self._L.fe_scene_get_tuning(self._h, ctypes.byref(t)))
+        return {"multigrid": t.multigrid, "cg_block_threads": t.cg_block_threads,
+                "mg_block_level_cells": t.mg_block_level_cells}
+
     def set_stream(self, stream_handle):
         """Issues the scene's work on an external cudaStream_t (an int handle, e.g. torch stream.cuda_stream)."""
         check(self._L.fe_scene_set_stream(self._h, ctypes.c_void_p(stream_handle) if stream_handle else None))
@@ -279,6 +300,36 @@ class Scene:
         d = ctypes.c_double()
         check(self._L.fe_scene_divergence(self._h, ctypes.byref(d)))
         return d.value
+
+
+class Snapshot:
+    """A device-side checkpoint of a scene (fe_snapshot); freed by close() or when collected."""
+
+    def __init__(self, handle, L):
+        self._h = handle
+        self._L = L
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise ValueError("snapshot is closed")
+        return self._h
+
+    def info(self):
+        n, b = ctypes.c_uint64(), ctypes.c_uint64()
+        check(self._L.fe_snapshot_info(self.handle, ctypes.byref(n), ctypes.byref(b)))
+        return {"particles": int(n.value), "bytes": int(b.value)}
+
+    def close(self):
+        if self._h is not None:
+            self._L.fe_snapshot_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

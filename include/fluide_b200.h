@@ -311,6 +311,41 @@ fe_status fe_project_noalloc(const int32_t n[3], const double h[3], const uint8_
                              float* w, double* p, double rel_tol, int32_t max_it, void* stream,
                              fe_step_stats* stats);
 
+/* Launch choices of a scene's pressure solve that change its speed, not its result (every choice reaches the same
+ * FP64 relative residual).  No reference counterpart: they are what the autotuner (fe_scene_autotune) searches.
+ * In fe_scene_set_tuning a negative or zero field keeps the current choice. */
+typedef struct fe_tuning {
+    int32_t multigrid;            /* 1: multigrid-preconditioned CG, 0: plain CG (grids too small for a hierarchy stay plain) */
+    int32_t cg_block_threads;     /* threads per persistent solver block: 256, 512 or 1024 (1024 threads per SM in total) */
+    int32_t mg_block_level_cells; /* multigrid levels of at most this many cells are processed by one block */
+} fe_tuning;
+/* Applies `t` (the scene's captured substeps are captured again on the next step); multigrid = 1 allocates the
+ * hierarchy on first use. */
+fe_status fe_scene_set_tuning(fe_scene* s, const fe_tuning* t);
+fe_status fe_scene_get_tuning(fe_scene* s, fe_tuning* t);
+/* The autotuner: times every candidate launch choice of the scene's pressure solve -- the plain CG at 256 / 512 /
+ * 1024 threads per block, and (grids with a multigrid hierarchy, no colliders) the multigrid-preconditioned CG at
+ * 512 / 1024 threads with one-block levels up to 2048 or 4096 cells -- over `substeps` substeps of dt each from the scene's current state (CUDA events on the scene's stream,
+ * after one untimed substep that captures the choice's graphs), keeps the fastest whose solves all converged,
+ * restores the scene's state and applies the choice.  The choice is also stored for (device, grid, transfer):
+ * scenes created later with FE_PRESSURE_AUTO start from it.  best / best_ms (ms per substep) may be NULL. */
+fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, fe_tuning* best, float* best_ms);
+/* The autotuner's per-process store (e.g. filled from a file a previous process wrote): */
+fe_status fe_tuning_store(int32_t device, const int32_t n[3], int32_t solver, const fe_tuning* t);
+fe_status fe_tuning_lookup(int32_t device, const int32_t n[3], int32_t solver, fe_tuning* t);  /* FE_ERR_STATE: none */
+
+/* Per-job checkpoint / resume (no reference counterpart: FileSystem::SaveFrame, file_systems/file_system.cpp:14-17,
+ * is empty).  fe_scene_snapshot copies the scene's state at a substep boundary on the device -- its particles in
+ * slot order, the positions at the start of the last substep, the pressure warm start, the current velocity grid and
+ * the counters that steer the next substeps -- into memory from the scene's device pool; fe_scene_restore puts it
+ * back into a scene of the same grid, solver and device (the one it came from, or a fresh one), after which the scene
+ * steps as the original did from that point (within the solve tolerance: the solver's reduction order varies). */
+typedef struct fe_snapshot fe_snapshot;
+fe_status fe_scene_snapshot(fe_scene* s, fe_snapshot** out);
+fe_status fe_scene_restore(fe_scene* s, const fe_snapshot* snap);
+fe_status fe_snapshot_info(const fe_snapshot* snap, uint64_t* particles, uint64_t* bytes);
+fe_status fe_snapshot_destroy(fe_snapshot* snap);
+
 /* Stream the scene's work is issued on (a cudaStream_t); NULL selects the scene's own stream. */
 fe_status fe_scene_set_stream(fe_scene* s, void* stream);
 fe_status fe_scene_synchronize(fe_scene* s);

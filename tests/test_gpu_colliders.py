@@ -258,7 +258,12 @@ def test_enclosed_component_inconsistent_rhs_matches_oracle():
     assert o.cg_rel_residual() < 1e-9
     assert rel_l2(g.rhs(), o.rhs()) < 1e-12
     assert abs(g.rhs()[enc].sum()) < 1e-9 * np.abs(g.rhs()[enc]).sum()
-    assert rel_l2(pg, o.pressure()) < 1e-4
+    # the enclosed block's pressure is defined up to a constant (a pure-Neumann block): the solvers may drift
+    # apart along that constant by rounding, which changes no velocity, so it is removed before comparing
+    po = o.pressure()
+    pg = pg.copy()
+    pg[enc] -= (pg[enc] - po[enc]).mean()
+    assert rel_l2(pg, po) < 1e-4
     for a, b in zip((ug, vg, wg), o.grid()):
         assert rel_l2(a, b) < 1e-5
 

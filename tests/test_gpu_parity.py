@@ -275,3 +275,36 @@ def test_multigrid_iterations_bounded():
         stats[ps] = max(x["cg_iterations"] for x in st)
         g.close()
     assert stats[fe.MGPCG] < 40 < 200 < stats[fe.CG], stats
+
+
+@pytest.mark.parametrize("tuning", [dict(multigrid=0, cg_block_threads=1024),
+                                    dict(multigrid=0, cg_block_threads=512),
+                                    dict(multigrid=0, cg_block_threads=256),
+                                    dict(multigrid=1, cg_block_threads=1024, mg_block_level_cells=4096),
+                                    dict(multigrid=1, cg_block_threads=512, mg_block_level_cells=2048)])
+def test_tuning_choices_reach_the_oracle(tuning):
+    """Every launch choice the autotuner can make (fe_scene_set_tuning) solves to the same FP64 residual and the
+    oracle's pressure; only the speed differs."""
+    n = (40, 40, 40)
+    g, o, *_ = make_scene_pair(n, fe.FLIP, seed=13, cg_rel_tol=1e-8, oracle_tol=1e-12)
+    g.set_tuning(**tuning)
+    got = g.tuning()
+    for k, val in tuning.items():
+        assert got[k] == val, (k, got)
+    dt = 1 / 240
+    g.run_stages(dt, fe.STAGE_SORT, fe.STAGE_PRE)
+    u, v, w, _, _ = g.grid()
+    for st in ("p2g", "sdf"):
+        o.stage(st)
+    o.set_grid(u.astype(np.float64), v.astype(np.float64), w.astype(np.float64))
+    g.run_stages(dt, fe.STAGE_PRESSURE, fe.STAGE_PRESSURE)
+    o.stage("pressure", dt)
+    ug, vg, wg, pg, mg = g.grid()
+    assert np.array_equal(mg, o.marks())
+    assert rel_l2(pg, o.pressure()) < 1e-4
+    for a, b in zip((ug, vg, wg), o.grid()):
+        assert rel_l2(a, b) < 1e-5
+    # and whole substeps through the captured graphs
+    st = g.step(dt, 3)
+    assert all(x["converged"] == 1 and x["rel_residual"] <= 1e-8 for x in st), st
+    g.close()
