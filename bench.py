@@ -716,6 +716,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--ref-steps", type=int, default=1, help="substeps of the CPU reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="single workload: keep the default launch shape")
     ap.add_argument("--no-extras", action="store_true",
                     help="single workload: skip the accuracy-vs-oracle, batched and served objects of the line")
     ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
@@ -780,6 +781,17 @@ def main():
     scene.set_stream(stream.cuda_stream)
     scene.set_particles(pos, vel)
     scene.step(DT, args.warmup)
+    # launch shape of the pressure solve picked by the autotuner on this scene's state after the warm-up (untimed;
+    # the state is restored); the solver family stays the automatic choice, whose iteration count over a whole run
+    # the first substeps do not predict
+    tuning = None
+    if not args.no_autotune:
+        from fluide_engine_b200 import autotune
+
+        t0 = time.perf_counter()
+        choice, tuned_ms = autotune.tune(scene, DT, substeps=4, device=local, save=False, shape_only=True)
+        tuning = {"choice": choice, "ms_per_substep_in_search": tuned_ms, "search_s": time.perf_counter() - t0,
+                  "by": "fe_scene_autotune (FE_TUNE_SHAPE), 4 substeps per candidate"}
 
     def barrier():
         if world > 1:
@@ -870,7 +882,8 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 refinement)", "data": "synthetic (seeded analytic scene)",
-            "config": workload_config(n, args.steps, args.warmup, world, N, args.viscosity, args.collider),
+            "config": dict(workload_config(n, args.steps, args.warmup, world, N, args.viscosity, args.collider),
+                           tuning=tuning),
             "roofline": {"bound": "hbm",
                          "kernel": ("k_mgcg (persistent multigrid-preconditioned FP32 CG + FP64 refinement, one "
                                     "launch/substep)" if multigrid else

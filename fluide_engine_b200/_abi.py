@@ -12,6 +12,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libfluide_b200.so")
 
 FE_OK = 0
+TUNE_ALL, TUNE_SHAPE = 0, 1
 FE_ERR_CUDA, FE_ERR_BAD_ARG, FE_ERR_OOM, FE_ERR_NOT_CONVERGED, FE_ERR_TIMEOUT, FE_ERR_STATE, FE_ERR_NO_DEVICE = range(1, 8)
 PIC, FLIP, APIC = 0, 1, 2
 AUTO, MGPCG, CG = 0, 1, 2  # fe_pressure_solver
@@ -166,7 +167,7 @@ def lib():
     L.fe_scene_restore.argtypes = [P, P]
     L.fe_snapshot_info.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.fe_snapshot_destroy.argtypes = [P]
-    L.fe_scene_autotune.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(Tuning),
+    L.fe_scene_autotune.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Tuning),
                                     ctypes.POINTER(ctypes.c_float)]
     L.fe_tuning_store.argtypes = [ctypes.c_int32, P, ctypes.c_int32, ctypes.POINTER(Tuning)]
     L.fe_tuning_lookup.argtypes = [ctypes.c_int32, P, ctypes.c_int32, ctypes.POINTER(Tuning)]

@@ -98,12 +98,14 @@ def load(device=0, path=None):
     return len(entries)
 
 
-def tune(scene, dt, substeps=6, device=0, path=None, save=True):
+def tune(scene, dt, substeps=6, device=0, path=None, save=True, shape_only=False):
     """Runs the search on `scene` (its state is restored afterwards), applies and returns the fastest choice with
-    its ms per substep; with save, merges it into this GPU model's file."""
+    its ms per substep; shape_only keeps the scene's solver family (plain or multigrid CG) and searches its launch
+    shapes; with save, merges the choice into this GPU model's file."""
     best = _abi.Tuning()
     ms = ctypes.c_float()
-    _abi.check(_abi.lib().fe_scene_autotune(scene.handle, float(dt), int(substeps), ctypes.byref(best),
+    scope = _abi.TUNE_SHAPE if shape_only else _abi.TUNE_ALL
+    _abi.check(_abi.lib().fe_scene_autotune(scene.handle, float(dt), int(substeps), scope, ctypes.byref(best),
                                             ctypes.byref(ms)))
     choice = to_dict(best)
     if save:

@@ -2331,23 +2331,26 @@ fe_status fe_tuning_lookup(int32_t device, const int32_t n[3], int32_t solver, f
     return FE_OK;
 }
 
-fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, fe_tuning* best, float* best_ms)
+fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, int32_t scope, fe_tuning* best, float* best_ms)
 {
-    if (!s || !(dt > 0.0) || substeps < 1) return set_error(FE_ERR_BAD_ARG, "bad autotune arguments");
+    if (!s || !(dt > 0.0) || substeps < 1 || scope < FE_TUNE_ALL || scope > FE_TUNE_SHAPE)
+        return set_error(FE_ERR_BAD_ARG, "bad autotune arguments");
     if (!s->have_particles || s->base.np == 0) return set_error(FE_ERR_STATE, "autotune needs particles");
     // candidates: the plain CG at 256 / 512 / 1024 threads per block and, where the grid has a multigrid hierarchy
     // and no colliders, the multigrid-preconditioned CG at 512 / 1024 threads with one-block levels up to 2048 or
     // 4096 cells
-    std::vector<fe_tuning> cand;
-    for (int th : {1024, 512, 256}) cand.push_back(fe_tuning{0, th, 4096});
-    MgLevel lv[kMaxMgLevels];
-    const SceneView& b = s->base;
-    if (mg_plan(b.g.nx, b.g.ny, b.g.nz, b.h, lv) >= 2 && s->colliders.count == 0)
-        for (int th : {1024, 512})
-            for (int cells : {4096, 2048}) cand.push_back(fe_tuning{1, th, cells});
     fe_tuning before;
     fe_status st = fe_scene_get_tuning(s, &before);
     if (st != FE_OK) return st;
+    std::vector<fe_tuning> cand;
+    MgLevel lv[kMaxMgLevels];
+    const SceneView& b = s->base;
+    const bool mg_ok = mg_plan(b.g.nx, b.g.ny, b.g.nz, b.h, lv) >= 2 && s->colliders.count == 0;
+    if (scope == FE_TUNE_ALL || before.multigrid == 0)
+        for (int th : {1024, 512, 256}) cand.push_back(fe_tuning{0, th, 4096});
+    if (mg_ok && (scope == FE_TUNE_ALL || before.multigrid == 1))
+        for (int th : {1024, 512})
+            for (int cells : {4096, 2048}) cand.push_back(fe_tuning{1, th, cells});
     fe_snapshot* snap = nullptr;
     st = fe_scene_snapshot(s, &snap);
     if (st != FE_OK) return st;

@@ -323,13 +323,20 @@ typedef struct fe_tuning {
  * hierarchy on first use. */
 fe_status fe_scene_set_tuning(fe_scene* s, const fe_tuning* t);
 fe_status fe_scene_get_tuning(fe_scene* s, fe_tuning* t);
+/* Search scope of the autotuner: every candidate, or only the launch shapes of the scene's current solver family
+ * (plain or multigrid CG).  The family's iteration count can change over a run (the multigrid solver's grows as the
+ * free surface gets ragged), so a family picked from the first substeps need not stay the faster one; the shape of
+ * a given family does not depend on that. */
+enum { FE_TUNE_ALL = 0, FE_TUNE_SHAPE = 1 };
 /* The autotuner: times every candidate launch choice of the scene's pressure solve -- the plain CG at 256 / 512 /
  * 1024 threads per block, and (grids with a multigrid hierarchy, no colliders) the multigrid-preconditioned CG at
- * 512 / 1024 threads with one-block levels up to 2048 or 4096 cells -- over `substeps` substeps of dt each from the scene's current state (CUDA events on the scene's stream,
+ * 512 / 1024 threads with one-block levels up to 2048 or 4096 cells; with FE_TUNE_SHAPE only the current family's --
+ * over `substeps` substeps of dt each from the scene's current state (CUDA events on the scene's stream,
  * after one untimed substep that captures the choice's graphs), keeps the fastest whose solves all converged,
  * restores the scene's state and applies the choice.  The choice is also stored for (device, grid, transfer):
  * scenes created later with FE_PRESSURE_AUTO start from it.  best / best_ms (ms per substep) may be NULL. */
-fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, fe_tuning* best, float* best_ms);
+fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, int32_t scope, fe_tuning* best,
+                            float* best_ms);
 /* The autotuner's per-process store (e.g. filled from a file a previous process wrote): */
 fe_status fe_tuning_store(int32_t device, const int32_t n[3], int32_t solver, const fe_tuning* t);
 fe_status fe_tuning_lookup(int32_t device, const int32_t n[3], int32_t solver, fe_tuning* t);  /* FE_ERR_STATE: none */
