@@ -466,6 +466,21 @@ def run_pool(args):
     return 0
 
 
+def tune_scenes(make_scene, keys, dt, device=0):
+    """Runs the autotuner (all candidates) once per (grid, transfer) key on a scene make_scene(key) builds, a few
+    substeps after it starts; the choices go into the library's table, so the scenes both arms create afterwards
+    (automatic solver choice) start from them.  Returns {key: (choice, ms per substep)}."""
+    from fluide_engine_b200 import autotune
+
+    out = {}
+    for key in keys:
+        sc = make_scene(key)
+        sc.step(dt, 2, stats=False)
+        out[key] = autotune.tune(sc, dt, substeps=3, device=device, save=False)
+        sc.close()
+    return out
+
+
 def batched_measure(n_scenes=48, steps=50, warmup=5, device=0):
     """Batched independent scenes vs the same scenes one at a time on the plain single-scene path.
 
@@ -486,14 +501,23 @@ def batched_measure(n_scenes=48, steps=50, warmup=5, device=0):
         solver = int(rng.integers(0, 3))
         specs.append((n, solver, tuple(float(e) for e in ext), k))
 
+    def make(spec):
+        n, solver, ext, k = spec
+        pos, vel = fe.seed_regions([dict(kind=0, lo=(0.0, 0.0, 0.0), hi=ext)], (n, n, n), seed=k)
+        sc = fe.Scene((n, n, n), solver=solver, max_cfl=1.0, cg_rel_tol=1e-6, device=device)
+        sc.set_particles(pos, vel)
+        return sc
+
     def build():
-        out = []
-        for n, solver, ext, k in specs:
-            pos, vel = fe.seed_regions([dict(kind=0, lo=(0.0, 0.0, 0.0), hi=ext)], (n, n, n), seed=k)
-            sc = fe.Scene((n, n, n), solver=solver, max_cfl=1.0, cg_rel_tol=1e-6, device=device)
-            sc.set_particles(pos, vel)
-            out.append(sc)
-        return out
+        return [make(sp) for sp in specs]
+
+    # the autotuner's choice per (grid, transfer), tuned on the first scene of each kind; both arms use it
+    first = {}
+    for sp in specs:
+        first.setdefault((sp[0], sp[1]), sp)
+    t0 = time.perf_counter()
+    tuned = tune_scenes(lambda key: make(first[key]), sorted(first), DT, device)
+    tune_s = time.perf_counter() - t0
 
     # one at a time (each scene's own graph-captured substeps, scene after scene)
     scenes = build()
@@ -539,6 +563,8 @@ def batched_measure(n_scenes=48, steps=50, warmup=5, device=0):
             "batched_over_one_at_a_time": v_batch / v_alone,
             "accuracy": {"rel_residual_max_batched": max(res_batch), "rel_residual_max_alone": max(res_alone),
                          "converged_all": conv},
+            "tuning": {"%d^3 %s" % (n, ["PIC", "FLIP", "APIC"][sv]): choice for (n, sv), (choice, _) in tuned.items()},
+            "tuning_s": tune_s,
             "gpu_launches": int(launches)}
 
 
@@ -568,6 +594,21 @@ def served_measure(rate, seconds, res, fr, budget_gb, max_batch, device=0):
     from fluide_engine_b200 import serving
 
     jobs = serving.poisson_trace(rate, seconds, 3, resolutions=res, frames=fr)
+    # the autotuner's choice per job resolution (tuned on the first job of each), used by both arms' scenes
+    first = {}
+    for j in jobs:
+        first.setdefault(j.n, j)
+
+    def make(n):
+        j = first[n]
+        pos, vel = fe.seed_regions(j.regions, (n,) * 3, seed=j.seed)
+        sc = fe.Scene((n,) * 3, solver=j.solver, max_cfl=1.0, cg_rel_tol=1e-6, device=device)
+        sc.set_particles(pos, vel)
+        return sc
+
+    t0 = time.perf_counter()
+    tuned = tune_scenes(make, sorted(first), jobs[0].dt, device)
+    tune_s = time.perf_counter() - t0
     srv = serving.Server(hbm_budget_bytes=int(budget_gb * 1e9), max_batch=max_batch, device=device)
     for j in jobs:
         srv.submit(j)
@@ -616,7 +657,8 @@ def served_measure(rate, seconds, res, fr, budget_gb, max_batch, device=0):
                                       "the queueing delay before a job starts"},
             "served_over_one_at_a_time": served / (ps_alone / t_alone), "wall_s": wall,
             "server_time_s": dict(srv.timing), "batch_rebuilds": srv.rebuilds, "scenes_reused": srv.reused,
-            "device_step_ratio": alone_split["step"] / max(srv.timing["step"], 1e-9)}
+            "device_step_ratio": alone_split["step"] / max(srv.timing["step"], 1e-9),
+            "tuning": {"%d^3" % n: choice for n, (choice, _) in tuned.items()}, "tuning_s": tune_s}
 
 
 def run_served(args):

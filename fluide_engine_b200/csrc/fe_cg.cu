@@ -174,7 +174,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
             const int c = (int)(entry(k, e) >> 6);
             p64[c] += (double)X[c];
         }
-        if (!grid_sync(w, gen, nblk)) return;
+        if (!grid_sync(w, gen, nblk, sh)) return;
     }
     if (blk == 0 && threadIdx.x == 0 && out_its) {
         *out_its = total_it;
@@ -196,22 +196,25 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgParams prm)
 {
     __shared__ SolverSmem smem;
+    cluster_begin(w, smem.sh);
     cg_body(smem, v, w, prm, blockIdx.x, gridDim.x);
+    cluster_end(w);
 }
 
 // The same solve with the multigrid-preconditioned inner loop (fe_mg_body.cuh).
 __global__ void __launch_bounds__(kCgThreads, 1) k_mgcg(SceneView v, CgWork w, MgWork mg, CgParams prm)
 {
     __shared__ SolverSmem smem;
+    cluster_begin(w, smem.sh);
     mg_body(smem, v, w, mg, prm, blockIdx.x, gridDim.x);
+    cluster_end(w);
 }
 
 // Many scenes in one cooperative launch: blocks [start[s], start[s+1]) solve scene s with their own barrier
-// and reductions, so scenes iterate independently and concurrently.  Every scene uses the plain CG body
-// here: its one barrier per iteration overlaps with the other scenes' barriers, and the multigrid body would
-// more than double this kernel's registers (fewer co-resident blocks for every scene of the batch).  A
-// scene's own multigrid setting applies when it steps alone.
-__global__ void __launch_bounds__(kMultiThreads) k_multi_cg(MultiCgScene* __restrict__ scenes, int S)
+// and reductions, so scenes iterate independently and concurrently.  Each scene runs the solver body it runs
+// alone: the plain CG body, or the multigrid-preconditioned body for scenes tuned to it (both fit the kernel's
+// register budget of 3 co-resident 256-thread blocks per SM).
+__global__ void __launch_bounds__(kMultiThreads, 3) k_multi_cg(MultiCgScene* __restrict__ scenes, int S)
 {
     int sc = 0;
     while (sc + 1 < S && (int)blockIdx.x >= scenes[sc + 1].block_start) ++sc;
@@ -227,7 +230,8 @@ __global__ void __launch_bounds__(kMultiThreads) k_multi_cg(MultiCgScene* __rest
     int its = 0, fluid = 0;
     const int blk = (int)blockIdx.x - m.block_start;
     __shared__ SolverSmem smem;
-    cg_body(smem, m.view, m.work, prm, blk, m.block_count, &its, &fluid);
+    if (m.use_mg) mg_body(smem, m.view, m.work, m.mg, prm, blk, m.block_count, &its, &fluid);
+    else cg_body(smem, m.view, m.work, prm, blk, m.block_count, &its, &fluid);
     if (blk == 0 && threadIdx.x == 0) {  // read by the next solve's k_multi_partition
         m.last_its = its;
         m.last_fluid = fluid;
@@ -238,20 +242,28 @@ __global__ void __launch_bounds__(kMultiThreads) k_multi_cg(MultiCgScene* __rest
 // proportion to the previous solve's work of the scene (FLUID cells x (inner iterations + 3 residual
 // passes); weight0 before its first solve), leftovers to the heaviest scenes.  Scenes then take about
 // equally long, instead of the scene with the most iterations finishing last on a small share.
+// Relative cost of one inner iteration per FLUID cell: the multigrid body's passes and grid barriers (4 L - 2 per
+// iteration) against the plain body's one.
+__device__ __forceinline__ double multi_work(const MultiCgScene& m)
+{
+    if (m.last_its < 0) return m.weight0;
+    const double per_it = m.use_mg ? 12.0 : 1.0;
+    return (double)m.last_fluid * ((double)m.last_its * per_it + 3.0);
+}
+
 __global__ void k_multi_partition(MultiCgScene* __restrict__ scenes, int S, int total_blocks)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double wsum = 0.0;
     for (int i = 0; i < S; ++i) {
         const MultiCgScene& m = scenes[i];
-        const double w = m.last_its >= 0 ? (double)m.last_fluid * (double)(m.last_its + 3) : m.weight0;
-        wsum += fmax(w, 0.0);
+        wsum += fmax(multi_work(m), 0.0);
     }
     const int spare = total_blocks - S;
     int start = 0, used = 0;
     for (int i = 0; i < S; ++i) {
         MultiCgScene& m = scenes[i];
-        const double w = fmax(m.last_its >= 0 ? (double)m.last_fluid * (double)(m.last_its + 3) : m.weight0, 0.0);
+        const double w = fmax(multi_work(m), 0.0);
         const int extra = wsum > 0.0 ? (int)floor(spare * (w / wsum)) : spare / S;
         m.block_count = 1 + extra;
         used += 1 + extra;
@@ -262,8 +274,7 @@ __global__ void k_multi_partition(MultiCgScene* __restrict__ scenes, int S, int 
         double bw = -1.0;
         for (int i = 0; i < S; ++i) {
             const MultiCgScene& m = scenes[i];
-            double w = m.last_its >= 0 ? (double)m.last_fluid * (double)(m.last_its + 3) : m.weight0;
-            w = w / (double)m.block_count;  // work per block: give the block where it is most needed
+            const double w = multi_work(m) / (double)m.block_count;  // work per block: give it where most needed
             if (w > bw) {
                 bw = w;
                 best = i;
@@ -318,9 +329,11 @@ cudaError_t launch_multi_cg(MultiCgScene* scenes, int S, int total_blocks, cudaS
     return e;
 }
 
-cudaError_t cg_prepare(CgWork& w, int device, int threads)
+cudaError_t cg_prepare(CgWork& w, int device, int threads, int cluster)
 {
     if (threads != 256 && threads != 512 && threads != 1024) return cudaErrorInvalidValue;
+    if (cluster < 1) cluster = 1;
+    if (cluster > kMaxCluster || (cluster & (cluster - 1)) != 0) return cudaErrorInvalidValue;
     int sms = 0, per_sm = 0, per_sm_mg = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
@@ -332,9 +345,33 @@ cudaError_t cg_prepare(CgWork& w, int device, int threads)
     const int want = kCgThreads / threads;
     const int per = std::min(want, std::min(per_sm, per_sm_mg));
     if (per < 1) return cudaErrorCooperativeLaunchTooLarge;
-    if (sms * per > kMaxCgBlocks) return cudaErrorCooperativeLaunchTooLarge;
-    w.blocks = sms * per;
+    int blocks = sms * per;
+    if (cluster > 1) {
+        // whole clusters only, as many as the device holds at once for both solver kernels
+        int clusters = blocks / cluster;
+        for (int kind = 0; kind < 2; ++kind) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)(clusters * cluster));
+            cfg.blockDim = dim3((unsigned)threads);
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)cluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int n = 0;
+            e = kind == 0 ? cudaOccupancyMaxActiveClusters(&n, k_cg, &cfg) : cudaOccupancyMaxActiveClusters(&n, k_mgcg, &cfg);
+            if (e != cudaSuccess) return e;
+            clusters = std::min(clusters, n);
+        }
+        if (clusters < 1) return cudaErrorCooperativeLaunchTooLarge;
+        blocks = clusters * cluster;
+    }
+    if (blocks > kMaxCgBlocks) return cudaErrorCooperativeLaunchTooLarge;
+    w.blocks = blocks;
     w.threads = threads;
+    w.cluster = cluster;
     return cudaSuccess;
 }
 
@@ -384,11 +421,15 @@ cudaError_t launch_mgcg(const SceneView& v, const CgWork& w, const MgWork& mg, d
     cfg.gridDim = dim3((unsigned)w.blocks);
     cfg.blockDim = dim3((unsigned)w.threads);
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
+    attr[1].id = cudaLaunchAttributeClusterDimension;
+    attr[1].val.clusterDim.x = (unsigned)std::max(w.cluster, 1);
+    attr[1].val.clusterDim.y = 1;
+    attr[1].val.clusterDim.z = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = w.cluster > 1 ? 2 : 1;
     cudaError_t e = cudaLaunchKernelEx(&cfg, k_mgcg, v, w, mg, prm);
     count_launch();
     return e;
@@ -409,11 +450,15 @@ cudaError_t launch_cg(const SceneView& v, const CgWork& w, double rel_tol, doubl
     cfg.gridDim = dim3((unsigned)w.blocks);
     cfg.blockDim = dim3((unsigned)w.threads);
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
+    attr[1].id = cudaLaunchAttributeClusterDimension;
+    attr[1].val.clusterDim.x = (unsigned)std::max(w.cluster, 1);
+    attr[1].val.clusterDim.y = 1;
+    attr[1].val.clusterDim.z = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = w.cluster > 1 ? 2 : 1;
     cudaError_t e = cudaLaunchKernelEx(&cfg, k_cg, v, w, prm);
     count_launch();
     return e;

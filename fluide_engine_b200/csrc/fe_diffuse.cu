@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
     k_jacobi(DiffWork d, CgWork w, FaceArrays3 fa, JacobiParams prm)
 {
     double* __restrict__ snap = d.snap;
-    __shared__ double sh[32 * 4 + 4];
+    __shared__ double sh[kShDoubles];
     extern __shared__ unsigned long long s_ent[];  // [kJacobiCache] entries, then [kJacobiCache] floats
     float* s_b = (float*)(s_ent + kJacobiCache);
     const int nblk = gridDim.x, blk = blockIdx.x;
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
                 ctl.take = next_take;
                 ctl.cmp = next_cmp;
             }
-        } else if (!grid_sync(w, gen, nblk)) {
+        } else if (!grid_sync(w, gen, nblk, sh)) {
             return;
         }
         if (threadIdx.x == 0) {
@@ -403,7 +403,9 @@ cudaError_t launch_diffuse(const SceneView& v, const DiffWork& d, const CgWork& 
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_jacobi, d, w, fa, prm);
+    CgWork jw = w;
+    jw.cluster = 1;  // the Jacobi kernel shares the solver's barrier words, never its cluster launch
+    e = cudaLaunchKernelEx(&cfg, k_jacobi, d, jw, fa, prm);
     count_launch();
     return e;
 }

@@ -18,6 +18,7 @@ namespace {
 struct G2PArgs {
     float dt_sub;
     int nsub;
+    int same_origins;        // the FLIP residual grid's data origins equal the velocity grid's (domain origin 0)
     float dom_lo[3], dom_hi[3];
     const float *u, *v, *w;  // final velocity buffers
 };
@@ -42,6 +43,28 @@ __device__ __forceinline__ float sample_diff(const float* __restrict__ a, const 
                          lerpf_ref(FE_D(s.i, s.jp, s.kp), FE_D(s.ip, s.jp, s.kp), s.fx), s.fy);
 #undef FE_D
     return lerpf_ref(b0, b1, s.fz);
+}
+
+// The FLIP residual sample and the plain sample of the same face array at the same stencil (the residual grid and
+// the velocity grid share their data origins when the domain origin is zero): one load of each face value serves
+// both Lerp trees.
+__device__ __forceinline__ void sample_diff_and_plain(const float* __restrict__ a, const float* __restrict__ b,
+                                                      const Stencil& s, int sx, int sy, float& diff, float& plain)
+{
+    float av[8], dv[8];
+    const int ii[2] = {s.i, s.ip}, jj[2] = {s.j, s.jp}, kk[2] = {s.k, s.kp};
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const size_t f = idx3(ii[t & 1], jj[(t >> 1) & 1], kk[t >> 2], sx, sy);
+        av[t] = __ldg(a + f);
+        dv[t] = av[t] - __ldg(b + f);
+    }
+    float b0 = lerpf_ref(lerpf_ref(dv[0], dv[1], s.fx), lerpf_ref(dv[2], dv[3], s.fx), s.fy);
+    float b1 = lerpf_ref(lerpf_ref(dv[4], dv[5], s.fx), lerpf_ref(dv[6], dv[7], s.fx), s.fy);
+    diff = lerpf_ref(b0, b1, s.fz);
+    b0 = lerpf_ref(lerpf_ref(av[0], av[1], s.fx), lerpf_ref(av[2], av[3], s.fx), s.fy);
+    b1 = lerpf_ref(lerpf_ref(av[4], av[5], s.fx), lerpf_ref(av[6], av[7], s.fx), s.fy);
+    plain = lerpf_ref(b0, b1, s.fz);
 }
 
 // sum_t gradweight_t * face_t for one velocity component (apic_simulator.cpp:311-336).
@@ -87,12 +110,26 @@ __global__ void __launch_bounds__(256) k_g2p(SceneView v, G2PArgs g)
             const Stencil su = stencil(x, y, z, v.rxo, v.inv_hf, nx + 1, ny, nz);
             const Stencil sv = stencil(x, y, z, v.ryo, v.inv_hf, nx, ny + 1, nz);
             const Stencil sw = stencil(x, y, z, v.rzo, v.inv_hf, nx, ny, nz + 1);
-            float flip[3] = {v.vx[p] + sample_diff(g.u, v.su, su, nx + 1, ny),
-                             v.vy[p] + sample_diff(g.v, v.sv, sv, nx, ny + 1),
-                             v.vz[p] + sample_diff(g.w, v.sw, sw, nx, ny)};
-            if (v.blend > 0.f) {
-                sample_vel(v, g, x, y, z, pic);
+            float flip[3];
+            if (g.same_origins && v.blend > 0.f) {
+                float d[3];
+                sample_diff_and_plain(g.u, v.su, su, nx + 1, ny, d[0], pic[0]);
+                sample_diff_and_plain(g.v, v.sv, sv, nx, ny + 1, d[1], pic[1]);
+                sample_diff_and_plain(g.w, v.sw, sw, nx, ny, d[2], pic[2]);
+                flip[0] = v.vx[p] + d[0];
+                flip[1] = v.vy[p] + d[1];
+                flip[2] = v.vz[p] + d[2];
                 have_pic = true;
+            } else {
+                flip[0] = v.vx[p] + sample_diff(g.u, v.su, su, nx + 1, ny);
+                flip[1] = v.vy[p] + sample_diff(g.v, v.sv, sv, nx, ny + 1);
+                flip[2] = v.vz[p] + sample_diff(g.w, v.sw, sw, nx, ny);
+                if (v.blend > 0.f) {
+                    sample_vel(v, g, x, y, z, pic);
+                    have_pic = true;
+                }
+            }
+            if (v.blend > 0.f) {
 #pragma unroll
                 for (int a = 0; a < 3; ++a) flip[a] = (1.f - v.blend) * flip[a] + v.blend * pic[a];
             }
@@ -190,6 +227,9 @@ cudaError_t launch_g2p(const SceneView& v, double dt, bool do_g2p, bool do_move,
         g.dom_lo[a] = (float)v.origin[a];
         g.dom_hi[a] = (float)(v.origin[a] + v.size[a]);
     }
+    g.same_origins = 1;
+    for (int a = 0; a < 3; ++a)
+        g.same_origins &= (v.rxo[a] == v.xo[a] && v.ryo[a] == v.yo[a] && v.rzo[a] == v.zo[a]) ? 1 : 0;
     g.u = v.u;  // after the post group the velocity is back in buffer A
     g.v = v.v;
     g.w = v.w;

@@ -238,10 +238,11 @@ struct CgWork {
     fe_step_stats* stats;   // device ring of solve statistics
     unsigned stats_cap;     // entries of that ring (solves wrap around it)
     int blocks, threads;
+    int cluster;            // thread-block cluster size of the persistent solver launch (0 / 1: no clusters)
 };
 // Persistent-solver launch shape: `threads` per block (256, 512 or 1024), as many blocks per SM as make 1024
 // threads, all co-resident.
-cudaError_t cg_prepare(CgWork& w, int device, int threads = 1024);
+cudaError_t cg_prepare(CgWork& w, int device, int threads = 1024, int cluster = 1);
 // Bounded-wait limits of the pressure solvers' grid barrier on the current device (spin_limit 0: the default;
 // extra_arrivals > 0 makes every barrier wait for blocks that do not exist, so each wait runs out).
 cudaError_t set_solver_barrier_limits(unsigned long long spin_limit, unsigned extra_arrivals);
@@ -280,6 +281,8 @@ int mg_block_from(const MgLevel* lv, int levels, int block_cells);
 struct MultiCgScene {
     SceneView view;
     CgWork work;
+    MgWork mg;                     // the scene's multigrid hierarchy (used when use_mg)
+    int use_mg;                    // solve this scene with the multigrid-preconditioned body
     double rel_tol, inner_tol;
     int max_it, max_refine;
     int block_start, block_count;  // this scene's block range, re-split before every solve

@@ -56,7 +56,7 @@ __device__ __forceinline__ bool visited(const SceneView& v, int pbx, int pby, in
 
 // One thread per particle: the nodes within r of it (2 per axis for cubic cells, where 2r = 1.7 h;
 // more along an axis whose spacing is finer than max(h)) get the reference's exact FP64 test.
-__global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double crit_eps)
+__global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double rin2, double crit_eps)
 {
     uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (p >= v.np) return;
@@ -81,11 +81,11 @@ __global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double cri
                 if (pb[0] != v.q_b0[0][i] && pb[0] != v.q_b1[0][i]) continue;
                 const double d2 = dist2_ref(X[0], X[1], X[2], v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]);
                 if (!(d2 <= R2)) continue;
-                const double dist = __dsqrt_rn(d2);
                 const size_t c = idx3(i, j, k, n[0], n[1]);
-                if (dist < v.radius) v.marks[c] = FE_CELL_FLUID;
+                // sqrt(d2) < r exactly when d2 <= rin2 (correctly rounded sqrt is monotonic): no square root
+                if (d2 <= rin2) v.marks[c] = FE_CELL_FLUID;
                 if (v.any_inexact && !(v.q_exact[0][i] && v.q_exact[1][j] && v.q_exact[2][k]) &&
-                    fabs(dist - v.radius) <= crit_eps) {
+                    fabs(__dsqrt_rn(d2) - v.radius) <= crit_eps) {
                     unsigned* word = (unsigned*)(v.crit_flag + (c & ~(size_t)3));
                     unsigned bit = 1u << (8 * (c & 3));
                     if (!(atomicOr(word, bit) & bit)) {
@@ -272,6 +272,16 @@ __global__ void k_face_mark(SceneView v, DiffWork d)
 }
 }  // namespace
 
+// Largest double d with sqrt(d) < r (sqrt correctly rounded, as IEEE 754 requires of the host's and the device's
+// square root): the marking test sqrt(d2) < r becomes d2 <= sqrt_below(r), with the same outcome for every d2.
+static double sqrt_below(double r)
+{
+    double t = r * r;
+    while (t > 0.0 && std::sqrt(t) >= r) t = std::nextafter(t, 0.0);
+    while (std::sqrt(std::nextafter(t, HUGE_VAL)) < r) t = std::nextafter(t, HUGE_VAL);
+    return t;
+}
+
 cudaError_t launch_mark(const SceneView& v, cudaStream_t st)
 {
     const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
@@ -283,7 +293,7 @@ cudaError_t launch_mark(const SceneView& v, cudaStream_t st)
         if ((e = cudaMemsetAsync(v.crit_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     }
     if (v.np > 0) {
-        k_mark<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, R2, 1e-9 * v.radius);
+        k_mark<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, R2, sqrt_below(v.radius), 1e-9 * v.radius);
         count_launch();
         if (v.any_inexact) {
             k_mark_fixup<<<148, 128, 0, st>>>(v, R2, (uint32_t)nc);

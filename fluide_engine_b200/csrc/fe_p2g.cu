@@ -10,9 +10,10 @@
 // B200 design: one CTA per 8x8x8-cell tile and one thread per cell of it.  The tile's particles are one
 // contiguous run of the sorted arrays (fe_keys.h) and a cell's particles a contiguous piece of that run, so
 // each thread walks its own cell's particles and sums their contributions in registers.  With the domain origin
-// at zero every face a particle of cell (cx, cy, cz) can touch has indices within one of the cell's (the clamps
-// of GetBarycentric included), so a thread's sums live in 27 slots per component -- (numerator, weight) of the
-// faces (cx + a, cy + b, cz + c), a, b, c in {-1, 0, 1} -- plus a 27-bit touched mask.  Only then does the
+// at zero the faces a particle of cell (cx, cy, cz) touches lie in a window around the cell -- faces c and c + 1
+// along the component's own axis, c - 1 .. c + 1 along the two others (the clamps of GetBarycentric at the domain
+// walls excepted: those particles take the direct path below) -- so a thread's sums live in 18 slots per
+// component, (numerator, weight) per window face, plus a touched mask.  Only then does the
 // thread add its touched slots into the tile's 10x10x10 face box in shared memory: one shared atomic per
 // (cell, face) pair instead of one per (particle, face) pair, and the 32 lanes of an atomic instruction hit 32
 // different faces.  Cells with more than kCellCap particles (particles clamped onto a wall pile up in one
@@ -128,65 +129,157 @@ __device__ void splat_direct(const SceneView& v, const P2gComp& k, const Stencil
     }
 }
 
-// One particle of cell (cx, cy, cz) into the cell's 27 slots for component c; returns false (and adds nothing)
-// when its stencil leaves the window, in which case the caller takes the direct path.
-template <int SOLVER>
+// Window of component C's faces around a cell: along the component's own (staggered) axis a particle of cell c
+// touches faces c and c + 1, along the two other axes c - 1 .. c + 1.  Slot (i, j, k) of the window is face
+// (cx + lo<C>(0) + i, cy + lo<C>(1) + j, cz + lo<C>(2) + k), slot index i + W0 (j + W1 k).
+template <int C> __host__ __device__ constexpr int win(int axis) { return axis == C ? 2 : 3; }
+template <int C> __host__ __device__ constexpr int wlo(int axis) { return axis == C ? 0 : -1; }
+template <int C> __host__ __device__ constexpr int nslots() { return win<C>(0) * win<C>(1) * win<C>(2); }  // 18
+
+// One particle of cell (cx, cy, cz) into the cell's 18 slots of component C; returns false (and adds nothing)
+// when its stencil leaves the window, in which case the caller takes the direct path.  The trilinear weight of
+// slot (i, j, k) is wx_i wy_j wz_k, so the sums are formed as wx_i (wy_j wz_k v) per (j, k) pair: 2 FMAs per slot
+// (APIC: v + C . (x_face - x_p) splits the same way, 3 FMAs per slot).
+template <int SOLVER, int C>
 __device__ __forceinline__ bool splat_slots(const SceneView& v, const P2gComp& k, const Stencil& s,
-                                            const P2gParticle<SOLVER>& q, int cx, int cy, int cz, float (&num)[27],
-                                            float (&den)[27], uint32_t& mask)
+                                            const P2gParticle<SOLVER>& q, int cx, int cy, int cz,
+                                            float (&num)[nslots<C>()], float (&den)[nslots<C>()], uint32_t& mask)
 {
+    constexpr int W0 = win<C>(0), W1 = win<C>(1), W2 = win<C>(2);
+    constexpr int L0 = wlo<C>(0), L1 = wlo<C>(1), L2 = wlo<C>(2);
     const int oi = s.i - cx, oip = s.ip - cx, oj = s.j - cy, ojp = s.jp - cy, ok = s.k - cz, okp = s.kp - cz;
-    if (oi < -1 || oip > 1 || oj < -1 || ojp > 1 || ok < -1 || okp > 1) return false;
-    // 1D weights and touched bits on the window offsets -1, 0, 1 (i and ip coincide only on a one-face axis)
-    float wx[3], wy[3], wz[3];
+    if (oi < L0 || oip > L0 + W0 - 1 || oj < L1 || ojp > L1 + W1 - 1 || ok < L2 || okp > L2 + W2 - 1) return false;
+    // 1D weights and touched bits on the window (i and ip coincide only on a one-face axis)
+    float wx[W0], wy[W1], wz[W2];
     uint32_t tx = 0, ty = 0, tz = 0;
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        const int o = r - 1;
-        wx[r] = (oi == o ? 1.f - s.fx : 0.f) + (oip == o ? s.fx : 0.f);
-        wy[r] = (oj == o ? 1.f - s.fy : 0.f) + (ojp == o ? s.fy : 0.f);
-        wz[r] = (ok == o ? 1.f - s.fz : 0.f) + (okp == o ? s.fz : 0.f);
-        tx |= (oi == o || oip == o) ? 1u << r : 0u;
-        ty |= (oj == o || ojp == o) ? 1u << r : 0u;
-        tz |= (ok == o || okp == o) ? 1u << r : 0u;
+    for (int r = 0; r < W0; ++r) {
+        wx[r] = (oi == L0 + r ? 1.f - s.fx : 0.f) + (oip == L0 + r ? s.fx : 0.f);
+        tx |= (oi == L0 + r || oip == L0 + r) ? 1u << r : 0u;
     }
 #pragma unroll
-    for (int c3 = 0; c3 < 3; ++c3)
+    for (int r = 0; r < W1; ++r) {
+        wy[r] = (oj == L1 + r ? 1.f - s.fy : 0.f) + (ojp == L1 + r ? s.fy : 0.f);
+        ty |= (oj == L1 + r || ojp == L1 + r) ? 1u << r : 0u;
+    }
 #pragma unroll
-        for (int b3 = 0; b3 < 3; ++b3)
-            if (((ty >> b3) & (tz >> c3)) & 1u) mask |= tx << (3 * b3 + 9 * c3);
-    // APIC: face position minus the clamped particle position per window offset and axis
-    float dx[3], dy[3], dz[3];
+    for (int r = 0; r < W2; ++r) {
+        wz[r] = (ok == L2 + r ? 1.f - s.fz : 0.f) + (okp == L2 + r ? s.fz : 0.f);
+        tz |= (ok == L2 + r || okp == L2 + r) ? 1u << r : 0u;
+    }
+#pragma unroll
+    for (int c3 = 0; c3 < W2; ++c3)
+#pragma unroll
+        for (int b3 = 0; b3 < W1; ++b3)
+            if (((ty >> b3) & (tz >> c3)) & 1u) mask |= tx << (W0 * (b3 + W1 * c3));
+    float gx[W0];  // APIC: wx_i C_x (x_face_i - x_p)
+    float dy[W1], dz[W2];
     if (SOLVER == FE_SOLVER_APIC) {
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            dx[r] = (k.org[0] + v.hf[0] * (float)(cx + r - 1)) - q.pc[0];
-            dy[r] = (k.org[1] + v.hf[1] * (float)(cy + r - 1)) - q.pc[1];
-            dz[r] = (k.org[2] + v.hf[2] * (float)(cz + r - 1)) - q.pc[2];
-        }
+        for (int r = 0; r < W0; ++r) gx[r] = wx[r] * (q.cr[0] * ((k.org[0] + v.hf[0] * (float)(cx + L0 + r)) - q.pc[0]));
+#pragma unroll
+        for (int r = 0; r < W1; ++r) dy[r] = (k.org[1] + v.hf[1] * (float)(cy + L1 + r)) - q.pc[1];
+#pragma unroll
+        for (int r = 0; r < W2; ++r) dz[r] = (k.org[2] + v.hf[2] * (float)(cz + L2 + r)) - q.pc[2];
     }
 #pragma unroll
-    for (int c3 = 0; c3 < 3; ++c3)
+    for (int c3 = 0; c3 < W2; ++c3)
 #pragma unroll
-        for (int b3 = 0; b3 < 3; ++b3) {
+        for (int b3 = 0; b3 < W1; ++b3) {
+            const float a = wy[b3] * wz[c3];
+            float val = q.vc;
+            if (SOLVER == FE_SOLVER_APIC) val += q.cr[1] * dy[b3] + q.cr[2] * dz[c3];
+            const float t = a * val;
 #pragma unroll
-            for (int a3 = 0; a3 < 3; ++a3) {
-                const int slot = a3 + 3 * b3 + 9 * c3;
-                const float wgt = wx[a3] * wy[b3] * wz[c3];
-                float val = q.vc;
-                if (SOLVER == FE_SOLVER_APIC) val += q.cr[0] * dx[a3] + q.cr[1] * dy[b3] + q.cr[2] * dz[c3];
-                num[slot] += val * wgt;
-                den[slot] += wgt;
+            for (int a3 = 0; a3 < W0; ++a3) {
+                const int slot = a3 + W0 * (b3 + W1 * c3);
+                if (SOLVER == FE_SOLVER_APIC) num[slot] += wx[a3] * t + gx[a3] * a;
+                else num[slot] += wx[a3] * t;
+                den[slot] += wx[a3] * a;
             }
         }
     return true;
 }
 
-// Box index of slot `slot` of the cell at tile-local (lx, ly, lz): the box starts one face before the tile.
+// Box index of slot `slot` of component C for the cell at tile-local (lx, ly, lz): the box starts one face before
+// the tile.
+template <int C>
 __device__ __forceinline__ int slot_box(int lx, int ly, int lz, int slot)
 {
-    const int a = slot % 3, b = (slot / 3) % 3, c = slot / 9;
-    return (lx + a) + kBox * ((ly + b) + kBox * (lz + c));
+    constexpr int W0 = win<C>(0), W1 = win<C>(1);
+    const int a = slot % W0, b = (slot / W0) % W1, c = slot / (W0 * W1);
+    return (lx + 1 + wlo<C>(0) + a) + kBox * ((ly + 1 + wlo<C>(1) + b) + kBox * (lz + 1 + wlo<C>(2) + c));
+}
+
+// Component C of the cell's particles [pb, pe) (a thread's own cell, or a warp's share of a crowded cell with
+// lane stride 32) into the slots.
+template <int SOLVER, int C>
+__device__ __forceinline__ void cell_component(const SceneView& v, uint32_t pb, uint32_t pe, uint32_t stride, int cx,
+                                               int cy, int cz, int bx, int by, int bz, const float lo[3],
+                                               const float hi[3], float (&num)[nslots<C>()],
+                                               float (&den)[nslots<C>()], uint32_t& mask, float* s_num, float* s_den,
+                                               uint8_t* s_mk)
+{
+    const P2gComp k = p2g_comp<SOLVER>(v, C);
+#pragma unroll
+    for (int t = 0; t < nslots<C>(); ++t) num[t] = den[t] = 0.f;
+    mask = 0;
+    for (uint32_t p = pb; p < pe; p += stride) {
+        const float x = v.px[p], y = v.py[p], z = v.pz[p];
+        const Stencil s = stencil(x, y, z, k.org, v.inv_hf, k.csx, k.csy, k.csz);
+        const P2gParticle<SOLVER> q = load_particle<SOLVER>(v, p, C, x, y, z, lo, hi);
+        if (!splat_slots<SOLVER, C>(v, k, s, q, cx, cy, cz, num, den, mask))
+            splat_direct<SOLVER>(v, k, s, q, bx, by, bz, s_num, s_den, s_mk);
+    }
+}
+
+template <int SOLVER, int C>
+__device__ __forceinline__ void flush_slots(int lx, int ly, int lz, const float (&num)[nslots<C>()],
+                                            const float (&den)[nslots<C>()], uint32_t mask, float* s_num, float* s_den,
+                                            uint8_t* s_mk)
+{
+#pragma unroll
+    for (int t = 0; t < nslots<C>(); ++t) {
+        if (!((mask >> t) & 1u)) continue;
+        const int l = slot_box<C>(lx, ly, lz, t);
+        atomicAdd(&s_num[l], num[t]);
+        atomicAdd(&s_den[l], den[t]);
+        s_mk[l] = 1;
+    }
+}
+
+// A crowded cell's particles past kCellCap, spread over a warp's lanes; the lanes' slots are summed by shuffles
+// and lane 0 adds them into the box.
+template <int SOLVER, int C>
+__device__ __forceinline__ void crowded_component(const SceneView& v, uint32_t ob, uint32_t oe, int ox, int oy, int oz,
+                                                  int cx, int cy, int cz, int bx, int by, int bz, const float lo[3],
+                                                  const float hi[3], float* s_num, float* s_den, uint8_t* s_mk)
+{
+    const int lane = threadIdx.x & 31;
+    float num[nslots<C>()], den[nslots<C>()];
+    uint32_t mask;
+    cell_component<SOLVER, C>(v, ob + lane, oe, 32u, cx, cy, cz, bx, by, bz, lo, hi, num, den, mask, s_num, s_den,
+                              s_mk);
+    mask = __reduce_or_sync(0xffffffffu, mask);
+#pragma unroll
+    for (int q = 0; q < nslots<C>(); ++q)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            num[q] += __shfl_xor_sync(0xffffffffu, num[q], off);
+            den[q] += __shfl_xor_sync(0xffffffffu, den[q], off);
+        }
+    if (lane == 0) flush_slots<SOLVER, C>(ox, oy, oz, num, den, mask, s_num, s_den, s_mk);
+}
+
+template <int SOLVER, int C>
+__device__ __forceinline__ void own_component(const SceneView& v, uint32_t pb, uint32_t pe, int lx, int ly, int lz,
+                                              int cx, int cy, int cz, int bx, int by, int bz, const float lo[3],
+                                              const float hi[3], float* s_num, float* s_den, uint8_t* s_mk)
+{
+    float num[nslots<C>()], den[nslots<C>()];
+    uint32_t mask;
+    cell_component<SOLVER, C>(v, pb, pe, 1u, cx, cy, cz, bx, by, bz, lo, hi, num, den, mask, s_num, s_den, s_mk);
+    flush_slots<SOLVER, C>(lx, ly, lz, num, den, mask, s_num, s_den, s_mk);
 }
 
 template <int SOLVER>
@@ -230,34 +323,13 @@ __global__ void __launch_bounds__(kP2gThreads, 1) k_p2g(SceneView v)
         s_over[atomicAdd(&s_nover, 1)] = (uint16_t)threadIdx.x;
         pe = pb + kCellCap;
     }
-
-#pragma unroll 1
-    for (int c = 0; c < 3; ++c) {
-        const P2gComp k = p2g_comp<SOLVER>(v, c);
-        float num[27], den[27];
-#pragma unroll
-        for (int t = 0; t < 27; ++t) num[t] = den[t] = 0.f;
-        uint32_t mask = 0;
-        for (uint32_t p = pb; p < pe; ++p) {
-            const float x = v.px[p], y = v.py[p], z = v.pz[p];
-            const Stencil s = stencil(x, y, z, k.org, v.inv_hf, k.csx, k.csy, k.csz);
-            const P2gParticle<SOLVER> q = load_particle<SOLVER>(v, p, c, x, y, z, lo, hi);
-            if (!splat_slots<SOLVER>(v, k, s, q, cx, cy, cz, num, den, mask))
-                splat_direct<SOLVER>(v, k, s, q, bx, by, bz, s_num[c], s_den[c], s_mk[c]);
-        }
-#pragma unroll
-        for (int t = 0; t < 27; ++t) {
-            if (!((mask >> t) & 1u)) continue;
-            const int l = slot_box(lx, ly, lz, t);
-            atomicAdd(&s_num[c][l], num[t]);
-            atomicAdd(&s_den[c][l], den[t]);
-            s_mk[c][l] = 1;
-        }
-    }
+    own_component<SOLVER, 0>(v, pb, pe, lx, ly, lz, cx, cy, cz, bx, by, bz, lo, hi, s_num[0], s_den[0], s_mk[0]);
+    own_component<SOLVER, 1>(v, pb, pe, lx, ly, lz, cx, cy, cz, bx, by, bz, lo, hi, s_num[1], s_den[1], s_mk[1]);
+    own_component<SOLVER, 2>(v, pb, pe, lx, ly, lz, cx, cy, cz, bx, by, bz, lo, hi, s_num[2], s_den[2], s_mk[2]);
     __syncthreads();
 
-    // crowded cells: a warp per cell, lanes stride over the particles past kCellCap, slots summed by shuffles
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    // crowded cells: a warp per cell, lanes stride over the particles past kCellCap
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int nover = s_nover;
     for (int o = warp; o < nover; o += nwarps) {
         const int t = s_over[o];
@@ -265,40 +337,12 @@ __global__ void __launch_bounds__(kP2gThreads, 1) k_p2g(SceneView v)
         const int ocx = tx * FE_TILE + ox, ocy = ty * FE_TILE + oy, ocz = tz * FE_TILE + oz;
         const uint32_t key = (uint32_t)tile * FE_TILE_CELLS + (uint32_t)t;
         const uint32_t ob = v.cell_start[key] + kCellCap, oe = v.cell_start[key + 1];
-#pragma unroll 1
-        for (int c = 0; c < 3; ++c) {
-            const P2gComp k = p2g_comp<SOLVER>(v, c);
-            float num[27], den[27];
-#pragma unroll
-            for (int q = 0; q < 27; ++q) num[q] = den[q] = 0.f;
-            uint32_t mask = 0;
-            for (uint32_t p = ob + lane; p < oe; p += 32) {
-                const float x = v.px[p], y = v.py[p], z = v.pz[p];
-                const Stencil s = stencil(x, y, z, k.org, v.inv_hf, k.csx, k.csy, k.csz);
-                const P2gParticle<SOLVER> q = load_particle<SOLVER>(v, p, c, x, y, z, lo, hi);
-                if (!splat_slots<SOLVER>(v, k, s, q, ocx, ocy, ocz, num, den, mask))
-                    splat_direct<SOLVER>(v, k, s, q, bx, by, bz, s_num[c], s_den[c], s_mk[c]);
-            }
-            mask = __reduce_or_sync(0xffffffffu, mask);
-#pragma unroll
-            for (int q = 0; q < 27; ++q) {
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    num[q] += __shfl_xor_sync(0xffffffffu, num[q], off);
-                    den[q] += __shfl_xor_sync(0xffffffffu, den[q], off);
-                }
-            }
-            if (lane == 0) {
-#pragma unroll
-                for (int q = 0; q < 27; ++q) {
-                    if (!((mask >> q) & 1u)) continue;
-                    const int l = slot_box(ox, oy, oz, q);
-                    atomicAdd(&s_num[c][l], num[q]);
-                    atomicAdd(&s_den[c][l], den[q]);
-                    s_mk[c][l] = 1;
-                }
-            }
-        }
+        crowded_component<SOLVER, 0>(v, ob, oe, ox, oy, oz, ocx, ocy, ocz, bx, by, bz, lo, hi, s_num[0], s_den[0],
+                                     s_mk[0]);
+        crowded_component<SOLVER, 1>(v, ob, oe, ox, oy, oz, ocx, ocy, ocz, bx, by, bz, lo, hi, s_num[1], s_den[1],
+                                     s_mk[1]);
+        crowded_component<SOLVER, 2>(v, ob, oe, ox, oy, oz, ocx, ocy, ocz, bx, by, bz, lo, hi, s_num[2], s_den[2],
+                                     s_mk[2]);
     }
     __syncthreads();
 

@@ -171,9 +171,12 @@ struct fe_scene {
     float* staging = nullptr;          // interleaved particle staging (9 floats per particle)
     uint32_t* staging_u32 = nullptr;
     fe_step_stats* stats_ring = nullptr;
-    // graphs per particle parity, valid for graph_dt
+    // graphs per particle parity, valid for graph_dt: the three phases (profiled steps, batches) and the whole
+    // substep as one graph (plain steps)
     cudaGraphExec_t graph[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     uint64_t graph_kernels[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    cudaGraphExec_t whole[2] = {nullptr, nullptr};
+    uint64_t whole_kernels[2] = {0, 0};
     double graph_dt = -1.0;
     bool graphs_disabled = false;
     bool last_substep_empty = false;  // the last run_substep had no particles (an emitter scene before emission)
@@ -250,12 +253,17 @@ void free_list(std::vector<void*>& list, cudaStream_t st)
 
 void drop_graphs(fe_scene* s)
 {
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i) {
         for (int ph = 0; ph < 3; ++ph)
             if (s->graph[i][ph]) {
                 cudaGraphExecDestroy(s->graph[i][ph]);
                 s->graph[i][ph] = nullptr;
             }
+        if (s->whole[i]) {
+            cudaGraphExecDestroy(s->whole[i]);
+            s->whole[i] = nullptr;
+        }
+    }
     s->graph_dt = -1.0;
 }
 
@@ -781,6 +789,35 @@ fe_status check_device_error(fe_scene* s)
     return FE_OK;
 }
 
+// Captures steps [first, last] of one substep of particle parity `parity` as one graph.
+fe_status capture_one(fe_scene* s, int parity, double dt, int first, int last, cudaGraphExec_t* out, uint64_t* kernels)
+{
+    const int saved_parity = s->parity, saved_grid = s->grid_cur;
+    s->parity = parity;
+    s->grid_cur = 0;
+    cudaGraph_t g = nullptr;
+    g_capturing = true;
+    g_capture_launches = 0;
+    cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+    fe_status st = e == cudaSuccess ? enqueue_steps(s, dt, first, last) : cuda_check(e, "begin capture");
+    cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+    g_capturing = false;
+    s->parity = saved_parity;
+    s->grid_cur = saved_grid;
+    if (st != FE_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e2 != cudaSuccess) return cuda_check(e2, "end capture");
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_check(e, "graph instantiate");
+    *out = exec;
+    *kernels = g_capture_launches;
+    return FE_OK;
+}
+
 fe_status capture_graphs(fe_scene* s, int parity, double dt)
 {
     const int saved_parity = s->parity, saved_grid = s->grid_cur;
@@ -876,12 +913,26 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
         return FE_OK;
     }
     const int par = s->parity;
-    for (int ph = 0; ph < 3; ++ph) {
-        if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
-        FE_CUDA(cudaGraphLaunch(s->graph[par][ph], s->stream));
-        g_launches += s->graph_kernels[par][ph];
+    if (!ev && !s->whole[par]) {
+        // a plain step replays the whole substep as one graph (profiled steps keep the phase graphs, between
+        // which they record events)
+        fe_status st = capture_one(s, par, dt, kStepSort, kStepMove, &s->whole[par], &s->whole_kernels[par]);
+        if (st != FE_OK) {
+            cudaGetLastError();
+            s->whole[par] = nullptr;
+        }
     }
-    if (ev) FE_CUDA(cudaEventRecord(ev[3], s->stream));
+    if (!ev && s->whole[par]) {
+        FE_CUDA(cudaGraphLaunch(s->whole[par], s->stream));
+        g_launches += s->whole_kernels[par];
+    } else {
+        for (int ph = 0; ph < 3; ++ph) {
+            if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
+            FE_CUDA(cudaGraphLaunch(s->graph[par][ph], s->stream));
+            g_launches += s->graph_kernels[par][ph];
+        }
+        if (ev) FE_CUDA(cudaEventRecord(ev[3], s->stream));
+    }
     s->parity ^= 1;  // the sort inside the first graph flipped the buffer sets
     s->prev_valid = true;
     s->mesh_sdf = false;
@@ -1014,13 +1065,18 @@ fe_status apply_tuning(fe_scene* s, const fe_tuning* t)
         t->cg_block_threads != 1024)
         return set_error(FE_ERR_BAD_ARG, "cg_block_threads must be 256, 512 or 1024");
     if (t->multigrid > 1) return set_error(FE_ERR_BAD_ARG, "multigrid is 0 or 1");
+    if (t->cg_cluster > 16 || (t->cg_cluster > 0 && (t->cg_cluster & (t->cg_cluster - 1)) != 0))
+        return set_error(FE_ERR_BAD_ARG, "cg_cluster must be 1, 2, 4, 8 or 16");
     FE_CUDA(cudaSetDevice(s->device));
     FE_CUDA(cudaStreamSynchronize(s->stream));
-    if (t->cg_block_threads > 0 && t->cg_block_threads != s->cg.threads) {
+    const int want_threads = t->cg_block_threads > 0 ? t->cg_block_threads : s->cg.threads;
+    const int want_cluster = t->cg_cluster > 0 ? t->cg_cluster : std::max(s->cg.cluster, 1);
+    if (want_threads != s->cg.threads || want_cluster != std::max(s->cg.cluster, 1)) {
         CgWork w = s->cg;
-        FE_CUDA(cg_prepare(w, s->device, t->cg_block_threads));
+        FE_CUDA(cg_prepare(w, s->device, want_threads, want_cluster));
         s->cg.blocks = w.blocks;
         s->cg.threads = w.threads;
+        s->cg.cluster = w.cluster;
     }
     if (t->mg_block_level_cells > 0) {
         s->mg_block_cells = t->mg_block_level_cells;
@@ -2313,6 +2369,7 @@ fe_status fe_scene_get_tuning(fe_scene* s, fe_tuning* t)
     t->multigrid = s->use_mg && s->mg.levels >= 2 && s->colliders.count == 0 ? 1 : 0;
     t->cg_block_threads = s->cg.threads;
     t->mg_block_level_cells = s->mg_block_cells;
+    t->cg_cluster = std::max(s->cg.cluster, 1);
     return FE_OK;
 }
 
@@ -2347,10 +2404,12 @@ fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, int32_t sc
     const SceneView& b = s->base;
     const bool mg_ok = mg_plan(b.g.nx, b.g.ny, b.g.nz, b.h, lv) >= 2 && s->colliders.count == 0;
     if (scope == FE_TUNE_ALL || before.multigrid == 0)
-        for (int th : {1024, 512, 256}) cand.push_back(fe_tuning{0, th, 4096});
+        for (int th : {1024, 512, 256})
+            for (int cl : {1, 2, 4}) cand.push_back(fe_tuning{0, th, 4096, cl});
     if (mg_ok && (scope == FE_TUNE_ALL || before.multigrid == 1))
         for (int th : {1024, 512})
-            for (int cells : {4096, 2048}) cand.push_back(fe_tuning{1, th, cells});
+            for (int cells : {4096, 2048})
+                for (int cl : {1, 2}) cand.push_back(fe_tuning{1, th, cells, cl});
     fe_snapshot* snap = nullptr;
     st = fe_scene_snapshot(s, &snap);
     if (st != FE_OK) return st;
@@ -2363,10 +2422,16 @@ fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, int32_t sc
     fe_tuning pick = before;
     for (const fe_tuning& c : cand) {
         if ((st = fe_scene_restore(s, snap)) != FE_OK) break;
-        if ((st = fe_scene_set_tuning(s, &c)) != FE_OK) break;
-        if ((st = fe_scene_step(s, dt, 1, nullptr)) != FE_OK) break;  // captures this choice's graphs
+        // a choice the device cannot launch (e.g. a cluster shape it does not hold co-resident) is skipped
+        if (fe_scene_set_tuning(s, &c) != FE_OK || fe_scene_step(s, dt, 1, nullptr) != FE_OK) {
+            cudaGetLastError();
+            continue;
+        }
         cudaEventRecord(e0, s->stream);
-        if ((st = fe_scene_step(s, dt, substeps, stats.data())) != FE_OK) break;
+        if (fe_scene_step(s, dt, substeps, stats.data()) != FE_OK) {
+            cudaGetLastError();
+            continue;
+        }
         cudaEventRecord(e1, s->stream);
         cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -2635,6 +2700,9 @@ fe_status batch_set_members(fe_batch* b, fe_scene* const* scenes, int32_t count)
         MultiCgScene& t = table[i];
         t.view = s->base;
         t.work = s->cg;
+        t.work.cluster = 1;  // the multi-scene solve is not a cluster launch
+        t.mg = s->mg;
+        t.use_mg = s->use_mg && s->mg.levels >= 2 ? 1 : 0;
         t.rel_tol = s->desc.cg_rel_tol;
         t.inner_tol = s->desc.cg_inner_tol;
         t.max_it = s->desc.cg_max_it;

@@ -79,11 +79,122 @@ __device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigne
     return bar_wait(bar, err, gen);
 }
 
-__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk)
+// ---- Cluster pre-reduction (CgWork::cluster > 1: the solver was launched in thread-block clusters of that size).
+// Inside a cluster the blocks hand their partial sums to the cluster's first block (rank 0, the leader) through
+// distributed shared memory and a release add on a counter in the leader's shared memory; only the leader adds into
+// the global totals slot and arrives at the grid barrier (arrivals: one per cluster), while every block polls the
+// barrier's generation as before.  The leader's wait for its cluster is a bounded poll of its own shared memory,
+// so an error anywhere still ends every block's waits; the kernel's last step is a cluster barrier (all waits before
+// it are bounded), so no block exits while another block of its cluster may still write into its shared memory.
+// Shared-memory words of the leader: the partials at sh[kClusterSlots + 4 rank + k], the arrival counter and the
+// count of cluster gathers so far behind them.
+constexpr int kMaxCluster = 16;
+constexpr int kClusterSlots = 132;                         // after the block reduction's 132 doubles
+constexpr int kShDoubles = kClusterSlots + 4 * kMaxCluster + 2;
+
+__device__ __forceinline__ unsigned* cluster_counter(double* sh) { return reinterpret_cast<unsigned*>(sh + kClusterSlots + 4 * kMaxCluster); }
+__device__ __forceinline__ unsigned* cluster_rounds(double* sh) { return reinterpret_cast<unsigned*>(sh + kClusterSlots + 4 * kMaxCluster + 1); }
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// Generic address of `p` (this block's shared memory) in the shared memory of cluster block `rank`.
+template <class T>
+__device__ __forceinline__ T* cluster_map(T* p, unsigned rank)
+{
+    T* out;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(p), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void cluster_barrier_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Thread 0 of every block: hands this block's N partials to the leader (peers) or waits for the peers' (leader,
+// bounded) and returns the cluster's sums in part.  Returns false when the leader's wait gave up.
+template <int N>
+__device__ __forceinline__ bool cluster_gather(double* part, double* sh, int cs, int* err)
+{
+    const unsigned rank = cluster_rank();
+    if (rank != 0) {
+        double* dst = cluster_map(sh + kClusterSlots + 4 * rank, 0u);
+#pragma unroll
+        for (int k = 0; k < N; ++k) dst[k] = part[k];
+        unsigned* cnt = cluster_map(cluster_counter(sh), 0u);
+        asm volatile("red.release.cluster.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+        return true;
+    }
+    unsigned* rounds = cluster_rounds(sh);
+    const unsigned want = (*rounds + 1u) * (unsigned)(cs - 1);
+    *rounds += 1u;
+    unsigned* cnt = cluster_counter(sh);
+    unsigned long long spins = 0;
+    const unsigned long long limit = c_spin_limit;
+    cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
+    while (true) {
+        unsigned got;
+        asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(got) : "l"(cnt) : "memory");
+        if ((int)(got - want) >= 0) break;
+        if (++spins > limit) {
+            e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
+            return false;
+        }
+        if ((spins & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0) return false;
+    }
+    for (int r = 1; r < cs; ++r)
+#pragma unroll
+        for (int k = 0; k < N; ++k) part[k] += sh[kClusterSlots + 4 * r + k];
+    return true;
+}
+
+// Start of a clustered solver kernel: the leader's counters are zeroed before any block of the cluster can add.
+__device__ __forceinline__ void cluster_begin(const CgWork& w, double* sh)
+{
+    if (w.cluster <= 1) return;
+    if (threadIdx.x == 0) {
+        *cluster_counter(sh) = 0u;
+        *cluster_rounds(sh) = 0u;
+    }
+    cluster_barrier_all();
+}
+
+// End of a clustered solver kernel (every block reaches it: all waits before it are bounded).
+__device__ __forceinline__ void cluster_end(const CgWork& w)
+{
+    if (w.cluster > 1) cluster_barrier_all();
+}
+
+// Arrival of this block at grid barrier `gen` with N partial sums already reduced into `part` (thread 0): plain, or
+// through its cluster's leader.  Returns false when a wait gave up.
+template <int N>
+__device__ __forceinline__ bool arrive_and_wait(double* part, double* sh, const CgWork& w, unsigned gen, int nblk)
+{
+    double* totals = w.partial;  // [3][4]
+    double* slot = totals + 4 * (gen % 3u);  // zeroed by the release of this generation
+    if (w.cluster > 1) {
+        if (!cluster_gather<N>(part, sh, w.cluster, w.err)) return false;
+        if (cluster_rank() != 0) return bar_wait(w.bar, w.err, gen);
+#pragma unroll
+        for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
+        return bar_arrive_wait(w.bar, w.err, (unsigned)(nblk / w.cluster), totals, gen);
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
+    return bar_arrive_wait(w.bar, w.err, (unsigned)nblk, totals, gen);
+}
+
+__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk, double* sh)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        bar_arrive_wait(w.bar, w.err, (unsigned)nblk, w.partial, gen);
+        double none[1] = {0.0};
+        arrive_and_wait<0>(none, sh, w, gen, nblk);
         gen = next_gen(gen);
     }
     __syncthreads();
@@ -99,7 +210,7 @@ __device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nb
 // by the last arriver avoid the floating-point atomics but put one more L2 round trip on the critical
 // path, which measured slower.)
 template <int N>
-__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] */, const CgWork& w, unsigned& gen,
+__device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [kShDoubles] */, const CgWork& w, unsigned& gen,
                                             int nblk)
 {
     static_assert(N <= 4, "at most 4 sums per reduction");
@@ -127,11 +238,8 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [132] 
         if (lane == 0) {
             // slot of this barrier: generation modulo 3; thread 0 tracks the generation itself (it takes
             // part in every barrier), which saves a load round trip per barrier
-            double* totals = w.partial;  // [3][4]
-            double* slot = totals + 4 * (gen % 3u);  // zeroed by the release of this generation
-#pragma unroll
-            for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
-            const bool ok = bar_arrive_wait(w.bar, w.err, (unsigned)nblk, totals, gen);
+            const double* slot = w.partial + 4 * (gen % 3u);
+            const bool ok = arrive_and_wait<N>(part, sh, w, gen, nblk);
             gen = next_gen(gen);
             if (ok)
 #pragma unroll
@@ -185,7 +293,7 @@ __device__ __forceinline__ float apply_row(const Stencil7& st, int c, uint32_t m
 // Shared memory of one solver block, declared once per kernel and handed to whichever solver body runs.
 constexpr int kCoarseMaxCells = 512;  // the multigrid solver's coarsest level lives in shared memory
 struct SolverSmem {
-    double sh[32 * 4 + 4];                 // block reductions
+    double sh[kShDoubles];                 // block reductions, then the cluster pre-reduction's words
     uint32_t s_warp[32];                   // compaction counts
     uint32_t s_list[kListCache];           // cached FLUID-list entries
     float cz[2][kCoarseMaxCells];          // multigrid: coarsest-level correction (ping-pong)
@@ -303,7 +411,7 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
         base += total;
         __syncthreads();
     }
-    if (!grid_sync(w, gen, nblk)) return false;
+    if (!grid_sync(w, gen, nblk, sh)) return false;
     const int kc = kListCache / (int)blockDim.x;
     {
         int k = 0;

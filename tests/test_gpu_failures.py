@@ -29,10 +29,11 @@ def restore_limits():
     _abi.set_barrier_limits(0, 0)
 
 
-@pytest.mark.parametrize("psolver", [fe.CG, fe.MGPCG])
-def test_barrier_wait_runs_out_and_the_scene_recovers(psolver, restore_limits):
+@pytest.mark.parametrize("psolver,cluster", [(fe.CG, 1), (fe.MGPCG, 1), (fe.CG, 2)])
+def test_barrier_wait_runs_out_and_the_scene_recovers(psolver, cluster, restore_limits):
     n = (32, 32, 32)
     s = dam(n, pressure_solver=psolver)
+    s.set_tuning(cg_cluster=cluster)
     st = s.step(1 / 240, 2)  # graphs captured, solver warm
     assert all(x["converged"] == 1 for x in st)
     _abi.set_barrier_limits(spin_limit=1 << 12, extra_arrivals=1)

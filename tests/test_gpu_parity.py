@@ -277,11 +277,14 @@ def test_multigrid_iterations_bounded():
     assert stats[fe.MGPCG] < 40 < 200 < stats[fe.CG], stats
 
 
-@pytest.mark.parametrize("tuning", [dict(multigrid=0, cg_block_threads=1024),
-                                    dict(multigrid=0, cg_block_threads=512),
-                                    dict(multigrid=0, cg_block_threads=256),
-                                    dict(multigrid=1, cg_block_threads=1024, mg_block_level_cells=4096),
-                                    dict(multigrid=1, cg_block_threads=512, mg_block_level_cells=2048)])
+@pytest.mark.parametrize("tuning", [dict(multigrid=0, cg_block_threads=1024, cg_cluster=1),
+                                    dict(multigrid=0, cg_block_threads=512, cg_cluster=1),
+                                    dict(multigrid=0, cg_block_threads=256, cg_cluster=1),
+                                    dict(multigrid=0, cg_block_threads=1024, cg_cluster=2),
+                                    dict(multigrid=0, cg_block_threads=512, cg_cluster=4),
+                                    dict(multigrid=1, cg_block_threads=1024, mg_block_level_cells=4096, cg_cluster=1),
+                                    dict(multigrid=1, cg_block_threads=512, mg_block_level_cells=2048, cg_cluster=1),
+                                    dict(multigrid=1, cg_block_threads=1024, mg_block_level_cells=4096, cg_cluster=2)])
 def test_tuning_choices_reach_the_oracle(tuning):
     """Every launch choice the autotuner can make (fe_scene_set_tuning) solves to the same FP64 residual and the
     oracle's pressure; only the speed differs."""
