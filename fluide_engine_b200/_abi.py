@@ -59,7 +59,8 @@ class SceneDesc(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("multigrid", ctypes.c_int32), ("cg_block_threads", ctypes.c_int32),
-                ("mg_block_level_cells", ctypes.c_int32), ("cg_cluster", ctypes.c_int32)]
+                ("mg_block_level_cells", ctypes.c_int32), ("cg_cluster", ctypes.c_int32),
+                ("pressure_extrapolation", ctypes.c_int32)]
 
 
 class StepStats(ctypes.Structure):

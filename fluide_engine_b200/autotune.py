@@ -13,7 +13,7 @@ import os
 
 from . import _abi
 
-FIELDS = ("multigrid", "cg_block_threads", "mg_block_level_cells", "cg_cluster")
+FIELDS = ("multigrid", "cg_block_threads", "mg_block_level_cells", "cg_cluster", "pressure_extrapolation")
 SOLVER_NAMES = {_abi.PIC: "PIC", _abi.FLIP: "FLIP", _abi.APIC: "APIC"}
 
 

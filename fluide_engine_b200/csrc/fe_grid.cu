@@ -40,21 +40,22 @@ __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid
     // select by value (a runtime index into the parameter arrays would spill them to local memory)
     const float* in = c == 0 ? fa.in[0] : (c == 1 ? fa.in[1] : fa.in[2]);
     const uint8_t* vin = c == 0 ? fa.vin[0] : (c == 1 ? fa.vin[1] : fa.vin[2]);
+    // the face and its six neighbours (order i+1, i-1, j+1, j-1, k+1, k-1): every validity byte and value is
+    // loaded before any is used -- the neighbours whether or not the face turns out to need them -- so all are in
+    // flight together in one round trip instead of the face's own load followed by its neighbours'
+    const size_t sxy = (size_t)sx * sy;
+    const bool in_dom[6] = {i + 1 < sx, i > 0, j + 1 < sy, j > 0, k + 1 < sz, k > 0};
+    const long long off[6] = {1, -1, (long long)sx, -(long long)sx, (long long)sxy, -(long long)sxy};
     float val = in[f];
     uint8_t valid = vin[f];
-    if (!valid) {
-        const size_t sxy = (size_t)sx * sy;
-        // the six neighbours (order i+1, i-1, j+1, j-1, k+1, k-1): every validity byte and value is loaded
-        // before any is used, so they are in flight together instead of validity-then-value round trips
-        const bool in_dom[6] = {i + 1 < sx, i > 0, j + 1 < sy, j > 0, k + 1 < sz, k > 0};
-        const long long off[6] = {1, -1, (long long)sx, -(long long)sx, (long long)sxy, -(long long)sxy};
-        uint8_t nvalid[6];
-        float nval[6];
+    uint8_t nvalid[6];
+    float nval[6];
 #pragma unroll
-        for (int n = 0; n < 6; ++n) {
-            nvalid[n] = in_dom[n] ? vin[(long long)f + off[n]] : (uint8_t)0;
-            nval[n] = in_dom[n] ? in[(long long)f + off[n]] : 0.f;
-        }
+    for (int n = 0; n < 6; ++n) {
+        nvalid[n] = in_dom[n] ? vin[(long long)f + off[n]] : (uint8_t)0;
+        nval[n] = in_dom[n] ? in[(long long)f + off[n]] : 0.f;
+    }
+    if (!valid) {
         float sum = 0.f;
         unsigned count = 0;
 #pragma unroll
@@ -87,13 +88,21 @@ __global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __r
     if (i >= nx || j >= ny) return;
     const size_t c = idx3(i, j, k, nx, ny);
     double b = 0.0;
-    if (v.marks[c] == FE_CELL_FLUID) {
+    const bool fluid = v.marks[c] == FE_CELL_FLUID;
+    if (fluid) {
         const double left = u[idx3(i, j, k, nx + 1, ny)], right = u[idx3(i + 1, j, k, nx + 1, ny)];
         const double down = vv[idx3(i, j, k, nx, ny + 1)], up = vv[idx3(i, j + 1, k, nx, ny + 1)];
         const double back = w[idx3(i, j, k, nx, ny)], front = w[idx3(i, j, k + 1, nx, ny)];
         b = (right - left) / v.h[0] + (up - down) / v.h[1] + (front - back) / v.h[2];
     }
     v.b[c] = b;
+    if (v.pprev) {
+        // warm start extrapolated in time, 2 p(n-1) - p(n-2), where the cell held pressure in both substeps; the
+        // solve still runs to the same residual target, so only its iteration count changes
+        const double pn1 = v.p[c], pn2 = v.pprev[c];
+        if (fluid && pn1 != 0.0 && pn2 != 0.0) v.p[c] = 2.0 * pn1 - pn2;
+        v.pprev[c] = pn1;
+    }
 }
 
 __global__ void k_apply(SceneView v, float* u, float* vv, float* w)

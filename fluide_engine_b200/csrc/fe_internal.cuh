@@ -66,6 +66,7 @@ struct SceneView {
     uint8_t *mu2, *mv2, *mw2; // extrapolation validity ping-pong
     uint8_t* marks;
     double *p, *b;
+    double* pprev;         // the pressure of the substep before the last (time-extrapolated warm start), or null
     // marking tables (per axis, FP64)
     double* q_pos[3];      // sdf node coordinate of each index
     int* q_b0[3];          // hash bucket of the node

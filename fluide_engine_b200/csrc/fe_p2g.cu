@@ -135,6 +135,11 @@ __device__ void splat_direct(const SceneView& v, const P2gComp& k, const Stencil
 template <int C> __host__ __device__ constexpr int win(int axis) { return axis == C ? 2 : 3; }
 template <int C> __host__ __device__ constexpr int wlo(int axis) { return axis == C ? 0 : -1; }
 template <int C> __host__ __device__ constexpr int nslots() { return win<C>(0) * win<C>(1) * win<C>(2); }  // 18
+// `count` ones spaced `width` bits apart (bit 0, width, 2 width, ...).
+__host__ __device__ constexpr uint32_t rep_bits(int width, int count)
+{
+    return count <= 0 ? 0u : (rep_bits(width, count - 1) << width) | 1u;
+}
 
 // One particle of cell (cx, cy, cz) into the cell's 18 slots of component C; returns false (and adds nothing)
 // when its stencil leaves the window, in which case the caller takes the direct path.  The trilinear weight of
@@ -167,11 +172,16 @@ __device__ __forceinline__ bool splat_slots(const SceneView& v, const P2gComp& k
         wz[r] = (ok == L2 + r ? 1.f - s.fz : 0.f) + (okp == L2 + r ? s.fz : 0.f);
         tz |= (ok == L2 + r || okp == L2 + r) ? 1u << r : 0u;
     }
+    // touched slots: tx[a] & ty[b] & tz[c] over the window, by spreading each axis' bits over the slot layout
+    {
+        const uint32_t ex = tx * rep_bits(W0, W1 * W2);
+        uint32_t sy = 0, ez = 0;
 #pragma unroll
-    for (int c3 = 0; c3 < W2; ++c3)
+        for (int b3 = 0; b3 < W1; ++b3) sy |= ((ty >> b3) & 1u) * (((1u << W0) - 1u) << (W0 * b3));
 #pragma unroll
-        for (int b3 = 0; b3 < W1; ++b3)
-            if (((ty >> b3) & (tz >> c3)) & 1u) mask |= tx << (W0 * (b3 + W1 * c3));
+        for (int c3 = 0; c3 < W2; ++c3) ez |= ((tz >> c3) & 1u) * (((1u << (W0 * W1)) - 1u) << (W0 * W1 * c3));
+        mask |= ex & (sy * rep_bits(W0 * W1, W2)) & ez;
+    }
     float gx[W0];  // APIC: wx_i C_x (x_face_i - x_p)
     float dy[W1], dz[W2];
     if (SOLVER == FE_SOLVER_APIC) {

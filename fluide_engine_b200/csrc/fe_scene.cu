@@ -114,6 +114,7 @@ struct fe_scene {
     CgWork cg{};
     MgWork mg{};                       // multigrid levels (levels >= 2) once the multigrid solver was wanted
     bool use_mg = false;               // solve with the multigrid-preconditioned CG (if the grid has a hierarchy)
+    double* pprev_buf = nullptr;       // pressure of the substep before the last (time-extrapolated warm start)
     int mg_block_cells = 4096;         // multigrid levels of at most this many cells run in one block
     DiffWork diff{};                   // viscosity buffers (allocated once the viscosity is > 0)
     bool diff_ready = false;
@@ -1082,6 +1083,14 @@ fe_status apply_tuning(fe_scene* s, const fe_tuning* t)
         s->mg_block_cells = t->mg_block_level_cells;
         if (s->mg.levels >= 2) s->mg.block_from = mg_block_from(s->mg.lv, s->mg.levels, s->mg_block_cells);
     }
+    if (t->pressure_extrapolation > 1) return set_error(FE_ERR_BAD_ARG, "pressure_extrapolation is 0 or 1");
+    if (t->pressure_extrapolation == 1 && !s->pprev_buf) {
+        const size_t nc = (size_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+        FE_CUDA(dalloc(s->allocs, &s->pprev_buf, nc, s->device, s->own_stream));
+        FE_CUDA(cudaMemsetAsync(s->pprev_buf, 0, nc * sizeof(double), s->own_stream));
+        FE_CUDA(cudaStreamSynchronize(s->own_stream));
+    }
+    if (t->pressure_extrapolation >= 0) s->base.pprev = t->pressure_extrapolation == 1 ? s->pprev_buf : nullptr;
     if (t->multigrid >= 0) {
         if (t->multigrid == 1) {
             fe_status st = ensure_mg(s);
@@ -1293,6 +1302,7 @@ fe_status fe_scene_reset(fe_scene* s)
     FE_CUDA(cudaMemsetAsync(v.marks, 0, nc, st));
     FE_CUDA(cudaMemsetAsync(v.p, 0, nc * sizeof(double), st));
     FE_CUDA(cudaMemsetAsync(v.b, 0, nc * sizeof(double), st));
+    if (s->pprev_buf) FE_CUDA(cudaMemsetAsync(s->pprev_buf, 0, nc * sizeof(double), st));
     FE_CUDA(cudaMemsetAsync(v.cell_start, 0, ((size_t)v.g.key_space + 1) * sizeof(uint32_t), st));
     FE_CUDA(cudaMemsetAsync(s->cg.r0, 0, nc * 9 * sizeof(float), st));
     FE_CUDA(cudaMemsetAsync(s->cg.partial, 0, cg_partial_doubles(kMaxCgBlocks) * sizeof(double), st));
@@ -2220,6 +2230,7 @@ struct fe_snapshot {
     float* part = nullptr;    // channels x np floats (pos 3, vel 3, C 9 for APIC), then pid (np u32)
     float* prev = nullptr;    // 3 x np: positions at the start of the last substep (when prev_valid)
     double* p = nullptr;      // nc
+    double* pprev = nullptr;  // nc: the pressure before that (time-extrapolated warm start), when in use
     float* grid = nullptr;    // nf: the current velocity buffer
     int channels = 0;
     bool prev_valid = false, collider_built = false, last_substep_empty = false, have_particles = false;
@@ -2259,6 +2270,11 @@ fe_status fe_scene_snapshot(fe_scene* s, fe_snapshot** out)
     FE_CUDA(cudaMemcpyAsync(sn->p, b.p, nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
     FE_CUDA(cudaMemcpyAsync(sn->grid, s->grid_cur ? b.u2 : b.u, nf * sizeof(float), cudaMemcpyDeviceToDevice, st));
     sn->bytes = nc * sizeof(double) + nf * sizeof(float);
+    if (s->pprev_buf) {
+        FE_CUDA(dalloc(sn->allocs, &sn->pprev, nc, dev, st));
+        FE_CUDA(cudaMemcpyAsync(sn->pprev, s->pprev_buf, nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        sn->bytes += nc * sizeof(double);
+    }
     if (np) {
         const SceneView v = view_of(s, s->parity);
         FE_CUDA(dalloc(sn->allocs, &sn->part, np * (sn->channels + 1), dev, st));
@@ -2312,6 +2328,12 @@ fe_status fe_scene_restore(fe_scene* s, const fe_snapshot* sn)
     s->grid_cur = 0;
     FE_CUDA(cudaMemcpyAsync(b.p, sn->p, nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
     FE_CUDA(cudaMemcpyAsync(b.u, sn->grid, nf * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (s->pprev_buf) {
+        if (sn->pprev)
+            FE_CUDA(cudaMemcpyAsync(s->pprev_buf, sn->pprev, nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        else
+            FE_CUDA(cudaMemsetAsync(s->pprev_buf, 0, nc * sizeof(double), st));
+    }
     if (np) {
         const SceneView v = view_of(s, 0);
         float* ch[15] = {v.px, v.py, v.pz, v.vx, v.vy, v.vz};
@@ -2370,6 +2392,7 @@ fe_status fe_scene_get_tuning(fe_scene* s, fe_tuning* t)
     t->cg_block_threads = s->cg.threads;
     t->mg_block_level_cells = s->mg_block_cells;
     t->cg_cluster = std::max(s->cg.cluster, 1);
+    t->pressure_extrapolation = s->base.pprev ? 1 : 0;
     return FE_OK;
 }
 
@@ -2405,11 +2428,10 @@ fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, int32_t sc
     const bool mg_ok = mg_plan(b.g.nx, b.g.ny, b.g.nz, b.h, lv) >= 2 && s->colliders.count == 0;
     if (scope == FE_TUNE_ALL || before.multigrid == 0)
         for (int th : {1024, 512, 256})
-            for (int cl : {1, 2, 4}) cand.push_back(fe_tuning{0, th, 4096, cl});
+            for (int cl : {1, 2}) cand.push_back(fe_tuning{0, th, 4096, cl, -1});
     if (mg_ok && (scope == FE_TUNE_ALL || before.multigrid == 1))
         for (int th : {1024, 512})
-            for (int cells : {4096, 2048})
-                for (int cl : {1, 2}) cand.push_back(fe_tuning{1, th, cells, cl});
+            for (int cells : {4096, 2048}) cand.push_back(fe_tuning{1, th, cells, 1, -1});
     fe_snapshot* snap = nullptr;
     st = fe_scene_snapshot(s, &snap);
     if (st != FE_OK) return st;

@@ -112,16 +112,19 @@ class Scene:
     def restore(self, snap):
         check(self._L.fe_scene_restore(self._h, snap.handle))
 
-    def set_tuning(self, multigrid=-1, cg_block_threads=0, mg_block_level_cells=0, cg_cluster=0):
+    def set_tuning(self, multigrid=-1, cg_block_threads=0, mg_block_level_cells=0, cg_cluster=0,
+                   pressure_extrapolation=-1):
         """Launch choices of the pressure solve (fe_scene_set_tuning); -1 / 0 keeps a field's current choice."""
-        t = _abi.Tuning(int(multigrid), int(cg_block_threads), int(mg_block_level_cells), int(cg_cluster))
+        t = _abi.Tuning(int(multigrid), int(cg_block_threads), int(mg_block_level_cells), int(cg_cluster),
+                        int(pressure_extrapolation))
         check(self._L.fe_scene_set_tuning(self._h, ctypes.byref(t)))
 
     def tuning(self):
         t = _abi.Tuning()
         check(self._L.fe_scene_get_tuning(self._h, ctypes.byref(t)))
         return {"multigrid": t.multigrid, "cg_block_threads": t.cg_block_threads,
-                "mg_block_level_cells": t.mg_block_level_cells, "cg_cluster": t.cg_cluster}
+                "mg_block_level_cells": t.mg_block_level_cells, "cg_cluster": t.cg_cluster,
+                "pressure_extrapolation": t.pressure_extrapolation}
 
     def set_stream(self, stream_handle):
         """Issues the scene's work on an external cudaStream_t (an int handle, e.g. torch stream.cuda_stream)."""

@@ -321,6 +321,9 @@ typedef struct fe_tuning {
     int32_t cg_cluster;           /* thread-block cluster size of the persistent solve (1, 2, 4, 8, 16): the blocks of a
                                      cluster pre-reduce their sums in distributed shared memory and one block per
                                      cluster arrives at the grid barrier */
+    int32_t pressure_extrapolation; /* 1: warm-start each solve from 2 p(n-1) - p(n-2) where a cell held pressure in
+                                     both earlier substeps, instead of the reference's p(n-1) (linear_system.cpp:13-18);
+                                     the solve still stops at the same relative residual */
 } fe_tuning;
 /* Applies `t` (the scene's captured substeps are captured again on the next step); multigrid = 1 allocates the
  * hierarchy on first use. */
@@ -332,9 +335,9 @@ fe_status fe_scene_get_tuning(fe_scene* s, fe_tuning* t);
  * a given family does not depend on that. */
 enum { FE_TUNE_ALL = 0, FE_TUNE_SHAPE = 1 };
 /* The autotuner: times every candidate launch choice of the scene's pressure solve -- the plain CG at 256 / 512 /
- * 1024 threads per block in clusters of 1, 2 or 4 blocks, and (grids with a multigrid hierarchy, no colliders) the
- * multigrid-preconditioned CG at 512 / 1024 threads with one-block levels up to 2048 or 4096 cells in clusters of 1
- * or 2; with FE_TUNE_SHAPE only the current family's --
+ * 1024 threads per block, alone or in clusters of 2 blocks, and (grids with a multigrid hierarchy, no colliders)
+ * the multigrid-preconditioned CG at 512 / 1024 threads with one-block levels up to 2048 or 4096 cells; with
+ * FE_TUNE_SHAPE only the current family's --
  * over `substeps` substeps of dt each from the scene's current state (CUDA events on the scene's stream,
  * after one untimed substep that captures the choice's graphs), keeps the fastest whose solves all converged,
  * restores the scene's state and applies the choice.  The choice is also stored for (device, grid, transfer):

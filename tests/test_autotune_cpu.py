@@ -9,7 +9,7 @@ from fluide_engine_b200 import _abi, autotune
 
 
 def test_store_and_lookup_per_device_grid_and_transfer():
-    t = dict(multigrid=1, cg_block_threads=512, mg_block_level_cells=2048, cg_cluster=2)
+    t = dict(multigrid=1, cg_block_threads=512, mg_block_level_cells=2048, cg_cluster=2, pressure_extrapolation=0)
     autotune.store((96, 64, 48), _abi.APIC, t, device=3)
     assert autotune.lookup((96, 64, 48), _abi.APIC, device=3) == t
     assert autotune.lookup((96, 64, 48), _abi.FLIP, device=3) is None      # another transfer
@@ -23,9 +23,11 @@ def test_store_and_lookup_per_device_grid_and_transfer():
 def test_file_round_trip_and_load(tmp_path):
     path = str(tmp_path / "sub" / "tuning_B200.json")
     entries = {((128, 128, 128), _abi.FLIP): dict(multigrid=0, cg_block_threads=1024,
-                                                  mg_block_level_cells=4096, cg_cluster=1),
+                                                  mg_block_level_cells=4096, cg_cluster=1,
+                                                  pressure_extrapolation=1),
                ((256, 256, 256), _abi.APIC): dict(multigrid=1, cg_block_threads=512,
-                                                  mg_block_level_cells=2048, cg_cluster=1)}
+                                                  mg_block_level_cells=2048, cg_cluster=1,
+                                                  pressure_extrapolation=0)}
     autotune.write_file(path, entries, "NVIDIA B200")
     with open(path) as f:
         data = json.load(f)

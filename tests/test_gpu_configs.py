@@ -89,3 +89,23 @@ def test_apic_pool_sphere_48_tracks_oracle(psolver):
     solver."""
     first, again = run_scene((48, 48, 48), fe.APIC, POOL, 1, 1.0 / 480.0, 1e-8, 80, pressure_solver=psolver)
     assert first["C"] < 1e-4 and again["C"] < 1e-4
+
+
+def test_time_extrapolated_warm_start_reaches_the_oracle():
+    """With the solve warm-started from 2 p(n-1) - p(n-2) (a tuning choice; the reference starts from p(n-1)) every
+    solve still meets its residual target, and a substep from an identical snapshot matches the oracle, which keeps
+    the reference's warm start, within the same tolerances."""
+    n = (40, 40, 40)
+    pos, vel = fe.seed_regions(DAM, n, seed=5)
+    g = fe.Scene(n, solver=fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-6)
+    g.set_tuning(pressure_extrapolation=1)
+    assert g.tuning()["pressure_extrapolation"] == 1
+    g.set_particles(pos, vel)
+    st = g.step(1.0 / 240.0, 12)
+    assert all(x["converged"] == 1 and x["rel_residual"] <= 1e-6 for x in st), st
+    P, V, _ = g.particles()
+    o = oracle.OracleSim(n, fe.FLIP, max_cfl=1.0, cg_rel_tol=1e-10, cg_max_it=20000)
+    o.set_particles(P.astype(np.float64), V.astype(np.float64))
+    o.set_pressure(g.grid()[3])
+    compare_substep(g, o, 1.0 / 240.0, fe.FLIP, 1e-6)
+    g.close()
