@@ -39,7 +39,7 @@ EXPORTS = [
     "fe_batch_step", "fe_batch_step_profiled", "fe_kernel_launch_count", "fe_seed_regions", "fe_last_error",
     "fe_abi_version", "fe_debug_set_barrier_limits", "fe_scene_set_tuning", "fe_scene_get_tuning",
     "fe_scene_snapshot", "fe_scene_restore", "fe_snapshot_info", "fe_snapshot_destroy",
-    "fe_scene_autotune", "fe_tuning_store", "fe_tuning_lookup",
+    "fe_scene_autotune", "fe_tuning_store", "fe_tuning_lookup", "fe_batch_set_overlap",
 ]
 
 
@@ -157,6 +157,7 @@ def lib():
     L.fe_batch_create.argtypes = [ctypes.POINTER(P), ctypes.c_int32, ctypes.POINTER(P)]
     L.fe_batch_set_scenes.argtypes = [P, ctypes.POINTER(P), ctypes.c_int32]
     L.fe_batch_destroy.argtypes = [P]
+    L.fe_batch_set_overlap.argtypes = [P, ctypes.c_int32]
     L.fe_batch_step.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats)]
     L.fe_batch_step_profiled.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats),
                                          ctypes.POINTER(ctypes.c_float)]

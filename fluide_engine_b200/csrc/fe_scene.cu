@@ -2547,6 +2547,12 @@ struct fe_batch {
     uint64_t graph_epoch = 0;  // sum of the scenes' epochs when the graphs were captured
     int parity = 0;
     int64_t steps_done = 0;   // substeps since creation: a young batch replays per-scene graphs
+    // overlap mode: every scene runs its whole substep (pre-solve, its own cooperative solve on `share` blocks,
+    // post-solve) on its own stream, so one scene's latency-bound solve overlaps other scenes' transfer kernels;
+    // the shares add up to the multi-scene solve's co-resident capacity, so all solves in flight fit at once
+    bool overlap = false;
+    bool shares_measured = false;      // shares re-split from measured solve work since the membership was set
+    std::vector<int> share;
 };
 
 // A batch replays its scenes' own phase graphs around the multi-scene solve for its first
@@ -2661,6 +2667,34 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = null
     return FE_OK;
 }
 
+fe_status batch_enqueue_overlap(fe_batch* b, double dt, bool scene_graphs);
+
+// Overlap mode's young-batch substep: the scenes' own phase graphs around each scene's own solve.
+fe_status batch_step_overlap_scene_graphs(fe_batch* b, double dt)
+{
+    for (fe_scene* s : b->scenes) {
+        if (s->graph_dt != dt) {
+            drop_graphs(s);
+            s->graph_dt = dt;
+        }
+        if (!s->graph[s->parity][0]) {
+            fe_status st = capture_graphs(s, s->parity, dt);
+            if (st != FE_OK) return st;
+        }
+    }
+    fe_status st = batch_enqueue_overlap(b, dt, true);
+    if (st != FE_OK) return st;
+    for (fe_scene* s : b->scenes) {
+        s->parity ^= 1;  // the pre-solve graph's sort flipped the particle buffer sets
+        s->prev_valid = true;
+        s->mesh_sdf = false;
+        s->collider_built = true;
+        s->grid_cur = 0;
+    }
+    b->parity ^= 1;
+    return FE_OK;
+}
+
 fe_status batch_check_scenes(fe_scene* const* scenes, int32_t count)
 {
     if (!scenes || count < 1) return set_error(FE_ERR_BAD_ARG, "need at least one scene");
@@ -2747,6 +2781,80 @@ fe_status batch_set_members(fe_batch* b, fe_scene* const* scenes, int32_t count)
     b->scenes.assign(scenes, scenes + count);
     b->total_blocks = start;
     b->steps_done = 0;
+    b->share = nblk;
+    b->shares_measured = false;
+    return FE_OK;
+}
+
+// Overlap mode: re-splits the solver blocks among the scenes in proportion to their measured solve work (read back
+// from the solver table once the batch has run a few substeps), as k_multi_partition does on the device.
+fe_status batch_resplit(fe_batch* b)
+{
+    const int S = (int)b->scenes.size();
+    std::vector<MultiCgScene> table(S);
+    FE_CUDA(cudaStreamSynchronize(b->stream));
+    FE_CUDA(cudaMemcpy(table.data(), b->table, S * sizeof(MultiCgScene), cudaMemcpyDeviceToHost));
+    std::vector<double> work(S);
+    double total = 0.0;
+    for (int i = 0; i < S; ++i) {
+        const MultiCgScene& m = table[i];
+        const double per_it = m.use_mg ? 12.0 : 1.0;
+        work[i] = m.last_its >= 0 ? (double)m.last_fluid * ((double)m.last_its * per_it + 3.0) : m.weight0;
+        work[i] = std::max(work[i], 0.0);
+        total += work[i];
+    }
+    std::vector<int> nblk(S, 1);
+    int used = S;
+    for (int i = 0; i < S; ++i) {
+        const int extra = total > 0.0 ? (int)std::floor((b->total_blocks - S) * work[i] / total) : 0;
+        nblk[i] += extra;
+        used += extra;
+    }
+    for (; used < b->total_blocks; ++used) {  // leftovers where the work per block is largest
+        int best = 0;
+        for (int i = 1; i < S; ++i)
+            if (work[i] / nblk[i] > work[best] / nblk[best]) best = i;
+        nblk[best] += 1;
+    }
+    b->share = nblk;
+    b->shares_measured = true;
+    return FE_OK;
+}
+
+bool batch_has_viscosity(const fe_batch* b)
+{
+    return std::any_of(b->scenes.begin(), b->scenes.end(), [](const fe_scene* s) { return s->desc.viscosity > 0.0; });
+}
+
+// Overlap mode, one batch substep: each scene's pre-solve steps, its own solve and its post-solve steps on its own
+// stream, forked from and joined to the batch stream; scene_graphs replays the scenes' own phase graphs (young
+// batches), otherwise the steps are enqueued directly (for the batch graph's capture).
+fe_status batch_enqueue_overlap(fe_batch* b, double dt, bool scene_graphs)
+{
+    const int S = (int)b->scenes.size();
+    cudaEvent_t fork0 = b->events[2 * S];
+    FE_CUDA(cudaEventRecord(fork0, b->stream));
+    for (int i = 0; i < S; ++i) {
+        fe_scene* s = b->scenes[i];
+        FE_CUDA(cudaStreamWaitEvent(s->stream, fork0, 0));
+        if (scene_graphs) {
+            FE_CUDA(cudaGraphLaunch(s->graph[s->parity][0], s->stream));
+            g_launches += s->graph_kernels[s->parity][0];
+        } else {
+            fe_status st = enqueue_steps(s, dt, kStepSort, kStepRhs, s->stream);
+            if (st != FE_OK) return st;
+        }
+        FE_CUDA(launch_multi_cg(b->table + i, 1, b->share[i], s->stream));
+        if (scene_graphs) {
+            FE_CUDA(cudaGraphLaunch(s->graph[s->parity][2], s->stream));
+            g_launches += s->graph_kernels[s->parity][2];
+        } else {
+            fe_status st = enqueue_steps(s, dt, kStepApply, kStepMove);
+            if (st != FE_OK) return st;
+        }
+        FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
+        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
+    }
     return FE_OK;
 }
 
@@ -2762,7 +2870,9 @@ fe_status batch_capture(fe_batch* b, int parity, double dt)
     g_capturing = true;
     g_capture_launches = 0;
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-    fe_status st = e == cudaSuccess ? batch_enqueue(b, dt) : cuda_check(e, "begin capture");
+    const bool overlap = b->overlap && !batch_has_viscosity(b);
+    fe_status st = e == cudaSuccess ? (overlap ? batch_enqueue_overlap(b, dt, false) : batch_enqueue(b, dt))
+                                    : cuda_check(e, "begin capture");
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     g_capturing = false;
     for (int i = 0; i < S; ++i) {
@@ -2815,6 +2925,18 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
     if (st != FE_OK) return fail(st);
     // no host synchronisation: a scene's earlier work precedes the batch's work in its own stream order
     *out = b;
+    return FE_OK;
+}
+
+fe_status fe_batch_set_overlap(fe_batch* b, int32_t on)
+{
+    if (!b) return set_error(FE_ERR_BAD_ARG, "null batch");
+    FE_CUDA(cudaSetDevice(b->device));
+    FE_CUDA(cudaStreamSynchronize(b->stream));
+    if (b->overlap != (on != 0)) {
+        b->overlap = on != 0;
+        batch_drop_graphs(b);
+    }
     return FE_OK;
 }
 
@@ -2891,13 +3013,19 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
     FE_CUDA(cudaSetDevice(b->device));
     if (stats)
         for (fe_scene* s : b->scenes) FE_CUDA(cudaMemsetAsync(s->cg.bar + 2, 0, sizeof(unsigned), b->stream));
+    const bool overlap = b->overlap && !batch_has_viscosity(b);
     for (int it = 0; it < nsub; ++it) {
         if (b->steps_done < kBatchCaptureAfter || std::any_of(b->scenes.begin(), b->scenes.end(),
                                                                  [](fe_scene* s) { return s->graphs_disabled; })) {
-            fe_status st = batch_step_scene_graphs(b, dt);
+            fe_status st = overlap ? batch_step_overlap_scene_graphs(b, dt) : batch_step_scene_graphs(b, dt);
             if (st != FE_OK) return st;
             ++b->steps_done;
             continue;
+        }
+        if (overlap && !b->shares_measured) {
+            fe_status st = batch_resplit(b);  // the young substeps measured each scene's solve work
+            if (st != FE_OK) return st;
+            batch_drop_graphs(b);
         }
         uint64_t epoch = 0;
         for (const fe_scene* s : b->scenes) epoch += s->epoch;

@@ -346,6 +346,11 @@ class Batch:
         check(self._L.fe_batch_create(arr, len(self.scenes), ctypes.byref(h)))
         self._h = h
 
+    def set_overlap(self, on=True):
+        """Overlap mode (fe_batch_set_overlap): each scene's whole substep on its own stream, its solve on its
+        share of the solver blocks, so solves overlap other scenes' transfer kernels."""
+        check(self._L.fe_batch_set_overlap(self._h, 1 if on else 0))
+
     def set_scenes(self, scenes):
         """Changes the batch's scenes in place (no device allocation)."""
         scenes = list(scenes)

@@ -68,12 +68,13 @@ class Server:
     """
 
     def __init__(self, hbm_budget_bytes, max_batch=32, device=0, cg_rel_tol=1e-6, seed_threads=4,
-                 reuse_scenes=True):
+                 reuse_scenes=True, overlap=False):
         self.budget = int(hbm_budget_bytes)
         self.max_batch = min(int(max_batch), 64)
         self.device = device
         self.cg_rel_tol = cg_rel_tol
         self.reuse_scenes = reuse_scenes
+        self.overlap = overlap   # batch overlap mode (each job's substep on its own stream, see Batch.set_overlap)
         self.seed_threads = max(1, int(seed_threads))
         self.used = 0            # bytes of live scenes (running, pooled, being prepared or released)
         self.reserved = 0        # bytes reserved for preparations that need a new scene
@@ -218,6 +219,8 @@ class Server:
                 self.batch.step(dt, nsub, stats=False)
             else:
                 b = Batch([j.scene for j in jobs])
+                if self.overlap:
+                    b.set_overlap(True)
                 b.step(dt, nsub, stats=False)
                 b.close()
             out.append((jobs, nsub, (time.perf_counter() - f0) * 1e3))
@@ -312,6 +315,8 @@ class Server:
                     t = time.perf_counter()
                     if self.batch is None:
                         self.batch = Batch([j.scene for j in self.running])
+                        if self.overlap:
+                            self.batch.set_overlap(True)
                     else:
                         self.batch.set_scenes([j.scene for j in self.running])
                     self.rebuilds += 1

@@ -378,6 +378,13 @@ fe_status fe_batch_destroy(fe_batch* b);
  * a server whose running set changes between frames keeps one batch; the batch graph is captured again
  * once the new membership has run a few substeps.  Waits for the batch's earlier work to finish. */
 fe_status fe_batch_set_scenes(fe_batch* b, fe_scene* const* scenes, int32_t count);
+/* Overlap mode (on != 0): instead of all scenes' pre-solve, then one multi-scene solve, then all post-solve, every
+ * scene runs its whole substep on its own stream -- pre-solve, its own cooperative solve on its share of the
+ * co-resident solver blocks (split by each scene's measured solve work; the shares add up to the device's
+ * capacity, so every solve in flight fits at once), post-solve -- so one scene's latency-bound solve overlaps other
+ * scenes' transfer kernels.  Same results; ignored while any scene has viscosity (its cooperative Jacobi solve
+ * stays alone).  fe_batch_step_profiled always runs the phase-separated form. */
+fe_status fe_batch_set_overlap(fe_batch* b, int32_t on);
 /* nsub substeps of dt for every scene; stats (NULL or count * nsub entries, scene-major) as fe_scene_step. */
 fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats);
 /* fe_batch_step with per-substep device timing of the batch's three phases (all scenes' pre-solve, the

@@ -246,3 +246,26 @@ def test_server_job_cancelled_mid_run_leaves_the_others_unchanged():
         assert rel_l2(j.final[0], P) < 1e-5
         assert rel_l2(j.final[1], V) < 1e-4
         s.close()
+
+
+def test_overlap_mode_matches_alone():
+    """Overlap mode (each scene's whole substep on its own stream with its own solve on its share of the solver
+    blocks): every scene still matches the same scene stepped alone, through the young substeps, the re-split of
+    the shares and the captured batch graph."""
+    dt = 1.0 / 240.0
+    alone = [make(sp, 60 + i) for i, sp in enumerate(SPECS)]
+    mixed = [make(sp, 60 + i) for i, sp in enumerate(SPECS)]
+    mixed[1].set_tuning(multigrid=1)  # one scene on the multigrid body
+    alone[1].set_tuning(multigrid=1)
+    for s in alone:
+        s.step(dt, 14)
+    b = fe.Batch(mixed)
+    b.set_overlap(True)
+    stats = b.step(dt, 14)
+    b.close()
+    for a, m, st in zip(alone, mixed, stats):
+        assert all(x["converged"] == 1 and x["rel_residual"] <= 1e-6 for x in st), st
+        Pa, Va, _ = a.particles()
+        Pm, Vm, _ = m.particles()
+        assert rel_l2(Pm, Pa) < 1e-5
+        assert rel_l2(Vm, Va) < 1e-4

@@ -48,6 +48,9 @@ class FakeBatch:
     def set_scenes(self, scenes):
         self.__init__(scenes)
 
+    def set_overlap(self, on=True):
+        self.overlap = on
+
     def step(self, dt, nsub, stats=True):
         time.sleep(0.002)
         for s in self.scenes:
