@@ -1027,7 +1027,7 @@ fe_status emit_particles(fe_scene* s)
                              view_of(s, s->parity), np, em.vel, st));
         s->base.np = np + total;
         s->have_particles = true;
-        drop_graphs(s);  // graphs are sized by the particle count
+            drop_graphs(s);  // graphs are sized by the particle count
     }
     return FE_OK;
 }

@@ -200,19 +200,58 @@ __global__ void k_place_final(SceneView v)
     v.perm[v.rank[i]] = (uint32_t)i;
 }
 
-__global__ void k_gather(SceneView src, SceneView dst, int ncomp)
+// Each thread moves kGatherBatch particles, all their loads issued before any store, so a thread keeps several
+// rows of requests in flight instead of one.
+constexpr int kGatherBatch = 4;
+
+template <bool APIC>
+__global__ void __launch_bounds__(256) k_gather(SceneView src, SceneView dst)
 {
-    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= src.np) return;
-    uint32_t j = src.perm[i];
-    dst.px[i] = src.px[j];
-    dst.py[i] = src.py[j];
-    dst.pz[i] = src.pz[j];
-    dst.vx[i] = src.vx[j];
-    dst.vy[i] = src.vy[j];
-    dst.vz[i] = src.vz[j];
-    dst.pid[i] = src.pid[j];
-    for (int c = 0; c < ncomp; ++c) dst.c[c][i] = src.c[c][j];
+    const uint64_t base = (blockIdx.x * (uint64_t)blockDim.x) * kGatherBatch + threadIdx.x;
+    uint32_t j[kGatherBatch];
+    bool ok[kGatherBatch];
+#pragma unroll
+    for (int b = 0; b < kGatherBatch; ++b) {
+        const uint64_t i = base + (uint64_t)b * blockDim.x;
+        ok[b] = i < src.np;
+        j[b] = ok[b] ? src.perm[i] : 0u;
+    }
+    float a[kGatherBatch][6];
+    uint32_t id[kGatherBatch];
+#pragma unroll
+    for (int b = 0; b < kGatherBatch; ++b) {
+        if (!ok[b]) continue;
+        a[b][0] = src.px[j[b]];
+        a[b][1] = src.py[j[b]];
+        a[b][2] = src.pz[j[b]];
+        a[b][3] = src.vx[j[b]];
+        a[b][4] = src.vy[j[b]];
+        a[b][5] = src.vz[j[b]];
+        id[b] = src.pid[j[b]];
+    }
+#pragma unroll
+    for (int b = 0; b < kGatherBatch; ++b) {
+        if (!ok[b]) continue;
+        const uint64_t i = base + (uint64_t)b * blockDim.x;
+        dst.px[i] = a[b][0];
+        dst.py[i] = a[b][1];
+        dst.pz[i] = a[b][2];
+        dst.vx[i] = a[b][3];
+        dst.vy[i] = a[b][4];
+        dst.vz[i] = a[b][5];
+        dst.pid[i] = id[b];
+    }
+    if (APIC) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            float t[kGatherBatch];
+#pragma unroll
+            for (int b = 0; b < kGatherBatch; ++b) t[b] = ok[b] ? src.c[c][j[b]] : 0.f;
+#pragma unroll
+            for (int b = 0; b < kGatherBatch; ++b)
+                if (ok[b]) dst.c[c][base + (uint64_t)b * blockDim.x] = t[b];
+        }
+    }
 }
 
 }  // namespace
@@ -267,7 +306,9 @@ cudaError_t launch_gather(const SceneView& v, const SceneView& dst, cudaStream_t
 {
     if (v.np == 0) return cudaSuccess;
     const int T = 256;
-    k_gather<<<(unsigned)((v.np + T - 1) / T), T, 0, st>>>(v, dst, v.solver == FE_SOLVER_APIC ? 9 : 0);
+    const unsigned nb = (unsigned)((v.np + (uint64_t)T * kGatherBatch - 1) / ((uint64_t)T * kGatherBatch));
+    if (v.solver == FE_SOLVER_APIC) k_gather<true><<<nb, T, 0, st>>>(v, dst);
+    else k_gather<false><<<nb, T, 0, st>>>(v, dst);
     count_launch();
     return cudaGetLastError();
 }
