@@ -20,11 +20,11 @@
 //              iteration's neighbour values; r, w and s ping-pong so those stay intact within the pass.
 //              A cell's (r, w, s, p) sit together in one float4, so a neighbour costs one 16-byte load and
 //              the cell's new state one 16-byte store.
-// The grid-wide barrier is a counter + generation word with a bounded spin: if a block waits longer than
-// a few seconds it records FE_ERR_TIMEOUT, every block leaves its loops and the kernel returns, so a stuck
-// solve surfaces as a status instead of a hung device.  Dot products travel with the barrier: blocks
-// add their partials into a rotating totals slot before arriving and read the totals once after it, so
-// all blocks take identical branch decisions.
+// The grid-wide barrier is an arrival count polled with a bounded spin: if a block waits longer than a few
+// seconds it records FE_ERR_TIMEOUT, every block leaves its loops and the kernel returns, so a stuck solve
+// surfaces as a status instead of a hung device.  Dot products travel with the barrier: blocks add their
+// partials into a rotating totals slot before arriving and read the totals once after it, so all blocks take
+// identical branch decisions.
 #include <algorithm>
 
 #include "fe_solver_common.cuh"
@@ -100,7 +100,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
             racc[0] += rr * rr;
         }
         cur = 0;
-        if (!grid_reduce<1>(racc, sh, w, gen, nblk)) return;
+        if (!grid_reduce<1>(racc, sh, w, gen, nblk, blk)) return;
         rnorm = sqrt(racc[0]);
         if (rnorm <= target) {
             converged = true;
@@ -121,7 +121,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
             d0[0] += (double)rc * (double)rc;
             d0[1] += (double)wc * (double)rc;
         }
-        if (!grid_reduce<2>(d0, sh, w, gen, nblk)) return;
+        if (!grid_reduce<2>(d0, sh, w, gen, nblk, blk)) return;
         double gamma = d0[0], delta = d0[1];
         const double gamma0 = gamma;
         const double want = fmax(prm.inner_tol, 0.25 * target / rnorm);
@@ -160,7 +160,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
                 dd[0] += (double)rc * (double)rc;
                 dd[1] += (double)wc * (double)rc;
             }
-            if (!grid_reduce<2>(dd, sh, w, gen, nblk)) return;
+            if (!grid_reduce<2>(dd, sh, w, gen, nblk, blk)) return;
             ++total_it;
             cur ^= 1;
             gamma_prev = gamma;
@@ -174,7 +174,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
             const int c = (int)(entry(k, e) >> 6);
             p64[c] += (double)X[c];
         }
-        if (!grid_sync(w, gen, nblk, sh)) return;
+        if (!grid_sync(w, gen, nblk, sh, blk)) return;
     }
     if (blk == 0 && threadIdx.x == 0 && out_its) {
         *out_its = total_it;
@@ -198,6 +198,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(SceneView v, CgWork w, CgP
     __shared__ SolverSmem smem;
     cluster_begin(w, smem.sh);
     cg_body(smem, v, w, prm, blockIdx.x, gridDim.x);
+    solver_exit(w, gridDim.x);
     cluster_end(w);
 }
 
@@ -207,6 +208,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_mgcg(SceneView v, CgWork w, M
     __shared__ SolverSmem smem;
     cluster_begin(w, smem.sh);
     mg_body(smem, v, w, mg, prm, blockIdx.x, gridDim.x);
+    solver_exit(w, gridDim.x);
     cluster_end(w);
 }
 
@@ -232,6 +234,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_multi_cg(MultiCgScene* __r
     __shared__ SolverSmem smem;
     if (m.use_mg) mg_body(smem, m.view, m.work, m.mg, prm, blk, m.block_count, &its, &fluid);
     else cg_body(smem, m.view, m.work, prm, blk, m.block_count, &its, &fluid);
+    solver_exit(m.work, m.block_count);
     if (blk == 0 && threadIdx.x == 0) {  // read by the next solve's k_multi_partition
         m.last_its = its;
         m.last_fluid = fluid;

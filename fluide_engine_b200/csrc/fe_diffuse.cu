@@ -115,9 +115,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
     extern __shared__ unsigned long long s_ent[];  // [kJacobiCache] entries, then [kJacobiCache] floats
     float* s_b = (float*)(s_ent + kJacobiCache);
     const int nblk = gridDim.x, blk = blockIdx.x;
-    unsigned gen = 0;
-    if (threadIdx.x == 0)
-        gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[32]).load(cuda::memory_order_relaxed);
+    unsigned gen = 0;  // barriers passed in this launch
     const unsigned count = __ldcg(d.count);
     // The list is in face order, component by component; it is dealt to the blocks in tiles of blockDim.x
     // consecutive entries (tile t to block t % nblk), so every block holds a share of each component and the
@@ -267,7 +265,10 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
             const int a2 = __syncthreads_or((int)(chg & 4u));
             double red[4] = {acc[0], acc[1], acc[2],
                              threadIdx.x == 0 ? (a0 ? 1.0 : 0.0) + (a1 ? 1024.0 : 0.0) + (a2 ? 1048576.0 : 0.0) : 0.0};
-            if (!grid_reduce<4>(red, sh, w, gen, nblk)) return;
+            if (!grid_reduce<4>(red, sh, w, gen, nblk, blk)) {
+                solver_exit(w, nblk);
+                return;
+            }
             if (threadIdx.x == 0) {
                 const double packed = red[3];
                 const double changed[3] = {fmod(packed, 1024.0), fmod(floor(packed / 1024.0), 1024.0),
@@ -305,7 +306,8 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
                 ctl.take = next_take;
                 ctl.cmp = next_cmp;
             }
-        } else if (!grid_sync(w, gen, nblk, sh)) {
+        } else if (!grid_sync(w, gen, nblk, sh, blk)) {
+            solver_exit(w, nblk);
             return;
         }
         if (threadIdx.x == 0) {
@@ -348,6 +350,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
         d.its[2] = ctl.its[2];
         d.its[3] = ctl.passes;
     }
+    solver_exit(w, nblk);
 }
 
 }  // namespace

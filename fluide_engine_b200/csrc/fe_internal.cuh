@@ -20,12 +20,16 @@ namespace fe {
 
 constexpr int kMaxRefineDefault = 12;
 constexpr int kMaxCgBlocks = 4096;  // solver blocks one scene can be given (sizes its partial-sum buffer)
-// Grid-barrier words of one solver: [0] arrival count, [2] statistics counter, [32] generation (its own
-// 128-byte line, so the blocks polling it do not contend with the arrivals on [0]).
+// Grid-barrier words of one solver: [0] arrivals of the current launch, [2] statistics counter (kept across
+// launches), [32] blocks that have left the current launch (its own 128-byte line).
 constexpr int kCgBarWords = 64;
-// Doubles of one solver's partial buffer for up to max_blocks blocks: the reduction totals slots, then the
-// per-block FLUID counts of the solver's setup.
-constexpr size_t cg_partial_doubles(size_t max_blocks) { return 16 + max_blocks; }
+// Grid-reduction totals: 3 rotating slots x 4 groups x 4 sums, every total on its own 128-byte line (16 doubles).
+constexpr int kCgTotalsGroups = 4;
+constexpr int kCgTotalsStride = 16;
+constexpr int kCgTotalsDoubles = 3 * kCgTotalsGroups * 4 * kCgTotalsStride;
+// Doubles of one solver's partial buffer for up to max_blocks blocks: the reduction totals, then the per-block
+// FLUID counts of the solver's setup.
+constexpr size_t cg_partial_doubles(size_t max_blocks) { return kCgTotalsDoubles + max_blocks; }
 constexpr int kBatchMaxScenes = 64;
 // Entries of a scene's device ring of solve statistics (one per pressure solve; solves wrap around it).
 constexpr unsigned kStatsRingEntries = 1u << 16;
@@ -233,7 +237,7 @@ struct CgWork {
     float4 *rws0, *rws1;
     float* xcg;
     uint32_t* list;         // compacted FLUID cells: (cell << 6) | in-domain neighbour mask
-    double* partial;        // [0, 12) three rotating reduction totals slots, [16, 16 + max blocks) FLUID counts
+    double* partial;        // [0, kCgTotalsDoubles) reduction totals, then one FLUID count per block
     unsigned* bar;          // kCgBarWords barrier words
     int* err;
     fe_step_stats* stats;   // device ring of solve statistics

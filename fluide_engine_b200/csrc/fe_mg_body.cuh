@@ -216,7 +216,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                     }
             C.mask[t] = any;
         }
-        if (!grid_sync(w, gen, nblk, sh)) return;
+        if (!grid_sync(w, gen, nblk, sh, blk)) return;
     }
 
     const double target = prm.rel_tol * bnorm;
@@ -248,7 +248,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
             P[0][c] = 0.f;
             racc[0] += rr * rr;
         }
-        if (!grid_reduce<1>(racc, sh, w, gen, nblk)) return;
+        if (!grid_reduce<1>(racc, sh, w, gen, nblk, blk)) return;
         rnorm = sqrt(racc[0]);
         if (rnorm <= target) {
             converged = true;
@@ -289,7 +289,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                     RES[c] = rc - Az1;
                     acc[0] += (double)rc * (double)rc;
                 }
-                if (!grid_reduce<1>(acc, sh, w, gen, nblk)) return;
+                if (!grid_reduce<1>(acc, sh, w, gen, nblk, blk)) return;
                 cur ^= 1;
                 if (first) stop = want * want * acc[0];
                 else ++total_it;
@@ -306,7 +306,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                         val = restrict_at(I, J, K, C, nx, ny, nz, [&](size_t q) { return __ldcg(RES + q); });
                     C.r[t] = val;
                 }
-                if (!grid_sync(w, gen, nblk, sh)) return;
+                if (!grid_sync(w, gen, nblk, sh, blk)) return;
             }
             // Per level: residual (stored in t), restriction into the next level's r (going down); pre-smoothed
             // correction t = z1 + P z_next, one Jacobi sweep into z (going up).  `sync` separates the passes:
@@ -350,7 +350,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                 }
                 return sync();
             };
-            auto gsync = [&]() { return grid_sync(w, gen, nblk, sh); };
+            auto gsync = [&]() { return grid_sync(w, gen, nblk, sh, blk); };
             auto bsync = [&]() {
                 __threadfence();
                 __syncthreads();
@@ -399,7 +399,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                 bsync();
                 for (int l = L - 2; l >= LB; --l) level_up(l, threadIdx.x, blockDim.x, bsync);
             }
-            if (!grid_sync(w, gen, nblk, sh)) return;
+            if (!grid_sync(w, gen, nblk, sh, blk)) return;
             for (int l = LB - 1; l >= 1; --l)
                 if (!level_up(l, tid, T, gsync)) return;
             // level 0: pre-smoothed correction into the residual vector (free again), then one Jacobi sweep
@@ -412,7 +412,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                     const int i = c % nx, j = (c / nx) % ny, kk = c / sxy;
                     RES[c] = kOmega * r[c] / level_diag(i, j, kk, nx, ny, nz, ih2) + prolong_at(C, i, j, kk);
                 }
-                if (!grid_sync(w, gen, nblk, sh)) return;
+                if (!grid_sync(w, gen, nblk, sh, blk)) return;
                 double acc[1] = {0.0};
                 for (int e = tid, k = 0; e < F; e += T, ++k) {
                     const uint32_t ent = entry(k, e);
@@ -423,7 +423,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                     Z[c] = zc;
                     acc[0] += (double)r[c] * (double)zc;
                 }
-                if (!grid_reduce<1>(acc, sh, w, gen, nblk)) return;
+                if (!grid_reduce<1>(acc, sh, w, gen, nblk, blk)) return;
                 rho = acc[0];
             }
             // search direction: p' = z + beta p, q = A p', (p', q)
@@ -445,7 +445,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                     Q[c] = qc;
                     acc[0] += (double)pc_ * (double)qc;
                 }
-                if (!grid_reduce<1>(acc, sh, w, gen, nblk)) return;
+                if (!grid_reduce<1>(acc, sh, w, gen, nblk, blk)) return;
                 pc ^= 1;
                 const double a = rho / acc[0];
                 if (!(a > 0.0) || !isfinite(a)) break;  // FP32 breakdown: leave it to the outer loop
@@ -457,7 +457,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
             const int c = (int)(entry(k, e) >> 6);
             p64[c] += (double)X[c];
         }
-        if (!grid_sync(w, gen, nblk, sh)) return;
+        if (!grid_sync(w, gen, nblk, sh, blk)) return;
     }
     if (blk == 0 && threadIdx.x == 0 && out_its) {
         *out_its = total_it;

@@ -168,10 +168,10 @@ extern "C" fe_status fe_project_noalloc(const int32_t n[3], const double h[3], c
     view.p = p;
     view.b = (double*)(base + kOffB);
 
-    // barrier words (arrival count, generation, statistics counter), reduction totals slots and the error
+    // barrier words (arrival and exit counts, statistics counter), reduction totals slots and the error
     // flag start at zero on every call
     FE_CUDA(cudaMemsetAsync(work.bar, 0, kCgBarWords * sizeof(unsigned), s));
-    FE_CUDA(cudaMemsetAsync(work.partial, 0, 12 * sizeof(double), s));
+    FE_CUDA(cudaMemsetAsync(work.partial, 0, kCgTotalsDoubles * sizeof(double), s));
     FE_CUDA(cudaMemsetAsync(work.err, 0, sizeof(int), s));
     FE_CUDA(launch_rhs(view, s));
     FE_CUDA(launch_cg(view, work, rel_tol, 1e-4, max_it, kMaxRefineDefault, s));

@@ -782,8 +782,8 @@ fe_status check_device_error(fe_scene* s)
     FE_CUDA(cudaStreamSynchronize(s->stream));
     if (err) {
         cudaMemsetAsync(s->cg.err, 0, sizeof(int), s->stream);
-        cudaMemsetAsync(s->cg.bar, 0, kCgBarWords * sizeof(unsigned), s->stream);  // count and generation
-        cudaMemsetAsync(s->cg.partial, 0, 12 * sizeof(double), s->stream);  // totals slots restart at zero
+        cudaMemsetAsync(s->cg.bar, 0, kCgBarWords * sizeof(unsigned), s->stream);  // arrival and exit counts
+        cudaMemsetAsync(s->cg.partial, 0, kCgTotalsDoubles * sizeof(double), s->stream);  // totals restart at zero
         cudaStreamSynchronize(s->stream);
         return set_error((fe_status)err, "pressure solve: grid barrier wait exceeded its limit");
     }

@@ -28,42 +28,32 @@ struct CgParams {
     unsigned stats_cap;
 };
 
-// Barrier generations count modulo 65535 (a multiple of 3), so the three rotating totals slots keep their
-// order across the wrap.
-__device__ __forceinline__ unsigned next_gen(unsigned g) { return g + 1u == 65535u ? 0u : g + 1u; }
-
-// Grid-wide barrier on two words in different 128-byte lines: bar[0] counts arrivals (one acq_rel
-// fetch_add per block), bar[32] holds the generation.  The last arriver resets the count, zeroes the totals
-// slot of the next generation and bumps the generation with a release store; the others poll the
-// generation (bounded) with acquire loads, away from the line the arrivals hit.  The release/acquire pair at
-// device scope, with the __syncthreads on either side, orders every thread's memory traffic of the block
-// across the barrier.  `gen` is the generation this barrier started in (tracked by thread 0).  The two
-// halves can be used apart (a split-phase barrier: arrive, do work that needs nothing from the others, then
-// wait); bar_arrive returns true for the last arriver, whose barrier is then already complete.
-__device__ __forceinline__ bool bar_arrive(unsigned* bar, unsigned nblocks, double* totals, unsigned gen)
+// ---- Grid barrier.  The barrier words and the totals start every launch at zero: the last block to leave a
+// solver kernel puts them back (solver_exit), and the host clears them after a solve that failed.  bar[0] counts
+// the arrivals of the whole launch: each arriving block (or cluster leader) adds 1 with a release reduction and
+// polls the count with acquire loads until it reaches (gen + 1) x arrivals, so nothing on the critical path resets
+// a word or bumps a generation: a barrier costs the release (which waits for the block's own totals adds) and
+// the poll.  `gen` is the number of barriers this launch has passed, tracked by every thread.
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
 {
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
-    const unsigned old = count.fetch_add(1u, cuda::memory_order_acq_rel);
-    if (old == nblocks - 1 + c_extra_arrivals) {
-        double* next = totals + 4 * (next_gen(gen) % 3u);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) next[k] = 0.0;
-        count.store(0u, cuda::memory_order_relaxed);
-        genw.store(next_gen(gen), cuda::memory_order_release);
-        return true;  // last arriver: the barrier is complete
-    }
-    return false;
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// The waiting half: polls the generation until it leaves `gen` (bounded); false when the wait gave up.
-__device__ __forceinline__ bool bar_wait(unsigned* bar, int* err, unsigned gen)
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
 {
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> genw(bar[32]);
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Polls bar[0] until it reaches `target` (bounded: FE_ERR_TIMEOUT after the limit; gives up early when another
+// block has set the error flag).  False when the wait gave up.
+__device__ __forceinline__ bool bar_poll(const unsigned* bar, int* err, unsigned target)
+{
     cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
     unsigned long long spins = 0;
     const unsigned long long limit = c_spin_limit;
-    while (genw.load(cuda::memory_order_acquire) == gen) {
+    while ((int)(ld_acquire(bar) - target) < 0) {
         if (++spins > limit) {
             e.store(FE_ERR_TIMEOUT, cuda::memory_order_relaxed);
             return false;
@@ -73,24 +63,37 @@ __device__ __forceinline__ bool bar_wait(unsigned* bar, int* err, unsigned gen)
     return true;
 }
 
-__device__ __forceinline__ bool bar_arrive_wait(unsigned* bar, int* err, unsigned nblocks, double* totals, unsigned gen)
+// Total k of group g in rotating slot `slot` (one 128-byte line each).
+__device__ __forceinline__ double* totals_at(double* partial, unsigned slot, int g, int k)
 {
-    if (bar_arrive(bar, nblocks, totals, gen)) return true;
-    return bar_wait(bar, err, gen);
+    return partial + (size_t)(((int)slot * kCgTotalsGroups + g) * 4 + k) * kCgTotalsStride;
+}
+
+// Last act of every block of a solver kernel (thread 0, after its last barrier): the last block to leave puts
+// the arrival count and the totals back to zero for the next launch.  The others have finished all their polls
+// and totals reads before their exit add (release), which the last one observes (acquire).
+__device__ __forceinline__ void solver_exit(const CgWork& w, int nblk)
+{
+    if (threadIdx.x != 0) return;
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> left(w.bar[32]);
+    if (left.fetch_add(1u, cuda::memory_order_acq_rel) != (unsigned)nblk - 1u) return;
+    for (int i = 0; i < 3 * kCgTotalsGroups * 4; ++i) w.partial[(size_t)i * kCgTotalsStride] = 0.0;
+    w.bar[0] = 0u;
+    left.store(0u, cuda::memory_order_relaxed);
 }
 
 // ---- Cluster pre-reduction (CgWork::cluster > 1: the solver was launched in thread-block clusters of that size).
 // Inside a cluster the blocks hand their partial sums to the cluster's first block (rank 0, the leader) through
 // distributed shared memory and a release add on a counter in the leader's shared memory; only the leader adds into
 // the global totals slot and arrives at the grid barrier (arrivals: one per cluster), while every block polls the
-// barrier's generation as before.  The leader's wait for its cluster is a bounded poll of its own shared memory,
+// barrier's arrival count as before.  The leader's wait for its cluster is a bounded poll of its own shared memory,
 // so an error anywhere still ends every block's waits; the kernel's last step is a cluster barrier (all waits before
 // it are bounded), so no block exits while another block of its cluster may still write into its shared memory.
 // Shared-memory words of the leader: the partials at sh[kClusterSlots + 4 rank + k], the arrival counter and the
 // count of cluster gathers so far behind them.
 constexpr int kMaxCluster = 16;
 constexpr int kClusterSlots = 132;                         // after the block reduction's 132 doubles
-constexpr int kShDoubles = kClusterSlots + 4 * kMaxCluster + 2;
+constexpr int kShDoubles = kClusterSlots + 4 * kMaxCluster + 3;  // + the barrier outcome word
 
 __device__ __forceinline__ unsigned* cluster_counter(double* sh) { return reinterpret_cast<unsigned*>(sh + kClusterSlots + 4 * kMaxCluster); }
 __device__ __forceinline__ unsigned* cluster_rounds(double* sh) { return reinterpret_cast<unsigned*>(sh + kClusterSlots + 4 * kMaxCluster + 1); }
@@ -170,50 +173,89 @@ __device__ __forceinline__ void cluster_end(const CgWork& w)
     if (w.cluster > 1) cluster_barrier_all();
 }
 
-// Arrival of this block at grid barrier `gen` with N partial sums already reduced into `part` (thread 0): plain, or
-// through its cluster's leader.  Returns false when a wait gave up.
+// Blocks that arrive at each barrier: every block, or one per cluster; plus the test hook's extra arrivals.
+__device__ __forceinline__ int barrier_members(const CgWork& w, int nblk) { return w.cluster > 1 ? nblk / w.cluster : nblk; }
+
+// Copies of the totals: several groups of arriving blocks add into their own copy once there are many arrivals.
+__device__ __forceinline__ int totals_groups(int members) { return members > 256 ? kCgTotalsGroups : 1; }
+
+// Warp 0 of every block, at grid barrier `gen` with N partial sums in lane 0's `part` (already reduced over the
+// block): the arrival (plain, or through its cluster's leader), the bounded poll by lane 0, and the totals read by
+// lanes g N + k of every group g in parallel with the error flag (lane 31).  Lanes k < N return total k in `out`,
+// summed over the groups in group order, so every block gets the same bits.  All lanes return whether the waits
+// ended and no block has reported an error.  Block 0 then zeroes the slot two barriers ahead: its last readers
+// arrived at this barrier, and its next adders only start after this block's next arrival (a release).
 template <int N>
-__device__ __forceinline__ bool arrive_and_wait(double* part, double* sh, const CgWork& w, unsigned gen, int nblk)
+__device__ __forceinline__ bool warp0_barrier(double* part, double& out, double* sh, const CgWork& w, unsigned gen,
+                                              int nblk, int blk)
 {
-    double* totals = w.partial;  // [3][4]
-    double* slot = totals + 4 * (gen % 3u);  // zeroed by the release of this generation
-    if (w.cluster > 1) {
-        if (!cluster_gather<N>(part, sh, w.cluster, w.err)) return false;
-        if (cluster_rank() != 0) return bar_wait(w.bar, w.err, gen);
+    const int lane = threadIdx.x & 31;
+    const unsigned slot = gen % 3u;
+    const int members = barrier_members(w, nblk);
+    const int G = totals_groups(members);
+    bool ok = true;
+    if (lane == 0) {
+        bool arrive = true;
+        int member = blk;
+        if (w.cluster > 1) {
+            ok = cluster_gather<N>(part, sh, w.cluster, w.err);
+            arrive = cluster_rank() == 0;
+            member = blk / w.cluster;
+        }
+        if (ok && arrive) {
 #pragma unroll
-        for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
-        return bar_arrive_wait(w.bar, w.err, (unsigned)(nblk / w.cluster), totals, gen);
+            for (int k = 0; k < N; ++k) atomicAdd(totals_at(w.partial, slot, member % G, k), part[k]);
+            red_release_add(w.bar, 1u);
+        }
+        if (ok) ok = bar_poll(w.bar, w.err, (gen + 1u) * (unsigned)(members + (int)c_extra_arrivals));
     }
+    __syncwarp();
+    double t = 0.0;
+    int e = 0;
+    if (N > 0 && lane < G * N) t = __ldcg(totals_at(w.partial, slot, lane / (N > 0 ? N : 1), lane % (N > 0 ? N : 1)));
+    if (N > 0 && lane == 31) e = __ldcg(w.err);
+    ok = __all_sync(0xffffffffu, ok && e == 0) != 0;
+    double sum = 0.0;
+    for (int g = 0; g < G; ++g)
 #pragma unroll
-    for (int k = 0; k < N; ++k) atomicAdd(slot + k, part[k]);
-    return bar_arrive_wait(w.bar, w.err, (unsigned)nblk, totals, gen);
+        for (int k = 0; k < N; ++k) {
+            const double x = __shfl_sync(0xffffffffu, t, g * N + k);
+            if (lane == k) sum += x;
+        }
+    if (blk == 0 && lane < 4 * G) *totals_at(w.partial, (slot + 2u) % 3u, lane >> 2, lane & 3) = 0.0;
+    out = sum;
+    return ok;
 }
 
-__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk, double* sh)
+// Shared-memory word through which warp 0 hands the barrier's outcome to the whole block.
+constexpr int kShFlag = kShDoubles - 1;
+
+__device__ __forceinline__ bool grid_sync(const CgWork& w, unsigned& gen, int nblk, double* sh, int blk)
 {
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         double none[1] = {0.0};
-        arrive_and_wait<0>(none, sh, w, gen, nblk);
-        gen = next_gen(gen);
+        double out;
+        const bool ok = warp0_barrier<0>(none, out, sh, w, gen, nblk, blk);
+        if (threadIdx.x == 0) sh[kShFlag] = ok ? 0.0 : 1.0;
     }
+    ++gen;
     __syncthreads();
-    return *(volatile int*)w.err == 0;
+    return sh[kShFlag] == 0.0;
 }
 
-// Grid-wide sum of N doubles fused with the barrier.  Each block reduces to warp 0, whose lane 0 adds
-// the block partials into the totals slot of this barrier (FP64 red.add, ordered before the arrival by
-// its release) and arrives; after the barrier it reads the totals once.  Three total slots rotate: the
-// last arriver of barrier k zeroes slot k+1 before releasing it, and slot k is read only until the
-// readers arrive at barrier k+1.  All blocks read the same final totals, so their branch decisions
-// agree (the summation order, and hence the last bits, can vary from run to run).  (Per-block slots summed
-// by the last arriver avoid the floating-point atomics but put one more L2 round trip on the critical
-// path, which measured slower.)
+// Grid-wide sum of N doubles fused with the barrier.  Each block reduces to warp 0, whose lane 0 adds the block
+// partials into its group's copy of the totals slot of this barrier (FP64 red.add, ordered before the arrival by
+// its release) and arrives; after the barrier warp 0 reads the totals once.  All blocks read the same totals and
+// sum the groups in the same order, so their branch decisions agree (the order of the atomic adds, and hence the
+// last bits, can vary from run to run).  (Measured alternatives: per-block slots summed by the last arriver, an
+// arrival tree, an all-gather of per-block slots, and a generation word bumped by the last arriver all put more
+// L2 round trips on the critical path.)
 template <int N>
 __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [kShDoubles] */, const CgWork& w, unsigned& gen,
-                                            int nblk)
+                                            int nblk, int blk)
 {
-    static_assert(N <= 4, "at most 4 sums per reduction");
+    static_assert(N >= 1 && N <= 4, "1 to 4 sums per reduction");
     // warp partials use sh[0, 32 N), the totals sh[128, 128 + N): disjoint, so a warp that races ahead into
     // the next reduction cannot overwrite totals another warp has not read yet
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -235,21 +277,16 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [kShDo
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             part[k] = s;
         }
-        if (lane == 0) {
-            // slot of this barrier: generation modulo 3; thread 0 tracks the generation itself (it takes
-            // part in every barrier), which saves a load round trip per barrier
-            const double* slot = w.partial + 4 * (gen % 3u);
-            const bool ok = arrive_and_wait<N>(part, sh, w, gen, nblk);
-            gen = next_gen(gen);
-            if (ok)
-#pragma unroll
-                for (int k = 0; k < N; ++k) sh[128 + k] = __ldcg(slot + k);
-        }
+        double out;
+        const bool ok = warp0_barrier<N>(part, out, sh, w, gen, nblk, blk);
+        if (lane < N) sh[128 + lane] = out;
+        if (lane == 0) sh[kShFlag] = ok ? 0.0 : 1.0;
     }
+    ++gen;
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < N; ++k) v[k] = sh[128 + k];
-    return *(volatile int*)w.err == 0;
+    return sh[kShFlag] == 0.0;
 }
 
 // Block-wide sum of one double, valid in all threads (setup only).
@@ -350,9 +387,7 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
     float* __restrict__ W[2] = {w.w0, w.w1};
     float* __restrict__ S[2] = {w.s0, w.s1};
     uint32_t* __restrict__ list = w.list;
-    // barrier generation as of this launch (thread 0 keeps it from here on)
-    gen = 0;
-    if (threadIdx.x == 0) gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(w.bar[32]).load(cuda::memory_order_relaxed);
+    gen = 0;  // barriers passed in this launch
 
     // ---- setup: zero non-FLUID entries, ||b||^2, per-block FLUID counts over the block's cell range
     const int chunk = (nc + nblk - 1) / nblk;
@@ -380,13 +415,13 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
     }
     // block offset = FLUID count of all earlier blocks (fixed order), total = all blocks
     const double mine = block_sum1(acc[1], sh);
-    if (threadIdx.x == 0) w.partial[16 + blk] = mine;
+    if (threadIdx.x == 0) w.partial[kCgTotalsDoubles + blk] = mine;
     double tot[2] = {acc[0], acc[1]};
-    if (!grid_reduce<2>(tot, sh, w, gen, nblk)) return false;
+    if (!grid_reduce<2>(tot, sh, w, gen, nblk, blk)) return false;
     const double bnorm = sqrt(tot[0]);
     const int F = (int)tot[1];
     double before = 0.0;
-    for (int bb = threadIdx.x; bb < blk; bb += blockDim.x) before += __ldcg(w.partial + 16 + bb);
+    for (int bb = threadIdx.x; bb < blk; bb += blockDim.x) before += __ldcg(w.partial + kCgTotalsDoubles + bb);
     before = block_sum1(before, sh);
     // ordered compaction of this block's FLUID cells with their in-domain masks
     uint32_t base = (uint32_t)before;
@@ -411,7 +446,7 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
         base += total;
         __syncthreads();
     }
-    if (!grid_sync(w, gen, nblk, sh)) return false;
+    if (!grid_sync(w, gen, nblk, sh, blk)) return false;
     const int kc = kListCache / (int)blockDim.x;
     {
         int k = 0;
