@@ -42,6 +42,14 @@ __device__ __forceinline__ float level_diag(int i, int j, int k, int nx, int ny,
            ih2[2] * (float)((k > 0) + (k < nz - 1));
 }
 
+// The Jacobi scale omega / D of cell (i, j, k).  Every pass that applies the smoother (or recomputes a
+// neighbour's pre-smoothed value) takes it from here, so the V-cycle applies one operator throughout and
+// stays symmetric; the fast division is within 2 ulp of omega / D.
+__device__ __forceinline__ float wdiag(int i, int j, int k, int nx, int ny, int nz, const float* ih2)
+{
+    return __fdividef(kOmega, level_diag(i, j, k, nx, ny, nz, ih2));
+}
+
 // Per axis: the two coarse indices of a fine index i and their prolongation weights (the parent twice at
 // a wall, 0.75 + 0.25).
 __device__ __forceinline__ void prolong_axis(int i, int nc, int& c0, int& c1)
@@ -60,7 +68,7 @@ __device__ __forceinline__ float prolong_at(const MgLevel& coarse, int i, int j,
     prolong_axis(k, coarse.nz, k0, k1);
     const float* z = coarse.z;
     const size_t sx = (size_t)coarse.nx, sxy = (size_t)coarse.nx * coarse.ny;
-    auto zz = [&](int a, int b, int c) { return __ldcg(z + (size_t)a + sx * (size_t)b + sxy * (size_t)c); };
+    auto zz = [&](int a, int b, int c) { return z[(size_t)a + sx * (size_t)b + sxy * (size_t)c]; };
     const float y00 = 0.75f * zz(i0, j0, k0) + 0.25f * zz(i1, j0, k0);
     const float y10 = 0.75f * zz(i0, j1, k0) + 0.25f * zz(i1, j1, k0);
     const float y01 = 0.75f * zz(i0, j0, k1) + 0.25f * zz(i1, j0, k1);
@@ -85,13 +93,13 @@ __device__ __forceinline__ float level_residual(const MgLevel& L, int i, int j, 
 {
     const size_t sx = (size_t)L.nx, sxy = (size_t)L.nx * L.ny;
     const size_t c = (size_t)i + sx * j + sxy * k;
-    if (!__ldcg(L.mask + c)) return 0.f;
+    if (!L.mask[c]) return 0.f;
     auto z1 = [&](int a, int b, int d) {
         const size_t q = (size_t)a + sx * b + sxy * d;
-        return kOmega * __ldcg(L.r + q) / level_diag(a, b, d, L.nx, L.ny, L.nz, L.ih2);
+        return L.r[q] * wdiag(a, b, d, L.nx, L.ny, L.nz, L.ih2);
     };
-    const float rc = __ldcg(L.r + c);
-    const float zc = kOmega * rc / level_diag(i, j, k, L.nx, L.ny, L.nz, L.ih2);
+    const float rc = L.r[c];
+    const float zc = rc * wdiag(i, j, k, L.nx, L.ny, L.nz, L.ih2);
     float ax = 0.f, ay = 0.f, az = 0.f;
     if (i > 0) ax += zc - z1(i - 1, j, k);
     if (i + 1 < L.nx) ax += zc - z1(i + 1, j, k);
@@ -108,18 +116,18 @@ __device__ __forceinline__ float level_smooth(const MgLevel& L, int i, int j, in
 {
     const size_t sx = (size_t)L.nx, sxy = (size_t)L.nx * L.ny;
     const size_t c = (size_t)i + sx * j + sxy * k;
-    if (!__ldcg(L.mask + c)) return 0.f;
+    if (!L.mask[c]) return 0.f;
     const float* t = L.t;
-    const float tc = __ldcg(t + c);
+    const float tc = t[c];
     float ax = 0.f, ay = 0.f, az = 0.f;
-    if (i > 0) ax += tc - __ldcg(t + c - 1);
-    if (i + 1 < L.nx) ax += tc - __ldcg(t + c + 1);
-    if (j > 0) ay += tc - __ldcg(t + c - sx);
-    if (j + 1 < L.ny) ay += tc - __ldcg(t + c + sx);
-    if (k > 0) az += tc - __ldcg(t + c - sxy);
-    if (k + 1 < L.nz) az += tc - __ldcg(t + c + sxy);
+    if (i > 0) ax += tc - t[c - 1];
+    if (i + 1 < L.nx) ax += tc - t[c + 1];
+    if (j > 0) ay += tc - t[c - sx];
+    if (j + 1 < L.ny) ay += tc - t[c + sx];
+    if (k > 0) az += tc - t[c - sxy];
+    if (k + 1 < L.nz) az += tc - t[c + sxy];
     const float At = L.ih2[0] * ax + L.ih2[1] * ay + L.ih2[2] * az;
-    return tc + kOmega * (__ldcg(L.r + c) - At) / level_diag(i, j, k, L.nx, L.ny, L.nz, L.ih2);
+    return tc + (L.r[c] - At) * wdiag(i, j, k, L.nx, L.ny, L.nz, L.ih2);
 }
 
 // Restriction gather: kRestrictScale x sum over the fine cells whose prolongation uses coarse (I, J, K)
@@ -280,7 +288,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                         const int qi = ci + (q == c - 1 ? -1 : q == c + 1 ? 1 : 0);
                         const int qj = cj + (q == c - nx ? -1 : q == c + nx ? 1 : 0);
                         const int qk = ck + (q == c - sxy ? -1 : q == c + sxy ? 1 : 0);
-                        return kOmega * (r[q] - alpha * Q[q]) / level_diag(qi, qj, qk, nx, ny, nz, ih2);
+                        return (r[q] - alpha * Q[q]) * wdiag(qi, qj, qk, nx, ny, nz, ih2);
                     };
                     const float rc = r[c] - alpha * Q[c];
                     const float Az1 = apply_row(st0, c, ent & 63u, z1);
@@ -302,8 +310,8 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                 for (int t = tid; t < ncells; t += T) {
                     const int I = t % C.nx, J = (t / C.nx) % C.ny, K = t / (C.nx * C.ny);
                     float val = 0.f;
-                    if (__ldcg(C.mask + t))
-                        val = restrict_at(I, J, K, C, nx, ny, nz, [&](size_t q) { return __ldcg(RES + q); });
+                    if (C.mask[t])
+                        val = restrict_at(I, J, K, C, nx, ny, nz, [&](size_t q) { return RES[q]; });
                     C.r[t] = val;
                 }
                 if (!grid_sync(w, gen, nblk, sh, blk)) return;
@@ -325,8 +333,8 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                 for (int t = t0; t < ncells; t += stride) {
                     const int I = t % C.nx, J = (t / C.nx) % C.ny, K = t / (C.nx * C.ny);
                     float val = 0.f;
-                    if (__ldcg(C.mask + t))
-                        val = restrict_at(I, J, K, C, Fl.nx, Fl.ny, Fl.nz, [&](size_t q) { return __ldcg(Fl.t + q); });
+                    if (C.mask[t])
+                        val = restrict_at(I, J, K, C, Fl.nx, Fl.ny, Fl.nz, [&](size_t q) { return Fl.t[q]; });
                     C.r[t] = val;
                 }
                 return sync();
@@ -338,8 +346,8 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                 for (int t = t0; t < nf; t += stride) {
                     const int i = t % Fl.nx, j = (t / Fl.nx) % Fl.ny, k = t / (Fl.nx * Fl.ny);
                     float val = 0.f;
-                    if (__ldcg(Fl.mask + t))
-                        val = kOmega * __ldcg(Fl.r + t) / level_diag(i, j, k, Fl.nx, Fl.ny, Fl.nz, Fl.ih2) +
+                    if (Fl.mask[t])
+                        val = Fl.r[t] * wdiag(i, j, k, Fl.nx, Fl.ny, Fl.nz, Fl.ih2) +
                               prolong_at(C, i, j, k);
                     Fl.t[t] = val;
                 }
@@ -367,9 +375,9 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                 // right-hand side, omega / diagonal (0 outside the mask) and neighbour bits, once
                 for (int t = threadIdx.x; t < ncells; t += blockDim.x) {
                     const int I = t % C.nx, J = (t / C.nx) % C.ny, K = t / (C.nx * C.ny);
-                    const bool in = __ldcg(C.mask + t) != 0;
-                    s_cr[t] = in ? __ldcg(C.r + t) : 0.f;
-                    s_cw[t] = in ? kOmega / level_diag(I, J, K, C.nx, C.ny, C.nz, C.ih2) : 0.f;
+                    const bool in = C.mask[t] != 0;
+                    s_cr[t] = in ? C.r[t] : 0.f;
+                    s_cw[t] = in ? wdiag(I, J, K, C.nx, C.ny, C.nz, C.ih2) : 0.f;
                     s_cb[t] = (I > 0 ? 1u : 0u) | (I + 1 < C.nx ? 2u : 0u) | (J > 0 ? 4u : 0u) | (J + 1 < C.ny ? 8u : 0u) |
                               (K > 0 ? 16u : 0u) | (K + 1 < C.nz ? 32u : 0u);
                     s_cz[0][t] = 0.f;
@@ -410,7 +418,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                 for (int e = tid, k = 0; e < F; e += T, ++k) {
                     const int c = (int)(entry(k, e) >> 6);
                     const int i = c % nx, j = (c / nx) % ny, kk = c / sxy;
-                    RES[c] = kOmega * r[c] / level_diag(i, j, kk, nx, ny, nz, ih2) + prolong_at(C, i, j, kk);
+                    RES[c] = r[c] * wdiag(i, j, kk, nx, ny, nz, ih2) + prolong_at(C, i, j, kk);
                 }
                 if (!grid_sync(w, gen, nblk, sh, blk)) return;
                 double acc[1] = {0.0};
@@ -418,8 +426,8 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
                     const uint32_t ent = entry(k, e);
                     const int c = (int)(ent >> 6);
                     const int i = c % nx, j = (c / nx) % ny, kk = c / sxy;
-                    const float At = apply_row(st0, c, ent & 63u, [&](int q) { return __ldcg(RES + q); });
-                    const float zc = __ldcg(RES + c) + kOmega * (r[c] - At) / level_diag(i, j, kk, nx, ny, nz, ih2);
+                    const float At = apply_row(st0, c, ent & 63u, [&](int q) { return RES[q]; });
+                    const float zc = RES[c] + (r[c] - At) * wdiag(i, j, kk, nx, ny, nz, ih2);
                     Z[c] = zc;
                     acc[0] += (double)r[c] * (double)zc;
                 }
