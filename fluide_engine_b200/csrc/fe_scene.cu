@@ -115,7 +115,7 @@ struct fe_scene {
     MgWork mg{};                       // multigrid levels (levels >= 2) once the multigrid solver was wanted
     bool use_mg = false;               // solve with the multigrid-preconditioned CG (if the grid has a hierarchy)
     double* pprev_buf = nullptr;       // pressure of the substep before the last (time-extrapolated warm start)
-    int mg_block_cells = 4096;         // multigrid levels of at most this many cells run in one block
+    int mg_block_cells = 2048;         // multigrid levels of at most this many cells run in one block
     DiffWork diff{};                   // viscosity buffers (allocated once the viscosity is > 0)
     bool diff_ready = false;
     // Surface extraction (fe_surface.cu), allocated on first use: node distances and SDF values, per-item case
