@@ -68,13 +68,19 @@ class Server:
     """
 
     def __init__(self, hbm_budget_bytes, max_batch=32, device=0, cg_rel_tol=1e-6, seed_threads=4,
-                 reuse_scenes=True, overlap=False):
+                 reuse_scenes=True, overlap=False, batch_family=None):
         self.budget = int(hbm_budget_bytes)
         self.max_batch = min(int(max_batch), 64)
         self.device = device
         self.cg_rel_tol = cg_rel_tol
         self.reuse_scenes = reuse_scenes
         self.overlap = overlap   # batch overlap mode (each job's substep on its own stream, see Batch.set_overlap)
+        # solver family of the jobs' scenes inside the batches: None keeps each scene's own choice (the automatic
+        # one, or the autotuner's for its grid), "cg" runs the plain CG body for every job (the multi-scene solve
+        # overlaps the scenes' barrier latency, which is what the multigrid solver saves a lone scene)
+        if batch_family not in (None, "cg"):
+            raise ValueError("batch_family is None or 'cg'")
+        self.batch_family = batch_family
         self.seed_threads = max(1, int(seed_threads))
         self.used = 0            # bytes of live scenes (running, pooled, being prepared or released)
         self.reserved = 0        # bytes reserved for preparations that need a new scene
@@ -153,6 +159,8 @@ class Server:
             nbytes = need
             scene = Scene((job.n,) * 3, solver=job.solver, max_cfl=1.0, cg_rel_tol=self.cg_rel_tol,
                           device=self.device)
+        if self.batch_family == "cg":
+            scene.set_tuning(multigrid=0)
         pos, vel = job.seeded
         scene.set_particles(pos, vel)
         job.scene = scene

@@ -12,6 +12,7 @@ from fluide_engine_b200 import serving
 class FakeScene:
     live = 0
     created = 0
+    tunings = []
 
     def __init__(self, n, solver=0, max_cfl=1.0, cg_rel_tol=1e-6, device=0):
         self.n, self.solver = n, solver
@@ -29,6 +30,9 @@ class FakeScene:
 
     def reset(self):
         self.resets += 1
+
+    def set_tuning(self, **kw):
+        FakeScene.tunings.append(kw)
 
     def particles(self):
         return self.pos + self.steps, np.full_like(self.pos, self.steps), np.zeros((self.np, 9), np.float32)
@@ -73,6 +77,7 @@ def stand_ins(monkeypatch):
     monkeypatch.setattr(serving._abi, "seed_regions", fake_seed)
     FakeScene.live = 0
     FakeScene.created = 0
+    FakeScene.tunings = []
 
 
 def jobs(k, n=16, frames=3, spacing=0.0, nsub=2):
@@ -181,3 +186,16 @@ def test_cancelled_jobs_leave_and_release_their_memory():
         assert np.all(j.final[1] == j.frames * j.substeps_per_frame)
     assert sum(1 in f for f in frames) == 2
     assert FakeScene.live == 0 and srv.used == 0
+
+
+def test_batch_family_cg_puts_every_job_on_the_plain_solver():
+    js = jobs(5, n=(16, 24), spacing=0.001)
+    srv = serving.Server(hbm_budget_bytes=1 << 40, max_batch=3, batch_family="cg")
+    for j in js:
+        srv.submit(j)
+    srv.run()
+    assert len(srv.done) == 5
+    # every job's scene (new or reused from the pool) was put on the plain CG before it joined a batch
+    assert FakeScene.tunings == [{"multigrid": 0}] * 5
+    with pytest.raises(ValueError):
+        serving.Server(hbm_budget_bytes=1 << 40, batch_family="mg")
