@@ -141,6 +141,25 @@ __host__ __device__ constexpr uint32_t rep_bits(int width, int count)
     return count <= 0 ? 0u : (rep_bits(width, count - 1) << width) | 1u;
 }
 
+// Touched slots of the window from each axis' touched bits (tx over W0, ty over W1, tz over W2): slot (a, b, c)
+// is touched when bit a of tx, b of ty and c of tz are, found by spreading each axis' bits over the slot layout.
+template <int C>
+__host__ __device__ constexpr uint32_t spread_mask(uint32_t tx, uint32_t ty, uint32_t tz)
+{
+    constexpr int W0 = win<C>(0), W1 = win<C>(1), W2 = win<C>(2);
+    uint32_t sy = 0, ez = 0;
+    for (int b3 = 0; b3 < W1; ++b3) sy |= ((ty >> b3) & 1u) * (((1u << W0) - 1u) << (W0 * b3));
+    for (int c3 = 0; c3 < W2; ++c3) ez |= ((tz >> c3) & 1u) * (((1u << (W0 * W1)) - 1u) << (W0 * W1 * c3));
+    return (tx * rep_bits(W0, W1 * W2)) & (sy * rep_bits(W0 * W1, W2)) & ez;
+}
+// Touched slots of an unclamped particle in the lower half of the cell on every transverse axis (the first two
+// faces of each axis); the upper halves shift it by one face per axis.
+template <int C>
+__host__ __device__ constexpr uint32_t regular_mask()
+{
+    return spread_mask<C>(3u, 3u, 3u);
+}
+
 // One particle of cell (cx, cy, cz) into the cell's 18 slots of component C; returns false (and adds nothing)
 // when its stencil leaves the window, in which case the caller takes the direct path.  The trilinear weight of
 // slot (i, j, k) is wx_i wy_j wz_k, so the sums are formed as wx_i (wy_j wz_k v) per (j, k) pair: 2 FMAs per slot
@@ -154,33 +173,53 @@ __device__ __forceinline__ bool splat_slots(const SceneView& v, const P2gComp& k
     constexpr int L0 = wlo<C>(0), L1 = wlo<C>(1), L2 = wlo<C>(2);
     const int oi = s.i - cx, oip = s.ip - cx, oj = s.j - cy, ojp = s.jp - cy, ok = s.k - cz, okp = s.kp - cz;
     if (oi < L0 || oip > L0 + W0 - 1 || oj < L1 || ojp > L1 + W1 - 1 || ok < L2 || okp > L2 + W2 - 1) return false;
-    // 1D weights and touched bits on the window (i and ip coincide only on a one-face axis)
     float wx[W0], wy[W1], wz[W2];
-    uint32_t tx = 0, ty = 0, tz = 0;
+    // The usual case: no clamp on any axis, so the stencil is the cell's two own-axis faces and, on each transverse
+    // axis, the lower or the upper two of the window's three faces (the half of the cell the particle is in).  The
+    // weights are then selects of (1 - f, f), the same values the general sums below give, and the touched slots a
+    // fixed pattern shifted by those halves.
+    auto axis_regular = [](int o, int op, int W, int lo) { return op == o + 1 && (o == lo || (W == 3 && o == lo + 1)); };
+    const bool regular = axis_regular(oi, oip, W0, L0) && axis_regular(oj, ojp, W1, L1) && axis_regular(ok, okp, W2, L2);
+    if (regular) {
+        const bool hx = W0 == 3 && oi == L0 + 1;
+        const bool hy = W1 == 3 && oj == L1 + 1;
+        const bool hz = W2 == 3 && ok == L2 + 1;
+        const float f[3] = {s.fx, s.fy, s.fz};
+        const bool h[3] = {hx, hy, hz};
 #pragma unroll
-    for (int r = 0; r < W0; ++r) {
-        wx[r] = (oi == L0 + r ? 1.f - s.fx : 0.f) + (oip == L0 + r ? s.fx : 0.f);
-        tx |= (oi == L0 + r || oip == L0 + r) ? 1u << r : 0u;
-    }
+        for (int a = 0; a < 3; ++a) {
+            const int W = a == 0 ? W0 : (a == 1 ? W1 : W2);
+            float* w = a == 0 ? wx : (a == 1 ? wy : wz);
+            const float lo = 1.f - f[a];
+            if (W == 2) {
+                w[0] = lo;
+                w[1] = f[a];
+            } else {
+                w[0] = h[a] ? 0.f : lo;
+                w[1] = h[a] ? lo : f[a];
+                w[2 % W] = h[a] ? f[a] : 0.f;
+            }
+        }
+        mask |= regular_mask<C>() << ((hx ? 1 : 0) + W0 * ((hy ? 1 : 0) + W1 * (hz ? 1 : 0)));
+    } else {
+        // 1D weights and touched bits on the window (i and ip coincide only on a one-face axis)
+        uint32_t tx = 0, ty = 0, tz = 0;
 #pragma unroll
-    for (int r = 0; r < W1; ++r) {
-        wy[r] = (oj == L1 + r ? 1.f - s.fy : 0.f) + (ojp == L1 + r ? s.fy : 0.f);
-        ty |= (oj == L1 + r || ojp == L1 + r) ? 1u << r : 0u;
-    }
+        for (int r = 0; r < W0; ++r) {
+            wx[r] = (oi == L0 + r ? 1.f - s.fx : 0.f) + (oip == L0 + r ? s.fx : 0.f);
+            tx |= (oi == L0 + r || oip == L0 + r) ? 1u << r : 0u;
+        }
 #pragma unroll
-    for (int r = 0; r < W2; ++r) {
-        wz[r] = (ok == L2 + r ? 1.f - s.fz : 0.f) + (okp == L2 + r ? s.fz : 0.f);
-        tz |= (ok == L2 + r || okp == L2 + r) ? 1u << r : 0u;
-    }
-    // touched slots: tx[a] & ty[b] & tz[c] over the window, by spreading each axis' bits over the slot layout
-    {
-        const uint32_t ex = tx * rep_bits(W0, W1 * W2);
-        uint32_t sy = 0, ez = 0;
+        for (int r = 0; r < W1; ++r) {
+            wy[r] = (oj == L1 + r ? 1.f - s.fy : 0.f) + (ojp == L1 + r ? s.fy : 0.f);
+            ty |= (oj == L1 + r || ojp == L1 + r) ? 1u << r : 0u;
+        }
 #pragma unroll
-        for (int b3 = 0; b3 < W1; ++b3) sy |= ((ty >> b3) & 1u) * (((1u << W0) - 1u) << (W0 * b3));
-#pragma unroll
-        for (int c3 = 0; c3 < W2; ++c3) ez |= ((tz >> c3) & 1u) * (((1u << (W0 * W1)) - 1u) << (W0 * W1 * c3));
-        mask |= ex & (sy * rep_bits(W0 * W1, W2)) & ez;
+        for (int r = 0; r < W2; ++r) {
+            wz[r] = (ok == L2 + r ? 1.f - s.fz : 0.f) + (okp == L2 + r ? s.fz : 0.f);
+            tz |= (ok == L2 + r || okp == L2 + r) ? 1u << r : 0u;
+        }
+        mask |= spread_mask<C>(tx, ty, tz);
     }
     float gx[W0];  // APIC: wx_i C_x (x_face_i - x_p)
     float dy[W1], dz[W2];
