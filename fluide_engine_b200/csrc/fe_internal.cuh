@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "../../include/fluide_b200.h"
@@ -19,6 +20,16 @@
 namespace fe {
 
 constexpr int kMaxRefineDefault = 12;
+
+// NVTX range for the lifetime of the object: each public call (a step, a substep and its phases, a batch step,
+// the autotuner, checkpoints, particle transfers, surface extraction) shows as a named range in an NVTX-aware
+// profiler; without one attached the push and pop do nothing.
+struct TraceRange {
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+};
 constexpr int kMaxCgBlocks = 4096;  // solver blocks one scene can be given (sizes its partial-sum buffer)
 // Grid-barrier words of one solver: [0] arrivals of the current launch, [2] statistics counter (kept across
 // launches), [32] blocks that have left the current launch (its own 128-byte line).

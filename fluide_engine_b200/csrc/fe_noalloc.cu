@@ -131,6 +131,7 @@ extern "C" fe_status fe_project_noalloc(const int32_t n[3], const double h[3], c
                                         float* v, float* w, double* p, double rel_tol, int32_t max_it,
                                         void* stream, fe_step_stats* stats)
 {
+    TraceRange trace("fe_project_noalloc");
     if (!n || !h || !marks || !u || !v || !w || !p) return set_error(FE_ERR_BAD_ARG, "null argument");
     for (int a = 0; a < 3; ++a) {
         if (n[a] < 2) return set_error(FE_ERR_BAD_ARG, "grid size must be >= 2 per axis");

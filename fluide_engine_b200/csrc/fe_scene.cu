@@ -774,6 +774,7 @@ fe_status enqueue_stages(fe_scene* s, double dt, int first_stage, int last_stage
 // The three phases a substep graph is split into: everything before the solve, the solve, the rest.
 const int kPhaseFirst[3] = {kStepSort, kStepCg, kStepApply};
 const int kPhaseLast[3] = {kStepRhs, kStepCg, kStepMove};
+const char* const kPhaseName[3] = {"pre-solve", "pressure solve", "post-solve"};
 
 fe_status check_device_error(fe_scene* s)
 {
@@ -864,6 +865,7 @@ fe_status emit_particles(fe_scene* s);
 
 fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
 {
+    TraceRange trace("substep");
     s->last_substep_empty = false;
     if (!s->emitters.empty()) {
         // emitters change the particle count every substep: direct launches, no graphs
@@ -881,6 +883,7 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
         }
         s->last_substep_empty = false;
         for (int ph = 0; ph < 3; ++ph) {
+            TraceRange phase(kPhaseName[ph]);
             if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
             st = enqueue_steps(s, dt, kPhaseFirst[ph], kPhaseLast[ph]);
             if (st != FE_OK) return st;
@@ -906,6 +909,7 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
     }
     if (s->graphs_disabled) {
         for (int ph = 0; ph < 3; ++ph) {
+            TraceRange phase(kPhaseName[ph]);
             if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
             fe_status st = enqueue_steps(s, dt, kPhaseFirst[ph], kPhaseLast[ph]);
             if (st != FE_OK) return st;
@@ -928,6 +932,7 @@ fe_status run_substep(fe_scene* s, double dt, cudaEvent_t* ev)
         g_launches += s->whole_kernels[par];
     } else {
         for (int ph = 0; ph < 3; ++ph) {
+            TraceRange phase(kPhaseName[ph]);
             if (ev) FE_CUDA(cudaEventRecord(ev[ph], s->stream));
             FE_CUDA(cudaGraphLaunch(s->graph[par][ph], s->stream));
             g_launches += s->graph_kernels[par][ph];
@@ -1247,6 +1252,7 @@ fe_status fe_scene_destroy(fe_scene* s)
 
 fe_status fe_scene_set_particles(fe_scene* s, const float* pos, const float* vel, const float* C, uint64_t n)
 {
+    TraceRange trace("fe_scene_set_particles");
     if (!s || (!pos && n)) return set_error(FE_ERR_BAD_ARG, "null argument");
     if (n >= (1ull << 32) - 1) return set_error(FE_ERR_BAD_ARG, "at most 2^32-2 particles per scene");
     std::lock_guard<std::mutex> lk(s->mu);
@@ -1321,6 +1327,7 @@ fe_status fe_scene_reset(fe_scene* s)
 
 fe_status fe_scene_get_particles(fe_scene* s, float* pos, float* vel, float* C, uint64_t n)
 {
+    TraceRange trace("fe_scene_get_particles");
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
     std::lock_guard<std::mutex> lk(s->mu);
     if (n != s->base.np) return set_error(FE_ERR_BAD_ARG, "particle count mismatch (%llu vs %llu)",
@@ -1355,6 +1362,7 @@ fe_status fe_scene_num_particles(const fe_scene* s, uint64_t* n)
 
 fe_status fe_scene_step(fe_scene* s, double dt, int32_t nsub, fe_step_stats* stats)
 {
+    TraceRange trace("fe_scene_step");
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
     if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
     if (!s->have_particles && s->emitters.empty()) return set_error(FE_ERR_STATE, "set particles before stepping");
@@ -1399,6 +1407,7 @@ fe_status fe_scene_step(fe_scene* s, double dt, int32_t nsub, fe_step_stats* sta
 
 fe_status fe_scene_step_profiled(fe_scene* s, double dt, int32_t nsub, fe_step_stats* stats, float* phase_ms)
 {
+    TraceRange trace("fe_scene_step_profiled");
     if (!s || !phase_ms) return set_error(FE_ERR_BAD_ARG, "null argument");
     if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
     if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles before stepping");
@@ -1446,6 +1455,7 @@ fe_status fe_scene_cfl(fe_scene* s, double dt, double* cfl)
 
 fe_status fe_scene_advance_frame(fe_scene* s, double frame_dt, int32_t* substeps)
 {
+    TraceRange trace("fe_scene_advance_frame");
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
     if (!(frame_dt > 0.0)) return set_error(FE_ERR_BAD_ARG, "frame_dt must be > 0");
     if (!s->have_particles && s->emitters.empty()) return set_error(FE_ERR_STATE, "set particles before stepping");
@@ -2065,6 +2075,7 @@ fe_status fe_scene_clear_emitters(fe_scene* s)
 
 fe_status fe_scene_build_surface(fe_scene* s, uint64_t* n_vertices, uint64_t* n_triangles)
 {
+    TraceRange trace("fe_scene_build_surface");
     if (!s) return set_error(FE_ERR_BAD_ARG, "null scene");
     if (!s->have_particles) return set_error(FE_ERR_STATE, "set particles first");
     std::lock_guard<std::mutex> lk(s->mu);
@@ -2242,6 +2253,7 @@ extern "C" {
 
 fe_status fe_scene_snapshot(fe_scene* s, fe_snapshot** out)
 {
+    TraceRange trace("fe_scene_snapshot");
     if (!s || !out) return set_error(FE_ERR_BAD_ARG, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
     FE_CUDA(cudaSetDevice(s->device));
@@ -2301,6 +2313,7 @@ fe_status fe_scene_snapshot(fe_scene* s, fe_snapshot** out)
 
 fe_status fe_scene_restore(fe_scene* s, const fe_snapshot* sn)
 {
+    TraceRange trace("fe_scene_restore");
     if (!s || !sn) return set_error(FE_ERR_BAD_ARG, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
     const SceneView& b0 = s->base;
@@ -2413,6 +2426,7 @@ fe_status fe_tuning_lookup(int32_t device, const int32_t n[3], int32_t solver, f
 
 fe_status fe_scene_autotune(fe_scene* s, double dt, int32_t substeps, int32_t scope, fe_tuning* best, float* best_ms)
 {
+    TraceRange trace("fe_scene_autotune");
     if (!s || !(dt > 0.0) || substeps < 1 || scope < FE_TUNE_ALL || scope > FE_TUNE_SHAPE)
         return set_error(FE_ERR_BAD_ARG, "bad autotune arguments");
     if (!s->have_particles || s->base.np == 0) return set_error(FE_ERR_STATE, "autotune needs particles");
@@ -2966,6 +2980,7 @@ fe_status fe_batch_destroy(fe_batch* b)
 
 fe_status fe_batch_step_profiled(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats, float* phase_ms)
 {
+    TraceRange trace("fe_batch_step_profiled");
     if (!b || !phase_ms) return set_error(FE_ERR_BAD_ARG, "null argument");
     if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
     const int S = (int)b->scenes.size();
@@ -3005,6 +3020,7 @@ fe_status fe_batch_step_profiled(fe_batch* b, double dt, int32_t nsub, fe_step_s
 
 fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats)
 {
+    TraceRange trace("fe_batch_step");
     if (!b) return set_error(FE_ERR_BAD_ARG, "null batch");
     if (!(dt > 0.0) || nsub < 0) return set_error(FE_ERR_BAD_ARG, "dt must be > 0 and nsub >= 0");
     const int S = (int)b->scenes.size();
