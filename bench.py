@@ -413,6 +413,7 @@ def run_pool(args):
     N = pos.shape[0]
     dt = 1.0 / 480.0
     scene = fe.Scene((n, n, n), solver=fe.APIC, max_cfl=1.0, cg_rel_tol=1e-8, cg_max_it=4000, max_refine=24,
+                     cg_inner_tol=args.cg_inner_tol,
                      pressure_solver={"auto": fe.AUTO, "mgpcg": fe.MGPCG, "cg": fe.CG}[args.pressure_solver])
     stream = torch.cuda.Stream()
     scene.set_stream(stream.cuda_stream)
@@ -768,7 +769,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="single workload: keep the default launch shape")
     ap.add_argument("--no-extras", action="store_true",
                     help="single workload: skip the accuracy-vs-oracle, batched and served objects of the line")
-    ap.add_argument("--cg-inner-tol", type=float, default=1e-4, help="inner FP32 CG residual reduction per refinement")
+    ap.add_argument("--cg-inner-tol", type=float, default=0.0,
+                    help="inner FP32 CG residual reduction per refinement (0: the solver's default)")
     ap.add_argument("--pressure-solver", default="auto", choices=["auto", "mgpcg", "cg"],
                     help="inner pressure solver: auto (multigrid-preconditioned CG from 2^19 cells, plain CG below), "
                          "mgpcg or cg")

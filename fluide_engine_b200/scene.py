@@ -25,7 +25,7 @@ class Scene:
     """Owns an fe_scene.  All arrays exchanged are numpy (host) unless a torch CUDA tensor is passed."""
 
     def __init__(self, n, solver=_abi.FLIP, origin=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0), flip_blend=0.05,
-                 gravity=(0.0, -9.81, 0.0), max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-4,
+                 gravity=(0.0, -9.81, 0.0), max_cfl=1.0, cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=0.0,
                  max_refine=12, device=0, max_particles=0, pressure_solver=_abi.AUTO, viscosity=0.0):
         L = _abi.lib()
         d = _abi.SceneDesc()

@@ -395,7 +395,7 @@ class HybridSimulator:
         self._currentFrame = Frame()
         self._currentTime = 0.0
         self._numberOfTimeSteps = 0
-        self._cg = dict(cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=1e-4, max_refine=12)
+        self._cg = dict(cg_rel_tol=1e-6, cg_max_it=2000, cg_inner_tol=0.0, max_refine=12)
         self.last_stats = []
 
     # settings -------------------------------------------------------------------------------------

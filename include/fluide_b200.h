@@ -50,7 +50,9 @@ typedef struct {
     double max_cfl;          /* extrapolation depth ceil(max_cfl), RK2 sub-steps max(max_cfl,1) */
     double cg_rel_tol;       /* stop when ||b - A p||_2 <= cg_rel_tol * ||b||_2 (FP64 test) */
     int32_t cg_max_it;       /* cap on inner FP32 CG iterations per pressure solve */
-    double cg_inner_tol;     /* relative residual reduction asked of each FP32 inner solve */
+    double cg_inner_tol;     /* relative residual reduction asked of each FP32 inner solve; 0 (default): 1e-4 for the
+                                plain CG; for the multigrid-preconditioned CG cg_rel_tol split evenly over the fewest
+                                refinements that 1e-4 per inner solve allows (1e-3 at 1e-6, 1e-4 at 1e-8) */
     int32_t max_refine;      /* cap on FP64 outer refinement steps per pressure solve */
     int32_t device;          /* CUDA device ordinal */
     uint64_t max_particles;  /* capacity; 0 = sized by the first fe_scene_set_particles */
