@@ -81,17 +81,8 @@ __device__ __forceinline__ float prolong_at(const MgLevel& coarse, int i, int j,
     return 0.75f * x0 + 0.25f * x1;
 }
 
-// Weight of coarse index I in the prolongation to fine index i (per axis; the transpose gives the
-// restriction).
-__device__ __forceinline__ float pweight(int i, int I, int nc)
-{
-    int c0, c1;
-    prolong_axis(i, nc, c0, c1);
-    return (c0 == I ? 0.75f : 0.f) + (c1 == I ? 0.25f : 0.f);
-}
-
 // Level-l residual of the pre-smoothed correction, res = r - A (omega r / D), at cell (i, j, k) of a dense
-// level (0 outside the mask); r is 0 outside the mask.
+// level (0 outside the mask); r outside the mask (where the restriction scatter may have added) counts as 0.
 __device__ __forceinline__ float level_residual(const MgLevel& L, int i, int j, int k)
 {
     const size_t sx = (size_t)L.nx, sxy = (size_t)L.nx * L.ny;
@@ -99,7 +90,7 @@ __device__ __forceinline__ float level_residual(const MgLevel& L, int i, int j, 
     if (!L.mask[c]) return 0.f;
     auto z1 = [&](int a, int b, int d) {
         const size_t q = (size_t)a + sx * b + sxy * d;
-        return L.r[q] * wdiag(a, b, d, L.nx, L.ny, L.nz, L.ih2);
+        return L.mask[q] ? L.r[q] * wdiag(a, b, d, L.nx, L.ny, L.nz, L.ih2) : 0.f;
     };
     const float rc = L.r[c];
     const float zc = rc * wdiag(i, j, k, L.nx, L.ny, L.nz, L.ih2);
@@ -133,48 +124,13 @@ __device__ __forceinline__ float level_smooth(const MgLevel& L, int i, int j, in
     return tc + (L.r[c] - At) * wdiag(i, j, k, L.nx, L.ny, L.nz, L.ih2);
 }
 
-// Restriction gather: kRestrictScale x sum over the fine cells whose prolongation uses coarse (I, J, K)
-// (fine indices 2I-1 .. 2I+2 per axis) of weight x fine residual; `res(q)` gives the fine residual at linear
-// index q of the fine level.  The 4 x 4 x 4 window is fully unrolled with predicated loads, so the 64
-// loads are in flight together instead of one dependent round trip each.
-template <class Res>
-__device__ __forceinline__ float restrict_at(int I, int J, int K, const MgLevel& coarse, int fnx, int fny, int fnz,
-                                             Res res)
-{
-    float wx[4], wy[4], wz[4];
-    int ix[4], iy[4], iz[4];
-#pragma unroll
-    for (int d = 0; d < 4; ++d) {
-        ix[d] = 2 * I + d - 1;
-        iy[d] = 2 * J + d - 1;
-        iz[d] = 2 * K + d - 1;
-        wx[d] = (ix[d] >= 0 && ix[d] < fnx) ? pweight(ix[d], I, coarse.nx) : 0.f;
-        wy[d] = (iy[d] >= 0 && iy[d] < fny) ? pweight(iy[d], J, coarse.ny) : 0.f;
-        wz[d] = (iz[d] >= 0 && iz[d] < fnz) ? pweight(iz[d], K, coarse.nz) : 0.f;
-    }
-    const size_t sx = (size_t)fnx, sxy = (size_t)fnx * fny;
-    float acc = 0.f;
-#pragma unroll
-    for (int dk = 0; dk < 4; ++dk) {
-#pragma unroll
-        for (int dj = 0; dj < 4; ++dj) {
-            const float wjk = wz[dk] * wy[dj];
-#pragma unroll
-            for (int di = 0; di < 4; ++di) {
-                const float wgt = wjk * wx[di];
-                const float val = wgt != 0.f ? res((size_t)ix[di] + sx * (size_t)iy[dj] + sxy * (size_t)iz[dk]) : 0.f;
-                acc += wgt * val;
-            }
-        }
-    }
-    return kRestrictScale * acc;
-}
-
-// The same restriction as a scatter: fine cell (i, j, k) with residual `val` adds kRestrictScale x its
-// prolongation weight x val into every masked coarse cell whose prolongation reaches it (up to 2 per axis; the
-// parent twice at a wall, weight 1), with FP32 atomics into C.r, which must start at zero.  It lets the pass
-// that computes a level's residual restrict it too, without a barrier and a gather pass between them; each coarse
-// cell receives the terms of the gather above, summed in arrival order.
+// Restriction = kRestrictScale x the transpose of the prolongation, as a scatter: fine cell (i, j, k) with residual
+// `val` adds kRestrictScale x its prolongation weight x val into every coarse cell whose prolongation reaches it
+// (up to 2 per axis; the parent twice at a wall, weight 1), with FP32 atomics into C.r, which must start at zero.
+// It lets the pass that computes a level's residual restrict it too, without a barrier and a gather pass between
+// them (each coarse cell's sum is formed in arrival order).  Coarse cells outside the mask receive terms too (a
+// fine cell at the fluid's edge reaches a parent with no fluid child); every reader of C.r ignores it outside the
+// mask, so no mask load stands between the residual and its atomics.
 __device__ __forceinline__ void restrict_scatter(const MgLevel& C, int i, int j, int k, float val)
 {
     if (val == 0.f) return;
@@ -193,8 +149,7 @@ __device__ __forceinline__ void restrict_scatter(const MgLevel& C, int i, int j,
         const int a = d & 1, b = (d >> 1) & 1, e = d >> 2;
         const float wgt = wi[a] * wj[b] * wk[e];
         if (wgt == 0.f) continue;
-        const size_t q = (size_t)ii[a] + sx * (size_t)jj[b] + sxy * (size_t)kk[e];
-        if (C.mask[q]) atomicAdd(C.r + q, wgt * sv);
+        atomicAdd(C.r + (size_t)ii[a] + sx * (size_t)jj[b] + sxy * (size_t)kk[e], wgt * sv);
     }
 }
 

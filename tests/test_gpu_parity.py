@@ -311,3 +311,38 @@ def test_tuning_choices_reach_the_oracle(tuning):
     st = g.step(dt, 3)
     assert all(x["converged"] == 1 and x["rel_residual"] <= 1e-8 for x in st), st
     g.close()
+
+
+@pytest.mark.gpu
+def test_launch_shape_changes_between_solves_keep_the_barrier_state():
+    """The solvers' grid barrier counts arrivals over a whole launch and the last block to leave puts the count and
+    the reduction totals back to zero; consecutive solves of one scene with different block counts, block sizes,
+    clusters and solver families (each launch expects a different number of arrivals) must all start from a clean
+    state: every solve converges to the FP64 tolerance, and the final pressure matches the oracle's stage solve."""
+    n = (40, 40, 40)
+    g, o, *_ = make_scene_pair(n, fe.FLIP, seed=21, cg_rel_tol=1e-8, oracle_tol=1e-12)
+    dt = 1 / 240
+    shapes = [dict(multigrid=0, cg_block_threads=1024, cg_cluster=1),
+              dict(multigrid=0, cg_block_threads=256, cg_cluster=1),
+              dict(multigrid=1, cg_block_threads=512, mg_block_level_cells=2048, cg_cluster=1),
+              dict(multigrid=0, cg_block_threads=512, cg_cluster=2),
+              dict(multigrid=1, cg_block_threads=1024, mg_block_level_cells=4096, cg_cluster=1),
+              dict(multigrid=0, cg_block_threads=1024, cg_cluster=1)]
+    for shape in shapes:
+        g.set_tuning(**shape)
+        st = g.step(dt, 2)
+        assert all(x["converged"] == 1 and x["rel_residual"] <= 1e-8 for x in st), (shape, st)
+    # one more pressure stage against the oracle from the GPU's state
+    g.run_stages(dt, fe.STAGE_SORT, fe.STAGE_PRE)
+    P, V, _ = g.particles()
+    o.set_particles(P.astype(np.float64), V.astype(np.float64))
+    u, v, w, _, _ = g.grid()
+    for stg in ("p2g", "sdf"):
+        o.stage(stg)
+    o.set_grid(u.astype(np.float64), v.astype(np.float64), w.astype(np.float64))
+    g.run_stages(dt, fe.STAGE_PRESSURE, fe.STAGE_PRESSURE)
+    o.stage("pressure", dt)
+    _, _, _, pg, mg = g.grid()
+    assert np.array_equal(mg, o.marks())
+    assert rel_l2(pg, o.pressure()) < 1e-4
+    g.close()
