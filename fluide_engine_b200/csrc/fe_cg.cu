@@ -50,7 +50,7 @@ __device__ __forceinline__ void cg_body(SolverSmem& smem, const SceneView& v, co
     const int nx = v.g.nx, ny = v.g.ny;
     const int sxy = nx * ny;
     const int T = nblk * blockDim.x;
-    const int tid = blk * blockDim.x + threadIdx.x;
+    const int tid = solver_thread(blk, nblk);
     const double ih2d[3] = {v.inv_h[0] * v.inv_h[0], v.inv_h[1] * v.inv_h[1], v.inv_h[2] * v.inv_h[2]};
     Stencil7 st;
     st.sx = nx;

@@ -170,7 +170,7 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
     const int sxy = nx * ny;
     const int T = nblk * blockDim.x;
-    const int tid = blk * blockDim.x + threadIdx.x;
+    const int tid = solver_thread(blk, nblk);
     const uint8_t* __restrict__ marks = v.marks;
     const double ih2d[3] = {v.inv_h[0] * v.inv_h[0], v.inv_h[1] * v.inv_h[1], v.inv_h[2] * v.inv_h[2]};
     const float ih2[3] = {(float)ih2d[0], (float)ih2d[1], (float)ih2d[2]};

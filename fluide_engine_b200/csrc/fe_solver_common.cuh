@@ -289,6 +289,16 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[N], double* sh /* [kShDo
     return sh[kShFlag] == 0.0;
 }
 
+// Index of this thread among the nblk x blockDim.x threads of a solver for the loops over the FLUID list and the
+// multigrid levels (entry e = index + k x all threads): warps are interleaved across the blocks (warp j of block
+// blk is warp j nblk + blk), so a partial last round of the list spreads over every block instead of landing on
+// the first blocks -- at 128^3, 3.4 rounds per thread gave blocks 0..56 four rounds and the rest three -- while
+// each warp still takes 32 consecutive entries.
+__device__ __forceinline__ int solver_thread(int blk, int nblk)
+{
+    return (((int)(threadIdx.x >> 5) * nblk + blk) << 5) + (int)(threadIdx.x & 31);
+}
+
 // Block-wide sum of one double, valid in all threads (setup only).
 __device__ __forceinline__ double block_sum1(double x, double* sh)
 {
@@ -379,7 +389,7 @@ __device__ __forceinline__ bool solver_setup(const SceneView& v, const CgWork& w
     const int sxy = nx * ny;
     const int nc = sxy * nz;
     const int T = nblk * blockDim.x;
-    const int tid = blk * blockDim.x + threadIdx.x;
+    const int tid = solver_thread(blk, nblk);
     const uint8_t* __restrict__ marks = v.marks;
     double* __restrict__ p64 = v.p;
     const double* __restrict__ b = v.b;
