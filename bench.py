@@ -136,7 +136,7 @@ def mg_coarse_cells(n):
 
 
 def uses_multigrid(n, pressure_solver):
-    return pressure_solver == "mgpcg" or (pressure_solver == "auto" and n ** 3 >= (1 << 19))
+    return pressure_solver == "mgpcg" or (pressure_solver == "auto" and n ** 3 >= (1 << 15))
 
 
 def solver_alg_bytes(fluid, its, refs, n, multigrid):
@@ -772,7 +772,7 @@ def main():
     ap.add_argument("--cg-inner-tol", type=float, default=0.0,
                     help="inner FP32 CG residual reduction per refinement (0: the solver's default)")
     ap.add_argument("--pressure-solver", default="auto", choices=["auto", "mgpcg", "cg"],
-                    help="inner pressure solver: auto (multigrid-preconditioned CG from 2^19 cells, plain CG below), "
+                    help="inner pressure solver: auto (multigrid-preconditioned CG from 2^15 cells, plain CG below), "
                          "mgpcg or cg")
     ap.add_argument("--workload", default="single", choices=["single", "batched", "served", "pool256"])
     ap.add_argument("--surface", action="store_true",

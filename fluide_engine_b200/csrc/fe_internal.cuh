@@ -268,10 +268,10 @@ cudaError_t set_solver_barrier_limits(unsigned long long spin_limit, unsigned ex
 // the largest axis is <= 8, and that last level is solved by one block.
 constexpr int kMaxMgLevels = 12;
 // FE_PRESSURE_AUTO picks the multigrid solver from this many grid cells on.  Measured on B200 over whole
-// 240-substep dam-break runs (ms per solve, plain / multigrid): 48^3 0.77 / 0.91, 64^3 1.00 / 0.99, 96^3
-// 1.86 / 1.77, 128^3 3.58 / 2.56; at 256^3 the multigrid one wins by 6x (the plain CG streams its vectors from
-// HBM about 1,000 times per solve).
-constexpr size_t kMgAutoCells = (size_t)1 << 19;
+// 240-substep dam-break runs (ms per solve, plain / multigrid): 24^3 0.36 / 0.39, 32^3 0.46 / 0.39, 40^3 0.55 /
+// 0.52, 48^3 0.64 / 0.63, 64^3 0.85 / 0.67, 96^3 - / 1.27, 128^3 3.24 / 1.91; at 256^3 the multigrid one wins by
+// 8x (the plain CG streams its vectors from HBM about 1,000 times per solve).
+constexpr size_t kMgAutoCells = (size_t)1 << 15;
 struct MgLevel {
     int nx, ny, nz;
     float ih2[3];      // 1 / h_l^2 per axis, h_l = 2^l h

@@ -11,7 +11,7 @@
 // Hierarchy: level l >= 1 halves every axis of level l-1 (rounding up) until the largest axis is <= 8;
 // a coarse cell holds fluid when any child does; the operator of level l is the same 7-point matrix on the
 // coarse cells with spacing 2^l h (AIR neighbours Dirichlet 0, walls Neumann).
-// V-cycle (symmetric, so the preconditioner is SPD): one damped-Jacobi sweep (omega = 2/3) down, starting
+// V-cycle (symmetric, so the preconditioner is SPD): one damped-Jacobi sweep (omega = kOmega) down, starting
 // from zero (z1 = omega r / D, pointwise, never stored: recomputed wherever a pass needs it); residual;
 // restriction = kRestrictScale x the transpose of the prolongation; the coarsest level gets kCoarseSweeps
 // Jacobi sweeps from zero in one block's shared memory; up: z = z1 + P z_coarse, then one Jacobi sweep.
@@ -35,7 +35,14 @@
 namespace fe {
 namespace {
 
-constexpr float kOmega = 2.0f / 3.0f;
+// Jacobi damping of the smoother.  The iteration matrix I - omega D^-1 A contracts for omega < 1 on these M-matrices
+// (Gershgorin: D^-1 A has its spectrum in [0, 2]), which keeps the V-cycle symmetric positive definite.  Swept over
+// the 240-substep 128^3 dam break (inner iterations, ms per solve): 0.6 27.0 / 2.25, 2/3 26.0 / 2.17, 0.75 24.2 /
+// 2.03, 0.8 23.7 / 1.99, 0.85 23.0 / 1.93, 0.9 22.6 / 1.91, 0.95 25.2 / 2.11; 0.9 was also the faster of 0.85 / 0.9
+// at 48^3, 64^3, 96^3 and on the 256^3 APIC pool to 1e-8.
+constexpr float kOmega = 0.9f;
+// Scale of the restriction (the transpose of the trilinear prolongation): 0.0875 / 0.1 / 0.125 gave 25.2 / 26.0 /
+// 28.5 inner iterations at omega 2/3 and 22.6 / 22.6 / - at 0.9 on the same run.
 constexpr float kRestrictScale = 0.1f;
 // Jacobi sweeps from zero on the coarsest level.  Measured over the 240-substep 128^3 dam break (inner iterations,
 // ms per solve): 4 sweeps 26.8 / 2.20, 8 25.8 / 2.15, 11 25.8 / 2.16, 15 25.6 / 2.17, 20 25.6 / 2.20, 30 26.0 / 2.28,

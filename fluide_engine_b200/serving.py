@@ -85,6 +85,7 @@ class Server:
         self.used = 0            # bytes of live scenes (running, pooled, being prepared or released)
         self.reserved = 0        # bytes reserved for preparations that need a new scene
         self._releasing = 0      # finished jobs whose read-back / release is still queued
+        self._releasing_shapes = collections.Counter()  # (n, solver) of those jobs: scenes about to enter the pool
         self.waiting = []        # heap of (arrival, job_id, job)
         self.running = []
         self.preparing = []
@@ -179,11 +180,13 @@ class Server:
             with self._lock:
                 self.pool[(job.n, job.solver, id(scene))] = (scene, job.bytes)
                 self._releasing -= 1
+                self._releasing_shapes[(job.n, job.solver)] -= 1
         else:
             scene.close()
             with self._lock:
                 self.used -= job.bytes
                 self._releasing -= 1
+                self._releasing_shapes[(job.n, job.solver)] -= 1
         self.timing["retire"] += time.perf_counter() - t
 
     def _admit(self, now, io):
@@ -206,6 +209,11 @@ class Server:
             pos, _ = job.seeded
             need = scene_bytes(job.n, pos.shape[0], job.solver)
             claimed = self._claim_pooled(job.n, job.solver) if self.reuse_scenes else None
+            if claimed is None and self.reuse_scenes:
+                with self._lock:
+                    coming = self._releasing_shapes[(job.n, job.solver)] > 0
+                if coming:
+                    break  # a scene of this shape is being read back and pooled: take it once it is there
             if claimed is None:
                 if not self._evict_for(need):
                     if not (self.running or self.preparing or self._releasing):
@@ -279,6 +287,7 @@ class Server:
                         for j in finished:
                             with self._lock:
                                 self._releasing += 1
+                                self._releasing_shapes[(j.n, j.solver)] += 1
                             releases.append(io.submit(self._release_job, j, done_at))
                             self.done.append(j)
                 with self._lock:
@@ -300,6 +309,7 @@ class Server:
                         for j in leaving:
                             with self._lock:
                                 self._releasing += 1
+                                self._releasing_shapes[(j.n, j.solver)] += 1
                             releases.append(io.submit(self._release_job, j, done_at, False))
                     gone += leaving
                     for j in gone:

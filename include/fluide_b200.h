@@ -65,7 +65,7 @@ typedef struct {
  * refinement; they differ in how many inner iterations that takes.  The reference uses unpreconditioned CG
  * (linear_system/conjugate_gradient_solver.cpp:14-55). */
 typedef enum {
-    FE_PRESSURE_AUTO = 0,    /* default: MGPCG for grids of 2^19 cells (about 81^3) or more, CG below (faster there) */
+    FE_PRESSURE_AUTO = 0,    /* default: MGPCG for grids of 2^15 cells (32^3) or more, CG below (faster there) */
     FE_PRESSURE_MGPCG = 1,   /* CG preconditioned by one multigrid V-cycle: 10-25 inner iterations, 4 L - 2 barriers each */
     FE_PRESSURE_CG = 2       /* unpreconditioned CG: one grid barrier per iteration, 130-1100 iterations */
 } fe_pressure_solver;
