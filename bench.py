@@ -488,9 +488,9 @@ def batched_measure(n_scenes=48, steps=50, warmup=5, device=0, batch_family=None
     Scenes: cubic grids drawn from {32,48,64,96,128}, a dam-break block with extents U[0.2,0.6] per axis,
     8 particles per cell, solver drawn from PIC / FLIP(0.95) / APIC (seed 2).  Both arms use the same
     pressure tolerance (rel 1e-6); times are wall clock around synchronised device work.  The one-at-a-time arm
-    runs every scene with the autotuner's choice for its kind; batch_family="cg" runs the batched arm's scenes on
-    the plain CG body inside the multi-scene solve (measured faster there for this set: 11.96 against 12.58 ms per
-    substep), None keeps the autotuner's choice in the batch too.  Returns a dict.
+    runs every scene with the autotuner's choice for its kind, and so does the batched arm by default;
+    batch_family="cg" runs the batched arm's scenes on the plain CG body inside the multi-scene solve instead (with
+    the current multigrid solver slower for this set: 12.29 against 11.31 ms per substep).  Returns a dict.
     """
     import numpy as np
     import torch
@@ -579,7 +579,7 @@ def run_batched(args):
     import torch
 
     torch.cuda.set_device(0)
-    b = batched_measure(args.scenes, args.steps, args.warmup, batch_family="cg")
+    b = batched_measure(args.scenes, args.steps, args.warmup)
     line = {"metric": METRIC, "value": b["value"], "unit": METRIC, "n_gpus": 1, "steps": b["steps"],
             "warmup": b["warmup"], "ms_per_step": b["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 refinement)",
@@ -914,7 +914,7 @@ def main():
             oracle64 = oracle_snapshot_report(64, 30, local)
         except Exception as ex:  # reported, never required
             oracle64 = {"error": str(ex)[:200]}
-    batched = batched_measure(48, 50, 5, local, batch_family="cg") if extras else None
+    batched = batched_measure(48, 50, 5, local) if extras else None
     served = None
     if extras:
         res = tuple(int(x) for x in args.trace_res.split(","))
