@@ -9,7 +9,7 @@
 // tolerance (both stop on the same FP64 residual test).
 //
 // Hierarchy: level l >= 1 halves every axis of level l-1 (rounding up) until the largest axis is <= 8;
-// a coarse cell holds fluid when any child does; the operator of level l is the same 7-point matrix on the
+// a coarse cell holds fluid when most of its children do (more than half of those inside the grid: 5 of 8); the operator of level l is the same 7-point matrix on the
 // coarse cells with spacing 2^l h (AIR neighbours Dirichlet 0, walls Neumann).
 // V-cycle (symmetric, so the preconditioner is SPD): one damped-Jacobi sweep (omega = kOmega) down, starting
 // from zero (z1 = omega r / D, pointwise, never stored: recomputed wherever a pass needs it); residual;
@@ -203,23 +203,29 @@ __device__ __forceinline__ void mg_body(SolverSmem& smem, const SceneView& v, co
     const double bnorm = su.bnorm;
     auto entry = [&](int k, int e) -> uint32_t { return k < kc ? s_list[k * blockDim.x + threadIdx.x] : list[e]; };
 
-    // coarse-level masks, finest first (level 1 from the cell marks)
+    // coarse-level masks, finest first (level 1 from the cell marks): a coarse cell is fluid when more than half of
+    // its children are.  Marking it fluid when any child is (a free surface moved outward by up to a coarse cell)
+    // models the fine operator poorly where the surface is thin and ragged; measured over the 240-substep 128^3 dam
+    // break, inner iterations with "at least k of 8 children": any 22.6, 2 21.0, 3 18.8, 4 17.2, 5 14.6, 6 14.9,
+    // 8 17.2 (ms per solve 1.91 / 1.78 / 1.61 / 1.48 / 1.28 / 1.30 / 1.47).  Masks, restriction and prolongation
+    // stay a transpose pair, so the V-cycle stays symmetric positive definite for any such choice.
     for (int l = 1; l < L; ++l) {
         const MgLevel& C = mg.lv[l];
         const MgLevel& Fl = mg.lv[l - 1];
         const int ncells = C.nx * C.ny * C.nz;
         for (int t = tid; t < ncells; t += T) {
             const int I = t % C.nx, J = (t / C.nx) % C.ny, K = t / (C.nx * C.ny);
-            uint8_t any = 0;
+            int fluid = 0, children = 0;
             for (int dk = 0; dk < 2; ++dk)
                 for (int dj = 0; dj < 2; ++dj)
                     for (int di = 0; di < 2; ++di) {
                         const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
                         if (i >= Fl.nx || j >= Fl.ny || k >= Fl.nz) continue;
                         const size_t f = (size_t)i + (size_t)Fl.nx * j + (size_t)Fl.nx * Fl.ny * k;
-                        any |= l == 1 ? (uint8_t)(marks[f] == FE_CELL_FLUID) : Fl.mask[f];
+                        fluid += l == 1 ? (marks[f] == FE_CELL_FLUID ? 1 : 0) : (Fl.mask[f] ? 1 : 0);
+                        ++children;
                     }
-            C.mask[t] = any;
+            C.mask[t] = 2 * fluid > children ? 1 : 0;
         }
         if (!grid_sync(w, gen, nblk, sh, blk)) return;
     }
