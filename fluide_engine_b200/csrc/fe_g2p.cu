@@ -27,14 +27,33 @@ struct G2PArgs {
 struct FaceSource {
     const float* g[6];          // u, v, w, su, sv, sw
     int sx[3], sy[3];           // face-array sizes of the components (x, y)
-    // the 8 corner values of array a at stencil st, in the reference's corner order (x fastest)
+    // Offset of corner (i, j, k) of component comp's stencil and the steps to its other corners (0 where the stencil
+    // is clamped onto one face): one 64-bit index, then 32-bit steps (a step spans at most one plane of faces).
+    __device__ __forceinline__ size_t corner_base(int comp, const Stencil& st, int& dx, int& dy, int& dz) const
+    {
+        dx = st.ip - st.i;
+        dy = (st.jp - st.j) * sx[comp];
+        dz = (st.kp - st.k) * sx[comp] * sy[comp];
+        return idx3(st.i, st.j, st.k, sx[comp], sy[comp]);
+    }
+    // the 8 corner values of array a from its base, in the reference's corner order (x fastest)
+    __device__ __forceinline__ void load8(int a, size_t base, int dx, int dy, int dz, float c[8]) const
+    {
+        const float* p = g[a] + base;
+        c[0] = __ldg(p);
+        c[1] = __ldg(p + dx);
+        c[2] = __ldg(p + dy);
+        c[3] = __ldg(p + dx + dy);
+        c[4] = __ldg(p + dz);
+        c[5] = __ldg(p + dx + dz);
+        c[6] = __ldg(p + dy + dz);
+        c[7] = __ldg(p + dx + dy + dz);
+    }
     __device__ __forceinline__ void corners(int a, const Stencil& st, float c[8]) const
     {
-        const int comp = a % 3;
-        const int ii[2] = {st.i, st.ip}, jj[2] = {st.j, st.jp}, kk[2] = {st.k, st.kp};
-        const float* gg = g[a];
-#pragma unroll
-        for (int t = 0; t < 8; ++t) c[t] = __ldg(gg + idx3(ii[t & 1], jj[(t >> 1) & 1], kk[t >> 2], sx[comp], sy[comp]));
+        int dx, dy, dz;
+        const size_t base = corner_base(a % 3, st, dx, dy, dz);
+        load8(a, base, dx, dy, dz, c);
     }
 };
 
@@ -67,8 +86,10 @@ __device__ __forceinline__ void sample_vel(const SceneView& v, const FaceSource&
 __device__ __forceinline__ float sample_diff(const FaceSource& fs, int comp, const Stencil& s, float* plain)
 {
     float a[8], b[8], d[8];
-    fs.corners(comp, s, a);
-    fs.corners(comp + 3, s, b);
+    int dx, dy, dz;
+    const size_t base = fs.corner_base(comp, s, dx, dy, dz);  // the grid and its snapshot share the layout
+    fs.load8(comp, base, dx, dy, dz, a);
+    fs.load8(comp + 3, base, dx, dy, dz, b);
 #pragma unroll
     for (int t = 0; t < 8; ++t) d[t] = a[t] - b[t];
     if (plain) *plain = lerp8(a, s);
@@ -212,7 +233,7 @@ __device__ __forceinline__ FaceSource global_source(const SceneView& v, const G2
 // gathers hit L1/L2.  (A variant staging each tile's faces in shared memory, 13^3 per array, measured slower:
 // 260 us against 183 us per launch at 128^3 FLIP.)
 template <int SOLVER, bool G2P, bool MOVE>
-__global__ void __launch_bounds__(256) k_g2p(SceneView v, G2PArgs g)
+__global__ void __launch_bounds__(256, 4) k_g2p(SceneView v, G2PArgs g)
 {
     const uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (p >= v.np) return;
