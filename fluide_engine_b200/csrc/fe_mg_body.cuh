@@ -80,13 +80,14 @@ __device__ __forceinline__ float prolong_at(const MgLevel& coarse, int i, int j,
     prolong_axis(i, coarse.nx, i0, i1);
     prolong_axis(j, coarse.ny, j0, j1);
     prolong_axis(k, coarse.nz, k0, k1);
-    const float* z = coarse.z;
-    const size_t sx = (size_t)coarse.nx, sxy = (size_t)coarse.nx * coarse.ny;
-    auto zz = [&](int a, int b, int c) { return z[(size_t)a + sx * (size_t)b + sxy * (size_t)c]; };
-    const float y00 = 0.75f * zz(i0, j0, k0) + 0.25f * zz(i1, j0, k0);
-    const float y10 = 0.75f * zz(i0, j1, k0) + 0.25f * zz(i1, j1, k0);
-    const float y01 = 0.75f * zz(i0, j0, k1) + 0.25f * zz(i1, j0, k1);
-    const float y11 = 0.75f * zz(i0, j1, k1) + 0.25f * zz(i1, j1, k1);
+    // one 64-bit index for the parent, 32-bit steps (-1, 0 or +1 cell per axis) to the other corners
+    const int sx = coarse.nx, sxy = coarse.nx * coarse.ny;
+    const float* p = coarse.z + ((size_t)i0 + (size_t)sx * (size_t)j0 + (size_t)sxy * (size_t)k0);
+    const int dx = i1 - i0, dy = (j1 - j0) * sx, dz = (k1 - k0) * sxy;
+    const float y00 = 0.75f * p[0] + 0.25f * p[dx];
+    const float y10 = 0.75f * p[dy] + 0.25f * p[dx + dy];
+    const float y01 = 0.75f * p[dz] + 0.25f * p[dx + dz];
+    const float y11 = 0.75f * p[dy + dz] + 0.25f * p[dx + dy + dz];
     const float x0 = 0.75f * y00 + 0.25f * y10;
     const float x1 = 0.75f * y01 + 0.25f * y11;
     return 0.75f * x0 + 0.25f * x1;
