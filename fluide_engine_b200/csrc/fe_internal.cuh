@@ -69,7 +69,8 @@ struct SceneView {
     float *px, *py, *pz, *vx, *vy, *vz;
     float* c[9];
     uint32_t* pid;
-    // sort scratch
+    // the sort's scratch: key per particle; rank = a particle's atomic slot in its cell, then (after the sort) the
+    // sorted order, slot -> particle; perm = the runs in arbitrary order; cell counts and starts per cell key
     uint32_t *key, *rank, *perm, *cell_count, *cell_start;
     // grid
     float *u, *v, *w;

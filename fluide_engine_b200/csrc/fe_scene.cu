@@ -75,7 +75,7 @@ __global__ void k_sorted_keys(SceneView v, uint32_t* out)
 {
     uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (s >= v.np) return;
-    out[s] = v.key[v.perm[s]];
+    out[s] = v.key[v.rank[s]];
 }
 
 __global__ void k_perm_ids(const uint32_t* perm, const uint32_t* pid_old, uint32_t* out, uint64_t n)
@@ -2218,7 +2218,7 @@ fe_status fe_scene_get_sort(fe_scene* s, uint32_t* keys, uint32_t* perm, uint64_
     if (perm) {
         // slot -> particle id (the ids the particles carried before the last sort)
         SceneView prev = view_of(s, s->parity ^ 1);
-        k_perm_ids<<<nb, 256, 0, s->stream>>>(v.perm, prev.pid, s->staging_u32, n);
+        k_perm_ids<<<nb, 256, 0, s->stream>>>(v.rank, prev.pid, s->staging_u32, n);
         count_launch();
         FE_CUDA(cudaMemcpyAsync(perm, s->staging_u32, n * 4, cudaMemcpyDefault, s->stream));
     }

@@ -12,11 +12,11 @@
 //   k_cellrank each particle's final slot = run start + the number of particles of its run with a smaller
 //              index, so the runs end up ordered by particle index and the result is identical to a stable
 //              sort by key (the oracle is a CPU stable counting sort of the same keys); O(run length) per
-//              particle, all particles of a run in parallel
+//              particle, all particles of a run in parallel; the particle is written at its final slot of
+//              `rank`, which from then on holds the sorted order (slot -> particle) that the gather reads
 //   k_bigcell  runs longer than kBigCell (particles piled into one cell, e.g. clamped into a wall corner)
 //              are ordered by one block each with a bitonic network instead, so the cost stays
 //              O(n log^2 n) per run rather than O(n^2)
-//   k_place_final  perm[final slot] = particle
 //   k_gather   particle arrays permuted into the second buffer set
 #include "fe_internal.cuh"
 
@@ -141,7 +141,8 @@ __global__ void k_place(SceneView v, uint32_t* __restrict__ long_count)
     v.perm[v.cell_start[v.key[i]] + v.rank[i]] = (uint32_t)i;
 }
 
-// rank[x] = final slot of particle x (rank's atomic slots were consumed by k_place).
+// rank[final slot of particle x] = x (rank's atomic slots were consumed by k_place; perm, the runs in arbitrary
+// order, is only read here).
 __global__ void k_cellrank(SceneView v, uint32_t* __restrict__ long_count)
 {
     uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -156,13 +157,13 @@ __global__ void k_cellrank(SceneView v, uint32_t* __restrict__ long_count)
     }
     uint32_t r = 0;
     for (uint32_t t = b; t < e; ++t) r += perm[t] < x ? 1u : 0u;
-    v.rank[x] = b + r;
+    v.rank[b + r] = x;
 }
 
 // One block per listed long run.  Ascending-only bitonic network (each merge of size k starts with the
 // mirrored comparator i <-> i ^ (k - 1), then half-cleaners of distance k/4 .. 1) over the run padded to
 // a power of two; padded positions count as +infinity, so a pair whose upper element is past the run's
-// end never swaps and is skipped.  Sorted in place in perm, then rank[x] = final slot.
+// end never swaps and is skipped.  Sorted in place in perm, then copied to the run's slots of rank.
 __global__ void __launch_bounds__(1024) k_bigcell(SceneView v, const uint32_t* __restrict__ long_count)
 {
     const uint32_t count = *long_count;
@@ -188,16 +189,9 @@ __global__ void __launch_bounds__(1024) k_bigcell(SceneView v, const uint32_t* _
                 __syncthreads();
             }
         }
-        for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) v.rank[a[t]] = b + t;
+        for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) v.rank[b + t] = a[t];
         __syncthreads();
     }
-}
-
-__global__ void k_place_final(SceneView v)
-{
-    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= v.np) return;
-    v.perm[v.rank[i]] = (uint32_t)i;
 }
 
 // Each thread moves kGatherBatch particles, all their loads issued before any store, so a thread keeps several
@@ -214,7 +208,7 @@ __global__ void __launch_bounds__(256) k_gather(SceneView src, SceneView dst)
     for (int b = 0; b < kGatherBatch; ++b) {
         const uint64_t i = base + (uint64_t)b * blockDim.x;
         ok[b] = i < src.np;
-        j[b] = ok[b] ? src.perm[i] : 0u;
+        j[b] = ok[b] ? src.rank[i] : 0u;  // the sorted order (slot -> particle)
     }
     float a[kGatherBatch][6];
     uint32_t id[kGatherBatch];
@@ -296,8 +290,7 @@ cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, siz
         k_place<<<pb, T, 0, st>>>(v, long_count);
         k_cellrank<<<pb, T, 0, st>>>(v, long_count);
         k_bigcell<<<kBigCellBlocks, 1024, 0, st>>>(v, long_count);
-        k_place_final<<<pb, T, 0, st>>>(v);
-        count_launch(4);
+        count_launch(3);
     }
     return cudaGetLastError();
 }
