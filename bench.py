@@ -523,11 +523,18 @@ def batched_measure(n_scenes=48, steps=50, warmup=5, device=0, batch_family=None
     tuned = tune_scenes(lambda key: make(first[key]), sorted(first), DT, device)
     tune_s = time.perf_counter() - t0
 
+    # both arms time the same substep window: the batched arm's warm-up (at least the 8 substeps after which a batch
+    # runs from its captured graph) plus the batch tuner's substeps come first in both
+    from fluide_engine_b200 import autotune
+
+    flat_candidates = autotune.FLAT_CANDIDATES
+    tune_sub = 3
+    pre = max(warmup, 8) + 2 * len(flat_candidates) * (tune_sub + 1)
     # one at a time (each scene's own graph-captured substeps, scene after scene)
     scenes = build()
     particles = sum(sc.num_particles() for sc in scenes)
     for sc in scenes:
-        sc.step(DT, warmup, stats=False)
+        sc.step(DT, pre, stats=False)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res_alone = []
@@ -544,7 +551,9 @@ def batched_measure(n_scenes=48, steps=50, warmup=5, device=0, batch_family=None
         for sc in scenes:
             sc.set_tuning(multigrid=0)
     batch = fe.Batch(scenes)
-    batch.step(DT, warmup, stats=False)
+    batch.step(DT, max(warmup, 8), stats=False)
+    # which scenes run in the flat (scene, block) launches: timed on the batch's own substeps
+    flat_best, flat_ms = autotune.tune_batch(batch, DT, substeps=tune_sub, candidates=flat_candidates)
     torch.cuda.synchronize()
     launches0 = fe.kernel_launch_count()
     t0 = time.perf_counter()
@@ -559,15 +568,22 @@ def batched_measure(n_scenes=48, steps=50, warmup=5, device=0, batch_family=None
         sc.close()
     v_batch = particles * steps / t_batch
     v_alone = particles * steps / t_alone
-    return {"value": v_batch, "unit": METRIC, "steps": steps, "warmup": warmup,
+    return {"value": v_batch, "unit": METRIC, "steps": steps, "warmup": pre,
             "ms_per_step": t_batch / steps * 1e3,
             "workload": "%d batched scenes, n in {32,48,64,96,128}, block extents U[0.2,0.6], solver "
-                        "U{PIC,FLIP,APIC} (seed 2), dt=1/240, CG rel 1e-6, %d substeps after %d warm-up"
-                        % (len(specs), steps, warmup),
+                        "U{PIC,FLIP,APIC} (seed 2), dt=1/240, CG rel 1e-6, %d substeps after %d warm-up and tuning "
+                        "substeps in both arms" % (len(specs), steps, pre),
             "scenes": [[n, ["PIC", "FLIP", "APIC"][sv]] for n, sv, _, _ in specs],
             "particles_total": particles, "timing": "wall clock around synchronised device work",
             "one_at_a_time": {"value": v_alone, "ms_per_step_all_scenes": t_alone / steps * 1e3},
             "batched_over_one_at_a_time": v_batch / v_alone, "batch_family": batch_family or "autotuned per kind",
+            "flat_launches": {"max_cells": flat_best,
+                              "note": "scenes of at most max_cells cells run each pre/post-solve pass as one launch "
+                                      "for all of them over a (scene, block) work list, the rest on their own "
+                                      "streams (0: none, -1: all); picked by timing each choice over %d substeps "
+                                      "(ms per substep below); %d substeps precede both arms' timed window"
+                                      % (tune_sub, pre),
+                              "ms_per_substep": {str(k): v for k, v in flat_ms.items()}},
             "accuracy": {"rel_residual_max_batched": max(res_batch), "rel_residual_max_alone": max(res_alone),
                          "converged_all": conv},
             "tuning": {"%d^3 %s" % (n, ["PIC", "FLIP", "APIC"][sv]): choice for (n, sv), (choice, _) in tuned.items()},
@@ -587,7 +603,7 @@ def run_batched(args):
             "config": {"workload": b["workload"], "scenes": b["scenes"], "particles_total": b["particles_total"],
                        "timing": b["timing"]},
             "one_at_a_time": b["one_at_a_time"], "batched_over_one_at_a_time": b["batched_over_one_at_a_time"],
-            "accuracy": b["accuracy"], "gpu_launches": b["gpu_launches"]}
+            "flat_launches": b["flat_launches"], "accuracy": b["accuracy"], "gpu_launches": b["gpu_launches"]}
     print(json.dumps(line), flush=True)
     return 0
 

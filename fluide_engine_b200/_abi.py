@@ -40,6 +40,7 @@ EXPORTS = [
     "fe_abi_version", "fe_debug_set_barrier_limits", "fe_scene_set_tuning", "fe_scene_get_tuning",
     "fe_scene_snapshot", "fe_scene_restore", "fe_snapshot_info", "fe_snapshot_destroy",
     "fe_scene_autotune", "fe_tuning_store", "fe_tuning_lookup", "fe_batch_set_overlap",
+    "fe_batch_set_flat",
 ]
 
 
@@ -158,6 +159,7 @@ def lib():
     L.fe_batch_set_scenes.argtypes = [P, ctypes.POINTER(P), ctypes.c_int32]
     L.fe_batch_destroy.argtypes = [P]
     L.fe_batch_set_overlap.argtypes = [P, ctypes.c_int32]
+    L.fe_batch_set_flat.argtypes = [P, ctypes.c_int64]
     L.fe_batch_step.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats)]
     L.fe_batch_step_profiled.argtypes = [P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(StepStats),
                                          ctypes.POINTER(ctypes.c_float)]

@@ -115,3 +115,36 @@ def tune(scene, dt, substeps=6, device=0, path=None, save=True, shape_only=False
         entries[(tuple(scene.n), scene.solver)] = choice
         write_file(path, entries, name)
     return choice, float(ms.value)
+
+
+FLAT_CANDIDATES = (0, 32 ** 3, 48 ** 3, 64 ** 3, -1)
+
+
+def tune_batch(batch, dt, substeps=3, candidates=FLAT_CANDIDATES, timer=None, rounds=2):
+    """Picks which of a batch's scenes run in the flat launches (Batch.set_flat: scenes up to max_cells cells run
+    every pre- and post-solve pass as one launch for all of them; the rest on their own streams).
+
+    Every candidate computes the same substeps, so the search times them on the batch's own live substeps: per
+    candidate and round one untimed substep (the batch graph's capture, once the batch is old enough to be captured)
+    and `substeps` timed ones; the rounds visit the candidates in alternating order and each candidate keeps its best
+    round, so a slow moment of the device does not decide.  The scenes advance by rounds * len(candidates) *
+    (substeps + 1) substeps.  Applies the fastest and returns (max_cells, {candidate: ms per substep}).  `timer`
+    (seconds, monotonic) defaults to time.perf_counter; the batch's step() synchronises before returning, so the wall
+    clock spans the device work.
+    """
+    import time
+
+    clock = timer or time.perf_counter
+    times = {}
+    order = list(candidates)
+    for r in range(max(1, rounds)):
+        for c in (order if r % 2 == 0 else order[::-1]):
+            batch.set_flat(c)
+            batch.step(dt, 1, stats=False)
+            t0 = clock()
+            batch.step(dt, substeps, stats=False)
+            ms = (clock() - t0) / max(substeps, 1) * 1e3
+            times[c] = min(times.get(c, ms), ms)
+    best = min(times, key=times.get)
+    batch.set_flat(best)
+    return best, times

@@ -15,14 +15,6 @@
 namespace fe {
 namespace {
 
-struct G2PArgs {
-    float dt_sub;
-    int nsub;
-    int same_origins;        // the FLIP residual grid's data origins equal the velocity grid's (domain origin 0)
-    float dom_lo[3], dom_hi[3];
-    const float *u, *v, *w;  // final velocity buffers
-};
-
 // Face values of the six arrays a transfer reads (u, v, w and the FLIP snapshot su, sv, sw).
 struct FaceSource {
     const float* g[6];          // u, v, w, su, sv, sw
@@ -240,6 +232,22 @@ __global__ void __launch_bounds__(256, 4) k_g2p(SceneView v, G2PArgs g)
     g2p_particle<SOLVER, G2P, MOVE>(v, g, global_source(v, g), p);
 }
 
+// Flat multi-scene form (BatchPlan, fe_internal.cuh): every scene's particles in one launch, transfer and move
+// fused, each block running its scene's transfer kind.
+__global__ void __launch_bounds__(256, 4) k_multi_g2p(const BatchPlan* __restrict__ plan)
+{
+    __shared__ SceneView v;
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkPart, b);
+    const BatchScene& e = plan->sc[s];
+    stage_view(v, e.dst);
+    const uint64_t p = b * (uint64_t)blockDim.x + threadIdx.x;
+    if (p >= v.np) return;
+    if (v.solver == FE_SOLVER_PIC) g2p_particle<FE_SOLVER_PIC, true, true>(v, e.g2p, global_source(v, e.g2p), p);
+    else if (v.solver == FE_SOLVER_FLIP) g2p_particle<FE_SOLVER_FLIP, true, true>(v, e.g2p, global_source(v, e.g2p), p);
+    else g2p_particle<FE_SOLVER_APIC, true, true>(v, e.g2p, global_source(v, e.g2p), p);
+}
+
 template <int SOLVER>
 void launch_solver(const SceneView& v, const G2PArgs& g, bool do_g2p, bool do_move, cudaStream_t st)
 {
@@ -251,9 +259,16 @@ void launch_solver(const SceneView& v, const G2PArgs& g, bool do_g2p, bool do_mo
 
 }  // namespace
 
-cudaError_t launch_g2p(const SceneView& v, double dt, bool do_g2p, bool do_move, cudaStream_t st)
+cudaError_t launch_multi_g2p(const BatchLaunch& L, cudaStream_t st)
 {
-    if (v.np == 0 || (!do_g2p && !do_move)) return cudaSuccess;
+    if (!L.total[kBkPart]) return cudaSuccess;
+    k_multi_g2p<<<L.total[kBkPart], 256, 0, st>>>(L.plan);
+    count_launch();
+    return cudaGetLastError();
+}
+
+G2PArgs g2p_args(const SceneView& v, double dt)
+{
     G2PArgs g;
     g.nsub = v.rk_substeps;
     g.dt_sub = (float)(dt / g.nsub);
@@ -267,6 +282,13 @@ cudaError_t launch_g2p(const SceneView& v, double dt, bool do_g2p, bool do_move,
     g.u = v.u;  // after the post group the velocity is back in buffer A
     g.v = v.v;
     g.w = v.w;
+    return g;
+}
+
+cudaError_t launch_g2p(const SceneView& v, double dt, bool do_g2p, bool do_move, cudaStream_t st)
+{
+    if (v.np == 0 || (!do_g2p && !do_move)) return cudaSuccess;
+    const G2PArgs g = g2p_args(v, dt);
     if (v.solver == FE_SOLVER_PIC) launch_solver<FE_SOLVER_PIC>(v, g, do_g2p, do_move, st);
     else if (v.solver == FE_SOLVER_FLIP) launch_solver<FE_SOLVER_FLIP>(v, g, do_g2p, do_move, st);
     else launch_solver<FE_SOLVER_APIC>(v, g, do_g2p, do_move, st);

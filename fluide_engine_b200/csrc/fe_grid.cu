@@ -30,38 +30,54 @@ struct FaceArrays {
 enum { kModePlain = 0, kModePre = 1, kModePost = 2 };
 
 
-template <int MODE>
-__global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid, float gx, float gy, float gz)
-{
+// The loads of one face of an extrapolation pass: the face and its six neighbours (order i+1, i-1, j+1, j-1, k+1,
+// k-1).  Every validity byte and value is loaded before any is used -- the neighbours whether or not the face turns
+// out to need them -- so all are in flight together in one round trip instead of the face's own load followed by
+// its neighbours'.
+struct ExtrapFace {
     FaceCoord fc;
-    if (!face_coord(nx, ny, nz, fc)) return;
-    const int c = fc.c, i = fc.i, j = fc.j, k = fc.k, sx = fc.sx, sy = fc.sy, sz = fc.sz;
-    const size_t f = fc.f;
+    bool ok;
+    float val, nval[6];
+    uint8_t valid, nvalid[6];
+};
+
+__device__ __forceinline__ void extrap_load(const FaceArrays& fa, int nx, int ny, int nz, Blk3 blk, ExtrapFace& e)
+{
+    e.ok = face_coord(nx, ny, nz, blk, e.fc);
+    if (!e.ok) return;
+    const int c = e.fc.c, i = e.fc.i, j = e.fc.j, k = e.fc.k, sx = e.fc.sx, sy = e.fc.sy, sz = e.fc.sz;
+    const size_t f = e.fc.f;
     // select by value (a runtime index into the parameter arrays would spill them to local memory)
     const float* in = c == 0 ? fa.in[0] : (c == 1 ? fa.in[1] : fa.in[2]);
     const uint8_t* vin = c == 0 ? fa.vin[0] : (c == 1 ? fa.vin[1] : fa.vin[2]);
-    // the face and its six neighbours (order i+1, i-1, j+1, j-1, k+1, k-1): every validity byte and value is
-    // loaded before any is used -- the neighbours whether or not the face turns out to need them -- so all are in
-    // flight together in one round trip instead of the face's own load followed by its neighbours'
     const size_t sxy = (size_t)sx * sy;
     const bool in_dom[6] = {i + 1 < sx, i > 0, j + 1 < sy, j > 0, k + 1 < sz, k > 0};
     const long long off[6] = {1, -1, (long long)sx, -(long long)sx, (long long)sxy, -(long long)sxy};
-    float val = in[f];
-    uint8_t valid = vin[f];
-    uint8_t nvalid[6];
-    float nval[6];
+    e.val = in[f];
+    e.valid = vin[f];
 #pragma unroll
     for (int n = 0; n < 6; ++n) {
-        nvalid[n] = in_dom[n] ? vin[(long long)f + off[n]] : (uint8_t)0;
-        nval[n] = in_dom[n] ? in[(long long)f + off[n]] : 0.f;
+        e.nvalid[n] = in_dom[n] ? vin[(long long)f + off[n]] : (uint8_t)0;
+        e.nval[n] = in_dom[n] ? in[(long long)f + off[n]] : 0.f;
     }
+}
+
+// An invalid face takes the mean of its valid neighbours; then the pass's tail (walls, gravity) and the stores.
+template <int MODE>
+__device__ __forceinline__ void extrap_store(const FaceArrays& fa, bool write_valid, float gx, float gy, float gz,
+                                             const ExtrapFace& e)
+{
+    const int c = e.fc.c, i = e.fc.i, j = e.fc.j, k = e.fc.k, sx = e.fc.sx, sy = e.fc.sy, sz = e.fc.sz;
+    const size_t f = e.fc.f;
+    float val = e.val;
+    uint8_t valid = e.valid;
     if (!valid) {
         float sum = 0.f;
         unsigned count = 0;
 #pragma unroll
         for (int n = 0; n < 6; ++n)
-            if (nvalid[n]) {
-                sum += nval[n];
+            if (e.nvalid[n]) {
+                sum += e.nval[n];
                 ++count;
             }
         if (count > 0) {
@@ -79,12 +95,46 @@ __global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid
     (c == 0 ? fa.out[0] : (c == 1 ? fa.out[1] : fa.out[2]))[f] = val;
 }
 
-__global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
-                      const float* __restrict__ w)
+template <int MODE>
+__device__ __forceinline__ void extrap_body(const FaceArrays& fa, int nx, int ny, int nz, bool write_valid, float gx,
+                                            float gy, float gz, Blk3 blk)
+{
+    ExtrapFace e;
+    extrap_load(fa, nx, ny, nz, blk, e);
+    if (e.ok) extrap_store<MODE>(fa, write_valid, gx, gy, gz, e);
+}
+
+// kFaceLayers consecutive face layers (blk.z .. blk.z + kFaceLayers - 1, below zend) per thread: all their loads are
+// issued before the first store, so a thread keeps several faces' round trips in flight.
+constexpr int kFaceLayers = 4;
+
+template <int MODE>
+__device__ __forceinline__ void extrap_layers(const FaceArrays& fa, int nx, int ny, int nz, bool write_valid,
+                                              float gx, float gy, float gz, Blk3 blk, unsigned zend)
+{
+    ExtrapFace e[kFaceLayers];
+#pragma unroll
+    for (int t = 0; t < kFaceLayers; ++t) {
+        e[t].ok = false;
+        if (blk.z + t < zend) extrap_load(fa, nx, ny, nz, Blk3{blk.x, blk.y, blk.z + t}, e[t]);
+    }
+#pragma unroll
+    for (int t = 0; t < kFaceLayers; ++t)
+        if (e[t].ok) extrap_store<MODE>(fa, write_valid, gx, gy, gz, e[t]);
+}
+
+template <int MODE>
+__global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid, float gx, float gy, float gz)
+{
+    extrap_body<MODE>(fa, nx, ny, nz, write_valid, gx, gy, gz, hw_blk3());
+}
+
+__device__ __forceinline__ void rhs_body(const SceneView& v, const float* __restrict__ u, const float* __restrict__ vv,
+                                         const float* __restrict__ w, Blk3 blk)
 {
     const int nx = v.g.nx, ny = v.g.ny;
-    const int i = (int)(blockIdx.x * kTileX + threadIdx.x), j = (int)(blockIdx.y * kTileY + threadIdx.y);
-    const int k = (int)blockIdx.z;
+    const int i = (int)(blk.x * kTileX + threadIdx.x), j = (int)(blk.y * kTileY + threadIdx.y);
+    const int k = (int)blk.z;
     if (i >= nx || j >= ny) return;
     const size_t c = idx3(i, j, k, nx, ny);
     double b = 0.0;
@@ -105,11 +155,17 @@ __global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __r
     }
 }
 
-__global__ void k_apply(SceneView v, float* u, float* vv, float* w)
+__global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
+                      const float* __restrict__ w)
+{
+    rhs_body(v, u, vv, w, hw_blk3());
+}
+
+__device__ __forceinline__ void apply_body(const SceneView& v, float* u, float* vv, float* w, Blk3 blk)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
     FaceCoord fc;
-    if (!face_coord(nx, ny, nz, fc)) return;
+    if (!face_coord(nx, ny, nz, blk, fc)) return;
     const double* p = v.p;
     const int i = fc.i, j = fc.j, k = fc.k;
     if (fc.c == 0) {
@@ -129,6 +185,8 @@ __global__ void k_apply(SceneView v, float* u, float* vv, float* w)
         w[fc.f] = (float)((double)w[fc.f] + v.inv_h[2] * (p[cm + (size_t)nx * ny] - p[cm]));
     }
 }
+
+__global__ void k_apply(SceneView v, float* u, float* vv, float* w) { apply_body(v, u, vv, w, hw_blk3()); }
 
 __global__ void k_cfl(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
                       const float* __restrict__ w, double dt, unsigned long long* out_bits)
@@ -260,11 +318,11 @@ cudaError_t launch_extrap_faces(const SceneView& v, float* const src[3], float* 
 
 namespace {
 
-__global__ void k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g, float gx, float gy,
-                            float gz)
+__device__ __forceinline__ void wall_tail_body(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g,
+                                               float gx, float gy, float gz, Blk3 blk)
 {
     FaceCoord fc;
-    if (!face_coord(nx, ny, nz, fc)) return;
+    if (!face_coord(nx, ny, nz, blk, fc)) return;
     const int c = fc.c, i = fc.i, j = fc.j, k = fc.k, sx = fc.sx, sy = fc.sy, sz = fc.sz;
     const size_t f = fc.f;
     float* a = c == 0 ? u : (c == 1 ? vv : w);
@@ -272,6 +330,129 @@ __global__ void k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int n
                       (c == 2 && (k == 0 || k == sz - 1));
     if (wall) a[f] = 0.f;
     else if (add_g) a[f] += (c == 0 ? gx : (c == 1 ? gy : gz));
+}
+
+__global__ void k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g, float gx, float gy,
+                            float gz)
+{
+    wall_tail_body(u, vv, w, nx, ny, nz, add_g, gx, gy, gz, hw_blk3());
+}
+
+// ---- flat multi-scene forms (BatchPlan, fe_internal.cuh)
+
+// The substep's clears of every scene (fill bytes over the plan's ranges), 16-byte stores where aligned.
+__global__ void __launch_bounds__(256) k_multi_clear(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkClear, b);
+    const BatchScene& e = plan->sc[s];
+    const uint32_t nblk = plan->start[kBkClear][s + 1] - plan->start[kBkClear][s];
+    const uint64_t stride = (uint64_t)nblk * blockDim.x;
+    for (int r = 0; r < e.nclr; ++r) {
+        uint8_t* p = e.clr_ptr[r];
+        const uint64_t n = e.clr_bytes[r];
+        const uint8_t val = (uint8_t)e.clr_val[r];
+        const uint32_t w = 0x01010101u * val;
+        const uint64_t head = min(n, (uint64_t)((16u - ((uintptr_t)p & 15u)) & 15u));
+        const uint64_t nq = (n - head) / 16;
+        const uint64_t tail = head + nq * 16;
+        if (b == 0 && threadIdx.x < head) p[threadIdx.x] = val;
+        if (b == 0 && threadIdx.x < n - tail) p[tail + threadIdx.x] = val;
+        uint4* q = (uint4*)(p + head);
+        for (uint64_t u = (uint64_t)b * blockDim.x + threadIdx.x; u < nq; u += stride) q[u] = make_uint4(w, w, w, w);
+    }
+}
+
+// The face grid of the flat face passes: blocks of kFaceLayers layers.
+__host__ __device__ inline dim3 layer_grid(dim3 fg) { return dim3(fg.x, fg.y, (fg.z + kFaceLayers - 1) / kFaceLayers); }
+
+// Buffers of pass `pass` of a scene's extrapolation group (run_extrap_group's assignment, evaluated per scene):
+// A = (u, v, w), B = (u2, v2, w2); the pre group starts from A and ends in A (even depth) or B (odd); the post
+// group starts where the pre group ended and ends in A.
+__device__ __forceinline__ void group_arrays(const SceneView& v, bool pre, int pass, int d, FaceArrays& fa)
+{
+    float* A[3] = {v.u, v.v, v.w};
+    float* B[3] = {v.u2, v.v2, v.w2};
+    float* const* src = pre ? A : ((d & 1) ? B : A);
+    float* const* oth = pre ? B : ((d & 1) ? A : B);
+    float* const* fin = pre ? ((d & 1) ? B : A) : A;
+    const size_t nu = (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz, nvv = (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz;
+    const size_t total = nu + nvv + (size_t)v.g.nx * v.g.ny * (v.g.nz + 1);
+    uint8_t* vs0 = v.mu2 + (size_t)(pass & 1) * total;        // this pass's validity output
+    uint8_t* vs1 = v.mu2 + (size_t)((pass - 1) & 1) * total;  // the previous pass's
+    // pass p reads what pass p - 1 wrote: src at p = 0, then alternately oth (p odd) and src (p even)
+    float* const* in = pass == 0 ? src : ((pass & 1) ? oth : src);
+    float* const* out = pass == d - 1 ? fin : ((pass & 1) ? src : oth);
+    for (int c = 0; c < 3; ++c) {
+        fa.in[c] = in[c];
+        fa.out[c] = out[c];
+    }
+    fa.vin[0] = pass == 0 ? v.mu : vs1;
+    fa.vin[1] = pass == 0 ? v.mv : vs1 + nu;
+    fa.vin[2] = pass == 0 ? v.mw : vs1 + nu + nvv;
+    fa.vout[0] = vs0;
+    fa.vout[1] = vs0 + nu;
+    fa.vout[2] = vs0 + nu + nvv;
+}
+
+// Pass `pass` of every scene's pre (PRE) or post extrapolation group; a scene whose group is shorter skips the pass,
+// a scene with no extrapolation runs its wall tail at pass 0.
+template <bool PRE>
+__global__ void __launch_bounds__(kTileX * kTileY) k_multi_extrap(const BatchPlan* __restrict__ plan, int pass)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkFaces, b);
+    const BatchScene& e = plan->sc[s];
+    const SceneView& v = e.dst;
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const dim3 fg = face_grid(nx, ny, nz);
+    Blk3 blk = flat_blk3(b, layer_grid(fg));
+    blk.z *= kFaceLayers;
+    const int d = v.extrap_depth;
+    const float gx = PRE ? e.gdt[0] : 0.f, gy = PRE ? e.gdt[1] : 0.f, gz = PRE ? e.gdt[2] : 0.f;
+    if (d <= 0) {
+        if (pass == 0)
+            for (int t = 0; t < kFaceLayers && blk.z + t < fg.z; ++t)
+                wall_tail_body(v.u, v.v, v.w, nx, ny, nz, PRE, gx, gy, gz, Blk3{blk.x, blk.y, blk.z + t});
+        return;
+    }
+    if (pass >= d) return;
+    FaceArrays fa;
+    group_arrays(v, PRE, pass, d, fa);
+    if (pass == d - 1) extrap_layers<PRE ? kModePre : kModePost>(fa, nx, ny, nz, false, gx, gy, gz, blk, fg.z);
+    else extrap_layers<kModePlain>(fa, nx, ny, nz, true, 0.f, 0.f, 0.f, blk, fg.z);
+}
+
+// The velocity buffers the pressure stage reads and writes: B after an odd pre group, else A.
+__device__ __forceinline__ void stage_buffers(const SceneView& v, float*& u, float*& vv, float*& w)
+{
+    const bool odd = v.extrap_depth > 0 && (v.extrap_depth & 1);
+    u = odd ? v.u2 : v.u;
+    vv = odd ? v.v2 : v.v;
+    w = odd ? v.w2 : v.w;
+}
+
+__global__ void __launch_bounds__(kTileX * kTileY) k_multi_rhs(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkCells, b);
+    const SceneView& v = plan->sc[s].dst;
+    float *u, *vv, *w;
+    stage_buffers(v, u, vv, w);
+    rhs_body(v, u, vv, w, flat_blk3(b, cell_grid(v.g.nx, v.g.ny, v.g.nz)));
+}
+
+__global__ void __launch_bounds__(kTileX * kTileY) k_multi_apply(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkFaces, b);
+    const SceneView& v = plan->sc[s].dst;
+    float *u, *vv, *w;
+    stage_buffers(v, u, vv, w);
+    const dim3 fg = face_grid(v.g.nx, v.g.ny, v.g.nz);
+    Blk3 blk = flat_blk3(b, layer_grid(fg));
+    blk.z *= kFaceLayers;
+    for (int t = 0; t < kFaceLayers && blk.z + t < fg.z; ++t) apply_body(v, u, vv, w, Blk3{blk.x, blk.y, blk.z + t});
 }
 
 }  // namespace
@@ -359,6 +540,66 @@ cudaError_t launch_scatter_out(const SceneView& v, float* pos, float* vel, float
 {
     if (v.np == 0) return cudaSuccess;
     k_scatter_out<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, pos, vel, C);
+    count_launch();
+    return cudaGetLastError();
+}
+
+uint32_t batch_blocks(const SceneView& v, int kind)
+{
+    const size_t faces = faces_total(v);
+    switch (kind) {
+    case kBkClear: return 0;  // set by the plan builder from its clear ranges
+    case kBkPart: return (uint32_t)((v.np + 255) / 256);
+    case kBkP2g: return v.np > 0 ? (uint32_t)(v.g.tnx * v.g.tny * v.g.tnz) : 0u;
+    case kBkNormalize: return (uint32_t)((faces + 255) / 256);
+    case kBkFaces: {
+        const dim3 g = layer_grid(face_grid(v.g.nx, v.g.ny, v.g.nz));
+        return g.x * g.y * g.z;
+    }
+    case kBkCells: {
+        const dim3 g = cell_grid(v.g.nx, v.g.ny, v.g.nz);
+        return g.x * g.y * g.z;
+    }
+    case kBkFixup: return v.np > 0 && v.any_inexact ? 148u : 0u;
+    default: return sort_batch_blocks(v, kind);
+    }
+}
+
+cudaError_t launch_multi_clear(const BatchLaunch& L, cudaStream_t st)
+{
+    k_multi_clear<<<L.total[kBkClear], 256, 0, st>>>(L.plan);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_multi_pre(const BatchLaunch& L, cudaStream_t st)
+{
+    for (int pass = 0; pass < (L.max_depth > 0 ? L.max_depth : 1); ++pass) {
+        k_multi_extrap<true><<<L.total[kBkFaces], dim3(kTileX, kTileY), 0, st>>>(L.plan, pass);
+        count_launch();
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_multi_post(const BatchLaunch& L, cudaStream_t st)
+{
+    for (int pass = 0; pass < (L.max_depth > 0 ? L.max_depth : 1); ++pass) {
+        k_multi_extrap<false><<<L.total[kBkFaces], dim3(kTileX, kTileY), 0, st>>>(L.plan, pass);
+        count_launch();
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_multi_rhs(const BatchLaunch& L, cudaStream_t st)
+{
+    k_multi_rhs<<<L.total[kBkCells], dim3(kTileX, kTileY), 0, st>>>(L.plan);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_multi_apply(const BatchLaunch& L, cudaStream_t st)
+{
+    k_multi_apply<<<L.total[kBkFaces], dim3(kTileX, kTileY), 0, st>>>(L.plan);
     count_launch();
     return cudaGetLastError();
 }

@@ -179,26 +179,40 @@ struct FaceCoord {
     int c, i, j, k, sx, sy, sz;
     size_t f;
 };
-inline dim3 face_grid(int nx, int ny, int nz)
+__host__ __device__ inline dim3 face_grid(int nx, int ny, int nz)
 {
     return dim3((unsigned)((nx + 1 + kTileX - 1) / kTileX), (unsigned)((ny + 1 + kTileY - 1) / kTileY),
                 (unsigned)(3 * nz + 1));
 }
-inline dim3 cell_grid(int nx, int ny, int nz)
+__host__ __device__ inline dim3 cell_grid(int nx, int ny, int nz)
 {
     return dim3((unsigned)((nx + kTileX - 1) / kTileX), (unsigned)((ny + kTileY - 1) / kTileY), (unsigned)nz);
 }
-__device__ __forceinline__ bool face_coord(int nx, int ny, int nz, FaceCoord& fc)
+// Block coordinates of a 3D launch: the hardware's, or those of a block of a flat multi-scene launch (block
+// `local` of its scene's share, x fastest over the scene's own grid of gx x gy blocks).
+struct Blk3 {
+    unsigned x, y, z;
+};
+__device__ __forceinline__ Blk3 hw_blk3() { return {blockIdx.x, blockIdx.y, blockIdx.z}; }
+__device__ __forceinline__ Blk3 flat_blk3(uint32_t local, dim3 grid)
 {
-    const int z = (int)blockIdx.z;
+    return {local % grid.x, (local / grid.x) % grid.y, local / (grid.x * grid.y)};
+}
+__device__ __forceinline__ bool face_coord(int nx, int ny, int nz, Blk3 b, FaceCoord& fc)
+{
+    const int z = (int)b.z;
     if (z < nz) { fc.c = 0; fc.k = z; fc.sx = nx + 1; fc.sy = ny; fc.sz = nz; }
     else if (z < 2 * nz) { fc.c = 1; fc.k = z - nz; fc.sx = nx; fc.sy = ny + 1; fc.sz = nz; }
     else { fc.c = 2; fc.k = z - 2 * nz; fc.sx = nx; fc.sy = ny; fc.sz = nz + 1; }
-    fc.i = (int)(blockIdx.x * kTileX + threadIdx.x);
-    fc.j = (int)(blockIdx.y * kTileY + threadIdx.y);
+    fc.i = (int)(b.x * kTileX + threadIdx.x);
+    fc.j = (int)(b.y * kTileY + threadIdx.y);
     if (fc.i >= fc.sx || fc.j >= fc.sy) return false;
     fc.f = (size_t)fc.i + (size_t)fc.sx * ((size_t)fc.j + (size_t)fc.sy * (size_t)fc.k);
     return true;
+}
+__device__ __forceinline__ bool face_coord(int nx, int ny, int nz, FaceCoord& fc)
+{
+    return face_coord(nx, ny, nz, hw_blk3(), fc);
 }
 
 // Viscosity (fe_diffuse.cu): buffers of the implicit diffusion solve, allocated when a scene's viscosity is > 0.
@@ -442,5 +456,110 @@ cudaError_t launch_forces(const SceneView& v, const ForceList& fl, float* u, flo
 cudaError_t launch_diffuse(const SceneView& v, const DiffWork& d, const CgWork& w, float* u, float* vv, float* ww,
                            double dt, double viscosity, cudaStream_t st);
 cudaError_t diffuse_prepare(DiffWork& d, int device);
+
+// ------------------------------------------------------------------ flat multi-scene launches (batches)
+//
+// A batch substep launches every transfer and grid pass ONCE for all its scenes: the launch's blocks are a flat
+// work list of (scene, block) entries, the scenes' blocks back to back in membership order.  Each kind of launch
+// (block shape) has its own prefix of per-scene block counts; a block finds its scene from that prefix (one ballot
+// over at most 64 scene ends) and runs the same body as the one-scene kernel with its block index inside the
+// scene.  Per-scene data (the two particle buffer sets, scratch, dt-dependent constants) lives in a device table
+// built on the host when the membership or dt changes.
+enum BatchKind {
+    kBkClear,      // 256 threads: the substep's accumulator / count / marker clears
+    kBkPart,       // 256 threads, one particle each: keys, placement, ranks, marking, transfer and move
+    kBkGather,     // 256 threads, 4 particles each
+    kBkScan,       // 1024 threads, 4096 counts each
+    kBkScanSums,   // 1024 threads, one block per scene
+    kBkBigcell,    // 1024 threads, striding over the scene's long runs
+    kBkP2g,        // one 8^3 cell tile each
+    kBkNormalize,  // 256 threads, one face each
+    kBkFaces,      // 32 x 8 threads, face_grid
+    kBkCells,      // 32 x 8 threads, cell_grid
+    kBkFixup,      // 128 threads: marks needing the full SDF sample (scenes with inexact cell-centre samples)
+    kBkCount
+};
+
+// MoveParticles' and the transfer's launch constants (fe_g2p.cu).
+struct G2PArgs {
+    float dt_sub;
+    int nsub;
+    int same_origins;        // the FLIP residual grid's data origins equal the velocity grid's (domain origin 0)
+    float dom_lo[3], dom_hi[3];
+    const float *u, *v, *w;  // final velocity buffers
+};
+G2PArgs g2p_args(const SceneView& v, double dt);
+
+constexpr int kBatchClearRanges = 8;
+struct BatchScene {
+    SceneView src;               // particle buffer set the substep starts from (the sort's input)
+    SceneView dst;               // the other set: the gather's output, used by every later pass
+    uint32_t* scan_sums;         // the sort's scan scratch (block sums, then the long-run counter)
+    uint32_t* long_count;
+    uint32_t scan_blocks;
+    // byte ranges cleared at the start of the substep: cell counts, P2G numerators / weights / face markers, marks
+    uint8_t* clr_ptr[kBatchClearRanges];
+    uint64_t clr_bytes[kBatchClearRanges];
+    uint32_t clr_val[kBatchClearRanges];
+    int nclr;
+    float gdt[3];                // dt * gravity, FP32
+    double R2, rin2, crit_eps;   // marking constants (fe_mark.cu)
+    G2PArgs g2p;
+};
+struct BatchPlan {
+    int count;
+    uint32_t start[kBkCount][kBatchMaxScenes + 1];  // per kind: first block of each scene, then the total
+    BatchScene sc[kBatchMaxScenes];
+};
+// Host-side totals of a plan (grid sizes of the flat launches).
+struct BatchLaunch {
+    const BatchPlan* plan;       // device copy
+    uint32_t total[kBkCount];
+    int max_depth;               // largest extrapolation depth among the scenes
+    bool any_particles;
+};
+
+// The block's scene and its block index inside that scene's share of a kind's launch.  Every lane of the block's
+// first warps must be active (called at kernel entry).
+__device__ __forceinline__ int batch_scene_of(const BatchPlan* __restrict__ plan, int kind, uint32_t& local)
+{
+    const uint32_t b = blockIdx.x;
+    const int lane = (int)((threadIdx.x + threadIdx.y * blockDim.x) & 31);
+    const int S = plan->count;
+    const uint32_t* st = plan->start[kind];
+    const uint32_t e0 = lane < S ? st[lane + 1] : 0xffffffffu;
+    const uint32_t e1 = lane + 32 < S ? st[lane + 33] : 0xffffffffu;
+    const int s = __popc(__ballot_sync(0xffffffffu, b >= e0)) + __popc(__ballot_sync(0xffffffffu, b >= e1));
+    local = b - st[s];
+    return s;
+}
+
+// Copies a scene's view into the block's shared memory (register-heavy kernels read their scene's fields from there
+// instead of keeping loaded copies in registers); ends with a block barrier.
+__device__ __forceinline__ void stage_view(SceneView& dst, const SceneView& src)
+{
+    static_assert(sizeof(SceneView) % 8 == 0, "SceneView is copied in 8-byte words");
+    const int t = (int)(threadIdx.x + threadIdx.y * blockDim.x), n = (int)(blockDim.x * blockDim.y);
+    for (int i = t; i < (int)(sizeof(SceneView) / 8); i += n)
+        reinterpret_cast<unsigned long long*>(&dst)[i] = reinterpret_cast<const unsigned long long*>(&src)[i];
+    __syncthreads();
+}
+
+// Per-kind block count of one scene (host; the same grids the one-scene launchers use); the sort's kinds come from
+// fe_sort.cu.
+uint32_t batch_blocks(const SceneView& v, int kind);
+uint32_t sort_batch_blocks(const SceneView& v, int kind);
+// launch_mark's constants (fe_mark.cu).
+void mark_constants(const SceneView& v, double* R2, double* rin2, double* crit_eps);
+// Flat launches of one batch substep's passes (fe_sort.cu, fe_p2g.cu, fe_mark.cu, fe_grid.cu, fe_g2p.cu).
+cudaError_t launch_multi_clear(const BatchLaunch& L, cudaStream_t st);
+cudaError_t launch_multi_sort(const BatchLaunch& L, cudaStream_t st);    // keys, scan, placement, ranks, gather
+cudaError_t launch_multi_p2g(const BatchLaunch& L, cudaStream_t st);     // splat + normalise
+cudaError_t launch_multi_mark(const BatchLaunch& L, cudaStream_t st);
+cudaError_t launch_multi_pre(const BatchLaunch& L, cudaStream_t st);     // extrapolation + walls + gravity
+cudaError_t launch_multi_rhs(const BatchLaunch& L, cudaStream_t st);
+cudaError_t launch_multi_apply(const BatchLaunch& L, cudaStream_t st);
+cudaError_t launch_multi_post(const BatchLaunch& L, cudaStream_t st);    // extrapolation + walls
+cudaError_t launch_multi_g2p(const BatchLaunch& L, cudaStream_t st);     // transfer + move
 
 }  // namespace fe

@@ -56,9 +56,9 @@ __device__ __forceinline__ bool visited(const SceneView& v, int pbx, int pby, in
 
 // One thread per particle: the nodes within r of it (2 per axis for cubic cells, where 2r = 1.7 h;
 // more along an axis whose spacing is finer than max(h)) get the reference's exact FP64 test.
-__global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double rin2, double crit_eps)
+__device__ __forceinline__ void mark_body(const SceneView& v, double R2, double rin2, double crit_eps, uint32_t blk)
 {
-    uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t p = blk * (uint64_t)blockDim.x + threadIdx.x;
     if (p >= v.np) return;
     const double X[3] = {(double)v.px[p], (double)v.py[p], (double)v.pz[p]};
     const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
@@ -96,6 +96,11 @@ __global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double rin
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double rin2, double crit_eps)
+{
+    mark_body(v, R2, rin2, crit_eps, blockIdx.x);
 }
 
 // Band-limited SDF value of node (i, j, k) exactly as BuildSignedDistanceField computes it.
@@ -150,14 +155,37 @@ __device__ double sample_cell_sdf(const SceneView& v, int i, int j, int k, doubl
     return lerp_ref(b0, b1, fz);
 }
 
-__global__ void k_mark_fixup(SceneView v, double R2, uint32_t cap)
+__device__ __forceinline__ void mark_fixup_body(const SceneView& v, double R2, uint32_t cap, uint32_t blk, uint32_t nblk)
 {
     const uint32_t count = min(*v.crit_count, cap);
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = blk * blockDim.x + threadIdx.x; t < count; t += nblk * blockDim.x) {
         const uint32_t c = v.crit_list[t];
         const int i = c % v.g.nx, j = (c / v.g.nx) % v.g.ny, k = c / (v.g.nx * v.g.ny);
         v.marks[c] = sample_cell_sdf(v, i, j, k, R2) < 0.0 ? FE_CELL_FLUID : FE_CELL_AIR;
     }
+}
+
+__global__ void k_mark_fixup(SceneView v, double R2, uint32_t cap) { mark_fixup_body(v, R2, cap, blockIdx.x, gridDim.x); }
+
+// ---- flat multi-scene forms (BatchPlan, fe_internal.cuh); marks, crit flags and counts are cleared by
+// launch_multi_clear
+__global__ void __launch_bounds__(256) k_multi_mark(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkPart, b);
+    const BatchScene& e = plan->sc[s];
+    mark_body(e.dst, e.R2, e.rin2, e.crit_eps, b);
+}
+
+__global__ void __launch_bounds__(128) k_multi_mark_fixup(const BatchPlan* __restrict__ plan)
+{
+    __shared__ SceneView v;
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkFixup, b);
+    const BatchScene& e = plan->sc[s];
+    stage_view(v, e.dst);
+    mark_fixup_body(v, e.R2, (uint32_t)((size_t)v.g.nx * v.g.ny * v.g.nz), b,
+                    plan->start[kBkFixup][s + 1] - plan->start[kBkFixup][s]);
 }
 
 __global__ void k_fluid_sdf(SceneView v, double R2, double* out)
@@ -280,6 +308,28 @@ static double sqrt_below(double r)
     while (t > 0.0 && std::sqrt(t) >= r) t = std::nextafter(t, 0.0);
     while (std::sqrt(std::nextafter(t, HUGE_VAL)) < r) t = std::nextafter(t, HUGE_VAL);
     return t;
+}
+
+cudaError_t launch_multi_mark(const BatchLaunch& L, cudaStream_t st)
+{
+    if (L.total[kBkPart]) {
+        k_multi_mark<<<L.total[kBkPart], 256, 0, st>>>(L.plan);
+        count_launch();
+    }
+    if (L.total[kBkFixup]) {
+        k_multi_mark_fixup<<<L.total[kBkFixup], 128, 0, st>>>(L.plan);
+        count_launch();
+    }
+    return cudaGetLastError();
+}
+
+// The marking constants of launch_mark: band^2, the largest squared distance whose square root is below r, and the
+// window around r in which an inexact cell-centre sample is recomputed.
+void mark_constants(const SceneView& v, double* R2, double* rin2, double* crit_eps)
+{
+    *R2 = v.band * v.band;
+    *rin2 = sqrt_below(v.radius);
+    *crit_eps = 1e-9 * v.radius;
 }
 
 cudaError_t launch_mark(const SceneView& v, cudaStream_t st)

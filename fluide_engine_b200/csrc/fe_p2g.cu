@@ -331,16 +331,25 @@ __device__ __forceinline__ void own_component(const SceneView& v, uint32_t pb, u
     flush_slots<SOLVER, C>(lx, ly, lz, num, den, mask, s_num, s_den, s_mk);
 }
 
-template <int SOLVER>
-__global__ void __launch_bounds__(kP2gThreads, 1) k_p2g(SceneView v)
-{
-    __shared__ float s_num[3][kBoxFaces];
-    __shared__ float s_den[3][kBoxFaces];
-    __shared__ uint8_t s_mk[3][kBoxFaces];
-    __shared__ uint16_t s_over[FE_TILE_CELLS];  // cells with more than kCellCap particles (tile-local index)
-    __shared__ int s_nover;
+// The tile's face box in shared memory (declared by the kernels, so a kernel that runs several transfer kinds holds
+// one box, not one per kind).
+struct P2gShared {
+    float num[3][kBoxFaces];
+    float den[3][kBoxFaces];
+    uint8_t mk[3][kBoxFaces];
+    uint16_t over[FE_TILE_CELLS];  // cells with more than kCellCap particles (tile-local index)
+    int nover;
+};
 
-    const int tile = blockIdx.x;
+template <int SOLVER>
+__device__ __forceinline__ void p2g_body(const SceneView& v, int tile, P2gShared& sh)
+{
+    float (&s_num)[3][kBoxFaces] = sh.num;
+    float (&s_den)[3][kBoxFaces] = sh.den;
+    uint8_t (&s_mk)[3][kBoxFaces] = sh.mk;
+    uint16_t* s_over = sh.over;
+    int& s_nover = sh.nover;
+
     const int tx = tile % v.g.tnx, ty = (tile / v.g.tnx) % v.g.tny, tz = tile / (v.g.tnx * v.g.tny);
     const int bx = tx * FE_TILE - 1, by = ty * FE_TILE - 1, bz = tz * FE_TILE - 1;  // box origin (face index)
     const uint32_t beg = v.cell_start[(uint32_t)tile * FE_TILE_CELLS];
@@ -411,11 +420,18 @@ __global__ void __launch_bounds__(kP2gThreads, 1) k_p2g(SceneView v)
     }
 }
 
+template <int SOLVER>
+__global__ void __launch_bounds__(kP2gThreads, 1) k_p2g(SceneView v)
+{
+    __shared__ P2gShared sh;
+    p2g_body<SOLVER>(v, (int)blockIdx.x, sh);
+}
+
 // u = num / weight where weight > 0 (pic_simulator.cpp:414-436); FLIP also snapshots the result.
 template <bool FLIP>
-__global__ void k_p2g_normalize(SceneView v, size_t nu, size_t nvv, size_t nww)
+__device__ __forceinline__ void normalize_body(const SceneView& v, size_t nu, size_t nvv, size_t nww, uint32_t blk)
 {
-    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t t = blk * (size_t)blockDim.x + threadIdx.x;
     const size_t total = nu + nvv + nww;
     if (t >= total) return;
     const float* num;
@@ -432,7 +448,50 @@ __global__ void k_p2g_normalize(SceneView v, size_t nu, size_t nvv, size_t nww)
     if (FLIP) snap[f] = val;
 }
 
+template <bool FLIP>
+__global__ void k_p2g_normalize(SceneView v, size_t nu, size_t nvv, size_t nww)
+{
+    normalize_body<FLIP>(v, nu, nvv, nww, blockIdx.x);
+}
+
+// ---- flat multi-scene forms (BatchPlan, fe_internal.cuh): every scene's tiles in one launch, each block running
+// its scene's transfer kind
+__global__ void __launch_bounds__(kP2gThreads, 1) k_multi_p2g(const BatchPlan* __restrict__ plan)
+{
+    __shared__ P2gShared sh;
+    __shared__ SceneView v;
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkP2g, b);
+    stage_view(v, plan->sc[s].dst);
+    if (v.solver == FE_SOLVER_PIC) p2g_body<FE_SOLVER_PIC>(v, (int)b, sh);
+    else if (v.solver == FE_SOLVER_FLIP) p2g_body<FE_SOLVER_FLIP>(v, (int)b, sh);
+    else p2g_body<FE_SOLVER_APIC>(v, (int)b, sh);
+}
+
+__global__ void __launch_bounds__(256) k_multi_p2g_normalize(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkNormalize, b);
+    const SceneView& v = plan->sc[s].dst;
+    const size_t nu = (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz, nvv = (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz,
+                 nww = (size_t)v.g.nx * v.g.ny * (v.g.nz + 1);
+    if (v.solver == FE_SOLVER_FLIP) normalize_body<true>(v, nu, nvv, nww, b);
+    else normalize_body<false>(v, nu, nvv, nww, b);
+}
+
 }  // namespace
+
+// Every scene's splat (accumulators cleared by launch_multi_clear) and normalisation: launch_p2g's passes.
+cudaError_t launch_multi_p2g(const BatchLaunch& L, cudaStream_t st)
+{
+    if (L.total[kBkP2g]) {
+        k_multi_p2g<<<L.total[kBkP2g], kP2gThreads, 0, st>>>(L.plan);
+        count_launch();
+    }
+    k_multi_p2g_normalize<<<L.total[kBkNormalize], 256, 0, st>>>(L.plan);
+    count_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_p2g(const SceneView& v, cudaStream_t st)
 {

@@ -2561,6 +2561,13 @@ int32_t fe_abi_version(void) { return 10600; }
 // scene's post-solve phase runs on its own stream again.  The whole batch substep is captured as one CUDA
 // graph (fork/join across the scenes' streams) per particle-buffer parity and replayed.
 
+// Scenes of at most this many cells join a batch's flat launches (fe_batch_set_flat).  Off by default: on the B200 the
+// per-scene form measured as fast or faster -- the scenes' passes on their own streams run concurrently, so one
+// scene's latency-bound pass overlaps another's bandwidth-bound one, while a flat launch runs one kind of pass at a
+// time for all scenes (48 scenes of 32^3..128^3: 10.45 ms per substep per-scene, 10.57 with scenes up to 48^3
+// flat, 12.44 all flat; 64 scenes of 24^3..48^3: 2.94 against 2.98).  autotune.tune_batch picks it per batch.
+constexpr int64_t kFlatMaxCellsDefault = 0;
+
 struct fe_batch {
     std::vector<fe_scene*> scenes;
     int device = 0;
@@ -2581,6 +2588,18 @@ struct fe_batch {
     bool overlap = false;
     bool shares_measured = false;      // shares re-split from measured solve work since the membership was set
     std::vector<int> share;
+    // flat launches: every transfer and grid pass of a substep launched once for all flat members over a (scene,
+    // block) work list (BatchPlan, fe_internal.cuh), one device plan per batch parity, on the batch stream, while the
+    // other scenes run their passes on their own streams
+    int64_t flat_max_cells = kFlatMaxCellsDefault;  // scenes up to this many cells run in the flat launches
+    std::vector<int> flat_members;   // indices (into scenes) of the scenes in the flat launches, in plan order
+    BatchPlan* plan_dev[2] = {nullptr, nullptr};
+    BatchLaunch launch[2] = {};
+    bool plan_valid = false;
+    double plan_dt = -1.0;
+    uint64_t plan_epoch = 0;
+    int plan_bparity = 0;             // the batch parity the scene parities below were recorded at
+    std::vector<int> plan_parity;     // each scene's particle parity at that batch parity
 };
 
 // A batch replays its scenes' own phase graphs around the multi-scene solve for its first
@@ -2589,6 +2608,170 @@ struct fe_batch {
 constexpr int64_t kBatchCaptureAfter = 8;
 
 namespace {
+
+// A scene can run in the flat launches when its substep is the plain sequence those launches implement.
+bool flat_scene_ok(const fe_scene* s)
+{
+    return s->desc.viscosity <= 0.0 && s->forces.count == 0 && s->colliders.count == 0 && s->emitters.empty();
+}
+
+bool flat_member(const fe_batch* b, const fe_scene* s)
+{
+    const int64_t cells = (int64_t)s->base.g.nx * s->base.g.ny * s->base.g.nz;
+    return !b->overlap && flat_scene_ok(s) && (b->flat_max_cells < 0 || cells <= b->flat_max_cells);
+}
+
+// Recomputes the flat members (after a membership or mode change).
+void batch_set_flat_members(fe_batch* b)
+{
+    b->flat_members.clear();
+    for (int i = 0; i < (int)b->scenes.size(); ++i)
+        if (flat_member(b, b->scenes[i])) b->flat_members.push_back(i);
+    b->plan_valid = false;
+}
+
+bool batch_flat(const fe_batch* b) { return !b->flat_members.empty(); }
+bool is_flat(const fe_batch* b, int i)
+{
+    return std::binary_search(b->flat_members.begin(), b->flat_members.end(), i);
+}
+
+uint64_t batch_epoch(const fe_batch* b)
+{
+    uint64_t epoch = 0;
+    for (const fe_scene* s : b->scenes) epoch += s->epoch;
+    return epoch;
+}
+
+// The flat plans of both batch parities for the current membership, scene parities and dt (copied to the device
+// after the batch stream has drained, so no launch of an earlier plan can still read it).  No device allocation.
+fe_status batch_build_plans(fe_batch* b, double dt)
+{
+    const int S = (int)b->scenes.size();
+    const int F = (int)b->flat_members.size();
+    FE_CUDA(cudaStreamSynchronize(b->stream));
+    std::unique_ptr<BatchPlan> hp(new (std::nothrow) BatchPlan());
+    if (!hp) return set_error(FE_ERR_OOM, "host allocation failed");
+    for (int q = 0; q < 2; ++q) {
+        BatchPlan& P = *hp;
+        std::memset(&P, 0, sizeof(BatchPlan));
+        P.count = F;
+        BatchLaunch& L = b->launch[q];
+        L = BatchLaunch{};
+        for (int i = 0; i < F; ++i) {
+            fe_scene* s = b->scenes[b->flat_members[i]];
+            const int par = s->parity ^ q ^ b->parity;
+            BatchScene& e = P.sc[i];
+            e.src = view_of(s, par);
+            e.dst = view_of(s, par ^ 1);
+            const SceneView& v = e.dst;
+            const uint32_t K = v.g.key_space;
+            e.scan_blocks = sort_batch_blocks(v, kBkScan);
+            if (sort_scan_tmp_bytes(K) > s->scan_tmp_bytes) return set_error(FE_ERR_STATE, "scan scratch too small");
+            e.scan_sums = (uint32_t*)s->scan_tmp;
+            e.long_count = e.scan_sums + e.scan_blocks + 1;
+            const size_t nu = (size_t)(v.g.nx + 1) * v.g.ny * v.g.nz, nvv = (size_t)v.g.nx * (v.g.ny + 1) * v.g.nz,
+                         nww = (size_t)v.g.nx * v.g.ny * (v.g.nz + 1), faces = nu + nvv + nww;
+            const size_t cells = (size_t)v.g.nx * v.g.ny * v.g.nz;
+            int r = 0;
+            auto range = [&](void* ptr, uint64_t bytes, uint32_t val) {
+                e.clr_ptr[r] = (uint8_t*)ptr;
+                e.clr_bytes[r] = bytes;
+                e.clr_val[r] = val;
+                ++r;
+            };
+            // launch_sort's count clear, launch_p2g's accumulator clears, launch_mark's mark (and crit) clears: all
+            // these buffers are dead between substeps
+            range(v.cell_count, (uint64_t)K * sizeof(uint32_t), 0);
+            range(v.nu, faces * sizeof(float), 0);
+            range(v.du, faces * sizeof(float), 0);
+            range(v.mu, faces, 0);
+            range(v.marks, cells, FE_CELL_AIR);
+            if (v.any_inexact) {
+                range(v.crit_flag, (cells + 3) & ~(size_t)3, 0);
+                range(v.crit_count, sizeof(uint32_t), 0);
+            }
+            e.nclr = r;
+            uint64_t clear_bytes = 0;
+            for (int k = 0; k < r; ++k) clear_bytes += e.clr_bytes[k];
+            e.gdt[0] = (float)(dt * v.gravity[0]);
+            e.gdt[1] = (float)(dt * v.gravity[1]);
+            e.gdt[2] = (float)(dt * v.gravity[2]);
+            mark_constants(v, &e.R2, &e.rin2, &e.crit_eps);
+            e.g2p = g2p_args(v, dt);
+            for (int k = 0; k < kBkCount; ++k) {
+                // a block clears 256 threads x 16 B x 8 per pass of its range loop
+                const uint32_t n = k == kBkClear ? (uint32_t)std::max<uint64_t>(1, (clear_bytes + 32767) / 32768)
+                                                 : batch_blocks(v, k);
+                P.start[k][i + 1] = P.start[k][i] + n;
+            }
+            L.max_depth = std::max(L.max_depth, v.extrap_depth);
+            L.any_particles |= v.np > 0;
+        }
+        for (int k = 0; k < kBkCount; ++k) L.total[k] = P.start[k][F];
+        L.plan = b->plan_dev[q];
+        FE_CUDA(cudaMemcpy(b->plan_dev[q], &P, sizeof(BatchPlan), cudaMemcpyHostToDevice));
+    }
+    b->plan_parity.resize(S);
+    for (int i = 0; i < S; ++i) b->plan_parity[i] = b->scenes[i]->parity;
+    b->plan_bparity = b->parity;
+    b->plan_dt = dt;
+    b->plan_epoch = batch_epoch(b);
+    b->plan_valid = true;
+    return FE_OK;
+}
+
+// True when the plans match the batch's current state (membership, dt, scene epochs and particle parities).
+bool batch_plans_current(const fe_batch* b, double dt)
+{
+    if (!b->plan_valid || b->plan_dt != dt || b->plan_epoch != batch_epoch(b)) return false;
+    const int flip = b->parity ^ b->plan_bparity;
+    for (size_t i = 0; i < b->scenes.size(); ++i)
+        if (b->scenes[i]->parity != (b->plan_parity[i] ^ flip)) return false;
+    return true;
+}
+
+// The flat members' pre-solve passes on the batch stream: the clears, the sort and gather, P2G, marking, the pre
+// group and the right-hand side, each one launch for all of them.
+fe_status batch_flat_pre(fe_batch* b)
+{
+    if (!batch_flat(b)) return FE_OK;
+    const BatchLaunch& L = b->launch[b->parity];
+    cudaStream_t st = b->stream;
+    FE_CUDA(launch_multi_clear(L, st));
+    FE_CUDA(launch_multi_sort(L, st));
+    FE_CUDA(launch_multi_p2g(L, st));
+    FE_CUDA(launch_multi_mark(L, st));
+    FE_CUDA(launch_multi_pre(L, st));
+    FE_CUDA(launch_multi_rhs(L, st));
+    return FE_OK;
+}
+
+// The flat members' post-solve passes on the batch stream: the pressure apply, the post group and the transfer +
+// move.
+fe_status batch_flat_post(fe_batch* b)
+{
+    if (!batch_flat(b)) return FE_OK;
+    const BatchLaunch& L = b->launch[b->parity];
+    cudaStream_t st = b->stream;
+    FE_CUDA(launch_multi_apply(L, st));
+    FE_CUDA(launch_multi_post(L, st));
+    FE_CUDA(launch_multi_g2p(L, st));
+    return FE_OK;
+}
+
+// Host bookkeeping after a batch substep was enqueued: every scene's sort flipped its particle buffer sets.
+void batch_after_substep(fe_batch* b)
+{
+    for (fe_scene* s : b->scenes) {
+        s->parity ^= 1;
+        s->prev_valid = true;
+        s->mesh_sdf = false;
+        s->collider_built = true;
+        s->grid_cur = 0;
+    }
+    b->parity ^= 1;
+}
 
 void batch_drop_graphs(fe_batch* b)
 {
@@ -2605,49 +2788,86 @@ void batch_drop_graphs(fe_batch* b)
 // run concurrently on their own streams.
 cudaStream_t pre_stream(const fe_batch* b, const fe_scene* s) { return s->desc.viscosity > 0.0 ? b->stream : s->stream; }
 
-// Enqueues one batch substep on b->stream with fork/join over the scenes' streams.
-fe_status batch_enqueue(fe_batch* b, double dt)
+// One batch substep on b->stream: the scenes outside the flat launches run their pre-solve passes on their own
+// streams (forked from the batch stream; viscous scenes one after another on the batch stream), concurrently with the
+// flat launches of the flat members on the batch stream; all join before the multi-scene solve; then the same for
+// the post-solve passes.  scene_graphs replays the forked scenes' own phase graphs (young batches, profiled steps);
+// otherwise their steps are enqueued directly (the batch graph's capture).  The flat plans must be current.  `ev`
+// (optional) gets events before, between and after the three phases.
+fe_status batch_enqueue_mixed(fe_batch* b, double dt, bool scene_graphs, cudaEvent_t* ev)
 {
     const int S = (int)b->scenes.size();
     cudaEvent_t fork0 = b->events[2 * S], fork1 = b->events[2 * S + 1];
+    if (ev) FE_CUDA(cudaEventRecord(ev[0], b->stream));
     FE_CUDA(cudaEventRecord(fork0, b->stream));
-    // forked scenes first, then the viscous ones on the batch stream, then the joins (a join enqueued before a
-    // viscous scene's steps would make them wait for the forked scene)
-    for (int pass = 0; pass < 3; ++pass)
-        for (int i = 0; i < S; ++i) {
-            fe_scene* s = b->scenes[i];
-            const cudaStream_t ps = pre_stream(b, s);
-            if (pass == 0 && ps != b->stream) {
-                FE_CUDA(cudaStreamWaitEvent(ps, fork0, 0));
-                fe_status st = enqueue_steps(s, dt, kStepSort, kStepRhs, ps);
-                if (st != FE_OK) return st;
-                FE_CUDA(cudaEventRecord(b->events[2 * i], ps));
-            } else if (pass == 1 && ps == b->stream) {
-                fe_status st = enqueue_steps(s, dt, kStepSort, kStepRhs, ps);
-                if (st != FE_OK) return st;
-            } else if (pass == 2 && ps != b->stream) {
-                FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
-            }
-        }
-    FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
-    FE_CUDA(cudaEventRecord(fork1, b->stream));
+    auto pre = [&](fe_scene* s, cudaStream_t ps) -> fe_status {
+        if (!scene_graphs) return enqueue_steps(s, dt, kStepSort, kStepRhs, ps);
+        FE_CUDA(cudaGraphLaunch(s->graph[s->parity][0], ps));
+        g_launches += s->graph_kernels[s->parity][0];
+        return FE_OK;
+    };
+    // forked scenes first, then the viscous ones and the flat launches on the batch stream, then the joins (a join
+    // enqueued earlier would make the batch stream's work wait for the forked scenes)
     for (int i = 0; i < S; ++i) {
         fe_scene* s = b->scenes[i];
-        FE_CUDA(cudaStreamWaitEvent(s->stream, fork1, 0));
-        fe_status st = enqueue_steps(s, dt, kStepApply, kStepMove);
+        const cudaStream_t ps = pre_stream(b, s);
+        if (is_flat(b, i) || ps == b->stream) continue;
+        FE_CUDA(cudaStreamWaitEvent(ps, fork0, 0));
+        fe_status st = pre(s, ps);
         if (st != FE_OK) return st;
-        FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
-        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
+        FE_CUDA(cudaEventRecord(b->events[2 * i], ps));
     }
+    for (int i = 0; i < S; ++i) {
+        fe_scene* s = b->scenes[i];
+        if (is_flat(b, i) || pre_stream(b, s) != b->stream) continue;
+        fe_status st = pre(s, b->stream);
+        if (st != FE_OK) return st;
+    }
+    fe_status st = batch_flat_pre(b);
+    if (st != FE_OK) return st;
+    for (int i = 0; i < S; ++i)
+        if (!is_flat(b, i) && pre_stream(b, b->scenes[i]) != b->stream)
+            FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
+    if (ev) FE_CUDA(cudaEventRecord(ev[1], b->stream));
+    FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
+    if (ev) FE_CUDA(cudaEventRecord(ev[2], b->stream));
+    FE_CUDA(cudaEventRecord(fork1, b->stream));
+    for (int i = 0; i < S; ++i) {
+        if (is_flat(b, i)) continue;
+        fe_scene* s = b->scenes[i];
+        FE_CUDA(cudaStreamWaitEvent(s->stream, fork1, 0));
+        if (scene_graphs) {
+            FE_CUDA(cudaGraphLaunch(s->graph[s->parity][2], s->stream));
+            g_launches += s->graph_kernels[s->parity][2];
+        } else {
+            st = enqueue_steps(s, dt, kStepApply, kStepMove);
+            if (st != FE_OK) return st;
+        }
+        FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
+    }
+    st = batch_flat_post(b);
+    if (st != FE_OK) return st;
+    for (int i = 0; i < S; ++i)
+        if (!is_flat(b, i)) FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
+    if (ev) FE_CUDA(cudaEventRecord(ev[3], b->stream));
     return FE_OK;
 }
 
-// One batch substep from the scenes' own captured phase graphs (pre-solve and post-solve, captured once
-// per scene and dt) around the multi-scene solve, forked and joined over the scenes' streams.
+// Enqueues one batch substep on b->stream (the batch graph's capture).
+fe_status batch_enqueue(fe_batch* b, double dt) { return batch_enqueue_mixed(b, dt, false, nullptr); }
+
+// One batch substep launched directly: the forked scenes' own captured phase graphs (pre-solve and post-solve,
+// captured once per scene and dt) and the flat launches around the multi-scene solve.
 fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = nullptr)
 {
     const int S = (int)b->scenes.size();
-    for (fe_scene* s : b->scenes) {
+    if (batch_flat(b) && !batch_plans_current(b, dt)) {
+        fe_status st = batch_build_plans(b, dt);
+        if (st != FE_OK) return st;
+    }
+    for (int i = 0; i < S; ++i) {
+        if (is_flat(b, i)) continue;
+        fe_scene* s = b->scenes[i];
         if (s->graph_dt != dt) {
             drop_graphs(s);
             s->graph_dt = dt;
@@ -2657,41 +2877,9 @@ fe_status batch_step_scene_graphs(fe_batch* b, double dt, cudaEvent_t* ev = null
             if (st != FE_OK) return st;
         }
     }
-    cudaEvent_t fork0 = b->events[2 * S], fork1 = b->events[2 * S + 1];
-    if (ev) FE_CUDA(cudaEventRecord(ev[0], b->stream));
-    FE_CUDA(cudaEventRecord(fork0, b->stream));
-    for (int pass = 0; pass < 3; ++pass)  // forked scenes, viscous scenes on the batch stream, joins
-        for (int i = 0; i < S; ++i) {
-            fe_scene* s = b->scenes[i];
-            const cudaStream_t ps = pre_stream(b, s);
-            if ((pass == 0 && ps != b->stream) || (pass == 1 && ps == b->stream)) {
-                if (pass == 0) FE_CUDA(cudaStreamWaitEvent(ps, fork0, 0));
-                FE_CUDA(cudaGraphLaunch(s->graph[s->parity][0], ps));
-                g_launches += s->graph_kernels[s->parity][0];
-                if (pass == 0) FE_CUDA(cudaEventRecord(b->events[2 * i], ps));
-            } else if (pass == 2 && ps != b->stream) {
-                FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i], 0));
-            }
-        }
-    if (ev) FE_CUDA(cudaEventRecord(ev[1], b->stream));
-    FE_CUDA(launch_multi_cg(b->table, S, b->total_blocks, b->stream));
-    if (ev) FE_CUDA(cudaEventRecord(ev[2], b->stream));
-    FE_CUDA(cudaEventRecord(fork1, b->stream));
-    for (int i = 0; i < S; ++i) {
-        fe_scene* s = b->scenes[i];
-        FE_CUDA(cudaStreamWaitEvent(s->stream, fork1, 0));
-        FE_CUDA(cudaGraphLaunch(s->graph[s->parity][2], s->stream));
-        g_launches += s->graph_kernels[s->parity][2];
-        FE_CUDA(cudaEventRecord(b->events[2 * i + 1], s->stream));
-        FE_CUDA(cudaStreamWaitEvent(b->stream, b->events[2 * i + 1], 0));
-        s->parity ^= 1;  // the pre-solve graph's sort flipped the particle buffer sets
-        s->prev_valid = true;
-        s->mesh_sdf = false;
-        s->collider_built = true;
-        s->grid_cur = 0;
-    }
-    if (ev) FE_CUDA(cudaEventRecord(ev[3], b->stream));
-    b->parity ^= 1;
+    fe_status st = batch_enqueue_mixed(b, dt, true, ev);
+    if (st != FE_OK) return st;
+    batch_after_substep(b);  // every scene's sort flipped its particle buffer sets
     return FE_OK;
 }
 
@@ -2809,6 +2997,7 @@ fe_status batch_set_members(fe_batch* b, fe_scene* const* scenes, int32_t count)
     b->scenes.assign(scenes, scenes + count);
     b->total_blocks = start;
     b->steps_done = 0;
+    batch_set_flat_members(b);
     b->share = nblk;
     b->shares_measured = false;
     return FE_OK;
@@ -2947,6 +3136,8 @@ fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_check(e, "stream create"));
     if ((e = dalloc(b->allocs, &b->table, kBatchMaxScenes, dev, b->stream)) != cudaSuccess ||
+        (e = dalloc(b->allocs, &b->plan_dev[0], 1, dev, b->stream)) != cudaSuccess ||
+        (e = dalloc(b->allocs, &b->plan_dev[1], 1, dev, b->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
         return fail(cuda_check(e, "batch allocation"));
     fe_status st = batch_set_members(b, scenes, count);
@@ -2963,6 +3154,20 @@ fe_status fe_batch_set_overlap(fe_batch* b, int32_t on)
     FE_CUDA(cudaStreamSynchronize(b->stream));
     if (b->overlap != (on != 0)) {
         b->overlap = on != 0;
+        batch_set_flat_members(b);
+        batch_drop_graphs(b);
+    }
+    return FE_OK;
+}
+
+fe_status fe_batch_set_flat(fe_batch* b, int64_t max_cells)
+{
+    if (!b) return set_error(FE_ERR_BAD_ARG, "null batch");
+    FE_CUDA(cudaSetDevice(b->device));
+    FE_CUDA(cudaStreamSynchronize(b->stream));
+    if (b->flat_max_cells != max_cells) {
+        b->flat_max_cells = max_cells;
+        batch_set_flat_members(b);
         batch_drop_graphs(b);
     }
     return FE_OK;
@@ -3057,12 +3262,18 @@ fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* sta
             if (st != FE_OK) return st;
             batch_drop_graphs(b);
         }
-        uint64_t epoch = 0;
-        for (const fe_scene* s : b->scenes) epoch += s->epoch;
+        const uint64_t epoch = batch_epoch(b);
         if (b->graph_dt != dt || b->graph_epoch != epoch) {
             batch_drop_graphs(b);
             b->graph_dt = dt;
             b->graph_epoch = epoch;
+        }
+        if (batch_flat(b) && !batch_plans_current(b, dt)) {
+            batch_drop_graphs(b);
+            b->graph_dt = dt;
+            b->graph_epoch = epoch;
+            fe_status st = batch_build_plans(b, dt);
+            if (st != FE_OK) return st;
         }
         const int par = b->parity;
         if (!b->graph[par]) {

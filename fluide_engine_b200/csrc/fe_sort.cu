@@ -27,14 +27,16 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__global__ void k_keys(SceneView v)
+__device__ __forceinline__ void keys_body(const SceneView& v, uint32_t blk)
 {
-    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t i = blk * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= v.np) return;
     uint32_t key = fe_particle_key(v.px[i], v.py[i], v.pz[i], v.originf, v.inv_hf, v.g.nx, v.g.ny, v.g.nz);
     v.key[i] = key;
     v.rank[i] = atomicAdd(v.cell_count + key, 1u);
 }
+
+__global__ void k_keys(SceneView v) { keys_body(v, blockIdx.x); }
 
 // Inclusive block scan of one value per thread; returns the block total through *total.
 __device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* warp_sums, uint32_t* total)
@@ -63,24 +65,29 @@ __device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* warp_s
     return x + before;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_partials(const uint32_t* __restrict__ in, uint32_t n,
-                                                                  uint32_t* __restrict__ block_sums)
+__device__ __forceinline__ void scan_partials_body(const uint32_t* __restrict__ in, uint32_t n,
+                                                   uint32_t* __restrict__ block_sums, uint32_t blk, uint32_t* ws)
 {
-    __shared__ uint32_t ws[32];
-    uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint64_t base = (uint64_t)blk * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t s = 0;
 #pragma unroll
     for (int t = 0; t < kScanItems; ++t)
         if (base + t < n) s += in[base + t];
     uint32_t total;
     block_incl_scan(s, ws, &total);
-    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+    if (threadIdx.x == 0) block_sums[blk] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_partials(const uint32_t* __restrict__ in, uint32_t n,
+                                                                  uint32_t* __restrict__ block_sums)
+{
+    __shared__ uint32_t ws[32];
+    scan_partials_body(in, n, block_sums, blockIdx.x, ws);
 }
 
 // Exclusive scan of the block sums by a single block, looping over chunks of kScanTile.
-__global__ void __launch_bounds__(kScanThreads) k_scan_block_sums(uint32_t* __restrict__ sums, uint32_t nb)
+__device__ __forceinline__ void scan_block_sums_body(uint32_t* __restrict__ sums, uint32_t nb, uint32_t* ws)
 {
-    __shared__ uint32_t ws[32];
     uint32_t carry = 0;
     for (uint32_t chunk = 0; chunk < nb; chunk += kScanTile) {
         uint32_t base = chunk + threadIdx.x * kScanItems;
@@ -103,12 +110,17 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_block_sums(uint32_t* __re
     }
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_final(const uint32_t* __restrict__ in, uint32_t n,
-                                                               const uint32_t* __restrict__ block_off,
-                                                               uint32_t* __restrict__ out)
+__global__ void __launch_bounds__(kScanThreads) k_scan_block_sums(uint32_t* __restrict__ sums, uint32_t nb)
 {
     __shared__ uint32_t ws[32];
-    uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    scan_block_sums_body(sums, nb, ws);
+}
+
+__device__ __forceinline__ void scan_final_body(const uint32_t* __restrict__ in, uint32_t n,
+                                                const uint32_t* __restrict__ block_off, uint32_t* __restrict__ out,
+                                                uint32_t blk, uint32_t* ws)
+{
+    uint64_t base = (uint64_t)blk * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t vals[kScanItems];
     uint32_t s = 0;
 #pragma unroll
@@ -118,7 +130,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const uint32_t* __r
     }
     uint32_t total;
     uint32_t incl = block_incl_scan(s, ws, &total);
-    uint32_t run = block_off[blockIdx.x] + incl - s;
+    uint32_t run = block_off[blk] + incl - s;
 #pragma unroll
     for (int t = 0; t < kScanItems; ++t) {
         if (base + t < n) out[base + t] = run;
@@ -127,25 +139,35 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const uint32_t* __r
     if (base + kScanItems >= n && base < n) out[n] = run;  // the thread holding the last element writes the total
 }
 
+__global__ void __launch_bounds__(kScanThreads) k_scan_final(const uint32_t* __restrict__ in, uint32_t n,
+                                                               const uint32_t* __restrict__ block_off,
+                                                               uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t ws[32];
+    scan_final_body(in, n, block_off, out, blockIdx.x, ws);
+}
+
 // After the scan the per-cell counts are dead until the next sort, so cell_count doubles as the list of
 // long runs (their keys, at most key_space of them); how many there are is counted in the word after the
 // scan's block sums (scan scratch holds nb + 2 words).
 constexpr uint32_t kBigCell = 1024;
 constexpr int kBigCellBlocks = 32;
 
-__global__ void k_place(SceneView v, uint32_t* __restrict__ long_count)
+__device__ __forceinline__ void place_body(const SceneView& v, uint32_t* __restrict__ long_count, uint32_t blk)
 {
-    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t i = blk * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= v.np) return;
     if (i == 0) *long_count = 0u;  // the long-run list starts empty
     v.perm[v.cell_start[v.key[i]] + v.rank[i]] = (uint32_t)i;
 }
 
+__global__ void k_place(SceneView v, uint32_t* __restrict__ long_count) { place_body(v, long_count, blockIdx.x); }
+
 // rank[final slot of particle x] = x (rank's atomic slots were consumed by k_place; perm, the runs in arbitrary
 // order, is only read here).
-__global__ void k_cellrank(SceneView v, uint32_t* __restrict__ long_count)
+__device__ __forceinline__ void cellrank_body(const SceneView& v, uint32_t* __restrict__ long_count, uint32_t blk)
 {
-    uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t s = blk * (uint64_t)blockDim.x + threadIdx.x;
     if (s >= v.np) return;
     const uint32_t* __restrict__ perm = v.perm;
     const uint32_t x = perm[s];
@@ -160,14 +182,17 @@ __global__ void k_cellrank(SceneView v, uint32_t* __restrict__ long_count)
     v.rank[b + r] = x;
 }
 
+__global__ void k_cellrank(SceneView v, uint32_t* __restrict__ long_count) { cellrank_body(v, long_count, blockIdx.x); }
+
 // One block per listed long run.  Ascending-only bitonic network (each merge of size k starts with the
 // mirrored comparator i <-> i ^ (k - 1), then half-cleaners of distance k/4 .. 1) over the run padded to
 // a power of two; padded positions count as +infinity, so a pair whose upper element is past the run's
 // end never swaps and is skipped.  Sorted in place in perm, then copied to the run's slots of rank.
-__global__ void __launch_bounds__(1024) k_bigcell(SceneView v, const uint32_t* __restrict__ long_count)
+__device__ __forceinline__ void bigcell_body(const SceneView& v, const uint32_t* __restrict__ long_count, uint32_t blk,
+                                             uint32_t nblk)
 {
     const uint32_t count = *long_count;
-    for (uint32_t li = blockIdx.x; li < count; li += gridDim.x) {
+    for (uint32_t li = blk; li < count; li += nblk) {
         const uint32_t key = v.cell_count[li];
         const uint32_t b = v.cell_start[key], n = v.cell_start[key + 1] - b;
         uint32_t* a = v.perm + b;
@@ -194,14 +219,19 @@ __global__ void __launch_bounds__(1024) k_bigcell(SceneView v, const uint32_t* _
     }
 }
 
+__global__ void __launch_bounds__(1024) k_bigcell(SceneView v, const uint32_t* __restrict__ long_count)
+{
+    bigcell_body(v, long_count, blockIdx.x, gridDim.x);
+}
+
 // Each thread moves kGatherBatch particles, all their loads issued before any store, so a thread keeps several
 // rows of requests in flight instead of one.
 constexpr int kGatherBatch = 4;
 
 template <bool APIC>
-__global__ void __launch_bounds__(256) k_gather(SceneView src, SceneView dst)
+__device__ __forceinline__ void gather_body(const SceneView& src, const SceneView& dst, uint32_t blk)
 {
-    const uint64_t base = (blockIdx.x * (uint64_t)blockDim.x) * kGatherBatch + threadIdx.x;
+    const uint64_t base = (blk * (uint64_t)blockDim.x) * kGatherBatch + threadIdx.x;
     uint32_t j[kGatherBatch];
     bool ok[kGatherBatch];
 #pragma unroll
@@ -248,6 +278,70 @@ __global__ void __launch_bounds__(256) k_gather(SceneView src, SceneView dst)
     }
 }
 
+template <bool APIC>
+__global__ void __launch_bounds__(256) k_gather(SceneView src, SceneView dst)
+{
+    gather_body<APIC>(src, dst, blockIdx.x);
+}
+
+// ---- flat multi-scene forms: one launch per pass for every scene of a batch (BatchPlan, fe_internal.cuh)
+
+__global__ void __launch_bounds__(256) k_multi_keys(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkPart, b);
+    keys_body(plan->sc[s].src, b);
+}
+
+template <int PASS>  // 0: partial sums, 2: final
+__global__ void __launch_bounds__(kScanThreads) k_multi_scan(const BatchPlan* __restrict__ plan)
+{
+    __shared__ uint32_t ws[32];
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkScan, b);
+    const BatchScene& e = plan->sc[s];
+    if (PASS == 0) scan_partials_body(e.src.cell_count, e.src.g.key_space, e.scan_sums, b, ws);
+    else scan_final_body(e.src.cell_count, e.src.g.key_space, e.scan_sums, e.src.cell_start, b, ws);
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_multi_scan_sums(const BatchPlan* __restrict__ plan)
+{
+    __shared__ uint32_t ws[32];
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkScanSums, b);
+    scan_block_sums_body(plan->sc[s].scan_sums, plan->sc[s].scan_blocks, ws);
+}
+
+__global__ void __launch_bounds__(256) k_multi_place(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkPart, b);
+    place_body(plan->sc[s].src, plan->sc[s].long_count, b);
+}
+
+__global__ void __launch_bounds__(256) k_multi_cellrank(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkPart, b);
+    cellrank_body(plan->sc[s].src, plan->sc[s].long_count, b);
+}
+
+__global__ void __launch_bounds__(1024) k_multi_bigcell(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkBigcell, b);
+    bigcell_body(plan->sc[s].src, plan->sc[s].long_count, b, plan->start[kBkBigcell][s + 1] - plan->start[kBkBigcell][s]);
+}
+
+__global__ void __launch_bounds__(256) k_multi_gather(const BatchPlan* __restrict__ plan)
+{
+    uint32_t b;
+    const int s = batch_scene_of(plan, kBkGather, b);
+    const BatchScene& e = plan->sc[s];
+    if (e.src.solver == FE_SOLVER_APIC) gather_body<true>(e.src, e.dst, b);
+    else gather_body<false>(e.src, e.dst, b);
+}
+
 }  // namespace
 
 // block sums (nb words), one spare, and the long-run counter
@@ -291,6 +385,40 @@ cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, siz
         k_cellrank<<<pb, T, 0, st>>>(v, long_count);
         k_bigcell<<<kBigCellBlocks, 1024, 0, st>>>(v, long_count);
         count_launch(3);
+    }
+    return cudaGetLastError();
+}
+
+// Blocks of the sort's passes in a batch: kBkBigcell gets a few blocks per scene (long runs are rare).
+constexpr uint32_t kMultiBigCellBlocks = 4;
+
+uint32_t sort_batch_blocks(const SceneView& v, int kind)
+{
+    switch (kind) {
+    case kBkGather: return (uint32_t)((v.np + 256 * kGatherBatch - 1) / (256 * kGatherBatch));
+    case kBkScan: return (v.g.key_space + kScanTile - 1) / kScanTile;
+    case kBkScanSums: return 1;
+    case kBkBigcell: return v.np > 0 ? kMultiBigCellBlocks : 0;
+    default: return 0;
+    }
+}
+
+// The sort of every scene: keys, the scan of the cell counts (cleared by launch_multi_clear), placement, ranks and
+// long runs, then the gather into the scenes' other buffer sets -- the passes of launch_sort + launch_gather.
+cudaError_t launch_multi_sort(const BatchLaunch& L, cudaStream_t st)
+{
+    const BatchPlan* p = L.plan;
+    if (L.total[kBkPart]) k_multi_keys<<<L.total[kBkPart], 256, 0, st>>>(p);
+    k_multi_scan<0><<<L.total[kBkScan], kScanThreads, 0, st>>>(p);
+    k_multi_scan_sums<<<L.total[kBkScanSums], kScanThreads, 0, st>>>(p);
+    k_multi_scan<2><<<L.total[kBkScan], kScanThreads, 0, st>>>(p);
+    count_launch(4);
+    if (L.total[kBkPart]) {
+        k_multi_place<<<L.total[kBkPart], 256, 0, st>>>(p);
+        k_multi_cellrank<<<L.total[kBkPart], 256, 0, st>>>(p);
+        k_multi_bigcell<<<L.total[kBkBigcell], 1024, 0, st>>>(p);
+        k_multi_gather<<<L.total[kBkGather], 256, 0, st>>>(p);
+        count_launch(4);
     }
     return cudaGetLastError();
 }

@@ -336,7 +336,9 @@ class Snapshot:
 
 
 class Batch:
-    """Many scenes advanced together (fe_batch_*): one batched pressure solve per substep, one CUDA graph."""
+    """Many scenes advanced together (fe_batch_*): one batched pressure solve per substep; the small scenes' transfer
+    and grid passes as one launch per pass for all of them, the larger scenes' on their own streams; one CUDA
+    graph per substep."""
 
     def __init__(self, scenes):
         self.scenes = list(scenes)
@@ -350,6 +352,17 @@ class Batch:
         """Overlap mode (fe_batch_set_overlap): each scene's whole substep on its own stream, its solve on its
         share of the solver blocks, so solves overlap other scenes' transfer kernels."""
         check(self._L.fe_batch_set_overlap(self._h, 1 if on else 0))
+
+    def set_flat(self, max_cells=-1):
+        """Scenes of at most max_cells cells run every pre- and post-solve pass as one launch for all of them over a
+        (scene, block) work list (fe_batch_set_flat); larger scenes run their passes on their own streams.  0 (the
+        library's default): no scene in the flat launches; -1: every scene.  True / False select -1 / 0.
+        autotune.tune_batch picks the threshold by timing."""
+        if max_cells is True:
+            max_cells = -1
+        elif max_cells is False:
+            max_cells = 0
+        check(self._L.fe_batch_set_flat(self._h, int(max_cells)))
 
     def set_scenes(self, scenes):
         """Changes the batch's scenes in place (no device allocation)."""

@@ -68,7 +68,7 @@ class Server:
     """
 
     def __init__(self, hbm_budget_bytes, max_batch=32, device=0, cg_rel_tol=1e-6, seed_threads=4,
-                 reuse_scenes=True, overlap=False, batch_family=None):
+                 reuse_scenes=True, overlap=False, batch_family=None, flat_max_cells=None):
         self.budget = int(hbm_budget_bytes)
         self.max_batch = min(int(max_batch), 64)
         self.device = device
@@ -81,6 +81,9 @@ class Server:
         if batch_family not in (None, "cg"):
             raise ValueError("batch_family is None or 'cg'")
         self.batch_family = batch_family
+        # scenes of at most this many cells run in the batches' flat launches (Batch.set_flat); None keeps the
+        # library's default
+        self.flat_max_cells = flat_max_cells
         self.seed_threads = max(1, int(seed_threads))
         self.used = 0            # bytes of live scenes (running, pooled, being prepared or released)
         self.reserved = 0        # bytes reserved for preparations that need a new scene
@@ -237,6 +240,8 @@ class Server:
                 b = Batch([j.scene for j in jobs])
                 if self.overlap:
                     b.set_overlap(True)
+                if self.flat_max_cells is not None:
+                    b.set_flat(self.flat_max_cells)
                 b.step(dt, nsub, stats=False)
                 b.close()
             out.append((jobs, nsub, (time.perf_counter() - f0) * 1e3))
@@ -335,6 +340,8 @@ class Server:
                         self.batch = Batch([j.scene for j in self.running])
                         if self.overlap:
                             self.batch.set_overlap(True)
+                        if self.flat_max_cells is not None:
+                            self.batch.set_flat(self.flat_max_cells)
                     else:
                         self.batch.set_scenes([j.scene for j in self.running])
                     self.rebuilds += 1

@@ -366,13 +366,16 @@ fe_status fe_snapshot_destroy(fe_snapshot* snap);
 fe_status fe_scene_set_stream(fe_scene* s, void* stream);
 fe_status fe_scene_synchronize(fe_scene* s);
 
-/* Batches: many independent scenes (up to 64, one device) advanced together.  Per substep every scene's
- * pre-solve phase runs on its own stream, ONE cooperative launch solves all scenes' pressure systems (each
- * scene on its own block range, sized by particle count x grid extent, with its own grid barrier, so the scenes
- * iterate independently and concurrently), and every scene's post-solve phase runs on its own stream; the
- * batch substep is one captured CUDA graph.  Results equal each scene stepped alone (same algorithm, each
- * scene's own tolerances).  No reference counterpart: the reference runs one simulator per process
- * (PhysicsAnimation::AdvanceSingleFrame, physics_animation.cpp:17-21). */
+/* Batches: many independent scenes (up to 64, one device) advanced together.  Per substep ONE cooperative
+ * launch solves all scenes' pressure systems (each scene on its own block range, sized by its measured solve work,
+ * with its own grid barrier, so the scenes iterate independently and concurrently).  Around it, each scene runs its
+ * pre- and post-solve passes on its own stream, concurrently with the others; scenes selected by fe_batch_set_flat
+ * instead run every pre- and post-solve pass (clears, sort, gather, P2G, marking, extrapolation + boundary
+ * conditions + gravity, right-hand side; pressure apply, extrapolation + boundary conditions, transfer + move) as
+ * ONE launch for all of them over a flat (scene, block) work list on the batch stream.  The batch substep is one
+ * captured CUDA graph.  Scenes with viscosity or external forces always run their passes on their own streams.
+ * Results equal each scene stepped alone (same algorithm, each scene's own tolerances).  No reference counterpart:
+ * the reference runs one simulator per process (PhysicsAnimation::AdvanceSingleFrame, physics_animation.cpp:17-21). */
 typedef struct fe_batch fe_batch;
 fe_status fe_batch_create(fe_scene* const* scenes, int32_t count, fe_batch** out);
 fe_status fe_batch_destroy(fe_batch* b);
@@ -387,11 +390,17 @@ fe_status fe_batch_set_scenes(fe_batch* b, fe_scene* const* scenes, int32_t coun
  * scenes' transfer kernels.  Same results; ignored while any scene has viscosity (its cooperative Jacobi solve
  * stays alone).  fe_batch_step_profiled always runs the phase-separated form. */
 fe_status fe_batch_set_overlap(fe_batch* b, int32_t on);
+/* Which scenes run in the flat launches: those of at most max_cells cells; 0 (the default) puts every scene on its
+ * own stream, a negative value puts every scene (without viscosity or forces) in the flat launches.  Same results
+ * either way; which is faster depends on the mix (fluide_engine_b200.autotune.tune_batch times the choices on the
+ * batch's own substeps).  Waits for the batch's earlier work.  No reference counterpart. */
+fe_status fe_batch_set_flat(fe_batch* b, int64_t max_cells);
 /* nsub substeps of dt for every scene; stats (NULL or count * nsub entries, scene-major) as fe_scene_step. */
 fe_status fe_batch_step(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats);
 /* fe_batch_step with per-substep device timing of the batch's three phases (all scenes' pre-solve, the
- * multi-scene solve, all scenes' post-solve; events on the batch stream between the joins), replaying the
- * scenes' own phase graphs around the solve launch; phase_ms receives nsub * 3 floats; synchronises. */
+ * multi-scene solve, all scenes' post-solve; events on the batch stream between them), launching the flat passes
+ * directly (or, when the batch is not flat, replaying the scenes' own phase graphs around the solve launch);
+ * phase_ms receives nsub * 3 floats; synchronises. */
 fe_status fe_batch_step_profiled(fe_batch* b, double dt, int32_t nsub, fe_step_stats* stats, float* phase_ms);
 
 /* Number of kernels the library launched since load (counts graph-launched kernels too). */

@@ -58,3 +58,36 @@ def test_store_rejects_null_arguments():
     assert L.fe_tuning_store(0, None, 1, None) == _abi.FE_ERR_BAD_ARG
     with pytest.raises(Exception):
         autotune.store((8, 8), _abi.FLIP, {})
+
+
+def test_tune_batch_picks_the_fastest_threshold_and_applies_it():
+    from fluide_engine_b200 import autotune
+
+    # a stand-in batch whose substeps take a per-threshold time on a fake clock
+    cost = {0: 10.0, 4096: 9.0, 32768: 8.5, -1: 12.0}
+
+    class FakeBatch:
+        def __init__(self):
+            self.flat = None
+            self.calls = []
+            self.now = 0.0
+
+        def set_flat(self, c):
+            self.flat = c
+            self.calls.append(("flat", c))
+
+        def step(self, dt, nsub, stats=True):
+            self.calls.append(("step", nsub))
+            self.now += cost[self.flat] * 1e-3 * nsub
+
+    b = FakeBatch()
+    best, times = autotune.tune_batch(b, 1.0 / 240.0, substeps=3, candidates=tuple(cost), timer=lambda: b.now,
+                                      rounds=2)
+    assert best == 32768 and b.flat == 32768
+    for c, ms in cost.items():
+        assert abs(times[c] - ms) < 1e-9
+    # every candidate: one untimed substep (the graph's capture), then the timed ones; the second round visits the
+    # candidates in reverse order
+    assert b.calls[:3] == [("flat", 0), ("step", 1), ("step", 3)]
+    flats = [c for k, c in b.calls if k == "flat"]
+    assert flats == list(cost) + list(cost)[::-1] + [32768]
