@@ -30,103 +30,75 @@ struct FaceArrays {
 enum { kModePlain = 0, kModePre = 1, kModePost = 2 };
 
 
-// The loads of one face of an extrapolation pass: the face and its six neighbours (order i+1, i-1, j+1, j-1, k+1,
-// k-1).  Every validity byte and value is loaded before any is used -- the neighbours whether or not the face turns
-// out to need them -- so all are in flight together in one round trip instead of the face's own load followed by
-// its neighbours'.
-struct ExtrapFace {
-    FaceCoord fc;
-    bool ok;
-    float val, nval[6];
-    uint8_t valid, nvalid[6];
-};
-
-__device__ __forceinline__ void extrap_load(const FaceArrays& fa, int nx, int ny, int nz, Blk3 blk, ExtrapFace& e)
+// One column of faces (FaceColumn) of an extrapolation pass.  The face's own value and validity and those of its
+// k - 1 and k + 1 neighbours slide along the column (one new plane loaded per step); the i and j neighbours are
+// loaded per face.  Same arithmetic as extrap_store, neighbours summed in the same order (i+1, i-1, j+1, j-1, k+1,
+// k-1).
+template <int MODE>
+__device__ __forceinline__ void extrap_column(const FaceArrays& fa, int nx, int ny, int nz, bool write_valid,
+                                              float gx, float gy, float gz, Blk3 blk)
 {
-    e.ok = face_coord(nx, ny, nz, blk, e.fc);
-    if (!e.ok) return;
-    const int c = e.fc.c, i = e.fc.i, j = e.fc.j, k = e.fc.k, sx = e.fc.sx, sy = e.fc.sy, sz = e.fc.sz;
-    const size_t f = e.fc.f;
-    // select by value (a runtime index into the parameter arrays would spill them to local memory)
-    const float* in = c == 0 ? fa.in[0] : (c == 1 ? fa.in[1] : fa.in[2]);
-    const uint8_t* vin = c == 0 ? fa.vin[0] : (c == 1 ? fa.vin[1] : fa.vin[2]);
+    FaceColumn fc;
+    if (!column_coord(nx, ny, nz, blk, fc)) return;
+    const int c = fc.c, i = fc.i, j = fc.j, sx = fc.sx, sy = fc.sy, sz = fc.sz;
+    const float* __restrict__ in = c == 0 ? fa.in[0] : (c == 1 ? fa.in[1] : fa.in[2]);
+    const uint8_t* __restrict__ vin = c == 0 ? fa.vin[0] : (c == 1 ? fa.vin[1] : fa.vin[2]);
+    float* __restrict__ out = c == 0 ? fa.out[0] : (c == 1 ? fa.out[1] : fa.out[2]);
+    uint8_t* __restrict__ vout = c == 0 ? fa.vout[0] : (c == 1 ? fa.vout[1] : fa.vout[2]);
     const size_t sxy = (size_t)sx * sy;
-    const bool in_dom[6] = {i + 1 < sx, i > 0, j + 1 < sy, j > 0, k + 1 < sz, k > 0};
-    const long long off[6] = {1, -1, (long long)sx, -(long long)sx, (long long)sxy, -(long long)sxy};
-    e.val = in[f];
-    e.valid = vin[f];
-#pragma unroll
-    for (int n = 0; n < 6; ++n) {
-        e.nvalid[n] = in_dom[n] ? vin[(long long)f + off[n]] : (uint8_t)0;
-        e.nval[n] = in_dom[n] ? in[(long long)f + off[n]] : 0.f;
+    size_t f = (size_t)i + (size_t)sx * ((size_t)j + (size_t)sy * (size_t)fc.k0);
+    const bool ip = i + 1 < sx, im = i > 0, jp = j + 1 < sy, jm = j > 0;
+    const bool wall_ij = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1));
+    const float g = c == 0 ? gx : (c == 1 ? gy : gz);
+    float vm = 0.f, vc = in[f];
+    uint8_t am = 0, ac = vin[f];
+    if (fc.k0 > 0) {
+        vm = in[f - sxy];
+        am = vin[f - sxy];
     }
-}
-
-// An invalid face takes the mean of its valid neighbours; then the pass's tail (walls, gravity) and the stores.
-template <int MODE>
-__device__ __forceinline__ void extrap_store(const FaceArrays& fa, bool write_valid, float gx, float gy, float gz,
-                                             const ExtrapFace& e)
-{
-    const int c = e.fc.c, i = e.fc.i, j = e.fc.j, k = e.fc.k, sx = e.fc.sx, sy = e.fc.sy, sz = e.fc.sz;
-    const size_t f = e.fc.f;
-    float val = e.val;
-    uint8_t valid = e.valid;
-    if (!valid) {
-        float sum = 0.f;
-        unsigned count = 0;
-#pragma unroll
-        for (int n = 0; n < 6; ++n)
-            if (e.nvalid[n]) {
-                sum += e.nval[n];
-                ++count;
+    for (int k = fc.k0; k < fc.k1; ++k, f += sxy) {
+        const bool kp = k + 1 < sz;
+        const float vp = kp ? in[f + sxy] : 0.f;
+        const uint8_t ap = kp ? vin[f + sxy] : (uint8_t)0;
+        const uint8_t a0 = ip ? vin[f + 1] : (uint8_t)0, a1 = im ? vin[f - 1] : (uint8_t)0;
+        const uint8_t a2 = jp ? vin[f + sx] : (uint8_t)0, a3 = jm ? vin[f - sx] : (uint8_t)0;
+        const float v0 = ip ? in[f + 1] : 0.f, v1 = im ? in[f - 1] : 0.f;
+        const float v2 = jp ? in[f + sx] : 0.f, v3 = jm ? in[f - sx] : 0.f;
+        float val = vc;
+        uint8_t valid = ac;
+        if (!valid) {
+            float sum = 0.f;
+            unsigned count = 0;
+            if (a0) { sum += v0; ++count; }
+            if (a1) { sum += v1; ++count; }
+            if (a2) { sum += v2; ++count; }
+            if (a3) { sum += v3; ++count; }
+            if (ap) { sum += vp; ++count; }
+            if (am) { sum += vm; ++count; }
+            if (count > 0) {
+                val = sum / (float)count;
+                valid = 1;
             }
-        if (count > 0) {
-            val = sum / (float)count;
-            valid = 1;
         }
+        if (write_valid) vout[f] = valid;
+        if (MODE != kModePlain) {
+            const bool wall = wall_ij || (c == 2 && (k == 0 || k == sz - 1));
+            if (wall) val = 0.f;
+            else if (MODE == kModePre) val += g;
+        }
+        out[f] = val;
+        vm = vc;
+        am = ac;
+        vc = vp;
+        ac = ap;
     }
-    if (write_valid) (c == 0 ? fa.vout[0] : (c == 1 ? fa.vout[1] : fa.vout[2]))[f] = valid;
-    if (MODE != kModePlain) {
-        const bool wall = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1)) ||
-                          (c == 2 && (k == 0 || k == sz - 1));
-        if (wall) val = 0.f;
-        else if (MODE == kModePre) val += (c == 0 ? gx : (c == 1 ? gy : gz));
-    }
-    (c == 0 ? fa.out[0] : (c == 1 ? fa.out[1] : fa.out[2]))[f] = val;
 }
 
 template <int MODE>
-__device__ __forceinline__ void extrap_body(const FaceArrays& fa, int nx, int ny, int nz, bool write_valid, float gx,
-                                            float gy, float gz, Blk3 blk)
+__global__ void __launch_bounds__(kTileX * kTileY) k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid,
+                                                            float gx, float gy, float gz)
 {
-    ExtrapFace e;
-    extrap_load(fa, nx, ny, nz, blk, e);
-    if (e.ok) extrap_store<MODE>(fa, write_valid, gx, gy, gz, e);
-}
-
-// kFaceLayers consecutive face layers (blk.z .. blk.z + kFaceLayers - 1, below zend) per thread: all their loads are
-// issued before the first store, so a thread keeps several faces' round trips in flight.
-constexpr int kFaceLayers = 4;
-
-template <int MODE>
-__device__ __forceinline__ void extrap_layers(const FaceArrays& fa, int nx, int ny, int nz, bool write_valid,
-                                              float gx, float gy, float gz, Blk3 blk, unsigned zend)
-{
-    ExtrapFace e[kFaceLayers];
-#pragma unroll
-    for (int t = 0; t < kFaceLayers; ++t) {
-        e[t].ok = false;
-        if (blk.z + t < zend) extrap_load(fa, nx, ny, nz, Blk3{blk.x, blk.y, blk.z + t}, e[t]);
-    }
-#pragma unroll
-    for (int t = 0; t < kFaceLayers; ++t)
-        if (e[t].ok) extrap_store<MODE>(fa, write_valid, gx, gy, gz, e[t]);
-}
-
-template <int MODE>
-__global__ void k_extrap(FaceArrays fa, int nx, int ny, int nz, bool write_valid, float gx, float gy, float gz)
-{
-    extrap_body<MODE>(fa, nx, ny, nz, write_valid, gx, gy, gz, hw_blk3());
+    extrap_column<MODE>(fa, nx, ny, nz, write_valid, gx, gy, gz, hw_blk3());
 }
 
 __device__ __forceinline__ void rhs_body(const SceneView& v, const float* __restrict__ u, const float* __restrict__ vv,
@@ -161,32 +133,46 @@ __global__ void k_rhs(SceneView v, const float* __restrict__ u, const float* __r
     rhs_body(v, u, vv, w, hw_blk3());
 }
 
-__device__ __forceinline__ void apply_body(const SceneView& v, float* u, float* vv, float* w, Blk3 blk)
+// One column of faces (FaceColumn) of the pressure apply: indices advance by one plane per step.
+__device__ __forceinline__ void apply_column(const SceneView& v, float* u, float* vv, float* w, Blk3 blk)
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
-    FaceCoord fc;
-    if (!face_coord(nx, ny, nz, blk, fc)) return;
-    const double* p = v.p;
-    const int i = fc.i, j = fc.j, k = fc.k;
+    FaceColumn fc;
+    if (!column_coord(nx, ny, nz, blk, fc)) return;
+    const double* __restrict__ p = v.p;
+    const uint8_t* __restrict__ mk = v.marks;
+    const int i = fc.i, j = fc.j;
+    const size_t nxy = (size_t)nx * ny;
     if (fc.c == 0) {
         if (i < 1 || i > nx - 1) return;
-        const size_t cm = idx3(i - 1, j, k, nx, ny);
-        if (v.marks[cm] != FE_CELL_FLUID || v.marks[cm + 1] == FE_CELL_BOUNDRY) return;
-        u[fc.f] = (float)((double)u[fc.f] + v.inv_h[0] * (p[cm + 1] - p[cm]));
+        const double ih = v.inv_h[0];
+        const size_t fs = (size_t)(nx + 1) * ny;
+        size_t cm = idx3(i - 1, j, fc.k0, nx, ny), f = idx3(i, j, fc.k0, nx + 1, ny);
+        for (int k = fc.k0; k < fc.k1; ++k, cm += nxy, f += fs)
+            if (mk[cm] == FE_CELL_FLUID && mk[cm + 1] != FE_CELL_BOUNDRY)
+                u[f] = (float)((double)u[f] + ih * (p[cm + 1] - p[cm]));
     } else if (fc.c == 1) {
         if (j < 1 || j > ny - 1) return;
-        const size_t cm = idx3(i, j - 1, k, nx, ny);
-        if (v.marks[cm] != FE_CELL_FLUID || v.marks[cm + nx] == FE_CELL_BOUNDRY) return;
-        vv[fc.f] = (float)((double)vv[fc.f] + v.inv_h[1] * (p[cm + nx] - p[cm]));
+        const double ih = v.inv_h[1];
+        const size_t fs = (size_t)nx * (ny + 1);
+        size_t cm = idx3(i, j - 1, fc.k0, nx, ny), f = idx3(i, j, fc.k0, nx, ny + 1);
+        for (int k = fc.k0; k < fc.k1; ++k, cm += nxy, f += fs)
+            if (mk[cm] == FE_CELL_FLUID && mk[cm + nx] != FE_CELL_BOUNDRY)
+                vv[f] = (float)((double)vv[f] + ih * (p[cm + nx] - p[cm]));
     } else {
-        if (k < 1 || k > nz - 1) return;
-        const size_t cm = idx3(i, j, k - 1, nx, ny);
-        if (v.marks[cm] != FE_CELL_FLUID || v.marks[cm + (size_t)nx * ny] == FE_CELL_BOUNDRY) return;
-        w[fc.f] = (float)((double)w[fc.f] + v.inv_h[2] * (p[cm + (size_t)nx * ny] - p[cm]));
+        const double ih = v.inv_h[2];
+        const int k0 = max(fc.k0, 1), k1 = min(fc.k1, nz);  // faces k = 1 .. nz - 1
+        size_t cm = idx3(i, j, k0 - 1, nx, ny), f = idx3(i, j, k0, nx, ny);
+        for (int k = k0; k < k1; ++k, cm += nxy, f += nxy)
+            if (mk[cm] == FE_CELL_FLUID && mk[cm + nxy] != FE_CELL_BOUNDRY)
+                w[f] = (float)((double)w[f] + ih * (p[cm + nxy] - p[cm]));
     }
 }
 
-__global__ void k_apply(SceneView v, float* u, float* vv, float* w) { apply_body(v, u, vv, w, hw_blk3()); }
+__global__ void __launch_bounds__(kTileX * kTileY) k_apply(SceneView v, float* u, float* vv, float* w)
+{
+    apply_column(v, u, vv, w, hw_blk3());
+}
 
 __global__ void k_cfl(SceneView v, const float* __restrict__ u, const float* __restrict__ vv,
                       const float* __restrict__ w, double dt, unsigned long long* out_bits)
@@ -268,7 +254,7 @@ cudaError_t run_extrap_group(const SceneView& v, float* const src[3], float* con
             fa.vin[c] = vin[c];
             fa.vout[c] = vset[pass & 1][c];
         }
-        const dim3 grid = face_grid(v.g.nx, v.g.ny, v.g.nz), block(kTileX, kTileY);
+        const dim3 grid = column_grid(v.g.nx, v.g.ny, v.g.nz), block(kTileX, kTileY);
         if (last) k_extrap<MODE><<<grid, block, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, false, gx, gy, gz);
         else k_extrap<kModePlain><<<grid, block, 0, st>>>(fa, v.g.nx, v.g.ny, v.g.nz, true, 0.f, 0.f, 0.f);
         count_launch();
@@ -305,7 +291,7 @@ cudaError_t launch_extrap_faces(const SceneView& v, float* const src[3], float* 
             fa.vin[c] = vin[c];
             fa.vout[c] = vset[pass & 1][c];
         }
-        k_extrap<kModePlain><<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(
+        k_extrap<kModePlain><<<column_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(
             fa, v.g.nx, v.g.ny, v.g.nz, !last, 0.f, 0.f, 0.f);
         count_launch();
         for (int c = 0; c < 3; ++c) {
@@ -318,24 +304,28 @@ cudaError_t launch_extrap_faces(const SceneView& v, float* const src[3], float* 
 
 namespace {
 
-__device__ __forceinline__ void wall_tail_body(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g,
-                                               float gx, float gy, float gz, Blk3 blk)
+// One column of faces of the wall tail with no extrapolation: wall faces 0, every other face gains dt g (add_g).
+__device__ __forceinline__ void wall_tail_column(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g,
+                                                 float gx, float gy, float gz, Blk3 blk)
 {
-    FaceCoord fc;
-    if (!face_coord(nx, ny, nz, blk, fc)) return;
-    const int c = fc.c, i = fc.i, j = fc.j, k = fc.k, sx = fc.sx, sy = fc.sy, sz = fc.sz;
-    const size_t f = fc.f;
+    FaceColumn fc;
+    if (!column_coord(nx, ny, nz, blk, fc)) return;
+    const int c = fc.c, i = fc.i, j = fc.j, sx = fc.sx, sy = fc.sy, sz = fc.sz;
     float* a = c == 0 ? u : (c == 1 ? vv : w);
-    const bool wall = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1)) ||
-                      (c == 2 && (k == 0 || k == sz - 1));
-    if (wall) a[f] = 0.f;
-    else if (add_g) a[f] += (c == 0 ? gx : (c == 1 ? gy : gz));
+    const size_t sxy = (size_t)sx * sy;
+    size_t f = idx3(i, j, fc.k0, sx, sy);
+    const bool wall_ij = (c == 0 && (i == 0 || i == sx - 1)) || (c == 1 && (j == 0 || j == sy - 1));
+    const float g = c == 0 ? gx : (c == 1 ? gy : gz);
+    for (int k = fc.k0; k < fc.k1; ++k, f += sxy) {
+        if (wall_ij || (c == 2 && (k == 0 || k == sz - 1))) a[f] = 0.f;
+        else if (add_g) a[f] += g;
+    }
 }
 
-__global__ void k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int nz, bool add_g, float gx, float gy,
-                            float gz)
+__global__ void __launch_bounds__(kTileX * kTileY) k_wall_tail(float* u, float* vv, float* w, int nx, int ny, int nz,
+                                                               bool add_g, float gx, float gy, float gz)
 {
-    wall_tail_body(u, vv, w, nx, ny, nz, add_g, gx, gy, gz, hw_blk3());
+    wall_tail_column(u, vv, w, nx, ny, nz, add_g, gx, gy, gz, hw_blk3());
 }
 
 // ---- flat multi-scene forms (BatchPlan, fe_internal.cuh)
@@ -362,9 +352,6 @@ __global__ void __launch_bounds__(256) k_multi_clear(const BatchPlan* __restrict
         for (uint64_t u = (uint64_t)b * blockDim.x + threadIdx.x; u < nq; u += stride) q[u] = make_uint4(w, w, w, w);
     }
 }
-
-// The face grid of the flat face passes: blocks of kFaceLayers layers.
-__host__ __device__ inline dim3 layer_grid(dim3 fg) { return dim3(fg.x, fg.y, (fg.z + kFaceLayers - 1) / kFaceLayers); }
 
 // Buffers of pass `pass` of a scene's extrapolation group (run_extrap_group's assignment, evaluated per scene):
 // A = (u, v, w), B = (u2, v2, w2); the pre group starts from A and ends in A (even depth) or B (odd); the post
@@ -405,22 +392,18 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_multi_extrap(const BatchPla
     const BatchScene& e = plan->sc[s];
     const SceneView& v = e.dst;
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
-    const dim3 fg = face_grid(nx, ny, nz);
-    Blk3 blk = flat_blk3(b, layer_grid(fg));
-    blk.z *= kFaceLayers;
+    const Blk3 blk = flat_blk3(b, column_grid(nx, ny, nz));
     const int d = v.extrap_depth;
     const float gx = PRE ? e.gdt[0] : 0.f, gy = PRE ? e.gdt[1] : 0.f, gz = PRE ? e.gdt[2] : 0.f;
     if (d <= 0) {
-        if (pass == 0)
-            for (int t = 0; t < kFaceLayers && blk.z + t < fg.z; ++t)
-                wall_tail_body(v.u, v.v, v.w, nx, ny, nz, PRE, gx, gy, gz, Blk3{blk.x, blk.y, blk.z + t});
+        if (pass == 0) wall_tail_column(v.u, v.v, v.w, nx, ny, nz, PRE, gx, gy, gz, blk);
         return;
     }
     if (pass >= d) return;
     FaceArrays fa;
     group_arrays(v, PRE, pass, d, fa);
-    if (pass == d - 1) extrap_layers<PRE ? kModePre : kModePost>(fa, nx, ny, nz, false, gx, gy, gz, blk, fg.z);
-    else extrap_layers<kModePlain>(fa, nx, ny, nz, true, 0.f, 0.f, 0.f, blk, fg.z);
+    if (pass == d - 1) extrap_column<PRE ? kModePre : kModePost>(fa, nx, ny, nz, false, gx, gy, gz, blk);
+    else extrap_column<kModePlain>(fa, nx, ny, nz, true, 0.f, 0.f, 0.f, blk);
 }
 
 // The velocity buffers the pressure stage reads and writes: B after an odd pre group, else A.
@@ -449,10 +432,7 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_multi_apply(const BatchPlan
     const SceneView& v = plan->sc[s].dst;
     float *u, *vv, *w;
     stage_buffers(v, u, vv, w);
-    const dim3 fg = face_grid(v.g.nx, v.g.ny, v.g.nz);
-    Blk3 blk = flat_blk3(b, layer_grid(fg));
-    blk.z *= kFaceLayers;
-    for (int t = 0; t < kFaceLayers && blk.z + t < fg.z; ++t) apply_body(v, u, vv, w, Blk3{blk.x, blk.y, blk.z + t});
+    apply_column(v, u, vv, w, flat_blk3(b, column_grid(v.g.nx, v.g.ny, v.g.nz)));
 }
 
 }  // namespace
@@ -466,7 +446,7 @@ cudaError_t launch_pre(const SceneView& v, double dt, cudaStream_t st)
     float* B[3] = {v.u2, v.v2, v.w2};
     const int d = v.extrap_depth;
     if (d <= 0) {
-        k_wall_tail<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny,
+        k_wall_tail<<<column_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny,
                                                                                       v.g.nz, true, gx, gy, gz);
         count_launch();
         return cudaGetLastError();
@@ -481,7 +461,7 @@ cudaError_t launch_post(const SceneView& v, cudaStream_t st)
     float* B[3] = {v.u2, v.v2, v.w2};
     const int d = v.extrap_depth;
     if (d <= 0) {
-        k_wall_tail<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny,
+        k_wall_tail<<<column_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v.u, v.v, v.w, v.g.nx, v.g.ny,
                                                                                       v.g.nz, false, 0, 0, 0);
         count_launch();
         return cudaGetLastError();
@@ -513,7 +493,7 @@ cudaError_t launch_apply(const SceneView& v, cudaStream_t st)
 {
     const float *u, *vv, *w;
     pressure_buffers(v, u, vv, w);
-    k_apply<<<face_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v, (float*)u, (float*)vv, (float*)w);
+    k_apply<<<column_grid(v.g.nx, v.g.ny, v.g.nz), dim3(kTileX, kTileY), 0, st>>>(v, (float*)u, (float*)vv, (float*)w);
     count_launch();
     return cudaGetLastError();
 }
@@ -551,9 +531,9 @@ uint32_t batch_blocks(const SceneView& v, int kind)
     case kBkClear: return 0;  // set by the plan builder from its clear ranges
     case kBkPart: return (uint32_t)((v.np + 255) / 256);
     case kBkP2g: return v.np > 0 ? (uint32_t)(v.g.tnx * v.g.tny * v.g.tnz) : 0u;
-    case kBkNormalize: return (uint32_t)((faces + 255) / 256);
+    case kBkNormalize: return (uint32_t)((faces + 1023) / 1024);  // four faces per thread
     case kBkFaces: {
-        const dim3 g = layer_grid(face_grid(v.g.nx, v.g.ny, v.g.nz));
+        const dim3 g = column_grid(v.g.nx, v.g.ny, v.g.nz);
         return g.x * g.y * g.z;
     }
     case kBkCells: {

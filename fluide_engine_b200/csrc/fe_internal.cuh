@@ -215,6 +215,32 @@ __device__ __forceinline__ bool face_coord(int nx, int ny, int nz, FaceCoord& fc
     return face_coord(nx, ny, nz, hw_blk3(), fc);
 }
 
+// Column launch over the three face arrays: blocks of 32 x 8 threads tile (i, j) as above, and each thread marches
+// kColumn consecutive faces along z, so values along z are carried from one face to the next and the index advances
+// by one plane per step; grid.z runs over the z chunks of u (nz faces), then v (nz), then w (nz + 1).
+constexpr int kColumn = 8;
+__host__ __device__ inline dim3 column_grid(int nx, int ny, int nz)
+{
+    return dim3((unsigned)((nx + 1 + kTileX - 1) / kTileX), (unsigned)((ny + 1 + kTileY - 1) / kTileY),
+                (unsigned)(2 * ((nz + kColumn - 1) / kColumn) + (nz + 1 + kColumn - 1) / kColumn));
+}
+struct FaceColumn {
+    int c, i, j, k0, k1, sx, sy, sz;
+};
+__device__ __forceinline__ bool column_coord(int nx, int ny, int nz, Blk3 b, FaceColumn& fc)
+{
+    const int cz = (nz + kColumn - 1) / kColumn;
+    int z = (int)b.z;
+    if (z < cz) { fc.c = 0; fc.sx = nx + 1; fc.sy = ny; fc.sz = nz; }
+    else if (z < 2 * cz) { fc.c = 1; z -= cz; fc.sx = nx; fc.sy = ny + 1; fc.sz = nz; }
+    else { fc.c = 2; z -= 2 * cz; fc.sx = nx; fc.sy = ny; fc.sz = nz + 1; }
+    fc.i = (int)(b.x * kTileX + threadIdx.x);
+    fc.j = (int)(b.y * kTileY + threadIdx.y);
+    fc.k0 = z * kColumn;
+    fc.k1 = min(fc.k0 + kColumn, fc.sz);
+    return fc.i < fc.sx && fc.j < fc.sy && fc.k0 < fc.sz;
+}
+
 // Viscosity (fe_diffuse.cu): buffers of the implicit diffusion solve, allocated when a scene's viscosity is > 0.
 // Face arrays are the three components concatenated (u | v | w) like the velocity buffers.
 struct DiffWork {
