@@ -493,8 +493,8 @@ cudaError_t diffuse_prepare(DiffWork& d, int device);
 // built on the host when the membership or dt changes.
 enum BatchKind {
     kBkClear,      // 256 threads: the substep's accumulator / count / marker clears
-    kBkPart,       // 256 threads, one particle each: keys, placement, ranks, marking, transfer and move
-    kBkGather,     // 256 threads, 4 particles each
+    kBkPart,       // 256 threads, one particle each: marking, transfer and move
+    kBkGather,     // 256 threads, 4 particles each: the gather, keys, placement and ranks
     kBkScan,       // 1024 threads, 4096 counts each
     kBkScanSums,   // 1024 threads, one block per scene
     kBkBigcell,    // 1024 threads, striding over the scene's long runs

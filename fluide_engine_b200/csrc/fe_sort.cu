@@ -27,16 +27,44 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
+// The per-particle passes of the sort (keys, placement, ranks) give each thread kSortBatch particles, a block's
+// threads stride over them (coalesced), and issue every particle's loads (and atomics) before the first use, so a
+// thread keeps several round trips in flight: the passes are bound by load and atomic latency.
+constexpr int kSortBatch = 4;
+
 __device__ __forceinline__ void keys_body(const SceneView& v, uint32_t blk)
 {
-    uint64_t i = blk * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= v.np) return;
-    uint32_t key = fe_particle_key(v.px[i], v.py[i], v.pz[i], v.originf, v.inv_hf, v.g.nx, v.g.ny, v.g.nz);
-    v.key[i] = key;
-    v.rank[i] = atomicAdd(v.cell_count + key, 1u);
+    const uint64_t base = (blk * (uint64_t)blockDim.x) * kSortBatch + threadIdx.x;
+    float x[kSortBatch], y[kSortBatch], z[kSortBatch];
+#pragma unroll
+    for (int b = 0; b < kSortBatch; ++b) {
+        const uint64_t i = base + (uint64_t)b * blockDim.x;
+        if (i < v.np) {
+            x[b] = v.px[i];
+            y[b] = v.py[i];
+            z[b] = v.pz[i];
+        }
+    }
+    uint32_t key[kSortBatch], slot[kSortBatch];
+#pragma unroll
+    for (int b = 0; b < kSortBatch; ++b) {
+        const uint64_t i = base + (uint64_t)b * blockDim.x;
+        if (i < v.np) {
+            key[b] = fe_particle_key(x[b], y[b], z[b], v.originf, v.inv_hf, v.g.nx, v.g.ny, v.g.nz);
+            slot[b] = atomicAdd(v.cell_count + key[b], 1u);
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kSortBatch; ++b) {
+        const uint64_t i = base + (uint64_t)b * blockDim.x;
+        if (i < v.np) {
+            v.key[i] = key[b];
+            v.rank[i] = slot[b];
+        }
+    }
 }
 
-__global__ void k_keys(SceneView v) { keys_body(v, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_keys(SceneView v) { keys_body(v, blockIdx.x); }
 
 // Inclusive block scan of one value per thread; returns the block total through *total.
 __device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* warp_sums, uint32_t* total)
@@ -155,34 +183,70 @@ constexpr int kBigCellBlocks = 32;
 
 __device__ __forceinline__ void place_body(const SceneView& v, uint32_t* __restrict__ long_count, uint32_t blk)
 {
-    uint64_t i = blk * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= v.np) return;
-    if (i == 0) *long_count = 0u;  // the long-run list starts empty
-    v.perm[v.cell_start[v.key[i]] + v.rank[i]] = (uint32_t)i;
+    const uint64_t base = (blk * (uint64_t)blockDim.x) * kSortBatch + threadIdx.x;
+    if (base == 0) *long_count = 0u;  // the long-run list starts empty
+    uint32_t key[kSortBatch], slot[kSortBatch], start[kSortBatch];
+#pragma unroll
+    for (int b = 0; b < kSortBatch; ++b) {
+        const uint64_t i = base + (uint64_t)b * blockDim.x;
+        if (i < v.np) {
+            key[b] = v.key[i];
+            slot[b] = v.rank[i];
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kSortBatch; ++b)
+        if (base + (uint64_t)b * blockDim.x < v.np) start[b] = v.cell_start[key[b]];
+#pragma unroll
+    for (int b = 0; b < kSortBatch; ++b) {
+        const uint64_t i = base + (uint64_t)b * blockDim.x;
+        if (i < v.np) v.perm[start[b] + slot[b]] = (uint32_t)i;
+    }
 }
 
-__global__ void k_place(SceneView v, uint32_t* __restrict__ long_count) { place_body(v, long_count, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_place(SceneView v, uint32_t* __restrict__ long_count)
+{
+    place_body(v, long_count, blockIdx.x);
+}
 
 // rank[final slot of particle x] = x (rank's atomic slots were consumed by k_place; perm, the runs in arbitrary
 // order, is only read here).
 __device__ __forceinline__ void cellrank_body(const SceneView& v, uint32_t* __restrict__ long_count, uint32_t blk)
 {
-    uint64_t s = blk * (uint64_t)blockDim.x + threadIdx.x;
-    if (s >= v.np) return;
+    const uint64_t base = (blk * (uint64_t)blockDim.x) * kSortBatch + threadIdx.x;
     const uint32_t* __restrict__ perm = v.perm;
-    const uint32_t x = perm[s];
-    const uint32_t key = v.key[x];
-    const uint32_t b = v.cell_start[key], e = v.cell_start[key + 1];
-    if (e - b > kBigCell) {
-        if (s == b) v.cell_count[atomicAdd(long_count, 1u)] = key;
-        return;
+    uint32_t x[kSortBatch], key[kSortBatch], rb[kSortBatch], re[kSortBatch];
+#pragma unroll
+    for (int q = 0; q < kSortBatch; ++q)
+        if (base + (uint64_t)q * blockDim.x < v.np) x[q] = perm[base + (uint64_t)q * blockDim.x];
+#pragma unroll
+    for (int q = 0; q < kSortBatch; ++q)
+        if (base + (uint64_t)q * blockDim.x < v.np) key[q] = v.key[x[q]];
+#pragma unroll
+    for (int q = 0; q < kSortBatch; ++q)
+        if (base + (uint64_t)q * blockDim.x < v.np) {
+            rb[q] = v.cell_start[key[q]];
+            re[q] = v.cell_start[key[q] + 1];
+        }
+#pragma unroll
+    for (int q = 0; q < kSortBatch; ++q) {
+        const uint64_t s = base + (uint64_t)q * blockDim.x;
+        if (s >= v.np) continue;
+        const uint32_t b = rb[q], e = re[q];
+        if (e - b > kBigCell) {
+            if (s == b) v.cell_count[atomicAdd(long_count, 1u)] = key[q];
+            continue;
+        }
+        uint32_t r = 0;
+        for (uint32_t t = b; t < e; ++t) r += perm[t] < x[q] ? 1u : 0u;
+        v.rank[b + r] = x[q];
     }
-    uint32_t r = 0;
-    for (uint32_t t = b; t < e; ++t) r += perm[t] < x ? 1u : 0u;
-    v.rank[b + r] = x;
 }
 
-__global__ void k_cellrank(SceneView v, uint32_t* __restrict__ long_count) { cellrank_body(v, long_count, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_cellrank(SceneView v, uint32_t* __restrict__ long_count)
+{
+    cellrank_body(v, long_count, blockIdx.x);
+}
 
 // One block per listed long run.  Ascending-only bitonic network (each merge of size k starts with the
 // mirrored comparator i <-> i ^ (k - 1), then half-cleaners of distance k/4 .. 1) over the run padded to
@@ -289,7 +353,7 @@ __global__ void __launch_bounds__(256) k_gather(SceneView src, SceneView dst)
 __global__ void __launch_bounds__(256) k_multi_keys(const BatchPlan* __restrict__ plan)
 {
     uint32_t b;
-    const int s = batch_scene_of(plan, kBkPart, b);
+    const int s = batch_scene_of(plan, kBkGather, b);
     keys_body(plan->sc[s].src, b);
 }
 
@@ -315,14 +379,14 @@ __global__ void __launch_bounds__(kScanThreads) k_multi_scan_sums(const BatchPla
 __global__ void __launch_bounds__(256) k_multi_place(const BatchPlan* __restrict__ plan)
 {
     uint32_t b;
-    const int s = batch_scene_of(plan, kBkPart, b);
+    const int s = batch_scene_of(plan, kBkGather, b);
     place_body(plan->sc[s].src, plan->sc[s].long_count, b);
 }
 
 __global__ void __launch_bounds__(256) k_multi_cellrank(const BatchPlan* __restrict__ plan)
 {
     uint32_t b;
-    const int s = batch_scene_of(plan, kBkPart, b);
+    const int s = batch_scene_of(plan, kBkGather, b);
     cellrank_body(plan->sc[s].src, plan->sc[s].long_count, b);
 }
 
@@ -367,7 +431,7 @@ cudaError_t launch_sort(const SceneView& v, cudaStream_t st, void* scan_tmp, siz
     cudaError_t e = cudaMemsetAsync(v.cell_count, 0, (size_t)K * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const int T = 256;
-    unsigned pb = (unsigned)((v.np + T - 1) / T);
+    const unsigned pb = (unsigned)((v.np + (uint64_t)T * kSortBatch - 1) / ((uint64_t)T * kSortBatch));
     if (v.np > 0) {
         k_keys<<<pb, T, 0, st>>>(v);
         count_launch();
@@ -408,14 +472,14 @@ uint32_t sort_batch_blocks(const SceneView& v, int kind)
 cudaError_t launch_multi_sort(const BatchLaunch& L, cudaStream_t st)
 {
     const BatchPlan* p = L.plan;
-    if (L.total[kBkPart]) k_multi_keys<<<L.total[kBkPart], 256, 0, st>>>(p);
+    if (L.total[kBkPart]) k_multi_keys<<<L.total[kBkGather], 256, 0, st>>>(p);
     k_multi_scan<0><<<L.total[kBkScan], kScanThreads, 0, st>>>(p);
     k_multi_scan_sums<<<L.total[kBkScanSums], kScanThreads, 0, st>>>(p);
     k_multi_scan<2><<<L.total[kBkScan], kScanThreads, 0, st>>>(p);
     count_launch(4);
     if (L.total[kBkPart]) {
-        k_multi_place<<<L.total[kBkPart], 256, 0, st>>>(p);
-        k_multi_cellrank<<<L.total[kBkPart], 256, 0, st>>>(p);
+        k_multi_place<<<L.total[kBkGather], 256, 0, st>>>(p);
+        k_multi_cellrank<<<L.total[kBkGather], 256, 0, st>>>(p);
         k_multi_bigcell<<<L.total[kBkBigcell], 1024, 0, st>>>(p);
         k_multi_gather<<<L.total[kBkGather], 256, 0, st>>>(p);
         count_launch(4);
