@@ -516,6 +516,14 @@ struct G2PArgs {
 };
 G2PArgs g2p_args(const SceneView& v, double dt);
 
+// The marking pass's launch constants (fe_mark.cu): band^2, the largest squared distance whose square root is below r,
+// the window around r in which an inexact cell-centre sample is recomputed, 1 / bucket spacing, and whether every
+// axis' node window around a particle holds at most two nodes (r / h + 1e-6 < 1 on every axis).
+struct MarkConst {
+    double R2, rin2, crit_eps, inv_bucket;
+    int two;
+};
+
 constexpr int kBatchClearRanges = 8;
 struct BatchScene {
     SceneView src;               // particle buffer set the substep starts from (the sort's input)
@@ -529,7 +537,7 @@ struct BatchScene {
     uint32_t clr_val[kBatchClearRanges];
     int nclr;
     float gdt[3];                // dt * gravity, FP32
-    double R2, rin2, crit_eps;   // marking constants (fe_mark.cu)
+    MarkConst mark;              // marking constants (fe_mark.cu)
     G2PArgs g2p;
 };
 struct BatchPlan {
@@ -576,7 +584,7 @@ __device__ __forceinline__ void stage_view(SceneView& dst, const SceneView& src)
 uint32_t batch_blocks(const SceneView& v, int kind);
 uint32_t sort_batch_blocks(const SceneView& v, int kind);
 // launch_mark's constants (fe_mark.cu).
-void mark_constants(const SceneView& v, double* R2, double* rin2, double* crit_eps);
+MarkConst mark_constants(const SceneView& v);
 // Flat launches of one batch substep's passes (fe_sort.cu, fe_p2g.cu, fe_mark.cu, fe_grid.cu, fe_g2p.cu).
 cudaError_t launch_multi_clear(const BatchLaunch& L, cudaStream_t st);
 cudaError_t launch_multi_sort(const BatchLaunch& L, cudaStream_t st);    // keys, scan, placement, ranks, gather

@@ -56,13 +56,70 @@ __device__ __forceinline__ bool visited(const SceneView& v, int pbx, int pby, in
 
 // One thread per particle: the nodes within r of it (2 per axis for cubic cells, where 2r = 1.7 h;
 // more along an axis whose spacing is finer than max(h)) get the reference's exact FP64 test.
-__device__ __forceinline__ void mark_body(const SceneView& v, double R2, double rin2, double crit_eps, uint32_t blk)
+// A node the particle is within band of: FLUID when within r; on grids with inexact cell-centre samples, a node
+// whose distance is within crit_eps of r is listed for the full trilinear sample.
+__device__ __forceinline__ void mark_node(const SceneView& v, const MarkConst& mc, double d2, int i, int j, int k)
+{
+    if (!(d2 <= mc.R2)) return;
+    const size_t c = idx3(i, j, k, v.g.nx, v.g.ny);
+    // sqrt(d2) < r exactly when d2 <= rin2 (correctly rounded sqrt is monotonic): no square root
+    if (d2 <= mc.rin2) v.marks[c] = FE_CELL_FLUID;
+    if (v.any_inexact && !(v.q_exact[0][i] && v.q_exact[1][j] && v.q_exact[2][k]) &&
+        fabs(__dsqrt_rn(d2) - v.radius) <= mc.crit_eps) {
+        unsigned* word = (unsigned*)(v.crit_flag + (c & ~(size_t)3));
+        unsigned bit = 1u << (8 * (c & 3));
+        if (!(atomicOr(word, bit) & bit)) {
+            uint32_t slot = atomicAdd(v.crit_count, 1u);
+            v.crit_list[slot] = (uint32_t)c;
+        }
+    }
+}
+
+// The common case, every axis' node window holding at most two nodes (cubic cells: 2r = 1.7 h): the 2 x 2 x 2
+// candidates are tested without loops, every table load issued first and each node's test predicated, so the
+// lanes of a warp stay converged.  Same nodes, same FP64 expressions and bucket tests as mark_body's loops.
+__device__ __forceinline__ void mark_body2(const SceneView& v, const MarkConst& mc, uint32_t blk)
+{
+    const uint64_t p = blk * (uint64_t)blockDim.x + threadIdx.x;
+    if (p >= v.np) return;
+    const double X[3] = {(double)v.px[p], (double)v.py[p], (double)v.pz[p]};
+    const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
+    int node[3][2];
+    bool ok[3][2];
+    double q[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double t = (X[a] - v.sdf_origin[a]) * v.inv_h[a];
+        const double rr = v.radius * v.inv_h[a] + 1e-6;
+        const int lo = max((int)floor(t - rr) + 1, 0);
+        const int hi = min((int)floor(t + rr), n[a] - 1);
+        const int pb = bucket_fast(X[a], v.bucket, mc.inv_bucket);
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const int idx = min(lo + s, n[a] - 1);  // clamped for the loads; out-of-window nodes are not ok
+            node[a][s] = idx;
+            ok[a][s] = lo + s <= hi && (pb == v.q_b0[a][idx] || pb == v.q_b1[a][idx]);
+            q[a][s] = v.q_pos[a][idx];
+        }
+    }
+#pragma unroll
+    for (int sk = 0; sk < 2; ++sk)
+#pragma unroll
+        for (int sj = 0; sj < 2; ++sj)
+#pragma unroll
+            for (int si = 0; si < 2; ++si)
+                if (ok[2][sk] && ok[1][sj] && ok[0][si])
+                    mark_node(v, mc, dist2_ref(X[0], X[1], X[2], q[0][si], q[1][sj], q[2][sk]), node[0][si],
+                              node[1][sj], node[2][sk]);
+}
+
+__device__ __forceinline__ void mark_body(const SceneView& v, const MarkConst& mc, uint32_t blk)
 {
     uint64_t p = blk * (uint64_t)blockDim.x + threadIdx.x;
     if (p >= v.np) return;
     const double X[3] = {(double)v.px[p], (double)v.py[p], (double)v.pz[p]};
     const int n[3] = {v.g.nx, v.g.ny, v.g.nz};
-    const double inv_bucket = 1.0 / v.bucket;
+    const double inv_bucket = mc.inv_bucket;
     int lo[3], hi[3], pb[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -79,28 +136,16 @@ __device__ __forceinline__ void mark_body(const SceneView& v, double R2, double 
             if (pb[1] != v.q_b0[1][j] && pb[1] != v.q_b1[1][j]) continue;
             for (int i = lo[0]; i <= hi[0]; ++i) {
                 if (pb[0] != v.q_b0[0][i] && pb[0] != v.q_b1[0][i]) continue;
-                const double d2 = dist2_ref(X[0], X[1], X[2], v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]);
-                if (!(d2 <= R2)) continue;
-                const size_t c = idx3(i, j, k, n[0], n[1]);
-                // sqrt(d2) < r exactly when d2 <= rin2 (correctly rounded sqrt is monotonic): no square root
-                if (d2 <= rin2) v.marks[c] = FE_CELL_FLUID;
-                if (v.any_inexact && !(v.q_exact[0][i] && v.q_exact[1][j] && v.q_exact[2][k]) &&
-                    fabs(__dsqrt_rn(d2) - v.radius) <= crit_eps) {
-                    unsigned* word = (unsigned*)(v.crit_flag + (c & ~(size_t)3));
-                    unsigned bit = 1u << (8 * (c & 3));
-                    if (!(atomicOr(word, bit) & bit)) {
-                        uint32_t slot = atomicAdd(v.crit_count, 1u);
-                        v.crit_list[slot] = (uint32_t)c;
-                    }
-                }
+                mark_node(v, mc, dist2_ref(X[0], X[1], X[2], v.q_pos[0][i], v.q_pos[1][j], v.q_pos[2][k]), i, j, k);
             }
         }
     }
 }
 
-__global__ void __launch_bounds__(256) k_mark(SceneView v, double R2, double rin2, double crit_eps)
+__global__ void __launch_bounds__(256) k_mark(SceneView v, MarkConst mc)
 {
-    mark_body(v, R2, rin2, crit_eps, blockIdx.x);
+    if (mc.two) mark_body2(v, mc, blockIdx.x);
+    else mark_body(v, mc, blockIdx.x);
 }
 
 // Band-limited SDF value of node (i, j, k) exactly as BuildSignedDistanceField computes it.
@@ -174,7 +219,8 @@ __global__ void __launch_bounds__(256) k_multi_mark(const BatchPlan* __restrict_
     uint32_t b;
     const int s = batch_scene_of(plan, kBkPart, b);
     const BatchScene& e = plan->sc[s];
-    mark_body(e.dst, e.R2, e.rin2, e.crit_eps, b);
+    if (e.mark.two) mark_body2(e.dst, e.mark, b);
+    else mark_body(e.dst, e.mark, b);
 }
 
 __global__ void __launch_bounds__(128) k_multi_mark_fixup(const BatchPlan* __restrict__ plan)
@@ -184,7 +230,7 @@ __global__ void __launch_bounds__(128) k_multi_mark_fixup(const BatchPlan* __res
     const int s = batch_scene_of(plan, kBkFixup, b);
     const BatchScene& e = plan->sc[s];
     stage_view(v, e.dst);
-    mark_fixup_body(v, e.R2, (uint32_t)((size_t)v.g.nx * v.g.ny * v.g.nz), b,
+    mark_fixup_body(v, e.mark.R2, (uint32_t)((size_t)v.g.nx * v.g.ny * v.g.nz), b,
                     plan->start[kBkFixup][s + 1] - plan->start[kBkFixup][s]);
 }
 
@@ -325,11 +371,17 @@ cudaError_t launch_multi_mark(const BatchLaunch& L, cudaStream_t st)
 
 // The marking constants of launch_mark: band^2, the largest squared distance whose square root is below r, and the
 // window around r in which an inexact cell-centre sample is recomputed.
-void mark_constants(const SceneView& v, double* R2, double* rin2, double* crit_eps)
+MarkConst mark_constants(const SceneView& v)
 {
-    *R2 = v.band * v.band;
-    *rin2 = sqrt_below(v.radius);
-    *crit_eps = 1e-9 * v.radius;
+    MarkConst mc;
+    mc.R2 = v.band * v.band;
+    mc.rin2 = sqrt_below(v.radius);
+    mc.crit_eps = 1e-9 * v.radius;
+    mc.inv_bucket = 1.0 / v.bucket;
+    mc.two = 1;
+    for (int a = 0; a < 3; ++a)  // window (t - rr, t + rr] with rr = r / h_a + 1e-6 holds at most ceil(2 rr) nodes
+        if (!(v.radius * v.inv_h[a] + 1e-6 < 1.0 - 1e-9)) mc.two = 0;
+    return mc;
 }
 
 cudaError_t launch_mark(const SceneView& v, cudaStream_t st)
@@ -337,16 +389,16 @@ cudaError_t launch_mark(const SceneView& v, cudaStream_t st)
     const size_t nc = (size_t)v.g.nx * v.g.ny * v.g.nz;
     cudaError_t e = cudaMemsetAsync(v.marks, FE_CELL_AIR, nc, st);
     if (e != cudaSuccess) return e;
-    const double R2 = v.band * v.band;
+    const MarkConst mc = mark_constants(v);
     if (v.any_inexact) {
         if ((e = cudaMemsetAsync(v.crit_flag, 0, (nc + 3) & ~(size_t)3, st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(v.crit_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     }
     if (v.np > 0) {
-        k_mark<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, R2, sqrt_below(v.radius), 1e-9 * v.radius);
+        k_mark<<<(unsigned)((v.np + 255) / 256), 256, 0, st>>>(v, mc);
         count_launch();
         if (v.any_inexact) {
-            k_mark_fixup<<<148, 128, 0, st>>>(v, R2, (uint32_t)nc);
+            k_mark_fixup<<<148, 128, 0, st>>>(v, mc.R2, (uint32_t)nc);
             count_launch();
         }
     }

@@ -2697,7 +2697,7 @@ fe_status batch_build_plans(fe_batch* b, double dt)
             e.gdt[0] = (float)(dt * v.gravity[0]);
             e.gdt[1] = (float)(dt * v.gravity[1]);
             e.gdt[2] = (float)(dt * v.gravity[2]);
-            mark_constants(v, &e.R2, &e.rin2, &e.crit_eps);
+            e.mark = mark_constants(v);
             e.g2p = g2p_args(v, dt);
             for (int k = 0; k < kBkCount; ++k) {
                 // a block clears 256 threads x 16 B x 8 per pass of its range loop
