@@ -241,10 +241,6 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_multi_cg(MultiCgScene* __r
     }
 }
 
-// One thread splits total_blocks among the scenes before a multi-scene solve: one block each, the rest in
-// proportion to the previous solve's work of the scene (FLUID cells x (inner iterations + 3 residual
-// passes); weight0 before its first solve), leftovers to the heaviest scenes.  Scenes then take about
-// equally long, instead of the scene with the most iterations finishing last on a small share.
 // Relative cost of one inner iteration per FLUID cell: the multigrid body's passes and grid barriers (4 L - 2 per
 // iteration) against the plain body's one.
 __device__ __forceinline__ double multi_work(const MultiCgScene& m)
@@ -254,40 +250,63 @@ __device__ __forceinline__ double multi_work(const MultiCgScene& m)
     return (double)m.last_fluid * ((double)m.last_its * per_it + 3.0);
 }
 
-__global__ void k_multi_partition(MultiCgScene* __restrict__ scenes, int S, int total_blocks)
+// Splits total_blocks among the scenes before a multi-scene solve: one block each, the rest in proportion to the
+// previous solve's work of the scene (FLUID cells x (inner iterations + 3 residual passes); weight0 before its
+// first solve), the leftovers (fewer than S) one each to the scenes with the most work per block.  Scenes then
+// take about equally long, instead of the scene with the most iterations finishing last on a small share.  One
+// thread per scene (S <= kBatchMaxScenes): each scene's work is read once into shared memory, and the ranking of the
+// leftovers runs in parallel, so the split costs a few microseconds rather than S^2 dependent global reads.
+__global__ void __launch_bounds__(kBatchMaxScenes) k_multi_partition(MultiCgScene* __restrict__ scenes, int S,
+                                                                       int total_blocks)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double wsum = 0.0;
-    for (int i = 0; i < S; ++i) {
-        const MultiCgScene& m = scenes[i];
-        wsum += fmax(multi_work(m), 0.0);
+    __shared__ double w[kBatchMaxScenes];
+    __shared__ int cnt[kBatchMaxScenes];
+    __shared__ int start[kBatchMaxScenes];
+    __shared__ double wsum_s;
+    __shared__ int left_s;
+    const int t = threadIdx.x;
+    w[t] = t < S ? fmax(multi_work(scenes[t]), 0.0) : 0.0;
+    __syncthreads();
+    if (t == 0) {
+        double wsum = 0.0;
+        for (int i = 0; i < S; ++i) wsum += w[i];  // in scene order
+        wsum_s = wsum;
     }
+    __syncthreads();
     const int spare = total_blocks - S;
-    int start = 0, used = 0;
-    for (int i = 0; i < S; ++i) {
-        MultiCgScene& m = scenes[i];
-        const double w = fmax(multi_work(m), 0.0);
-        const int extra = wsum > 0.0 ? (int)floor(spare * (w / wsum)) : spare / S;
-        m.block_count = 1 + extra;
-        used += 1 + extra;
+    const double wsum = wsum_s;
+    if (t < S) cnt[t] = 1 + (wsum > 0.0 ? (int)floor(spare * (w[t] / wsum)) : spare / S);
+    __syncthreads();
+    if (t == 0) {
+        int used = 0;
+        for (int i = 0; i < S; ++i) used += cnt[i];
+        left_s = total_blocks - used;
     }
-    // leftovers (fewer than S) one each to the heaviest scenes, heaviest first
-    for (int left = total_blocks - used; left > 0; --left) {
-        int best = -1;
-        double bw = -1.0;
-        for (int i = 0; i < S; ++i) {
-            const MultiCgScene& m = scenes[i];
-            const double w = multi_work(m) / (double)m.block_count;  // work per block: give it where most needed
-            if (w > bw) {
-                bw = w;
-                best = i;
-            }
+    __syncthreads();
+    // rank by work per block, heaviest first, ties to the lower index
+    int rank = S;
+    if (t < S) {
+        const double key = w[t] / (double)cnt[t];
+        rank = 0;
+        for (int j = 0; j < S; ++j) {
+            const double kj = w[j] / (double)cnt[j];
+            rank += (kj > key || (kj == key && j < t)) ? 1 : 0;
         }
-        scenes[best].block_count += 1;
     }
-    for (int i = 0; i < S; ++i) {
-        scenes[i].block_start = start;
-        start += scenes[i].block_count;
+    __syncthreads();  // every rank read the counts before any changes
+    if (t < S && rank < left_s) cnt[t] += 1;
+    __syncthreads();
+    if (t == 0) {
+        int st = 0;
+        for (int i = 0; i < S; ++i) {
+            start[i] = st;
+            st += cnt[i];
+        }
+    }
+    __syncthreads();
+    if (t < S) {
+        scenes[t].block_count = cnt[t];
+        scenes[t].block_start = start[t];
     }
 }
 
@@ -316,7 +335,7 @@ cudaError_t multi_cg_capacity(int device, int* max_blocks, int* threads)
 
 cudaError_t launch_multi_cg(MultiCgScene* scenes, int S, int total_blocks, cudaStream_t st)
 {
-    k_multi_partition<<<1, 32, 0, st>>>(scenes, S, total_blocks);
+    k_multi_partition<<<1, kBatchMaxScenes, 0, st>>>(scenes, S, total_blocks);
     count_launch();
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)total_blocks);
