@@ -591,10 +591,55 @@ def batched_measure(n_scenes=48, steps=50, warmup=5, device=0, batch_family=None
             "gpu_launches": int(launches)}
 
 
+def run_batch_only(args):
+    """The batched workload's scenes stepped as one batch only (no tuning, no one-at-a-time arm): `--batch-flat`
+    scenes' cells or fewer in the flat launches, `--warmup` untimed then `--steps` timed substeps; a profiling
+    target for the batch's launches."""
+    import numpy as np
+    import torch
+
+    import fluide_engine_b200 as fe
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(2)
+    scenes = []
+    for k in range(args.scenes):
+        n = int(rng.choice([32, 48, 64, 96, 128]))
+        ext = rng.uniform(0.2, 0.6, 3)
+        solver = int(rng.integers(0, 3))
+        pos, vel = fe.seed_regions([dict(kind=0, lo=(0.0, 0.0, 0.0), hi=tuple(float(e) for e in ext))], (n, n, n),
+                                   seed=k)
+        sc = fe.Scene((n, n, n), solver=solver, max_cfl=1.0, cg_rel_tol=1e-6, device=0)
+        sc.set_particles(pos, vel)
+        scenes.append(sc)
+    particles = sum(sc.num_particles() for sc in scenes)
+    batch = fe.Batch(scenes)
+    flat = 0 if args.batch_flat is None else args.batch_flat
+    batch.set_flat(flat)
+    if args.warmup:
+        batch.step(DT, args.warmup, stats=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.step(DT, args.steps, stats=False)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    line = {"metric": METRIC, "value": particles * args.steps / t, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / max(args.steps, 1) * 1e3, "workload_kind": "batched-only",
+            "config": {"scenes": args.scenes, "particles_total": particles, "flat_max_cells": flat,
+                       "timing": "wall clock around synchronised device work"}}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for sc in scenes:
+        sc.close()
+    return 0
+
+
 def run_batched(args):
     import torch
 
     torch.cuda.set_device(0)
+    if args.batch_only:
+        return run_batch_only(args)
     b = batched_measure(args.scenes, args.steps, args.warmup)
     line = {"metric": METRIC, "value": b["value"], "unit": METRIC, "n_gpus": 1, "steps": b["steps"],
             "warmup": b["warmup"], "ms_per_step": b["ms_per_step"], "higher_is_better": True,
@@ -800,6 +845,10 @@ def main():
     ap.add_argument("--mesh-init", action="store_true",
                     help="single workload: also time InitializeFromTriangleMesh (GPU and reference CPU)")
     ap.add_argument("--scenes", type=int, default=48, help="batched workload: number of scenes")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="batched workload: step the batch alone (no tuning, no one-at-a-time arm)")
+    ap.add_argument("--batch-flat", type=int, default=None,
+                    help="with --batch-only: scenes of at most this many cells in the flat launches (-1: all)")
     # served: 20 jobs/s as the served configuration, over 6 s instead of 10 min and with resolutions <= 128 so
     # that a run takes tens of seconds; the work still exceeds the arrival window several times (saturated)
     ap.add_argument("--trace-rate", type=float, default=20.0)
