@@ -56,18 +56,64 @@ __device__ __forceinline__ float lerp8(const float c[8], const Stencil& s)
     return lerpf_ref(b0, b1, s.fz);
 }
 
+// GetBarycentric index pair and fraction of a point along one axis of one staggered grid (stencil() per axis).
+struct AxisFrac {
+    int i, ip;
+    float f;
+};
+__device__ __forceinline__ AxisFrac axis_frac(float x, float o, float ih, int size)
+{
+    AxisFrac a;
+    bary((x - o) * ih, size - 1, a.i, a.f);
+    a.ip = min(a.i + 1, size - 1);
+    return a;
+}
+__device__ __forceinline__ Stencil stencil_of(const AxisFrac& a, const AxisFrac& b, const AxisFrac& c)
+{
+    Stencil s;
+    s.i = a.i; s.ip = a.ip; s.fx = a.f;
+    s.j = b.i; s.jp = b.ip; s.fy = b.f;
+    s.k = c.i; s.kp = c.ip; s.fz = c.f;
+    return s;
+}
+
+// The three staggered grids' stencils at one point, as stencil() gives them.  Along each axis the two grids that are
+// not staggered along it have the same data origin (both offset by half a cell, set side by side with the scene:
+// xo[1] == zo[1], yo[0] == zo[0], xo[2] == yo[2], and likewise for the FLIP residual origins) and the same size, so
+// their index and fraction are one computation: 6 per point instead of 9.
+__device__ __forceinline__ void stencils3(float x, float y, float z, const float ou[3], const float ov[3],
+                                          const float ow[3], const float ih[3], int nx, int ny, int nz, Stencil& su,
+                                          Stencil& sv, Stencil& sw)
+{
+    const AxisFrac xf = axis_frac(x, ou[0], ih[0], nx + 1), xc = axis_frac(x, ov[0], ih[0], nx);
+    const AxisFrac yf = axis_frac(y, ov[1], ih[1], ny + 1), yc = axis_frac(y, ou[1], ih[1], ny);
+    const AxisFrac zf = axis_frac(z, ow[2], ih[2], nz + 1), zc = axis_frac(z, ou[2], ih[2], nz);
+    su = stencil_of(xf, yc, zc);
+    sv = stencil_of(xc, yf, zc);
+    sw = stencil_of(xc, yc, zf);
+}
+
+// The grid velocity at a point: the three components' trilinear samples, each stencil built just before its loads
+// (the shared fractions of stencils3 carried from one component to the next).
 __device__ __forceinline__ void sample_vel(const SceneView& v, const FaceSource& fs, float x, float y, float z,
                                            float out[3])
 {
     const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const float* ih = v.inv_hf;
     float c[8];
-    const Stencil su = stencil(x, y, z, v.xo, v.inv_hf, nx + 1, ny, nz);
+    const AxisFrac xf = axis_frac(x, v.xo[0], ih[0], nx + 1);
+    const AxisFrac yc = axis_frac(y, v.xo[1], ih[1], ny);
+    const AxisFrac zc = axis_frac(z, v.xo[2], ih[2], nz);
+    const Stencil su = stencil_of(xf, yc, zc);
     fs.corners(0, su, c);
     out[0] = lerp8(c, su);
-    const Stencil sv = stencil(x, y, z, v.yo, v.inv_hf, nx, ny + 1, nz);
+    const AxisFrac xc = axis_frac(x, v.yo[0], ih[0], nx);
+    const AxisFrac yf = axis_frac(y, v.yo[1], ih[1], ny + 1);
+    const Stencil sv = stencil_of(xc, yf, zc);
     fs.corners(1, sv, c);
     out[1] = lerp8(c, sv);
-    const Stencil sw = stencil(x, y, z, v.zo, v.inv_hf, nx, ny, nz + 1);
+    const AxisFrac zf = axis_frac(z, v.zo[2], ih[2], nz + 1);
+    const Stencil sw = stencil_of(xc, yc, zf);
     fs.corners(2, sw, c);
     out[2] = lerp8(c, sw);
 }
@@ -128,9 +174,8 @@ __device__ __forceinline__ void g2p_particle(const SceneView& v, const G2PArgs& 
     bool have_pic = false;
     if (G2P) {
         if (SOLVER == FE_SOLVER_FLIP) {
-            const Stencil su = stencil(x, y, z, v.rxo, v.inv_hf, nx + 1, ny, nz);
-            const Stencil sv = stencil(x, y, z, v.ryo, v.inv_hf, nx, ny + 1, nz);
-            const Stencil sw = stencil(x, y, z, v.rzo, v.inv_hf, nx, ny, nz + 1);
+            Stencil su, sv, sw;
+            stencils3(x, y, z, v.rxo, v.ryo, v.rzo, v.inv_hf, nx, ny, nz, su, sv, sw);
             const bool share = g.same_origins && v.blend > 0.f;
             float flip[3] = {v.vx[p] + sample_diff(fs, 0, su, share ? &pic[0] : nullptr),
                              v.vy[p] + sample_diff(fs, 1, sv, share ? &pic[1] : nullptr),
