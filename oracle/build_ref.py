@@ -1,8 +1,8 @@
 """Build recipe for oracle/_ref/ -- TEST INFRASTRUCTURE ONLY.
 
 Compiles the reference's own CPU simulator (AleksanderSiwek/Fluide_Engine, src/) from the sources
-where they lie (the reference checkout named by FE_REFERENCE_SRC, else the `reference_path` entry of the
-repository's BASELINE.json, + "/src"), together with oracle/ref_harness.cpp, into two shared
+where they lie (the reference checkout's src/ named by FE_REFERENCE_SRC, else /root/reference/src when that
+exists), together with oracle/ref_harness.cpp, into two shared
 libraries under oracle/_ref/ (git-ignored):
 
 * libfe_ref_serial.so   -- parallel_utils loops run on the calling thread (use_threads=false).  The
@@ -35,18 +35,12 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 def _reference_src():
-    """Reference source tree: $FE_REFERENCE_SRC, else BASELINE.json's reference_path + /src (None if neither)."""
+    """Reference source tree: $FE_REFERENCE_SRC, else the read-only checkout at /root/reference/src (None if neither)."""
     env = os.environ.get("FE_REFERENCE_SRC")
     if env:
         return env
-    try:
-        import json
-
-        with open(os.path.join(os.path.dirname(HERE), "BASELINE.json")) as f:
-            base = json.load(f).get("reference_path")
-    except (OSError, ValueError):
-        base = None
-    return os.path.join(base, "src") if base else None
+    default = "/root/reference/src"
+    return default if os.path.isdir(default) else None
 
 
 REF = _reference_src()

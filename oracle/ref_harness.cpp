@@ -56,7 +56,7 @@ void CudaJacobiIterationSolver::Solve(LinearSystem*) { throw std::runtime_error(
 
 namespace {
 
-// ConjugateGradientSolver with tol = rel * ||b||_2, as BASELINE's "CG to relative residual".
+// ConjugateGradientSolver with tol = rel * ||b||_2: the benchmark scenes' "CG to relative residual".
 struct RelTolCG : public LinearSystemSolver {
     double rel;
     size_t maxIt;
