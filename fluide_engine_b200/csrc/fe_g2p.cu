@@ -134,9 +134,9 @@ __device__ __forceinline__ float sample_diff(const FaceSource& fs, int comp, con
     return lerp8(d, s);
 }
 
-// sum_t gradweight_t * face_t for one velocity component (apic_simulator.cpp:311-336).
-__device__ __forceinline__ void apic_row(const FaceSource& fs, int comp, const Stencil& s, const float ih[3],
-                                         float out[3])
+// sum_t gradweight_t * face_t for one velocity component (apic_simulator.cpp:311-336), from the stencil's 8 corner
+// values.
+__device__ __forceinline__ void apic_row_vals(const float val[8], const Stencil& s, const float ih[3], float out[3])
 {
     const float fx = s.fx, fy = s.fy, fz = s.fz;
     const float gx[8] = {-ih[0] * (1 - fy) * (1 - fz), ih[0] * (1 - fy) * (1 - fz), (-ih[0]) * fy * (1 - fz),
@@ -148,8 +148,6 @@ __device__ __forceinline__ void apic_row(const FaceSource& fs, int comp, const S
     const float gz[8] = {-ih[2] * (1 - fx) * (1 - fy), fx * (1 - fy) * (-ih[2]), (1 - fx) * fy * (-ih[2]),
                          fx * fy * (-ih[2]),           (1 - fx) * (1 - fy) * ih[2], fx * (1 - fy) * ih[2],
                          (1 - fx) * fy * ih[2],        fx * fy * ih[2]};
-    float val[8];
-    fs.corners(comp, s, val);
     float r0 = 0.f, r1 = 0.f, r2 = 0.f;
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
@@ -160,6 +158,64 @@ __device__ __forceinline__ void apic_row(const FaceSource& fs, int comp, const S
     out[0] = r0;
     out[1] = r1;
     out[2] = r2;
+}
+
+__device__ __forceinline__ void apic_row(const FaceSource& fs, int comp, const Stencil& s, const float ih[3],
+                                         float out[3])
+{
+    float val[8];
+    fs.corners(comp, s, val);
+    apic_row_vals(val, s, ih, out);
+}
+
+// APIC: component c's grid sample at the particle (stencil s, the velocity grid's face counts as sizes) and its C row.
+// The row's stencil is taken at the particle clamped by h/2 on the two transverse axes with the CELL counts as sizes;
+// where no clamp moves the particle and its index along the component's own axis is below n - 1 (the two sizes then
+// give the same GetBarycentric result), it is s itself, and the row reuses the sample's 8 corner values.
+__device__ __forceinline__ float apic_component(const SceneView& v, const FaceSource& fs, int c, const Stencil& s,
+                                                const float P[3], const float lo[3], const float hi[3], uint64_t p)
+{
+    float c8[8];
+    fs.corners(c, s, c8);
+    const float pic = lerp8(c8, s);
+    float q[3] = {P[0], P[1], P[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        if (a != c) q[a] = q[a] < lo[a] ? lo[a] : (q[a] > hi[a] ? hi[a] : q[a]);
+    const int n_c = c == 0 ? v.g.nx : (c == 1 ? v.g.ny : v.g.nz);
+    const int i_c = c == 0 ? s.i : (c == 1 ? s.j : s.k);
+    float row[3];
+    if (q[0] == P[0] && q[1] == P[1] && q[2] == P[2] && i_c <= n_c - 2) {
+        apic_row_vals(c8, s, v.inv_hf, row);
+    } else {
+        const float* org = c == 0 ? v.xo : (c == 1 ? v.yo : v.zo);
+        apic_row(fs, c, stencil(q[0], q[1], q[2], org, v.inv_hf, v.g.nx, v.g.ny, v.g.nz), v.inv_hf, row);
+    }
+    v.c[3 * c][p] = row[0];
+    v.c[3 * c + 1][p] = row[1];
+    v.c[3 * c + 2][p] = row[2];
+    return pic;
+}
+
+// APIC's transfer at the particle: the grid velocity (as sample_vel) and the three C rows.
+__device__ __forceinline__ void sample_vel_apic(const SceneView& v, const FaceSource& fs, float x, float y, float z,
+                                                uint64_t p, float out[3])
+{
+    const int nx = v.g.nx, ny = v.g.ny, nz = v.g.nz;
+    const float* ih = v.inv_hf;
+    const float lo[3] = {v.originf[0] + 0.5f * v.hf[0], v.originf[1] + 0.5f * v.hf[1], v.originf[2] + 0.5f * v.hf[2]};
+    const float hi[3] = {v.originf[0] + v.sizef[0] - 0.5f * v.hf[0], v.originf[1] + v.sizef[1] - 0.5f * v.hf[1],
+                         v.originf[2] + v.sizef[2] - 0.5f * v.hf[2]};
+    const float P[3] = {x, y, z};
+    const AxisFrac xf = axis_frac(x, v.xo[0], ih[0], nx + 1);
+    const AxisFrac yc = axis_frac(y, v.xo[1], ih[1], ny);
+    const AxisFrac zc = axis_frac(z, v.xo[2], ih[2], nz);
+    out[0] = apic_component(v, fs, 0, stencil_of(xf, yc, zc), P, lo, hi, p);
+    const AxisFrac xc = axis_frac(x, v.yo[0], ih[0], nx);
+    const AxisFrac yf = axis_frac(y, v.yo[1], ih[1], ny + 1);
+    out[1] = apic_component(v, fs, 1, stencil_of(xc, yf, zc), P, lo, hi, p);
+    const AxisFrac zf = axis_frac(z, v.zo[2], ih[2], nz + 1);
+    out[2] = apic_component(v, fs, 2, stencil_of(xc, yc, zf), P, lo, hi, p);
 }
 
 // The transfer and move of particle p (pic_simulator.cpp:239-312, flip_simulator.cpp:121-161,
@@ -190,33 +246,12 @@ __device__ __forceinline__ void g2p_particle(const SceneView& v, const G2PArgs& 
             vel[1] = flip[1];
             vel[2] = flip[2];
         } else {
-            sample_vel(v, fs, x, y, z, pic);
+            if (SOLVER == FE_SOLVER_APIC) sample_vel_apic(v, fs, x, y, z, p, pic);
+            else sample_vel(v, fs, x, y, z, pic);
             have_pic = true;
             vel[0] = pic[0];
             vel[1] = pic[1];
             vel[2] = pic[2];
-            if (SOLVER == FE_SOLVER_APIC) {
-                const float lo[3] = {v.originf[0] + 0.5f * v.hf[0], v.originf[1] + 0.5f * v.hf[1],
-                                     v.originf[2] + 0.5f * v.hf[2]};
-                const float hi[3] = {v.originf[0] + v.sizef[0] - 0.5f * v.hf[0],
-                                     v.originf[1] + v.sizef[1] - 0.5f * v.hf[1],
-                                     v.originf[2] + v.sizef[2] - 0.5f * v.hf[2]};
-                const float P[3] = {x, y, z};
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    float q[3] = {P[0], P[1], P[2]};
-#pragma unroll
-                    for (int a = 0; a < 3; ++a)
-                        if (a != c) q[a] = q[a] < lo[a] ? lo[a] : (q[a] > hi[a] ? hi[a] : q[a]);
-                    const float* org = c == 0 ? v.xo : (c == 1 ? v.yo : v.zo);
-                    const Stencil s = stencil(q[0], q[1], q[2], org, v.inv_hf, nx, ny, nz);
-                    float row[3];
-                    apic_row(fs, c, s, v.inv_hf, row);
-                    v.c[3 * c][p] = row[0];
-                    v.c[3 * c + 1][p] = row[1];
-                    v.c[3 * c + 2][p] = row[2];
-                }
-            }
         }
     } else {
         vel[0] = v.vx[p];
