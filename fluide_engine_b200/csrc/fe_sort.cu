@@ -289,7 +289,8 @@ __global__ void __launch_bounds__(1024) k_bigcell(SceneView v, const uint32_t* _
 }
 
 // Each thread moves kGatherBatch particles, all their loads issued before any store, so a thread keeps several
-// rows of requests in flight instead of one.
+// rows of requests in flight instead of one.  The source set is read-only during the pass (the two particle buffer
+// sets never alias), so its loads go through the read-only path and may be scheduled ahead of the stores.
 constexpr int kGatherBatch = 4;
 
 template <bool APIC>
@@ -302,20 +303,20 @@ __device__ __forceinline__ void gather_body(const SceneView& src, const SceneVie
     for (int b = 0; b < kGatherBatch; ++b) {
         const uint64_t i = base + (uint64_t)b * blockDim.x;
         ok[b] = i < src.np;
-        j[b] = ok[b] ? src.rank[i] : 0u;  // the sorted order (slot -> particle)
+        j[b] = ok[b] ? __ldg(src.rank + i) : 0u;  // the sorted order (slot -> particle)
     }
     float a[kGatherBatch][6];
     uint32_t id[kGatherBatch];
 #pragma unroll
     for (int b = 0; b < kGatherBatch; ++b) {
         if (!ok[b]) continue;
-        a[b][0] = src.px[j[b]];
-        a[b][1] = src.py[j[b]];
-        a[b][2] = src.pz[j[b]];
-        a[b][3] = src.vx[j[b]];
-        a[b][4] = src.vy[j[b]];
-        a[b][5] = src.vz[j[b]];
-        id[b] = src.pid[j[b]];
+        a[b][0] = __ldg(src.px + j[b]);
+        a[b][1] = __ldg(src.py + j[b]);
+        a[b][2] = __ldg(src.pz + j[b]);
+        a[b][3] = __ldg(src.vx + j[b]);
+        a[b][4] = __ldg(src.vy + j[b]);
+        a[b][5] = __ldg(src.vz + j[b]);
+        id[b] = __ldg(src.pid + j[b]);
     }
 #pragma unroll
     for (int b = 0; b < kGatherBatch; ++b) {
@@ -334,7 +335,7 @@ __device__ __forceinline__ void gather_body(const SceneView& src, const SceneVie
         for (int c = 0; c < 9; ++c) {
             float t[kGatherBatch];
 #pragma unroll
-            for (int b = 0; b < kGatherBatch; ++b) t[b] = ok[b] ? src.c[c][j[b]] : 0.f;
+            for (int b = 0; b < kGatherBatch; ++b) t[b] = ok[b] ? __ldg(src.c[c] + j[b]) : 0.f;
 #pragma unroll
             for (int b = 0; b < kGatherBatch; ++b)
                 if (ok[b]) dst.c[c][base + (uint64_t)b * blockDim.x] = t[b];
