@@ -550,7 +550,6 @@ struct BatchLaunch {
     const BatchPlan* plan;       // device copy
     uint32_t total[kBkCount];
     int max_depth;               // largest extrapolation depth among the scenes
-    bool any_particles;
 };
 
 // The block's scene and its block index inside that scene's share of a kind's launch.  Every lane of the block's

@@ -2706,7 +2706,6 @@ fe_status batch_build_plans(fe_batch* b, double dt)
                 P.start[k][i + 1] = P.start[k][i] + n;
             }
             L.max_depth = std::max(L.max_depth, v.extrap_depth);
-            L.any_particles |= v.np > 0;
         }
         for (int k = 0; k < kBkCount; ++k) L.total[k] = P.start[k][F];
         L.plan = b->plan_dev[q];
