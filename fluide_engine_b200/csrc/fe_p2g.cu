@@ -78,15 +78,15 @@ __device__ __forceinline__ P2gParticle<SOLVER> load_particle(const SceneView& v,
                                                              float z, const float lo[3], const float hi[3])
 {
     P2gParticle<SOLVER> q;
-    q.vc = c == 0 ? v.vx[p] : (c == 1 ? v.vy[p] : v.vz[p]);
+    q.vc = __ldg((c == 0 ? v.vx : (c == 1 ? v.vy : v.vz)) + p);
     q.pc[0] = x;
     q.pc[1] = y;
     q.pc[2] = z;
     q.cr[0] = q.cr[1] = q.cr[2] = 0.f;
     if (SOLVER == FE_SOLVER_APIC) {
-        q.cr[0] = v.c[3 * c][p];
-        q.cr[1] = v.c[3 * c + 1][p];
-        q.cr[2] = v.c[3 * c + 2][p];
+        q.cr[0] = __ldg(v.c[3 * c] + p);
+        q.cr[1] = __ldg(v.c[3 * c + 1] + p);
+        q.cr[2] = __ldg(v.c[3 * c + 2] + p);
         // Clamp(val, max, min) on the two transverse axes (apic_simulator.cpp:55-57,68-70,81-83)
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -274,7 +274,7 @@ __device__ __forceinline__ void cell_component(const SceneView& v, uint32_t pb, 
     for (int t = 0; t < nslots<C>(); ++t) num[t] = den[t] = 0.f;
     mask = 0;
     for (uint32_t p = pb; p < pe; p += stride) {
-        const float x = v.px[p], y = v.py[p], z = v.pz[p];
+        const float x = __ldg(v.px + p), y = __ldg(v.py + p), z = __ldg(v.pz + p);  // read-only during P2G
         const Stencil s = stencil(x, y, z, k.org, v.inv_hf, k.csx, k.csy, k.csz);
         const P2gParticle<SOLVER> q = load_particle<SOLVER>(v, p, C, x, y, z, lo, hi);
         if (!splat_slots<SOLVER, C>(v, k, s, q, cx, cy, cz, num, den, mask))

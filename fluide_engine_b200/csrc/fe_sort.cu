@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(256) k_place(SceneView v, uint32_t* __restrict
 }
 
 // rank[final slot of particle x] = x (rank's atomic slots were consumed by k_place; perm, the runs in arbitrary
-// order, is only read here).
+// order, key and cell_start are only read here, through the read-only path).
 __device__ __forceinline__ void cellrank_body(const SceneView& v, uint32_t* __restrict__ long_count, uint32_t blk)
 {
     const uint64_t base = (blk * (uint64_t)blockDim.x) * kSortBatch + threadIdx.x;
@@ -218,15 +218,15 @@ __device__ __forceinline__ void cellrank_body(const SceneView& v, uint32_t* __re
     uint32_t x[kSortBatch], key[kSortBatch], rb[kSortBatch], re[kSortBatch];
 #pragma unroll
     for (int q = 0; q < kSortBatch; ++q)
-        if (base + (uint64_t)q * blockDim.x < v.np) x[q] = perm[base + (uint64_t)q * blockDim.x];
+        if (base + (uint64_t)q * blockDim.x < v.np) x[q] = __ldg(perm + base + (uint64_t)q * blockDim.x);
 #pragma unroll
     for (int q = 0; q < kSortBatch; ++q)
-        if (base + (uint64_t)q * blockDim.x < v.np) key[q] = v.key[x[q]];
+        if (base + (uint64_t)q * blockDim.x < v.np) key[q] = __ldg(v.key + x[q]);
 #pragma unroll
     for (int q = 0; q < kSortBatch; ++q)
         if (base + (uint64_t)q * blockDim.x < v.np) {
-            rb[q] = v.cell_start[key[q]];
-            re[q] = v.cell_start[key[q] + 1];
+            rb[q] = __ldg(v.cell_start + key[q]);
+            re[q] = __ldg(v.cell_start + key[q] + 1);
         }
 #pragma unroll
     for (int q = 0; q < kSortBatch; ++q) {
@@ -238,7 +238,7 @@ __device__ __forceinline__ void cellrank_body(const SceneView& v, uint32_t* __re
             continue;
         }
         uint32_t r = 0;
-        for (uint32_t t = b; t < e; ++t) r += perm[t] < x[q] ? 1u : 0u;
+        for (uint32_t t = b; t < e; ++t) r += __ldg(perm + t) < x[q] ? 1u : 0u;
         v.rank[b + r] = x[q];
     }
 }
